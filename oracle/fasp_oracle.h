@@ -1,0 +1,101 @@
+/*
+ * fasp_oracle.h -- CPU ORACLE for the iterative-solve path. TEST INFRASTRUCTURE ONLY.
+ *
+ * This header is shared by two interchangeable CPU back ends that tests load side by side:
+ *   - liboracle_port.so  : fasp_oracle.c, a plain-C restatement of the FASP++ algorithms
+ *                          (each function cites the reference file:line it follows);
+ *   - _ref/liboracle_ref.so : ref_shim.cxx linked against the FASP++ sources compiled from
+ *                          their own tree (build_ref.sh), used to pin the restatement.
+ * Only tests/, __graft_entry__.smoke() and bench.py (its CPU-baseline leg and the
+ * reference arm) may load either library, and only as the checker or the timed CPU
+ * baseline -- never as part of the product path.
+ *
+ * Index arrays are 32-bit unsigned, like the reference's USI. values == NULL means a
+ * pattern-only matrix (MAT.cxx:420-451 treats every stored entry as 1).
+ */
+#ifndef FASP_ORACLE_H
+#define FASP_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Solver kinds; numbers follow SOLType (src/Param.hxx:36-54). GMRES_LEFT is the
+ * left-preconditioned GMRES::LSolve (src/GMRES.cxx:283-453). */
+enum {
+    ORC_IDENTITY   = 0,
+    ORC_CG         = 1,
+    ORC_BICGSTAB   = 2,
+    ORC_GMRES      = 4,
+    ORC_FGMRES     = 5,
+    ORC_JACOBI     = 11,
+    ORC_MG         = 21,
+    ORC_GMRES_LEFT = 104
+};
+
+/* Mirrors SOLParams (src/Param.hxx:57-80) minus the name/verbosity fields. */
+typedef struct {
+    uint32_t maxIter, minIter, savIter, restart;
+    double   relTol, absTol;
+} orc_params_t;
+
+typedef struct {
+    int          alg;        /* ORC_* above */
+    orc_params_t prm;        /* the solver's own SOLParams */
+    double       weight;     /* Jacobi weight when alg == ORC_JACOBI (Iter.hxx:45) */
+    uint32_t     maxRestart, minRestart; /* GMRES/FGMRES::SetMaxMinRestart; 0,0 = 30,10 */
+    int          pcd;        /* preconditioner: 0 identity, 1 Jacobi */
+    double       pcdWeight;
+    orc_params_t pcdPrm;     /* the Jacobi preconditioner's SOLParams */
+    uint32_t     mgLevels;   /* MG: number of coarse levels (TestMG.cxx:80) */
+    uint32_t     mgCycles;   /* MG: SetNumCycles (MG.cxx:19-23) */
+    double       mgSmoothWeight, mgCoarseWeight;
+    orc_params_t mgSmoothPrm, mgCoarsePrm;
+} orc_config_t;
+
+/* SOLParams() defaults (src/Param.hxx:68-79). */
+void orc_default_params(orc_params_t* p);
+void orc_default_config(orc_config_t* c, int alg);
+
+/* A solver object bound to one CSRx matrix: the Setup(...) of the reference. The
+ * arrays are copied. Returns NULL on a bad config. */
+void* orc_create(const orc_config_t* cfg, uint32_t nrow, uint32_t mcol, uint32_t nnz,
+                 const uint32_t* rowPtr, const uint32_t* colInd, const double* values);
+
+/* Solve(b, x): x is the initial guess in and the solution out. hist[k] receives the
+ * residual norm the solver holds at the end of iteration k (k = 0..numIter, entries the
+ * solver never computes are NaN). Returns the FaspRetCode. */
+int orc_solve(void* h, const double* b, double* x, uint32_t* numIter, double* norm2,
+              double* normInf, double* hist, uint32_t histCap);
+
+/* Clean(): reset work vectors (FGMRES Z basis included). */
+void orc_clean(void* h);
+void orc_destroy(void* h);
+
+/* Elementary operators on a CSRx matrix given by arrays. */
+void   orc_spmv(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
+                const double* values, const double* x, double* y);
+void   orc_residual(uint32_t nrow, uint32_t mcol, const uint32_t* rowPtr,
+                    const uint32_t* colInd, const double* values, const double* b,
+                    const double* x, double* r);
+double orc_dot(uint32_t n, const double* a, const double* b);
+double orc_norm2(uint32_t n, const double* a);
+double orc_norminf(uint32_t n, const double* a);
+/* MAT::TransInPlace: (nrow x mcol) -> (mcol x nrow); outputs sized mcol+1, nnz, nnz, mcol. */
+void   orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+                     const uint32_t* colInd, const double* values, uint32_t* tRowPtr,
+                     uint32_t* tColInd, double* tValues, uint32_t* tDiagPtr);
+/* MAT::FormDiagPtr */
+void   orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
+                   uint32_t* diagPtr);
+
+/* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
+int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
+                       uint32_t* colInd, double* values);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

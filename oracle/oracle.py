@@ -1,0 +1,210 @@
+"""CPU ORACLE loader -- test infrastructure only.
+
+Loads one of the two CPU back ends that share fasp_oracle.h:
+
+* ``port`` -- ``liboracle_port.so``, the plain-C restatement (fasp_oracle.c);
+* ``ref``  -- ``_ref/liboracle_ref.so``, the FASP++ sources compiled from their own tree
+  by build_ref.sh, with the shim in ref_shim.cxx.
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py`` (CPU baseline and reference arm)
+import this module, as the checker or the timed CPU baseline. The GPU library never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle_port.so")
+REF_SO = os.path.join(HERE, "_ref", "liboracle_ref.so")
+
+# Solver kinds (fasp_oracle.h; SOLType numbers, src/Param.hxx:36-54).
+IDENTITY, CG, BICGSTAB, GMRES, FGMRES, JACOBI, MG, GMRES_LEFT = 0, 1, 2, 4, 5, 11, 21, 104
+ALG_BY_NAME = {"cg": CG, "bicgstab": BICGSTAB, "gmres": GMRES, "fgmres": FGMRES,
+               "jacobi": JACOBI, "mg": MG, "gmres_left": GMRES_LEFT}
+
+
+class Params(C.Structure):
+    _fields_ = [("maxIter", C.c_uint32), ("minIter", C.c_uint32), ("savIter", C.c_uint32),
+                ("restart", C.c_uint32), ("relTol", C.c_double), ("absTol", C.c_double)]
+
+
+class Config(C.Structure):
+    _fields_ = [("alg", C.c_int), ("prm", Params), ("weight", C.c_double),
+                ("maxRestart", C.c_uint32), ("minRestart", C.c_uint32),
+                ("pcd", C.c_int), ("pcdWeight", C.c_double), ("pcdPrm", Params),
+                ("mgLevels", C.c_uint32), ("mgCycles", C.c_uint32),
+                ("mgSmoothWeight", C.c_double), ("mgCoarseWeight", C.c_double),
+                ("mgSmoothPrm", Params), ("mgCoarsePrm", Params)]
+
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool = True) -> None:
+    """Compile the restatement (and the reference, when its tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle_port.so"], check=True)
+    if ref and os.path.isdir("/root/reference/src"):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+_LIBS: dict = {}
+
+
+def load(kind: str = "port") -> C.CDLL:
+    if kind in _LIBS:
+        return _LIBS[kind]
+    path = PORT_SO if kind == "port" else REF_SO
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library {path} is not built")
+    lib = C.CDLL(path)
+    lib.orc_default_params.argtypes = [C.POINTER(Params)]
+    lib.orc_default_config.argtypes = [C.POINTER(Config), C.c_int]
+    lib.orc_create.restype = C.c_void_p
+    lib.orc_create.argtypes = [C.POINTER(Config), C.c_uint32, C.c_uint32, C.c_uint32,
+                               _u32p, _u32p, C.c_void_p]
+    lib.orc_solve.restype = C.c_int
+    lib.orc_solve.argtypes = [C.c_void_p, _f64p, _f64p, C.POINTER(C.c_uint32),
+                              C.POINTER(C.c_double), C.POINTER(C.c_double), _f64p, C.c_uint32]
+    lib.orc_clean.argtypes = [C.c_void_p]
+    lib.orc_destroy.argtypes = [C.c_void_p]
+    lib.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, C.c_void_p, _f64p, _f64p]
+    lib.orc_residual.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p,
+                                 _f64p]
+    for f in ("orc_dot",):
+        getattr(lib, f).restype = C.c_double
+        getattr(lib, f).argtypes = [C.c_uint32, _f64p, _f64p]
+    for f in ("orc_norm2", "orc_norminf"):
+        getattr(lib, f).restype = C.c_double
+        getattr(lib, f).argtypes = [C.c_uint32, _f64p]
+    lib.orc_transpose.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p, C.c_void_p,
+                                  _u32p, _u32p, C.c_void_p, C.c_void_p]
+    lib.orc_diagptr.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
+    _LIBS[kind] = lib
+    return lib
+
+
+def _vptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class Result:
+    code: int
+    x: np.ndarray
+    iters: int
+    norm2: float
+    normInf: float
+    hist: np.ndarray = field(repr=False)
+
+
+def make_config(lib, alg: str, maxIter=1, minIter=0, savIter=100000, restart=30, relTol=1e-6,
+                absTol=1e-8, weight=1.0, maxRestart=0, minRestart=0, pcd=None, pcdWeight=1.0,
+                pcdIter=1, pcdMinIter=None, pcdRelTol=1e-6, pcdAbsTol=1e-8, mgLevels=3,
+                mgCycles=1, mgSmooth=None, mgCoarse=None) -> Config:
+    cfg = Config()
+    lib.orc_default_config(C.byref(cfg), ALG_BY_NAME[alg])
+    cfg.prm.maxIter, cfg.prm.minIter, cfg.prm.savIter = maxIter, minIter, savIter
+    cfg.prm.restart, cfg.prm.relTol, cfg.prm.absTol = restart, relTol, absTol
+    cfg.weight = weight
+    cfg.maxRestart, cfg.minRestart = maxRestart, minRestart
+    cfg.pcd = 1 if pcd == "jacobi" else 0
+    cfg.pcdWeight = pcdWeight
+    cfg.pcdPrm.maxIter = pcdIter
+    cfg.pcdPrm.minIter = pcdIter if pcdMinIter is None else pcdMinIter
+    cfg.pcdPrm.relTol, cfg.pcdPrm.absTol = pcdRelTol, pcdAbsTol
+    cfg.mgLevels, cfg.mgCycles = mgLevels, mgCycles
+    for name, spec in (("mgSmooth", mgSmooth), ("mgCoarse", mgCoarse)):
+        if spec:
+            prm = getattr(cfg, name + "Prm")
+            for k, v in spec.items():
+                if k == "weight":
+                    setattr(cfg, name + "Weight", v)
+                else:
+                    setattr(prm, k, v)
+    return cfg
+
+
+class Solver:
+    """One oracle solver object (the reference's Setup), reusable across solves."""
+
+    def __init__(self, kind: str, mat, alg: str, **kw):
+        self.lib = load(kind)
+        self.cfg = make_config(self.lib, alg, **kw)
+        rp, ci, va, n, m = mat.rowPtr, mat.colInd, mat.values, mat.nrow, mat.mcol
+        self._keep = (rp, ci, va)
+        self.n, self.m = n, m
+        self.h = self.lib.orc_create(C.byref(self.cfg), n, m, len(ci), rp, ci, _vptr(va))
+        if not self.h:
+            raise ValueError("oracle rejected the configuration")
+        self.histCap = self.cfg.prm.maxIter + 2
+
+    def solve(self, b, x0) -> Result:
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x0, dtype=np.float64, copy=True)
+        hist = np.empty(self.histCap, dtype=np.float64)
+        it, n2, ni = C.c_uint32(), C.c_double(), C.c_double()
+        code = self.lib.orc_solve(self.h, b, x, C.byref(it), C.byref(n2), C.byref(ni), hist,
+                                  self.histCap)
+        return Result(code, x, it.value, n2.value, ni.value, hist[: it.value + 1].copy())
+
+    def clean(self):
+        self.lib.orc_clean(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.orc_destroy(self.h)
+            self.h = None
+
+
+def solve(kind, mat, alg, b, x0, **kw) -> Result:
+    return Solver(kind, mat, alg, **kw).solve(b, x0)
+
+
+def spmv(kind, mat, x):
+    lib = load(kind)
+    y = np.empty(mat.nrow, dtype=np.float64)
+    lib.orc_spmv(mat.nrow, mat.rowPtr, mat.colInd, _vptr(mat.values),
+                 np.ascontiguousarray(x, dtype=np.float64), y)
+    return y
+
+
+def residual(kind, mat, b, x):
+    lib = load(kind)
+    r = np.empty(mat.nrow, dtype=np.float64)
+    lib.orc_residual(mat.nrow, mat.mcol, mat.rowPtr, mat.colInd, mat.values,
+                     np.ascontiguousarray(b, np.float64), np.ascontiguousarray(x, np.float64), r)
+    return r
+
+
+def dot(kind, a, b):
+    a = np.ascontiguousarray(a, np.float64)
+    return load(kind).orc_dot(len(a), a, np.ascontiguousarray(b, np.float64))
+
+
+def norm2(kind, a):
+    a = np.ascontiguousarray(a, np.float64)
+    return load(kind).orc_norm2(len(a), a)
+
+
+def norminf(kind, a):
+    a = np.ascontiguousarray(a, np.float64)
+    return load(kind).orc_norminf(len(a), a)
+
+
+def transpose(kind, mat):
+    """MAT::TransInPlace: returns (rowPtr, colInd, values, diagPtr) of the transpose."""
+    lib = load(kind)
+    nnz = len(mat.colInd)
+    trp = np.empty(mat.mcol + 1, np.uint32)
+    tci = np.empty(nnz, np.uint32)
+    tva = None if mat.values is None else np.empty(nnz, np.float64)
+    tdp = np.empty(mat.mcol, np.uint32)
+    lib.orc_transpose(mat.nrow, mat.mcol, nnz, mat.rowPtr, mat.colInd, _vptr(mat.values),
+                      trp, tci, _vptr(tva), tdp.ctypes.data_as(C.c_void_p))
+    return trp, tci, tva, tdp

@@ -1,0 +1,383 @@
+/*
+ * ref_shim.cxx -- exposes the FASP++ reference solvers through the oracle C API
+ * (fasp_oracle.h). TEST INFRASTRUCTURE ONLY: it is compiled together with the reference
+ * sources by build_ref.sh into _ref/liboracle_ref.so, so that tests can run the real
+ * reference next to the C restatement and the GPU library on the same inputs.
+ *
+ * The residual history comes from the reference's own iteration table: the main solver
+ * runs with verbose = PRINT_MAX (SOL::PrintInfo prints every iteration when
+ * verbose > PRINT_SOME, src/SOL.cxx:46-64), std::cout is captured during Solve, and
+ * each "iter | resRel | resAbs |" row fills hist[iter]. Those values carry the
+ * 6 significant digits the reference prints.
+ */
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "BiCGStab.hxx"
+#include "CG.hxx"
+#include "FGMRES.hxx"
+#include "GMRES.hxx"
+#include "Iter.hxx"
+#include "MAT.hxx"
+#include "MG.hxx"
+#include "ReadData.hxx"
+#include "VEC.hxx"
+
+#include "fasp_oracle.h"
+
+namespace {
+
+struct RefHandle {
+    orc_config_t           cfg;
+    MAT                    mat;
+    SOL*                   sol = nullptr;
+    SOL*                   pcd = nullptr;
+    std::vector<Jacobi*>   levelSolvers;
+    std::vector<IdentityMatrix*> transfers;
+    std::string            log;
+};
+
+void apply_params(SOL& s, const orc_params_t& p, Output verbose)
+{
+    s.SetOutput(verbose);
+    s.SetMaxIter(p.maxIter);
+    s.SetMinIter(p.minIter);
+    s.SetSavIter(p.savIter);
+    s.SetRestart(p.restart);
+    s.SetRelTol(p.relTol);
+    s.SetAbsTol(p.absTol);
+}
+
+Jacobi* make_jacobi(const orc_params_t& p, double w, const MAT& A)
+{
+    Jacobi* j = new Jacobi();
+    apply_params(*j, p, PRINT_NONE);
+    j->SetWeight(w);
+    j->Setup(A);
+    return j;
+}
+
+} // namespace
+
+extern "C" {
+
+void orc_default_params(orc_params_t* p)
+{
+    SOLParams d;
+    p->maxIter = d.maxIter;
+    p->minIter = d.minIter;
+    p->savIter = d.savIter;
+    p->restart = d.restart;
+    p->relTol  = d.relTol;
+    p->absTol  = d.absTol;
+}
+
+void orc_default_config(orc_config_t* c, int alg)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->alg = alg;
+    orc_default_params(&c->prm);
+    c->weight = 1.0;
+    c->pcdWeight = 1.0;
+    orc_default_params(&c->pcdPrm);
+    c->mgLevels = 3;
+    c->mgCycles = 1;
+    c->mgSmoothWeight = 1.0;
+    c->mgCoarseWeight = 1.0;
+    orc_default_params(&c->mgSmoothPrm);
+    orc_default_params(&c->mgCoarsePrm);
+}
+
+void* orc_create(const orc_config_t* cfg, uint32_t nrow, uint32_t mcol, uint32_t nnz,
+                 const uint32_t* rowPtr, const uint32_t* colInd, const double* values)
+{
+    if (!cfg || nrow == 0 || mcol == 0 || nnz == 0) return nullptr;
+    RefHandle* h = new RefHandle();
+    h->cfg = *cfg;
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    if (values) {
+        std::vector<DBL> va(values, values + nnz);
+        h->mat = MAT(nrow, mcol, nnz, va, ci, rp);
+    } else {
+        h->mat = MAT(nrow, mcol, nnz, ci, rp);
+    }
+    const Output loud = PRINT_MAX;
+
+    if (cfg->pcd == 1)
+        h->pcd = make_jacobi(cfg->pcdPrm, cfg->pcdWeight, h->mat);
+    else
+        h->pcd = new Identity();
+
+    std::ostringstream sink; // Setup prints parameters at this verbosity
+    std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
+    switch (cfg->alg) {
+        case ORC_CG: {
+            CG* s = new CG();
+            apply_params(*s, cfg->prm, loud);
+            s->SetupPCD(*h->pcd);
+            s->Setup(h->mat);
+            h->sol = s;
+            break;
+        }
+        case ORC_BICGSTAB: {
+            BiCGStab* s = new BiCGStab();
+            apply_params(*s, cfg->prm, loud);
+            s->SetupPCD(*h->pcd);
+            s->Setup(h->mat);
+            h->sol = s;
+            break;
+        }
+        case ORC_GMRES:
+        case ORC_GMRES_LEFT: {
+            GMRES* s = new GMRES();
+            apply_params(*s, cfg->prm, loud);
+            if (cfg->maxRestart) s->SetMaxMinRestart(cfg->maxRestart, cfg->minRestart);
+            if (cfg->alg == ORC_GMRES_LEFT) s->SetLeftPrecond();
+            s->SetupPCD(*h->pcd);
+            s->Setup(h->mat);
+            h->sol = s;
+            break;
+        }
+        case ORC_FGMRES: {
+            FGMRES* s = new FGMRES();
+            apply_params(*s, cfg->prm, loud);
+            if (cfg->maxRestart) s->SetMaxMinRestart(cfg->maxRestart, cfg->minRestart);
+            s->SetupPCD(*h->pcd);
+            s->Setup(h->mat);
+            h->sol = s;
+            break;
+        }
+        case ORC_JACOBI: {
+            Jacobi* s = new Jacobi();
+            apply_params(*s, cfg->prm, loud);
+            s->SetWeight(cfg->weight);
+            s->Setup(h->mat);
+            h->sol = s;
+            break;
+        }
+        case ORC_MG: {
+            MG<MAT>* s = new MG<MAT>();
+            apply_params(*s, cfg->prm, loud);
+            const USI L = cfg->mgLevels;
+            s->SetupALL(h->mat, L);
+            for (USI i = 0; i < L; ++i) {
+                IdentityMatrix* t = new IdentityMatrix(h->mat.GetRowSize());
+                Jacobi* sm = make_jacobi(cfg->mgSmoothPrm, cfg->mgSmoothWeight, h->mat);
+                Jacobi* co = make_jacobi(cfg->mgCoarsePrm, cfg->mgCoarseWeight, h->mat);
+                h->transfers.push_back(t);
+                h->levelSolvers.push_back(sm);
+                h->levelSolvers.push_back(co);
+                s->SetupLevel(h->mat, i, t, sm, co);
+            }
+            s->SetNumCycles(cfg->mgCycles);
+            h->sol = s;
+            break;
+        }
+        default:
+            break;
+    }
+    std::cout.rdbuf(old);
+    if (!h->sol) {
+        delete h->pcd;
+        delete h;
+        return nullptr;
+    }
+    return h;
+}
+
+int orc_solve(void* hv, const double* b, double* x, uint32_t* numIter, double* norm2,
+              double* normInf, double* hist, uint32_t histCap)
+{
+    RefHandle* h = static_cast<RefHandle*>(hv);
+    const USI nrow = h->mat.GetRowSize(), mcol = h->mat.GetColSize();
+    VEC vb(nrow, b), vx(mcol, x);
+    std::ostringstream cap;
+    std::streambuf* old = std::cout.rdbuf(cap.rdbuf());
+    const FaspRetCode code = h->sol->Solve(vb, vx);
+    std::cout.rdbuf(old);
+    h->log = cap.str();
+    for (USI i = 0; i < mcol; ++i) x[i] = vx[i];
+    if (numIter) *numIter = h->sol->GetIterations();
+    if (norm2) *norm2 = h->sol->GetNorm2();
+    if (normInf) *normInf = h->sol->GetInfNorm();
+    for (uint32_t k = 0; k < histCap; ++k) hist[k] = NAN;
+    std::istringstream in(h->log);
+    std::string line;
+    while (std::getline(in, line)) {
+        unsigned it;
+        double rr, ra;
+        if (std::sscanf(line.c_str(), "%u | %lf | %lf |", &it, &rr, &ra) == 3 && it < histCap)
+            hist[it] = ra;
+    }
+    return static_cast<int>(code);
+}
+
+void orc_clean(void* hv)
+{
+    RefHandle* h = static_cast<RefHandle*>(hv);
+    if (h->cfg.alg == ORC_GMRES || h->cfg.alg == ORC_GMRES_LEFT ||
+        h->cfg.alg == ORC_FGMRES || h->cfg.alg == ORC_CG || h->cfg.alg == ORC_BICGSTAB)
+        h->sol->Clean();
+}
+
+void orc_destroy(void* hv)
+{
+    RefHandle* h = static_cast<RefHandle*>(hv);
+    if (!h) return;
+    /* SOL has no virtual destructor (src/SOL.hxx:54): delete through the real type. */
+    switch (h->cfg.alg) {
+        case ORC_CG: delete static_cast<CG*>(h->sol); break;
+        case ORC_BICGSTAB: delete static_cast<BiCGStab*>(h->sol); break;
+        case ORC_GMRES:
+        case ORC_GMRES_LEFT: delete static_cast<GMRES*>(h->sol); break;
+        case ORC_FGMRES: delete static_cast<FGMRES*>(h->sol); break;
+        case ORC_JACOBI: delete static_cast<Jacobi*>(h->sol); break;
+        case ORC_MG: delete static_cast<MG<MAT>*>(h->sol); break;
+        default: break;
+    }
+    if (h->cfg.pcd == 1)
+        delete static_cast<Jacobi*>(h->pcd);
+    else
+        delete static_cast<Identity*>(h->pcd);
+    for (auto* j : h->levelSolvers) delete j;
+    for (auto* t : h->transfers) delete t;
+    delete h;
+}
+
+void orc_spmv(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
+              const double* values, const double* x, double* y)
+{
+    const uint32_t nnz = rowPtr[nrow];
+    uint32_t mcol = 0;
+    for (uint32_t k = 0; k < nnz; ++k) mcol = colInd[k] + 1 > mcol ? colInd[k] + 1 : mcol;
+    if (mcol < nrow) mcol = nrow;
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    MAT A;
+    if (values) {
+        std::vector<DBL> va(values, values + nnz);
+        A = MAT(nrow, mcol, nnz, va, ci, rp);
+    } else {
+        A = MAT(nrow, mcol, nnz, ci, rp);
+    }
+    VEC vx(mcol, x), vy(nrow, 0.0);
+    A.Apply(vx, vy);
+    for (uint32_t i = 0; i < nrow; ++i) y[i] = vy[i];
+}
+
+void orc_residual(uint32_t nrow, uint32_t mcol, const uint32_t* rowPtr,
+                  const uint32_t* colInd, const double* values, const double* b,
+                  const double* x, double* r)
+{
+    const uint32_t nnz = rowPtr[nrow];
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    std::vector<DBL> va(values, values + nnz);
+    MAT A(nrow, mcol, nnz, va, ci, rp);
+    VEC vb(nrow, b), vx(mcol, x), vr(nrow, 0.0);
+    A.Residual(vb, vx, vr);
+    for (uint32_t i = 0; i < nrow; ++i) r[i] = vr[i];
+}
+
+double orc_dot(uint32_t n, const double* a, const double* b)
+{
+    VEC va(n, a), vb(n, b);
+    return va.Dot(vb);
+}
+
+double orc_norm2(uint32_t n, const double* a)
+{
+    VEC va(n, a);
+    return va.Norm2();
+}
+
+double orc_norminf(uint32_t n, const double* a)
+{
+    VEC va(n, a);
+    return va.NormInf();
+}
+
+void orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+                   const uint32_t* colInd, const double* values, uint32_t* tRowPtr,
+                   uint32_t* tColInd, double* tValues, uint32_t* tDiagPtr)
+{
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    MAT A;
+    if (values) {
+        std::vector<DBL> va(values, values + nnz);
+        A = MAT(nrow, mcol, nnz, va, ci, rp);
+    } else {
+        A = MAT(nrow, mcol, nnz, ci, rp);
+    }
+    A.TransInPlace();
+    int* trp = A.GetRowPtr();
+    int* tci = A.GetColInd();
+    for (uint32_t i = 0; i <= mcol; ++i) tRowPtr[i] = (uint32_t)trp[i];
+    for (uint32_t k = 0; k < nnz; ++k) tColInd[k] = (uint32_t)tci[k];
+    delete[] trp;
+    delete[] tci;
+    if (values && tValues) {
+        double* tv = A.GetValues();
+        for (uint32_t k = 0; k < nnz; ++k) tValues[k] = tv[k];
+        delete[] tv;
+    }
+    if (tDiagPtr) {
+        /* MAT keeps diagPtr private; FormDiagPtr's search is restated here. */
+        for (uint32_t j = 0; j < mcol; ++j) {
+            tDiagPtr[j] = 0;
+            for (uint32_t k = tRowPtr[j]; k < tRowPtr[j + 1]; ++k)
+                if (tColInd[k] == j) {
+                    tDiagPtr[j] = k;
+                    break;
+                }
+        }
+    }
+}
+
+void orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
+                 uint32_t* diagPtr)
+{
+    for (uint32_t j = 0; j < nrow; ++j) {
+        diagPtr[j] = 0;
+        for (uint32_t k = rowPtr[j]; k < rowPtr[j + 1]; ++k)
+            if (colInd[k] == j) {
+                diagPtr[j] = k;
+                break;
+            }
+    }
+}
+
+/* ReadMat (src/ReadData.cxx:361-446) of a .csr/.mtx file: call once with NULL arrays to
+ * get nrow and nnz, then with arrays of those sizes. Returns the FaspRetCode. */
+int orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
+                    uint32_t* colInd, double* values)
+{
+    MAT A;
+    std::ostringstream sink;
+    std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
+    const FaspRetCode code = ReadMat(path, A);
+    std::cout.rdbuf(old);
+    if (code < 0) return static_cast<int>(code);
+    *nrow = A.GetRowSize();
+    *nnz = A.GetNNZ();
+    if (rowPtr && colInd && values) {
+        int* rp = A.GetRowPtr();
+        int* ci = A.GetColInd();
+        double* va = A.GetValues();
+        for (uint32_t i = 0; i <= *nrow; ++i) rowPtr[i] = (uint32_t)rp[i];
+        for (uint32_t k = 0; k < *nnz; ++k) {
+            colInd[k] = (uint32_t)ci[k];
+            values[k] = va[k];
+        }
+        delete[] rp;
+        delete[] ci;
+        delete[] va;
+    }
+    return static_cast<int>(code);
+}
+
+} // extern "C"
+
