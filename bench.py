@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark: time to an FP64 relative residual of 1e-8 on the 3D 7-point Poisson problem
+(128^3 grid, n = 2,097,152, nnz = 14,581,760), Jacobi-preconditioned CG (weight 1, one
+sweep), mixed precision (FP32 inner CG inside FP64 refinement) against plain FP64 CG on
+the same B200, plus SpMV GB/s. One JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one complete solve from x0 = 0 of A x = b, b = A x*, x* ~ U[0,1) (seed 42).
+`value` is the device time of the mixed-precision solve (CUDA events on the solver's
+stream, inputs resident in HBM); `e2e` the same solve through the host entry point with
+b and x0 copied in from pinned host memory and x copied back every step. Under torchrun
+every rank solves its own replica of the system (the single system does not shard) and
+the slowest rank's time is reported. `--impl reference` times the FASP++ reference
+(compiled from its own sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 128
+METRIC = ("Time-to-1e-8 FP64 residual, 128³ Poisson CG: mixed vs FP64 on B200; "
+          "SpMV GB/s")
+REL_TOL = 1e-8
+MAX_ITER = 3000
+
+
+def problem(ngrid: int):
+    from faspxx_b200 import problems as P
+    A = P.poisson3d(ngrid)
+    xs = P.seeded_uniform(A.nrow, 42)
+    b = A.matvec(xs)
+    return A, b
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+        return False
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
+        loaded = [s for s in sm if s > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def dist_max(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---- CPU reference / baseline ---------------------------------------------------------
+
+def reference_sample(A, b, sample_iters: int, kind: str = "ref"):
+    """Time `sample_iters` Jacobi-PCG iterations of the CPU oracle (the reference compiled
+    from its own sources when kind == 'ref') from x0 = 0; returns ms per iteration."""
+    from oracle import oracle as O
+    kw = dict(maxIter=sample_iters, minIter=0, relTol=1e-300, absTol=0.0, pcd="jacobi",
+              pcdWeight=1.0, pcdIter=1)
+    s = O.Solver(kind, A, "cg", **kw)
+    x0 = np.zeros(A.nrow)
+    t = time.perf_counter()
+    r = s.solve(b, x0)
+    dt = time.perf_counter() - t
+    return dt * 1e3 / max(1, r.iters), r.iters
+
+
+def reference_full(A, b, kind: str = "ref"):
+    from oracle import oracle as O
+    s = O.Solver(kind, A, "cg", maxIter=MAX_ITER, minIter=0, relTol=REL_TOL, absTol=0.0,
+                 pcd="jacobi", pcdWeight=1.0, pcdIter=1)
+    t = time.perf_counter()
+    r = s.solve(b, np.zeros(A.nrow))
+    return (time.perf_counter() - t) * 1e3, r.iters, r.code
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    kind = "ref" if os.path.exists(O.REF_SO) else "port"
+    A, b = problem(args.size)
+    full_ms, iters, code = reference_full(A, b, kind)
+    sample = args.ref_sample
+    for _ in range(args.warmup):
+        reference_sample(A, b, 2, kind)
+    per_iter = [reference_sample(A, b, sample, kind)[0] for _ in range(args.steps)]
+    value = statistics.median(per_iter) * iters
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(value, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3D Poisson 7-point {args.size}^3, Jacobi-PCG, rtol 1e-8",
+                   "n": A.nrow, "nnz": A.nnz, "solver": "FASP++ CG + Jacobi(w=1, 1 sweep)"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": 1,
+                         "kind": "reference" if kind == "ref" else "port",
+                         "sample": f"{sample} PCG iterations per step, time per iteration x "
+                                   f"{iters} iterations to rtol 1e-8 (one full calibration "
+                                   f"solve took {full_ms:.0f} ms, code {code}); the solve "
+                                   f"path is serial"},
+        "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "full_solve_ms": round(full_ms, 1), "iterations": iters,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- GPU arm ------------------------------------------------------------------------
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    dist = dist_init(ws)
+    from faspxx_b200 import capi, sol
+    capi.init(local)
+    lib = capi.lib
+    A, b = problem(args.size)
+    n, nnz = A.nrow, A.nnz
+    M = sol.MAT(A)
+    lanes = M.Autotune()
+
+    def make(precision):
+        s = sol.CG()
+        s.SetMaxIter(MAX_ITER)
+        s.SetMinIter(0)
+        s.SetRelTol(REL_TOL)
+        s.SetAbsTol(0.0)
+        p = sol.Jacobi(1.0)
+        p.SetMaxIter(1)
+        p.SetMinIter(1)
+        s.SetupPCD(p)
+        if precision == capi.MIXED:
+            s.SetPrecision(capi.MIXED, innerRelTol=args.inner_tol, maxOuter=50)
+        s.Setup(M)
+        return s
+
+    mixed, fp64 = make(capi.MIXED), make(capi.FP64)
+    db = sol.DVec.from_numpy(b)
+    dx = sol.DVec(n)
+
+    def solve(s):
+        dx.Scale(0.0)  # x0 = 0 on the device
+        code = s.Solve(db, dx)
+        if code != 0:
+            raise RuntimeError(f"solve failed with code {code}")
+        return s.LastTimeMs(), s.info.numIter, s.info.launches, s.info.outerIter
+
+    for _ in range(args.warmup):
+        solve(mixed)
+        solve(fp64)
+
+    # accuracy of each variant: FP64 residual and error against an FP64 CG solve to 1e-13
+    tight = make(capi.FP64)
+    tight.SetRelTol(1e-13)
+    dx.Scale(0.0)
+    tight.Solve(db, dx)
+    xref = dx.numpy()
+    del tight
+
+    def accuracy(s):
+        solve(s)
+        x = dx.numpy()
+        r = b - A.matvec(x)
+        return (float(np.linalg.norm(r) / np.linalg.norm(b)),
+                float(np.linalg.norm(x - xref) / np.linalg.norm(xref)))
+
+    acc_mixed, acc_fp64 = accuracy(mixed), accuracy(fp64)
+
+    lib.fasp_gpu_synchronize()
+    barrier(dist)
+    with ClockSampler(local) as clk:
+        times, its, launches, outer = [], [], 0, 0
+        for _ in range(args.steps):
+            t, it, la, ou = solve(mixed)
+            times.append(t)
+            its.append(it)
+            launches += la + 1
+            outer = ou
+        lib.fasp_gpu_synchronize()
+        times64, its64 = [], []
+        for _ in range(args.steps):
+            t, it, la, _ = solve(fp64)
+            times64.append(t)
+            its64.append(it)
+        lib.fasp_gpu_synchronize()
+    barrier(dist)
+    clocks = clk.summary()
+    mixed_ms = dist_max(dist, statistics.mean(times))
+    fp64_ms = dist_max(dist, statistics.mean(times64))
+
+    # end to end: host b, x0 in pinned memory -> device -> solve -> x back to host
+    hb = C.c_void_p()
+    hx = C.c_void_p()
+    capi.check(lib.fasp_gpu_host_alloc(C.byref(hb), n * 8), "host_alloc")
+    capi.check(lib.fasp_gpu_host_alloc(C.byref(hx), n * 8), "host_alloc")
+    bh = np.ctypeslib.as_array((C.c_double * n).from_address(hb.value))
+    xh = np.ctypeslib.as_array((C.c_double * n).from_address(hx.value))
+    bh[:] = b
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        xh[:] = 0.0
+        lib.fasp_gpu_synchronize()
+        t0 = time.perf_counter()
+        code = lib.fasp_gpu_solver_solve_host(mixed.h, hb, hx, C.byref(mixed.info))
+        t1 = time.perf_counter()
+        if code != 0 or mixed.info.code != 0:
+            raise RuntimeError("end-to-end solve failed")
+        if i >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = dist_max(dist, statistics.mean(e2e))
+    e2e_err = float(np.linalg.norm(xh - xref) / np.linalg.norm(xref))
+    lib.fasp_gpu_host_free(hb)
+    lib.fasp_gpu_host_free(hx)
+
+    # kernel rooflines (each kernel alone, CUDA events on the library's stream)
+    hbm, peak_kind = peaks()
+    km = (C.c_double * 2)()
+    capi.check(lib.fasp_gpu_solver_kernel_times(mixed.h, 50, km), "kernel_times")
+    k64 = (C.c_double * 2)()
+    capi.check(lib.fasp_gpu_solver_kernel_times(fp64.h, 50, k64), "kernel_times")
+    sp = C.c_double()
+    capi.check(lib.fasp_gpu_mat_time_apply(M.h, 50, 0, C.byref(sp)), "time_apply")
+    # algorithmic bytes per launch (compulsory traffic)
+    b_spmv32 = 8 * nnz + 4 * (n + 1) + 4 * n * 4   # vals+cols, rowPtr, read z,p_old write p,q
+    b_upd32 = 4 * n * 5 + 4 * n * 3                 # read p,x,r,q,dinv write x,r,z
+    b_spmv64 = 12 * nnz + 4 * (n + 1) + 8 * n * 4
+    b_upd64 = 8 * n * 5 + 8 * n * 3
+    b_apply = 12 * nnz + 4 * (n + 1) + 16 * n
+    gbs = lambda byt, ms: byt / (ms * 1e-3) / 1e9  # noqa: E731
+    ach = gbs(b_spmv32, km[0])
+    roofline = {"kernel": "cg_spmv<float> (SpMV + p update + (Ap,p), FP32 inner CG)",
+                "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 3), "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "bytes_per_launch": b_spmv32, "ms_per_launch": round(km[0], 5)}
+    kernels = {
+        "cg_spmv_f32": {"ms": round(km[0], 5), "gbs": round(gbs(b_spmv32, km[0]), 1)},
+        "cg_update_f32": {"ms": round(km[1], 5), "gbs": round(gbs(b_upd32, km[1]), 1)},
+        "cg_spmv_f64": {"ms": round(k64[0], 5), "gbs": round(gbs(b_spmv64, k64[0]), 1)},
+        "cg_update_f64": {"ms": round(k64[1], 5), "gbs": round(gbs(b_upd64, k64[1]), 1)},
+        "spmv_f64_apply": {"ms": round(sp.value, 5), "gbs": round(gbs(b_apply, sp.value), 1),
+                           "frac": round(gbs(b_apply, sp.value) / hbm, 3)},
+    }
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            kind = "ref" if os.path.exists(O.REF_SO) else "port"
+            per_iter, _ = reference_sample(A, b, args.ref_sample, kind)
+            cpu = {"value": round(per_iter * statistics.median(its64), 1), "unit": "ms",
+                   "cores": 1, "kind": "reference" if kind == "ref" else "port",
+                   "sample": f"{args.ref_sample} Jacobi-PCG iterations of the reference on "
+                             f"this problem, time per iteration x {statistics.median(its64)} "
+                             f"iterations (the FP64 iteration count); serial solve path"}
+        except Exception as exc:  # the baseline must not sink the GPU line
+            cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(mixed_ms, 3), "unit": "ms", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mixed_ms, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"3D Poisson 7-point {args.size}^3 (n={n}, nnz={nnz}), "
+                                   f"Jacobi-PCG, FP64 rtol 1e-8, x0=0, b=A x*, x*~U[0,1)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (FP32 matrix 125 MB + vectors)",
+                       "spmv_lanes_per_row": lanes,
+                       "inner_rel_tol": args.inner_tol},
+            "fp64_ms": round(fp64_ms, 3), "mixed_over_fp64": round(mixed_ms / fp64_ms, 3),
+            "iterations": {"mixed_inner_total": int(statistics.median(its)),
+                           "mixed_outer": outer, "fp64": int(statistics.median(its64))},
+            "accuracy": {"mixed_rel_residual": acc_mixed[0], "mixed_err_vs_fp64_1e-13": acc_mixed[1],
+                         "fp64_rel_residual": acc_fp64[0], "fp64_err_vs_fp64_1e-13": acc_fp64[1],
+                         "e2e_err_vs_fp64_1e-13": e2e_err},
+            "spmv_gbs": kernels["spmv_f64_apply"]["gbs"],
+            "roofline": roofline, "kernels": kernels,
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * 8 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=N_GRID)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--ref-sample", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,598 @@
+// cg.cu -- kernels and engine of the device-driven PCG (see cg.cuh).
+//
+// One iteration is two fused kernels:
+//   cg_spmv   ax = A p with p = z + beta p_old formed on the fly for every gathered
+//             entry (the XPAY of CG.cxx:233 folded into the SpMV), p written once for the
+//             owned rows, and the partials of (ax, p) (CG.cxx:101-104);
+//   cg_update x += alpha p, r -= alpha ax, z = diagInv .* r, with the partials of
+//             (r,r), (z,r), (x,x), max|x| and (p,p) (CG.cxx:122-133,141-152,224-228).
+// The last block of each kernel reduces the partials in a fixed order and runs the
+// scalar part of CG::Solve on one thread. Branches that need more vector work than these
+// two kernels do (breakdown, safe-guard copy, stagnation restart, false-convergence check)
+// set status = kEsc and are finished by the host, which then relaunches cg_resume.
+#include <cstring>
+
+#include "cg.cuh"
+
+namespace fb {
+
+#define GRID_STRIDE(i, n) \
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)(n); \
+         i += (size_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void cg_rec(CGCtl* c, unsigned k, double v)
+{
+    const unsigned g = k + c->histOffset;
+    if (c->hist && g < c->histCap) c->hist[g] = v * c->histScale;
+}
+
+__device__ __forceinline__ void cg_done(CGCtl* c, int code)
+{
+    c->code = code;
+    c->status = kDone;
+}
+
+__device__ __forceinline__ void cg_esc(CGCtl* c, int reason, int phase, const double* red)
+{
+    for (int k = 0; k < 5; ++k) c->red[k] = red[k];
+    c->reason = reason;
+    c->phase = phase;
+    c->status = kEsc;
+}
+
+// while (numIter < maxIter) + the minIter check at the top of the loop (CG.cxx:82-91).
+__device__ void cg_looptop(CGCtl* c, double rr)
+{
+    if (c->numIter >= c->maxIter) {
+        cg_done(c, c->code);
+        return;
+    }
+    if (c->numIter == c->minIter) {
+        const double resAbs = sqrt(rr);
+        c->resAbs = resAbs;
+        c->resAbsOld = resAbs;
+        c->denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+        c->resRel = resAbs / c->denAbs;
+        cg_rec(c, c->numIter, resAbs);
+        if (c->inner ? (c->resRel < c->innerTol) : (c->resRel < c->relTol || resAbs < c->absTol))
+            cg_done(c, c->code);
+    }
+}
+
+// Prepare for the next iteration (CG.cxx:219-234), then the next loop top.
+__device__ void cg_prepare_next(CGCtl* c, double zr, double rr)
+{
+    if (c->numIter < c->maxIter) {
+        c->resAbsOld = c->resAbs;
+        const double beta = zr / c->tmpa;
+        c->tmpa = zr;
+        c->beta = beta;
+        c->pmode = c->pzero ? 0 : 1;
+        c->pzero = 0;
+    }
+    cg_looptop(c, rr);
+}
+
+// CG.cxx:99-119: ++numIter, then alpha = tmpa / (ax, p) unless |(ax, p)| <= 1e-40.
+__device__ void cg_after_spmv(CGCtl* c, double tmpb)
+{
+    c->numIter += 1;
+    c->tmpb = tmpb;
+    if (fabs(tmpb) > kCloseZero * kCloseZero)
+        c->alpha = c->tmpa / tmpb;
+    else if (c->inner)
+        cg_done(c, kErrDivZero);
+    else {
+        const double red[5] = {0, 0, 0, 0, 0};
+        cg_esc(c, kBreakdown, 0, red);
+    }
+}
+
+// CG.cxx:130-216 from `phase` on; red = {rr, zr, xx, max|x|, pp} of the updated vectors.
+__device__ void cg_checks(CGCtl* c, const double* red, int phase)
+{
+    if (c->inner) {
+        const double resAbs = sqrt(red[0]);
+        c->resAbs = resAbs;
+        c->resRel = resAbs / c->denAbs;
+        cg_rec(c, c->numIter, resAbs);
+        if (c->resRel < c->innerTol) {
+            cg_done(c, kOk);
+            return;
+        }
+        cg_prepare_next(c, red[1], red[0]);
+        return;
+    }
+    const unsigned it = c->numIter;
+    if (it >= c->minIter) {
+        if (phase <= 0) {
+            c->resAbs = sqrt(red[0]);
+            c->resRel = c->resAbs / c->denAbs;
+            c->ratio = c->resAbs / c->resAbsOld;
+            if (it >= c->savIter && c->resAbs < c->resAbsOld) {
+                cg_esc(c, kSave, 1, red);
+                return;
+            }
+        }
+        if (phase <= 1 && c->ratio > kKsmChkRatio) {
+            if (red[3] < kCloseZero) { // Check I: x vanishes
+                cg_rec(c, it, c->resAbs);
+                cg_done(c, kErrSolStag);
+                return;
+            }
+            const double xRelDiff = fabs(c->alpha) * sqrt(red[4]) / sqrt(red[2]);
+            if ((c->stagStep <= kMaxStagNum) && (xRelDiff < c->solStagTol)) { // Check II
+                c->xRelDiff = xRelDiff;
+                cg_esc(c, kStag, 2, red);
+                return;
+            }
+        }
+        if (phase <= 2 && c->resRel < c->relTol) { // Check III: confirm with b - A x
+            cg_esc(c, kCheck3, 3, red);
+            return;
+        }
+        cg_rec(c, it, c->resAbs);
+    }
+    cg_prepare_next(c, red[1], red[0]);
+}
+
+// ---- kernels ---------------------------------------------------------------------------
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restrict__ z,
+                                                  T* P0, T* P1, T* __restrict__ q, CGCtl* c,
+                                                  Scratch s)
+{
+    if (c->status != kRun) return;
+    const int mode = c->pmode, par = c->par;
+    const T beta = (T)c->beta;
+    const T* __restrict__ pOld = par ? P1 : P0;
+    T* __restrict__ pNew = par ? P0 : P1;
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    T acc = T(0);
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t row = base + sub;
+        T sum = T(0);
+        if (row < A.nrow) {
+            const uint32_t b = A.rowPtr[row], e = A.rowPtr[row + 1];
+            for (uint32_t k = b + lane; k < e; k += L) {
+                const uint32_t j = A.colInd[k];
+                const T pj = mode ? fma(beta, pOld[j], z[j]) : z[j];
+                sum = fma(A.val[k], pj, sum);
+            }
+        }
+        sum = group_sum<L>(sum);
+        if (lane == 0 && row < A.nrow) {
+            const T pi = mode ? fma(beta, pOld[row], z[row]) : z[row];
+            pNew[row] = pi;
+            q[row] = sum;
+            acc = fma(sum, pi, acc);
+        }
+    }
+    double a[1] = {(double)acc};
+    const int ops[1] = {kSum};
+    grid_reduce<1>(a, ops, s, [=] __device__(const double* t) {
+        c->par = par ^ 1;
+        if (!c->bench) cg_after_spmv(c, t[0]);
+    });
+}
+
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kBlock) cg_update(uint32_t n, T* __restrict__ x,
+                                                    T* __restrict__ r, T* __restrict__ z,
+                                                    const T* P0, const T* P1,
+                                                    const T* __restrict__ q,
+                                                    const T* __restrict__ dinv, CGCtl* c,
+                                                    Scratch s)
+{
+    if (c->status != kRun) return;
+    const T alpha = (T)c->alpha;
+    const T* __restrict__ p = c->par ? P1 : P0;
+    T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
+    GRID_STRIDE(i, n)
+    {
+        const T pi = p[i];
+        const T xi = fma(alpha, pi, x[i]);
+        const T ri = fma(-alpha, q[i], r[i]);
+        x[i] = xi;
+        r[i] = ri;
+        T zi = ri;
+        if (JAC) {
+            zi = dinv[i] * ri;
+            z[i] = zi;
+        }
+        rr = fma(ri, ri, rr);
+        zr = fma(zi, ri, zr);
+        xx = fma(xi, xi, xx);
+        xm = fmax(xm, fabs(xi));
+        pp = fma(pi, pi, pp);
+    }
+    double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
+    const int ops[5] = {kSum, kSum, kSum, kMax, kSum};
+    grid_reduce<5>(a, ops, s, [=] __device__(const double* t) {
+        if (!c->bench) cg_checks(c, t, 0);
+    });
+}
+
+// Start of CG::Solve after rk = b - A x (CG.cxx:69-79): z = B(r), tmpa = (z, r), p = z.
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kBlock) cg_start(uint32_t n, const T* __restrict__ r,
+                                                   T* __restrict__ z, const T* __restrict__ dinv,
+                                                   CGCtl* c, Scratch s)
+{
+    T rr = 0, zr = 0;
+    GRID_STRIDE(i, n)
+    {
+        const T ri = r[i];
+        T zi = ri;
+        if (JAC) {
+            zi = dinv[i] * ri;
+            z[i] = zi;
+        }
+        rr = fma(ri, ri, rr);
+        zr = fma(zi, ri, zr);
+    }
+    double a[2] = {(double)rr, (double)zr};
+    const int ops[2] = {kSum, kSum};
+    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+        c->status = kRun;
+        c->numIter = 0;
+        c->code = kOk;
+        c->tmpa = t[1];
+        c->pmode = 0;
+        c->pzero = 0;
+        c->resAbs = 1.0;
+        c->resRel = 1.0;
+        c->denAbs = 1.0;
+        c->ratio = 0.0;
+        c->resAbsOld = 1.0;
+        c->alpha = 0.0;
+        cg_looptop(c, t[0]);
+    });
+}
+
+// After the host finished an escalated branch (r may have been recomputed): z = B(r), then
+// the control flow continues at c->phase with fresh (r,r), (z,r).
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restrict__ r,
+                                                    T* __restrict__ z,
+                                                    const T* __restrict__ dinv, CGCtl* c,
+                                                    Scratch s)
+{
+    T rr = 0, zr = 0;
+    GRID_STRIDE(i, n)
+    {
+        const T ri = r[i];
+        T zi = ri;
+        if (JAC) {
+            zi = dinv[i] * ri;
+            z[i] = zi;
+        }
+        rr = fma(ri, ri, rr);
+        zr = fma(zi, ri, zr);
+    }
+    double a[2] = {(double)rr, (double)zr};
+    const int ops[2] = {kSum, kSum};
+    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+        const double red[5] = {t[0], t[1], c->red[2], c->red[3], c->red[4]};
+        c->status = kRun;
+        c->reason = kNoReason;
+        cg_checks(c, red, c->phase);
+    });
+}
+
+// ---- engine ------------------------------------------------------------------------------
+
+static int spmv_grid_cg(const Ctx& c, uint32_t nrow, int L)
+{
+    long long g = ((long long)nrow * L + kBlock - 1) / kBlock;
+    long long cap = (long long)c.nsm * 16;
+    if (cap > kMaxGrid) cap = kMaxGrid;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+template <typename T>
+static CSRView<T> view_of(const Mat& A);
+template <>
+CSRView<double> view_of<double>(const Mat& A) { return A.v64(); }
+template <>
+CSRView<float> view_of<float>(const Mat& A) { return A.v32(); }
+
+template <typename T>
+int CGEngine<T>::launch_iter()
+{
+    const CSRView<T> V = view_of<T>(*A);
+    const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
+    const int g2 = c->grid(n, kBlock);
+    const T* zz = jacobi ? z : r;
+    if (!capturing) c->launches += 2;
+    switch (A->lanes) {
+        case 1: cg_spmv<T, 1><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        case 2: cg_spmv<T, 2><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        case 4: cg_spmv<T, 4><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        case 8: cg_spmv<T, 8><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        case 16: cg_spmv<T, 16><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        default: cg_spmv<T, 32><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+    }
+    if (jacobi)
+        cg_update<T, 1><<<g2, kBlock, 0, c->stream>>>(n, x, r, z, P0, P1, q, dinv, ctl, c->red);
+    else
+        cg_update<T, 0><<<g2, kBlock, 0, c->stream>>>(n, x, r, r, P0, P1, q, dinv, ctl, c->red);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int CGEngine<T>::launch_init()
+{
+    const int g2 = c->grid(n, kBlock);
+    ++c->launches;
+    if (jacobi)
+        cg_start<T, 1><<<g2, kBlock, 0, c->stream>>>(n, r, z, dinv, ctl, c->red);
+    else
+        cg_start<T, 0><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int CGEngine<T>::launch_resume()
+{
+    const int g2 = c->grid(n, kBlock);
+    ++c->launches;
+    if (jacobi)
+        cg_resume<T, 1><<<g2, kBlock, 0, c->stream>>>(n, r, z, dinv, ctl, c->red);
+    else
+        cg_resume<T, 0><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int CGEngine<T>::push_ctl()
+{
+    FB_CUDA(cudaMemcpyAsync(ctl, hctl, sizeof(CGCtl), cudaMemcpyHostToDevice, c->stream));
+    return kOk;
+}
+
+template <typename T>
+int CGEngine<T>::pull_ctl()
+{
+    FB_CUDA(cudaMemcpyAsync(hctl, ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost, c->stream));
+    FB_CUDA(cudaStreamSynchronize(c->stream));
+    return kOk;
+}
+
+template <typename T>
+int CGEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph)
+{
+    c = ctx;
+    A = M;
+    n = M->nrow;
+    jacobi = jac;
+    dinv = dinvv;
+    useGraph = graph;
+    const size_t bytes = ((size_t)n + 4) * sizeof(T);
+    if (cudaMalloc(&x, bytes) || cudaMalloc(&r, bytes) || cudaMalloc(&q, bytes) ||
+        cudaMalloc(&P0, bytes) || cudaMalloc(&P1, bytes) ||
+        (jacobi && cudaMalloc(&z, bytes)) || cudaMalloc(&ctl, sizeof(CGCtl)) ||
+        cudaMallocHost(&hctl, sizeof(CGCtl)) || cudaMallocHost(&hstatus, sizeof(int))) {
+        cudaGetLastError();
+        destroy();
+        return kErrAlloc;
+    }
+    if (!jacobi) z = r;
+    std::memset(hctl, 0, sizeof(CGCtl));
+    hctl->histScale = 1.0;
+    FB_CUDA(cudaMemsetAsync(P0, 0, bytes, c->stream));
+    FB_CUDA(cudaMemsetAsync(P1, 0, bytes, c->stream));
+    if (useGraph) {
+        // itersPerGraph iterations + a status read-back, captured once; kernels read every
+        // scalar from the control block, so the graph never needs updating.
+        cudaGraph_t g;
+        FB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        for (int i = 0; i < itersPerGraph; ++i) launch_iter();
+        capturing = false;
+        cudaMemcpyAsync(hstatus, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        FB_CUDA(cudaStreamEndCapture(c->stream, &g));
+        FB_CUDA(cudaGraphInstantiate(&gexec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    return kOk;
+}
+
+template <typename T>
+void CGEngine<T>::destroy()
+{
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    cudaFree(x);
+    cudaFree(r);
+    cudaFree(q);
+    cudaFree(P0);
+    cudaFree(P1);
+    if (jacobi) cudaFree(z);
+    cudaFree(ctl);
+    if (hctl) cudaFreeHost(hctl);
+    if (hstatus) cudaFreeHost(hstatus);
+    x = r = z = q = P0 = P1 = nullptr;
+    ctl = nullptr;
+    hctl = nullptr;
+    hstatus = nullptr;
+}
+
+// Keeps two graph launches in flight; after each completes, its status word says whether
+// to go on. Overshoot after the end is a few no-op kernels (each checks status first).
+template <typename T>
+int CGEngine<T>::run(unsigned* launches)
+{
+    if (!useGraph) {
+        // plain launches, status polled every itersPerGraph iterations
+        for (;;) {
+            for (int i = 0; i < itersPerGraph; ++i) {
+                int e = launch_iter();
+                if (e) return e;
+            }
+            FB_CUDA(cudaMemcpyAsync(hstatus, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost,
+                                    c->stream));
+            FB_CUDA(cudaStreamSynchronize(c->stream));
+            if (launches) *launches += 2 * itersPerGraph;
+            if (*hstatus != kRun) return kOk;
+        }
+    }
+    cudaEvent_t ev[2];
+    FB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    FB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    *hstatus = kRun;
+    int cur = 0;
+    FB_CUDA(cudaGraphLaunch(gexec, c->stream));
+    FB_CUDA(cudaEventRecord(ev[cur], c->stream));
+    int err = kOk;
+    for (;;) {
+        if (cudaGraphLaunch(gexec, c->stream) != cudaSuccess ||
+            cudaEventRecord(ev[cur ^ 1], c->stream) != cudaSuccess) {
+            err = kErrCuda;
+            break;
+        }
+        if (launches) *launches += 2 * itersPerGraph;
+        if (cudaEventSynchronize(ev[cur]) != cudaSuccess) {
+            err = kErrCuda;
+            break;
+        }
+        // hstatus was written by the graph that ev[cur] follows (stream order)
+        if (*hstatus != kRun) break;
+        cur ^= 1;
+    }
+    if (launches) *launches += 2 * itersPerGraph;
+    cudaStreamSynchronize(c->stream);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return err;
+}
+
+// Times each fused kernel alone: reps launches of cg_spmv, then reps of cg_update, each
+// bracketed by events on the engine's stream, with the control block in bench mode.
+template <typename T>
+int CGEngine<T>::time_kernels(unsigned reps, double* ms)
+{
+    std::memset(hctl, 0, sizeof(CGCtl));
+    hctl->status = kRun;
+    hctl->bench = 1;
+    hctl->pmode = 1;
+    hctl->beta = 0.5;
+    hctl->alpha = 1e-3;
+    hctl->histScale = 1.0;
+    int e = push_ctl();
+    if (e) return e;
+    const CSRView<T> V = view_of<T>(*A);
+    const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
+    const int g2 = c->grid(n, kBlock);
+    const T* zz = jacobi ? z : r;
+    cudaEvent_t ev[3];
+    for (auto& x0 : ev) FB_CUDA(cudaEventCreate(&x0));
+    auto spmv = [&]() {
+        switch (A->lanes) {
+            case 1: cg_spmv<T, 1><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+            case 2: cg_spmv<T, 2><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+            case 4: cg_spmv<T, 4><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+            case 8: cg_spmv<T, 8><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+            case 16: cg_spmv<T, 16><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+            default: cg_spmv<T, 32><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
+        }
+    };
+    auto update = [&]() {
+        if (jacobi)
+            cg_update<T, 1><<<g2, kBlock, 0, c->stream>>>(n, x, r, z, P0, P1, q, dinv, ctl, c->red);
+        else
+            cg_update<T, 0><<<g2, kBlock, 0, c->stream>>>(n, x, r, r, P0, P1, q, dinv, ctl, c->red);
+    };
+    for (int w = 0; w < 3; ++w) {
+        spmv();
+        update();
+    }
+    cudaEventRecord(ev[0], c->stream);
+    for (unsigned i = 0; i < reps; ++i) spmv();
+    cudaEventRecord(ev[1], c->stream);
+    for (unsigned i = 0; i < reps; ++i) update();
+    cudaEventRecord(ev[2], c->stream);
+    FB_CUDA(cudaEventSynchronize(ev[2]));
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    ms[0] = a / reps;
+    ms[1] = b / reps;
+    for (auto& x0 : ev) cudaEventDestroy(x0);
+    hctl->bench = 0;
+    hctl->status = kDone;
+    e = push_ctl();
+    if (e) return e;
+    FB_CUDA(cudaStreamSynchronize(c->stream));
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template struct CGEngine<double>;
+template struct CGEngine<float>;
+
+// ---- mixed-precision helpers -----------------------------------------------------------
+
+__global__ void k_convert_scaled(uint32_t n, const double* __restrict__ src, double inv,
+                                 float* __restrict__ dst)
+{
+    GRID_STRIDE(i, n) dst[i] = (float)(src[i] * inv);
+}
+
+__global__ void k_update_from32(uint32_t n, double scale, const float* __restrict__ e,
+                                double* __restrict__ x)
+{
+    GRID_STRIDE(i, n) x[i] = fma(scale, (double)e[i], x[i]);
+}
+
+__global__ void k_set32(uint32_t n, float* __restrict__ x)
+{
+    GRID_STRIDE(i, n) x[i] = 0.0f;
+}
+
+__global__ void k_to32(uint32_t n, const double* __restrict__ s, float* __restrict__ d)
+{
+    GRID_STRIDE(i, n) d[i] = (float)s[i];
+}
+
+int convert_scaled(Ctx& c, uint32_t n, const double* src, double inv, float* dst)
+{
+    ++c.launches;
+    k_convert_scaled<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, src, inv, dst);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int update_from32(Ctx& c, uint32_t n, double scale, const float* e, double* x)
+{
+    ++c.launches;
+    k_update_from32<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, scale, e, x);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int set32(Ctx& c, uint32_t n, float* x)
+{
+    ++c.launches;
+    k_set32<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, x);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int to32(Ctx& c, uint32_t n, const double* s, float* d)
+{
+    ++c.launches;
+    k_to32<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, s, d);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+} // namespace fb

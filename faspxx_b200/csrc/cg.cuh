@@ -1,0 +1,74 @@
+// cg.cuh -- device-driven preconditioned CG (CG::Solve, src/CG.cxx:53-249) for FP64 and
+// for the FP32 inner solves of mixed-precision refinement.
+#pragma once
+
+#include "internal.h"
+
+namespace fb {
+
+enum CGStatus { kRun = 0, kDone = 1, kEsc = 2 };
+enum CGReason { kNoReason = 0, kBreakdown = 1, kSave = 2, kStag = 3, kCheck3 = 4 };
+
+// The locals of CG::Solve (CG.cxx:55-64) plus the parameters it reads, kept in device
+// memory so that the finalize thread of each fused kernel can run the reference's control
+// flow between iterations without a host round trip.
+struct CGCtl {
+    int      status, reason, code, phase;
+    int      pmode;     // 0: p = z (first iteration or restart), 1: p = z + beta p
+    int      par;       // which of the two p buffers holds the current direction
+    int      pzero;     // the host zeroed p (a restart): next p = z
+    int      inner;     // 1: inner solve of mixed refinement (plain relative stop)
+    int      bench;     // 1: kernel timing, the finalize steps do nothing
+    unsigned numIter, stagStep, moreStep;
+    unsigned maxIter, minIter, savIter, restart;
+    double   relTol, absTol, solStagTol, innerTol;
+    double   tmpa, tmpb, alpha, beta, resAbs, resRel, denAbs, ratio, resAbsOld, xRelDiff;
+    double   red[5];    // rr, zr, xx, max|x|, pp saved at an escalation
+    double*  hist;
+    unsigned histCap;
+    unsigned histOffset; // global index of this solve's iteration 0 (mixed refinement)
+    double   histScale;  // inner solves record scale * residual
+};
+
+// Device-driven PCG on one square matrix. T = double (the reference's arithmetic) or
+// float (inner solves). The preconditioner is fused: identity (z aliases r) or one Jacobi
+// sweep from zero, z = weight/diag .* r (Jacobi::Solve with minIter = maxIter = 1).
+template <typename T>
+struct CGEngine {
+    Ctx*       c = nullptr;
+    const Mat* A = nullptr;
+    int        jacobi = 0;
+    const T*   dinv = nullptr;
+    T *x = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *P0 = nullptr, *P1 = nullptr;
+    CGCtl*     ctl = nullptr;    // device
+    CGCtl*     hctl = nullptr;   // pinned host copy
+    int*       hstatus = nullptr;// pinned, written at the end of every graph launch
+    cudaGraphExec_t gexec = nullptr;
+    int        itersPerGraph = 16;
+    bool       useGraph = true;
+    bool       capturing = false;
+    uint32_t   n = 0;
+
+    int  init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph);
+    void destroy();
+    // Runs iterations until the control block leaves kRun; returns kOk or an error.
+    int  run(unsigned* launches);
+    // Kernels: start from the residual in r and the guess in x.
+    int  launch_init();
+    int  launch_iter();
+    int  launch_resume();
+    int  time_kernels(unsigned reps, double* ms);
+    int  push_ctl();   // hctl -> ctl
+    int  pull_ctl();   // ctl -> hctl (synchronous)
+    T*   cur_p() const { return hctl->par ? P1 : P0; }
+};
+
+extern template struct CGEngine<double>;
+extern template struct CGEngine<float>;
+
+int convert_scaled(Ctx& c, uint32_t n, const double* src, double inv_scale, float* dst);
+int update_from32(Ctx& c, uint32_t n, double scale, const float* e, double* x);
+int set32(Ctx& c, uint32_t n, float* x);
+int to32(Ctx& c, uint32_t n, const double* src, float* dst);
+
+} // namespace fb

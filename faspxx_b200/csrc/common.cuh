@@ -1,0 +1,128 @@
+// common.cuh -- shared device helpers of the B200 iterative-solve library.
+//
+// Reductions are deterministic: every kernel that reduces runs on a fixed grid, each block
+// reduces its grid-stride share in a fixed shuffle order and writes one partial per value;
+// the last block to finish (ticket counter) sums the partials in a fixed order and runs the
+// kernel's scalar "finalize" step on one thread. Reruns are therefore bit-identical.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+
+namespace fb {
+
+constexpr int kBlock = 256;          // threads per block for vector kernels
+constexpr int kMaxRedValues = 8;     // values one fused reduction may carry
+constexpr int kMaxGrid = 148 * 16;   // upper bound of any reducing grid (partials sizing)
+
+struct Scratch {
+    double*   partials;  // [kMaxRedValues][kMaxGrid]
+    unsigned* ticket;    // one counter, always returned to 0 by the last block
+};
+
+enum RedOp { kSum = 0, kMax = 1 };
+
+__device__ __forceinline__ double red_ident(int op) { return op == kMax ? 0.0 : 0.0; }
+
+__device__ __forceinline__ double red_apply(double a, double b, int op)
+{
+    // max of magnitudes: operands are |.| >= 0 or NaN; fmax drops a NaN like VEC::NormInf
+    return op == kMax ? fmax(a, b) : a + b;
+}
+
+__device__ __forceinline__ double warp_reduce(double v, int op)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_apply(v, __shfl_down_sync(0xffffffffu, v, o), op);
+    return v;
+}
+
+// Reduces acc[0..NV) over the block; on return thread 0 holds the block totals.
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&acc)[NV], const int (&ops)[NV])
+{
+    __shared__ double sh[32][NV];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = warp_reduce(acc[k], ops[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[wid][k] = acc[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = lane < nw ? sh[lane][k] : red_ident(ops[k]);
+            acc[k] = warp_reduce(t, ops[k]);
+        }
+    }
+    __syncthreads();
+}
+
+// Grid-wide deterministic reduction. Every thread of every block must call it (after its
+// grid-stride work). The last block runs fin(totals) on thread 0. Returns nothing useful to
+// other threads.
+template <int NV, typename Fin>
+__device__ __forceinline__ void grid_reduce(double (&acc)[NV], const int (&ops)[NV],
+                                            Scratch s, Fin fin)
+{
+    __shared__ bool amLast;
+    block_reduce<NV>(acc, ops);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s.partials[k * kMaxGrid + blockIdx.x] = acc[k];
+        __threadfence();
+        const unsigned prev = atomicAdd(s.ticket, 1u);
+        amLast = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!amLast) return;
+    __threadfence();
+    double tot[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = red_ident(ops[k]);
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            t = red_apply(t, __ldcg(&s.partials[k * kMaxGrid + b]), ops[k]);
+        tot[k] = t;
+    }
+    block_reduce<NV>(tot, ops);
+    if (threadIdx.x == 0) {
+        *s.ticket = 0;
+        fin(tot);
+    }
+}
+
+// Reduction over L consecutive lanes (L a power of two <= 32), result in the group's lane 0.
+template <int L, typename T>
+__device__ __forceinline__ T group_sum(T v)
+{
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o, L);
+    return v;
+}
+
+// CSRx matrix view: 32-bit unsigned indices as in FASP++'s MAT (src/MAT.hxx:43-47).
+template <typename T>
+struct CSRView {
+    uint32_t        nrow, mcol, nnz;
+    const uint32_t* rowPtr;
+    const uint32_t* colInd;
+    const T*        val;   // nullptr: pattern only (every stored entry is 1)
+};
+
+__host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+} // namespace fb
+
+#define FB_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            std::fprintf(stderr, "fasp_b200: CUDA error %s at %s:%d\n",                      \
+                         cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+            return ::fb::kErrCuda;                                                           \
+        }                                                                                    \
+    } while (0)

@@ -1,0 +1,136 @@
+// internal.h -- host-side structures and kernel launchers shared by the library's sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace fb {
+
+// Return codes: the FaspRetCode values of FASP++ (src/RetCode.hxx:24-55), plus two for the
+// device layer.
+enum Err {
+    kOk = 0,
+    kErrInputPar = -12,
+    kErrVecSize = -14,
+    kErrMatSize = -15,
+    kErrNonmatch = -16,
+    kErrMatData = -17,
+    kErrDivZero = -18,
+    kErrZeroDiag = -19,
+    kErrAlloc = -20,
+    kErrSolverType = -30,
+    kErrPcdType = -31,
+    kErrStag = -32,
+    kErrSolStag = -33,
+    kErrTolSmall = -34,
+    kErrMaxIt = -39,
+    kErrCuda = -101,
+    kErrNoDevice = -102,
+};
+
+// Constants of include/Faspxx.hxx:31-46.
+constexpr double kCloseZero = 1e-20;
+constexpr double kSmallDbl = -1e+60;
+constexpr double kKsmChkRatio = 0.95;
+constexpr unsigned kMaxStagNum = 20;
+
+// A scalar operand: a host value, or (m * *p) / (m / *p when inv) read on the device, so
+// that one kernel can consume another's reduction without a host round trip.
+struct Scal {
+    double        v;
+    const double* p;
+    double        m;
+    int           inv;
+    static Scal h(double x) { return Scal{x, nullptr, 1.0, 0}; }
+    static Scal d(const double* q, double mul = 1.0) { return Scal{0.0, q, mul, 0}; }
+    static Scal dinv(const double* q, double mul = 1.0) { return Scal{0.0, q, mul, 1}; }
+};
+
+__device__ __forceinline__ double eval(const Scal& s)
+{
+    if (!s.p) return s.v;
+    return s.inv ? s.m / *s.p : s.m * *s.p;
+}
+
+constexpr int kSlots = 256;
+
+// Execution context: one stream, its reduction scratch and scalar slots.
+struct Ctx {
+    int          dev = 0;
+    int          nsm = 148;
+    cudaStream_t stream = nullptr;
+    bool         ownStream = false;
+    Scratch      red{nullptr, nullptr};
+    double*      dslot = nullptr;  // device scalars [kSlots]
+    double*      hslot = nullptr;  // pinned host mirror [kSlots]
+    unsigned long long launches = 0; // kernels launched on this context
+    int init(int device);
+    void destroy();
+    int  grid(long long work, int perBlock) const;  // fixed-size grids for reductions
+    int  sync();
+    int  fetch(int slot, double* out);               // read one device scalar (synchronous)
+};
+
+// CSRx matrix resident in device memory.
+struct Mat {
+    uint32_t  nrow = 0, mcol = 0, nnz = 0;
+    uint32_t* rowPtr = nullptr;
+    uint32_t* colInd = nullptr;
+    uint32_t* diagPtr = nullptr;
+    double*   val = nullptr;     // nullptr: pattern only
+    float*    val32 = nullptr;   // FP32 copy for the mixed-precision inner solves (lazy)
+    double*   diag = nullptr;    // GetDiag (1 for pattern-only)
+    int       lanes = 8;         // lanes per row of the SpMV (autotuned or from row lengths)
+    uint32_t  maxRowLen = 0;
+    double    meanRowLen = 0;
+    int       dev = 0;
+    CSRView<double> v64() const { return CSRView<double>{nrow, mcol, nnz, rowPtr, colInd, val}; }
+    CSRView<float>  v32() const { return CSRView<float>{nrow, mcol, nnz, rowPtr, colInd, val32}; }
+    int ensure32(cudaStream_t s);
+};
+
+// ---- vector kernels (blas.cu) ---------------------------------------------------------
+// Reductions write their result to a device scalar (dres); vector updates take Scal.
+int v_dot(Ctx& c, uint32_t n, const double* a, const double* b, double* dres);
+int v_norm2(Ctx& c, uint32_t n, const double* a, double* dres);
+int v_norminf(Ctx& c, uint32_t n, const double* a, double* dres);
+int v_axpy(Ctx& c, uint32_t n, Scal a, const double* x, double* y);      // y += a x
+int v_xpay(Ctx& c, uint32_t n, Scal a, const double* x, double* y);      // y = a y + x
+int v_axpby(Ctx& c, uint32_t n, Scal a, Scal b, const double* y, double* x); // x = a x + b y
+int v_waxpby(Ctx& c, uint32_t n, Scal a, const double* v1, Scal b, const double* v2,
+             double* w);                                                 // w = a v1 + b v2
+int v_scale(Ctx& c, uint32_t n, Scal a, double* x);
+int v_set(Ctx& c, uint32_t n, double v, double* x);
+int v_copy(Ctx& c, uint32_t n, const double* src, double* dst);
+int v_pmult(Ctx& c, uint32_t n, const double* d, double* x);            // x *= d
+int v_add(Ctx& c, uint32_t n, const double* d, double* x);              // x += d
+int v_recip_scale(Ctx& c, uint32_t n, double w, const double* d, double* out); // out = w*(1/d)
+// Classical Gram-Schmidt blocks over a basis stored at V + j*ld:
+// dres[j] = (V_j, w) for j < k, in one pass over w;
+int v_multidot(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* w,
+               double* dres);
+// w -= sign * sum_j h[j] V_j (h on the device); dnorm (nullable) receives ||w_new||.
+int v_multiaxpy(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* h,
+                double sign, double* w, double* dnorm);
+
+// ---- sparse kernels (spmv.cu) ---------------------------------------------------------
+int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+             const uint32_t* colInd, const double* values, bool hostPtrs, cudaStream_t s);
+void m_free(Mat& M);
+int m_spmv(Ctx& c, const Mat& A, const double* x, double* y);           // y = A x
+int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y);
+// r = b - A x with the x ~ 0 shortcut of MAT::Residual; the NormInf(x) comes from xinf
+// (device scalar computed by the caller) unless xinf is null (then computed here).
+int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
+               const double* xinf);
+int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR -> CSC, exact
+int m_autotune(Ctx& c, Mat& A);
+// dA[k] = scale * lam[row(k)] * x[col(k)] on the sparsity pattern (sampled outer product)
+int m_sampled_outer(Ctx& c, const Mat& A, const double* lam, const double* x, double scale,
+                    double* dA);
+
+} // namespace fb

@@ -1,0 +1,97 @@
+// solver.h -- the solver object behind fasp_gpu_solver (SOL and its subclasses).
+#pragma once
+
+#include <limits>
+#include <vector>
+
+#include "../../include/fasp_b200.h"
+#include "cg.cuh"
+#include "internal.h"
+
+struct fasp_gpu_mat_s {
+    fb::Mat         M;
+    fb::Ctx         c;            // stream for matrix-level calls
+    fasp_gpu_mat_s* T = nullptr;  // cached exact transpose (adjoint solves), owned
+};
+
+namespace fb {
+
+// The preconditioner of a solver: Identity (Iter.cxx:16-20) or Jacobi (Iter.cxx:29-112).
+struct Pcd {
+    int             type = 0;    // 0 identity, 1 Jacobi
+    fasp_gpu_params prm{};
+    double          weight = 1.0;
+    const Mat*      A = nullptr;
+    double*         dinv = nullptr;   // weight / diag
+    float*          dinv32 = nullptr;
+    double*         work = nullptr;
+    uint32_t        numIter = 0;
+    bool pure() const { return type == 1 && prm.minIter == prm.maxIter; }
+    int  setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p);
+    void destroy();
+    // Solve(b, x): x is read as the initial guess (callers zero it where the reference does)
+    int  solve(Ctx& c, const double* b, double* x, std::vector<double>* hist = nullptr,
+               double* norm2 = nullptr, double* normInf = nullptr);
+};
+
+struct SolverImpl {
+    fasp_gpu_config cfg{};
+    Ctx             c;
+    Mat*            A = nullptr;    // bound by Setup (borrowed)
+    fasp_gpu_mat    Ah = nullptr;
+    Pcd             pcd;
+    uint32_t        n = 0;
+    // work vectors (FP64)
+    std::vector<double*> w;
+    double*         V = nullptr;    // GMRES/FGMRES basis, (maxRestart+1) x n
+    double*         Z = nullptr;    // FGMRES preconditioned basis
+    double*         gm = nullptr;   // device Hessenberg block: hh, hcos, hsin, var, dots
+    uint32_t        maxRestart = 0, minRestart = 0, restart = 0;
+    // MG (identity transfers): per level smoother and coarse solver, coarse b and x
+    std::vector<Pcd> mgSmooth, mgCoarse;
+    std::vector<double*> mgB, mgX;
+    int             mgLevel = -1;
+    // device-driven CG
+    CGEngine<double>* cg64 = nullptr;
+    CGEngine<float>*  cg32 = nullptr;
+    double*         safe = nullptr;
+    double*         dhist = nullptr;
+    double*         hostB = nullptr;  // staging of the host entry point
+    double*         hostX = nullptr;
+    uint32_t        dhistCap = 0;
+    // results
+    std::vector<double> hist;
+    double          lastMs = 0.0;
+    // adjoint
+    SolverImpl*     adj = nullptr;
+
+    int  setup(fasp_gpu_mat M);
+    int  solve(const double* b, double* x, fasp_gpu_info* info);
+    void clean();
+    void destroy();
+
+    // solver bodies (host-orchestrated, device vectors)
+    int cg_generic(const double* b, double* x, fasp_gpu_info* info);
+    int cg_device(const double* b, double* x, fasp_gpu_info* info);
+    int cg_mixed(const double* b, double* x, fasp_gpu_info* info);
+    int bicgstab(const double* b, double* x, fasp_gpu_info* info);
+    int gmres_right(const double* b, double* x, fasp_gpu_info* info, bool flexible);
+    int gmres_left(const double* b, double* x, fasp_gpu_info* info);
+    int jacobi(const double* b, double* x, fasp_gpu_info* info);
+    int mg(const double* b, double* x, fasp_gpu_info* info);
+    void mg_cycle(const double* b, double* x);
+
+    // helpers
+    double fetch(const double* dptr);
+    void   rec(uint32_t k, double v)
+    {
+        if (k >= hist.size()) hist.resize((size_t)k + 1, std::numeric_limits<double>::quiet_NaN());
+        hist[k] = v;
+    }
+};
+
+} // namespace fb
+
+struct fasp_gpu_solver_s {
+    fb::SolverImpl s;
+};

@@ -1,0 +1,1187 @@
+// solvers.cu -- the SOL subclasses of FASP++ on the GPU.
+//
+// Each solver keeps the reference's control flow statement by statement (file:line cited
+// per function) while every vector operation is a kernel on the solver's stream. Scalars
+// stay on the device (kernels read them through Scal) until a branch needs one on the host.
+// CG with an Identity or single-sweep Jacobi preconditioner runs device-driven (cg.cu); the
+// other configurations run the host-orchestrated restatement below.
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "solver.h"
+
+namespace fb {
+
+static const double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+// scalar slots of the solver context
+enum {
+    SL_T0 = 0, SL_T1, SL_T2, SL_T3, SL_T4, SL_T5, SL_T6, SL_T7,
+    SL_XINF = 16,  // NormInf of a residual's x (MAT::Residual shortcut)
+    SL_ONE = 17,   // constant 1: disables the shortcut (MAT::Apply + XPAY paths)
+};
+
+double SolverImpl::fetch(const double* dptr)
+{
+    double v = kNaN;
+    if (cudaMemcpyAsync(c.hslot, dptr, sizeof(double), cudaMemcpyDeviceToHost, c.stream) ==
+            cudaSuccess &&
+        cudaStreamSynchronize(c.stream) == cudaSuccess)
+        v = c.hslot[0];
+    return v;
+}
+
+// A->Apply(x, r); r.XPAY(-1.0, b)  -> r = b - A x without the NormInf shortcut
+static int apply_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r)
+{
+    return m_residual(c, A, b, x, r, c.dslot + SL_ONE);
+}
+
+// ---- Jacobi (src/Iter.cxx) ---------------------------------------------------------------
+
+__global__ void k_jacobi_update(uint32_t n, const double* __restrict__ dinv,
+                                const double* __restrict__ work, double* __restrict__ x,
+                                Scratch s, double* dxinf)
+{
+    // work .*= diagInv; x += work (Iter.cxx:91-92); also NormInf(x_new) for the next
+    // residual's shortcut test
+    double acc[1] = {0.0};
+    const int ops[1] = {kMax};
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double xi = x[i] + work[i] * dinv[i];
+        x[i] = xi;
+        acc[0] = fmax(acc[0], fabs(xi));
+    }
+    grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dxinf = t[0]; });
+}
+
+int Pcd::setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p)
+{
+    type = t;
+    weight = w;
+    prm = p;
+    A = M;
+    if (type != 1) return kOk;
+    const size_t n = M->nrow;
+    if (cudaMalloc(&dinv, (n + 2) * 8) || cudaMalloc(&dinv32, (n + 4) * 4) ||
+        cudaMalloc(&work, (n + 2) * 8)) {
+        cudaGetLastError();
+        return kErrAlloc;
+    }
+    // Jacobi::Setup: GetDiag, Reciprocal, Scale(weight) (Iter.cxx:45-47)
+    int e = v_recip_scale(c, M->nrow, weight, M->diag, dinv);
+    if (e) return e;
+    return to32(c, M->nrow, dinv, dinv32);
+}
+
+void Pcd::destroy()
+{
+    cudaFree(dinv);
+    cudaFree(dinv32);
+    cudaFree(work);
+    dinv = nullptr;
+    dinv32 = nullptr;
+    work = nullptr;
+}
+
+// Identity::Solve (Iter.cxx:16-20) or Jacobi::Solve (Iter.cxx:56-112).
+int Pcd::solve(Ctx& c, const double* b, double* x, std::vector<double>* hist, double* norm2,
+               double* normInf)
+{
+    const uint32_t n = A->nrow;
+    if (type == 0) return v_copy(c, n, b, x);
+    auto fetch = [&](const double* d) {
+        double v = kNaN;
+        cudaMemcpyAsync(c.hslot + 1, d, 8, cudaMemcpyDeviceToHost, c.stream);
+        cudaStreamSynchronize(c.stream);
+        v = c.hslot[1];
+        return v;
+    };
+    auto rec = [&](uint32_t k, double v) {
+        if (!hist) return;
+        if (k >= hist->size()) hist->resize((size_t)k + 1, kNaN);
+        (*hist)[k] = v;
+    };
+    double* xinf = c.dslot + SL_XINF;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0;
+    int e = v_norminf(c, n, x, xinf);
+    if (e) return e;
+    numIter = 0;
+    while (numIter < prm.maxIter) {
+        if ((e = m_residual(c, *A, b, x, work, xinf))) return e;
+        if (numIter >= prm.minIter) {
+            v_norm2(c, n, work, c.dslot + SL_T7);
+            resAbs = fetch(c.dslot + SL_T7);
+            if (numIter == prm.minIter) denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+            resRel = resAbs / denAbs;
+            rec(numIter, resAbs);
+            if (resRel < prm.relTol || resAbs < prm.absTol) break;
+        }
+        ++c.launches;
+        k_jacobi_update<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, dinv, work, x, c.red, xinf);
+        FB_CUDA(cudaGetLastError());
+        ++numIter;
+    }
+    if (!(numIter == prm.minIter && numIter == prm.maxIter)) {
+        if ((e = m_residual(c, *A, b, x, work, xinf))) return e;
+        v_norm2(c, n, work, c.dslot + SL_T7);
+        v_norminf(c, n, work, c.dslot + SL_T6);
+        resAbs = fetch(c.dslot + SL_T7);
+        const double ni = fetch(c.dslot + SL_T6);
+        if (norm2) *norm2 = resAbs;
+        if (normInf) *normInf = ni;
+        rec(numIter, resAbs);
+    }
+    return kOk;
+}
+
+// ---- setup -------------------------------------------------------------------------------
+
+static int alloc_vecs(std::vector<double*>& w, int k, uint32_t n)
+{
+    for (int i = 0; i < k; ++i) {
+        double* p = nullptr;
+        if (cudaMalloc(&p, ((size_t)n + 2) * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return kErrAlloc;
+        }
+        cudaMemset(p, 0, ((size_t)n + 2) * 8);
+        w.push_back(p);
+    }
+    return kOk;
+}
+
+int SolverImpl::setup(fasp_gpu_mat Mh)
+{
+    if (!Mh) return kErrInputPar;
+    clean();
+    for (double* p : w) cudaFree(p);
+    w.clear();
+    Ah = Mh;
+    A = &Mh->M;
+    n = A->nrow;
+    if (A->nrow != A->mcol) return kErrMatSize;
+    int e;
+    const double one = 1.0;
+    FB_CUDA(cudaMemcpyAsync(c.dslot + SL_ONE, &one, 8, cudaMemcpyHostToDevice, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    const int alg = cfg.alg;
+    if (alg == FASP_GPU_JACOBI) {
+        // the solver is itself a Jacobi object with its own weight and SOLParams
+        if ((e = pcd.setup(c, A, 1, cfg.weight, cfg.prm))) return e;
+        FB_CUDA(cudaStreamSynchronize(c.stream));
+        return kOk;
+    }
+    if (cfg.pcd != 0 && cfg.pcd != 1) return kErrPcdType;
+    if ((e = pcd.setup(c, A, cfg.pcd, cfg.pcdWeight, cfg.pcdPrm))) return e;
+    switch (alg) {
+        case FASP_GPU_CG: {
+            if ((e = alloc_vecs(w, 5, n))) return e; // rk pk zk ax safe
+            dhistCap = cfg.prm.maxIter + 2;
+            if (cudaMalloc(&dhist, (size_t)dhistCap * 8) != cudaSuccess) return kErrAlloc;
+            const bool fusable = cfg.pcd == 0 || (pcd.pure() && pcd.prm.maxIter == 1);
+            if (fusable && cfg.precision == FASP_GPU_FP64) {
+                cg64 = new CGEngine<double>();
+                if ((e = cg64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
+            }
+            if (cfg.precision == FASP_GPU_MIXED) {
+                if (!fusable) return kErrPcdType; // mixed mode fuses its preconditioner
+                if ((e = Ah->M.ensure32(c.stream))) return e;
+                cg32 = new CGEngine<float>();
+                if ((e = cg32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
+            }
+            break;
+        }
+        case FASP_GPU_BICGSTAB:
+            if ((e = alloc_vecs(w, 12, n))) return e;
+            break;
+        case FASP_GPU_GMRES:
+        case FASP_GPU_FGMRES: {
+            // GMRES::Setup (GMRES.cxx:38-88) / FGMRES::Setup (FGMRES.cxx:23-80)
+            const uint32_t maxR = cfg.maxRestart ? cfg.maxRestart : 30;
+            const uint32_t minR = cfg.maxRestart ? cfg.minRestart : 10;
+            restart = cfg.prm.restart;
+            maxRestart = maxR > cfg.prm.maxIter ? cfg.prm.maxIter : maxR;
+            minRestart = minR > maxRestart ? maxRestart : minR;
+            if (restart > maxRestart)
+                restart = maxRestart;
+            else if (restart < minRestart)
+                restart = minRestart;
+            if (maxRestart == 0 || restart == 0) return kErrInputPar;
+            if ((e = alloc_vecs(w, 3, n))) return e; // wk tmp safe
+            const size_t vb = (size_t)(maxRestart + 1) * n * 8;
+            if (cudaMalloc(&V, vb + 16) != cudaSuccess) return kErrAlloc;
+            cudaMemset(V, 0, vb);
+            if (alg == FASP_GPU_FGMRES) {
+                if (cudaMalloc(&Z, vb + 16) != cudaSuccess) return kErrAlloc;
+                cudaMemset(Z, 0, vb);
+            }
+            const size_t m = maxRestart;
+            const size_t gmSize = (m + 1) * m + (m + 1) + m + (m + 1) + 2 * (m + 1) + 4;
+            if (cudaMalloc(&gm, gmSize * 8) != cudaSuccess) return kErrAlloc;
+            cudaMemset(gm, 0, gmSize * 8);
+            break;
+        }
+        case FASP_GPU_MG: {
+            // MG::SetupALL + SetupLevel with identity transfers (MG.cxx:26-79)
+            if ((e = alloc_vecs(w, 1, n))) return e; // r
+            const uint32_t L = cfg.mgLevels;
+            mgSmooth.resize(L);
+            mgCoarse.resize(L);
+            for (uint32_t l = 0; l < L; ++l) {
+                if ((e = mgSmooth[l].setup(c, A, 1, cfg.mgSmoothWeight, cfg.mgSmoothPrm))) return e;
+                if ((e = mgCoarse[l].setup(c, A, 1, cfg.mgCoarseWeight, cfg.mgCoarsePrm))) return e;
+            }
+            std::vector<double*> lv;
+            if ((e = alloc_vecs(lv, 2 * L, n))) return e;
+            for (uint32_t l = 0; l < L; ++l) {
+                mgB.push_back(lv[2 * l]);
+                mgX.push_back(lv[2 * l + 1]);
+            }
+            break;
+        }
+        default:
+            return kErrSolverType;
+    }
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+void SolverImpl::clean()
+{
+    // SOL::Clean: restart value restored, Krylov bases zeroed (GMRES.cxx:91-111,
+    // FGMRES.cxx:83-105)
+    if (cfg.alg == FASP_GPU_GMRES || cfg.alg == FASP_GPU_FGMRES) {
+        restart = cfg.prm.restart;
+        if (restart > maxRestart)
+            restart = maxRestart;
+        else if (restart < minRestart)
+            restart = minRestart;
+        const size_t vb = (size_t)(maxRestart + 1) * n * 8;
+        if (V) cudaMemsetAsync(V, 0, vb, c.stream);
+        if (Z) cudaMemsetAsync(Z, 0, vb, c.stream);
+        cudaStreamSynchronize(c.stream);
+    }
+}
+
+void SolverImpl::destroy()
+{
+    for (double* p : w) cudaFree(p);
+    w.clear();
+    cudaFree(V);
+    cudaFree(Z);
+    cudaFree(gm);
+    cudaFree(safe);
+    cudaFree(dhist);
+    cudaFree(hostB);
+    cudaFree(hostX);
+    V = Z = gm = safe = dhist = hostB = hostX = nullptr;
+    pcd.destroy();
+    for (auto& p : mgSmooth) p.destroy();
+    for (auto& p : mgCoarse) p.destroy();
+    for (double* p : mgB) cudaFree(p);
+    for (double* p : mgX) cudaFree(p);
+    mgSmooth.clear();
+    mgCoarse.clear();
+    mgB.clear();
+    mgX.clear();
+    if (cg64) {
+        cg64->destroy();
+        delete cg64;
+        cg64 = nullptr;
+    }
+    if (cg32) {
+        cg32->destroy();
+        delete cg32;
+        cg32 = nullptr;
+    }
+    if (adj) {
+        adj->destroy();
+        adj->c.destroy();
+        delete adj;
+        adj = nullptr;
+    }
+}
+
+// ---- CG (src/CG.cxx:53-249) ---------------------------------------------------------------
+
+int SolverImpl::cg_generic(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double *rk = w[0], *pk = w[1], *zk = w[2], *ax = w[3], *sv = w[4];
+    double* d = c.dslot;
+    int err = kOk, e;
+    const unsigned maxStag = kMaxStagNum;
+    const double solStagTol = 1e-4 * P.relTol, solZeroTol = kCloseZero;
+    unsigned stagStep = 0, moreStep = 0;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, ratio = 0.0, resAbsOld = 1.0;
+    double alpha = 0.0, beta, tmpa, tmpb;
+    uint32_t numIter = 0;
+
+    if ((e = apply_residual(c, *A, b, x, rk))) return e;
+    v_set(c, n, 0.0, zk);
+    if ((e = pcd.solve(c, rk, zk))) return e;
+    v_copy(c, n, zk, pk);
+    v_dot(c, n, zk, rk, d + SL_T0);
+    tmpa = fetch(d + SL_T0);
+
+    while (numIter < P.maxIter) {
+        if (numIter == P.minIter) {
+            v_norm2(c, n, rk, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            resAbsOld = resAbs;
+            denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+            resRel = resAbs / denAbs;
+            rec(numIter, resAbs);
+            if (resRel < P.relTol || resAbs < P.absTol) break;
+        }
+        ++numIter;
+        m_spmv(c, *A, pk, ax);
+        v_dot(c, n, ax, pk, d + SL_T0);
+        tmpb = fetch(d + SL_T0);
+        if (std::fabs(tmpb) > kCloseZero * kCloseZero)
+            alpha = tmpa / tmpb;
+        else {
+            v_axpy(c, n, Scal::h(alpha), pk, x);
+            v_axpy(c, n, Scal::h(-alpha), ax, rk);
+            v_norm2(c, n, rk, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            resRel = resAbs / denAbs;
+            if (resRel > P.relTol && resAbs > P.absTol) err = kErrDivZero;
+            rec(numIter, resAbs);
+            break;
+        }
+        v_axpy(c, n, Scal::h(alpha), pk, x);
+        v_axpy(c, n, Scal::h(-alpha), ax, rk);
+        if (numIter >= P.minIter) {
+            bool stop = false;
+            v_norm2(c, n, rk, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            resRel = resAbs / denAbs;
+            ratio = resAbs / resAbsOld;
+            if (numIter >= P.savIter && resAbs < resAbsOld) v_copy(c, n, x, sv);
+            if (ratio > kKsmChkRatio) {
+                v_norminf(c, n, x, d + SL_T2);
+                const double xNormInf = fetch(d + SL_T2);
+                if (xNormInf < solZeroTol) {
+                    err = kErrSolStag;
+                    stop = true;
+                } else {
+                    v_norm2(c, n, pk, d + SL_T3);
+                    v_norm2(c, n, x, d + SL_T4);
+                    const double xRelDiff =
+                        std::fabs(alpha) * fetch(d + SL_T3) / fetch(d + SL_T4);
+                    if ((stagStep <= maxStag) && (xRelDiff < solStagTol)) {
+                        apply_residual(c, *A, b, x, rk);
+                        v_norm2(c, n, rk, d + SL_T1);
+                        resAbs = fetch(d + SL_T1);
+                        resRel = resAbs / denAbs;
+                        if (resRel < P.relTol || resAbs < P.absTol)
+                            stop = true;
+                        else if (stagStep >= maxStag) {
+                            err = kErrStag;
+                            stop = true;
+                        } else {
+                            v_set(c, n, 0.0, pk);
+                            ++stagStep;
+                        }
+                    }
+                }
+            }
+            if (!stop && resRel < P.relTol) {
+                apply_residual(c, *A, b, x, rk);
+                v_norm2(c, n, rk, d + SL_T1);
+                resAbs = fetch(d + SL_T1);
+                resRel = resAbs / denAbs;
+                if (resRel < P.relTol || resAbs < P.absTol)
+                    stop = true;
+                else if (moreStep >= P.restart) {
+                    err = kErrTolSmall;
+                    stop = true;
+                } else {
+                    v_set(c, n, 0.0, pk); // CG.cxx:213 resizes pk to 0; zero is the intent
+                    ++moreStep;
+                }
+            }
+            rec(numIter, resAbs);
+            if (stop) break;
+        }
+        if (numIter < P.maxIter) {
+            resAbsOld = resAbs;
+            v_set(c, n, 0.0, zk);
+            if ((e = pcd.solve(c, rk, zk))) return e;
+            v_dot(c, n, zk, rk, d + SL_T0);
+            tmpb = fetch(d + SL_T0);
+            beta = tmpb / tmpa;
+            tmpa = tmpb;
+            v_xpay(c, n, Scal::h(beta), zk, pk);
+        }
+    }
+    info->numIter = numIter;
+    info->code = err;
+    if (!(numIter == P.minIter && numIter == P.maxIter)) {
+        info->norm2 = resAbs;
+        v_norminf(c, n, rk, d + SL_T2);
+        info->normInf = fetch(d + SL_T2);
+    }
+    if (numIter > P.savIter) v_copy(c, n, sv, x);
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+__global__ void k_fill(uint32_t n, double v, double* x)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+
+int SolverImpl::cg_device(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    CGEngine<double>& E = *cg64;
+    CGCtl& h = *E.hctl;
+    std::vector<std::pair<uint32_t, double>> patches; // history entries set by the host
+    int e;
+    std::memset(&h, 0, sizeof(CGCtl));
+    h.maxIter = P.maxIter;
+    h.minIter = P.minIter;
+    h.savIter = P.savIter;
+    h.restart = P.restart;
+    h.relTol = P.relTol;
+    h.absTol = P.absTol;
+    h.solStagTol = 1e-4 * P.relTol;
+    h.hist = dhist;
+    h.histCap = dhistCap;
+    h.histScale = 1.0;
+    ++c.launches;
+    k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    v_copy(c, n, x, E.x);
+    if ((e = apply_residual(c, *A, b, E.x, E.r))) return e;
+    if ((e = E.push_ctl()) || (e = E.launch_init()) || (e = E.pull_ctl())) return e;
+    unsigned launches = 0;
+    info->escalations = 0;
+    for (int guard = 0; h.status != kDone; ++guard) {
+        if (h.status == kRun) {
+            if ((e = E.run(&launches)) || (e = E.pull_ctl())) return e;
+            c.launches += launches;
+            launches = 0;
+            continue;
+        }
+        // kEsc: the host finishes the branch the device could not (CG.cxx references)
+        info->escalations++;
+        const int reason = h.reason;
+        double* p = E.cur_p();
+        auto true_res = [&]() {
+            apply_residual(c, *A, b, E.x, E.r);
+            v_norm2(c, n, E.r, c.dslot + SL_T1);
+            h.resAbs = fetch(c.dslot + SL_T1);
+            h.resRel = h.resAbs / h.denAbs;
+        };
+        bool finished = false;
+        if (reason == kBreakdown) { // CG.cxx:107-118
+            v_axpy(c, n, Scal::h(h.alpha), p, E.x);
+            v_axpy(c, n, Scal::h(-h.alpha), E.q, E.r);
+            v_norm2(c, n, E.r, c.dslot + SL_T1);
+            h.resAbs = fetch(c.dslot + SL_T1);
+            h.resRel = h.resAbs / h.denAbs;
+            if (h.resRel > P.relTol && h.resAbs > P.absTol) h.code = kErrDivZero;
+            patches.push_back({h.numIter, h.resAbs});
+            finished = true;
+        } else if (reason == kSave) { // CG.cxx:138
+            if (!safe && cudaMalloc(&safe, ((size_t)n + 2) * 8) != cudaSuccess) return kErrAlloc;
+            v_copy(c, n, E.x, safe);
+        } else if (reason == kStag) { // CG.cxx:153-181
+            true_res();
+            if (h.resRel < P.relTol || h.resAbs < P.absTol) {
+                patches.push_back({h.numIter, h.resAbs});
+                finished = true;
+            } else if (h.stagStep >= kMaxStagNum) {
+                h.code = kErrStag;
+                patches.push_back({h.numIter, h.resAbs});
+                finished = true;
+            } else {
+                h.pzero = 1;
+                ++h.stagStep;
+            }
+        } else if (reason == kCheck3) { // CG.cxx:186-215
+            true_res();
+            if (h.resRel < P.relTol || h.resAbs < P.absTol) {
+                patches.push_back({h.numIter, h.resAbs});
+                finished = true;
+            } else if (h.moreStep >= P.restart) {
+                h.code = kErrTolSmall;
+                patches.push_back({h.numIter, h.resAbs});
+                finished = true;
+            } else {
+                h.pzero = 1;
+                ++h.moreStep;
+            }
+        }
+        if (finished) {
+            h.status = kDone;
+            if ((e = E.push_ctl())) return e;
+            break;
+        }
+        h.status = kRun;
+        if ((e = E.push_ctl()) || (e = E.launch_resume()) || (e = E.pull_ctl())) return e;
+        if (guard > (int)P.maxIter + 64) return kErrCuda; // cannot happen: each pass advances
+    }
+    info->numIter = h.numIter;
+    info->code = h.code;
+    info->norm2 = kNaN;
+    info->normInf = kNaN;
+    if (!(h.numIter == P.minIter && h.numIter == P.maxIter)) {
+        info->norm2 = h.resAbs;
+        v_norminf(c, n, E.r, c.dslot + SL_T2);
+        info->normInf = fetch(c.dslot + SL_T2);
+    }
+    v_copy(c, n, E.x, x);
+    if (h.numIter > P.savIter && safe) v_copy(c, n, safe, x);
+    const uint32_t len = std::min<uint32_t>(h.numIter + 1, dhistCap);
+    hist.assign(len, kNaN);
+    FB_CUDA(cudaMemcpyAsync(hist.data(), dhist, (size_t)len * 8, cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& pt : patches) rec(pt.first, pt.second);
+    (void)launches;
+    return kOk;
+}
+
+// Mixed precision: FP64 residual and update around FP32 inner CG solves (no reference
+// counterpart). Each outer step solves A e = r / ||r|| in FP32 to innerRelTol, then
+// x += ||r|| e in FP64; it stops when ||b - A x|| / ||b - A x0|| < relTol (or < absTol).
+int SolverImpl::cg_mixed(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    CGEngine<float>& E = *cg32;
+    CGCtl& h = *E.hctl;
+    double *x64 = w[0], *r64 = w[1];
+    int e;
+    v_copy(c, n, x, x64);
+    const double innerTol = cfg.innerRelTol > 0 ? cfg.innerRelTol : 1e-4;
+    const uint32_t innerMax = cfg.innerMaxIter ? cfg.innerMaxIter : P.maxIter;
+    const uint32_t maxOuter = cfg.maxOuter ? cfg.maxOuter : 50;
+    ++c.launches;
+    k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    uint32_t total = 0, outer = 0;
+    double den = 1.0, rn = 0.0;
+    int code = kOk;
+    std::vector<std::pair<uint32_t, double>> outerHist;
+    for (;;) {
+        if ((e = apply_residual(c, *A, b, x64, r64))) return e;
+        v_norm2(c, n, r64, c.dslot + SL_T1);
+        rn = fetch(c.dslot + SL_T1);
+        if (outer == 0) den = (kCloseZero > rn) ? kCloseZero : rn;
+        outerHist.push_back({total, rn});
+        if (rn / den < P.relTol || rn < P.absTol) break;
+        if (outer >= maxOuter || total >= P.maxIter || !std::isfinite(rn)) {
+            code = kErrMaxIt;
+            break;
+        }
+        if ((e = convert_scaled(c, n, r64, 1.0 / rn, E.r)) || (e = set32(c, n, E.x))) return e;
+        std::memset(&h, 0, sizeof(CGCtl));
+        h.maxIter = std::min<uint32_t>(innerMax, P.maxIter - total);
+        h.minIter = 0;
+        h.savIter = 0xffffffffu;
+        h.inner = 1;
+        h.innerTol = innerTol;
+        h.relTol = innerTol;
+        h.hist = dhist;
+        h.histCap = dhistCap;
+        h.histOffset = total;
+        h.histScale = rn;
+        if ((e = E.push_ctl()) || (e = E.launch_init()) || (e = E.pull_ctl())) return e;
+        unsigned gl = 0;
+        if (h.status == kRun && ((e = E.run(&gl)) || (e = E.pull_ctl()))) return e;
+        c.launches += gl;
+        const uint32_t it = h.numIter;
+        total += it;
+        if ((e = update_from32(c, n, rn, E.x, x64))) return e;
+        ++outer;
+        if (it == 0) {
+            code = h.code ? h.code : kErrMaxIt;
+            if ((e = apply_residual(c, *A, b, x64, r64))) return e;
+            v_norm2(c, n, r64, c.dslot + SL_T1);
+            rn = fetch(c.dslot + SL_T1);
+            break;
+        }
+    }
+    info->numIter = total;
+    info->outerIter = outer;
+    info->code = code;
+    info->norm2 = rn;
+    v_norminf(c, n, r64, c.dslot + SL_T2);
+    info->normInf = fetch(c.dslot + SL_T2);
+    v_copy(c, n, x64, x);
+    const uint32_t len = std::min<uint32_t>(total + 1, dhistCap);
+    hist.assign(len, kNaN);
+    FB_CUDA(cudaMemcpyAsync(hist.data(), dhist, (size_t)len * 8, cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& pt : outerHist) rec(pt.first, pt.second);
+    return kOk;
+}
+
+// ---- BiCGStab (src/BiCGStab.cxx:68-270) ---------------------------------------------------
+
+int SolverImpl::bicgstab(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double *r0star = w[0], *tmp = w[1], *apj = w[2], *asj = w[3], *pj = w[4], *rj = w[5],
+           *sj = w[6], *ptmp = w[7], *stmp = w[8], *ms = w[9], *mp = w[10], *sv = w[11];
+    double* d = c.dslot;
+    int err = kOk, e;
+    const unsigned maxStag = kMaxStagNum;
+    const double solStagTol = 1e-4 * P.relTol;
+    unsigned stagStep = 0, moreStep = 0;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, ratio = 0.0, resAbsOld = 1.0;
+    double alpha = 0.0, beta, rjr0star = 0.0, rjr0startmp, omega = 0.0, tmp12;
+    uint32_t numIter = 0;
+
+    m_spmv(c, *A, x, tmp);
+    v_waxpby(c, n, Scal::h(1.0), b, Scal::h(-1.0), tmp, rj);
+    v_copy(c, n, rj, r0star);
+    v_copy(c, n, rj, pj);
+
+    while (numIter < P.maxIter) {
+        if (numIter == P.minIter) {
+            v_norm2(c, n, rj, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+            resRel = resAbs / denAbs;
+            rec(numIter, resAbs);
+            if (resRel < P.relTol || resAbs < P.absTol) break;
+        }
+        ++numIter;
+        v_dot(c, n, rj, r0star, d + SL_T0);
+        m_spmv(c, *A, pj, apj);
+        v_set(c, n, 0.0, ptmp);
+        if ((e = pcd.solve(c, apj, ptmp))) return e;
+        v_dot(c, n, ptmp, r0star, d + SL_T2);
+        rjr0star = fetch(d + SL_T0);
+        tmp12 = fetch(d + SL_T2);
+        if (std::fabs(tmp12) > 1e-40)
+            alpha = rjr0star / tmp12;
+        else {
+            err = kErrDivZero;
+            rec(numIter, resAbs);
+            break;
+        }
+        v_waxpby(c, n, Scal::h(1.0), rj, Scal::h(-alpha), ptmp, sj);
+        m_spmv(c, *A, sj, asj);
+        v_set(c, n, 0.0, stmp);
+        if ((e = pcd.solve(c, asj, stmp))) return e;
+        v_dot(c, n, stmp, sj, d + SL_T3);
+        v_dot(c, n, stmp, stmp, d + SL_T4);
+        omega = fetch(d + SL_T3) / fetch(d + SL_T4);
+        v_set(c, n, 0.0, mp);
+        if ((e = pcd.solve(c, pj, mp))) return e;
+        v_set(c, n, 0.0, ms);
+        if ((e = pcd.solve(c, sj, ms))) return e;
+        v_waxpby(c, n, Scal::h(alpha), mp, Scal::h(omega), ms, tmp);
+        v_xpay(c, n, Scal::h(1.0), tmp, x);
+        v_waxpby(c, n, Scal::h(1.0), sj, Scal::h(-omega), stmp, rj);
+
+        if (numIter >= P.minIter) {
+            bool stop = false;
+            v_norm2(c, n, rj, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            resRel = resAbs / denAbs;
+            ratio = resAbs / resAbsOld;
+            if (numIter >= P.savIter && resAbs < resAbsOld) v_copy(c, n, x, sv);
+            if (ratio > kKsmChkRatio && numIter > P.minIter) {
+                v_norminf(c, n, x, d + SL_T2);
+                const double xNorminf = fetch(d + SL_T2);
+                if (xNorminf < solStagTol) {
+                    err = kErrSolStag;
+                    stop = true;
+                } else {
+                    v_norm2(c, n, pj, d + SL_T3);
+                    v_norm2(c, n, x, d + SL_T4);
+                    const double xRelDiff =
+                        std::fabs(alpha) * fetch(d + SL_T3) / fetch(d + SL_T4);
+                    if ((stagStep <= maxStag) && (xRelDiff < solStagTol)) {
+                        apply_residual(c, *A, b, x, rj);
+                        v_norm2(c, n, rj, d + SL_T1);
+                        resAbs = fetch(d + SL_T1);
+                        resRel = resAbs / denAbs;
+                        if (resRel < P.relTol || resAbs < P.absTol)
+                            stop = true;
+                        else if (stagStep >= maxStag) {
+                            err = kErrStag;
+                            stop = true;
+                        } else {
+                            v_set(c, n, 0.0, pj);
+                            ++stagStep;
+                        }
+                    }
+                }
+            }
+            if (!stop && resRel < P.relTol) {
+                apply_residual(c, *A, b, x, rj);
+                v_norm2(c, n, rj, d + SL_T1);
+                resAbs = fetch(d + SL_T1);
+                resRel = resAbs / denAbs;
+                if (resRel < P.relTol || resAbs < P.absTol)
+                    stop = true;
+                else if (moreStep >= P.restart) {
+                    err = kErrTolSmall;
+                    stop = true;
+                } else {
+                    v_set(c, n, 0.0, pj);
+                    ++moreStep;
+                }
+            }
+            rec(numIter, resAbs);
+            if (stop) break;
+        }
+        if (numIter < P.maxIter) {
+            resAbsOld = resAbs;
+            rjr0startmp = rjr0star;
+            v_dot(c, n, rj, r0star, d + SL_T0);
+            rjr0star = fetch(d + SL_T0);
+            beta = rjr0star / rjr0startmp * alpha / omega;
+            v_waxpby(c, n, Scal::h(1.0), pj, Scal::h(-omega), ptmp, tmp);
+            v_waxpby(c, n, Scal::h(1.0), rj, Scal::h(beta), tmp, pj);
+        }
+    }
+    info->numIter = numIter;
+    info->code = err;
+    if (!(numIter == P.minIter && numIter == P.maxIter)) {
+        info->norm2 = resAbs;
+        v_norminf(c, n, rj, d + SL_T2);
+        info->normInf = fetch(d + SL_T2);
+    }
+    if (numIter > P.savIter) v_copy(c, n, sv, x);
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+// ---- GMRES / FGMRES: the Hessenberg least-squares stays in FP64 on the device -----------
+
+struct GmLayout {
+    double *hh, *hcos, *hsin, *var, *h1, *h2, *out;
+    size_t  m;
+};
+
+static GmLayout gm_layout(double* gm, size_t m)
+{
+    GmLayout L;
+    L.m = m;
+    L.hh = gm;
+    L.hcos = L.hh + (m + 1) * m;
+    L.hsin = L.hcos + (m + 1);
+    L.var = L.hsin + m;
+    L.h1 = L.var + (m + 1);
+    L.h2 = L.h1 + (m + 1);
+    L.out = L.h2 + (m + 1);
+    return L;
+}
+
+// GMRES.cxx:168-203 after the dots: hh[j][c1] (CGS2: h1+h2), t = ||w||, then the previous
+// rotations, the new rotation and the updated residual estimate |var[count]|. out[1] = 0
+// when t is not > SMALL_DBL (the reference leaves the restart cycle before rotating).
+__global__ void k_gmres_givens(GmLayout L, int count, int c1, int cgs, const double* tnorm)
+{
+    const size_t m = L.m;
+#define HH(i, j) L.hh[(size_t)(i) * m + (j)]
+    if (cgs)
+        for (int j = 0; j < count; ++j) HH(j, c1) = L.h1[j] + L.h2[j];
+    double t = *tnorm;
+    HH(count, c1) = t;
+    if (!(fabs(t) > kSmallDbl)) {
+        L.out[1] = 0.0;
+        return;
+    }
+    L.out[1] = 1.0;
+    for (int j = 1; j < count; ++j) {
+        t = HH(j - 1, c1);
+        HH(j - 1, c1) = L.hsin[j - 1] * HH(j, c1) + L.hcos[j - 1] * t;
+        HH(j, c1) = -L.hsin[j - 1] * t + L.hcos[j - 1] * HH(j, c1);
+    }
+    t = HH(count, c1) * HH(count, c1);
+    t += HH(c1, c1) * HH(c1, c1);
+    t = sqrt(t);
+    const double gamma = t > kSmallDbl ? t : kSmallDbl;
+    L.hcos[c1] = HH(c1, c1) / gamma;
+    L.hsin[c1] = HH(count, c1) / gamma;
+    HH(c1, c1) = L.hsin[c1] * HH(count, c1) + L.hcos[c1] * HH(c1, c1);
+    L.var[count] = -L.hsin[c1] * L.var[c1];
+    L.var[c1] = L.hcos[c1] * L.var[c1];
+    L.out[0] = fabs(L.var[count]);
+#undef HH
+}
+
+// GMRES.cxx:213-219 (signed loop): back substitution into var[0..count)
+__global__ void k_gmres_backsolve(GmLayout L, int count, int c1)
+{
+    const size_t m = L.m;
+#define HH(i, j) L.hh[(size_t)(i) * m + (j)]
+    L.var[c1] = L.var[c1] / HH(c1, c1);
+    for (int k = count - 2; k >= 0; --k) {
+        double t = 0.0;
+        for (int j = k + 1; j < count; ++j) t -= HH(k, j) * L.var[j];
+        t += L.var[k];
+        L.var[k] = t / HH(k, k);
+    }
+#undef HH
+}
+
+__global__ void k_set_scalar(double* dst, double v) { *dst = v; }
+
+static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, double* wv)
+{
+    Ctx& c = S.c;
+    const uint32_t n = S.n;
+    const size_t ld = n;
+    double* tn = c.dslot + SL_T5;
+    if (S.cfg.orth == FASP_GPU_ORTH_MGS) { // GMRES.cxx:169-172
+        for (int j = 0; j < count; ++j) {
+            double* hj = L.hh + (size_t)j * L.m + c1;
+            v_dot(c, n, wv, S.V + j * ld, hj);
+            v_axpby(c, n, Scal::h(1.0), Scal::d(hj, -1.0), S.V + j * ld, wv);
+        }
+        v_norm2(c, n, wv, tn);
+    } else { // CGS2: two fused multi-dot / multi-AXPY passes
+        v_multidot(c, n, count, S.V, ld, wv, L.h1);
+        v_multiaxpy(c, n, count, S.V, ld, L.h1, 1.0, wv, nullptr);
+        v_multidot(c, n, count, S.V, ld, wv, L.h2);
+        v_multiaxpy(c, n, count, S.V, ld, L.h2, 1.0, wv, tn);
+    }
+    ++c.launches;
+    k_gmres_givens<<<1, 1, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn);
+    FB_CUDA(cudaGetLastError());
+    v_scale(c, n, Scal::dinv(tn), wv);
+    return kOk;
+}
+
+static void adapt_restart(SolverImpl& S, double cr, bool inclusive)
+{
+    const double maxCr = 0.99026806874157040, minCr = 0.17364817766693041;
+    const unsigned dec = 3;
+    const bool mid = inclusive ? (cr <= maxCr && cr >= minCr) : (cr < maxCr && cr > minCr);
+    if (cr > maxCr)
+        S.restart = S.maxRestart;
+    else if (mid) {
+        if (S.restart - dec > S.minRestart) // unsigned, as USI
+            S.restart -= dec;
+        else
+            S.restart = S.maxRestart;
+    }
+    if (S.restart > S.maxRestart) S.restart = S.maxRestart; // guard against the wrap
+}
+
+// GMRES::RSolve (GMRES.cxx:114-280) and FGMRES::Solve (FGMRES.cxx:108-271)
+int SolverImpl::gmres_right(const double* b, double* x, fasp_gpu_info* info, bool flexible)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double *wk = w[0], *tmp = w[1], *sv = w[2];
+    const size_t ld = n;
+    const GmLayout L = gm_layout(gm, maxRestart);
+    double* d = c.dslot;
+    int err = kOk, e;
+    double ri, rj, cr = 1.0;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, resAbsOld = 1.0;
+    uint32_t count = 1, count_1 = 2, numIter = 0;
+
+    v_copy(c, n, x, sv);
+    apply_residual(c, *A, b, x, V);
+    v_norm2(c, n, V, d + SL_T1);
+    resAbs = ri = fetch(d + SL_T1);
+    denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+
+    while (numIter < P.maxIter) {
+        if (numIter == P.minIter) {
+            resRel = resAbs / denAbs;
+            resAbsOld = resAbs;
+            rec(numIter, resAbs);
+            if (resRel < P.relTol || resAbs < P.absTol) break;
+        }
+        if (resAbs < kSmallDbl) break;
+        ++c.launches;
+        k_set_scalar<<<1, 1, 0, c.stream>>>(L.var, resAbs);
+        v_scale(c, n, Scal::h(1 / resAbs), V);
+
+        count = 0;
+        while (count < restart && numIter < P.maxIter) {
+            ++numIter;
+            count_1 = count++;
+            double* vnew = V + count * ld;
+            if (flexible) {
+                v_set(c, n, 0.0, tmp);
+                if ((e = pcd.solve(c, V + count_1 * ld, Z + count_1 * ld))) return e;
+                m_spmv(c, *A, Z + count_1 * ld, vnew);
+            } else {
+                v_set(c, n, 0.0, tmp);
+                if ((e = pcd.solve(c, V + count_1 * ld, tmp))) return e;
+                m_spmv(c, *A, tmp, vnew);
+            }
+            if ((e = orthogonalize(*this, L, count, count_1, vnew))) return e;
+            FB_CUDA(cudaMemcpyAsync(c.hslot + 2, L.out, 16, cudaMemcpyDeviceToHost, c.stream));
+            FB_CUDA(cudaStreamSynchronize(c.stream));
+            if (c.hslot[3] == 0.0) break;
+            resAbs = c.hslot[2];
+            resRel = resAbs / denAbs;
+            resAbsOld = resAbs;
+            rec(numIter, resAbs);
+            if ((resAbs < P.absTol || resRel < P.relTol) && numIter > P.minIter) break;
+        }
+
+        ++c.launches;
+
+        k_gmres_backsolve<<<1, 1, 0, c.stream>>>(L, (int)count, (int)count_1);
+        v_set(c, n, 0.0, wk);
+        v_multiaxpy(c, n, (int)count, flexible ? Z : V, ld, L.var, -1.0, wk, nullptr);
+        if (flexible) {
+            v_axpy(c, n, Scal::h(1.0), wk, x);
+        } else {
+            v_set(c, n, 0.0, tmp);
+            if ((e = pcd.solve(c, wk, tmp))) return e;
+            v_axpy(c, n, Scal::h(1.0), tmp, x);
+        }
+        if (numIter >= P.savIter && resAbs < resAbsOld) v_copy(c, n, x, sv);
+        if (numIter > P.maxIter) {
+            err = kErrMaxIt;
+            break;
+        }
+        apply_residual(c, *A, b, x, V);
+        v_norm2(c, n, V, d + SL_T1);
+        resAbs = rj = fetch(d + SL_T1);
+        resRel = resAbs / denAbs;
+        rec(numIter, resAbs);
+        if ((resRel < P.relTol || resAbs < P.absTol) && numIter >= P.minIter) break;
+        cr = rj / ri;
+        ri = rj;
+        adapt_restart(*this, cr, flexible);
+    }
+    info->numIter = numIter;
+    info->code = err;
+    if (!(numIter == P.minIter && numIter == P.maxIter)) {
+        v_norm2(c, n, V, d + SL_T1);
+        v_norminf(c, n, V, d + SL_T2);
+        info->norm2 = fetch(d + SL_T1);
+        info->normInf = fetch(d + SL_T2);
+    }
+    if (numIter > P.savIter) v_copy(c, n, sv, x);
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+// GMRES::LSolve (GMRES.cxx:283-453)
+int SolverImpl::gmres_left(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double *wk = w[0], *tmp = w[1], *sv = w[2];
+    const size_t ld = n;
+    const GmLayout L = gm_layout(gm, maxRestart);
+    double* d = c.dslot;
+    int err = kOk, e;
+    double ri, rj, cr = 1.0;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, resAbsOld = 1.0;
+    uint32_t count = 1, count_1 = 2, numIter = 0;
+
+    v_copy(c, n, x, sv);
+    apply_residual(c, *A, b, x, tmp);
+    v_norm2(c, n, tmp, d + SL_T1);
+    ri = fetch(d + SL_T1);
+    v_set(c, n, 0.0, V);
+    if ((e = pcd.solve(c, tmp, V))) return e;
+    v_norm2(c, n, V, d + SL_T1);
+    resAbs = fetch(d + SL_T1);
+    denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+
+    while (numIter < P.maxIter) {
+        if (numIter == P.minIter) {
+            resRel = resAbs / denAbs;
+            resAbsOld = resAbs;
+            rec(numIter, resAbs);
+            if (resRel < P.relTol || resAbs < P.absTol) break;
+        }
+        if (resAbs < kSmallDbl) break;
+        ++c.launches;
+        k_set_scalar<<<1, 1, 0, c.stream>>>(L.var, resAbs);
+        v_scale(c, n, Scal::h(1 / resAbs), V);
+
+        count = 0;
+        while (count < restart && numIter < P.maxIter) {
+            ++numIter;
+            count_1 = count++;
+            double* vnew = V + count * ld;
+            m_spmv(c, *A, V + count_1 * ld, tmp);
+            v_set(c, n, 0.0, vnew);
+            if ((e = pcd.solve(c, tmp, vnew))) return e;
+            if ((e = orthogonalize(*this, L, count, count_1, vnew))) return e;
+            FB_CUDA(cudaMemcpyAsync(c.hslot + 2, L.out, 16, cudaMemcpyDeviceToHost, c.stream));
+            FB_CUDA(cudaStreamSynchronize(c.stream));
+            if (c.hslot[3] == 0.0) break;
+            resAbs = c.hslot[2];
+            resAbsOld = resAbs;
+            resRel = resAbs / denAbs;
+            rec(numIter, resAbs);
+            if ((resAbs < P.absTol || resRel < P.relTol) && numIter > P.minIter) break;
+        }
+
+        ++c.launches;
+
+        k_gmres_backsolve<<<1, 1, 0, c.stream>>>(L, (int)count, (int)count_1);
+        v_set(c, n, 0.0, wk);
+        v_multiaxpy(c, n, (int)count, V, ld, L.var, -1.0, wk, nullptr);
+        v_axpy(c, n, Scal::h(1.0), wk, x);
+        if (numIter >= P.savIter && resAbs < resAbsOld) v_copy(c, n, x, sv);
+        if (numIter > P.maxIter) {
+            err = kErrMaxIt;
+            break;
+        }
+        apply_residual(c, *A, b, x, tmp);
+        v_norm2(c, n, tmp, d + SL_T1);
+        rj = fetch(d + SL_T1);
+        v_set(c, n, 0.0, V);
+        if ((e = pcd.solve(c, tmp, V))) return e;
+        v_norm2(c, n, V, d + SL_T1);
+        resAbs = fetch(d + SL_T1);
+        resRel = resAbs / denAbs;
+        rec(numIter, resAbs);
+        if ((resRel < P.relTol || resAbs < P.absTol) && numIter >= P.minIter) break;
+        cr = rj / ri;
+        ri = rj;
+        adapt_restart(*this, cr, false);
+    }
+    info->numIter = numIter;
+    info->code = err;
+    if (!(numIter == P.minIter && numIter == P.maxIter)) {
+        v_norm2(c, n, tmp, d + SL_T1);
+        v_norminf(c, n, tmp, d + SL_T2);
+        info->norm2 = fetch(d + SL_T1);
+        info->normInf = fetch(d + SL_T2);
+    }
+    if (numIter > P.savIter) v_copy(c, n, sv, x);
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+// ---- Jacobi as a solver (Iter.cxx:56-112) --------------------------------------------------
+
+int SolverImpl::jacobi(const double* b, double* x, fasp_gpu_info* info)
+{
+    double n2 = kNaN, ni = kNaN;
+    int e = pcd.solve(c, b, x, &hist, &n2, &ni);
+    if (e) return e;
+    info->code = kOk;
+    info->numIter = pcd.numIter;
+    info->norm2 = n2;
+    info->normInf = ni;
+    return kOk;
+}
+
+// ---- MG (src/MG.cxx:105-210), identity transfers, residual with the top-level A ----------
+
+void SolverImpl::mg_cycle(const double* b, double* x)
+{
+    const uint32_t NL = (uint32_t)mgSmooth.size();
+    double* r = w[0];
+    if (NL > 0) {
+        ++mgLevel;
+        if ((uint32_t)mgLevel - NL == 0) return;
+        const uint32_t L = (uint32_t)mgLevel;
+        mgSmooth[L].solve(c, b, x);
+        m_residual(c, *A, b, x, r, nullptr);
+        v_copy(c, n, r, mgB[L]);     // restriction: IdentityMatrix::Apply (MAT.cxx:1095)
+        v_set(c, n, 0.0, mgX[L]);
+        if (L + 1 - NL == 0)
+            mgCoarse[L].solve(c, mgB[L], mgX[L]);
+        else
+            for (uint32_t i = 0; i < cfg.mgCycles; ++i) mg_cycle(mgB[L], mgX[L]);
+        v_copy(c, n, mgX[L], r);     // prolongation
+        v_axpy(c, n, Scal::h(1.0), r, x);
+        mgSmooth[L].solve(c, b, x);
+        --mgLevel;
+    } else {
+        v_copy(c, n, b, x);
+    }
+}
+
+int SolverImpl::mg(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double* r = w[0];
+    double* d = c.dslot;
+    double resAbs = 1.0, resRel = 1.0, denAbs = 1.0;
+    uint32_t numIter = 0;
+    mgLevel = -1;
+    while (numIter < P.maxIter) {
+        m_residual(c, *A, b, x, r, nullptr);
+        if (numIter >= P.minIter) {
+            v_norm2(c, n, r, d + SL_T1);
+            resAbs = fetch(d + SL_T1);
+            if (numIter == P.minIter) denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+            resRel = resAbs / denAbs;
+            rec(numIter, resAbs);
+            if (resRel < P.relTol || resAbs < P.absTol) break;
+        }
+        mg_cycle(b, x);
+        ++numIter;
+    }
+    info->numIter = numIter;
+    info->code = kOk;
+    if (!(numIter == P.minIter && numIter == P.maxIter)) {
+        m_residual(c, *A, b, x, r, nullptr);
+        v_norm2(c, n, r, d + SL_T1);
+        v_norminf(c, n, r, d + SL_T2);
+        info->norm2 = resAbs = fetch(d + SL_T1);
+        info->normInf = fetch(d + SL_T2);
+        rec(numIter, resAbs);
+    }
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+// ---- dispatch ------------------------------------------------------------------------------
+
+int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
+{
+    if (!A) return kErrInputPar;
+    fasp_gpu_info tmp;
+    if (!info) info = &tmp;
+    std::memset(info, 0, sizeof(*info));
+    info->norm2 = 1e60; // SOL() initial norms (SOL.hxx:46-51)
+    info->normInf = 1e60;
+    hist.clear();
+    const unsigned long long l0 = c.launches;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, c.stream);
+    int e;
+    switch (cfg.alg) {
+        case FASP_GPU_CG:
+            if (cfg.precision == FASP_GPU_MIXED)
+                e = cg_mixed(b, x, info);
+            else if (cg64)
+                e = cg_device(b, x, info);
+            else
+                e = cg_generic(b, x, info);
+            break;
+        case FASP_GPU_BICGSTAB: e = bicgstab(b, x, info); break;
+        case FASP_GPU_GMRES:
+            e = cfg.leftPrecond ? gmres_left(b, x, info) : gmres_right(b, x, info, false);
+            break;
+        case FASP_GPU_FGMRES: e = gmres_right(b, x, info, true); break;
+        case FASP_GPU_JACOBI: e = jacobi(b, x, info); break;
+        case FASP_GPU_MG: e = mg(b, x, info); break;
+        default: e = kErrSolverType;
+    }
+    cudaEventRecord(t1, c.stream);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    lastMs = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (e == kOk && cudaGetLastError() != cudaSuccess) e = kErrCuda;
+    if (hist.size() < (size_t)info->numIter + 1) hist.resize((size_t)info->numIter + 1, kNaN);
+    info->launches = (uint32_t)(c.launches - l0);
+    return e;
+}
+
+} // namespace fb

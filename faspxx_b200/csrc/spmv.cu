@@ -1,0 +1,478 @@
+// spmv.cu -- CSRx matrices in HBM: upload and validation, SpMV (MAT::Apply), residual
+// (MAT::Residual), CSR->CSC transpose (MAT::TransInPlace), the lanes-per-row autotuner and
+// the sampled outer product of the adjoint gradient.
+//
+// SpMV mapping: a group of L lanes (L = 1, 2, ..., 32) owns one row; the lanes stride over
+// the row's entries so that a warp reads 32/L consecutive rows' values and column indices
+// as one contiguous, coalesced stream; x is gathered through L1/L2 (the stencil rows touch
+// nearby columns, so x stays cache resident). L = 1 is the scalar thread-per-row kernel and
+// L = 32 the warp-per-row vector kernel; L is chosen from the mean row length or timed.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+
+namespace fb {
+
+constexpr int kSlotResidualXinf = kSlots - 1;
+
+template <typename T, int L, bool PAT>
+__global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restrict__ x,
+                                                 T* __restrict__ y)
+{
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t r = base + sub;
+        T s = T(0);
+        if (r < A.nrow) {
+            const uint32_t b = A.rowPtr[r], e = A.rowPtr[r + 1];
+            for (uint32_t k = b + lane; k < e; k += L) {
+                const T xv = x[A.colInd[k]];
+                s = PAT ? s + xv : fma(A.val[k], xv, s);
+            }
+        }
+        s = group_sum<L>(s);
+        if (lane == 0 && r < A.nrow) y[r] = s;
+    }
+}
+
+// r = b - A x, or r = b when the device flag says NormInf(x) < CLOSE_ZERO (MAT.cxx:459-462).
+template <int L>
+__global__ void __launch_bounds__(kBlock) k_residual(CSRView<double> A, const double* __restrict__ b,
+                                                     const double* __restrict__ x,
+                                                     double* __restrict__ r,
+                                                     const double* __restrict__ xinf)
+{
+    const bool shortcut = *xinf < kCloseZero;
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t row = base + sub;
+        double s = 0.0;
+        if (row < A.nrow && !shortcut) {
+            const uint32_t bb = A.rowPtr[row], e = A.rowPtr[row + 1];
+            for (uint32_t k = bb + lane; k < e; k += L) s = fma(A.val[k], x[A.colInd[k]], s);
+        }
+        s = group_sum<L>(s);
+        if (lane == 0 && row < A.nrow) r[row] = b[row] - s;
+    }
+}
+
+static int spmv_grid(const Ctx& c, uint32_t nrow, int L)
+{
+    long long threads = (long long)nrow * L;
+    long long g = (threads + kBlock - 1) / kBlock;
+    long long cap = (long long)c.nsm * 16;
+    return (int)std::max<long long>(1, std::min(g, cap));
+}
+
+template <typename T>
+static int launch_spmv(Ctx& c, CSRView<T> A, int L, const T* x, T* y)
+{
+    if (A.nrow == 0) return kOk;
+    const int g = spmv_grid(c, A.nrow, L);
+    const bool pat = A.val == nullptr;
+#define SPMV_CASE(LL)                                                                     \
+    case LL:                                                                              \
+        if (pat)                                                                          \
+            k_spmv<T, LL, true><<<g, kBlock, 0, c.stream>>>(A, x, y);                     \
+        else                                                                              \
+            k_spmv<T, LL, false><<<g, kBlock, 0, c.stream>>>(A, x, y);                    \
+        break;
+    ++c.launches;
+    switch (L) {
+        SPMV_CASE(1)
+        SPMV_CASE(2)
+        SPMV_CASE(4)
+        SPMV_CASE(8)
+        SPMV_CASE(16)
+        SPMV_CASE(32)
+        default: return kErrInputPar;
+    }
+#undef SPMV_CASE
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+int m_spmv(Ctx& c, const Mat& A, const double* x, double* y)
+{
+    return launch_spmv<double>(c, A.v64(), A.lanes, x, y);
+}
+
+int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y)
+{
+    return launch_spmv<float>(c, A.v32(), A.lanes, x, y);
+}
+
+int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
+               const double* xinf)
+{
+    if (A.nrow == 0) return kOk;
+    if (!A.val) return kErrMatData; // MAT::Residual reads values (MAT.cxx:466)
+    if (!xinf) {
+        double* slot = c.dslot + kSlotResidualXinf;
+        int e = v_norminf(c, A.mcol, x, slot);
+        if (e) return e;
+        xinf = slot;
+    }
+    const int g = spmv_grid(c, A.nrow, A.lanes);
+    ++c.launches;
+    switch (A.lanes) {
+        case 1: k_residual<1><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        case 2: k_residual<2><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        case 4: k_residual<4><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        case 8: k_residual<8><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        case 16: k_residual<16><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        default: k_residual<32><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+    }
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+// ---- setup-time kernels ----------------------------------------------------------------
+
+// MAT::FormDiagPtr (MAT.cxx:917-928): first position whose column equals the row; rows
+// without a diagonal keep 0. GetDiag (MAT.cxx:256-267) reads values there (1 if pattern).
+__global__ void k_diag(uint32_t nrow, const uint32_t* __restrict__ rowPtr,
+                       const uint32_t* __restrict__ colInd, const double* __restrict__ val,
+                       uint32_t* __restrict__ diagPtr, double* __restrict__ diag)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nrow;
+         i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t d = 0;
+        for (uint32_t k = rowPtr[i]; k < rowPtr[i + 1]; ++k)
+            if (colInd[k] == i) {
+                d = k;
+                break;
+            }
+        diagPtr[i] = d;
+        if (diag) diag[i] = val ? val[d] : 1.0;
+    }
+}
+
+__global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+static int dmalloc(void** p, size_t bytes)
+{
+    // 16 spare bytes keep vectorised/bulk tail accesses inside the allocation
+    cudaError_t e = cudaMalloc(p, bytes + 16);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return kErrAlloc;
+    }
+    return kOk;
+}
+
+void m_free(Mat& M)
+{
+    cudaFree(M.rowPtr);
+    cudaFree(M.colInd);
+    cudaFree(M.diagPtr);
+    cudaFree(M.val);
+    cudaFree(M.val32);
+    cudaFree(M.diag);
+    M = Mat();
+}
+
+// CheckCSR (src/MATUtil.cxx:110-174) on host arrays: sizes, monotone row pointers, column
+// indices in range. A failed check returns ERROR_MAT_DATA and uploads nothing, so no kernel
+// ever indexes outside the matrix.
+static int check_csr(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+                     const uint32_t* colInd)
+{
+    if (nrow == 0 || mcol == 0 || nnz == 0) return kErrMatSize;
+    if (rowPtr[0] != 0 || rowPtr[nrow] != nnz) return kErrMatData;
+    for (uint32_t j = 0; j < nrow; ++j)
+        if (rowPtr[j] > rowPtr[j + 1]) return kErrMatData;
+    for (uint32_t k = 0; k < nnz; ++k)
+        if (colInd[k] >= mcol) return kErrMatData;
+    return kOk;
+}
+
+int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+             const uint32_t* colInd, const double* values, bool hostPtrs, cudaStream_t s)
+{
+    std::vector<uint32_t> hrp, hci;
+    const uint32_t* crp = rowPtr;
+    const uint32_t* cci = colInd;
+    if (!hostPtrs) {
+        // device arrays: validate a host copy before any kernel touches them
+        hrp.resize((size_t)nrow + 1);
+        hci.resize(nnz);
+        FB_CUDA(cudaMemcpy(hrp.data(), rowPtr, hrp.size() * 4, cudaMemcpyDeviceToHost));
+        FB_CUDA(cudaMemcpy(hci.data(), colInd, hci.size() * 4, cudaMemcpyDeviceToHost));
+        crp = hrp.data();
+        cci = hci.data();
+    }
+    int e = check_csr(nrow, mcol, nnz, crp, cci);
+    if (e) return e;
+    uint32_t maxLen = 0;
+    for (uint32_t j = 0; j < nrow; ++j) maxLen = std::max(maxLen, crp[j + 1] - crp[j]);
+
+    Mat T;
+    T.nrow = nrow;
+    T.mcol = mcol;
+    T.nnz = nnz;
+    T.maxRowLen = maxLen;
+    T.meanRowLen = (double)nnz / nrow;
+    cudaGetDevice(&T.dev);
+    const cudaMemcpyKind kind = hostPtrs ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if ((e = dmalloc((void**)&T.rowPtr, ((size_t)nrow + 1) * 4)) ||
+        (e = dmalloc((void**)&T.colInd, (size_t)nnz * 4)) ||
+        (e = dmalloc((void**)&T.diagPtr, (size_t)nrow * 4)) ||
+        (e = dmalloc((void**)&T.diag, (size_t)nrow * 8)) ||
+        (values && (e = dmalloc((void**)&T.val, (size_t)nnz * 8)))) {
+        m_free(T);
+        return e;
+    }
+    FB_CUDA(cudaMemcpyAsync(T.rowPtr, rowPtr, ((size_t)nrow + 1) * 4, kind, s));
+    FB_CUDA(cudaMemcpyAsync(T.colInd, colInd, (size_t)nnz * 4, kind, s));
+    if (values) FB_CUDA(cudaMemcpyAsync(T.val, values, (size_t)nnz * 8, kind, s));
+    k_diag<<<std::max(1, std::min(ceil_div(nrow, kBlock), 148 * 8)), kBlock, 0, s>>>(
+        nrow, T.rowPtr, T.colInd, T.val, T.diagPtr, T.diag);
+    FB_CUDA(cudaGetLastError());
+    // rows-per-warp from the row length: about two entries per lane
+    const double mean = T.meanRowLen;
+    int L = 1;
+    while (L < 32 && L * 2 <= mean) L *= 2;
+    T.lanes = L;
+    FB_CUDA(cudaStreamSynchronize(s));
+    M = T;
+    return kOk;
+}
+
+int Mat::ensure32(cudaStream_t s)
+{
+    if (val32 || !val) return kOk;
+    int e = dmalloc((void**)&val32, (size_t)nnz * 4);
+    if (e) return e;
+    k_to_f32<<<std::max(1, std::min(ceil_div(nnz, kBlock), 148 * 8)), kBlock, 0, s>>>(nnz, val,
+                                                                                      val32);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+// ---- transpose: CSR -> CSC in exactly MAT::TransInPlace's order (MAT.cxx:479-538) -------
+// Column counts by atomics, an exclusive scan, a scatter that records each entry's original
+// position, then each output row (input column) sorted by original position: since CSR
+// positions increase with the row index, that is the ascending-row order the reference's
+// row-by-row scatter produces.
+
+__global__ void k_col_count(uint32_t nnz, const uint32_t* __restrict__ colInd,
+                            uint32_t* __restrict__ cnt)
+{
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (size_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[colInd[k]], 1u);
+}
+
+// single-block exclusive scan of cnt[0..m) into out[0..m]
+__global__ void k_scan(uint32_t m, const uint32_t* __restrict__ cnt, uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t warpTot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < m; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t v = i < m ? cnt[i] : 0, incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warpTot[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            uint32_t w = lane < (int)(blockDim.x >> 5) ? warpTot[lane] : 0, wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            warpTot[lane] = wi - w; // exclusive warp offsets
+        }
+        __syncthreads();
+        if (i < m) out[i] = carry + warpTot[wid] + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += warpTot[wid] + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[m] = carry;
+}
+
+__global__ void k_row_of(uint32_t nrow, const uint32_t* __restrict__ rowPtr,
+                         uint32_t* __restrict__ rowOf)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nrow;
+         i += (size_t)gridDim.x * blockDim.x)
+        for (uint32_t k = rowPtr[i]; k < rowPtr[i + 1]; ++k) rowOf[k] = (uint32_t)i;
+}
+
+__global__ void k_scatter_pos(uint32_t nnz, const uint32_t* __restrict__ colInd,
+                              const uint32_t* __restrict__ tRowPtr, uint32_t* __restrict__ fill,
+                              uint32_t* __restrict__ pos)
+{
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t c = colInd[k];
+        const uint32_t slot = tRowPtr[c] + atomicAdd(&fill[c], 1u);
+        pos[slot] = (uint32_t)k;
+    }
+}
+
+// sort each segment of pos by value (insertion sort per thread), then gather rows/values
+__global__ void k_sort_gather(uint32_t m, const uint32_t* __restrict__ tRowPtr,
+                              uint32_t* __restrict__ pos, const uint32_t* __restrict__ rowOf,
+                              const double* __restrict__ val, uint32_t* __restrict__ tColInd,
+                              double* __restrict__ tVal)
+{
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < m;
+         c += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t b = tRowPtr[c], e = tRowPtr[c + 1];
+        for (uint32_t i = b + 1; i < e; ++i) {
+            const uint32_t key = pos[i];
+            uint32_t j = i;
+            while (j > b && pos[j - 1] > key) {
+                pos[j] = pos[j - 1];
+                --j;
+            }
+            pos[j] = key;
+        }
+        for (uint32_t i = b; i < e; ++i) {
+            const uint32_t p = pos[i];
+            tColInd[i] = rowOf[p];
+            if (val) tVal[i] = val[p];
+        }
+    }
+}
+
+int m_transpose(Ctx& c, const Mat& A, Mat& T)
+{
+    const uint32_t m = A.mcol, n = A.nrow, nnz = A.nnz;
+    Mat R;
+    R.nrow = m;
+    R.mcol = n;
+    R.nnz = nnz;
+    R.dev = A.dev;
+    uint32_t *cnt = nullptr, *fill = nullptr, *pos = nullptr, *rowOf = nullptr;
+    int e;
+    if ((e = dmalloc((void**)&R.rowPtr, ((size_t)m + 1) * 4)) ||
+        (e = dmalloc((void**)&R.colInd, (size_t)nnz * 4)) ||
+        (e = dmalloc((void**)&R.diagPtr, (size_t)m * 4)) ||
+        (e = dmalloc((void**)&R.diag, (size_t)m * 8)) ||
+        (A.val && (e = dmalloc((void**)&R.val, (size_t)nnz * 8))) ||
+        (e = dmalloc((void**)&cnt, (size_t)m * 4)) || (e = dmalloc((void**)&fill, (size_t)m * 4)) ||
+        (e = dmalloc((void**)&pos, (size_t)nnz * 4)) ||
+        (e = dmalloc((void**)&rowOf, (size_t)nnz * 4))) {
+        m_free(R);
+        cudaFree(cnt);
+        cudaFree(fill);
+        cudaFree(pos);
+        cudaFree(rowOf);
+        return e;
+    }
+    cudaStream_t s = c.stream;
+    const int gn = std::max(1, std::min(ceil_div(nnz, kBlock), c.nsm * 8));
+    const int gm = std::max(1, std::min(ceil_div(m, kBlock), c.nsm * 8));
+    const int gr = std::max(1, std::min(ceil_div(n, kBlock), c.nsm * 8));
+    FB_CUDA(cudaMemsetAsync(cnt, 0, (size_t)m * 4, s));
+    FB_CUDA(cudaMemsetAsync(fill, 0, (size_t)m * 4, s));
+    k_col_count<<<gn, kBlock, 0, s>>>(nnz, A.colInd, cnt);
+    k_scan<<<1, 1024, 0, s>>>(m, cnt, R.rowPtr);
+    k_row_of<<<gr, kBlock, 0, s>>>(n, A.rowPtr, rowOf);
+    k_scatter_pos<<<gn, kBlock, 0, s>>>(nnz, A.colInd, R.rowPtr, fill, pos);
+    k_sort_gather<<<gm, kBlock, 0, s>>>(m, R.rowPtr, pos, rowOf, A.val, R.colInd, R.val);
+    k_diag<<<gm, kBlock, 0, s>>>(m, R.rowPtr, R.colInd, R.val, R.diagPtr, R.diag);
+    FB_CUDA(cudaGetLastError());
+    FB_CUDA(cudaStreamSynchronize(s));
+    cudaFree(cnt);
+    cudaFree(fill);
+    cudaFree(pos);
+    cudaFree(rowOf);
+    R.meanRowLen = (double)nnz / m;
+    std::vector<uint32_t> hrp((size_t)m + 1);
+    FB_CUDA(cudaMemcpy(hrp.data(), R.rowPtr, hrp.size() * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t j = 0; j < m; ++j) R.maxRowLen = std::max(R.maxRowLen, hrp[j + 1] - hrp[j]);
+    R.lanes = A.lanes;
+    T = R;
+    return kOk;
+}
+
+// ---- autotuner: time each lanes-per-row choice on this matrix ---------------------------
+int m_autotune(Ctx& c, Mat& A)
+{
+    double *x = nullptr, *y = nullptr;
+    int e;
+    if ((e = dmalloc((void**)&x, (size_t)A.mcol * 8)) || (e = dmalloc((void**)&y, (size_t)A.nrow * 8))) {
+        cudaFree(x);
+        return e;
+    }
+    FB_CUDA(cudaMemsetAsync(x, 0, (size_t)A.mcol * 8, c.stream));
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    float best = 1e30f;
+    int bestL = A.lanes;
+    const int orig = A.lanes;
+    for (int L = 1; L <= 32; L *= 2) {
+        if (L > 2 * (int)A.maxRowLen && L > 1) break;
+        A.lanes = L;
+        for (int w = 0; w < 2; ++w) m_spmv(c, A, x, y);
+        cudaEventRecord(t0, c.stream);
+        for (int r = 0; r < 5; ++r) m_spmv(c, A, x, y);
+        cudaEventRecord(t1, c.stream);
+        cudaEventSynchronize(t1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t0, t1);
+        if (ms < best) {
+            best = ms;
+            bestL = L;
+        }
+    }
+    A.lanes = cudaGetLastError() == cudaSuccess ? bestL : orig;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(x);
+    cudaFree(y);
+    return kOk;
+}
+
+// ---- sampled outer product: dA_k = scale * lam[row(k)] * x[col(k)] ----------------------
+__global__ void k_sampled_outer(CSRView<double> A, const double* __restrict__ lam,
+                                const double* __restrict__ x, double scale,
+                                double* __restrict__ dA)
+{
+    // one warp per 32 rows' worth of entries: lanes stride the contiguous entry range
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.nrow;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double li = scale * lam[i];
+        for (uint32_t k = A.rowPtr[i]; k < A.rowPtr[i + 1]; ++k) dA[k] = li * x[A.colInd[k]];
+    }
+}
+
+int m_sampled_outer(Ctx& c, const Mat& A, const double* lam, const double* x, double scale,
+                    double* dA)
+{
+    const int g = std::max(1, std::min(ceil_div(A.nrow, kBlock), c.nsm * 8));
+    k_sampled_outer<<<g, kBlock, 0, c.stream>>>(A.v64(), lam, x, scale, dA);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+} // namespace fb

@@ -1,0 +1,192 @@
+/*
+ * fasp_b200.h -- C ABI of the B200 (sm_100a) iterative-solve library.
+ *
+ * Drop-in device backend for the iterative-solve path of FASP++ (FaspDevTeam/faspxx):
+ * the CSRx matrix (src/MAT.hxx), the VEC kernels the solvers use (src/VEC.hxx) and the
+ * SOL-derived solvers CG, BiCGStab, GMRES, FGMRES, Jacobi and the abstract MG
+ * (src/SOL.hxx, CG.hxx, BiCGStab.hxx, GMRES.hxx, FGMRES.hxx, Iter.hxx, MG.hxx), with the
+ * SOLParams of src/Param.hxx:57-80. Plain pointers and sizes only; every function returns
+ * an int that is a FaspRetCode value (src/RetCode.hxx:24-55) or one of the
+ * FASP_GPU_ERROR_* codes below. Index arrays are 32-bit unsigned like the reference's USI.
+ *
+ * Threading: one handle per host thread. All device work of a handle runs on the handle's
+ * own CUDA stream; calls that return results block until they are ready.
+ */
+#ifndef FASP_B200_H
+#define FASP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FASP_GPU_ABI_VERSION 1
+
+/* Device-layer failures (outside the FaspRetCode range). */
+#define FASP_GPU_ERROR_CUDA (-101)
+#define FASP_GPU_ERROR_NO_DEVICE (-102)
+
+/* Solver kinds: SOLType numbers (src/Param.hxx:36-54). */
+enum fasp_gpu_alg {
+    FASP_GPU_IDENTITY = 0,
+    FASP_GPU_CG = 1,
+    FASP_GPU_BICGSTAB = 2,
+    FASP_GPU_GMRES = 4,
+    FASP_GPU_FGMRES = 5,
+    FASP_GPU_JACOBI = 11,
+    FASP_GPU_MG = 21
+};
+
+/* Arithmetic of a solve. */
+enum fasp_gpu_precision {
+    FASP_GPU_FP64 = 0,  /* every vector and reduction in FP64, the reference's arithmetic */
+    FASP_GPU_MIXED = 1  /* FP32 inner Krylov iterations inside FP64 iterative refinement */
+};
+
+/* Gram-Schmidt variant of the GMRES/FGMRES Arnoldi step. */
+enum fasp_gpu_orth {
+    FASP_GPU_ORTH_CGS2 = 0, /* classical GS + one reorthogonalisation, fused multi-dot/AXPY */
+    FASP_GPU_ORTH_MGS = 1   /* modified GS, the reference's op sequence (GMRES.cxx:169-172) */
+};
+
+/* SOLParams (src/Param.hxx:57-80) without the name and verbosity fields. */
+typedef struct {
+    uint32_t maxIter, minIter, savIter, restart;
+    double   relTol, absTol;
+} fasp_gpu_params;
+
+/* Everything a reference driver sets on a solver and its preconditioner. The first
+ * block mirrors the oracle's configuration so parity tests pass both the same values. */
+typedef struct {
+    int             alg;        /* fasp_gpu_alg */
+    fasp_gpu_params prm;        /* SOL::Set{Max,Min,Sav}Iter, SetRestart, SetRelTol, ... */
+    double          weight;     /* Jacobi::SetWeight when alg == FASP_GPU_JACOBI */
+    uint32_t        maxRestart, minRestart; /* GMRES/FGMRES::SetMaxMinRestart; 0,0 = 30,10 */
+    int             pcd;        /* preconditioner: 0 Identity, 1 Jacobi */
+    double          pcdWeight;  /* its Jacobi weight */
+    fasp_gpu_params pcdPrm;     /* its SOLParams (maxIter = minIter = sweeps in the examples) */
+    uint32_t        mgLevels, mgCycles; /* MG::SetupALL levels, MG::SetNumCycles */
+    double          mgSmoothWeight, mgCoarseWeight;
+    fasp_gpu_params mgSmoothPrm, mgCoarsePrm;
+    /* B200 options (no reference counterpart) */
+    int             leftPrecond; /* GMRES::SetLeftPrecond (GMRES.cxx:28) */
+    int             precision;   /* fasp_gpu_precision */
+    int             orth;        /* fasp_gpu_orth */
+    double          innerRelTol; /* MIXED: relative tolerance of each FP32 inner solve */
+    uint32_t        innerMaxIter;/* MIXED: iteration cap of each inner solve */
+    uint32_t        maxOuter;    /* MIXED: refinement steps cap */
+    int             useGraph;    /* 1: device-driven iterations captured in CUDA graphs */
+} fasp_gpu_config;
+
+/* Outcome of one Solve. */
+typedef struct {
+    int      code;        /* FaspRetCode */
+    uint32_t numIter;     /* SOL::GetIterations (MIXED: inner iterations summed) */
+    double   norm2;       /* SOL::GetNorm2 */
+    double   normInf;     /* SOL::GetInfNorm */
+    uint32_t outerIter;   /* MIXED: refinement steps; otherwise 0 */
+    uint32_t escalations; /* device-driven CG: rare branches handed back to the host */
+    uint32_t launches;    /* kernels this Solve launched (graph nodes included) */
+} fasp_gpu_info;
+
+typedef struct fasp_gpu_mat_s*    fasp_gpu_mat;
+typedef struct fasp_gpu_solver_s* fasp_gpu_solver;
+
+/* ---- library ------------------------------------------------------------------------ */
+int         fasp_gpu_init(int device);              /* select the device; checks sm_100 */
+int         fasp_gpu_abi_version(void);
+const char* fasp_gpu_strerror(int code);            /* GetRetCode (src/RetCode.cxx:19-83) */
+void        fasp_gpu_default_config(fasp_gpu_config* cfg, int alg); /* SOLParams() defaults */
+
+/* ---- device memory helpers (so hosts need no CUDA runtime of their own) -------------- */
+int fasp_gpu_malloc(void** dptr, size_t bytes);
+int fasp_gpu_free(void* dptr);
+int fasp_gpu_memcpy_h2d(void* dst, const void* src, size_t bytes);
+int fasp_gpu_memcpy_d2h(void* dst, const void* src, size_t bytes);
+int fasp_gpu_synchronize(void);
+int fasp_gpu_host_alloc(void** hptr, size_t bytes); /* page-locked host memory */
+int fasp_gpu_host_free(void* hptr);
+
+/* ---- MAT: CSRx matrix in HBM (src/MAT.hxx, MAT.cxx) --------------------------------- */
+/* MAT(nrow, mcol, nnz, values, colInd, rowPtr) (MAT.cxx:41-57) from HOST arrays; the
+ * diagonal pointers are formed as FormDiagPtr does (MAT.cxx:917-928). values == NULL
+ * builds a sparsity structure (MAT.cxx:60-75). Structure is checked like CheckCSR
+ * (MATUtil.cxx:110-174): ERROR_MAT_DATA and no upload if it fails. */
+int fasp_gpu_mat_create(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+                        const uint32_t* colInd, const double* values, fasp_gpu_mat* out);
+/* Same from DEVICE arrays (copied). */
+int fasp_gpu_mat_create_device(uint32_t nrow, uint32_t mcol, uint32_t nnz,
+                               const uint32_t* rowPtr, const uint32_t* colInd,
+                               const double* values, fasp_gpu_mat* out);
+int fasp_gpu_mat_destroy(fasp_gpu_mat A);
+/* GetRowSize / GetColSize / GetNNZ (LOP.hxx:50-53, MAT.hxx:113) */
+int fasp_gpu_mat_info(fasp_gpu_mat A, uint32_t* nrow, uint32_t* mcol, uint32_t* nnz);
+/* GetRowPtr / GetColInd / GetValues / diagPtr to HOST arrays (MAT.cxx:627-649); any may be
+ * NULL. */
+int fasp_gpu_mat_download(fasp_gpu_mat A, uint32_t* rowPtr, uint32_t* colInd, double* values,
+                          uint32_t* diagPtr);
+/* MAT::Apply, w = A v (MAT.cxx:373-452), device vectors. */
+int fasp_gpu_mat_apply(fasp_gpu_mat A, const double* v, double* w);
+/* MAT::Residual, r = b - A x with its x ~ 0 shortcut (MAT.cxx:455-476). */
+int fasp_gpu_mat_residual(fasp_gpu_mat A, const double* b, const double* x, double* r);
+/* MAT::TransInPlace (MAT.cxx:479-538) into a new handle; structure and order bit-exact. */
+int fasp_gpu_mat_transpose(fasp_gpu_mat A, fasp_gpu_mat* out);
+/* MAT::GetDiag (MAT.cxx:256-267) into a device vector. */
+int fasp_gpu_mat_diag(fasp_gpu_mat A, double* diag);
+/* Rows-per-warp autotuner: times every lanes-per-row choice on A; returns the pick. */
+int fasp_gpu_mat_autotune(fasp_gpu_mat A, int* lanes);
+int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes);
+/* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
+ * value copy (fp32 = 1), timed with CUDA events on the matrix's stream (inputs: x = 0). */
+int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, double* ms);
+/* Sampled outer product on A's pattern: dA[k] = scale * lam[row(k)] * x[col(k)]. The
+ * matrix gradient dL/dA of x = A^-1 b is the case scale = -1 (no reference counterpart). */
+int fasp_gpu_mat_sampled_outer(fasp_gpu_mat A, const double* lam, const double* x,
+                               double scale, double* dA);
+
+/* ---- VEC kernels on device vectors (src/VEC.cxx) ------------------------------------ */
+int fasp_gpu_vec_dot(uint32_t n, const double* a, const double* b, double* result);    /* :468 */
+int fasp_gpu_vec_norm2(uint32_t n, const double* a, double* result);                   /* :424 */
+int fasp_gpu_vec_norminf(uint32_t n, const double* a, double* result);                 /* :441 */
+int fasp_gpu_vec_axpy(uint32_t n, double a, const double* x, double* y);               /* :245 */
+int fasp_gpu_vec_xpay(uint32_t n, double a, const double* x, double* y);               /* :259 */
+int fasp_gpu_vec_axpby(uint32_t n, double a, double b, const double* y, double* x);    /* :274 */
+int fasp_gpu_vec_waxpby(uint32_t n, double a, const double* v1, double b, const double* v2,
+                        double* w);                                                    /* :329 */
+int fasp_gpu_vec_scale(uint32_t n, double a, double* x);                               /* :154 */
+
+/* ---- SOL: solvers (src/SOL.hxx and subclasses) -------------------------------------- */
+int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out);
+/* Setup(const LOP& A): binds A (the caller keeps it alive, as SOL keeps a raw pointer,
+ * SOL.hxx:28), builds the preconditioner (Jacobi::Setup, Iter.cxx:29-53) and work space. */
+int fasp_gpu_solver_setup(fasp_gpu_solver s, fasp_gpu_mat A);
+/* Solve(b, x) on DEVICE vectors: x is the initial guess in, the solution out. */
+int fasp_gpu_solver_solve(fasp_gpu_solver s, const double* b, double* x, fasp_gpu_info* info);
+/* Solve(b, x) on HOST vectors: copies in, solves, copies out (end-to-end path). */
+int fasp_gpu_solver_solve_host(fasp_gpu_solver s, const double* b, double* x,
+                               fasp_gpu_info* info);
+/* Residual norms the last Solve held at the end of each iteration (NaN where the solver
+ * computes none); *len receives numIter + 1. */
+int fasp_gpu_solver_history(fasp_gpu_solver s, double* hist, uint32_t cap, uint32_t* len);
+int fasp_gpu_solver_clean(fasp_gpu_solver s);     /* SOL::Clean */
+int fasp_gpu_solver_destroy(fasp_gpu_solver s);
+/* Device time of the last Solve in milliseconds (CUDA events around its device work). */
+int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms);
+/* Device-driven CG only: average duration (ms) of each of its two fused kernels over reps
+ * launches, timed alone with CUDA events on the solver's stream (control logic bypassed;
+ * the solver's internal vectors are overwritten). ms[0]: SpMV kernel, ms[1]: update kernel.
+ * Times the FP32 engine when the solver is MIXED. */
+int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, double* ms);
+
+/* ---- adjoint (no reference counterpart) --------------------------------------------- */
+/* Solve A^T lam = g with the same Krylov kernels on the exact CSC transpose of the bound
+ * matrix (built once, cached). */
+int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* lam,
+                                  fasp_gpu_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASP_B200_H */
