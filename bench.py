@@ -205,7 +205,7 @@ def run_ours(args):
     A, b = problem(args.size)
     n, nnz = A.nrow, A.nnz
     M = sol.MAT(A)
-    lanes = M.Autotune()
+    lanes = M.Autotune() if not args.lanes else (M.SetLanes(args.lanes) or args.lanes)
 
     def make(precision):
         s = sol.CG()
@@ -223,6 +223,13 @@ def run_ours(args):
         return s
 
     mixed, fp64 = make(capi.MIXED), make(capi.FP64)
+    if args.profile:
+        # 3 warm-up + 1 launch of cg_spmv and cg_update per engine: FP32 first, then FP64
+        km = (C.c_double * 2)()
+        for s in (mixed, fp64):
+            capi.check(lib.fasp_gpu_solver_kernel_times(s.h, 1, km), "kernel_times")
+            print(f"profile lanes={lanes} spmv {km[0]*1e3:.1f} us update {km[1]*1e3:.1f} us")
+        return 0
     db = sol.DVec.from_numpy(b)
     dx = sol.DVec(n)
 
@@ -387,6 +394,9 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=1e-4)
     ap.add_argument("--ref-sample", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0, help="force SpMV lanes per row")
+    ap.add_argument("--profile", action="store_true",
+                    help="only set up and launch each fused CG kernel 4 times (for ncu)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

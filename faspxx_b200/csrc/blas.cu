@@ -13,10 +13,10 @@ namespace fb {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)(n); \
          i += (size_t)gridDim.x * blockDim.x)
 
-int Ctx::grid(long long work, int perBlock) const
+int Ctx::grid(long long work, int perBlock, int perSM) const
 {
     long long g = (work + perBlock - 1) / perBlock;
-    long long cap = (long long)nsm * 8;
+    long long cap = (long long)nsm * perSM;
     if (cap > kMaxGrid) cap = kMaxGrid;
     if (g > cap) g = cap;
     if (g < 1) g = 1;

@@ -138,6 +138,19 @@ __device__ void cg_checks(CGCtl* c, const double* red, int phase)
 
 // ---- kernels ---------------------------------------------------------------------------
 
+template <typename T>
+struct V16;
+template <>
+struct V16<float> {
+    typedef float4 t;
+    enum { W = 4 };
+};
+template <>
+struct V16<double> {
+    typedef double2 t;
+    enum { W = 2 };
+};
+
 template <typename T, int L>
 __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, CGCtl* c,
@@ -148,13 +161,26 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
+    T acc = T(0);
+    if (L == 1) { // thread per row
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x) {
+            const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
+            const T sum = row_dot<T, false>(A, b, e, [&](uint32_t j) {
+                return mode ? fma(beta, pOld[j], z[j]) : z[j];
+            });
+            const T pi = mode ? fma(beta, pOld[row], z[row]) : z[row];
+            pNew[row] = pi;
+            q[row] = sum;
+            acc = fma(sum, pi, acc);
+        }
+    }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
     const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
     const size_t sub = (threadIdx.x & 31) / L;
-    T acc = T(0);
-    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+    for (size_t base = gw * warpRows; L > 1 && base < A.nrow; base += nwarps * warpRows) {
         const size_t row = base + sub;
         T sum = T(0);
         if (row < A.nrow) {
@@ -193,23 +219,41 @@ __global__ void __launch_bounds__(kBlock) cg_update(uint32_t n, T* __restrict__ 
     const T alpha = (T)c->alpha;
     const T* __restrict__ p = c->par ? P1 : P0;
     T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
-    GRID_STRIDE(i, n)
-    {
-        const T pi = p[i];
-        const T xi = fma(alpha, pi, x[i]);
-        const T ri = fma(-alpha, q[i], r[i]);
-        x[i] = xi;
-        r[i] = ri;
-        T zi = ri;
-        if (JAC) {
-            zi = dinv[i] * ri;
-            z[i] = zi;
-        }
+    auto one = [&](T pi, T& xi, T& ri, T qi, T di, T& zi) {
+        xi = fma(alpha, pi, xi);
+        ri = fma(-alpha, qi, ri);
+        zi = JAC ? di * ri : ri;
         rr = fma(ri, ri, rr);
         zr = fma(zi, ri, zr);
         xx = fma(xi, xi, xx);
         xm = fmax(xm, fabs(xi));
         pp = fma(pi, pi, pp);
+    };
+    // 16-byte accesses: all vectors are the engine's own 256-byte aligned allocations
+    using V = typename V16<T>::t;
+    constexpr int W = V16<T>::W;
+    const size_t nv = n / W;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i < nv; i += stride) {
+        T pa[W], xa[W], ra[W], qa[W], da[W], za[W];
+        *(V*)pa = ((const V*)p)[i];
+        *(V*)xa = ((const V*)x)[i];
+        *(V*)ra = ((const V*)r)[i];
+        *(V*)qa = ((const V*)q)[i];
+        if (JAC) *(V*)da = ((const V*)dinv)[i];
+#pragma unroll
+        for (int u = 0; u < W; ++u) one(pa[u], xa[u], ra[u], qa[u], JAC ? da[u] : T(0), za[u]);
+        ((V*)x)[i] = *(V*)xa;
+        ((V*)r)[i] = *(V*)ra;
+        if (JAC) ((V*)z)[i] = *(V*)za;
+    }
+    for (size_t i = nv * W + tid; i < n; i += stride) {
+        T xi = x[i], ri = r[i], zi;
+        one(p[i], xi, ri, q[i], JAC ? dinv[i] : T(0), zi);
+        x[i] = xi;
+        r[i] = ri;
+        if (JAC) z[i] = zi;
     }
     double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
     const int ops[5] = {kSum, kSum, kSum, kMax, kSum};
@@ -290,7 +334,7 @@ __global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restr
 static int spmv_grid_cg(const Ctx& c, uint32_t nrow, int L)
 {
     long long g = ((long long)nrow * L + kBlock - 1) / kBlock;
-    long long cap = (long long)c.nsm * 16;
+    long long cap = (long long)c.nsm * 8;
     if (cap > kMaxGrid) cap = kMaxGrid;
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
@@ -307,7 +351,7 @@ int CGEngine<T>::launch_iter()
 {
     const CSRView<T> V = view_of<T>(*A);
     const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
-    const int g2 = c->grid(n, kBlock);
+    const int g2 = c->grid(n / V16<T>::W + 1, kBlock, 4);
     const T* zz = jacobi ? z : r;
     if (!capturing) c->launches += 2;
     switch (A->lanes) {
@@ -491,7 +535,7 @@ int CGEngine<T>::time_kernels(unsigned reps, double* ms)
     if (e) return e;
     const CSRView<T> V = view_of<T>(*A);
     const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
-    const int g2 = c->grid(n, kBlock);
+    const int g2 = c->grid(n / V16<T>::W + 1, kBlock, 4);
     const T* zz = jacobi ? z : r;
     cudaEvent_t ev[3];
     for (auto& x0 : ev) FB_CUDA(cudaEventCreate(&x0));

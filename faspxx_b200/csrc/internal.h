@@ -70,7 +70,8 @@ struct Ctx {
     unsigned long long launches = 0; // kernels launched on this context
     int init(int device);
     void destroy();
-    int  grid(long long work, int perBlock) const;  // fixed-size grids for reductions
+    // fixed-size grids (reductions depend on them): at most perSM blocks per SM
+    int  grid(long long work, int perBlock, int perSM = 8) const;
     int  sync();
     int  fetch(int slot, double* out);               // read one device scalar (synchronous)
 };
@@ -128,6 +129,7 @@ int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y);
 int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
                const double* xinf);
 int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR -> CSC, exact
+int lanes_for(double meanRowLen);                                         // SpMV mapping
 int m_autotune(Ctx& c, Mat& A);
 // dA[k] = scale * lam[row(k)] * x[col(k)] on the sparsity pattern (sampled outer product)
 int m_sampled_outer(Ctx& c, const Mat& A, const double* lam, const double* x, double scale,

@@ -21,6 +21,14 @@ template <typename T, int L, bool PAT>
 __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restrict__ x,
                                                  T* __restrict__ y)
 {
+    if (L == 1) { // thread per row: short rows (stencils)
+        for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.nrow;
+             r += (size_t)gridDim.x * blockDim.x) {
+            const uint32_t b = ld_stream(A.rowPtr + r), e = ld_stream(A.rowPtr + r + 1);
+            y[r] = row_dot<T, PAT>(A, b, e, [&](uint32_t j) { return x[j]; });
+        }
+        return;
+    }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
     const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -32,8 +40,8 @@ __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restri
         if (r < A.nrow) {
             const uint32_t b = A.rowPtr[r], e = A.rowPtr[r + 1];
             for (uint32_t k = b + lane; k < e; k += L) {
-                const T xv = x[A.colInd[k]];
-                s = PAT ? s + xv : fma(A.val[k], xv, s);
+                const T xv = x[ld_stream(A.colInd + k)];
+                s = PAT ? s + xv : fma(ld_stream(A.val + k), xv, s);
             }
         }
         s = group_sum<L>(s);
@@ -49,6 +57,18 @@ __global__ void __launch_bounds__(kBlock) k_residual(CSRView<double> A, const do
                                                      const double* __restrict__ xinf)
 {
     const bool shortcut = *xinf < kCloseZero;
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x) {
+            double s = 0.0;
+            if (!shortcut) {
+                const uint32_t bb = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
+                s = row_dot<double, false>(A, bb, e, [&](uint32_t j) { return x[j]; });
+            }
+            r[row] = b[row] - s;
+        }
+        return;
+    }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
     const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -70,8 +90,18 @@ static int spmv_grid(const Ctx& c, uint32_t nrow, int L)
 {
     long long threads = (long long)nrow * L;
     long long g = (threads + kBlock - 1) / kBlock;
-    long long cap = (long long)c.nsm * 16;
+    long long cap = (long long)c.nsm * 8; // resident at 2048 threads per SM
     return (int)std::max<long long>(1, std::min(g, cap));
+}
+
+// Lanes per row from the mean row length: one thread per row up to 16 entries (measured
+// fastest for 5- and 7-point stencils on B200), then about 8 entries per lane.
+int lanes_for(double mean)
+{
+    if (mean <= 16) return 1;
+    int L = 2;
+    while (L < 32 && L * 8 < mean) L *= 2;
+    return L;
 }
 
 template <typename T>
@@ -245,11 +275,7 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
     k_diag<<<std::max(1, std::min(ceil_div(nrow, kBlock), 148 * 8)), kBlock, 0, s>>>(
         nrow, T.rowPtr, T.colInd, T.val, T.diagPtr, T.diag);
     FB_CUDA(cudaGetLastError());
-    // rows-per-warp from the row length: about two entries per lane
-    const double mean = T.meanRowLen;
-    int L = 1;
-    while (L < 32 && L * 2 <= mean) L *= 2;
-    T.lanes = L;
+    T.lanes = lanes_for(T.meanRowLen);
     FB_CUDA(cudaStreamSynchronize(s));
     M = T;
     return kOk;
