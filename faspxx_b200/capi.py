@@ -82,6 +82,7 @@ SIGNATURES = {
     "fasp_gpu_vec_axpby": (_i, [_u32, _d, _d, _vp, _vp]),
     "fasp_gpu_vec_waxpby": (_i, [_u32, _d, _vp, _d, _vp, _vp]),
     "fasp_gpu_vec_scale": (_i, [_u32, _d, _vp]),
+    "fasp_gpu_vec_dot_noalloc": (_i, [_u32, _vp, _vp, _P(_d)]),
     "fasp_gpu_solver_create": (_i, [_P(Config), _P(_vp)]),
     "fasp_gpu_solver_setup": (_i, [_vp, _vp]),
     "fasp_gpu_solver_solve": (_i, [_vp, _vp, _vp, _P(Info)]),

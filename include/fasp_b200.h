@@ -156,6 +156,17 @@ int fasp_gpu_vec_axpby(uint32_t n, double a, double b, const double* y, double* 
 int fasp_gpu_vec_waxpby(uint32_t n, double a, const double* v1, double b, const double* v2,
                         double* w);                                                    /* :329 */
 int fasp_gpu_vec_scale(uint32_t n, double a, double* x);                               /* :154 */
+/* No counterpart in the reference. The dot product of fasp_gpu_vec_dot for callers that
+ * cannot allocate device memory (for example code running while a CUDA graph is being
+ * captured in global mode, code under a memory pool that has reserved the device, or a
+ * latency-critical loop where cudaMalloc/cudaFree would synchronize the device). It calls
+ * no allocator: its reduction scratch (about 32 KB) is a static device array that every GPU
+ * loading this library holds until exit. n is limited to 8,388,608 elements; larger n
+ * returns ERROR_VEC_SIZE. Runs on the legacy default stream and blocks until *result (host)
+ * is written. All calls share the one scratch array: calls that overlap on the GPU race and
+ * must be serialised by the caller. The first call on each device sets up the array's
+ * address with that device current; make it before any stream capture begins. */
+int fasp_gpu_vec_dot_noalloc(uint32_t n, const double* a, const double* b, double* result);
 
 /* ---- SOL: solvers (src/SOL.hxx and subclasses) -------------------------------------- */
 int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out);
