@@ -225,10 +225,11 @@ def run_ours(args):
     mixed, fp64 = make(capi.MIXED), make(capi.FP64)
     if args.profile:
         # 3 warm-up + 1 launch of cg_spmv and cg_update per engine: FP32 first, then FP64
-        km = (C.c_double * 2)()
+        km = (C.c_double * 3)()
         for s in (mixed, fp64):
             capi.check(lib.fasp_gpu_solver_kernel_times(s.h, 1, km), "kernel_times")
-            print(f"profile lanes={lanes} spmv {km[0]*1e3:.1f} us update {km[1]*1e3:.1f} us")
+            print(f"profile lanes={lanes} spmv {km[0]*1e3:.1f} us update {km[1]*1e3:.1f} us "
+                  f"persistent iteration {km[2]*1e3:.1f} us")
         return 0
     db = sol.DVec.from_numpy(b)
     dx = sol.DVec(n)
@@ -309,9 +310,9 @@ def run_ours(args):
 
     # kernel rooflines (each kernel alone, CUDA events on the library's stream)
     hbm, peak_kind = peaks()
-    km = (C.c_double * 2)()
+    km = (C.c_double * 3)()
     capi.check(lib.fasp_gpu_solver_kernel_times(mixed.h, 50, km), "kernel_times")
-    k64 = (C.c_double * 2)()
+    k64 = (C.c_double * 3)()
     capi.check(lib.fasp_gpu_solver_kernel_times(fp64.h, 50, k64), "kernel_times")
     sp = C.c_double()
     capi.check(lib.fasp_gpu_mat_time_apply(M.h, 50, 0, C.byref(sp)), "time_apply")
@@ -322,13 +323,29 @@ def run_ours(args):
     b_upd64 = 8 * n * 5 + 8 * n * 3
     b_apply = 12 * nnz + 4 * (n + 1) + 16 * n
     gbs = lambda byt, ms: byt / (ms * 1e-3) / 1e9  # noqa: E731
-    ach = gbs(b_spmv32, km[0])
-    roofline = {"kernel": "cg_spmv<float> (SpMV + p update + (Ap,p), FP32 inner CG)",
-                "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(ach / hbm, 3), "traffic": None,
-                "peak_source": f"{peak_kind} hbm_gbs",
-                "bytes_per_launch": b_spmv32, "ms_per_launch": round(km[0], 5)}
+    if km[2] > 0:
+        # the persistent kernel runs the whole FP32 inner solve: one iteration = both phases
+        b_it32 = b_spmv32 + b_upd32
+        ach = gbs(b_it32, km[2])
+        roofline = {"kernel": "cg_persistent<float,JAC> (one FP32 PCG iteration: SpMV + p "
+                              "update + x,r,z updates + 6 reductions, 2 grid barriers)",
+                    "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 3), "traffic": None,
+                    "peak_source": f"{peak_kind} hbm_gbs",
+                    "bytes_per_launch": b_it32, "ms_per_launch": round(km[2], 5),
+                    "unit_of_work": "one CG iteration (the kernel loops over iterations)"}
+    else:
+        ach = gbs(b_spmv32, km[0])
+        roofline = {"kernel": "cg_spmv<float> (SpMV + p update + (Ap,p), FP32 inner CG)",
+                    "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 3), "traffic": None,
+                    "peak_source": f"{peak_kind} hbm_gbs",
+                    "bytes_per_launch": b_spmv32, "ms_per_launch": round(km[0], 5)}
     kernels = {
+        "cg_persistent_f32_iter": {"ms": round(km[2], 5),
+                                   "gbs": round(gbs(b_spmv32 + b_upd32, km[2]), 1) if km[2] else None},
+        "cg_persistent_f64_iter": {"ms": round(k64[2], 5),
+                                   "gbs": round(gbs(b_spmv64 + b_upd64, k64[2]), 1) if k64[2] else None},
         "cg_spmv_f32": {"ms": round(km[0], 5), "gbs": round(gbs(b_spmv32, km[0]), 1)},
         "cg_update_f32": {"ms": round(km[1], 5), "gbs": round(gbs(b_upd32, km[1]), 1)},
         "cg_spmv_f64": {"ms": round(k64[0], 5), "gbs": round(gbs(b_spmv64, k64[0]), 1)},

@@ -37,7 +37,7 @@ class Config(C.Structure):
                 ("mgSmoothPrm", Params), ("mgCoarsePrm", Params),
                 ("leftPrecond", C.c_int), ("precision", C.c_int), ("orth", C.c_int),
                 ("innerRelTol", C.c_double), ("innerMaxIter", C.c_uint32),
-                ("maxOuter", C.c_uint32), ("useGraph", C.c_int)]
+                ("maxOuter", C.c_uint32), ("useGraph", C.c_int), ("persistent", C.c_int)]
 
 
 class Info(C.Structure):
@@ -93,6 +93,11 @@ SIGNATURES = {
     "fasp_gpu_solver_last_time": (_i, [_vp, _P(_d)]),
     "fasp_gpu_solver_kernel_times": (_i, [_vp, _u32, _P(_d)]),
     "fasp_gpu_solver_solve_adjoint": (_i, [_vp, _vp, _vp, _P(Info)]),
+    "fasp_gpu_batch_create": (_i, [_u32, _vp, _u32, _vp, _vp, _vp, _u32, _P(_vp)]),
+    "fasp_gpu_batch_set_shape": (_i, [_vp, _i, _i]),
+    "fasp_gpu_batch_solve": (_i, [_vp, _vp, _vp, _d, _u32, _i, _d, _vp, _vp]),
+    "fasp_gpu_batch_last_time": (_i, [_vp, _P(_d)]),
+    "fasp_gpu_batch_destroy": (_i, [_vp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -1,0 +1,496 @@
+// batch.cu -- many independent Jacobi-PCG solves in one persistent launch.
+//
+// The systems are the diagonal blocks of one CSRx matrix (global row and column indices,
+// block k = rows sysRow[k]..sysRow[k+1]); each has nrhs right-hand sides stored right-hand-
+// side-major, b[r * N + row]. A fixed grid of blocks pulls work items from an atomic queue
+// ordered by decreasing size (longest first balances the tail); one work item is one
+// system with all its right-hand sides, so every matrix entry is loaded once for all of
+// them. A CUDA block runs CG for its system with block-level reductions only: no grid-wide
+// synchronisation, no host round trip, convergence decided on the device. Each iteration
+// is two passes over the system's rows:
+//   1. q = A p with p = z + beta p_old formed on the fly (double-buffered p), and (q, p);
+//   2. x += alpha p, r -= alpha q, z = diagInv .* r, and (r, r), (z, r).
+// The CG recurrences are those of CG::Solve (src/CG.cxx:69-234) with x0 = 0 and the
+// stopping test ||r|| < relTol ||r0||; right-hand sides converge (and freeze) separately.
+// Precision FP64, or FP32 (values, vectors and per-thread sums) inside FP64 refinement:
+// r = b - A x in FP64, the FP32 CG solves A e = r / ||r|| to innerTol, x += ||r|| e.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "../../include/fasp_b200.h"
+#include "internal.h"
+
+namespace fb {
+
+constexpr int kMaxRhs = 4;
+
+template <typename T>
+struct BatchArgs {
+    uint32_t        count, nrhs, N;
+    const uint32_t* sysRow;
+    const uint32_t* order;
+    const uint32_t* rowPtr;
+    const uint32_t* colInd;
+    const T*        val;
+    const T*        dinv;
+    const T*        b;        // rhs-major [nrhs][N]
+    T*              x;
+    T*              r;
+    T*              z;
+    T*              p0;
+    T*              p1;
+    T*              q;
+    uint32_t*       iters;    // [count][nrhs], accumulated across calls (refinement)
+    double*         resRel;   // [count][nrhs] final relative residual estimate
+    double          relTol;
+    uint32_t        maxIter;
+    unsigned*       queue;
+};
+
+template <int NV>
+__device__ __forceinline__ void bsum(double (&v)[NV])
+{
+    int ops[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) ops[k] = kSum;
+    block_reduce<NV>(v, ops);
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(512) batch_pcg(BatchArgs<T> a)
+{
+    __shared__ unsigned item;
+    __shared__ double sh[3 * kMaxRhs];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        if (item >= a.count) return;
+        const uint32_t sys = a.order[item];
+        const uint32_t r0 = a.sysRow[sys], r1 = a.sysRow[sys + 1];
+        // start: x = 0, r = b, z = diagInv .* r, (r, r), (z, r)
+        double acc[2 * NR];
+#pragma unroll
+        for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+        for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+            const T d = a.dinv[i];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                const size_t o = (size_t)k * a.N + i;
+                const T bi = a.b[o];
+                a.x[o] = T(0);
+                a.r[o] = bi;
+                a.z[o] = d * bi;
+                acc[k] += (double)bi * bi;
+                acc[NR + k] += (double)(d * bi) * bi;
+            }
+        }
+        bsum<2 * NR>(acc);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) sh[k] = acc[k];
+        __syncthreads();
+        double tol[NR], rz[NR], beta[NR];
+        bool active[NR];
+        int nact = 0;
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            tol[k] = a.relTol * sqrt(sh[k]);
+            rz[k] = sh[NR + k];
+            beta[k] = 0.0;
+            active[k] = sqrt(sh[k]) > tol[k] && sh[k] > 0.0;
+            nact += active[k];
+        }
+        uint32_t it = 0;
+        int par = 0;
+        double last[NR];
+#pragma unroll
+        for (int k = 0; k < NR; ++k) last[k] = 1.0;
+        while (nact > 0 && it < a.maxIter) {
+            ++it;
+            const T* pOld = par ? a.p1 : a.p0;
+            T* pNew = par ? a.p0 : a.p1;
+            // pass 1: q = A p, p formed on the fly; (q, p)
+            double pq[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) pq[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const uint32_t kb = a.rowPtr[i], ke = a.rowPtr[i + 1];
+                T s[NR];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) s[k] = T(0);
+                for (uint32_t e = kb; e < ke; ++e) {
+                    const uint32_t j = __ldg(a.colInd + e);
+                    const T v = __ldg(a.val + e);
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) {
+                        if (!active[k]) continue;
+                        const size_t o = (size_t)k * a.N + j;
+                        const T pj = it == 1 ? a.z[o] : fma((T)beta[k], pOld[o], a.z[o]);
+                        s[k] = fma(v, pj, s[k]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    if (!active[k]) continue;
+                    const size_t o = (size_t)k * a.N + i;
+                    const T pi = it == 1 ? a.z[o] : fma((T)beta[k], pOld[o], a.z[o]);
+                    pNew[o] = pi;
+                    a.q[o] = s[k];
+                    pq[k] += (double)s[k] * pi;
+                }
+            }
+            bsum<NR>(pq);
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int k = 0; k < NR; ++k) sh[k] = pq[k];
+            __syncthreads();
+            T alpha[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) alpha[k] = active[k] && sh[k] != 0.0 ? (T)(rz[k] / sh[k]) : T(0);
+            // pass 2: x += alpha p, r -= alpha q, z = diagInv .* r; (r, r), (z, r)
+            double red[2 * NR];
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) red[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const T d = a.dinv[i];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    if (!active[k]) continue;
+                    const size_t o = (size_t)k * a.N + i;
+                    const T xi = fma(alpha[k], pNew[o], a.x[o]);
+                    const T ri = fma(-alpha[k], a.q[o], a.r[o]);
+                    const T zi = d * ri;
+                    a.x[o] = xi;
+                    a.r[o] = ri;
+                    a.z[o] = zi;
+                    red[k] += (double)ri * ri;
+                    red[NR + k] += (double)zi * ri;
+                }
+            }
+            bsum<2 * NR>(red);
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int k = 0; k < 2 * NR; ++k) sh[k] = red[k];
+            __syncthreads();
+            nact = 0;
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                if (!active[k]) continue;
+                const double res = sqrt(sh[k]);
+                last[k] = res;
+                if (res < tol[k] || !(sh[NR + k] == sh[NR + k])) {
+                    active[k] = false;
+                } else {
+                    beta[k] = sh[NR + k] / rz[k];
+                    rz[k] = sh[NR + k];
+                    ++nact;
+                }
+            }
+            par ^= 1;
+        }
+        if (threadIdx.x < NR) {
+            const int k = threadIdx.x;
+            a.iters[(size_t)sys * a.nrhs + k] += it;
+            a.resRel[(size_t)sys * a.nrhs + k] = tol[k] > 0 ? last[k] * a.relTol / tol[k] : 0.0;
+        }
+    }
+}
+
+// FP64 residual of every system and right-hand side, r64 = b - A x (the outer step of the
+// mixed solve), with ||r|| per (system, rhs) and the FP32 right-hand side r / ||r||.
+__global__ void __launch_bounds__(256) batch_residual(uint32_t count, uint32_t nrhs, uint32_t N,
+                                                      const uint32_t* sysRow,
+                                                      const uint32_t* rowPtr,
+                                                      const uint32_t* colInd, const double* val,
+                                                      const double* b, const double* x,
+                                                      double* r64, double* rnorm)
+{
+    // one block per (system, rhs)
+    const uint32_t id = blockIdx.x;
+    if (id >= count * nrhs) return;
+    const uint32_t sys = id / nrhs, k = id % nrhs;
+    const uint32_t r0 = sysRow[sys], r1 = sysRow[sys + 1];
+    double acc[1] = {0.0};
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t e = rowPtr[i]; e < rowPtr[i + 1]; ++e)
+            s = fma(val[e], x[(size_t)k * N + colInd[e]], s);
+        const double ri = b[(size_t)k * N + i] - s;
+        r64[(size_t)k * N + i] = ri;
+        acc[0] = fma(ri, ri, acc[0]);
+    }
+    bsum<1>(acc);
+    if (threadIdx.x == 0) rnorm[id] = sqrt(acc[0]);
+}
+
+__global__ void batch_scale_to32(uint32_t count, uint32_t nrhs, uint32_t N,
+                                 const uint32_t* sysRow, const double* r64,
+                                 const double* rnorm, float* b32)
+{
+    const uint32_t id = blockIdx.x;
+    if (id >= count * nrhs) return;
+    const uint32_t sys = id / nrhs, k = id % nrhs;
+    const double s = rnorm[id] > 0 ? 1.0 / rnorm[id] : 0.0;
+    for (uint32_t i = sysRow[sys] + threadIdx.x; i < sysRow[sys + 1]; i += blockDim.x)
+        b32[(size_t)k * N + i] = (float)(r64[(size_t)k * N + i] * s);
+}
+
+__global__ void batch_update64(uint32_t count, uint32_t nrhs, uint32_t N,
+                               const uint32_t* sysRow, const double* rnorm, const float* e32,
+                               double* x)
+{
+    const uint32_t id = blockIdx.x;
+    if (id >= count * nrhs) return;
+    const uint32_t sys = id / nrhs, k = id % nrhs;
+    const double s = rnorm[id];
+    for (uint32_t i = sysRow[sys] + threadIdx.x; i < sysRow[sys + 1]; i += blockDim.x)
+        x[(size_t)k * N + i] = fma(s, (double)e32[(size_t)k * N + i], x[(size_t)k * N + i]);
+}
+
+__global__ void batch_dinv(uint32_t N, const double* diag, double* d64, float* d32)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double v = 1.0 / diag[i];
+        d64[i] = v;
+        d32[i] = (float)v;
+    }
+}
+
+} // namespace fb
+
+using namespace fb;
+
+struct fasp_gpu_batch_s {
+    Ctx       c;
+    Mat       M;
+    uint32_t  count = 0, nrhs = 0;
+    uint32_t* sysRow = nullptr;
+    uint32_t* order = nullptr;
+    double*   dinv = nullptr;
+    float*    dinv32 = nullptr;
+    double *  r64 = nullptr, *z64 = nullptr, *p0 = nullptr, *p1 = nullptr, *q64 = nullptr;
+    float *   b32 = nullptr, *x32 = nullptr, *r32 = nullptr, *z32 = nullptr, *p032 = nullptr,
+          *p132 = nullptr, *q32 = nullptr;
+    double*   rnorm = nullptr;
+    double*   resRel = nullptr;
+    uint32_t* iters = nullptr;
+    unsigned* queue = nullptr;
+    int       block = 256;  // autotuned
+    int       blocksPerSM = 4;
+    double    lastMs = 0.0;
+};
+
+namespace {
+
+template <typename T>
+int launch_batch(fasp_gpu_batch_s& B, BatchArgs<T> a)
+{
+    const int grid = B.c.nsm * B.blocksPerSM;
+    cudaMemsetAsync(B.queue, 0, sizeof(unsigned), B.c.stream);
+    switch (B.nrhs) {
+        case 1: batch_pcg<T, 1><<<grid, B.block, 0, B.c.stream>>>(a); break;
+        case 2: batch_pcg<T, 2><<<grid, B.block, 0, B.c.stream>>>(a); break;
+        case 3: batch_pcg<T, 3><<<grid, B.block, 0, B.c.stream>>>(a); break;
+        default: batch_pcg<T, 4><<<grid, B.block, 0, B.c.stream>>>(a); break;
+    }
+    B.c.launches += 1;
+    return cudaGetLastError() == cudaSuccess ? kOk : kErrCuda;
+}
+
+} // namespace
+
+extern "C" {
+
+int fasp_gpu_batch_create(uint32_t count, const uint32_t* sysRow, uint32_t nnz,
+                          const uint32_t* rowPtr, const uint32_t* colInd, const double* values,
+                          uint32_t nrhs, fasp_gpu_batch* out)
+{
+    if (!out || !sysRow || !rowPtr || !colInd || !values || count == 0 || nrhs == 0 ||
+        nrhs > (uint32_t)kMaxRhs)
+        return kErrInputPar;
+    *out = nullptr;
+    std::vector<uint32_t> hs(count + 1);
+    if (cudaMemcpy(hs.data(), sysRow, (count + 1) * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return kErrCuda;
+    for (uint32_t k = 0; k < count; ++k)
+        if (hs[k + 1] <= hs[k]) return kErrMatData; // empty or unordered system
+    if (hs[0] != 0) return kErrMatData;
+    const uint32_t N = hs[count];
+    fasp_gpu_batch h = new (std::nothrow) fasp_gpu_batch_s();
+    if (!h) return kErrAlloc;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int e = h->c.init(dev);
+    // the matrix upload validates the structure (CheckCSR) before any kernel reads it
+    if (!e) e = m_upload(h->M, N, N, nnz, rowPtr, colInd, values, false, h->c.stream);
+    if (!e) {
+        // each row's columns must stay inside its own system (block diagonal)
+        std::vector<uint32_t> rp(N + 1), ci(nnz);
+        cudaMemcpy(rp.data(), h->M.rowPtr, (N + 1) * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ci.data(), h->M.colInd, (size_t)nnz * 4, cudaMemcpyDeviceToHost);
+        for (uint32_t k = 0; k < count && !e; ++k)
+            for (uint32_t i = hs[k]; i < hs[k + 1] && !e; ++i)
+                for (uint32_t q = rp[i]; q < rp[i + 1]; ++q)
+                    if (ci[q] < hs[k] || ci[q] >= hs[k + 1]) {
+                        e = kErrMatData;
+                        break;
+                    }
+    }
+    h->count = count;
+    h->nrhs = nrhs;
+    const size_t vN = (size_t)nrhs * N;
+    auto dm = [&](void** p, size_t bytes) {
+        if (!e && cudaMalloc(p, bytes + 16) != cudaSuccess) {
+            cudaGetLastError();
+            e = kErrAlloc;
+        }
+    };
+    dm((void**)&h->sysRow, (count + 1) * 4);
+    dm((void**)&h->order, count * 4);
+    dm((void**)&h->dinv, N * 8);
+    dm((void**)&h->dinv32, N * 4);
+    dm((void**)&h->r64, vN * 8);
+    dm((void**)&h->z64, vN * 8);
+    dm((void**)&h->p0, vN * 8);
+    dm((void**)&h->p1, vN * 8);
+    dm((void**)&h->q64, vN * 8);
+    dm((void**)&h->b32, vN * 4);
+    dm((void**)&h->x32, vN * 4);
+    dm((void**)&h->r32, vN * 4);
+    dm((void**)&h->z32, vN * 4);
+    dm((void**)&h->p032, vN * 4);
+    dm((void**)&h->p132, vN * 4);
+    dm((void**)&h->q32, vN * 4);
+    dm((void**)&h->rnorm, (size_t)count * nrhs * 8);
+    dm((void**)&h->resRel, (size_t)count * nrhs * 8);
+    dm((void**)&h->iters, (size_t)count * nrhs * 4);
+    dm((void**)&h->queue, 16);
+    if (!e) e = h->M.ensure32(h->c.stream);
+    if (!e) {
+        // longest systems first
+        std::vector<uint32_t> ord(count);
+        std::iota(ord.begin(), ord.end(), 0u);
+        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+            return hs[a + 1] - hs[a] > hs[b + 1] - hs[b];
+        });
+        cudaMemcpy(h->sysRow, hs.data(), (count + 1) * 4, cudaMemcpyHostToDevice);
+        cudaMemcpy(h->order, ord.data(), count * 4, cudaMemcpyHostToDevice);
+        batch_dinv<<<std::max(1, std::min(ceil_div(N, 256), 148 * 8)), 256, 0, h->c.stream>>>(
+            N, h->M.diag, h->dinv, h->dinv32);
+        if (cudaStreamSynchronize(h->c.stream) != cudaSuccess) e = kErrCuda;
+    }
+    if (e) {
+        fasp_gpu_batch_destroy(h);
+        return e;
+    }
+    *out = h;
+    return kOk;
+}
+
+int fasp_gpu_batch_destroy(fasp_gpu_batch h)
+{
+    if (!h) return kOk;
+    cudaStreamSynchronize(h->c.stream);
+    m_free(h->M);
+    for (void* p : {(void*)h->sysRow, (void*)h->order, (void*)h->dinv, (void*)h->dinv32,
+                    (void*)h->r64, (void*)h->z64, (void*)h->p0, (void*)h->p1, (void*)h->q64,
+                    (void*)h->b32, (void*)h->x32, (void*)h->r32, (void*)h->z32,
+                    (void*)h->p032, (void*)h->p132, (void*)h->q32, (void*)h->rnorm,
+                    (void*)h->resRel, (void*)h->iters, (void*)h->queue})
+        cudaFree(p);
+    h->c.destroy();
+    delete h;
+    return kOk;
+}
+
+int fasp_gpu_batch_set_shape(fasp_gpu_batch h, int block, int blocksPerSM)
+{
+    if (!h || (block != 128 && block != 256 && block != 512) || blocksPerSM < 1 ||
+        blocksPerSM > 16 || block * blocksPerSM > 2048)
+        return kErrInputPar;
+    h->block = block;
+    h->blocksPerSM = blocksPerSM;
+    return kOk;
+}
+
+int fasp_gpu_batch_solve(fasp_gpu_batch h, const double* b, double* x, double relTol,
+                         uint32_t maxIter, int precision, double innerRelTol,
+                         uint32_t* iters, double* resRel)
+{
+    if (!h || !b || !x || relTol <= 0) return kErrInputPar;
+    fasp_gpu_batch_s& B = *h;
+    const uint32_t N = B.M.nrow, cnt = B.count, nr = B.nrhs;
+    const size_t vN = (size_t)nr * N;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, B.c.stream);
+    cudaMemsetAsync(B.iters, 0, (size_t)cnt * nr * 4, B.c.stream);
+    int e = kOk;
+    if (precision == FASP_GPU_FP64) {
+        BatchArgs<double> a{cnt, nr, N, B.sysRow, B.order, B.M.rowPtr, B.M.colInd, B.M.val,
+                            B.dinv, b, x, B.r64, B.z64, B.p0, B.p1, B.q64, B.iters, B.resRel,
+                            relTol, maxIter, B.queue};
+        e = launch_batch<double>(B, a);
+    } else {
+        // FP64 refinement around FP32 inner solves, x0 = 0
+        cudaMemsetAsync(x, 0, vN * 8, B.c.stream);
+        const double inner = innerRelTol > 0 ? innerRelTol : 1e-4;
+        int steps = 0;
+        const int maxSteps = 2 + (int)(std::log(relTol) / std::log(inner)) + 4;
+        std::vector<double> hn((size_t)cnt * nr), h0;
+        for (; steps < maxSteps; ++steps) {
+            batch_residual<<<cnt * nr, 256, 0, B.c.stream>>>(cnt, nr, N, B.sysRow, B.M.rowPtr,
+                                                           B.M.colInd, B.M.val, b, x, B.r64,
+                                                           B.rnorm);
+            cudaMemcpyAsync(hn.data(), B.rnorm, hn.size() * 8, cudaMemcpyDeviceToHost,
+                            B.c.stream);
+            cudaStreamSynchronize(B.c.stream);
+            if (steps == 0) h0 = hn;
+            bool done = true;
+            for (size_t k = 0; k < hn.size(); ++k)
+                if (hn[k] > relTol * h0[k]) done = false;
+            if (done) break;
+            batch_scale_to32<<<cnt * nr, 256, 0, B.c.stream>>>(cnt, nr, N, B.sysRow, B.r64,
+                                                             B.rnorm, B.b32);
+            BatchArgs<float> a{cnt, nr, N, B.sysRow, B.order, B.M.rowPtr, B.M.colInd,
+                               B.M.val32, B.dinv32, B.b32, B.x32, B.r32, B.z32, B.p032,
+                               B.p132, B.q32, B.iters, B.resRel, inner, maxIter, B.queue};
+            if ((e = launch_batch<float>(B, a))) break;
+            batch_update64<<<cnt * nr, 256, 0, B.c.stream>>>(cnt, nr, N, B.sysRow, B.rnorm,
+                                                           B.x32, x);
+            B.c.launches += 3;
+        }
+        if (!e) {
+            // final FP64 relative residual per (system, rhs)
+            for (size_t k = 0; k < hn.size(); ++k) hn[k] = h0[k] > 0 ? hn[k] / h0[k] : 0.0;
+            cudaMemcpyAsync(B.resRel, hn.data(), hn.size() * 8, cudaMemcpyHostToDevice,
+                            B.c.stream);
+        }
+    }
+    cudaEventRecord(t1, B.c.stream);
+    cudaEventSynchronize(t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    B.lastMs = ms;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (!e && cudaGetLastError() != cudaSuccess) e = kErrCuda;
+    if (!e && iters)
+        e = cudaMemcpy(iters, B.iters, (size_t)cnt * nr * 4, cudaMemcpyDeviceToHost) ? kErrCuda : kOk;
+    if (!e && resRel)
+        e = cudaMemcpy(resRel, B.resRel, (size_t)cnt * nr * 8, cudaMemcpyDeviceToHost) ? kErrCuda : kOk;
+    return e;
+}
+
+int fasp_gpu_batch_last_time(fasp_gpu_batch h, double* ms)
+{
+    if (!h || !ms) return kErrInputPar;
+    *ms = h->lastMs;
+    return kOk;
+}
+
+} // extern "C"

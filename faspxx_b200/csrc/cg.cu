@@ -329,6 +329,176 @@ __global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restr
     });
 }
 
+// ---- persistent kernel: every iteration in one cooperative launch -----------------------
+// The two phases of an iteration (the cg_spmv and cg_update work above) are separated by
+// a grid barrier. Instead of one last block finishing each reduction, every block reads
+// all block partials after the barrier and sums them in the same fixed order, so all
+// blocks hold bit-identical scalars and run the same control flow on a shared-memory copy
+// of the control block; block 0 writes it back when the launch ends. Vectors that other
+// blocks wrote inside this launch are read with ld.global.cg (L2), since L1 is not coherent.
+
+constexpr int kPBlock = 512;
+constexpr int kSlotPhase1 = kMaxRedValues - 1; // partial slot of the SpMV phase
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Software grid barrier for a co-resident (cooperatively launched) grid. The spin is
+// bounded: after ~2^24 polls it raises bar->error and every block leaves the kernel.
+__device__ bool grid_sync(GridBar* bar, unsigned* gen)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned g = *gen;
+        int good = 1;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&bar->count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&bar->count, 0u);
+            __threadfence();
+            atomicExch(&bar->gen, g + 1);
+        } else {
+            unsigned spins = 0;
+            while (ld_acquire_u32(&bar->gen) == g) {
+                if (ld_acquire_u32(&bar->error)) {
+                    good = 0;
+                    break;
+                }
+                if (++spins > (1u << 24)) {
+                    atomicExch(&bar->error, 1u);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        *gen = g + 1;
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Sum of the partials of slot k over all blocks, fixed order; every block gets the same.
+template <int NV>
+__device__ __forceinline__ void all_reduce_partials(const Scratch s, const int (&slot)[NV],
+                                                    const int (&ops)[NV], double (&tot)[NV])
+{
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = red_ident(ops[k]);
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            t = red_apply(t, __ldcg(&s.partials[slot[k] * kMaxGrid + b]), ops[k]);
+        tot[k] = t;
+    }
+    block_reduce<NV>(tot, ops);
+}
+
+template <int NV>
+__device__ __forceinline__ void write_partials(Scratch s, const int (&slot)[NV],
+                                               const int (&ops)[NV], double (&acc)[NV])
+{
+    block_reduce<NV>(acc, ops);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) s.partials[slot[k] * kMaxGrid + blockIdx.x] = acc[k];
+}
+
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kPBlock, 2)
+cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __restrict__ dinv,
+              CGCtl* gctl, Scratch s, GridBar* bar, unsigned iterCap)
+{
+    __shared__ CGCtl c;
+    __shared__ unsigned gen;
+    __shared__ double bc[5];
+    if (threadIdx.x == 0) {
+        c = *gctl;
+        gen = ld_acquire_u32(&bar->gen);
+    }
+    __syncthreads();
+    const uint32_t n = A.nrow;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const T* zz = JAC ? z : r;
+    unsigned done = 0;
+    while (c.status == kRun && done < iterCap) {
+        // phase 1: ax = A p with p = z + beta p_old formed on the fly, and (ax, p)
+        {
+            const int mode = c.pmode, par = c.par;
+            const T beta = (T)c.beta;
+            const T* pOld = par ? P1 : P0;
+            T* pNew = par ? P0 : P1;
+            T acc = T(0);
+            for (size_t row = tid; row < n; row += stride) {
+                const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
+                const T sum = row_dot<T, false>(A, b, e, [&](uint32_t j) {
+                    return mode ? fma(beta, __ldcg(pOld + j), __ldcg(zz + j)) : __ldcg(zz + j);
+                });
+                const T pi = mode ? fma(beta, __ldcg(pOld + row), __ldcg(zz + row))
+                                  : __ldcg(zz + row);
+                pNew[row] = pi;
+                q[row] = sum;
+                acc = fma(sum, pi, acc);
+            }
+            double a[1] = {(double)acc};
+            const int sl[1] = {kSlotPhase1}, ops[1] = {kSum};
+            write_partials<1>(s, sl, ops, a);
+            if (!grid_sync(bar, &gen)) return;
+            double t[1];
+            all_reduce_partials<1>(s, sl, ops, t);
+            if (threadIdx.x == 0) {
+                c.par = par ^ 1;
+                if (!c.bench) cg_after_spmv(&c, t[0]);
+            }
+            __syncthreads();
+            if (c.status != kRun) break;
+        }
+        // phase 2: x += alpha p, r -= alpha ax, z = diagInv .* r, and the five reductions
+        {
+            const T alpha = (T)c.alpha;
+            const T* p = c.par ? P1 : P0;
+            T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
+            for (size_t i = tid; i < n; i += stride) {
+                const T pi = __ldcg(p + i);
+                const T xi = fma(alpha, pi, __ldcg(x + i));
+                const T ri = fma(-alpha, __ldcg(q + i), __ldcg(r + i));
+                x[i] = xi;
+                r[i] = ri;
+                T zi = ri;
+                if (JAC) {
+                    zi = __ldg(dinv + i) * ri;
+                    z[i] = zi;
+                }
+                rr = fma(ri, ri, rr);
+                zr = fma(zi, ri, zr);
+                xx = fma(xi, xi, xx);
+                xm = fmax(xm, fabs(xi));
+                pp = fma(pi, pi, pp);
+            }
+            double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
+            const int sl[5] = {0, 1, 2, 3, 4}, ops[5] = {kSum, kSum, kSum, kMax, kSum};
+            write_partials<5>(s, sl, ops, a);
+            if (!grid_sync(bar, &gen)) return;
+            double t[5];
+            all_reduce_partials<5>(s, sl, ops, t);
+            if (threadIdx.x == 0) {
+                for (int k = 0; k < 5; ++k) bc[k] = t[k];
+                if (!c.bench) cg_checks(&c, bc, 0);
+            }
+            __syncthreads();
+        }
+        ++done;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *gctl = c;
+}
+
 // ---- engine ------------------------------------------------------------------------------
 
 static int spmv_grid_cg(const Ctx& c, uint32_t nrow, int L)
@@ -447,6 +617,49 @@ int CGEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool grap
         FB_CUDA(cudaGraphInstantiate(&gexec, g, 0));
         cudaGraphDestroy(g);
     }
+    if (wantPersistent) {
+        // one cooperative launch needs every block resident: size the grid from occupancy
+        int coop = 0, nb = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->dev);
+        if (jacobi)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cg_persistent<T, 1>, kPBlock, 0);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cg_persistent<T, 0>, kPBlock, 0);
+        cudaGetLastError();
+        if (nb > 2) nb = 2;
+        pgrid = nb * c->nsm;
+        if (pgrid > kMaxGrid) pgrid = kMaxGrid;
+        if (coop && nb > 0) {
+            if (cudaMalloc(&bar, sizeof(GridBar)) != cudaSuccess) {
+                cudaGetLastError();
+                return kErrAlloc;
+            }
+            FB_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBar), c->stream));
+            persistent = true;
+        }
+    }
+    return kOk;
+}
+
+// One cooperative launch that iterates until the control block leaves kRun or iterCap
+// iterations have run. A barrier time-out (bar->error) is reported as a CUDA error.
+template <typename T>
+int CGEngine<T>::run_persistent(unsigned iterCap)
+{
+    CSRView<T> V = view_of<T>(*A);
+    T* zz = jacobi ? z : r;
+    Scratch s = c->red;
+    void* args[] = {&V, &x, &r, &zz, &P0, &P1, &q, (void*)&dinv, &ctl, &s, &bar, &iterCap};
+    const void* fn = jacobi ? (const void*)cg_persistent<T, 1> : (const void*)cg_persistent<T, 0>;
+    FB_CUDA(cudaLaunchCooperativeKernel(fn, pgrid, kPBlock, args, 0, c->stream));
+    GridBar hb;
+    FB_CUDA(cudaMemcpyAsync(&hb, bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
+    FB_CUDA(cudaStreamSynchronize(c->stream));
+    if (hb.error) {
+        cudaMemsetAsync(bar, 0, sizeof(GridBar), c->stream);
+        cudaStreamSynchronize(c->stream);
+        return kErrCuda;
+    }
     return kOk;
 }
 
@@ -462,6 +675,9 @@ void CGEngine<T>::destroy()
     cudaFree(P1);
     if (jacobi) cudaFree(z);
     cudaFree(ctl);
+    cudaFree(bar);
+    bar = nullptr;
+    persistent = false;
     if (hctl) cudaFreeHost(hctl);
     if (hstatus) cudaFreeHost(hstatus);
     x = r = z = q = P0 = P1 = nullptr;
@@ -475,6 +691,11 @@ void CGEngine<T>::destroy()
 template <typename T>
 int CGEngine<T>::run(unsigned* launches)
 {
+    if (persistent) {
+        const int e = run_persistent(0xffffffffu);
+        if (launches) *launches += 1;
+        return e;
+    }
     if (!useGraph) {
         // plain launches, status polled every itersPerGraph iterations
         for (;;) {
@@ -570,6 +791,22 @@ int CGEngine<T>::time_kernels(unsigned reps, double* ms)
     cudaEventElapsedTime(&b, ev[1], ev[2]);
     ms[0] = a / reps;
     ms[1] = b / reps;
+    ms[2] = 0.0;
+    if (persistent) {
+        // the persistent kernel, reps iterations in one launch (bench mode: no control flow)
+        e = push_ctl();
+        if (e) return e;
+        run_persistent(2);
+        push_ctl();
+        cudaEventRecord(ev[0], c->stream);
+        e = run_persistent(reps);
+        cudaEventRecord(ev[1], c->stream);
+        cudaEventSynchronize(ev[1]);
+        float p = 0.f;
+        cudaEventElapsedTime(&p, ev[0], ev[1]);
+        ms[2] = p / reps;
+        if (e) return e;
+    }
     for (auto& x0 : ev) cudaEventDestroy(x0);
     hctl->bench = 0;
     hctl->status = kDone;

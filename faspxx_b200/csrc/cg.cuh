@@ -12,6 +12,11 @@ enum CGReason { kNoReason = 0, kBreakdown = 1, kSave = 2, kStag = 3, kCheck3 = 4
 // The locals of CG::Solve (CG.cxx:55-64) plus the parameters it reads, kept in device
 // memory so that the finalize thread of each fused kernel can run the reference's control
 // flow between iterations without a host round trip.
+// Grid barrier state of the persistent kernel (device memory, zero at creation).
+struct GridBar {
+    unsigned count, gen, error, pad;
+};
+
 struct CGCtl {
     int      status, reason, code, phase;
     int      pmode;     // 0: p = z (first iteration or restart), 1: p = z + beta p
@@ -48,6 +53,12 @@ struct CGEngine {
     bool       useGraph = true;
     bool       capturing = false;
     uint32_t   n = 0;
+    // persistent engine: one cooperative launch runs the iterations
+    bool       wantPersistent = true; // set before init
+    bool       persistent = false;
+    int        pgrid = 0;
+    GridBar*   bar = nullptr;
+    int        run_persistent(unsigned iterCap);
 
     int  init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph);
     void destroy();

@@ -184,12 +184,14 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             const bool fusable = cfg.pcd == 0 || (pcd.pure() && pcd.prm.maxIter == 1);
             if (fusable && cfg.precision == FASP_GPU_FP64) {
                 cg64 = new CGEngine<double>();
+                cg64->wantPersistent = cfg.persistent != 0;
                 if ((e = cg64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
             }
             if (cfg.precision == FASP_GPU_MIXED) {
                 if (!fusable) return kErrPcdType; // mixed mode fuses its preconditioner
                 if ((e = Ah->M.ensure32(c.stream))) return e;
                 cg32 = new CGEngine<float>();
+                cg32->wantPersistent = cfg.persistent != 0;
                 if ((e = cg32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
             }
             break;

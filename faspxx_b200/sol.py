@@ -217,6 +217,9 @@ class SOL:
     def SetOrth(self, orth):
         self.cfg.orth = orth
 
+    def SetPersistent(self, flag: bool):
+        self.cfg.persistent = 1 if flag else 0
+
     def SetUseGraph(self, flag: bool):
         self.cfg.useGraph = 1 if flag else 0
 

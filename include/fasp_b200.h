@@ -78,6 +78,8 @@ typedef struct {
     uint32_t        innerMaxIter;/* MIXED: iteration cap of each inner solve */
     uint32_t        maxOuter;    /* MIXED: refinement steps cap */
     int             useGraph;    /* 1: device-driven iterations captured in CUDA graphs */
+    int             persistent;  /* 1: device-driven CG runs all iterations in one
+                                    cooperative launch (when the device allows it) */
 } fasp_gpu_config;
 
 /* Outcome of one Solve. */
@@ -187,8 +189,9 @@ int fasp_gpu_solver_destroy(fasp_gpu_solver s);
 int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms);
 /* Device-driven CG only: average duration (ms) of each of its two fused kernels over reps
  * launches, timed alone with CUDA events on the solver's stream (control logic bypassed;
- * the solver's internal vectors are overwritten). ms[0]: SpMV kernel, ms[1]: update kernel.
- * Times the FP32 engine when the solver is MIXED. */
+ * the solver's internal vectors are overwritten). ms must hold 3 values: ms[0] SpMV
+ * kernel, ms[1] update kernel, ms[2] one iteration of the persistent kernel (0 when the
+ * solver does not use it). Times the FP32 engine when the solver is MIXED. */
 int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, double* ms);
 
 /* ---- adjoint (no reference counterpart) --------------------------------------------- */
@@ -196,6 +199,29 @@ int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, double* ms);
  * matrix (built once, cached). */
 int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* lam,
                                   fasp_gpu_info* info);
+
+/* ---- batched CG (no reference counterpart) ------------------------------------------ */
+/* count independent SPD systems solved by Jacobi-PCG in one persistent launch. The systems
+ * are the diagonal blocks of one CSRx matrix on the DEVICE (global row/column indices;
+ * system k owns rows sysRow[k]..sysRow[k+1]-1 and its columns must stay inside that range;
+ * sysRow also on the device). nrhs (1..4) right-hand sides per system, stored
+ * right-hand-side-major: b[r * N + row], N = sysRow[count]. */
+typedef struct fasp_gpu_batch_s* fasp_gpu_batch;
+int fasp_gpu_batch_create(uint32_t count, const uint32_t* sysRow, uint32_t nnz,
+                          const uint32_t* rowPtr, const uint32_t* colInd,
+                          const double* values, uint32_t nrhs, fasp_gpu_batch* out);
+/* Thread-block shape of the persistent launch: block (128, 256 or 512 threads) and blocks
+ * per SM; the autotuner in the Python/C++ layers times the choices. */
+int fasp_gpu_batch_set_shape(fasp_gpu_batch bt, int block, int blocksPerSM);
+/* Solves all systems from x0 = 0 to ||r|| < relTol ||b|| per right-hand side (device b, x).
+ * precision FASP_GPU_MIXED runs FP32 inner CG to innerRelTol inside FP64 refinement.
+ * iters (host, count*nrhs, may be NULL): iterations per right-hand side; resRel (host,
+ * may be NULL): final relative residual per right-hand side. */
+int fasp_gpu_batch_solve(fasp_gpu_batch bt, const double* b, double* x, double relTol,
+                         uint32_t maxIter, int precision, double innerRelTol,
+                         uint32_t* iters, double* resRel);
+int fasp_gpu_batch_last_time(fasp_gpu_batch bt, double* ms);
+int fasp_gpu_batch_destroy(fasp_gpu_batch bt);
 
 #ifdef __cplusplus
 }

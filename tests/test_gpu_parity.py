@@ -155,12 +155,13 @@ def test_invalid_csr_is_rejected_before_upload(gpu):
     assert e.value.code == -17
 
 
-def _check_case(gpu, oracle, name, graph=True):
+def _check_case(gpu, oracle, name, engine="persistent"):
     case = CASES[name]
     A, b, x0 = G.case_inputs(case)
     M = gpu.MAT(A)
     s = gpu.configure(case["alg"], **case["kw"])
-    s.SetUseGraph(graph)
+    s.SetPersistent(engine == "persistent")
+    s.SetUseGraph(engine == "graph")
     s.Setup(M)
     po = oracle.Solver("port", A, case["alg"], **case["kw"])
     for rep in range(case.get("repeat", 1)):
@@ -176,10 +177,14 @@ def _check_case(gpu, oracle, name, graph=True):
         else:
             assert code == meta["code"], (key, code, meta["code"])
         it = s.GetIterations()
-        window = FLOOR.get(name, ERRATIC.get(name, 1))
-        assert abs(it - meta["iters"]) <= window, (key, it, meta["iters"])
         if name in FLOOR:
+            # the count of false-convergence restarts at the floor is chaotic: require the
+            # true residual to have reached the rounding floor instead
+            r = b - A.matvec(x)
+            assert np.linalg.norm(r) <= 1e-13 * np.linalg.norm(b), key
             continue
+        window = ERRATIC.get(name, 1)
+        assert abs(it - meta["iters"]) <= window, (key, it, meta["iters"])
         scale = max(np.max(np.abs(ref.x)), np.max(np.abs(x0)), 1e-300)
         xtol = 1e-3 if name in ERRATIC else 1e-6
         assert np.max(np.abs(x - ref.x)) <= xtol * scale, key
@@ -201,11 +206,14 @@ def test_solver_parity(gpu, oracle, name):
     _check_case(gpu, oracle, name)
 
 
+@pytest.mark.parametrize("engine", ["graph", "plain"])
 @pytest.mark.parametrize("name", ["fdm_pcg", "fem_pcg", "p2d_pcg", "p3d_cg", "vd_cg",
-                                  "fdm_cg_min5"])
-def test_cg_without_graphs_matches(gpu, oracle, name):
-    """The device-driven CG gives the same answers launched plainly as from CUDA graphs."""
-    _check_case(gpu, oracle, name, graph=False)
+                                  "fdm_cg_min5", "fdm_cg_tolsmall"])
+def test_cg_engines_match(gpu, oracle, name, engine):
+    """The device-driven CG meets the same bars run as one persistent cooperative kernel
+    (the default, exercised by test_solver_parity), as CUDA graphs of its two kernels, and
+    as plain launches."""
+    _check_case(gpu, oracle, name, engine=engine)
 
 
 def test_known_answer_jacobi(gpu):
