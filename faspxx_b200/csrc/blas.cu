@@ -5,6 +5,9 @@
 // scalar, so a following kernel can consume it without a host round trip. Sums use FMA and
 // a different association than the reference's 4 interleaved partial sums (VEC.cxx:424-485);
 // results agree to rounding, not bit for bit.
+#include <map>
+#include <mutex>
+
 #include "internal.h"
 
 namespace fb {
@@ -12,6 +15,25 @@ namespace fb {
 #define GRID_STRIDE(i, n) \
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)(n); \
          i += (size_t)gridDim.x * blockDim.x)
+
+int resident_grid(const Ctx& c, const void* fn, int block)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(fn, block);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    long long g = (long long)nb * c.nsm;
+    if (g > kMaxGrid) g = kMaxGrid;
+    cache[key] = (int)g;
+    return (int)g;
+}
 
 int Ctx::grid(long long work, int perBlock, int perSM) const
 {

@@ -146,7 +146,7 @@ void fasp_gpu_default_config(fasp_gpu_config* cfg, int alg)
     cfg->innerMaxIter = 0;
     cfg->maxOuter = 50;
     cfg->useGraph = 1;
-    cfg->persistent = 1;
+    cfg->persistent = 0;
 }
 
 // ---- memory ---------------------------------------------------------------------------

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
 }
 
 template <typename T, int JAC>
-__global__ void __launch_bounds__(kBlock) cg_update(uint32_t n, T* __restrict__ x,
+__global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict__ x,
                                                     T* __restrict__ r, T* __restrict__ z,
                                                     const T* P0, const T* P1,
                                                     const T* __restrict__ q,
@@ -236,17 +236,18 @@ __global__ void __launch_bounds__(kBlock) cg_update(uint32_t n, T* __restrict__ 
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = tid; i < nv; i += stride) {
-        T pa[W], xa[W], ra[W], qa[W], da[W], za[W];
+        T pa[W], xa[W], ra[W], qa[W], da[W];
         *(V*)pa = ((const V*)p)[i];
         *(V*)xa = ((const V*)x)[i];
         *(V*)ra = ((const V*)r)[i];
         *(V*)qa = ((const V*)q)[i];
         if (JAC) *(V*)da = ((const V*)dinv)[i];
+        // z overwrites q's registers: q is dead once r is updated
 #pragma unroll
-        for (int u = 0; u < W; ++u) one(pa[u], xa[u], ra[u], qa[u], JAC ? da[u] : T(0), za[u]);
+        for (int u = 0; u < W; ++u) one(pa[u], xa[u], ra[u], qa[u], JAC ? da[u] : T(0), qa[u]);
         ((V*)x)[i] = *(V*)xa;
         ((V*)r)[i] = *(V*)ra;
-        if (JAC) ((V*)z)[i] = *(V*)za;
+        if (JAC) ((V*)z)[i] = *(V*)qa;
     }
     for (size_t i = nv * W + tid; i < n; i += stride) {
         T xi = x[i], ri = r[i], zi;
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restr
 // of the control block; block 0 writes it back when the launch ends. Vectors that other
 // blocks wrote inside this launch are read with ld.global.cg (L2), since L1 is not coherent.
 
-constexpr int kPBlock = 512;
+constexpr int kPBlock = 256;
 constexpr int kSlotPhase1 = kMaxRedValues - 1; // partial slot of the SpMV phase
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
@@ -411,7 +412,7 @@ __device__ __forceinline__ void write_partials(Scratch s, const int (&slot)[NV],
 }
 
 template <typename T, int JAC>
-__global__ void __launch_bounds__(kPBlock, 2)
+__global__ void __launch_bounds__(kPBlock, 4)
 cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __restrict__ dinv,
               CGCtl* gctl, Scratch s, GridBar* bar, unsigned iterCap)
 {
@@ -516,26 +517,47 @@ CSRView<double> view_of<double>(const Mat& A) { return A.v64(); }
 template <>
 CSRView<float> view_of<float>(const Mat& A) { return A.v32(); }
 
+// The two fused kernels, each on one resident wave (grid from the occupancy limit).
+template <typename T>
+void CGEngine<T>::launch_spmv_kernel()
+{
+    const CSRView<T> V = view_of<T>(*A);
+    const int need = spmv_grid_cg(*c, A->nrow, A->lanes);
+    const T* zz = jacobi ? z : r;
+    auto go = [&](auto kern) {
+        const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
+        kern<<<g, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red);
+    };
+    switch (A->lanes) {
+        case 1: go(cg_spmv<T, 1>); break;
+        case 2: go(cg_spmv<T, 2>); break;
+        case 4: go(cg_spmv<T, 4>); break;
+        case 8: go(cg_spmv<T, 8>); break;
+        case 16: go(cg_spmv<T, 16>); break;
+        default: go(cg_spmv<T, 32>); break;
+    }
+}
+
+template <typename T>
+void CGEngine<T>::launch_update_kernel()
+{
+    const int need = c->grid(n / V16<T>::W + 1, kBlock, 16);
+    auto go = [&](auto kern, T* zz) {
+        const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
+        kern<<<g, kBlock, 0, c->stream>>>(n, x, r, zz, P0, P1, q, dinv, ctl, c->red);
+    };
+    if (jacobi)
+        go(cg_update<T, 1>, z);
+    else
+        go(cg_update<T, 0>, r);
+}
+
 template <typename T>
 int CGEngine<T>::launch_iter()
 {
-    const CSRView<T> V = view_of<T>(*A);
-    const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
-    const int g2 = c->grid(n / V16<T>::W + 1, kBlock, 4);
-    const T* zz = jacobi ? z : r;
     if (!capturing) c->launches += 2;
-    switch (A->lanes) {
-        case 1: cg_spmv<T, 1><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        case 2: cg_spmv<T, 2><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        case 4: cg_spmv<T, 4><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        case 8: cg_spmv<T, 8><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        case 16: cg_spmv<T, 16><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        default: cg_spmv<T, 32><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-    }
-    if (jacobi)
-        cg_update<T, 1><<<g2, kBlock, 0, c->stream>>>(n, x, r, z, P0, P1, q, dinv, ctl, c->red);
-    else
-        cg_update<T, 0><<<g2, kBlock, 0, c->stream>>>(n, x, r, r, P0, P1, q, dinv, ctl, c->red);
+    launch_spmv_kernel();
+    launch_update_kernel();
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -626,7 +648,7 @@ int CGEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool grap
         else
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, cg_persistent<T, 0>, kPBlock, 0);
         cudaGetLastError();
-        if (nb > 2) nb = 2;
+        if (nb > 4) nb = 4;
         pgrid = nb * c->nsm;
         if (pgrid > kMaxGrid) pgrid = kMaxGrid;
         if (coop && nb > 0) {
@@ -754,28 +776,10 @@ int CGEngine<T>::time_kernels(unsigned reps, double* ms)
     hctl->histScale = 1.0;
     int e = push_ctl();
     if (e) return e;
-    const CSRView<T> V = view_of<T>(*A);
-    const int g1 = spmv_grid_cg(*c, A->nrow, A->lanes);
-    const int g2 = c->grid(n / V16<T>::W + 1, kBlock, 4);
-    const T* zz = jacobi ? z : r;
     cudaEvent_t ev[3];
     for (auto& x0 : ev) FB_CUDA(cudaEventCreate(&x0));
-    auto spmv = [&]() {
-        switch (A->lanes) {
-            case 1: cg_spmv<T, 1><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-            case 2: cg_spmv<T, 2><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-            case 4: cg_spmv<T, 4><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-            case 8: cg_spmv<T, 8><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-            case 16: cg_spmv<T, 16><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-            default: cg_spmv<T, 32><<<g1, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red); break;
-        }
-    };
-    auto update = [&]() {
-        if (jacobi)
-            cg_update<T, 1><<<g2, kBlock, 0, c->stream>>>(n, x, r, z, P0, P1, q, dinv, ctl, c->red);
-        else
-            cg_update<T, 0><<<g2, kBlock, 0, c->stream>>>(n, x, r, r, P0, P1, q, dinv, ctl, c->red);
-    };
+    auto spmv = [&]() { launch_spmv_kernel(); };
+    auto update = [&]() { launch_update_kernel(); };
     for (int w = 0; w < 3; ++w) {
         spmv();
         update();

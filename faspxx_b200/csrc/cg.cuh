@@ -67,6 +67,8 @@ struct CGEngine {
     // Kernels: start from the residual in r and the guess in x.
     int  launch_init();
     int  launch_iter();
+    void launch_spmv_kernel();
+    void launch_update_kernel();
     int  launch_resume();
     int  time_kernels(unsigned reps, double* ms);
     int  push_ctl();   // hctl -> ctl

@@ -76,6 +76,11 @@ struct Ctx {
     int  fetch(int slot, double* out);               // read one device scalar (synchronous)
 };
 
+// Blocks of `fn` at `block` threads that are resident at once on the whole device (one
+// wave): SM count x the occupancy limit (registers, shared memory), capped at kMaxGrid.
+// Grid-stride kernels launched with min(work, this) never run a partial second wave.
+int resident_grid(const Ctx& c, const void* fn, int block);
+
 // CSRx matrix resident in device memory.
 struct Mat {
     uint32_t  nrow = 0, mcol = 0, nnz = 0;

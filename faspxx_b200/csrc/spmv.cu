@@ -108,14 +108,18 @@ template <typename T>
 static int launch_spmv(Ctx& c, CSRView<T> A, int L, const T* x, T* y)
 {
     if (A.nrow == 0) return kOk;
-    const int g = spmv_grid(c, A.nrow, L);
+    const int need = spmv_grid(c, A.nrow, L);
     const bool pat = A.val == nullptr;
+    auto go = [&](auto kern) {
+        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
+        kern<<<g, kBlock, 0, c.stream>>>(A, x, y);
+    };
 #define SPMV_CASE(LL)                                                                     \
     case LL:                                                                              \
         if (pat)                                                                          \
-            k_spmv<T, LL, true><<<g, kBlock, 0, c.stream>>>(A, x, y);                     \
+            go(k_spmv<T, LL, true>);                                                      \
         else                                                                              \
-            k_spmv<T, LL, false><<<g, kBlock, 0, c.stream>>>(A, x, y);                    \
+            go(k_spmv<T, LL, false>);                                                     \
         break;
     ++c.launches;
     switch (L) {
@@ -153,15 +157,19 @@ int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r
         if (e) return e;
         xinf = slot;
     }
-    const int g = spmv_grid(c, A.nrow, A.lanes);
+    const int need = spmv_grid(c, A.nrow, A.lanes);
+    auto go = [&](auto kern) {
+        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
+        kern<<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf);
+    };
     ++c.launches;
     switch (A.lanes) {
-        case 1: k_residual<1><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
-        case 2: k_residual<2><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
-        case 4: k_residual<4><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
-        case 8: k_residual<8><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
-        case 16: k_residual<16><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
-        default: k_residual<32><<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf); break;
+        case 1: go(k_residual<1>); break;
+        case 2: go(k_residual<2>); break;
+        case 4: go(k_residual<4>); break;
+        case 8: go(k_residual<8>); break;
+        case 16: go(k_residual<16>); break;
+        default: go(k_residual<32>); break;
     }
     FB_CUDA(cudaGetLastError());
     return kOk;
