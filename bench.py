@@ -1,8 +1,9 @@
 #!/usr/bin/env python
 """Benchmark: time to an FP64 relative residual of 1e-8 on the 3D 7-point Poisson problem
 (128^3 grid, n = 2,097,152, nnz = 14,581,760), Jacobi-preconditioned CG (weight 1, one
-sweep), mixed precision (FP32 inner CG inside FP64 refinement) against plain FP64 CG on
-the same B200, plus SpMV GB/s. One JSON line on rank 0.
+sweep), mixed precision (FP32 CG iterations with FP64 reliable updates of x and r) against
+plain FP64 CG on the same B200, plus SpMV GB/s. One JSON line on rank 0. The restarted
+variant (FP32 inner CG solves inside FP64 iterative refinement) is timed beside them.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -219,10 +220,13 @@ def run_ours(args):
         s.SetupPCD(p)
         if precision == capi.MIXED:
             s.SetPrecision(capi.MIXED, innerRelTol=args.inner_tol, maxOuter=50)
+        elif precision == capi.MIXED_RELIABLE:
+            s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=args.delta)
         s.Setup(M)
         return s
 
-    mixed, fp64 = make(capi.MIXED), make(capi.FP64)
+    mixed, fp64 = make(capi.MIXED_RELIABLE), make(capi.FP64)
+    restarted = make(capi.MIXED)
     if args.profile:
         # 3 warm-up + 1 launch of cg_spmv and cg_update per engine: FP32 first, then FP64
         km = (C.c_double * 3)()
@@ -244,6 +248,7 @@ def run_ours(args):
     for _ in range(args.warmup):
         solve(mixed)
         solve(fp64)
+        solve(restarted)
 
     # accuracy of each variant: FP64 residual and error against an FP64 CG solve to 1e-13
     tight = make(capi.FP64)
@@ -279,10 +284,17 @@ def run_ours(args):
             times64.append(t)
             its64.append(it)
         lib.fasp_gpu_synchronize()
+        timesR, itsR, outerR = [], [], 0
+        for _ in range(args.steps):
+            t, it, la, outerR = solve(restarted)
+            timesR.append(t)
+            itsR.append(it)
+        lib.fasp_gpu_synchronize()
     barrier(dist)
     clocks = clk.summary()
     mixed_ms = dist_max(dist, statistics.mean(times))
     fp64_ms = dist_max(dist, statistics.mean(times64))
+    restarted_ms = dist_max(dist, statistics.mean(timesR))
 
     # end to end: host b, x0 in pinned memory -> device -> solve -> x back to host
     hb = C.c_void_p()
@@ -352,6 +364,11 @@ def run_ours(args):
         "cg_update_f64": {"ms": round(k64[1], 5), "gbs": round(gbs(b_upd64, k64[1]), 1)},
         "spmv_f64_apply": {"ms": round(sp.value, 5), "gbs": round(gbs(b_apply, sp.value), 1),
                            "frac": round(gbs(b_apply, sp.value) / hbm, 3)},
+        # the whole mixed solve as FP32 iterations: algorithmic bytes of its iterations over
+        # the solve's device time (refreshes, reductions and launch gaps included)
+        "mixed_solve_effective": {
+            "ms_per_iter": round(mixed_ms / max(1, statistics.median(its)), 5),
+            "gbs": round(gbs((b_spmv32 + b_upd32) * statistics.median(its), mixed_ms), 1)},
     }
 
     cpu = None
@@ -374,16 +391,22 @@ def run_ours(args):
             "metric": METRIC, "value": round(mixed_ms, 3), "unit": "ms", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mixed_ms, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "dtype": "f32 Krylov iterations / f64 reliable updates", "data": "synthetic",
             "config": {"workload": f"3D Poisson 7-point {args.size}^3 (n={n}, nnz={nnz}), "
                                    f"Jacobi-PCG, FP64 rtol 1e-8, x0=0, b=A x*, x*~U[0,1)",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "inputs larger than L2 (FP32 matrix 125 MB + vectors)",
                        "spmv_lanes_per_row": lanes,
-                       "inner_rel_tol": args.inner_tol},
+                       "reliable_update_delta": args.delta,
+                       "precision_mode": "MIXED_RELIABLE"},
             "fp64_ms": round(fp64_ms, 3), "mixed_over_fp64": round(mixed_ms / fp64_ms, 3),
-            "iterations": {"mixed_inner_total": int(statistics.median(its)),
-                           "mixed_outer": outer, "fp64": int(statistics.median(its64))},
+            "restarted_refinement": {"ms": round(restarted_ms, 3),
+                                     "over_fp64": round(restarted_ms / fp64_ms, 3),
+                                     "inner_rel_tol": args.inner_tol,
+                                     "inner_total": int(statistics.median(itsR)),
+                                     "outer": outerR},
+            "iterations": {"mixed_fp32": int(statistics.median(its)),
+                           "mixed_fp64_refreshes": outer, "fp64": int(statistics.median(its64))},
             "accuracy": {"mixed_rel_residual": acc_mixed[0], "mixed_err_vs_fp64_1e-13": acc_mixed[1],
                          "fp64_rel_residual": acc_fp64[0], "fp64_err_vs_fp64_1e-13": acc_fp64[1],
                          "e2e_err_vs_fp64_1e-13": e2e_err},
@@ -450,7 +473,7 @@ def run_batch(args):
     line = {"metric": "Batched Jacobi-PCG, 4096 uneven systems x 4 RHS to rtol 1e-8",
             "value": round(res["mixed"][0], 3), "unit": "ms", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "dtype": "f32 Krylov iterations / f64 reliable updates", "data": "synthetic",
             "config": {"workload": f"{count} systems, 2D 5-point m~U{{16..128}} + sigma I, "
                                    f"sigma~U[0,1], 4 RHS b~N(0,1), rows {B.N}, nnz {B.A.nnz}",
                        "shape": list(shape64)},
@@ -472,7 +495,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=N_GRID)
-    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--inner-tol", type=float, default=1e-4,
+                    help="inner tolerance of the restarted-refinement variant")
+    ap.add_argument("--delta", type=float, default=1e-2,
+                    help="reliable-update factor of the headline mixed solve")
     ap.add_argument("--ref-sample", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lanes", type=int, default=0, help="force SpMV lanes per row")

@@ -46,101 +46,119 @@ int Ctx::grid(long long work, int perBlock, int perSM) const
 }
 
 // ---- reductions ------------------------------------------------------------------------
+// T = double (the reference's arithmetic) or float (mixed-precision inner solves: each
+// thread accumulates in T, the block and grid stages in FP64).
 
-__global__ void k_dot(uint32_t n, const double* __restrict__ a, const double* __restrict__ b,
-                      Scratch s, double* dres)
+template <typename T>
+__global__ void k_dot(uint32_t n, const T* __restrict__ a, const T* __restrict__ b, Scratch s,
+                      double* dres)
 {
-    double acc[1] = {0.0};
+    T t = T(0);
+    GRID_STRIDE(i, n) t = fma(a[i], b[i], t);
+    double acc[1] = {(double)t};
     const int ops[1] = {kSum};
-    GRID_STRIDE(i, n) acc[0] = fma(a[i], b[i], acc[0]);
-    grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dres = t[0]; });
+    grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dres = v[0]; });
 }
 
-__global__ void k_norm2(uint32_t n, const double* __restrict__ a, Scratch s, double* dres)
+template <typename T>
+__global__ void k_norm2(uint32_t n, const T* __restrict__ a, Scratch s, double* dres)
 {
-    double acc[1] = {0.0};
+    T t = T(0);
+    GRID_STRIDE(i, n) t = fma(a[i], a[i], t);
+    double acc[1] = {(double)t};
     const int ops[1] = {kSum};
-    GRID_STRIDE(i, n) acc[0] = fma(a[i], a[i], acc[0]);
-    grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dres = sqrt(t[0]); });
+    grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dres = sqrt(v[0]); });
 }
 
-__global__ void k_norminf(uint32_t n, const double* __restrict__ a, Scratch s, double* dres)
+template <typename T>
+__global__ void k_norminf(uint32_t n, const T* __restrict__ a, Scratch s, double* dres)
 {
-    double acc[1] = {0.0};
+    T t = T(0);
+    GRID_STRIDE(i, n) t = fmax(t, fabs(a[i]));
+    double acc[1] = {(double)t};
     const int ops[1] = {kMax};
-    GRID_STRIDE(i, n) acc[0] = fmax(acc[0], fabs(a[i]));
-    grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dres = t[0]; });
+    grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dres = v[0]; });
 }
 
-int v_dot(Ctx& c, uint32_t n, const double* a, const double* b, double* dres)
+template <typename T>
+int v_dot(Ctx& c, uint32_t n, const T* a, const T* b, double* dres)
 {
     ++c.launches;
-    k_dot<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, b, c.red, dres);
+    k_dot<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, b, c.red, dres);
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
-int v_norm2(Ctx& c, uint32_t n, const double* a, double* dres)
+template <typename T>
+int v_norm2(Ctx& c, uint32_t n, const T* a, double* dres)
 {
     ++c.launches;
-    k_norm2<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
+    k_norm2<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
-int v_norminf(Ctx& c, uint32_t n, const double* a, double* dres)
+template <typename T>
+int v_norminf(Ctx& c, uint32_t n, const T* a, double* dres)
 {
     ++c.launches;
-    k_norminf<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
+    k_norminf<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
 // ---- updates ---------------------------------------------------------------------------
 
-__global__ void k_axpy(uint32_t n, Scal a, const double* __restrict__ x, double* __restrict__ y)
+template <typename T>
+__global__ void k_axpy(uint32_t n, Scal a, const T* __restrict__ x, T* __restrict__ y)
 {
-    const double av = eval(a);
+    const T av = (T)eval(a);
     GRID_STRIDE(i, n) y[i] = fma(av, x[i], y[i]);
 }
 
-__global__ void k_xpay(uint32_t n, Scal a, const double* __restrict__ x, double* __restrict__ y)
+template <typename T>
+__global__ void k_xpay(uint32_t n, Scal a, const T* __restrict__ x, T* __restrict__ y)
 {
-    const double av = eval(a);
+    const T av = (T)eval(a);
     GRID_STRIDE(i, n) y[i] = fma(av, y[i], x[i]);
 }
 
-__global__ void k_axpby(uint32_t n, Scal a, Scal b, const double* __restrict__ y,
-                        double* __restrict__ x)
+template <typename T>
+__global__ void k_axpby(uint32_t n, Scal a, Scal b, const T* __restrict__ y, T* __restrict__ x)
 {
-    const double av = eval(a), bv = eval(b);
+    const T av = (T)eval(a), bv = (T)eval(b);
     GRID_STRIDE(i, n) x[i] = fma(av, x[i], bv * y[i]);
 }
 
-__global__ void k_waxpby(uint32_t n, Scal a, const double* __restrict__ v1, Scal b,
-                         const double* __restrict__ v2, double* __restrict__ w)
+template <typename T>
+__global__ void k_waxpby(uint32_t n, Scal a, const T* __restrict__ v1, Scal b,
+                         const T* __restrict__ v2, T* __restrict__ w)
 {
-    const double av = eval(a), bv = eval(b);
+    const T av = (T)eval(a), bv = (T)eval(b);
     GRID_STRIDE(i, n) w[i] = fma(av, v1[i], bv * v2[i]);
 }
 
-__global__ void k_scale(uint32_t n, Scal a, double* __restrict__ x)
+template <typename T>
+__global__ void k_scale(uint32_t n, Scal a, T* __restrict__ x)
 {
-    const double av = eval(a);
+    const T av = (T)eval(a);
     GRID_STRIDE(i, n) x[i] *= av;
 }
 
-__global__ void k_set(uint32_t n, double v, double* __restrict__ x)
+template <typename T>
+__global__ void k_set(uint32_t n, T v, T* __restrict__ x)
 {
     GRID_STRIDE(i, n) x[i] = v;
 }
 
-__global__ void k_pmult(uint32_t n, const double* __restrict__ d, double* __restrict__ x)
+template <typename T>
+__global__ void k_pmult(uint32_t n, const T* __restrict__ d, T* __restrict__ x)
 {
     GRID_STRIDE(i, n) x[i] *= d[i];
 }
 
-__global__ void k_add(uint32_t n, const double* __restrict__ d, double* __restrict__ x)
+template <typename T>
+__global__ void k_add(uint32_t n, const T* __restrict__ d, T* __restrict__ x)
 {
     GRID_STRIDE(i, n) x[i] += d[i];
 }
@@ -161,108 +179,145 @@ __global__ void k_recip_scale(uint32_t n, double w, const double* __restrict__ d
         return kOk;                                                                        \
     } while (0)
 
-int v_axpy(Ctx& c, uint32_t n, Scal a, const double* x, double* y) { LAUNCH_EW(k_axpy, n, a, x, y); }
-int v_xpay(Ctx& c, uint32_t n, Scal a, const double* x, double* y) { LAUNCH_EW(k_xpay, n, a, x, y); }
-int v_axpby(Ctx& c, uint32_t n, Scal a, Scal b, const double* y, double* x)
+template <typename T>
+int v_axpy(Ctx& c, uint32_t n, Scal a, const T* x, T* y) { LAUNCH_EW(k_axpy<T>, n, a, x, y); }
+template <typename T>
+int v_xpay(Ctx& c, uint32_t n, Scal a, const T* x, T* y) { LAUNCH_EW(k_xpay<T>, n, a, x, y); }
+template <typename T>
+int v_axpby(Ctx& c, uint32_t n, Scal a, Scal b, const T* y, T* x)
 {
-    LAUNCH_EW(k_axpby, n, a, b, y, x);
+    LAUNCH_EW(k_axpby<T>, n, a, b, y, x);
 }
-int v_waxpby(Ctx& c, uint32_t n, Scal a, const double* v1, Scal b, const double* v2, double* w)
+template <typename T>
+int v_waxpby(Ctx& c, uint32_t n, Scal a, const T* v1, Scal b, const T* v2, T* w)
 {
-    LAUNCH_EW(k_waxpby, n, a, v1, b, v2, w);
+    LAUNCH_EW(k_waxpby<T>, n, a, v1, b, v2, w);
 }
-int v_scale(Ctx& c, uint32_t n, Scal a, double* x) { LAUNCH_EW(k_scale, n, a, x); }
-int v_set(Ctx& c, uint32_t n, double v, double* x) { LAUNCH_EW(k_set, n, v, x); }
-int v_pmult(Ctx& c, uint32_t n, const double* d, double* x) { LAUNCH_EW(k_pmult, n, d, x); }
-int v_add(Ctx& c, uint32_t n, const double* d, double* x) { LAUNCH_EW(k_add, n, d, x); }
+template <typename T>
+int v_scale(Ctx& c, uint32_t n, Scal a, T* x) { LAUNCH_EW(k_scale<T>, n, a, x); }
+template <typename T>
+int v_set(Ctx& c, uint32_t n, double v, T* x) { LAUNCH_EW(k_set<T>, n, (T)v, x); }
+template <typename T>
+int v_pmult(Ctx& c, uint32_t n, const T* d, T* x) { LAUNCH_EW(k_pmult<T>, n, d, x); }
+template <typename T>
+int v_add(Ctx& c, uint32_t n, const T* d, T* x) { LAUNCH_EW(k_add<T>, n, d, x); }
 int v_recip_scale(Ctx& c, uint32_t n, double w, const double* d, double* out)
 {
     LAUNCH_EW(k_recip_scale, n, w, d, out);
 }
 
-int v_copy(Ctx& c, uint32_t n, const double* src, double* dst)
+template <typename T>
+int v_copy(Ctx& c, uint32_t n, const T* src, T* dst)
 {
     if (n == 0 || src == dst) return kOk;
-    FB_CUDA(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
+    FB_CUDA(cudaMemcpyAsync(dst, src, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice,
                             c.stream));
     return kOk;
 }
 
 // ---- classical Gram-Schmidt building blocks ------------------------------------------
-// V holds basis vectors at V + j*ld. KC vectors are handled per launch.
+// V holds basis vectors at V + j*ld. KC vectors are handled per launch; the coefficients
+// h stay FP64 for either vector type.
 
 constexpr int KC = 8;
 
 // dres[j] = (V_j, w), j in [j0, j0+k)
-__global__ void k_multidot(uint32_t n, int k, const double* __restrict__ V, size_t ld,
-                           const double* __restrict__ w, Scratch s, double* dres)
+template <typename T>
+__global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
+                           const T* __restrict__ w, Scratch s, double* dres)
 {
+    T t[KC];
     double acc[KC];
     int ops[KC];
 #pragma unroll
     for (int j = 0; j < KC; ++j) {
-        acc[j] = 0.0;
+        t[j] = T(0);
         ops[j] = kSum;
     }
     GRID_STRIDE(i, n)
     {
-        const double wi = w[i];
+        const T wi = w[i];
 #pragma unroll
         for (int j = 0; j < KC; ++j)
-            if (j < k) acc[j] = fma(V[j * ld + i], wi, acc[j]);
+            if (j < k) t[j] = fma(V[j * ld + i], wi, t[j]);
     }
-    grid_reduce<KC>(acc, ops, s, [=] __device__(const double* t) {
-        for (int j = 0; j < k; ++j) dres[j] = t[j];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) acc[j] = (double)t[j];
+    grid_reduce<KC>(acc, ops, s, [=] __device__(const double* v) {
+        for (int j = 0; j < k; ++j) dres[j] = v[j];
     });
 }
 
 // w -= sign * sum_j h[j] V_j; with dnorm != null also ||w_new|| -> *dnorm.
-__global__ void k_multiaxpy(uint32_t n, int k, const double* __restrict__ V, size_t ld,
-                            const double* __restrict__ h, double sign, double* __restrict__ w,
+template <typename T>
+__global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
+                            const double* __restrict__ h, double sign, T* __restrict__ w,
                             Scratch s, double* dnorm)
 {
-    double hj[KC];
+    T hj[KC];
 #pragma unroll
-    for (int j = 0; j < KC; ++j) hj[j] = j < k ? sign * h[j] : 0.0;
-    double acc[1] = {0.0};
-    const int ops[1] = {kSum};
+    for (int j = 0; j < KC; ++j) hj[j] = j < k ? (T)(sign * h[j]) : T(0);
+    T t = T(0);
     GRID_STRIDE(i, n)
     {
-        double wi = w[i];
+        T wi = w[i];
 #pragma unroll
         for (int j = 0; j < KC; ++j)
             if (j < k) wi = fma(-hj[j], V[j * ld + i], wi);
         w[i] = wi;
-        acc[0] = fma(wi, wi, acc[0]);
+        t = fma(wi, wi, t);
     }
-    if (dnorm) grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dnorm = sqrt(t[0]); });
+    double acc[1] = {(double)t};
+    const int ops[1] = {kSum};
+    if (dnorm) grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dnorm = sqrt(v[0]); });
 }
 
-int v_multidot(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* w,
-               double* dres)
+template <typename T>
+int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres)
 {
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         ++c.launches;
-    k_multidot<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, kk, V + j0 * ld, ld, w, c.red,
-                                                                 dres + j0);
+        k_multidot<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, kk, V + j0 * ld, ld, w,
+                                                                   c.red, dres + j0);
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
 }
 
-int v_multiaxpy(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* h,
-                double sign, double* w, double* dnorm)
+template <typename T>
+int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
+                double sign, T* w, double* dnorm)
 {
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         const bool last = j0 + KC >= k;
         ++c.launches;
-    k_multiaxpy<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
+        k_multiaxpy<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
             n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr);
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
 }
+
+#define FB_VEC_INSTANTIATE(T)                                                              \
+    template int v_dot<T>(Ctx&, uint32_t, const T*, const T*, double*);                   \
+    template int v_norm2<T>(Ctx&, uint32_t, const T*, double*);                           \
+    template int v_norminf<T>(Ctx&, uint32_t, const T*, double*);                         \
+    template int v_axpy<T>(Ctx&, uint32_t, Scal, const T*, T*);                           \
+    template int v_xpay<T>(Ctx&, uint32_t, Scal, const T*, T*);                           \
+    template int v_axpby<T>(Ctx&, uint32_t, Scal, Scal, const T*, T*);                    \
+    template int v_waxpby<T>(Ctx&, uint32_t, Scal, const T*, Scal, const T*, T*);         \
+    template int v_scale<T>(Ctx&, uint32_t, Scal, T*);                                    \
+    template int v_set<T>(Ctx&, uint32_t, double, T*);                                    \
+    template int v_copy<T>(Ctx&, uint32_t, const T*, T*);                                 \
+    template int v_pmult<T>(Ctx&, uint32_t, const T*, T*);                                \
+    template int v_add<T>(Ctx&, uint32_t, const T*, T*);                                  \
+    template int v_multidot<T>(Ctx&, uint32_t, int, const T*, size_t, const T*, double*); \
+    template int v_multiaxpy<T>(Ctx&, uint32_t, int, const T*, size_t, const double*,     \
+                                double, T*, double*);
+FB_VEC_INSTANTIATE(double)
+FB_VEC_INSTANTIATE(float)
+#undef FB_VEC_INSTANTIATE
 
 } // namespace fb

@@ -423,7 +423,14 @@ int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out)
         case FASP_GPU_JACOBI: case FASP_GPU_MG: break;
         default: return kErrSolverType;
     }
-    if (cfg->precision == FASP_GPU_MIXED && cfg->alg != FASP_GPU_CG) return kErrSolverType;
+    if (cfg->precision == FASP_GPU_MIXED && cfg->alg != FASP_GPU_CG &&
+        cfg->alg != FASP_GPU_BICGSTAB && cfg->alg != FASP_GPU_GMRES &&
+        cfg->alg != FASP_GPU_FGMRES)
+        return kErrSolverType;
+    if (cfg->precision == FASP_GPU_MIXED_RELIABLE && cfg->alg != FASP_GPU_CG)
+        return kErrSolverType;
+    if (cfg->precision < FASP_GPU_FP64 || cfg->precision > FASP_GPU_MIXED_RELIABLE)
+        return kErrInputPar;
     fasp_gpu_solver h = new (std::nothrow) fasp_gpu_solver_s();
     if (!h) return kErrAlloc;
     h->s.cfg = *cfg;

@@ -11,6 +11,7 @@
 // two kernels do (breakdown, safe-guard copy, stagnation restart, false-convergence check)
 // set status = kEsc and are finished by the host, which then relaunches cg_resume.
 #include <cstring>
+#include <type_traits>
 
 #include "cg.cuh"
 
@@ -96,6 +97,24 @@ __device__ void cg_checks(CGCtl* c, const double* red, int phase)
         c->resAbs = resAbs;
         c->resRel = resAbs / c->denAbs;
         cg_rec(c, c->numIter, resAbs);
+        if (c->reliable) {
+            // Reliable updates: hand x and r to the host for an FP64 refresh when the
+            // recursive residual meets the stop test or has fallen by delta since the last
+            // refresh. phase 1 = resumed right after a refresh (the host checked the stop).
+            if (resAbs > c->rmax) c->rmax = resAbs;
+            if (phase < 1 && (c->resRel < c->innerTol || resAbs < c->absTolIn ||
+                              resAbs < c->delta * c->rmax)) {
+                if (c->devRefresh) {
+                    c->status = kRefresh;
+                    c->reason = kReliable;
+                } else {
+                    cg_esc(c, kReliable, 1, red);
+                }
+                return;
+            }
+            cg_prepare_next(c, red[1], red[0]);
+            return;
+        }
         if (c->resRel < c->innerTol) {
             cg_done(c, kOk);
             return;
@@ -136,6 +155,77 @@ __device__ void cg_checks(CGCtl* c, const double* red, int phase)
     cg_prepare_next(c, red[1], red[0]);
 }
 
+// After the FP64 residual of a reliable update: t = {(r,r) FP64, (r,r) and (z,r) of the
+// rescaled FP32 copy}. Stops when the FP64 test passes; otherwise the FP32 iteration goes
+// on from the refreshed residual with the same p (beta = (z,r) / (z,r)_old).
+__device__ void cg_after_refresh(CGCtl* c, const double* t)
+{
+    const double rn = sqrt(t[0]);
+    c->res64 = rn;
+    c->refreshes += 1;
+    c->reason = kNoReason;
+    const bool conv = rn / c->den64 < c->relTol || rn < c->absTol;
+    if (conv || !isfinite(rn)) {
+        c->converged = conv ? 1 : 0;
+        cg_rec(c, c->numIter, rn / c->histScale);
+        cg_done(c, kOk);
+        return;
+    }
+    c->status = kRun;
+    c->rmax = sqrt(t[1]);
+    const double red[5] = {t[1], t[2], 0.0, 0.0, 0.0};
+    cg_checks(c, red, 1);
+    cg_rec(c, c->numIter, rn / c->histScale);
+}
+
+// Reliable update, part 1 (in the cg_spmv slot): x64 += s x32, x32 = 0.
+__device__ __forceinline__ void cg_refresh_fold(uint32_t n, float* x32, const CGCtl* c)
+{
+    double* x64 = c->rx;
+    const double s = c->histScale;
+    GRID_STRIDE(i, n)
+    {
+        x64[i] = fma(s, (double)x32[i], x64[i]);
+        x32[i] = 0.0f;
+    }
+}
+
+// Reliable update, part 2 (in the cg_update slot): r64 = b - A x64 on the FP64 values,
+// r32 = r64 / s, z32 = diagInv .* r32, with the three sums of cg_after_refresh.
+template <int JAC>
+__device__ __forceinline__ void cg_refresh_residual(const CSRView<float>& A, float* r32,
+                                                    float* z32, const float* dinv32,
+                                                    CGCtl* c, Scratch s)
+{
+    const CSRView<double> A64{A.nrow, A.mcol, A.nnz, A.rowPtr, A.colInd, c->rval};
+    const double* b = c->rb;
+    const double* x64 = c->rx;
+    double* r64 = c->rr;
+    const double inv = 1.0 / c->histScale;
+    double rr64 = 0.0;
+    float rr = 0.f, zr = 0.f;
+    GRID_STRIDE(row, A.nrow)
+    {
+        const uint32_t bb = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
+        const double ax = row_dot<double, false>(A64, bb, e, [&](uint32_t j) { return x64[j]; });
+        const double ri = b[row] - ax;
+        r64[row] = ri;
+        const float r32i = (float)(ri * inv);
+        r32[row] = r32i;
+        float zi = r32i;
+        if (JAC) {
+            zi = dinv32[row] * r32i;
+            z32[row] = zi;
+        }
+        rr64 = fma(ri, ri, rr64);
+        rr = fmaf(r32i, r32i, rr);
+        zr = fmaf(zi, r32i, zr);
+    }
+    double a[3] = {rr64, (double)rr, (double)zr};
+    const int ops[3] = {kSum, kSum, kSum};
+    grid_reduce<3>(a, ops, s, [=] __device__(const double* t) { cg_after_refresh(c, t); });
+}
+
 // ---- kernels ---------------------------------------------------------------------------
 
 template <typename T>
@@ -153,10 +243,14 @@ struct V16<double> {
 
 template <typename T, int L>
 __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restrict__ z,
-                                                  T* P0, T* P1, T* __restrict__ q, CGCtl* c,
-                                                  Scratch s)
+                                                  T* P0, T* P1, T* __restrict__ q, T* x,
+                                                  CGCtl* c, Scratch s)
 {
-    if (c->status != kRun) return;
+    if (c->status != kRun) {
+        if constexpr (std::is_same<T, float>::value)
+            if (c->status == kRefresh) cg_refresh_fold(A.nrow, x, c);
+        return;
+    }
     const int mode = c->pmode, par = c->par;
     const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
@@ -213,9 +307,13 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
                                                     const T* P0, const T* P1,
                                                     const T* __restrict__ q,
                                                     const T* __restrict__ dinv, CGCtl* c,
-                                                    Scratch s)
+                                                    Scratch s, CSRView<T> A)
 {
-    if (c->status != kRun) return;
+    if (c->status != kRun) {
+        if constexpr (std::is_same<T, float>::value)
+            if (c->status == kRefresh) cg_refresh_residual<JAC>(A, r, z, dinv, c, s);
+        return;
+    }
     const T alpha = (T)c->alpha;
     const T* __restrict__ p = c->par ? P1 : P0;
     T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
@@ -526,7 +624,7 @@ void CGEngine<T>::launch_spmv_kernel()
     const T* zz = jacobi ? z : r;
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, ctl, c->red);
+        kern<<<g, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, x, ctl, c->red);
     };
     switch (A->lanes) {
         case 1: go(cg_spmv<T, 1>); break;
@@ -542,9 +640,10 @@ template <typename T>
 void CGEngine<T>::launch_update_kernel()
 {
     const int need = c->grid(n / V16<T>::W + 1, kBlock, 16);
+    const CSRView<T> V = view_of<T>(*A);
     auto go = [&](auto kern, T* zz) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c->stream>>>(n, x, r, zz, P0, P1, q, dinv, ctl, c->red);
+        kern<<<g, kBlock, 0, c->stream>>>(n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
     };
     if (jacobi)
         go(cg_update<T, 1>, z);
@@ -729,7 +828,7 @@ int CGEngine<T>::run(unsigned* launches)
                                     c->stream));
             FB_CUDA(cudaStreamSynchronize(c->stream));
             if (launches) *launches += 2 * itersPerGraph;
-            if (*hstatus != kRun) return kOk;
+            if (*hstatus != kRun && *hstatus != kRefresh) return kOk;
         }
     }
     cudaEvent_t ev[2];
@@ -752,7 +851,7 @@ int CGEngine<T>::run(unsigned* launches)
             break;
         }
         // hstatus was written by the graph that ev[cur] follows (stream order)
-        if (*hstatus != kRun) break;
+        if (*hstatus != kRun && *hstatus != kRefresh) break;
         cur ^= 1;
     }
     if (launches) *launches += 2 * itersPerGraph;

@@ -6,8 +6,10 @@
 
 namespace fb {
 
-enum CGStatus { kRun = 0, kDone = 1, kEsc = 2 };
-enum CGReason { kNoReason = 0, kBreakdown = 1, kSave = 2, kStag = 3, kCheck3 = 4 };
+// kRefresh: a reliable update is in progress inside the iteration kernels (the next cg_spmv
+// folds x into FP64, the next cg_update recomputes the FP64 residual); the host keeps going.
+enum CGStatus { kRun = 0, kDone = 1, kEsc = 2, kRefresh = 3 };
+enum CGReason { kNoReason = 0, kBreakdown = 1, kSave = 2, kStag = 3, kCheck3 = 4, kReliable = 5 };
 
 // The locals of CG::Solve (CG.cxx:55-64) plus the parameters it reads, kept in device
 // memory so that the finalize thread of each fused kernel can run the reference's control
@@ -23,11 +25,25 @@ struct CGCtl {
     int      par;       // which of the two p buffers holds the current direction
     int      pzero;     // the host zeroed p (a restart): next p = z
     int      inner;     // 1: inner solve of mixed refinement (plain relative stop)
+    int      reliable;  // 1 (with inner): FP32 iterations with FP64 reliable updates
     int      bench;     // 1: kernel timing, the finalize steps do nothing
     unsigned numIter, stagStep, moreStep;
     unsigned maxIter, minIter, savIter, restart;
     double   relTol, absTol, solStagTol, innerTol;
     double   tmpa, tmpb, alpha, beta, resAbs, resRel, denAbs, ratio, resAbsOld, xRelDiff;
+    double   delta;     // reliable: refresh when resAbs < delta * rmax
+    double   rmax;      // reliable: largest recursive residual since the last refresh
+    double   absTolIn;  // reliable: absolute tolerance in the scaled units of the FP32 vectors
+    // reliable updates run by the iteration kernels (graph and plain engines): the FP64
+    // side, the stop test on the FP64 residual (relTol, absTol, den64) and its outcome
+    int      devRefresh;
+    int      converged;
+    unsigned refreshes;
+    double   den64, res64;
+    const double* rb;   // b
+    double*  rx;        // x (FP64)
+    double*  rr;        // r = b - A x (FP64), written by each refresh
+    const double* rval; // FP64 values of the matrix (same structure as the FP32 view)
     double   red[5];    // rr, zr, xx, max|x|, pp saved at an escalation
     double*  hist;
     unsigned histCap;

@@ -100,28 +100,31 @@ struct Mat {
 };
 
 // ---- vector kernels (blas.cu) ---------------------------------------------------------
-// Reductions write their result to a device scalar (dres); vector updates take Scal.
-int v_dot(Ctx& c, uint32_t n, const double* a, const double* b, double* dres);
-int v_norm2(Ctx& c, uint32_t n, const double* a, double* dres);
-int v_norminf(Ctx& c, uint32_t n, const double* a, double* dres);
-int v_axpy(Ctx& c, uint32_t n, Scal a, const double* x, double* y);      // y += a x
-int v_xpay(Ctx& c, uint32_t n, Scal a, const double* x, double* y);      // y = a y + x
-int v_axpby(Ctx& c, uint32_t n, Scal a, Scal b, const double* y, double* x); // x = a x + b y
-int v_waxpby(Ctx& c, uint32_t n, Scal a, const double* v1, Scal b, const double* v2,
-             double* w);                                                 // w = a v1 + b v2
-int v_scale(Ctx& c, uint32_t n, Scal a, double* x);
-int v_set(Ctx& c, uint32_t n, double v, double* x);
-int v_copy(Ctx& c, uint32_t n, const double* src, double* dst);
-int v_pmult(Ctx& c, uint32_t n, const double* d, double* x);            // x *= d
-int v_add(Ctx& c, uint32_t n, const double* d, double* x);              // x += d
+// T = double or float (explicitly instantiated for both). Reductions write their FP64 result
+// to a device scalar (dres); vector updates take Scal.
+template <typename T> int v_dot(Ctx& c, uint32_t n, const T* a, const T* b, double* dres);
+template <typename T> int v_norm2(Ctx& c, uint32_t n, const T* a, double* dres);
+template <typename T> int v_norminf(Ctx& c, uint32_t n, const T* a, double* dres);
+template <typename T> int v_axpy(Ctx& c, uint32_t n, Scal a, const T* x, T* y);   // y += a x
+template <typename T> int v_xpay(Ctx& c, uint32_t n, Scal a, const T* x, T* y);   // y = a y + x
+template <typename T>
+int v_axpby(Ctx& c, uint32_t n, Scal a, Scal b, const T* y, T* x);                 // x = a x + b y
+template <typename T>
+int v_waxpby(Ctx& c, uint32_t n, Scal a, const T* v1, Scal b, const T* v2, T* w); // w = a v1 + b v2
+template <typename T> int v_scale(Ctx& c, uint32_t n, Scal a, T* x);
+template <typename T> int v_set(Ctx& c, uint32_t n, double v, T* x);
+template <typename T> int v_copy(Ctx& c, uint32_t n, const T* src, T* dst);
+template <typename T> int v_pmult(Ctx& c, uint32_t n, const T* d, T* x);          // x *= d
+template <typename T> int v_add(Ctx& c, uint32_t n, const T* d, T* x);            // x += d
 int v_recip_scale(Ctx& c, uint32_t n, double w, const double* d, double* out); // out = w*(1/d)
 // Classical Gram-Schmidt blocks over a basis stored at V + j*ld:
 // dres[j] = (V_j, w) for j < k, in one pass over w;
-int v_multidot(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* w,
-               double* dres);
+template <typename T>
+int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres);
 // w -= sign * sum_j h[j] V_j (h on the device); dnorm (nullable) receives ||w_new||.
-int v_multiaxpy(Ctx& c, uint32_t n, int k, const double* V, size_t ld, const double* h,
-                double sign, double* w, double* dnorm);
+template <typename T>
+int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
+                double sign, T* w, double* dnorm);
 
 // ---- sparse kernels (spmv.cu) ---------------------------------------------------------
 int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
@@ -129,9 +132,13 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
 void m_free(Mat& M);
 int m_spmv(Ctx& c, const Mat& A, const double* x, double* y);           // y = A x
 int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y);
+inline int m_spmv(Ctx& c, const Mat& A, const float* x, float* y) { return m_spmv32(c, A, x, y); }
 // r = b - A x with the x ~ 0 shortcut of MAT::Residual; the NormInf(x) comes from xinf
-// (device scalar computed by the caller) unless xinf is null (then computed here).
+// (device scalar computed by the caller) unless xinf is null (then computed here). The
+// float overload runs on the matrix's FP32 values (Mat::ensure32 first).
 int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
+               const double* xinf);
+int m_residual(Ctx& c, const Mat& A, const float* b, const float* x, float* r,
                const double* xinf);
 int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR -> CSC, exact
 int lanes_for(double meanRowLen);                                         // SpMV mapping

@@ -25,13 +25,24 @@ struct Pcd {
     double*         dinv = nullptr;   // weight / diag
     float*          dinv32 = nullptr;
     double*         work = nullptr;
+    float*          work32 = nullptr; // FP32 sweeps of mixed-precision inner solves (lazy)
     uint32_t        numIter = 0;
     bool pure() const { return type == 1 && prm.minIter == prm.maxIter; }
     int  setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p);
     void destroy();
-    // Solve(b, x): x is read as the initial guess (callers zero it where the reference does)
-    int  solve(Ctx& c, const double* b, double* x, std::vector<double>* hist = nullptr,
+    // Solve(b, x): x is read as the initial guess (callers zero it where the reference does).
+    // T = float runs the same sweeps on the FP32 matrix values and diagInv.
+    template <typename T>
+    int  solve(Ctx& c, const T* b, T* x, std::vector<double>* hist = nullptr,
                double* norm2 = nullptr, double* normInf = nullptr);
+};
+
+// The vectors one precision of a host-orchestrated solver works on.
+template <typename T>
+struct Space {
+    std::vector<T*>* w = nullptr;  // work vectors
+    T*               V = nullptr;  // GMRES/FGMRES basis, (maxRestart+1) x n
+    T*               Z = nullptr;  // FGMRES preconditioned basis
 };
 
 struct SolverImpl {
@@ -45,6 +56,13 @@ struct SolverImpl {
     std::vector<double*> w;
     double*         V = nullptr;    // GMRES/FGMRES basis, (maxRestart+1) x n
     double*         Z = nullptr;    // FGMRES preconditioned basis
+    // FP32 copies for the inner solves of mixed-precision BiCGStab / GMRES / FGMRES
+    std::vector<float*> w32;
+    float*          V32 = nullptr;
+    float*          Z32 = nullptr;
+    // history entries are stored at histOff + k, scaled by histScale (inner solves)
+    uint32_t        histOff = 0;
+    double          histScale = 1.0;
     double*         gm = nullptr;   // device Hessenberg block: hh, hcos, hsin, var, dots
     uint32_t        maxRestart = 0, minRestart = 0, restart = 0;
     // MG (identity transfers): per level smoother and coarse solver, coarse b and x
@@ -74,9 +92,18 @@ struct SolverImpl {
     int cg_generic(const double* b, double* x, fasp_gpu_info* info);
     int cg_device(const double* b, double* x, fasp_gpu_info* info);
     int cg_mixed(const double* b, double* x, fasp_gpu_info* info);
-    int bicgstab(const double* b, double* x, fasp_gpu_info* info);
-    int gmres_right(const double* b, double* x, fasp_gpu_info* info, bool flexible);
-    int gmres_left(const double* b, double* x, fasp_gpu_info* info);
+    int cg_reliable(const double* b, double* x, fasp_gpu_info* info);
+    template <typename T>
+    int bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P, Space<T> S);
+    template <typename T>
+    int gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
+                    Space<T> S, bool flexible);
+    template <typename T>
+    int gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P, Space<T> S);
+    // FP64 iterative refinement around FP32 inner BiCGStab / GMRES / FGMRES solves
+    int refine(const double* b, double* x, fasp_gpu_info* info);
+    Space<double> sp64() { return Space<double>{&w, V, Z}; }
+    Space<float>  sp32() { return Space<float>{&w32, V32, Z32}; }
     int jacobi(const double* b, double* x, fasp_gpu_info* info);
     int mg(const double* b, double* x, fasp_gpu_info* info);
     void mg_cycle(const double* b, double* x);
@@ -85,8 +112,9 @@ struct SolverImpl {
     double fetch(const double* dptr);
     void   rec(uint32_t k, double v)
     {
+        k += histOff;
         if (k >= hist.size()) hist.resize((size_t)k + 1, std::numeric_limits<double>::quiet_NaN());
-        hist[k] = v;
+        hist[k] = v * histScale;
     }
 };
 

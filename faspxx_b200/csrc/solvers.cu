@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 
 #include "solver.h"
 
@@ -33,27 +34,30 @@ double SolverImpl::fetch(const double* dptr)
 }
 
 // A->Apply(x, r); r.XPAY(-1.0, b)  -> r = b - A x without the NormInf shortcut
-static int apply_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r)
+template <typename T>
+static int apply_residual(Ctx& c, const Mat& A, const T* b, const T* x, T* r)
 {
     return m_residual(c, A, b, x, r, c.dslot + SL_ONE);
 }
 
 // ---- Jacobi (src/Iter.cxx) ---------------------------------------------------------------
 
-__global__ void k_jacobi_update(uint32_t n, const double* __restrict__ dinv,
-                                const double* __restrict__ work, double* __restrict__ x,
+template <typename T>
+__global__ void k_jacobi_update(uint32_t n, const T* __restrict__ dinv,
+                                const T* __restrict__ work, T* __restrict__ x,
                                 Scratch s, double* dxinf)
 {
     // work .*= diagInv; x += work (Iter.cxx:91-92); also NormInf(x_new) for the next
     // residual's shortcut test
-    double acc[1] = {0.0};
-    const int ops[1] = {kMax};
+    T m = T(0);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const double xi = x[i] + work[i] * dinv[i];
+        const T xi = x[i] + work[i] * dinv[i];
         x[i] = xi;
-        acc[0] = fmax(acc[0], fabs(xi));
+        m = fmax(m, fabs(xi));
     }
+    double acc[1] = {(double)m};
+    const int ops[1] = {kMax};
     grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dxinf = t[0]; });
 }
 
@@ -81,17 +85,33 @@ void Pcd::destroy()
     cudaFree(dinv);
     cudaFree(dinv32);
     cudaFree(work);
+    cudaFree(work32);
     dinv = nullptr;
     dinv32 = nullptr;
     work = nullptr;
+    work32 = nullptr;
 }
 
 // Identity::Solve (Iter.cxx:16-20) or Jacobi::Solve (Iter.cxx:56-112).
-int Pcd::solve(Ctx& c, const double* b, double* x, std::vector<double>* hist, double* norm2,
+template <typename T>
+int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm2,
                double* normInf)
 {
     const uint32_t n = A->nrow;
     if (type == 0) return v_copy(c, n, b, x);
+    T* work;
+    const T* dinv;
+    if constexpr (std::is_same<T, float>::value) {
+        if (!work32 && cudaMalloc(&work32, ((size_t)n + 4) * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return kErrAlloc;
+        }
+        work = work32;
+        dinv = dinv32;
+    } else {
+        work = this->work;
+        dinv = this->dinv;
+    }
     auto fetch = [&](const double* d) {
         double v = kNaN;
         cudaMemcpyAsync(c.hslot + 1, d, 8, cudaMemcpyDeviceToHost, c.stream);
@@ -120,7 +140,8 @@ int Pcd::solve(Ctx& c, const double* b, double* x, std::vector<double>* hist, do
             if (resRel < prm.relTol || resAbs < prm.absTol) break;
         }
         ++c.launches;
-        k_jacobi_update<<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, dinv, work, x, c.red, xinf);
+        k_jacobi_update<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, dinv, work, x, c.red,
+                                                                        xinf);
         FB_CUDA(cudaGetLastError());
         ++numIter;
     }
@@ -137,17 +158,24 @@ int Pcd::solve(Ctx& c, const double* b, double* x, std::vector<double>* hist, do
     return kOk;
 }
 
+template int Pcd::solve<double>(Ctx&, const double*, double*, std::vector<double>*, double*,
+                                double*);
+template int Pcd::solve<float>(Ctx&, const float*, float*, std::vector<double>*, double*,
+                               double*);
+
 // ---- setup -------------------------------------------------------------------------------
 
-static int alloc_vecs(std::vector<double*>& w, int k, uint32_t n)
+template <typename T>
+static int alloc_vecs(std::vector<T*>& w, int k, uint32_t n)
 {
+    const size_t bytes = ((size_t)n + 4) * sizeof(T);
     for (int i = 0; i < k; ++i) {
-        double* p = nullptr;
-        if (cudaMalloc(&p, ((size_t)n + 2) * 8) != cudaSuccess) {
+        T* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
             cudaGetLastError();
             return kErrAlloc;
         }
-        cudaMemset(p, 0, ((size_t)n + 2) * 8);
+        cudaMemset(p, 0, bytes);
         w.push_back(p);
     }
     return kOk;
@@ -156,9 +184,7 @@ static int alloc_vecs(std::vector<double*>& w, int k, uint32_t n)
 int SolverImpl::setup(fasp_gpu_mat Mh)
 {
     if (!Mh) return kErrInputPar;
-    clean();
-    for (double* p : w) cudaFree(p);
-    w.clear();
+    destroy(); // a second Setup releases everything the first one allocated
     Ah = Mh;
     A = &Mh->M;
     n = A->nrow;
@@ -187,7 +213,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 cg64->wantPersistent = cfg.persistent != 0;
                 if ((e = cg64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
             }
-            if (cfg.precision == FASP_GPU_MIXED) {
+            if (cfg.precision == FASP_GPU_MIXED || cfg.precision == FASP_GPU_MIXED_RELIABLE) {
                 if (!fusable) return kErrPcdType; // mixed mode fuses its preconditioner
                 if ((e = Ah->M.ensure32(c.stream))) return e;
                 cg32 = new CGEngine<float>();
@@ -197,7 +223,13 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             break;
         }
         case FASP_GPU_BICGSTAB:
-            if ((e = alloc_vecs(w, 12, n))) return e;
+            if (cfg.precision == FASP_GPU_MIXED) {
+                // FP64: the outer residual; FP32: the inner solve's 12 vectors + b, e
+                if ((e = alloc_vecs(w, 1, n)) || (e = alloc_vecs(w32, 14, n))) return e;
+                if ((e = Ah->M.ensure32(c.stream))) return e;
+            } else if ((e = alloc_vecs(w, 12, n))) {
+                return e;
+            }
             break;
         case FASP_GPU_GMRES:
         case FASP_GPU_FGMRES: {
@@ -212,13 +244,26 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             else if (restart < minRestart)
                 restart = minRestart;
             if (maxRestart == 0 || restart == 0) return kErrInputPar;
-            if ((e = alloc_vecs(w, 3, n))) return e; // wk tmp safe
-            const size_t vb = (size_t)(maxRestart + 1) * n * 8;
-            if (cudaMalloc(&V, vb + 16) != cudaSuccess) return kErrAlloc;
-            cudaMemset(V, 0, vb);
-            if (alg == FASP_GPU_FGMRES) {
-                if (cudaMalloc(&Z, vb + 16) != cudaSuccess) return kErrAlloc;
-                cudaMemset(Z, 0, vb);
+            if (cfg.precision == FASP_GPU_MIXED) {
+                // FP64 outer residual; FP32 wk tmp safe + b, e and the FP32 bases
+                if ((e = alloc_vecs(w, 1, n)) || (e = alloc_vecs(w32, 5, n))) return e;
+                if ((e = Ah->M.ensure32(c.stream))) return e;
+                const size_t vb = (size_t)(maxRestart + 1) * n * 4;
+                if (cudaMalloc(&V32, vb + 16) != cudaSuccess) return kErrAlloc;
+                cudaMemset(V32, 0, vb);
+                if (alg == FASP_GPU_FGMRES) {
+                    if (cudaMalloc(&Z32, vb + 16) != cudaSuccess) return kErrAlloc;
+                    cudaMemset(Z32, 0, vb);
+                }
+            } else {
+                if ((e = alloc_vecs(w, 3, n))) return e; // wk tmp safe
+                const size_t vb = (size_t)(maxRestart + 1) * n * 8;
+                if (cudaMalloc(&V, vb + 16) != cudaSuccess) return kErrAlloc;
+                cudaMemset(V, 0, vb);
+                if (alg == FASP_GPU_FGMRES) {
+                    if (cudaMalloc(&Z, vb + 16) != cudaSuccess) return kErrAlloc;
+                    cudaMemset(Z, 0, vb);
+                }
             }
             const size_t m = maxRestart;
             const size_t gmSize = (m + 1) * m + (m + 1) + m + (m + 1) + 2 * (m + 1) + 4;
@@ -264,6 +309,8 @@ void SolverImpl::clean()
         const size_t vb = (size_t)(maxRestart + 1) * n * 8;
         if (V) cudaMemsetAsync(V, 0, vb, c.stream);
         if (Z) cudaMemsetAsync(Z, 0, vb, c.stream);
+        if (V32) cudaMemsetAsync(V32, 0, vb / 2, c.stream);
+        if (Z32) cudaMemsetAsync(Z32, 0, vb / 2, c.stream);
         cudaStreamSynchronize(c.stream);
     }
 }
@@ -272,6 +319,11 @@ void SolverImpl::destroy()
 {
     for (double* p : w) cudaFree(p);
     w.clear();
+    for (float* p : w32) cudaFree(p);
+    w32.clear();
+    cudaFree(V32);
+    cudaFree(Z32);
+    V32 = Z32 = nullptr;
     cudaFree(V);
     cudaFree(Z);
     cudaFree(gm);
@@ -625,13 +677,125 @@ int SolverImpl::cg_mixed(const double* b, double* x, fasp_gpu_info* info)
     return kOk;
 }
 
-// ---- BiCGStab (src/BiCGStab.cxx:68-270) ---------------------------------------------------
-
-int SolverImpl::bicgstab(const double* b, double* x, fasp_gpu_info* info)
+// Mixed precision with reliable updates (no reference counterpart): one FP32 PCG run whose
+// vectors are scaled by s = ||b - A x0||. Whenever the FP32 recursive residual meets the
+// stop test or has fallen by delta (innerRelTol) since the last refresh, the host folds the
+// FP32 correction into x in FP64 (x += s e, e = 0), recomputes r = b - A x in FP64, stops
+// if ||r|| / ||r0|| < relTol (or ||r|| < absTol), and otherwise continues the same Krylov
+// process from the refreshed residual: p is kept and beta = (z, r) / (z, r)_old uses the
+// refreshed r (the reliable-update scheme of Sleijpen and van der Vorst, 1996). Unlike
+// restarted refinement the conjugate directions survive each refresh, so the iteration
+// count stays that of FP64 CG while the SpMV and vector traffic is FP32.
+int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
 {
     const fasp_gpu_params& P = cfg.prm;
-    double *r0star = w[0], *tmp = w[1], *apj = w[2], *asj = w[3], *pj = w[4], *rj = w[5],
-           *sj = w[6], *ptmp = w[7], *stmp = w[8], *ms = w[9], *mp = w[10], *sv = w[11];
+    CGEngine<float>& E = *cg32;
+    CGCtl& h = *E.hctl;
+    double *x64 = w[0], *r64 = w[1];
+    int e;
+    v_copy(c, n, x, x64);
+    const double delta = cfg.innerRelTol > 0 && cfg.innerRelTol < 1 ? cfg.innerRelTol : 1e-2;
+    ++c.launches;
+    k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    std::vector<std::pair<uint32_t, double>> patches;
+    auto true_res = [&](double* rn) {
+        int err = apply_residual(c, *A, b, x64, r64);
+        if (err) return err;
+        if ((err = v_norm2(c, n, r64, c.dslot + SL_T1))) return err;
+        *rn = fetch(c.dslot + SL_T1);
+        return (int)kOk;
+    };
+    double rn = 0.0;
+    if ((e = true_res(&rn))) return e;
+    const double den = (kCloseZero > rn) ? kCloseZero : rn;
+    patches.push_back({0u, rn});
+    int code = kOk;
+    uint32_t iters = 0, refreshes = 0, hostRefreshes = 0;
+    bool converged = rn / den < P.relTol || rn < P.absTol;
+    if (!converged && std::isfinite(rn) && P.maxIter > 0) {
+        const double s = rn;
+        if ((e = convert_scaled(c, n, r64, 1.0 / s, E.r)) || (e = set32(c, n, E.x))) return e;
+        std::memset(&h, 0, sizeof(CGCtl));
+        h.maxIter = P.maxIter;
+        h.minIter = 0;
+        h.savIter = 0xffffffffu;
+        h.inner = 1;
+        h.reliable = 1;
+        h.innerTol = P.relTol * den / s;
+        h.relTol = P.relTol;
+        h.absTol = P.absTol;
+        h.absTolIn = P.absTol / s;
+        h.delta = delta;
+        h.hist = dhist;
+        h.histCap = dhistCap;
+        h.histScale = s;
+        // graph and plain engines refresh inside their kernels; the persistent one escalates
+        h.devRefresh = E.persistent ? 0 : 1;
+        h.den64 = den;
+        h.rb = b;
+        h.rx = x64;
+        h.rr = r64;
+        h.rval = A->val;
+        if ((e = E.push_ctl()) || (e = E.launch_init()) || (e = E.pull_ctl())) return e;
+        h.rmax = h.resAbs;
+        if ((e = E.push_ctl())) return e;
+        for (uint32_t guard = 0;; ++guard) {
+            if (h.status == kRun || h.status == kRefresh) {
+                unsigned gl = 0;
+                if ((e = E.run(&gl)) || (e = E.pull_ctl())) return e;
+                c.launches += gl;
+                continue;
+            }
+            if (h.status == kDone && h.converged) { // the last device refresh passed the test
+                rn = h.res64;
+                converged = true;
+                break;
+            }
+            // a host refresh: the stop test or delta reached (persistent engine), or the end
+            // of the FP32 run (maxIter, breakdown)
+            if ((e = update_from32(c, n, s, E.x, x64)) || (e = set32(c, n, E.x))) return e;
+            if ((e = true_res(&rn))) return e;
+            ++hostRefreshes;
+            patches.push_back({h.numIter, rn});
+            converged = rn / den < P.relTol || rn < P.absTol;
+            if (h.status == kDone || converged || !std::isfinite(rn) || guard > P.maxIter) {
+                if (h.status == kDone && h.code != kOk) code = h.code;
+                break;
+            }
+            if ((e = convert_scaled(c, n, r64, 1.0 / s, E.r))) return e;
+            h.rmax = rn / s;
+            h.phase = 1;
+            if ((e = E.push_ctl()) || (e = E.launch_resume()) || (e = E.pull_ctl())) return e;
+        }
+        iters = h.numIter;
+        refreshes = hostRefreshes + h.refreshes;
+    }
+    if (!converged && code == kOk) code = kErrMaxIt;
+    info->numIter = iters;
+    info->outerIter = refreshes;
+    info->escalations = hostRefreshes;
+    info->code = code;
+    info->norm2 = rn;
+    v_norminf(c, n, r64, c.dslot + SL_T2);
+    info->normInf = fetch(c.dslot + SL_T2);
+    v_copy(c, n, x64, x);
+    const uint32_t len = std::min<uint32_t>(iters + 1, dhistCap);
+    hist.assign(len, kNaN);
+    FB_CUDA(cudaMemcpyAsync(hist.data(), dhist, (size_t)len * 8, cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& pt : patches) rec(pt.first, pt.second);
+    return kOk;
+}
+
+// ---- BiCGStab (src/BiCGStab.cxx:68-270) ---------------------------------------------------
+
+template <typename T>
+int SolverImpl::bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
+                         Space<T> S)
+{
+    std::vector<T*>& w = *S.w;
+    T *r0star = w[0], *tmp = w[1], *apj = w[2], *asj = w[3], *pj = w[4], *rj = w[5],
+      *sj = w[6], *ptmp = w[7], *stmp = w[8], *ms = w[9], *mp = w[10], *sv = w[11];
     double* d = c.dslot;
     int err = kOk, e;
     const unsigned maxStag = kMaxStagNum;
@@ -832,7 +996,8 @@ __global__ void k_gmres_backsolve(GmLayout L, int count, int c1)
 
 __global__ void k_set_scalar(double* dst, double v) { *dst = v; }
 
-static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, double* wv)
+template <typename T>
+static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, const T* V, T* wv)
 {
     Ctx& c = S.c;
     const uint32_t n = S.n;
@@ -841,15 +1006,15 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, do
     if (S.cfg.orth == FASP_GPU_ORTH_MGS) { // GMRES.cxx:169-172
         for (int j = 0; j < count; ++j) {
             double* hj = L.hh + (size_t)j * L.m + c1;
-            v_dot(c, n, wv, S.V + j * ld, hj);
-            v_axpby(c, n, Scal::h(1.0), Scal::d(hj, -1.0), S.V + j * ld, wv);
+            v_dot(c, n, (const T*)wv, V + j * ld, hj);
+            v_axpby(c, n, Scal::h(1.0), Scal::d(hj, -1.0), V + j * ld, wv);
         }
-        v_norm2(c, n, wv, tn);
+        v_norm2(c, n, (const T*)wv, tn);
     } else { // CGS2: two fused multi-dot / multi-AXPY passes
-        v_multidot(c, n, count, S.V, ld, wv, L.h1);
-        v_multiaxpy(c, n, count, S.V, ld, L.h1, 1.0, wv, nullptr);
-        v_multidot(c, n, count, S.V, ld, wv, L.h2);
-        v_multiaxpy(c, n, count, S.V, ld, L.h2, 1.0, wv, tn);
+        v_multidot(c, n, count, V, ld, (const T*)wv, L.h1);
+        v_multiaxpy(c, n, count, V, ld, L.h1, 1.0, wv, nullptr);
+        v_multidot(c, n, count, V, ld, (const T*)wv, L.h2);
+        v_multiaxpy(c, n, count, V, ld, L.h2, 1.0, wv, tn);
     }
     ++c.launches;
     k_gmres_givens<<<1, 1, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn);
@@ -875,10 +1040,13 @@ static void adapt_restart(SolverImpl& S, double cr, bool inclusive)
 }
 
 // GMRES::RSolve (GMRES.cxx:114-280) and FGMRES::Solve (FGMRES.cxx:108-271)
-int SolverImpl::gmres_right(const double* b, double* x, fasp_gpu_info* info, bool flexible)
+template <typename T>
+int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
+                            Space<T> S, bool flexible)
 {
-    const fasp_gpu_params& P = cfg.prm;
-    double *wk = w[0], *tmp = w[1], *sv = w[2];
+    std::vector<T*>& w = *S.w;
+    T *wk = w[0], *tmp = w[1], *sv = w[2];
+    T *V = S.V, *Z = S.Z;
     const size_t ld = n;
     const GmLayout L = gm_layout(gm, maxRestart);
     double* d = c.dslot;
@@ -909,7 +1077,7 @@ int SolverImpl::gmres_right(const double* b, double* x, fasp_gpu_info* info, boo
         while (count < restart && numIter < P.maxIter) {
             ++numIter;
             count_1 = count++;
-            double* vnew = V + count * ld;
+            T* vnew = V + count * ld;
             if (flexible) {
                 v_set(c, n, 0.0, tmp);
                 if ((e = pcd.solve(c, V + count_1 * ld, Z + count_1 * ld))) return e;
@@ -919,7 +1087,7 @@ int SolverImpl::gmres_right(const double* b, double* x, fasp_gpu_info* info, boo
                 if ((e = pcd.solve(c, V + count_1 * ld, tmp))) return e;
                 m_spmv(c, *A, tmp, vnew);
             }
-            if ((e = orthogonalize(*this, L, count, count_1, vnew))) return e;
+            if ((e = orthogonalize<T>(*this, L, count, count_1, V, vnew))) return e;
             FB_CUDA(cudaMemcpyAsync(c.hslot + 2, L.out, 16, cudaMemcpyDeviceToHost, c.stream));
             FB_CUDA(cudaStreamSynchronize(c.stream));
             if (c.hslot[3] == 0.0) break;
@@ -971,10 +1139,13 @@ int SolverImpl::gmres_right(const double* b, double* x, fasp_gpu_info* info, boo
 }
 
 // GMRES::LSolve (GMRES.cxx:283-453)
-int SolverImpl::gmres_left(const double* b, double* x, fasp_gpu_info* info)
+template <typename T>
+int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
+                           Space<T> S)
 {
-    const fasp_gpu_params& P = cfg.prm;
-    double *wk = w[0], *tmp = w[1], *sv = w[2];
+    std::vector<T*>& w = *S.w;
+    T *wk = w[0], *tmp = w[1], *sv = w[2];
+    T *V = S.V;
     const size_t ld = n;
     const GmLayout L = gm_layout(gm, maxRestart);
     double* d = c.dslot;
@@ -1009,11 +1180,11 @@ int SolverImpl::gmres_left(const double* b, double* x, fasp_gpu_info* info)
         while (count < restart && numIter < P.maxIter) {
             ++numIter;
             count_1 = count++;
-            double* vnew = V + count * ld;
+            T* vnew = V + count * ld;
             m_spmv(c, *A, V + count_1 * ld, tmp);
             v_set(c, n, 0.0, vnew);
             if ((e = pcd.solve(c, tmp, vnew))) return e;
-            if ((e = orthogonalize(*this, L, count, count_1, vnew))) return e;
+            if ((e = orthogonalize<T>(*this, L, count, count_1, V, vnew))) return e;
             FB_CUDA(cudaMemcpyAsync(c.hslot + 2, L.out, 16, cudaMemcpyDeviceToHost, c.stream));
             FB_CUDA(cudaStreamSynchronize(c.stream));
             if (c.hslot[3] == 0.0) break;
@@ -1138,6 +1309,85 @@ int SolverImpl::mg(const double* b, double* x, fasp_gpu_info* info)
     return kOk;
 }
 
+// ---- mixed-precision BiCGStab / GMRES / FGMRES ------------------------------------------
+// FP64 iterative refinement (no reference counterpart): r = b - A x in FP64, the inner solver
+// runs its unchanged control flow in FP32 on A e = r / ||r|| (FP32 matrix values, vectors
+// and per-thread accumulation; FP64 block and grid reductions, and the GMRES Hessenberg and
+// Givens least-squares in FP64) to innerRelTol, then x += ||r|| e in FP64. Stops when
+// ||b - A x|| / ||b - A x0|| < relTol (or < absTol), after maxOuter steps, or when the
+// inner solve makes no iteration. History: inner residuals scaled back by ||r|| at their
+// global iteration index, each outer FP64 true residual at the index where it was taken.
+int SolverImpl::refine(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    double* r64 = w[0];
+    float* b32 = w32[w32.size() - 2];
+    float* e32 = w32[w32.size() - 1];
+    std::vector<float*> inner(w32.begin(), w32.end() - 2);
+    Space<float> S{&inner, V32, Z32};
+    const double innerTol = cfg.innerRelTol > 0 ? cfg.innerRelTol : 1e-4;
+    const uint32_t innerMax = cfg.innerMaxIter ? cfg.innerMaxIter : P.maxIter;
+    const uint32_t maxOuter = cfg.maxOuter ? cfg.maxOuter : 50;
+    uint32_t total = 0, outer = 0;
+    double den = 1.0, rn = 0.0;
+    int code = kOk, e;
+    std::vector<std::pair<uint32_t, double>> outerHist;
+    for (;;) {
+        if ((e = apply_residual(c, *A, b, (const double*)x, r64))) return e;
+        v_norm2(c, n, (const double*)r64, c.dslot + SL_T1);
+        rn = fetch(c.dslot + SL_T1);
+        if (outer == 0) den = (kCloseZero > rn) ? kCloseZero : rn;
+        outerHist.push_back({total, rn});
+        if (rn / den < P.relTol || rn < P.absTol) break;
+        if (outer >= maxOuter || total >= P.maxIter || !std::isfinite(rn)) {
+            code = kErrMaxIt;
+            break;
+        }
+        if ((e = convert_scaled(c, n, r64, 1.0 / rn, b32)) || (e = set32(c, n, e32))) return e;
+        fasp_gpu_params Q = P;
+        Q.relTol = innerTol;
+        Q.absTol = 0.0;
+        Q.minIter = 0;
+        Q.maxIter = std::min<uint32_t>(innerMax, P.maxIter - total);
+        Q.savIter = 0xffffffffu;
+        fasp_gpu_info ii;
+        std::memset(&ii, 0, sizeof(ii));
+        histOff = total;
+        histScale = rn;
+        if (cfg.alg == FASP_GPU_BICGSTAB)
+            e = bicgstab<float>(b32, e32, &ii, Q, S);
+        else if (cfg.alg == FASP_GPU_FGMRES)
+            e = gmres_right<float>(b32, e32, &ii, Q, S, true);
+        else if (cfg.leftPrecond)
+            e = gmres_left<float>(b32, e32, &ii, Q, S);
+        else
+            e = gmres_right<float>(b32, e32, &ii, Q, S, false);
+        histOff = 0;
+        histScale = 1.0;
+        if (e) return e;
+        total += ii.numIter;
+        if ((e = update_from32(c, n, rn, e32, x))) return e;
+        ++outer;
+        if (ii.numIter == 0) {
+            code = ii.code ? ii.code : kErrMaxIt;
+            if ((e = apply_residual(c, *A, b, (const double*)x, r64))) return e;
+            v_norm2(c, n, (const double*)r64, c.dslot + SL_T1);
+            rn = fetch(c.dslot + SL_T1);
+            outerHist.push_back({total, rn});
+            break;
+        }
+    }
+    info->numIter = total;
+    info->outerIter = outer;
+    info->code = code;
+    info->norm2 = rn;
+    v_norminf(c, n, (const double*)r64, c.dslot + SL_T2);
+    info->normInf = fetch(c.dslot + SL_T2);
+    for (auto& pt : outerHist) rec(pt.first, pt.second);
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
 // ---- dispatch ------------------------------------------------------------------------------
 
 int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
@@ -1159,16 +1409,30 @@ int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
         case FASP_GPU_CG:
             if (cfg.precision == FASP_GPU_MIXED)
                 e = cg_mixed(b, x, info);
+            else if (cfg.precision == FASP_GPU_MIXED_RELIABLE)
+                e = cg_reliable(b, x, info);
             else if (cg64)
                 e = cg_device(b, x, info);
             else
                 e = cg_generic(b, x, info);
             break;
-        case FASP_GPU_BICGSTAB: e = bicgstab(b, x, info); break;
-        case FASP_GPU_GMRES:
-            e = cfg.leftPrecond ? gmres_left(b, x, info) : gmres_right(b, x, info, false);
+        case FASP_GPU_BICGSTAB:
+            e = cfg.precision == FASP_GPU_MIXED ? refine(b, x, info)
+                                                : bicgstab<double>(b, x, info, cfg.prm, sp64());
             break;
-        case FASP_GPU_FGMRES: e = gmres_right(b, x, info, true); break;
+        case FASP_GPU_GMRES:
+            if (cfg.precision == FASP_GPU_MIXED)
+                e = refine(b, x, info);
+            else if (cfg.leftPrecond)
+                e = gmres_left<double>(b, x, info, cfg.prm, sp64());
+            else
+                e = gmres_right<double>(b, x, info, cfg.prm, sp64(), false);
+            break;
+        case FASP_GPU_FGMRES:
+            e = cfg.precision == FASP_GPU_MIXED
+                    ? refine(b, x, info)
+                    : gmres_right<double>(b, x, info, cfg.prm, sp64(), true);
+            break;
         case FASP_GPU_JACOBI: e = jacobi(b, x, info); break;
         case FASP_GPU_MG: e = mg(b, x, info); break;
         default: e = kErrSolverType;

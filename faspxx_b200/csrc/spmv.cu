@@ -50,20 +50,20 @@ __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restri
 }
 
 // r = b - A x, or r = b when the device flag says NormInf(x) < CLOSE_ZERO (MAT.cxx:459-462).
-template <int L>
-__global__ void __launch_bounds__(kBlock) k_residual(CSRView<double> A, const double* __restrict__ b,
-                                                     const double* __restrict__ x,
-                                                     double* __restrict__ r,
+template <typename T, int L>
+__global__ void __launch_bounds__(kBlock) k_residual(CSRView<T> A, const T* __restrict__ b,
+                                                     const T* __restrict__ x,
+                                                     T* __restrict__ r,
                                                      const double* __restrict__ xinf)
 {
     const bool shortcut = *xinf < kCloseZero;
     if (L == 1) {
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x) {
-            double s = 0.0;
+            T s = T(0);
             if (!shortcut) {
                 const uint32_t bb = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-                s = row_dot<double, false>(A, bb, e, [&](uint32_t j) { return x[j]; });
+                s = row_dot<T, false>(A, bb, e, [&](uint32_t j) { return x[j]; });
             }
             r[row] = b[row] - s;
         }
@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(CSRView<double> A, const do
     const size_t sub = (threadIdx.x & 31) / L;
     for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
         const size_t row = base + sub;
-        double s = 0.0;
+        T s = T(0);
         if (row < A.nrow && !shortcut) {
             const uint32_t bb = A.rowPtr[row], e = A.rowPtr[row + 1];
             for (uint32_t k = bb + lane; k < e; k += L) s = fma(A.val[k], x[A.colInd[k]], s);
@@ -146,11 +146,12 @@ int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y)
     return launch_spmv<float>(c, A.v32(), A.lanes, x, y);
 }
 
-int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
-               const double* xinf)
+template <typename T>
+static int residual_t(Ctx& c, const Mat& A, CSRView<T> V, const T* b, const T* x, T* r,
+                      const double* xinf)
 {
     if (A.nrow == 0) return kOk;
-    if (!A.val) return kErrMatData; // MAT::Residual reads values (MAT.cxx:466)
+    if (!V.val) return kErrMatData; // MAT::Residual reads values (MAT.cxx:466)
     if (!xinf) {
         double* slot = c.dslot + kSlotResidualXinf;
         int e = v_norminf(c, A.mcol, x, slot);
@@ -160,19 +161,32 @@ int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r
     const int need = spmv_grid(c, A.nrow, A.lanes);
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c.stream>>>(A.v64(), b, x, r, xinf);
+        kern<<<g, kBlock, 0, c.stream>>>(V, b, x, r, xinf);
     };
     ++c.launches;
     switch (A.lanes) {
-        case 1: go(k_residual<1>); break;
-        case 2: go(k_residual<2>); break;
-        case 4: go(k_residual<4>); break;
-        case 8: go(k_residual<8>); break;
-        case 16: go(k_residual<16>); break;
-        default: go(k_residual<32>); break;
+        case 1: go(k_residual<T, 1>); break;
+        case 2: go(k_residual<T, 2>); break;
+        case 4: go(k_residual<T, 4>); break;
+        case 8: go(k_residual<T, 8>); break;
+        case 16: go(k_residual<T, 16>); break;
+        default: go(k_residual<T, 32>); break;
     }
     FB_CUDA(cudaGetLastError());
     return kOk;
+}
+
+int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r,
+               const double* xinf)
+{
+    return residual_t<double>(c, A, A.v64(), b, x, r, xinf);
+}
+
+int m_residual(Ctx& c, const Mat& A, const float* b, const float* x, float* r,
+               const double* xinf)
+{
+    if (!A.val) return kErrMatData;
+    return residual_t<float>(c, A, A.v32(), b, x, r, xinf);
 }
 
 // ---- setup-time kernels ----------------------------------------------------------------

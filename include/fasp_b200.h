@@ -42,7 +42,9 @@ enum fasp_gpu_alg {
 /* Arithmetic of a solve. */
 enum fasp_gpu_precision {
     FASP_GPU_FP64 = 0,  /* every vector and reduction in FP64, the reference's arithmetic */
-    FASP_GPU_MIXED = 1  /* FP32 inner Krylov iterations inside FP64 iterative refinement */
+    FASP_GPU_MIXED = 1, /* FP32 inner Krylov iterations inside FP64 iterative refinement */
+    FASP_GPU_MIXED_RELIABLE = 2 /* CG only: one FP32 Krylov run with FP64 reliable updates of
+                                   x and r; the search direction survives each update */
 };
 
 /* Gram-Schmidt variant of the GMRES/FGMRES Arnoldi step. */
@@ -74,7 +76,9 @@ typedef struct {
     int             leftPrecond; /* GMRES::SetLeftPrecond (GMRES.cxx:28) */
     int             precision;   /* fasp_gpu_precision */
     int             orth;        /* fasp_gpu_orth */
-    double          innerRelTol; /* MIXED: relative tolerance of each FP32 inner solve */
+    double          innerRelTol; /* MIXED: relative tolerance of each FP32 inner solve;
+                                    MIXED_RELIABLE: an FP64 update each time the FP32
+                                    residual has fallen by this factor (0 or >= 1: 1e-2) */
     uint32_t        innerMaxIter;/* MIXED: iteration cap of each inner solve */
     uint32_t        maxOuter;    /* MIXED: refinement steps cap */
     int             useGraph;    /* 1: device-driven iterations captured in CUDA graphs */
