@@ -55,6 +55,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def profile_traffic(key: str):
+    """DRAM bytes (read + write) per launch of a kernel at this workload from the committed
+    ncu summaries (profiles/*.txt lines "dram_bytes_per_launch <key> <bytes>", key = kernel
+    and matrix form); null when no capture of the current kernel exists."""
+    prefix = key
+    try:
+        for fn in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
+            if not fn.endswith(".txt"):
+                continue
+            for line in open(os.path.join(ROOT, "profiles", fn)):
+                f = line.split()
+                if len(f) == 3 and f[0] == "dram_bytes_per_launch" and f[1] == prefix:
+                    return int(float(f[2]))
+    except OSError:
+        pass
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region."""
 
@@ -231,14 +249,16 @@ def run_ours(args):
         # 3 warm-up + 1 launch of cg_spmv and cg_update per engine: FP32 first, then FP64
         km = (C.c_double * 3)()
         for s in (mixed, fp64):
-            capi.check(lib.fasp_gpu_solver_kernel_times(s.h, 1, km), "kernel_times")
+            capi.check(lib.fasp_gpu_solver_kernel_times(s.h, 1, 0, km), "kernel_times")
             print(f"profile lanes={lanes} spmv {km[0]*1e3:.1f} us update {km[1]*1e3:.1f} us "
                   f"persistent iteration {km[2]*1e3:.1f} us")
         return 0
     db = sol.DVec.from_numpy(b)
     dx = sol.DVec(n)
+    l2flush = sol.DVec(32 << 20)  # 256 MB, written between solves to evict L2 (126 MB)
 
     def solve(s):
+        l2flush.Scale(0.0)
         dx.Scale(0.0)  # x0 = 0 on the device
         code = s.Solve(db, dx)
         if code != 0:
@@ -323,17 +343,27 @@ def run_ours(args):
     # kernel rooflines (each kernel alone, CUDA events on the library's stream)
     hbm, peak_kind = peaks()
     km = (C.c_double * 3)()
-    capi.check(lib.fasp_gpu_solver_kernel_times(mixed.h, 50, km), "kernel_times")
+    capi.check(lib.fasp_gpu_solver_kernel_times(mixed.h, 30, 1, km), "kernel_times")
     k64 = (C.c_double * 3)()
-    capi.check(lib.fasp_gpu_solver_kernel_times(fp64.h, 50, k64), "kernel_times")
+    capi.check(lib.fasp_gpu_solver_kernel_times(fp64.h, 30, 1, k64), "kernel_times")
     sp = C.c_double()
-    capi.check(lib.fasp_gpu_mat_time_apply(M.h, 50, 0, C.byref(sp)), "time_apply")
-    # algorithmic bytes per launch (compulsory traffic)
-    b_spmv32 = 8 * nnz + 4 * (n + 1) + 4 * n * 4   # vals+cols, rowPtr, read z,p_old write p,q
+    capi.check(lib.fasp_gpu_mat_time_apply(M.h, 30, 0, 1, C.byref(sp)), "time_apply")
+    rc_on, rc_classes, rc_entries = M.RowClassInfo()
+    sp_csr = C.c_double()
+    M.SetRowClass(False)
+    capi.check(lib.fasp_gpu_mat_time_apply(M.h, 30, 0, 1, C.byref(sp_csr)), "time_apply")
+    M.SetRowClass(rc_on)
+    # algorithmic bytes per launch (compulsory traffic); the matrix streams either the CSR
+    # arrays (values + column indices + row pointers) or one 2-byte class id per row (the
+    # class table, rc_entries entries, stays in L1/L2)
+    mat32 = 2 * n if rc_on else 8 * nnz + 4 * (n + 1)
+    mat64 = 2 * n if rc_on else 12 * nnz + 4 * (n + 1)
+    b_spmv32 = mat32 + 4 * n * 4                     # read z,p_old write p,q
     b_upd32 = 4 * n * 5 + 4 * n * 3                 # read p,x,r,q,dinv write x,r,z
-    b_spmv64 = 12 * nnz + 4 * (n + 1) + 8 * n * 4
+    b_spmv64 = mat64 + 8 * n * 4
     b_upd64 = 8 * n * 5 + 8 * n * 3
-    b_apply = 12 * nnz + 4 * (n + 1) + 16 * n
+    b_apply = mat64 + 16 * n
+    b_apply_csr = 12 * nnz + 4 * (n + 1) + 16 * n
     gbs = lambda byt, ms: byt / (ms * 1e-3) / 1e9  # noqa: E731
     if km[2] > 0:
         # the persistent kernel runs the whole FP32 inner solve: one iteration = both phases
@@ -347,12 +377,24 @@ def run_ours(args):
                     "bytes_per_launch": b_it32, "ms_per_launch": round(km[2], 5),
                     "unit_of_work": "one CG iteration (the kernel loops over iterations)"}
     else:
-        ach = gbs(b_spmv32, km[0])
-        roofline = {"kernel": "cg_spmv<float> (SpMV + p update + (Ap,p), FP32 inner CG)",
+        # the dominant kernel of the FP32 iteration: the larger of the two fused kernels
+        if km[0] >= km[1]:
+            name = ("cg_spmv<float> (SpMV + p update + (Ap,p), FP32 CG iteration"
+                    + (", row-class matrix form)" if rc_on else ", CSR)"))
+            byt, ms_k = b_spmv32, km[0]
+            key = "cg_spmv<float>/" + ("rowclass" if rc_on else "csr")
+        else:
+            name = ("cg_update<float,1> (x += alpha p, r -= alpha Ap, z = D^-1 r and five "
+                    "reductions, FP32 CG iteration)")
+            byt, ms_k = b_upd32, km[1]
+            key = "cg_update<float,1>"
+        ach = gbs(byt, ms_k)
+        roofline = {"kernel": name,
                     "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 3), "traffic": None,
-                    "peak_source": f"{peak_kind} hbm_gbs",
-                    "bytes_per_launch": b_spmv32, "ms_per_launch": round(km[0], 5)}
+                    "frac": round(ach / hbm, 3), "traffic": profile_traffic(key),
+                    "peak_source": f"{peak_kind} hbm_gbs (burst copy)",
+                    "bytes_per_launch": byt, "ms_per_launch": round(ms_k, 5),
+                    "timing": "CUDA events per launch after a 256 MB L2-evicting write"}
     kernels = {
         "cg_persistent_f32_iter": {"ms": round(km[2], 5),
                                    "gbs": round(gbs(b_spmv32 + b_upd32, km[2]), 1) if km[2] else None},
@@ -363,7 +405,11 @@ def run_ours(args):
         "cg_spmv_f64": {"ms": round(k64[0], 5), "gbs": round(gbs(b_spmv64, k64[0]), 1)},
         "cg_update_f64": {"ms": round(k64[1], 5), "gbs": round(gbs(b_upd64, k64[1]), 1)},
         "spmv_f64_apply": {"ms": round(sp.value, 5), "gbs": round(gbs(b_apply, sp.value), 1),
-                           "frac": round(gbs(b_apply, sp.value) / hbm, 3)},
+                           "frac": round(gbs(b_apply, sp.value) / hbm, 3),
+                           "form": "row classes" if rc_on else "CSR"},
+        "spmv_f64_apply_csr": {"ms": round(sp_csr.value, 5),
+                               "gbs": round(gbs(b_apply_csr, sp_csr.value), 1),
+                               "frac": round(gbs(b_apply_csr, sp_csr.value) / hbm, 3)},
         # the whole mixed solve as FP32 iterations: algorithmic bytes of its iterations over
         # the solve's device time (refreshes, reductions and launch gaps included)
         "mixed_solve_effective": {
@@ -395,7 +441,8 @@ def run_ours(args):
             "config": {"workload": f"3D Poisson 7-point {args.size}^3 (n={n}, nnz={nnz}), "
                                    f"Jacobi-PCG, FP64 rtol 1e-8, x0=0, b=A x*, x*~U[0,1)",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (FP32 matrix 125 MB + vectors)",
+                       "l2": "L2 flushed between timed solves (256 MB write); kernel "
+                             "rooflines timed per launch after the same flush",
                        "spmv_lanes_per_row": lanes,
                        "reliable_update_delta": args.delta,
                        "precision_mode": "MIXED_RELIABLE"},
@@ -410,7 +457,9 @@ def run_ours(args):
             "accuracy": {"mixed_rel_residual": acc_mixed[0], "mixed_err_vs_fp64_1e-13": acc_mixed[1],
                          "fp64_rel_residual": acc_fp64[0], "fp64_err_vs_fp64_1e-13": acc_fp64[1],
                          "e2e_err_vs_fp64_1e-13": e2e_err},
-            "spmv_gbs": kernels["spmv_f64_apply"]["gbs"],
+            "spmv_gbs": kernels["spmv_f64_apply_csr"]["gbs"],
+            "matrix_form": {"row_classes": rc_on, "classes": rc_classes,
+                            "table_entries": rc_entries},
             "roofline": roofline, "kernels": kernels,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 8 * n},
@@ -473,7 +522,7 @@ def run_batch(args):
     line = {"metric": "Batched Jacobi-PCG, 4096 uneven systems x 4 RHS to rtol 1e-8",
             "value": round(res["mixed"][0], 3), "unit": "ms", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-            "dtype": "f32 Krylov iterations / f64 reliable updates", "data": "synthetic",
+            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
             "config": {"workload": f"{count} systems, 2D 5-point m~U{{16..128}} + sigma I, "
                                    f"sigma~U[0,1], 4 RHS b~N(0,1), rows {B.N}, nnz {B.A.nnz}",
                        "shape": list(shape64)},
@@ -484,6 +533,218 @@ def run_batch(args):
             "loop_sample": f"{len(sample)} systems x 4 RHS timed, scaled by rows",
             "speedup_vs_loop": {"fp64": round(loop_full / res["fp64"][0], 1),
                                 "mixed": round(loop_full / res["mixed"][0], 1)}}
+    print(json.dumps(line))
+    return 0
+
+
+def _time_solve(s, db, dx, reps, warm=2, flush=None):
+    """Mean device time (ms) of reps solves from x0 = 0 (after warm untimed ones)."""
+    ts = []
+    for i in range(warm + reps):
+        if flush is not None:
+            flush.Scale(0.0)
+        dx.Scale(0.0)
+        code = s.Solve(db, dx)
+        if i >= warm:
+            ts.append(s.LastTimeMs())
+    return statistics.mean(ts), code
+
+
+def run_krylov(args):
+    """Nonsymmetric 3D convection-diffusion -Laplace(u) + beta.grad(u) on 96^3 (n = 884,736,
+    7-point, first-order upwind, direction (1, 0.5, 0.25), cell Peclet 0.1 and 10), b = A x*
+    with x* ~ U[-1,1) (seed 42), x0 = 0, rtol 1e-8, weighted Jacobi (omega = 2/3, one sweep):
+    BiCGStab, GMRES(30) and FGMRES(30) in FP64 and with FP32 inner iterations inside FP64
+    refinement (FP64 residual, update and Hessenberg/Givens least squares)."""
+    from faspxx_b200 import capi, problems as P, sol
+    capi.init(0)
+    N = args.size if args.size != N_GRID else 96
+    flush = sol.DVec(32 << 20)
+    rows, total_mixed = [], 0.0
+    for pe in (0.1, 10.0):
+        A = P.convdiff3d(N, pe)
+        xs = P.seeded_uniform(A.nrow, 42, -1.0, 1.0)
+        b = A.matvec(xs)
+        M = sol.MAT(A)
+        M.Autotune()
+        db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
+        for alg in ("bicgstab", "gmres", "fgmres"):
+            res = {}
+            for prec in ("fp64", "mixed"):
+                kw = dict(maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
+                          pcdWeight=2.0 / 3.0, pcdIter=1)
+                if alg != "bicgstab":
+                    kw.update(restart=30, maxRestart=30, minRestart=30)
+                s = sol.configure(alg, **kw)
+                if prec == "mixed":
+                    s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
+                s.Setup(M)
+                ms, code = _time_solve(s, db, dx, args.steps, flush=flush)
+                x = dx.numpy()
+                res[prec] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
+                             "outer": s.info.outerIter if prec == "mixed" else None,
+                             "rel_residual": float(np.linalg.norm(b - A.matvec(x)) /
+                                                   np.linalg.norm(b)),
+                             "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+            total_mixed += res["mixed"]["ms"]
+            rows.append({"peclet": pe, "solver": alg, **{k: v for k, v in res.items()},
+                         "mixed_over_fp64": round(res["mixed"]["ms"] / res["fp64"]["ms"], 3)})
+    line = {"metric": "Time to rtol 1e-8, 96^3 convection-diffusion, BiCGStab / GMRES(30) / "
+                      "FGMRES(30): FP32-inner refinement vs FP64",
+            "value": round(total_mixed, 3), "unit": "ms (sum of the six mixed solves)",
+            "n_gpus": 1, "steps": args.steps, "warmup": 2, "higher_is_better": False,
+            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"{N}^3 upwind convection-diffusion, Pe 0.1 and 10, "
+                                   "weighted Jacobi 2/3, x0=0, b=A x*, x*~U[-1,1)",
+                       "l2": "L2 flushed between timed solves"},
+            "results": rows}
+    print(json.dumps(line))
+    return 0
+
+
+def run_adjoint(args):
+    """Differentiable solve of -div(kappa grad u) = b on 64^3 (kappa = exp(N(0,1)) per cell,
+    harmonic face averages; b ~ N(0,1)); loss 0.5 ||x - x_t||^2 (x_t ~ N(0,1)). Forward CG to
+    rtol 1e-10 (Jacobi), backward the adjoint CG on the exact transpose + the sampled outer
+    product. FP64 and FP32-iteration (reliable-update) variants; gradients checked by central
+    differences (eps 1e-6) along 32 seeded random directions and against the FP64 gradient."""
+    from faspxx_b200 import capi, problems as P, sol
+    capi.init(0)
+    lib = capi.lib
+    N = args.size if args.size != N_GRID else 64
+    rng = np.random.default_rng(42)
+    kappa = np.exp(rng.standard_normal(N ** 3))
+    A = P.vardiff3d(N, kappa)
+    n, nnz = A.nrow, A.nnz
+    b = rng.standard_normal(n)
+    xt = rng.standard_normal(n)
+    db, dx, dg, dlam = sol.DVec.from_numpy(b), sol.DVec(n), sol.DVec(n), sol.DVec(n)
+    dA = sol.DVec(nnz)
+
+    def make(M, prec):
+        s = sol.configure("cg", maxIter=20000, relTol=1e-10, absTol=0.0, pcd="jacobi",
+                          pcdWeight=1.0, pcdIter=1)
+        if prec != capi.FP64:
+            s.SetPrecision(prec, innerRelTol=1e-2)
+        s.Setup(M)
+        return s
+
+    out = {}
+    M = sol.MAT(A)
+    for name, prec in (("fp64", capi.FP64), ("fp32_iter", capi.MIXED_RELIABLE)):
+        s = make(M, prec)
+        fwd, bwd, outer_ms = [], [], []
+        info = capi.Info()
+        for i in range(2 + args.steps):
+            dx.Scale(0.0)
+            s.Solve(db, dx)
+            f = s.LastTimeMs()
+            x = dx.numpy()
+            dg.set(x - xt)
+            lib.fasp_gpu_synchronize()
+            capi.check(lib.fasp_gpu_solver_solve_adjoint(s.h, dg.ptr, dlam.ptr, C.byref(info)),
+                       "adjoint")
+            bt = s.LastTimeMs()
+            lib.fasp_gpu_synchronize()
+            t0 = time.perf_counter()
+            capi.check(lib.fasp_gpu_mat_sampled_outer(M.h, dlam.ptr, dx.ptr, -1.0, dA.ptr),
+                       "sampled_outer")
+            lib.fasp_gpu_synchronize()
+            t1 = time.perf_counter()
+            if i >= 2:
+                fwd.append(f)
+                bwd.append(bt)
+                outer_ms.append((t1 - t0) * 1e3)
+        out[name] = {"forward_ms": round(statistics.mean(fwd), 3),
+                     "adjoint_ms": round(statistics.mean(bwd), 3),
+                     "outer_ms_wall": round(statistics.mean(outer_ms), 4),
+                     "iters_forward": s.GetIterations(), "adjoint_iters": info.numIter,
+                     "grad_b": dlam.numpy(), "grad_A": dA.numpy(), "x": dx.numpy()}
+    g64b, g64A = out["fp64"]["grad_b"], out["fp64"]["grad_A"]
+    rel = lambda u, v: float(np.linalg.norm(u - v) / np.linalg.norm(v))  # noqa: E731
+    # central differences of the FP64 loss along 32 random (b, A-values) directions
+    eps = 1e-6
+    s64 = make(M, capi.FP64)
+    x0 = out["fp64"]["x"]
+
+    def loss(vals, bb):
+        Mp = sol.MAT(P.CSRMatrix(n, n, A.rowPtr, A.colInd, vals))
+        sp = make(Mp, capi.FP64)
+        dbb = sol.DVec.from_numpy(bb)
+        dxx = sol.DVec(n)
+        sp.Solve(dbb, dxx)
+        xx = dxx.numpy()
+        return 0.5 * float(np.dot(xx - xt, xx - xt))
+
+    errs = []
+    drng = np.random.default_rng(7)
+    for _ in range(args.fd_dirs):
+        dbdir = drng.standard_normal(n)
+        dAdir = drng.standard_normal(nnz) * np.abs(A.values)
+        lp = loss(A.values + eps * dAdir, b + eps * dbdir)
+        lm = loss(A.values - eps * dAdir, b - eps * dbdir)
+        fd = (lp - lm) / (2 * eps)
+        an = float(np.dot(g64b, dbdir) + np.dot(g64A, dAdir))
+        errs.append(abs(fd - an) / max(abs(an), 1e-300))
+    del s64, x0
+    line = {"metric": "Differentiable 64^3 variable-coefficient solve: forward + adjoint time, "
+                      "gradient agreement",
+            "value": round(out["fp64"]["forward_ms"] + out["fp64"]["adjoint_ms"], 3),
+            "unit": "ms (FP64 forward + adjoint)", "n_gpus": 1, "steps": args.steps,
+            "warmup": 2, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{N}^3 -div(kappa grad u), kappa=exp(N(0,1)), n={n}, "
+                                   f"nnz={nnz}, CG rtol 1e-10, Jacobi"},
+            "fp64": {k: v for k, v in out["fp64"].items() if not k.startswith(("grad", "x"))},
+            "fp32_iter": {k: v for k, v in out["fp32_iter"].items()
+                          if not k.startswith(("grad", "x"))},
+            "fp32_iter_grad_rel_err_vs_fp64": {"b": rel(out["fp32_iter"]["grad_b"], g64b),
+                                                "A": rel(out["fp32_iter"]["grad_A"], g64A)},
+            "central_difference": {"directions": args.fd_dirs, "eps": eps,
+                                   "max_rel_err": max(errs) if errs else None,
+                                   "median_rel_err": statistics.median(errs) if errs else None}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_pcg2d(args):
+    """2D 5-point Poisson on a 256 x 256 grid (n = 65,536, nnz = 326,656), x* ~ U[0,1) (seed
+    42), b = A x*, x0 = 0, Jacobi-PCG to rtol 1e-8, max 2000 iterations: the reference's PCG
+    example at its own size, device-driven FP64 and FP32-iteration (reliable-update) CG."""
+    from faspxx_b200 import capi, problems as P, sol
+    capi.init(0)
+    A = P.poisson2d(256)
+    xs = P.seeded_uniform(A.nrow, 42)
+    b = A.matvec(xs)
+    M = sol.MAT(A)
+    M.Autotune()
+    db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
+    flush = sol.DVec(32 << 20)
+    res = {}
+    for name, prec in (("fp64", capi.FP64), ("mixed", capi.MIXED_RELIABLE)):
+        s = sol.configure("cg", maxIter=2000, relTol=1e-8, absTol=0.0, pcd="jacobi",
+                          pcdWeight=1.0, pcdIter=1)
+        if prec != capi.FP64:
+            s.SetPrecision(prec, innerRelTol=1e-2)
+        s.Setup(M)
+        ms, code = _time_solve(s, db, dx, args.steps, flush=flush)
+        x = dx.numpy()
+        res[name] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
+                     "rel_residual": float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)),
+                     "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        kind = "ref" if os.path.exists(O.REF_SO) else "port"
+        per_iter, _ = reference_sample(A, b, 200, kind)
+        cpu = {"value": round(per_iter * res["fp64"]["iters"], 2), "unit": "ms", "cores": 1,
+               "kind": "reference" if kind == "ref" else "port",
+               "sample": "200 Jacobi-PCG iterations, scaled by the FP64 iteration count"}
+    line = {"metric": "Time to rtol 1e-8, 2D Poisson 256x256 Jacobi-PCG",
+            "value": res["fp64"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": 2, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D 5-point 256x256 (n=65536, nnz=326656), Jacobi-PCG, "
+                                   "x0=0, b=A x*, x*~U[0,1)"},
+            "results": res, "cpu_baseline": cpu}
     print(json.dumps(line))
     return 0
 
@@ -504,7 +765,9 @@ def main():
     ap.add_argument("--lanes", type=int, default=0, help="force SpMV lanes per row")
     ap.add_argument("--profile", action="store_true",
                     help="only set up and launch each fused CG kernel 4 times (for ncu)")
-    ap.add_argument("--workload", choices=["poisson128", "batch"], default="poisson128")
+    ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",
+                                           "pcg2d256"], default="poisson128")
+    ap.add_argument("--fd-dirs", type=int, default=32)
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-sample", type=int, default=256)
     args = ap.parse_args()
@@ -513,6 +776,12 @@ def main():
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "krylov96":
+        return run_krylov(args)
+    if args.workload == "adjoint64":
+        return run_adjoint(args)
+    if args.workload == "pcg2d256":
+        return run_pcg2d(args)
     return run_ours(args)
 
 

@@ -37,7 +37,8 @@ class Config(C.Structure):
                 ("mgSmoothPrm", Params), ("mgCoarsePrm", Params),
                 ("leftPrecond", C.c_int), ("precision", C.c_int), ("orth", C.c_int),
                 ("innerRelTol", C.c_double), ("innerMaxIter", C.c_uint32),
-                ("maxOuter", C.c_uint32), ("useGraph", C.c_int), ("persistent", C.c_int)]
+                ("maxOuter", C.c_uint32), ("useGraph", C.c_int), ("persistent", C.c_int),
+                ("overlapLaunch", C.c_int)]
 
 
 class Info(C.Structure):
@@ -72,7 +73,9 @@ SIGNATURES = {
     "fasp_gpu_mat_diag": (_i, [_vp, _vp]),
     "fasp_gpu_mat_autotune": (_i, [_vp, _P(_i)]),
     "fasp_gpu_mat_set_lanes": (_i, [_vp, _i]),
-    "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _P(_d)]),
+    "fasp_gpu_mat_set_rowclass": (_i, [_vp, _i]),
+    "fasp_gpu_mat_rowclass_info": (_i, [_vp, _P(_i), _P(_u32), _P(_u32)]),
+    "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _i, _P(_d)]),
     "fasp_gpu_mat_sampled_outer": (_i, [_vp, _vp, _vp, _d, _vp]),
     "fasp_gpu_vec_dot": (_i, [_u32, _vp, _vp, _P(_d)]),
     "fasp_gpu_vec_norm2": (_i, [_u32, _vp, _P(_d)]),
@@ -91,7 +94,7 @@ SIGNATURES = {
     "fasp_gpu_solver_clean": (_i, [_vp]),
     "fasp_gpu_solver_destroy": (_i, [_vp]),
     "fasp_gpu_solver_last_time": (_i, [_vp, _P(_d)]),
-    "fasp_gpu_solver_kernel_times": (_i, [_vp, _u32, _P(_d)]),
+    "fasp_gpu_solver_kernel_times": (_i, [_vp, _u32, _i, _P(_d)]),
     "fasp_gpu_solver_solve_adjoint": (_i, [_vp, _vp, _vp, _P(Info)]),
     "fasp_gpu_batch_create": (_i, [_u32, _vp, _u32, _vp, _vp, _vp, _u32, _P(_vp)]),
     "fasp_gpu_batch_set_shape": (_i, [_vp, _i, _i]),

@@ -147,6 +147,7 @@ void fasp_gpu_default_config(fasp_gpu_config* cfg, int alg)
     cfg->maxOuter = 50;
     cfg->useGraph = 1;
     cfg->persistent = 0;
+    cfg->overlapLaunch = 1;
 }
 
 // ---- memory ---------------------------------------------------------------------------
@@ -322,7 +323,23 @@ int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes)
     return kOk;
 }
 
-int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, double* ms)
+int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int on)
+{
+    if (!A) return kErrInputPar;
+    A->M.rcOn = on != 0 && A->M.rcCls != nullptr;
+    return kOk;
+}
+
+int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* on, uint32_t* classes, uint32_t* entries)
+{
+    if (!A) return kErrInputPar;
+    if (on) *on = A->M.rcOn ? 1 : 0;
+    if (classes) *classes = A->M.rcClasses;
+    if (entries) *entries = A->M.rcEntries;
+    return kOk;
+}
+
+int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2, double* ms)
 {
     if (!A || !ms || reps == 0) return kErrInputPar;
     Ctx& c = A->c;
@@ -342,23 +359,12 @@ int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, double* ms)
                     : m_spmv(c, M, (const double*)x, (double*)y);
     };
     for (int w = 0; w < 3; ++w)
-        if ((e = one())) return e;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    cudaEventRecord(t0, c.stream);
-    for (uint32_t i = 0; i < reps; ++i) one();
-    cudaEventRecord(t1, c.stream);
-    cudaEventSynchronize(t1);
-    float t = 0.f;
-    cudaEventElapsedTime(&t, t0, t1);
-    *ms = t / reps;
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+        if ((e = one())) break;
+    if (!e) e = time_launches(c, reps, flushL2, one, ms);
     cudaFree(x);
     cudaFree(y);
     FB_CUDA(cudaGetLastError());
-    return kOk;
+    return e;
 }
 
 int fasp_gpu_mat_sampled_outer(fasp_gpu_mat A, const double* lam, const double* x,
@@ -513,12 +519,12 @@ int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms)
     return kOk;
 }
 
-int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, double* ms)
+int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, int flushL2, double* ms)
 {
     if (!s || !ms || reps == 0) return kErrInputPar;
     SolverImpl& S = s->s;
-    if (S.cg32) return S.cg32->time_kernels(reps, ms);
-    if (S.cg64) return S.cg64->time_kernels(reps, ms);
+    if (S.cg32) return S.cg32->time_kernels(reps, flushL2, ms);
+    if (S.cg64) return S.cg64->time_kernels(reps, flushL2, ms);
     return kErrSolverType;
 }
 
@@ -548,7 +554,9 @@ int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* la
             return e;
         }
     }
-    return S.adj->solve(g, lam, info);
+    const int e = S.adj->solve(g, lam, info);
+    S.lastMs = S.adj->lastMs; // last_time reports the most recent solve, adjoint included
+    return e;
 }
 
 } // extern "C"

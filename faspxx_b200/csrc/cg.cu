@@ -12,6 +12,7 @@
 // set status = kEsc and are finished by the host, which then relaunches cg_resume.
 #include <cstring>
 #include <type_traits>
+#include <utility>
 
 #include "cg.cuh"
 
@@ -197,7 +198,8 @@ __device__ __forceinline__ void cg_refresh_residual(const CSRView<float>& A, flo
                                                     float* z32, const float* dinv32,
                                                     CGCtl* c, Scratch s)
 {
-    const CSRView<double> A64{A.nrow, A.mcol, A.nnz, A.rowPtr, A.colInd, c->rval};
+    const CSRView<double> A64{A.nrow, A.mcol, A.nnz, A.rowPtr, A.colInd, c->rval,
+                              A.cls, A.coff, A.cdelta, c->rcval};
     const double* b = c->rb;
     const double* x64 = c->rx;
     double* r64 = c->rr;
@@ -206,8 +208,7 @@ __device__ __forceinline__ void cg_refresh_residual(const CSRView<float>& A, flo
     float rr = 0.f, zr = 0.f;
     GRID_STRIDE(row, A.nrow)
     {
-        const uint32_t bb = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-        const double ax = row_dot<double, false>(A64, bb, e, [&](uint32_t j) { return x64[j]; });
+        const double ax = row_apply<double, false>(A64, row, [&](uint32_t j) { return x64[j]; });
         const double ri = b[row] - ax;
         r64[row] = ri;
         const float r32i = (float)(ri * inv);
@@ -246,6 +247,8 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
                                                   CGCtl* c, Scratch s)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
             if (c->status == kRefresh) cg_refresh_fold(A.nrow, x, c);
@@ -259,8 +262,7 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     if (L == 1) { // thread per row
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x) {
-            const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-            const T sum = row_dot<T, false>(A, b, e, [&](uint32_t j) {
+            const T sum = row_apply<T, false>(A, row, [&](uint32_t j) {
                 return mode ? fma(beta, pOld[j], z[j]) : z[j];
             });
             const T pi = mode ? fma(beta, pOld[row], z[row]) : z[row];
@@ -309,6 +311,8 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
                                                     const T* __restrict__ dinv, CGCtl* c,
                                                     Scratch s, CSRView<T> A)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
             if (c->status == kRefresh) cg_refresh_residual<JAC>(A, r, z, dinv, c, s);
@@ -333,14 +337,41 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
     const size_t nv = n / W;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = tid; i < nv; i += stride) {
+    // FP32: two grid-stride steps per pass, all ten 16-byte loads issued before any use,
+    // doubling the bytes in flight per thread (the kernel is latency-bound at one step; the
+    // FP64 variant would spill under the 64-register cap).
+    constexpr bool kTwo = std::is_same<T, float>::value;
+    size_t i = tid;
+    for (; kTwo && i + stride < nv; i += 2 * stride) {
+        T pa[2][W], xa[2][W], ra[2][W], qa[2][W], da[2][W];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const size_t k = i + h * stride;
+            *(V*)pa[h] = ((const V*)p)[k];
+            *(V*)xa[h] = ((const V*)x)[k];
+            *(V*)ra[h] = ((const V*)r)[k];
+            *(V*)qa[h] = ((const V*)q)[k];
+            if (JAC) *(V*)da[h] = ((const V*)dinv)[k];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const size_t k = i + h * stride;
+            // z overwrites q's registers: q is dead once r is updated
+#pragma unroll
+            for (int u = 0; u < W; ++u)
+                one(pa[h][u], xa[h][u], ra[h][u], qa[h][u], JAC ? da[h][u] : T(0), qa[h][u]);
+            ((V*)x)[k] = *(V*)xa[h];
+            ((V*)r)[k] = *(V*)ra[h];
+            if (JAC) ((V*)z)[k] = *(V*)qa[h];
+        }
+    }
+    for (; i < nv; i += stride) {
         T pa[W], xa[W], ra[W], qa[W], da[W];
         *(V*)pa = ((const V*)p)[i];
         *(V*)xa = ((const V*)x)[i];
         *(V*)ra = ((const V*)r)[i];
         *(V*)qa = ((const V*)q)[i];
         if (JAC) *(V*)da = ((const V*)dinv)[i];
-        // z overwrites q's registers: q is dead once r is updated
 #pragma unroll
         for (int u = 0; u < W; ++u) one(pa[u], xa[u], ra[u], qa[u], JAC ? da[u] : T(0), qa[u]);
         ((V*)x)[i] = *(V*)xa;
@@ -536,8 +567,7 @@ cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __res
             T* pNew = par ? P0 : P1;
             T acc = T(0);
             for (size_t row = tid; row < n; row += stride) {
-                const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-                const T sum = row_dot<T, false>(A, b, e, [&](uint32_t j) {
+                const T sum = row_apply<T, false>(A, row, [&](uint32_t j) {
                     return mode ? fma(beta, __ldcg(pOld + j), __ldcg(zz + j)) : __ldcg(zz + j);
                 });
                 const T pi = mode ? fma(beta, __ldcg(pOld + row), __ldcg(zz + row))
@@ -615,6 +645,25 @@ CSRView<double> view_of<double>(const Mat& A) { return A.v64(); }
 template <>
 CSRView<float> view_of<float>(const Mat& A) { return A.v32(); }
 
+// Launch with programmatic stream serialization when pdl is set (captured into the graph as
+// a programmatic edge), so the kernel's launch overlaps its predecessor's reduction tail.
+template <typename... P, typename... A>
+static void launch_overlapped(void (*kern)(P...), int grid, cudaStream_t s, bool pdl,
+                              A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 // The two fused kernels, each on one resident wave (grid from the occupancy limit).
 template <typename T>
 void CGEngine<T>::launch_spmv_kernel()
@@ -624,7 +673,7 @@ void CGEngine<T>::launch_spmv_kernel()
     const T* zz = jacobi ? z : r;
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c->stream>>>(V, zz, P0, P1, q, x, ctl, c->red);
+        launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red);
     };
     switch (A->lanes) {
         case 1: go(cg_spmv<T, 1>); break;
@@ -643,7 +692,7 @@ void CGEngine<T>::launch_update_kernel()
     const CSRView<T> V = view_of<T>(*A);
     auto go = [&](auto kern, T* zz) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c->stream>>>(n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
+        launch_overlapped(kern, g, c->stream, pdl, n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
     };
     if (jacobi)
         go(cg_update<T, 1>, z);
@@ -864,7 +913,7 @@ int CGEngine<T>::run(unsigned* launches)
 // Times each fused kernel alone: reps launches of cg_spmv, then reps of cg_update, each
 // bracketed by events on the engine's stream, with the control block in bench mode.
 template <typename T>
-int CGEngine<T>::time_kernels(unsigned reps, double* ms)
+int CGEngine<T>::time_kernels(unsigned reps, int flushL2, double* ms)
 {
     std::memset(hctl, 0, sizeof(CGCtl));
     hctl->status = kRun;
@@ -875,42 +924,31 @@ int CGEngine<T>::time_kernels(unsigned reps, double* ms)
     hctl->histScale = 1.0;
     int e = push_ctl();
     if (e) return e;
-    cudaEvent_t ev[3];
-    for (auto& x0 : ev) FB_CUDA(cudaEventCreate(&x0));
-    auto spmv = [&]() { launch_spmv_kernel(); };
-    auto update = [&]() { launch_update_kernel(); };
+    auto spmv = [&]() {
+        launch_spmv_kernel();
+        return (int)kOk;
+    };
+    auto update = [&]() {
+        launch_update_kernel();
+        return (int)kOk;
+    };
     for (int w = 0; w < 3; ++w) {
         spmv();
         update();
     }
-    cudaEventRecord(ev[0], c->stream);
-    for (unsigned i = 0; i < reps; ++i) spmv();
-    cudaEventRecord(ev[1], c->stream);
-    for (unsigned i = 0; i < reps; ++i) update();
-    cudaEventRecord(ev[2], c->stream);
-    FB_CUDA(cudaEventSynchronize(ev[2]));
-    float a = 0.f, b = 0.f;
-    cudaEventElapsedTime(&a, ev[0], ev[1]);
-    cudaEventElapsedTime(&b, ev[1], ev[2]);
-    ms[0] = a / reps;
-    ms[1] = b / reps;
+    if ((e = time_launches(*c, reps, flushL2, spmv, &ms[0])) ||
+        (e = time_launches(*c, reps, flushL2, update, &ms[1])))
+        return e;
     ms[2] = 0.0;
     if (persistent) {
         // the persistent kernel, reps iterations in one launch (bench mode: no control flow)
-        e = push_ctl();
-        if (e) return e;
+        if ((e = push_ctl())) return e;
         run_persistent(2);
-        push_ctl();
-        cudaEventRecord(ev[0], c->stream);
-        e = run_persistent(reps);
-        cudaEventRecord(ev[1], c->stream);
-        cudaEventSynchronize(ev[1]);
-        float p = 0.f;
-        cudaEventElapsedTime(&p, ev[0], ev[1]);
-        ms[2] = p / reps;
-        if (e) return e;
+        if ((e = push_ctl())) return e;
+        auto all = [&]() { return run_persistent(reps); };
+        if ((e = time_launches(*c, 1, flushL2, all, &ms[2]))) return e;
+        ms[2] /= reps;
     }
-    for (auto& x0 : ev) cudaEventDestroy(x0);
     hctl->bench = 0;
     hctl->status = kDone;
     e = push_ctl();

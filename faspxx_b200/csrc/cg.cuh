@@ -44,6 +44,7 @@ struct CGCtl {
     double*  rx;        // x (FP64)
     double*  rr;        // r = b - A x (FP64), written by each refresh
     const double* rval; // FP64 values of the matrix (same structure as the FP32 view)
+    const double* rcval;// FP64 values of its row-class table (when the FP32 view uses one)
     double   red[5];    // rr, zr, xx, max|x|, pp saved at an escalation
     double*  hist;
     unsigned histCap;
@@ -68,6 +69,7 @@ struct CGEngine {
     int        itersPerGraph = 16;
     bool       useGraph = true;
     bool       capturing = false;
+    bool       pdl = true;      // programmatic dependent launch of the iteration kernels
     uint32_t   n = 0;
     // persistent engine: one cooperative launch runs the iterations
     bool       wantPersistent = true; // set before init
@@ -86,7 +88,7 @@ struct CGEngine {
     void launch_spmv_kernel();
     void launch_update_kernel();
     int  launch_resume();
-    int  time_kernels(unsigned reps, double* ms);
+    int  time_kernels(unsigned reps, int flushL2, double* ms);
     int  push_ctl();   // hctl -> ctl
     int  pull_ctl();   // ctl -> hctl (synchronous)
     T*   cur_p() const { return hctl->par ? P1 : P0; }

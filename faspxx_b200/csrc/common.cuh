@@ -111,6 +111,13 @@ struct CSRView {
     const uint32_t* rowPtr;
     const uint32_t* colInd;
     const T*        val;   // nullptr: pattern only (every stored entry is 1)
+    // Row classes (optional, thread-per-row kernels): rows with identical column offsets
+    // (col - row) and values share one table entry; cls[row] picks it. Entries of class k
+    // are [coff[k], coff[k+1]) in cdelta / cval, in the row's CSR order.
+    const uint16_t* cls;
+    const uint32_t* coff;
+    const int32_t*  cdelta;
+    const T*        cval;
 };
 
 // The matrix is streamed once per SpMV: evict-first loads keep it from displacing the
@@ -142,6 +149,48 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, uint32_t b, uint32_t e
             if (k + u < e) s = fma(v[u], xv(c[u]), s);
     }
     return s;
+}
+
+// Row `row` of A times the gathered vector, through the row-class table when A has one
+// (2 bytes streamed per row instead of the row's column indices and values), else through
+// the CSR arrays. Both accumulate the entries in CSR order with one FMA each, so the two
+// storage forms give bit-identical results.
+template <typename T, bool PAT, typename XV>
+__device__ __forceinline__ T row_apply(const CSRView<T>& A, size_t row, XV xv)
+{
+    if (!PAT && A.cls) {
+        const uint32_t k = __ldcs(A.cls + row);
+        const uint32_t b = __ldg(A.coff + k), e = __ldg(A.coff + k + 1);
+        T s = T(0);
+#pragma unroll 2
+        for (uint32_t i = b; i < e; i += 4) {
+            T v[4], xs[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool in = i + u < e;
+                const long long d = in ? (long long)__ldg(A.cdelta + i + u) : 0;
+                v[u] = in ? __ldg(A.cval + i + u) : T(0);
+                xs[u] = in ? xv((uint32_t)((long long)row + d)) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (i + u < e) s = fma(v[u], xs[u], s);
+        }
+        return s;
+    }
+    const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
+    return row_dot<T, PAT>(A, b, e, xv);
+}
+
+// Programmatic dependent launch: a kernel launched with the programmatic-serialization
+// attribute may start while its predecessor drains; pdl_wait() blocks until the predecessor
+// has completed and its writes are visible (a no-op for an ordinary launch), pdl_release()
+// lets the successor be scheduled. Every kernel that uses them calls pdl_wait() before its
+// first global-memory access.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }

@@ -81,6 +81,43 @@ struct Ctx {
 // Grid-stride kernels launched with min(work, this) never run a partial second wave.
 int resident_grid(const Ctx& c, const void* fn, int block);
 
+// Average device time (ms) of one call of `launch` over reps calls. flushL2 = 0: the calls
+// run back to back between two events. flushL2 = 1: each call is timed alone with events
+// after a 256 MB write that evicts L2 (126 MB), so its inputs come from HBM.
+template <typename F>
+int time_launches(Ctx& c, unsigned reps, int flushL2, F&& launch, double* ms)
+{
+    void* flush = nullptr;
+    const size_t fbytes = (size_t)256 << 20;
+    if (flushL2 && cudaMalloc(&flush, fbytes) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrAlloc;
+    }
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    double tot = 0.0;
+    int e = kOk;
+    for (unsigned i = 0; i < (flushL2 ? reps : 1u); ++i) {
+        if (flushL2) cudaMemsetAsync(flush, (int)(i & 0xff), fbytes, c.stream);
+        cudaEventRecord(t0, c.stream);
+        for (unsigned k = 0; k < (flushL2 ? 1u : reps); ++k)
+            if ((e = launch())) break;
+        cudaEventRecord(t1, c.stream);
+        cudaEventSynchronize(t1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, t0, t1);
+        tot += t;
+        if (e) break;
+    }
+    *ms = tot / reps;
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaFree(flush);
+    if (cudaGetLastError() != cudaSuccess && !e) e = kErrCuda;
+    return e;
+}
+
 // CSRx matrix resident in device memory.
 struct Mat {
     uint32_t  nrow = 0, mcol = 0, nnz = 0;
@@ -94,8 +131,26 @@ struct Mat {
     uint32_t  maxRowLen = 0;
     double    meanRowLen = 0;
     int       dev = 0;
-    CSRView<double> v64() const { return CSRView<double>{nrow, mcol, nnz, rowPtr, colInd, val}; }
-    CSRView<float>  v32() const { return CSRView<float>{nrow, mcol, nnz, rowPtr, colInd, val32}; }
+    // row-class form (built at upload when the rows fall into few classes; see CSRView)
+    uint16_t* rcCls = nullptr;
+    uint32_t* rcOff = nullptr;
+    int32_t*  rcDelta = nullptr;
+    double*   rcVal = nullptr;
+    float*    rcVal32 = nullptr;
+    uint32_t  rcClasses = 0, rcEntries = 0;
+    bool      rcOn = false;      // used by the thread-per-row kernels when built and enabled
+    CSRView<double> v64() const
+    {
+        const bool rc = rcOn && rcCls && val;
+        return CSRView<double>{nrow, mcol, nnz, rowPtr, colInd, val,
+                               rc ? rcCls : nullptr, rcOff, rcDelta, rcVal};
+    }
+    CSRView<float> v32() const
+    {
+        const bool rc = rcOn && rcCls && val32 && rcVal32;
+        return CSRView<float>{nrow, mcol, nnz, rowPtr, colInd, val32,
+                              rc ? rcCls : nullptr, rcOff, rcDelta, rcVal32};
+    }
     int ensure32(cudaStream_t s);
 };
 

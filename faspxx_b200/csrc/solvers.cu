@@ -211,6 +211,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             if (fusable && cfg.precision == FASP_GPU_FP64) {
                 cg64 = new CGEngine<double>();
                 cg64->wantPersistent = cfg.persistent != 0;
+                cg64->pdl = cfg.overlapLaunch != 0;
                 if ((e = cg64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
             }
             if (cfg.precision == FASP_GPU_MIXED || cfg.precision == FASP_GPU_MIXED_RELIABLE) {
@@ -218,6 +219,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 if ((e = Ah->M.ensure32(c.stream))) return e;
                 cg32 = new CGEngine<float>();
                 cg32->wantPersistent = cfg.persistent != 0;
+                cg32->pdl = cfg.overlapLaunch != 0;
                 if ((e = cg32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
             }
             break;
@@ -736,6 +738,7 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
         h.rx = x64;
         h.rr = r64;
         h.rval = A->val;
+        h.rcval = A->rcVal;
         if ((e = E.push_ctl()) || (e = E.launch_init()) || (e = E.pull_ctl())) return e;
         h.rmax = h.resAbs;
         if ((e = E.push_ctl())) return e;

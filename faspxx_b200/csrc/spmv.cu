@@ -9,6 +9,7 @@
 // L = 32 the warp-per-row vector kernel; L is chosen from the mean row length or timed.
 #include <algorithm>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 #include "internal.h"
@@ -24,8 +25,7 @@ __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restri
     if (L == 1) { // thread per row: short rows (stencils)
         for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.nrow;
              r += (size_t)gridDim.x * blockDim.x) {
-            const uint32_t b = ld_stream(A.rowPtr + r), e = ld_stream(A.rowPtr + r + 1);
-            y[r] = row_dot<T, PAT>(A, b, e, [&](uint32_t j) { return x[j]; });
+            y[r] = row_apply<T, PAT>(A, r, [&](uint32_t j) { return x[j]; });
         }
         return;
     }
@@ -61,10 +61,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(CSRView<T> A, const T* __re
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x) {
             T s = T(0);
-            if (!shortcut) {
-                const uint32_t bb = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-                s = row_dot<T, false>(A, bb, e, [&](uint32_t j) { return x[j]; });
-            }
+            if (!shortcut) s = row_apply<T, false>(A, row, [&](uint32_t j) { return x[j]; });
             r[row] = b[row] - s;
         }
         return;
@@ -237,7 +234,98 @@ void m_free(Mat& M)
     cudaFree(M.val);
     cudaFree(M.val32);
     cudaFree(M.diag);
+    cudaFree(M.rcCls);
+    cudaFree(M.rcOff);
+    cudaFree(M.rcDelta);
+    cudaFree(M.rcVal);
+    cudaFree(M.rcVal32);
     M = Mat();
+}
+
+// ---- row classes ------------------------------------------------------------------------
+// A row's class is its length, its column offsets col - row and its values (bit patterns),
+// in CSR order. Constant-coefficient stencil matrices have a handful of classes (interior,
+// faces, edges, corners), so the SpMV streams a 2-byte class id per row instead of 8 to 12
+// bytes per entry. The table is built only when it stays small against the matrix.
+
+constexpr uint32_t kRcMaxClasses = 4096;
+constexpr uint32_t kRcMaxRowLen = 64;
+
+struct RowClasses {
+    std::vector<uint16_t> cls;
+    std::vector<uint32_t> off{0};
+    std::vector<int32_t>  delta;
+    std::vector<double>   val;
+};
+
+static bool build_row_classes(uint32_t nrow, const uint32_t* rp, const uint32_t* ci,
+                              const double* v, RowClasses& R)
+{
+    if (nrow == 0 || nrow > 0x7fffffffu) return false;
+    const size_t nnz = rp[nrow];
+    const size_t maxEntries = std::max<size_t>(64, nnz / 8);
+    R.cls.resize(nrow);
+    std::unordered_map<uint64_t, std::vector<uint32_t>> buckets;
+    for (uint32_t row = 0; row < nrow; ++row) {
+        const uint32_t b = rp[row], e = rp[row + 1], len = e - b;
+        if (len > kRcMaxRowLen) return false;
+        uint64_t h = 1469598103934665603ull ^ len;
+        for (uint32_t k = b; k < e; ++k) {
+            const uint64_t d = (uint64_t)(uint32_t)(int32_t)((int64_t)ci[k] - (int64_t)row);
+            uint64_t bits;
+            std::memcpy(&bits, &v[k], 8);
+            h = (h ^ d) * 1099511628211ull;
+            h = (h ^ bits) * 1099511628211ull;
+        }
+        auto& cand = buckets[h];
+        uint32_t id = 0xffffffffu;
+        for (uint32_t c : cand) {
+            const uint32_t cb = R.off[c], ce = R.off[c + 1];
+            if (ce - cb != len) continue;
+            bool same = true;
+            for (uint32_t k = 0; k < len && same; ++k)
+                same = R.delta[cb + k] == (int32_t)((int64_t)ci[b + k] - (int64_t)row) &&
+                       std::memcmp(&R.val[cb + k], &v[b + k], 8) == 0;
+            if (same) {
+                id = c;
+                break;
+            }
+        }
+        if (id == 0xffffffffu) {
+            id = (uint32_t)R.off.size() - 1;
+            if (id >= kRcMaxClasses || R.delta.size() + len > maxEntries) return false;
+            for (uint32_t k = b; k < e; ++k) {
+                const int64_t d = (int64_t)ci[k] - (int64_t)row;
+                if (d < INT32_MIN || d > INT32_MAX) return false;
+                R.delta.push_back((int32_t)d);
+                R.val.push_back(v[k]);
+            }
+            R.off.push_back((uint32_t)R.delta.size());
+            cand.push_back(id);
+        }
+        R.cls[row] = (uint16_t)id;
+    }
+    return true;
+}
+
+static int upload_row_classes(Mat& T, const RowClasses& R, cudaStream_t s)
+{
+    const uint32_t C = (uint32_t)R.off.size() - 1, E = (uint32_t)R.delta.size();
+    int e;
+    if ((e = dmalloc((void**)&T.rcCls, (size_t)T.nrow * 2 + 16)) ||
+        (e = dmalloc((void**)&T.rcOff, ((size_t)C + 1) * 4)) ||
+        (e = dmalloc((void**)&T.rcDelta, (size_t)E * 4 + 16)) ||
+        (e = dmalloc((void**)&T.rcVal, (size_t)E * 8 + 16)))
+        return e;
+    FB_CUDA(cudaMemcpyAsync(T.rcCls, R.cls.data(), (size_t)T.nrow * 2, cudaMemcpyHostToDevice, s));
+    FB_CUDA(cudaMemcpyAsync(T.rcOff, R.off.data(), ((size_t)C + 1) * 4, cudaMemcpyHostToDevice, s));
+    FB_CUDA(cudaMemcpyAsync(T.rcDelta, R.delta.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
+    FB_CUDA(cudaMemcpyAsync(T.rcVal, R.val.data(), (size_t)E * 8, cudaMemcpyHostToDevice, s));
+    FB_CUDA(cudaStreamSynchronize(s)); // the host vectors die with the caller
+    T.rcClasses = C;
+    T.rcEntries = E;
+    T.rcOn = true;
+    return kOk;
 }
 
 // CheckCSR (src/MATUtil.cxx:110-174) on host arrays: sizes, monotone row pointers, column
@@ -298,6 +386,20 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
         nrow, T.rowPtr, T.colInd, T.val, T.diagPtr, T.diag);
     FB_CUDA(cudaGetLastError());
     T.lanes = lanes_for(T.meanRowLen);
+    if (values && T.lanes == 1) {
+        std::vector<double> hv;
+        const double* cv = values;
+        if (!hostPtrs) {
+            hv.resize(nnz);
+            FB_CUDA(cudaMemcpy(hv.data(), values, (size_t)nnz * 8, cudaMemcpyDeviceToHost));
+            cv = hv.data();
+        }
+        RowClasses R;
+        if (build_row_classes(nrow, crp, cci, cv, R) && (e = upload_row_classes(T, R, s))) {
+            m_free(T);
+            return e;
+        }
+    }
     FB_CUDA(cudaStreamSynchronize(s));
     M = T;
     return kOk;
@@ -305,12 +407,20 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
 
 int Mat::ensure32(cudaStream_t s)
 {
-    if (val32 || !val) return kOk;
-    int e = dmalloc((void**)&val32, (size_t)nnz * 4);
-    if (e) return e;
-    k_to_f32<<<std::max(1, std::min(ceil_div(nnz, kBlock), 148 * 8)), kBlock, 0, s>>>(nnz, val,
-                                                                                      val32);
-    FB_CUDA(cudaGetLastError());
+    if (!val) return kOk;
+    int e;
+    if (!val32) {
+        if ((e = dmalloc((void**)&val32, (size_t)nnz * 4))) return e;
+        k_to_f32<<<std::max(1, std::min(ceil_div(nnz, kBlock), 148 * 8)), kBlock, 0, s>>>(
+            nnz, val, val32);
+        FB_CUDA(cudaGetLastError());
+    }
+    if (rcVal && !rcVal32) {
+        if ((e = dmalloc((void**)&rcVal32, (size_t)rcEntries * 4 + 16))) return e;
+        k_to_f32<<<std::max(1, std::min(ceil_div(rcEntries, kBlock), 148 * 8)), kBlock, 0, s>>>(
+            rcEntries, rcVal, rcVal32);
+        FB_CUDA(cudaGetLastError());
+    }
     return kOk;
 }
 

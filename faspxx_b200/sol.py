@@ -129,6 +129,17 @@ class MAT:
     def Residual(self, b: DVec, x: DVec, r: DVec) -> None:
         check(lib.fasp_gpu_mat_residual(self.h, b.ptr, x.ptr, r.ptr), "Residual")
 
+    def SetRowClass(self, on: bool) -> None:
+        """Use (or stop using) the row-class form of the matrix in the SpMV kernels."""
+        check(lib.fasp_gpu_mat_set_rowclass(self.h, 1 if on else 0), "SetRowClass")
+
+    def RowClassInfo(self):
+        """(in use, classes, table entries); 0 classes: the matrix has no row-class form."""
+        on, k, e = C.c_int(), C.c_uint32(), C.c_uint32()
+        check(lib.fasp_gpu_mat_rowclass_info(self.h, C.byref(on), C.byref(k), C.byref(e)),
+              "RowClassInfo")
+        return bool(on.value), k.value, e.value
+
     def Transpose(self) -> "MAT":
         """MAT::TransInPlace into a new matrix (the original stays)."""
         h = C.c_void_p()
@@ -219,6 +230,9 @@ class SOL:
 
     def SetPersistent(self, flag: bool):
         self.cfg.persistent = 1 if flag else 0
+
+    def SetOverlapLaunch(self, flag: bool):
+        self.cfg.overlapLaunch = 1 if flag else 0
 
     def SetUseGraph(self, flag: bool):
         self.cfg.useGraph = 1 if flag else 0

@@ -86,6 +86,9 @@ typedef struct {
                                     cooperative launch (when the device allows it);
                                     default 0: CUDA graphs of the two fused kernels
                                     measure faster on B200 at every size */
+    int             overlapLaunch; /* 1 (default): the CG iteration kernels use programmatic
+                                    dependent launch, each one's launch overlapping its
+                                    predecessor's reduction tail */
 } fasp_gpu_config;
 
 /* Outcome of one Solve. */
@@ -146,9 +149,18 @@ int fasp_gpu_mat_diag(fasp_gpu_mat A, double* diag);
 /* Rows-per-warp autotuner: times every lanes-per-row choice on A; returns the pick. */
 int fasp_gpu_mat_autotune(fasp_gpu_mat A, int* lanes);
 int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes);
+/* Row-class storage: rows with identical column offsets (col - row) and values share one
+ * table entry, and the thread-per-row SpMV streams a 2-byte class id per row instead of the
+ * row's indices and values (same FMA order, bit-identical results). Built at upload when
+ * the rows fall into at most 4096 classes whose table is at most nnz/8 entries (constant-
+ * coefficient stencils); used when lanes = 1. set_rowclass(A, 0) falls back to plain CSR
+ * (set it before a solver's Setup, which captures the matrix form). */
+int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int on);
+int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* on, uint32_t* classes, uint32_t* entries);
 /* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
  * value copy (fp32 = 1), timed with CUDA events on the matrix's stream (inputs: x = 0). */
-int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, double* ms);
+int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2,
+                            double* ms);
 /* Sampled outer product on A's pattern: dA[k] = scale * lam[row(k)] * x[col(k)]. The
  * matrix gradient dL/dA of x = A^-1 b is the case scale = -1 (no reference counterpart). */
 int fasp_gpu_mat_sampled_outer(fasp_gpu_mat A, const double* lam, const double* x,
@@ -191,14 +203,15 @@ int fasp_gpu_solver_solve_host(fasp_gpu_solver s, const double* b, double* x,
 int fasp_gpu_solver_history(fasp_gpu_solver s, double* hist, uint32_t cap, uint32_t* len);
 int fasp_gpu_solver_clean(fasp_gpu_solver s);     /* SOL::Clean */
 int fasp_gpu_solver_destroy(fasp_gpu_solver s);
-/* Device time of the last Solve in milliseconds (CUDA events around its device work). */
+/* Device time of the last Solve (or adjoint solve) in milliseconds (CUDA events around its
+ * device work). */
 int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms);
 /* Device-driven CG only: average duration (ms) of each of its two fused kernels over reps
  * launches, timed alone with CUDA events on the solver's stream (control logic bypassed;
  * the solver's internal vectors are overwritten). ms must hold 3 values: ms[0] SpMV
  * kernel, ms[1] update kernel, ms[2] one iteration of the persistent kernel (0 when the
  * solver does not use it). Times the FP32 engine when the solver is MIXED. */
-int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, double* ms);
+int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, int flushL2, double* ms);
 
 /* ---- adjoint (no reference counterpart) --------------------------------------------- */
 /* Solve A^T lam = g with the same Krylov kernels on the exact CSC transpose of the bound

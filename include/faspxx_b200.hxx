@@ -155,6 +155,9 @@ public:
     {
         fasp_gpu_mat_residual(h_, b.data(), x.data(), r.data());
     }
+    /* B200 option: use (or not) the row-class form of a constant-coefficient matrix in the
+     * SpMV kernels (bit-identical results; set before a solver's Setup) */
+    void SetRowClass(bool on) { fasp_gpu_mat_set_rowclass(h_, on ? 1 : 0); }
     /* MAT::TransInPlace (MAT.cxx:479-538) */
     void TransInPlace()
     {
@@ -200,7 +203,11 @@ public:
     void SetAbsTol(double v) { cfg_.prm.absTol = v; dirty_ = true; }
     /* B200 options */
     void SetPrecision(int p) { cfg_.precision = p; dirty_ = true; }
+    void SetInnerRelTol(double t) { cfg_.innerRelTol = t; dirty_ = true; }
     void SetOrth(int o) { cfg_.orth = o; dirty_ = true; }
+    void SetUseGraph(bool on) { cfg_.useGraph = on ? 1 : 0; dirty_ = true; }
+    void SetPersistent(bool on) { cfg_.persistent = on ? 1 : 0; dirty_ = true; }
+    void SetOverlapLaunch(bool on) { cfg_.overlapLaunch = on ? 1 : 0; dirty_ = true; }
     const fasp_gpu_config& Config() const { return cfg_; }
     /* SOL::SetupPCD (SOL.cxx:249): Identity or Jacobi */
     virtual void SetupPCD(SOL& pc) { pc.AsPreconditionerOf(cfg_); dirty_ = true; }

@@ -161,7 +161,8 @@ def _check_case(gpu, oracle, name, engine="graph"):
     M = gpu.MAT(A)
     s = gpu.configure(case["alg"], **case["kw"])
     s.SetPersistent(engine == "persistent")
-    s.SetUseGraph(engine == "graph")
+    s.SetUseGraph(engine in ("graph", "graph_serial"))
+    s.SetOverlapLaunch(engine != "graph_serial")
     s.Setup(M)
     po = oracle.Solver("port", A, case["alg"], **case["kw"])
     for rep in range(case.get("repeat", 1)):
@@ -206,13 +207,13 @@ def test_solver_parity(gpu, oracle, name):
     _check_case(gpu, oracle, name)
 
 
-@pytest.mark.parametrize("engine", ["persistent", "plain"])
+@pytest.mark.parametrize("engine", ["persistent", "plain", "graph_serial"])
 @pytest.mark.parametrize("name", ["fdm_pcg", "fem_pcg", "p2d_pcg", "p3d_cg", "vd_cg",
                                   "fdm_cg_min5", "fdm_cg_tolsmall"])
 def test_cg_engines_match(gpu, oracle, name, engine):
-    """The device-driven CG meets the same bars run as CUDA graphs of its two kernels (the
-    default, exercised by test_solver_parity), as one persistent cooperative kernel, and
-    as plain launches."""
+    """The device-driven CG meets the same bars run as CUDA graphs of its two kernels with
+    overlapped launches (the default, exercised by test_solver_parity), as graphs with
+    ordinary launches, as one persistent cooperative kernel, and as plain launches."""
     _check_case(gpu, oracle, name, engine=engine)
 
 
