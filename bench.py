@@ -348,14 +348,15 @@ def run_ours(args):
     capi.check(lib.fasp_gpu_solver_kernel_times(fp64.h, 30, 1, k64), "kernel_times")
     sp = C.c_double()
     capi.check(lib.fasp_gpu_mat_time_apply(M.h, 30, 0, 1, C.byref(sp)), "time_apply")
-    rc_on, rc_classes, rc_entries = M.RowClassInfo()
+    rc_mode, rc_classes, rc_entries, rc_stencil = M.RowClassInfo()
+    rc_on = rc_mode > 0
     sp_csr = C.c_double()
-    M.SetRowClass(False)
+    M.SetRowClass(0)
     capi.check(lib.fasp_gpu_mat_time_apply(M.h, 30, 0, 1, C.byref(sp_csr)), "time_apply")
-    M.SetRowClass(rc_on)
+    M.SetRowClass(rc_mode)
     # algorithmic bytes per launch (compulsory traffic); the matrix streams either the CSR
-    # arrays (values + column indices + row pointers) or one 2-byte class id per row (the
-    # class table, rc_entries entries, stays in L1/L2)
+    # arrays (values + column indices + row pointers) or one 2-byte class id / stencil mask
+    # per row (the class table stays in L1/L2, the stencil travels as kernel parameters)
     mat32 = 2 * n if rc_on else 8 * nnz + 4 * (n + 1)
     mat64 = 2 * n if rc_on else 12 * nnz + 4 * (n + 1)
     b_spmv32 = mat32 + 4 * n * 4                     # read z,p_old write p,q
@@ -379,10 +380,11 @@ def run_ours(args):
     else:
         # the dominant kernel of the FP32 iteration: the larger of the two fused kernels
         if km[0] >= km[1]:
-            name = ("cg_spmv<float> (SpMV + p update + (Ap,p), FP32 CG iteration"
-                    + (", row-class matrix form)" if rc_on else ", CSR)"))
+            form = {0: "csr", 1: "rowclass", 2: "stencil"}[rc_mode]
+            name = (f"cg_spmv<float> (SpMV + p update + (Ap,p), FP32 CG iteration, {form} "
+                    "matrix form)")
             byt, ms_k = b_spmv32, km[0]
-            key = "cg_spmv<float>/" + ("rowclass" if rc_on else "csr")
+            key = f"cg_spmv<float>/{form}"
         else:
             name = ("cg_update<float,1> (x += alpha p, r -= alpha Ap, z = D^-1 r and five "
                     "reductions, FP32 CG iteration)")
@@ -406,7 +408,7 @@ def run_ours(args):
         "cg_update_f64": {"ms": round(k64[1], 5), "gbs": round(gbs(b_upd64, k64[1]), 1)},
         "spmv_f64_apply": {"ms": round(sp.value, 5), "gbs": round(gbs(b_apply, sp.value), 1),
                            "frac": round(gbs(b_apply, sp.value) / hbm, 3),
-                           "form": "row classes" if rc_on else "CSR"},
+                           "form": {0: "CSR", 1: "row classes", 2: "stencil masks"}[rc_mode]},
         "spmv_f64_apply_csr": {"ms": round(sp_csr.value, 5),
                                "gbs": round(gbs(b_apply_csr, sp_csr.value), 1),
                                "frac": round(gbs(b_apply_csr, sp_csr.value) / hbm, 3)},
@@ -458,8 +460,9 @@ def run_ours(args):
                          "fp64_rel_residual": acc_fp64[0], "fp64_err_vs_fp64_1e-13": acc_fp64[1],
                          "e2e_err_vs_fp64_1e-13": e2e_err},
             "spmv_gbs": kernels["spmv_f64_apply_csr"]["gbs"],
-            "matrix_form": {"row_classes": rc_on, "classes": rc_classes,
-                            "table_entries": rc_entries},
+            "matrix_form": {"mode": {0: "CSR", 1: "row classes", 2: "stencil masks"}[rc_mode],
+                            "classes": rc_classes, "table_entries": rc_entries,
+                            "stencil_offsets": rc_stencil},
             "roofline": roofline, "kernels": kernels,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 8 * n},

@@ -74,7 +74,7 @@ SIGNATURES = {
     "fasp_gpu_mat_autotune": (_i, [_vp, _P(_i)]),
     "fasp_gpu_mat_set_lanes": (_i, [_vp, _i]),
     "fasp_gpu_mat_set_rowclass": (_i, [_vp, _i]),
-    "fasp_gpu_mat_rowclass_info": (_i, [_vp, _P(_i), _P(_u32), _P(_u32)]),
+    "fasp_gpu_mat_rowclass_info": (_i, [_vp, _P(_i), _P(_u32), _P(_u32), _P(_u32)]),
     "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _i, _P(_d)]),
     "fasp_gpu_mat_sampled_outer": (_i, [_vp, _vp, _vp, _d, _vp]),
     "fasp_gpu_vec_dot": (_i, [_u32, _vp, _vp, _P(_d)]),

@@ -323,19 +323,23 @@ int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes)
     return kOk;
 }
 
-int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int on)
+int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode)
 {
-    if (!A) return kErrInputPar;
-    A->M.rcOn = on != 0 && A->M.rcCls != nullptr;
+    if (!A || mode < 0 || mode > 2) return kErrInputPar;
+    A->M.rcOn = mode >= 1 && A->M.rcCls != nullptr;
+    A->M.skOn = mode == 2;
     return kOk;
 }
 
-int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* on, uint32_t* classes, uint32_t* entries)
+int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uint32_t* entries,
+                               uint32_t* stencil)
 {
     if (!A) return kErrInputPar;
-    if (on) *on = A->M.rcOn ? 1 : 0;
-    if (classes) *classes = A->M.rcClasses;
-    if (entries) *entries = A->M.rcEntries;
+    const Mat& M = A->M;
+    if (mode) *mode = !M.rcOn ? 0 : (M.skOn && M.skMask ? 2 : 1);
+    if (classes) *classes = M.rcClasses;
+    if (entries) *entries = M.rcEntries;
+    if (stencil) *stencil = M.skMask ? M.skLen : 0;
     return kOk;
 }
 

@@ -191,15 +191,49 @@ __device__ __forceinline__ void cg_refresh_fold(uint32_t n, float* x32, const CG
     }
 }
 
-// Reliable update, part 2 (in the cg_update slot): r64 = b - A x64 on the FP64 values,
-// r32 = r64 / s, z32 = diagInv .* r32, with the three sums of cg_after_refresh.
-template <int JAC>
-__device__ __forceinline__ void cg_refresh_residual(const CSRView<float>& A, float* r32,
-                                                    float* z32, const float* dinv32,
-                                                    CGCtl* c, Scratch s)
+// The structure of the FP32 view that the FP64 refresh residual walks (small enough to pass
+// by value; the stencil offsets and all FP64 values come from the control block).
+struct RefreshView {
+    uint32_t        nrow, ulen;
+    const uint32_t* rowPtr;
+    const uint32_t* colInd;
+    const uint16_t* cls;
+    const uint32_t* coff;
+    const int32_t*  cdelta;
+    const uint16_t* mask;
+};
+
+// Row `row` of the FP64 matrix: the same storage form and entry order as row_apply.
+template <typename XV>
+__device__ __forceinline__ double row_fp64(const RefreshView& A, const CGCtl* c, size_t row,
+                                           XV xv)
 {
-    const CSRView<double> A64{A.nrow, A.mcol, A.nnz, A.rowPtr, A.colInd, c->rval,
-                              A.cls, A.coff, A.cdelta, c->rcval};
+    double s = 0.0;
+    if (A.mask) {
+        const uint32_t m = __ldcs(A.mask + row);
+        for (uint32_t k = 0; k < A.ulen; ++k)
+            if ((m >> k) & 1u)
+                s = fma(c->skval[k], xv((uint32_t)((long long)row + c->skdelta[k])), s);
+        return s;
+    }
+    if (A.cls) {
+        const uint32_t k = __ldcs(A.cls + row);
+        for (uint32_t i = A.coff[k]; i < A.coff[k + 1]; ++i)
+            s = fma(c->rcval[i], xv((uint32_t)((long long)row + A.cdelta[i])), s);
+        return s;
+    }
+    for (uint32_t k = A.rowPtr[row]; k < A.rowPtr[row + 1]; ++k)
+        s = fma(c->rval[k], xv(A.colInd[k]), s);
+    return s;
+}
+
+// Reliable update, part 2 (in the cg_update slot): r64 = b - A x64 on the FP64 values,
+// r32 = r64 / s, z32 = diagInv .* r32, with the three sums of cg_after_refresh. Not inlined:
+// it runs a few times per solve and must not cost the update kernel registers.
+template <int JAC>
+__device__ __noinline__ void cg_refresh_residual(RefreshView A, float* r32, float* z32,
+                                                 const float* dinv32, CGCtl* c, Scratch s)
+{
     const double* b = c->rb;
     const double* x64 = c->rx;
     double* r64 = c->rr;
@@ -208,7 +242,7 @@ __device__ __forceinline__ void cg_refresh_residual(const CSRView<float>& A, flo
     float rr = 0.f, zr = 0.f;
     GRID_STRIDE(row, A.nrow)
     {
-        const double ax = row_apply<double, false>(A64, row, [&](uint32_t j) { return x64[j]; });
+        const double ax = row_fp64(A, c, row, [&](uint32_t j) { return x64[j]; });
         const double ri = b[row] - ax;
         r64[row] = ri;
         const float r32i = (float)(ri * inv);
@@ -315,7 +349,10 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
     pdl_release();
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
-            if (c->status == kRefresh) cg_refresh_residual<JAC>(A, r, z, dinv, c, s);
+            if (c->status == kRefresh)
+                cg_refresh_residual<JAC>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd, A.cls,
+                                                     A.coff, A.cdelta, A.mask},
+                                         r, z, dinv, c, s);
         return;
     }
     const T alpha = (T)c->alpha;

@@ -45,6 +45,8 @@ struct CGCtl {
     double*  rr;        // r = b - A x (FP64), written by each refresh
     const double* rval; // FP64 values of the matrix (same structure as the FP32 view)
     const double* rcval;// FP64 values of its row-class table (when the FP32 view uses one)
+    double   skval[kMaxStencil]; // FP64 stencil values (when the FP32 view uses masks)
+    int32_t  skdelta[kMaxStencil];
     double   red[5];    // rr, zr, xx, max|x|, pp saved at an escalation
     double*  hist;
     unsigned histCap;

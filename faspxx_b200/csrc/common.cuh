@@ -105,6 +105,8 @@ __device__ __forceinline__ T group_sum(T v)
 }
 
 // CSRx matrix view: 32-bit unsigned indices as in FASP++'s MAT (src/MAT.hxx:43-47).
+constexpr int kMaxStencil = 16;
+
 template <typename T>
 struct CSRView {
     uint32_t        nrow, mcol, nnz;
@@ -118,6 +120,15 @@ struct CSRView {
     const uint32_t* coff;
     const int32_t*  cdelta;
     const T*        cval;
+    // Stencil masks (optional, thread-per-row kernels): every row is a subset of one sorted
+    // list of column offsets udelta[0..ulen) whose values uval are the same in every row
+    // that has them (constant coefficients, truncated at the boundary); mask[row] says which
+    // are present. The lists travel in the kernel's parameter space, so a row costs one
+    // 2-byte load plus its gathers.
+    const uint16_t* mask;
+    uint32_t        ulen;
+    int32_t         udelta[kMaxStencil];
+    T               uval[kMaxStencil];
 };
 
 // The matrix is streamed once per SpMV: evict-first loads keep it from displacing the
@@ -158,6 +169,28 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, uint32_t b, uint32_t e
 template <typename T, bool PAT, typename XV>
 __device__ __forceinline__ T row_apply(const CSRView<T>& A, size_t row, XV xv)
 {
+    if (!PAT && A.mask) {
+        const uint32_t m = __ldcs(A.mask + row);
+        T s = T(0);
+        // chunks of 8 offsets: a 7-point row issues all its gathers before the first FMA
+#pragma unroll
+        for (int c0 = 0; c0 < kMaxStencil; c0 += 8) {
+            if (c0 >= (int)A.ulen) break;
+            T xs[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = c0 + u;
+                const bool in = k < (int)A.ulen && ((m >> k) & 1u);
+                xs[u] = in ? xv((uint32_t)((long long)row + A.udelta[k])) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = c0 + u;
+                if (k < (int)A.ulen && ((m >> k) & 1u)) s = fma(A.uval[k], xs[u], s);
+            }
+        }
+        return s;
+    }
     if (!PAT && A.cls) {
         const uint32_t k = __ldcs(A.cls + row);
         const uint32_t b = __ldg(A.coff + k), e = __ldg(A.coff + k + 1);

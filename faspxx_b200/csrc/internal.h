@@ -139,18 +139,40 @@ struct Mat {
     float*    rcVal32 = nullptr;
     uint32_t  rcClasses = 0, rcEntries = 0;
     bool      rcOn = false;      // used by the thread-per-row kernels when built and enabled
-    CSRView<double> v64() const
+    // stencil-mask form (built with the classes when they are subsets of one stencil)
+    uint16_t* skMask = nullptr;
+    bool      skOn = true;       // masks used when built (and row classes are on)
+    uint32_t  skLen = 0;
+    int32_t   skDelta[kMaxStencil] = {};
+    double    skVal[kMaxStencil] = {};
+    template <typename T>
+    CSRView<T> view(const T* v, const T* cv) const
     {
-        const bool rc = rcOn && rcCls && val;
-        return CSRView<double>{nrow, mcol, nnz, rowPtr, colInd, val,
-                               rc ? rcCls : nullptr, rcOff, rcDelta, rcVal};
+        CSRView<T> V{};
+        V.nrow = nrow;
+        V.mcol = mcol;
+        V.nnz = nnz;
+        V.rowPtr = rowPtr;
+        V.colInd = colInd;
+        V.val = v;
+        if (rcOn && rcCls && v && cv) {
+            V.cls = rcCls;
+            V.coff = rcOff;
+            V.cdelta = rcDelta;
+            V.cval = cv;
+            if (skMask && skOn) {
+                V.mask = skMask;
+                V.ulen = skLen;
+                for (uint32_t u = 0; u < skLen; ++u) {
+                    V.udelta[u] = skDelta[u];
+                    V.uval[u] = (T)skVal[u];
+                }
+            }
+        }
+        return V;
     }
-    CSRView<float> v32() const
-    {
-        const bool rc = rcOn && rcCls && val32 && rcVal32;
-        return CSRView<float>{nrow, mcol, nnz, rowPtr, colInd, val32,
-                              rc ? rcCls : nullptr, rcOff, rcDelta, rcVal32};
-    }
+    CSRView<double> v64() const { return view<double>(val, rcVal); }
+    CSRView<float>  v32() const { return view<float>(val32, rcVal32); }
     int ensure32(cudaStream_t s);
 };
 

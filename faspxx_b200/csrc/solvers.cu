@@ -739,6 +739,10 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
         h.rr = r64;
         h.rval = A->val;
         h.rcval = A->rcVal;
+        for (int u = 0; u < kMaxStencil; ++u) {
+            h.skval[u] = A->skVal[u];
+            h.skdelta[u] = A->skDelta[u];
+        }
         if ((e = E.push_ctl()) || (e = E.launch_init()) || (e = E.pull_ctl())) return e;
         h.rmax = h.resAbs;
         if ((e = E.push_ctl())) return e;

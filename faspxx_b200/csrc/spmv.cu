@@ -9,6 +9,7 @@
 // L = 32 the warp-per-row vector kernel; L is chosen from the mean row length or timed.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -239,6 +240,7 @@ void m_free(Mat& M)
     cudaFree(M.rcDelta);
     cudaFree(M.rcVal);
     cudaFree(M.rcVal32);
+    cudaFree(M.skMask);
     M = Mat();
 }
 
@@ -308,6 +310,40 @@ static bool build_row_classes(uint32_t nrow, const uint32_t* rp, const uint32_t*
     return true;
 }
 
+// Stencil masks: when the classes' column offsets, taken together, are at most kMaxStencil
+// distinct values each carrying one value (bitwise) wherever it occurs, and every class
+// lists its offsets in ascending order (the CSR order), each row is a bit mask over that
+// sorted offset list. Summing the present entries in list order is the CSR order.
+static bool build_stencil_masks(const RowClasses& R, Mat& T, std::vector<uint16_t>& rowMask)
+{
+    std::map<int32_t, double> U;
+    const uint32_t C = (uint32_t)R.off.size() - 1;
+    for (uint32_t c = 0; c < C; ++c)
+        for (uint32_t k = R.off[c]; k < R.off[c + 1]; ++k) {
+            if (k > R.off[c] && R.delta[k] <= R.delta[k - 1]) return false;
+            auto it = U.find(R.delta[k]);
+            if (it == U.end())
+                U.emplace(R.delta[k], R.val[k]);
+            else if (std::memcmp(&it->second, &R.val[k], 8) != 0)
+                return false;
+        }
+    if (U.empty() || U.size() > (size_t)kMaxStencil) return false;
+    std::map<int32_t, int> pos;
+    T.skLen = 0;
+    for (auto& kv : U) {
+        pos[kv.first] = (int)T.skLen;
+        T.skDelta[T.skLen] = kv.first;
+        T.skVal[T.skLen] = kv.second;
+        ++T.skLen;
+    }
+    std::vector<uint16_t> cm(C, 0);
+    for (uint32_t c = 0; c < C; ++c)
+        for (uint32_t k = R.off[c]; k < R.off[c + 1]; ++k) cm[c] |= (uint16_t)(1u << pos[R.delta[k]]);
+    rowMask.resize(R.cls.size());
+    for (size_t r = 0; r < R.cls.size(); ++r) rowMask[r] = cm[R.cls[r]];
+    return true;
+}
+
 static int upload_row_classes(Mat& T, const RowClasses& R, cudaStream_t s)
 {
     const uint32_t C = (uint32_t)R.off.size() - 1, E = (uint32_t)R.delta.size();
@@ -321,6 +357,14 @@ static int upload_row_classes(Mat& T, const RowClasses& R, cudaStream_t s)
     FB_CUDA(cudaMemcpyAsync(T.rcOff, R.off.data(), ((size_t)C + 1) * 4, cudaMemcpyHostToDevice, s));
     FB_CUDA(cudaMemcpyAsync(T.rcDelta, R.delta.data(), (size_t)E * 4, cudaMemcpyHostToDevice, s));
     FB_CUDA(cudaMemcpyAsync(T.rcVal, R.val.data(), (size_t)E * 8, cudaMemcpyHostToDevice, s));
+    std::vector<uint16_t> rowMask;
+    if (build_stencil_masks(R, T, rowMask)) {
+        if ((e = dmalloc((void**)&T.skMask, (size_t)T.nrow * 2 + 16))) return e;
+        FB_CUDA(cudaMemcpyAsync(T.skMask, rowMask.data(), (size_t)T.nrow * 2,
+                                cudaMemcpyHostToDevice, s));
+    } else {
+        T.skLen = 0;
+    }
     FB_CUDA(cudaStreamSynchronize(s)); // the host vectors die with the caller
     T.rcClasses = C;
     T.rcEntries = E;

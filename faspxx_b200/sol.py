@@ -129,16 +129,19 @@ class MAT:
     def Residual(self, b: DVec, x: DVec, r: DVec) -> None:
         check(lib.fasp_gpu_mat_residual(self.h, b.ptr, x.ptr, r.ptr), "Residual")
 
-    def SetRowClass(self, on: bool) -> None:
-        """Use (or stop using) the row-class form of the matrix in the SpMV kernels."""
-        check(lib.fasp_gpu_mat_set_rowclass(self.h, 1 if on else 0), "SetRowClass")
+    def SetRowClass(self, mode) -> None:
+        """Matrix form of the SpMV kernels: 0/False = CSR, 1 = row classes, 2/True = row
+        classes with stencil masks (the default when built)."""
+        mode = 2 if mode is True else (0 if mode is False else int(mode))
+        check(lib.fasp_gpu_mat_set_rowclass(self.h, mode), "SetRowClass")
 
     def RowClassInfo(self):
-        """(in use, classes, table entries); 0 classes: the matrix has no row-class form."""
-        on, k, e = C.c_int(), C.c_uint32(), C.c_uint32()
-        check(lib.fasp_gpu_mat_rowclass_info(self.h, C.byref(on), C.byref(k), C.byref(e)),
-              "RowClassInfo")
-        return bool(on.value), k.value, e.value
+        """(mode in use, classes, table entries, stencil length); 0 classes: no row-class
+        form, stencil 0: no masks."""
+        mode, k, e, st = C.c_int(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(lib.fasp_gpu_mat_rowclass_info(self.h, C.byref(mode), C.byref(k), C.byref(e),
+                                             C.byref(st)), "RowClassInfo")
+        return mode.value, k.value, e.value, st.value
 
     def Transpose(self) -> "MAT":
         """MAT::TransInPlace into a new matrix (the original stays)."""

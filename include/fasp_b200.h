@@ -149,14 +149,21 @@ int fasp_gpu_mat_diag(fasp_gpu_mat A, double* diag);
 /* Rows-per-warp autotuner: times every lanes-per-row choice on A; returns the pick. */
 int fasp_gpu_mat_autotune(fasp_gpu_mat A, int* lanes);
 int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes);
-/* Row-class storage: rows with identical column offsets (col - row) and values share one
- * table entry, and the thread-per-row SpMV streams a 2-byte class id per row instead of the
- * row's indices and values (same FMA order, bit-identical results). Built at upload when
- * the rows fall into at most 4096 classes whose table is at most nnz/8 entries (constant-
- * coefficient stencils); used when lanes = 1. set_rowclass(A, 0) falls back to plain CSR
- * (set it before a solver's Setup, which captures the matrix form). */
-int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int on);
-int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* on, uint32_t* classes, uint32_t* entries);
+/* Compressed forms of constant-coefficient matrices for the thread-per-row SpMV (lanes = 1),
+ * both with the CSR entry order and one FMA per entry, so results are bit-identical to CSR:
+ *  - row classes: rows with identical column offsets (col - row) and values share one table
+ *    entry; a row streams a 2-byte class id instead of its indices and values. Built at
+ *    upload when the rows fall into at most 4096 classes whose table is at most nnz/8
+ *    entries;
+ *  - stencil masks: when every class is a subset of one sorted list of at most 16 offsets
+ *    with one value each, a row is a 16-bit mask over that list, which the kernels receive
+ *    as launch parameters (no table reads at all).
+ * mode 0 = CSR, 1 = row classes, 2 = row classes with stencil masks (the default when
+ * built). Set it before a solver's Setup, which captures the matrix form. info reports the
+ * mode in use, the class count, table entries and the stencil length (0 = no masks). */
+int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode);
+int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uint32_t* entries,
+                               uint32_t* stencil);
 /* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
  * value copy (fp32 = 1), timed with CUDA events on the matrix's stream (inputs: x = 0). */
 int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2,

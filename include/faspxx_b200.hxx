@@ -155,9 +155,9 @@ public:
     {
         fasp_gpu_mat_residual(h_, b.data(), x.data(), r.data());
     }
-    /* B200 option: use (or not) the row-class form of a constant-coefficient matrix in the
-     * SpMV kernels (bit-identical results; set before a solver's Setup) */
-    void SetRowClass(bool on) { fasp_gpu_mat_set_rowclass(h_, on ? 1 : 0); }
+    /* B200 option: matrix form of the SpMV kernels, 0 CSR, 1 row classes, 2 row classes
+     * with stencil masks (bit-identical results; set before a solver's Setup) */
+    void SetRowClass(int mode) { fasp_gpu_mat_set_rowclass(h_, mode); }
     /* MAT::TransInPlace (MAT.cxx:479-538) */
     void TransInPlace()
     {

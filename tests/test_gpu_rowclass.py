@@ -1,9 +1,11 @@
-"""Row-class storage of constant-coefficient matrices: the thread-per-row SpMV reads a 2-byte
-class id per row from a table of (column offset, value) lists instead of the CSR arrays.
+"""Compressed forms of constant-coefficient matrices in the thread-per-row SpMV kernels:
+row classes (a 2-byte class id per row into a table of (column offset, value) lists) and
+stencil masks (a 16-bit mask per row over one sorted offset list passed as kernel
+parameters).
 
-Bar: bit-exact. Both forms accumulate each row's entries in CSR order with one FMA per
-entry, so MAT::Apply, MAT::Residual and whole solves (iteration counts, solutions and
-residual histories) are identical with the form on and off.
+Bar: bit-exact. All three forms (CSR, classes, masks) accumulate each row's entries in CSR
+order with one FMA per entry, so MAT::Apply, MAT::Residual and whole solves (iteration
+counts, solutions and residual histories) are identical whichever form is in use.
 """
 import numpy as np
 import pytest
@@ -12,6 +14,8 @@ from faspxx_b200 import problems as P
 from tests.golden import cases as G
 
 pytestmark = pytest.mark.gpu
+
+CSR, CLASSES, MASKS = 0, 1, 2
 
 
 @pytest.fixture(scope="module")
@@ -23,56 +27,79 @@ def gpu():
 
 def _stencils():
     return {
-        "poisson2d_40": P.poisson2d(40),
-        "poisson3d_20": P.poisson3d(20),
-        "convdiff3d_16_pe10": P.convdiff3d(16, 10.0),
-        "fdm_10X10": G.matrix("fdm_10X10"),
+        "poisson2d_40": (P.poisson2d(40), 5),
+        "poisson3d_20": (P.poisson3d(20), 7),
+        "convdiff3d_16_pe10": (P.convdiff3d(16, 10.0), 7),
+        "fdm_10X10": (G.matrix("fdm_10X10"), None),
     }
 
 
 @pytest.mark.parametrize("name", list(_stencils()))
 def test_apply_and_residual_bit_exact(gpu, name):
-    A = _stencils()[name]
+    A, stencil = _stencils()[name]
     M = gpu.MAT(A)
-    on, classes, entries = M.RowClassInfo()
-    assert on and 0 < classes <= 4096 and entries <= max(64, A.nnz // 8)
+    mode, classes, entries, st = M.RowClassInfo()
+    assert 0 < classes <= 4096 and entries <= max(64, A.nnz // 8)
+    if stencil is not None:
+        assert mode == MASKS and st == stencil
     rng = np.random.default_rng(1)
     x = gpu.DVec.from_numpy(rng.standard_normal(A.mcol))
     b = gpu.DVec.from_numpy(rng.standard_normal(A.nrow))
-    y_rc, r_rc = gpu.DVec(A.nrow), gpu.DVec(A.nrow)
-    M.Apply(x, y_rc)
-    M.Residual(b, x, r_rc)
-    M.SetRowClass(False)
-    assert not M.RowClassInfo()[0]
-    y, r = gpu.DVec(A.nrow), gpu.DVec(A.nrow)
-    M.Apply(x, y)
-    M.Residual(b, x, r)
-    assert np.array_equal(y_rc.numpy(), y.numpy())
-    assert np.array_equal(r_rc.numpy(), r.numpy())
-    # and both agree with the host product to rounding
+    out = {}
+    for form in (MASKS, CLASSES, CSR):
+        M.SetRowClass(form)
+        y, r = gpu.DVec(A.nrow), gpu.DVec(A.nrow)
+        M.Apply(x, y)
+        M.Residual(b, x, r)
+        out[form] = (y.numpy(), r.numpy())
+    assert M.RowClassInfo()[0] == CSR
+    for form in (MASKS, CLASSES):
+        assert np.array_equal(out[form][0], out[CSR][0]), form
+        assert np.array_equal(out[form][1], out[CSR][1]), form
     ref = A.matvec(x.numpy())
-    assert np.max(np.abs(y.numpy() - ref)) <= 1e-13 * np.max(np.abs(ref))
+    assert np.max(np.abs(out[CSR][0] - ref)) <= 1e-13 * np.max(np.abs(ref))
 
 
 def test_variable_coefficients_stay_csr(gpu):
     kappa = 10.0 ** np.random.default_rng(2).uniform(-1, 1, 12 ** 3)
     M = gpu.MAT(P.vardiff3d(12, kappa))
-    assert M.RowClassInfo() == (False, 0, 0)
-    M.SetRowClass(True)  # nothing to switch on
-    assert M.RowClassInfo()[0] is False
+    assert M.RowClassInfo() == (CSR, 0, 0, 0)
+    M.SetRowClass(MASKS)  # nothing to switch on
+    assert M.RowClassInfo()[0] == CSR
+
+
+def test_classes_without_a_common_stencil(gpu):
+    """A Neumann-like boundary (diagonal differs on boundary rows) has few classes but no
+    single value per offset: classes are built, masks are not."""
+    A = P.poisson2d(30)
+    vals = A.values.copy()
+    diag = np.array([A.rowPtr[i] + np.nonzero(A.colInd[A.rowPtr[i]:A.rowPtr[i + 1]] == i)[0][0]
+                     for i in range(A.nrow)])
+    cnt = np.diff(A.rowPtr.astype(np.int64))
+    vals[diag] = cnt - 1.0  # diagonal = number of neighbours
+    B = P.CSRMatrix(A.nrow, A.mcol, A.rowPtr, A.colInd, vals)
+    M = gpu.MAT(B)
+    mode, classes, _, st = M.RowClassInfo()
+    assert mode == CLASSES and classes > 1 and st == 0
+    x = gpu.DVec.from_numpy(np.random.default_rng(3).standard_normal(B.nrow))
+    y1, y0 = gpu.DVec(B.nrow), gpu.DVec(B.nrow)
+    M.Apply(x, y1)
+    M.SetRowClass(CSR)
+    M.Apply(x, y0)
+    assert np.array_equal(y1.numpy(), y0.numpy())
 
 
 @pytest.mark.parametrize("alg,prec", [("cg", "FP64"), ("cg", "MIXED_RELIABLE"),
                                       ("bicgstab", "FP64"), ("gmres", "FP64"),
                                       ("fgmres", "MIXED")])
-def test_solves_identical_with_and_without_row_classes(gpu, alg, prec):
+def test_solves_identical_in_every_form(gpu, alg, prec):
     from faspxx_b200 import capi
     A = P.convdiff3d(14, 0.1) if alg != "cg" else P.poisson3d(18)
     b = A.matvec(np.random.default_rng(4).uniform(-1, 1, A.nrow))
     out = []
-    for rc in (True, False):
+    for form in (MASKS, CLASSES, CSR):
         M = gpu.MAT(A)
-        M.SetRowClass(rc)
+        M.SetRowClass(form)
         s = gpu.configure(alg, maxIter=2000, relTol=1e-9, absTol=0.0, pcd="jacobi",
                           pcdWeight=2.0 / 3.0 if alg != "cg" else 1.0, pcdIter=1)
         if prec != "FP64":
@@ -80,8 +107,8 @@ def test_solves_identical_with_and_without_row_classes(gpu, alg, prec):
         s.Setup(M)
         x = np.zeros(A.nrow)
         code = s.Solve(b, x)
-        out.append((code, s.GetIterations(), x, s.History()))
-    (c1, i1, x1, h1), (c2, i2, x2, h2) = out
-    assert c1 == c2 == 0 and i1 == i2
-    assert np.array_equal(x1, x2)
-    assert np.array_equal(np.nan_to_num(h1), np.nan_to_num(h2))
+        out.append((code, s.GetIterations(), x, np.nan_to_num(s.History())))
+    for o in out[1:]:
+        assert o[0] == out[0][0] == 0 and o[1] == out[0][1]
+        assert np.array_equal(o[2], out[0][2])
+        assert np.array_equal(o[3], out[0][3])
