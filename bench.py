@@ -644,6 +644,7 @@ def run_adjoint(args):
             f = s.LastTimeMs()
             x = dx.numpy()
             dg.set(x - xt)
+            dlam.Scale(0.0)  # lambda0 = 0
             lib.fasp_gpu_synchronize()
             capi.check(lib.fasp_gpu_solver_solve_adjoint(s.h, dg.ptr, dlam.ptr, C.byref(info)),
                        "adjoint")

@@ -1,0 +1,467 @@
+// bicgstab.cu -- kernels and engine of the device-driven BiCGStab (see bicgstab.cuh).
+//
+// The scalar part of BiCGStab::Solve runs on one thread at the end of each fused kernel's
+// deterministic grid reduction, on the control block in device memory. The branches that need
+// vector work the four kernels do not do -- the safe-guard copy (BiCGStab.cxx:133), the
+// stagnation check with its true residual and restart (:141-162) and the false-convergence
+// check (:164-175) -- set status = kEsc; the host finishes them and relaunches bi_resume.
+// Operand order of every update follows the reference's VEC calls (WAXPBY is
+// fma(a, v1, b * v2), XPAY with a = 1 is fma(1, y, x)), and a Jacobi sweep from zero is
+// diagInv .* v, which is what Jacobi::Solve computes from a zero guess.
+#include <cstring>
+#include <utility>
+
+#include "bicgstab.cuh"
+
+namespace fb {
+
+#define GRID_STRIDE(i, n) \
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)(n); \
+         i += (size_t)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void bi_rec(BiCtl* c, unsigned k, double v)
+{
+    const unsigned g = k + c->histOffset;
+    if (c->hist && g < c->histCap) c->hist[g] = v * c->histScale;
+}
+
+__device__ __forceinline__ void bi_done(BiCtl* c, int code)
+{
+    c->code = code;
+    c->status = kDone;
+}
+
+__device__ __forceinline__ void bi_esc(BiCtl* c, int reason, int phase, const double* red)
+{
+    for (int k = 0; k < 5; ++k) c->red[k] = red[k];
+    c->reason = reason;
+    c->phase = phase;
+    c->status = kEsc;
+}
+
+// Loop top (BiCGStab.cxx:79-87), ++numIter, rjr0star and alpha (:88-102).
+// t = {(ptmp, r0*), (rj, r0*), (rj, rj)}.
+__device__ void bi_after_p(BiCtl* c, const double* t)
+{
+    if (c->numIter >= c->maxIter) {
+        bi_done(c, c->code);
+        return;
+    }
+    if (c->numIter == c->minIter) {
+        const double resAbs = sqrt(t[2]);
+        c->resAbs = resAbs;
+        c->denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+        c->resRel = resAbs / c->denAbs;
+        bi_rec(c, c->numIter, resAbs);
+        if (c->resRel < c->relTol || resAbs < c->absTol) {
+            bi_done(c, c->code);
+            return;
+        }
+    }
+    c->numIter += 1;
+    c->rjr0star = t[1];
+    c->tmp12 = t[0];
+    if (fabs(t[0]) > 1e-40) {
+        c->alpha = c->rjr0star / t[0];
+    } else {
+        bi_rec(c, c->numIter, c->resAbs);
+        bi_done(c, kErrDivZero);
+    }
+}
+
+// The checks after the update (BiCGStab.cxx:117-175) from `phase` on, then beta (:177-183).
+// red = {(r,r), (r,r0*), max|x|, (p,p), (x,x)}.
+__device__ void bi_checks(BiCtl* c, const double* red, int phase)
+{
+    bool stop = false;
+    if (c->numIter >= c->minIter) {
+        if (phase <= 0) {
+            c->resAbs = sqrt(red[0]);
+            c->resRel = c->resAbs / c->denAbs;
+            c->ratio = c->resAbs / c->resAbsOld;
+            if (c->numIter >= c->savIter && c->resAbs < c->resAbsOld) {
+                bi_esc(c, kBiSave, 1, red);
+                return;
+            }
+        }
+        if (phase <= 1 && c->ratio > kKsmChkRatio && c->numIter > c->minIter) {
+            if (red[2] < c->solStagTol) {
+                c->code = kErrSolStag;
+                stop = true;
+            } else {
+                const double xRelDiff = fabs(c->alpha) * sqrt(red[3]) / sqrt(red[4]);
+                if (c->stagStep <= kMaxStagNum && xRelDiff < c->solStagTol) {
+                    bi_esc(c, kBiStag, 2, red);
+                    return;
+                }
+            }
+        }
+        if (phase <= 2 && !stop && c->resRel < c->relTol) {
+            bi_esc(c, kBiCheck, 3, red);
+            return;
+        }
+        bi_rec(c, c->numIter, c->resAbs);
+        if (stop) {
+            bi_done(c, c->code);
+            return;
+        }
+    }
+    if (c->numIter < c->maxIter) {
+        c->resAbsOld = c->resAbs;
+        c->rjr0startmp = c->rjr0star;
+        c->rjr0star = red[1];
+        c->beta = c->rjr0star / c->rjr0startmp * c->alpha / c->omega;
+    } else {
+        bi_done(c, c->code);
+    }
+}
+
+// ptmp = D (A pj) with the loop-top sums.
+template <typename T, int L, int JAC>
+__global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict__ pj,
+                                               const T* __restrict__ rj,
+                                               const T* __restrict__ r0s,
+                                               const T* __restrict__ dinv, T* __restrict__ ptmp,
+                                               BiCtl* c, Scratch s)
+{
+    if (c->status != kRun) return;
+    T a0 = 0, a1 = 0, a2 = 0;
+    auto own = [&](size_t row, T ap) {
+        const T pt = JAC ? ap * dinv[row] : ap;
+        ptmp[row] = pt;
+        const T r = rj[row], r0 = r0s[row];
+        a0 = fma(pt, r0, a0);
+        a1 = fma(r, r0, a1);
+        a2 = fma(r, r, a2);
+    };
+    auto xv = [&](uint32_t j) { return pj[j]; };
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x)
+            own(row, row_apply<T, false>(A, row, xv));
+    } else {
+        const int lane = threadIdx.x & (L - 1);
+        const size_t warpRows = 32 / L;
+        const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+        const size_t sub = (threadIdx.x & 31) / L;
+        for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+            const size_t row = base + sub;
+            T sum = T(0);
+            if (row < A.nrow)
+                for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
+                    sum = fma(A.val[k], pj[A.colInd[k]], sum);
+            sum = group_sum<L>(sum);
+            if (lane == 0 && row < A.nrow) own(row, sum);
+        }
+    }
+    double a[3] = {(double)a0, (double)a1, (double)a2};
+    const int ops[3] = {kSum, kSum, kSum};
+    grid_reduce<3>(a, ops, s, [=] __device__(const double* t) {
+        if (!c->bench) bi_after_p(c, t);
+    });
+}
+
+// sj = rj - alpha ptmp (on the fly for the gathers, stored for the owned rows),
+// stmp = D (A sj), omega = (stmp, sj) / (stmp, stmp)  (BiCGStab.cxx:103-113).
+template <typename T, int L, int JAC>
+__global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict__ rj,
+                                               const T* __restrict__ ptmp,
+                                               const T* __restrict__ dinv, T* __restrict__ sj,
+                                               T* __restrict__ stmp, BiCtl* c, Scratch s)
+{
+    if (c->status != kRun) return;
+    const T nalpha = (T)(-c->alpha);
+    auto sv = [&](uint32_t j) { return fma(T(1), rj[j], nalpha * ptmp[j]); };
+    T a0 = 0, a1 = 0;
+    auto own = [&](size_t row, T as) {
+        const T sjv = sv((uint32_t)row);
+        sj[row] = sjv;
+        const T st = JAC ? as * dinv[row] : as;
+        stmp[row] = st;
+        a0 = fma(st, sjv, a0);
+        a1 = fma(st, st, a1);
+    };
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x)
+            own(row, row_apply<T, false>(A, row, sv));
+    } else {
+        const int lane = threadIdx.x & (L - 1);
+        const size_t warpRows = 32 / L;
+        const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+        const size_t sub = (threadIdx.x & 31) / L;
+        for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+            const size_t row = base + sub;
+            T sum = T(0);
+            if (row < A.nrow)
+                for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
+                    sum = fma(A.val[k], sv(A.colInd[k]), sum);
+            sum = group_sum<L>(sum);
+            if (lane == 0 && row < A.nrow) own(row, sum);
+        }
+    }
+    double a[2] = {(double)a0, (double)a1};
+    const int ops[2] = {kSum, kSum};
+    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+        if (!c->bench) c->omega = t[0] / t[1];
+    });
+}
+
+// x += alpha D pj + omega D sj, rj = sj - omega stmp, then the checks (BiCGStab.cxx:114-183).
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T* __restrict__ rj,
+                                               const T* __restrict__ pj,
+                                               const T* __restrict__ sj,
+                                               const T* __restrict__ stmp,
+                                               const T* __restrict__ r0s,
+                                               const T* __restrict__ dinv, BiCtl* c, Scratch s)
+{
+    if (c->status != kRun) return;
+    const T alpha = (T)c->alpha, omega = (T)c->omega, nomega = (T)(-c->omega);
+    T rr = 0, rr0 = 0, xm = 0, pp = 0, xx = 0;
+    GRID_STRIDE(i, n)
+    {
+        const T p = pj[i], sv = sj[i];
+        const T mp = JAC ? p * dinv[i] : p;
+        const T ms = JAC ? sv * dinv[i] : sv;
+        const T tmp = fma(alpha, mp, omega * ms);
+        const T xi = fma(T(1), x[i], tmp);
+        const T r = fma(T(1), sv, nomega * stmp[i]);
+        x[i] = xi;
+        rj[i] = r;
+        rr = fma(r, r, rr);
+        rr0 = fma(r, r0s[i], rr0);
+        xm = fmax(xm, fabs(xi));
+        pp = fma(p, p, pp);
+        xx = fma(xi, xi, xx);
+    }
+    double a[5] = {(double)rr, (double)rr0, (double)xm, (double)pp, (double)xx};
+    const int ops[5] = {kSum, kSum, kMax, kSum, kSum};
+    grid_reduce<5>(a, ops, s, [=] __device__(const double* t) {
+        if (!c->bench) bi_checks(c, t, 0);
+    });
+}
+
+// pj = rj + beta (pj - omega ptmp)  (BiCGStab.cxx:184-185)
+template <typename T>
+__global__ void __launch_bounds__(kBlock) bi_dir(uint32_t n, T* __restrict__ pj,
+                                                 const T* __restrict__ rj,
+                                                 const T* __restrict__ ptmp, const BiCtl* c)
+{
+    if (c->status != kRun) return;
+    const T beta = (T)c->beta, nomega = (T)(-c->omega);
+    GRID_STRIDE(i, n)
+    {
+        const T tmp = fma(T(1), pj[i], nomega * ptmp[i]);
+        pj[i] = fma(T(1), rj[i], beta * tmp);
+    }
+}
+
+// After the host finished an escalated branch (rj may have been recomputed and pj zeroed):
+// the two sums of rj, then the checks continue at c->phase.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) bi_resume(uint32_t n, const T* __restrict__ rj,
+                                                    const T* __restrict__ r0s, BiCtl* c,
+                                                    Scratch s)
+{
+    T rr = 0, rr0 = 0;
+    GRID_STRIDE(i, n)
+    {
+        rr = fma(rj[i], rj[i], rr);
+        rr0 = fma(rj[i], r0s[i], rr0);
+    }
+    double a[2] = {(double)rr, (double)rr0};
+    const int ops[2] = {kSum, kSum};
+    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+        const double red[5] = {t[0], t[1], c->red[2], c->red[3], c->red[4]};
+        c->status = kRun;
+        c->reason = kBiNone;
+        bi_checks(c, red, c->phase);
+    });
+}
+
+// ---- engine ------------------------------------------------------------------------------
+
+template <typename T>
+static CSRView<T> bi_view(const Mat& A);
+template <>
+CSRView<double> bi_view<double>(const Mat& A) { return A.v64(); }
+template <>
+CSRView<float> bi_view<float>(const Mat& A) { return A.v32(); }
+
+template <typename T>
+int BiEngine<T>::launch_iter()
+{
+    const CSRView<T> V = bi_view<T>(*A);
+    const int L = A->lanes;
+    const long long rows = (long long)n * L;
+    const int needS = c->grid(rows, kBlock);
+    const int needV = c->grid(n, kBlock);
+    auto fit = [&](const void* k, int need) { return std::min(need, resident_grid(*c, k, kBlock)); };
+#define BI_SPMV(KP, KS, LL, JJ)                                                            \
+    do {                                                                                   \
+        KP<T, LL, JJ><<<fit((const void*)KP<T, LL, JJ>, needS), kBlock, 0, c->stream>>>(   \
+            V, pj, rj, r0s, dinv, ptmp, ctl, c->red);                                      \
+        KS<T, LL, JJ><<<fit((const void*)KS<T, LL, JJ>, needS), kBlock, 0, c->stream>>>(   \
+            V, rj, ptmp, dinv, sj, stmp, ctl, c->red);                                     \
+    } while (0)
+#define BI_LANES(JJ)                                                                       \
+    switch (L) {                                                                           \
+        case 1: BI_SPMV(bi_p, bi_s, 1, JJ); break;                                         \
+        case 2: BI_SPMV(bi_p, bi_s, 2, JJ); break;                                         \
+        case 4: BI_SPMV(bi_p, bi_s, 4, JJ); break;                                         \
+        case 8: BI_SPMV(bi_p, bi_s, 8, JJ); break;                                         \
+        case 16: BI_SPMV(bi_p, bi_s, 16, JJ); break;                                       \
+        default: BI_SPMV(bi_p, bi_s, 32, JJ); break;                                       \
+    }
+    if (jacobi) {
+        BI_LANES(1)
+        bi_x<T, 1><<<fit((const void*)bi_x<T, 1>, needV), kBlock, 0, c->stream>>>(
+            n, x, rj, pj, sj, stmp, r0s, dinv, ctl, c->red);
+    } else {
+        BI_LANES(0)
+        bi_x<T, 0><<<fit((const void*)bi_x<T, 0>, needV), kBlock, 0, c->stream>>>(
+            n, x, rj, pj, sj, stmp, r0s, dinv, ctl, c->red);
+    }
+#undef BI_LANES
+#undef BI_SPMV
+    bi_dir<T><<<fit((const void*)bi_dir<T>, needV), kBlock, 0, c->stream>>>(n, pj, rj, ptmp,
+                                                                             ctl);
+    if (!capturing) c->launches += 4;
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int BiEngine<T>::launch_resume()
+{
+    ++c->launches;
+    bi_resume<T><<<c->grid(n, kBlock), kBlock, 0, c->stream>>>(n, rj, r0s, ctl, c->red);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int BiEngine<T>::push_ctl()
+{
+    FB_CUDA(cudaMemcpyAsync(ctl, hctl, sizeof(BiCtl), cudaMemcpyHostToDevice, c->stream));
+    return kOk;
+}
+
+template <typename T>
+int BiEngine<T>::pull_ctl()
+{
+    FB_CUDA(cudaMemcpyAsync(hctl, ctl, sizeof(BiCtl), cudaMemcpyDeviceToHost, c->stream));
+    FB_CUDA(cudaStreamSynchronize(c->stream));
+    return kOk;
+}
+
+template <typename T>
+int BiEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph)
+{
+    c = ctx;
+    A = M;
+    n = M->nrow;
+    jacobi = jac;
+    dinv = dinvv;
+    useGraph = graph;
+    const size_t bytes = ((size_t)n + 4) * sizeof(T);
+    T** vecs[] = {&x, &rj, &r0s, &pj, &ptmp, &sj, &stmp};
+    for (T** v : vecs)
+        if (cudaMalloc(v, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            destroy();
+            return kErrAlloc;
+        }
+    if (cudaMalloc(&ctl, sizeof(BiCtl)) || cudaMallocHost(&hctl, sizeof(BiCtl)) ||
+        cudaMallocHost(&hstatus, sizeof(int))) {
+        cudaGetLastError();
+        destroy();
+        return kErrAlloc;
+    }
+    std::memset(hctl, 0, sizeof(BiCtl));
+    hctl->histScale = 1.0;
+    if (useGraph) {
+        cudaGraph_t g;
+        FB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        for (int i = 0; i < itersPerGraph; ++i) launch_iter();
+        capturing = false;
+        cudaMemcpyAsync(hstatus, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        FB_CUDA(cudaStreamEndCapture(c->stream, &g));
+        FB_CUDA(cudaGraphInstantiate(&gexec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    return kOk;
+}
+
+template <typename T>
+void BiEngine<T>::destroy()
+{
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    T** vecs[] = {&x, &rj, &r0s, &pj, &ptmp, &sj, &stmp};
+    for (T** v : vecs) {
+        cudaFree(*v);
+        *v = nullptr;
+    }
+    cudaFree(ctl);
+    ctl = nullptr;
+    if (hctl) cudaFreeHost(hctl);
+    if (hstatus) cudaFreeHost(hstatus);
+    hctl = nullptr;
+    hstatus = nullptr;
+}
+
+// Two graph launches in flight; after each completes its status word says whether to go on.
+template <typename T>
+int BiEngine<T>::run(unsigned* launches)
+{
+    if (!useGraph) {
+        for (;;) {
+            for (int i = 0; i < itersPerGraph; ++i) {
+                int e = launch_iter();
+                if (e) return e;
+            }
+            FB_CUDA(cudaMemcpyAsync(hstatus, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost,
+                                    c->stream));
+            FB_CUDA(cudaStreamSynchronize(c->stream));
+            if (launches) *launches += 4 * itersPerGraph;
+            if (*hstatus != kRun) return kOk;
+        }
+    }
+    cudaEvent_t ev[2];
+    FB_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    FB_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    *hstatus = kRun;
+    int cur = 0;
+    FB_CUDA(cudaGraphLaunch(gexec, c->stream));
+    FB_CUDA(cudaEventRecord(ev[cur], c->stream));
+    int err = kOk;
+    for (;;) {
+        if (cudaGraphLaunch(gexec, c->stream) != cudaSuccess ||
+            cudaEventRecord(ev[cur ^ 1], c->stream) != cudaSuccess) {
+            err = kErrCuda;
+            break;
+        }
+        if (launches) *launches += 4 * itersPerGraph;
+        if (cudaEventSynchronize(ev[cur]) != cudaSuccess) {
+            err = kErrCuda;
+            break;
+        }
+        if (*hstatus != kRun) break;
+        cur ^= 1;
+    }
+    if (launches) *launches += 4 * itersPerGraph;
+    cudaStreamSynchronize(c->stream);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return err;
+}
+
+template struct BiEngine<double>;
+template struct BiEngine<float>;
+
+} // namespace fb

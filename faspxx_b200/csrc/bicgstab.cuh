@@ -1,0 +1,65 @@
+// bicgstab.cuh -- device-driven BiCGStab (BiCGStab::Solve, src/BiCGStab.cxx:68-270) for FP64
+// and for the FP32 inner solves of mixed-precision refinement, with an Identity or one-sweep
+// Jacobi preconditioner fused into the kernels.
+#pragma once
+
+#include "cg.cuh"
+
+namespace fb {
+
+enum BiReason { kBiNone = 0, kBiSave = 1, kBiStag = 2, kBiCheck = 3 };
+
+// The locals of BiCGStab::Solve (BiCGStab.cxx:70-82) and the parameters it reads, in device
+// memory so that the finalize thread of each fused kernel runs the reference's control flow.
+struct BiCtl {
+    int      status, reason, code, phase;
+    int      bench;     // 1: kernel timing, the finalize steps do nothing
+    unsigned numIter, minIter, maxIter, savIter, restart, stagStep, moreStep;
+    double   relTol, absTol, solStagTol;
+    double   resAbs, resRel, denAbs, ratio, resAbsOld;
+    double   alpha, omega, beta, rjr0star, rjr0startmp, tmp12;
+    double   red[5];    // (r,r), (r,r0*), max|x|, (p,p), (x,x) of the last update kernel
+    double*  hist;
+    unsigned histCap;
+    unsigned histOffset;
+    double   histScale;
+};
+
+// One iteration is four kernels (Jacobi from zero is a diagonal scaling, D = weight/diag):
+//   bi_p      ptmp = D A pj, with (ptmp, r0*), (rj, r0*) and (rj, rj)      (CG.cxx-style
+//             loop top, BiCGStab.cxx:79-102)
+//   bi_s      sj = rj - alpha ptmp formed on the fly, stmp = D A sj, with (stmp, sj) and
+//             (stmp, stmp)                                                  (:103-113)
+//   bi_x      x += alpha D pj + omega D sj, rj = sj - omega stmp, with (r,r), (r,r0*), max|x|,
+//             (p,p), (x,x) and the checks of :117-175                        (:114-175)
+//   bi_dir    pj = rj + beta (pj - omega ptmp)                              (:177-186)
+template <typename T>
+struct BiEngine {
+    Ctx*       c = nullptr;
+    const Mat* A = nullptr;
+    int        jacobi = 0;
+    const T*   dinv = nullptr;
+    T *x = nullptr, *rj = nullptr, *r0s = nullptr, *pj = nullptr, *ptmp = nullptr,
+      *sj = nullptr, *stmp = nullptr;
+    BiCtl*     ctl = nullptr;     // device
+    BiCtl*     hctl = nullptr;    // pinned host copy
+    int*       hstatus = nullptr; // pinned, written at the end of every graph launch
+    cudaGraphExec_t gexec = nullptr;
+    int        itersPerGraph = 8;
+    bool       useGraph = true;
+    bool       capturing = false;
+    uint32_t   n = 0;
+
+    int  init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph);
+    void destroy();
+    int  run(unsigned* launches);
+    int  launch_iter();
+    int  launch_resume();
+    int  push_ctl();
+    int  pull_ctl();
+};
+
+extern template struct BiEngine<double>;
+extern template struct BiEngine<float>;
+
+} // namespace fb

@@ -166,13 +166,21 @@ __device__ void cg_after_refresh(CGCtl* c, const double* t)
     c->refreshes += 1;
     c->reason = kNoReason;
     const bool conv = rn / c->den64 < c->relTol || rn < c->absTol;
-    if (conv || !isfinite(rn)) {
+    // three refreshes in a row without real progress: the tolerance is below what FP32
+    // iterations with FP64 refreshes attain here (ERROR_SOLVER_TOLSMALL)
+    c->stall = rn > sqrt(c->delta) * c->resPrev ? c->stall + 1 : 0;
+    c->resPrev = rn;
+    if (conv || !isfinite(rn) || c->stall >= 3) {
         c->converged = conv ? 1 : 0;
         cg_rec(c, c->numIter, rn / c->histScale);
-        cg_done(c, kOk);
+        cg_done(c, conv ? kOk : kErrTolSmall);
         return;
     }
     c->status = kRun;
+    // A refreshed residual far above the recursive one (a start at the rounding floor, or
+    // FP32 drift) carries none of the Krylov space p was built for: beta would be huge and
+    // p would swamp it, so the direction restarts from z (p = z).
+    if (rn / c->histScale > 4.0 * c->resAbs) c->pzero = 1;
     c->rmax = sqrt(t[1]);
     const double red[5] = {t[1], t[2], 0.0, 0.0, 0.0};
     cg_checks(c, red, 1);
@@ -294,12 +302,12 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     T* __restrict__ pNew = par ? P0 : P1;
     T acc = T(0);
     if (L == 1) { // thread per row
+        auto pv = [&](uint32_t j) { return mode ? fma(beta, pOld[j], z[j]) : z[j]; };
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += (size_t)gridDim.x * blockDim.x) {
-            const T sum = row_apply<T, false>(A, row, [&](uint32_t j) {
-                return mode ? fma(beta, pOld[j], z[j]) : z[j];
-            });
-            const T pi = mode ? fma(beta, pOld[row], z[row]) : z[row];
+             row += stride) {
+            const T sum = row_apply<T, false>(A, row, pv);
+            const T pi = pv((uint32_t)row);
             pNew[row] = pi;
             q[row] = sum;
             acc = fma(sum, pi, acc);

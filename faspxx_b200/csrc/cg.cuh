@@ -39,7 +39,8 @@ struct CGCtl {
     int      devRefresh;
     int      converged;
     unsigned refreshes;
-    double   den64, res64;
+    unsigned stall;     // consecutive refreshes whose FP64 residual fell by less than sqrt(delta)
+    double   den64, res64, resPrev;
     const double* rb;   // b
     double*  rx;        // x (FP64)
     double*  rr;        // r = b - A x (FP64), written by each refresh

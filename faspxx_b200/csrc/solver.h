@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/fasp_b200.h"
+#include "bicgstab.cuh"
 #include "cg.cuh"
 #include "internal.h"
 
@@ -72,6 +73,9 @@ struct SolverImpl {
     // device-driven CG
     CGEngine<double>* cg64 = nullptr;
     CGEngine<float>*  cg32 = nullptr;
+    // device-driven BiCGStab (Identity or one Jacobi sweep as preconditioner)
+    BiEngine<double>* bi64 = nullptr;
+    BiEngine<float>*  bi32 = nullptr;
     double*         safe = nullptr;
     double*         dhist = nullptr;
     double*         hostB = nullptr;  // staging of the host entry point
@@ -95,6 +99,9 @@ struct SolverImpl {
     int cg_reliable(const double* b, double* x, fasp_gpu_info* info);
     template <typename T>
     int bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P, Space<T> S);
+    template <typename T>
+    int bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info* info,
+                        const fasp_gpu_params& P, Space<T> S);
     template <typename T>
     int gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
                     Space<T> S, bool flexible);

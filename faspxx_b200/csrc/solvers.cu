@@ -224,7 +224,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             }
             break;
         }
-        case FASP_GPU_BICGSTAB:
+        case FASP_GPU_BICGSTAB: {
             if (cfg.precision == FASP_GPU_MIXED) {
                 // FP64: the outer residual; FP32: the inner solve's 12 vectors + b, e
                 if ((e = alloc_vecs(w, 1, n)) || (e = alloc_vecs(w32, 14, n))) return e;
@@ -232,7 +232,21 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             } else if ((e = alloc_vecs(w, 12, n))) {
                 return e;
             }
+            // Identity or one Jacobi sweep from zero: the device-driven engine
+            const bool fusable = A->val && (cfg.pcd == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
+            if (fusable) {
+                dhistCap = cfg.prm.maxIter + 2;
+                if (cudaMalloc(&dhist, (size_t)dhistCap * 8) != cudaSuccess) return kErrAlloc;
+                if (cfg.precision == FASP_GPU_MIXED) {
+                    bi32 = new BiEngine<float>();
+                    if ((e = bi32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
+                } else {
+                    bi64 = new BiEngine<double>();
+                    if ((e = bi64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
+                }
+            }
             break;
+        }
         case FASP_GPU_GMRES:
         case FASP_GPU_FGMRES: {
             // GMRES::Setup (GMRES.cxx:38-88) / FGMRES::Setup (FGMRES.cxx:23-80)
@@ -352,6 +366,16 @@ void SolverImpl::destroy()
         cg32->destroy();
         delete cg32;
         cg32 = nullptr;
+    }
+    if (bi64) {
+        bi64->destroy();
+        delete bi64;
+        bi64 = nullptr;
+    }
+    if (bi32) {
+        bi32->destroy();
+        delete bi32;
+        bi32 = nullptr;
     }
     if (adj) {
         adj->destroy();
@@ -710,9 +734,10 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
     double rn = 0.0;
     if ((e = true_res(&rn))) return e;
     const double den = (kCloseZero > rn) ? kCloseZero : rn;
+    double hostPrev = den;
     patches.push_back({0u, rn});
     int code = kOk;
-    uint32_t iters = 0, refreshes = 0, hostRefreshes = 0;
+    uint32_t iters = 0, refreshes = 0, hostRefreshes = 0, hostStall = 0;
     bool converged = rn / den < P.relTol || rn < P.absTol;
     if (!converged && std::isfinite(rn) && P.maxIter > 0) {
         const double s = rn;
@@ -734,6 +759,7 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
         // graph and plain engines refresh inside their kernels; the persistent one escalates
         h.devRefresh = E.persistent ? 0 : 1;
         h.den64 = den;
+        h.resPrev = den;
         h.rb = b;
         h.rx = x64;
         h.rr = r64;
@@ -758,6 +784,11 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
                 converged = true;
                 break;
             }
+            if (h.status == kDone && h.code == kErrTolSmall) { // refreshes stopped gaining
+                rn = h.res64;
+                code = kErrTolSmall;
+                break;
+            }
             // a host refresh: the stop test or delta reached (persistent engine), or the end
             // of the FP32 run (maxIter, breakdown)
             if ((e = update_from32(c, n, s, E.x, x64)) || (e = set32(c, n, E.x))) return e;
@@ -765,11 +796,16 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
             ++hostRefreshes;
             patches.push_back({h.numIter, rn});
             converged = rn / den < P.relTol || rn < P.absTol;
-            if (h.status == kDone || converged || !std::isfinite(rn) || guard > P.maxIter) {
+            hostStall = rn > std::sqrt(delta) * hostPrev ? hostStall + 1 : 0;
+            hostPrev = rn;
+            if (!converged && hostStall >= 3) code = kErrTolSmall;
+            if (h.status == kDone || converged || !std::isfinite(rn) || guard > P.maxIter ||
+                code != kOk) {
                 if (h.status == kDone && h.code != kOk) code = h.code;
                 break;
             }
             if ((e = convert_scaled(c, n, r64, 1.0 / s, E.r))) return e;
+            if (rn / s > 4.0 * h.resAbs) h.pzero = 1; // see cg_after_refresh
             h.rmax = rn / s;
             h.phase = 1;
             if ((e = E.push_ctl()) || (e = E.launch_resume()) || (e = E.pull_ctl())) return e;
@@ -800,6 +836,11 @@ template <typename T>
 int SolverImpl::bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P,
                          Space<T> S)
 {
+    if constexpr (std::is_same<T, double>::value) {
+        if (bi64) return bicgstab_engine(*bi64, b, x, info, P, S);
+    } else {
+        if (bi32) return bicgstab_engine(*bi32, b, x, info, P, S);
+    }
     std::vector<T*>& w = *S.w;
     T *r0star = w[0], *tmp = w[1], *apj = w[2], *asj = w[3], *pj = w[4], *rj = w[5],
       *sj = w[6], *ptmp = w[7], *stmp = w[8], *ms = w[9], *mp = w[10], *sv = w[11];
@@ -928,6 +969,113 @@ int SolverImpl::bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_p
     }
     if (numIter > P.savIter) v_copy(c, n, sv, x);
     FB_CUDA(cudaStreamSynchronize(c.stream));
+    return kOk;
+}
+
+// Device-driven BiCGStab: the same control flow as bicgstab() above, run by the kernels of
+// bicgstab.cu; the host finishes the branches they escalate (BiCGStab.cxx references).
+template <typename T>
+int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info* info,
+                                const fasp_gpu_params& P, Space<T> S)
+{
+    BiCtl& h = *E.hctl;
+    T* sv = (*S.w)[11];
+    std::vector<std::pair<uint32_t, double>> patches; // raw values, recorded through rec()
+    int e;
+    // BiCGStab.cxx:70-78: rj = b - A x, r0star = rj, pj = rj
+    v_copy(c, n, (const T*)x, E.x);
+    if ((e = m_spmv(c, *A, (const T*)E.x, E.ptmp))) return e;
+    v_waxpby(c, n, Scal::h(1.0), b, Scal::h(-1.0), (const T*)E.ptmp, E.rj);
+    v_copy(c, n, (const T*)E.rj, E.r0s);
+    v_copy(c, n, (const T*)E.rj, E.pj);
+    std::memset(&h, 0, sizeof(BiCtl));
+    h.status = P.maxIter > 0 ? kRun : kDone;
+    h.code = kOk;
+    h.minIter = P.minIter;
+    h.maxIter = P.maxIter;
+    h.savIter = P.savIter;
+    h.restart = P.restart;
+    h.relTol = P.relTol;
+    h.absTol = P.absTol;
+    h.solStagTol = 1e-4 * P.relTol;
+    h.resAbs = h.resRel = h.denAbs = h.resAbsOld = 1.0;
+    h.hist = dhist;
+    h.histCap = dhistCap;
+    h.histOffset = histOff;
+    h.histScale = histScale;
+    ++c.launches;
+    k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    if ((e = E.push_ctl())) return e;
+    unsigned launches = 0;
+    info->escalations = 0;
+    auto true_res = [&]() { // rj = b - A x, resAbs, resRel (BiCGStab.cxx:146-149, 166-169)
+        apply_residual(c, *A, b, (const T*)E.x, E.rj);
+        v_norm2(c, n, (const T*)E.rj, c.dslot + SL_T1);
+        h.resAbs = fetch(c.dslot + SL_T1);
+        h.resRel = h.resAbs / h.denAbs;
+    };
+    for (uint32_t guard = 0; h.status != kDone; ++guard) {
+        if (h.status == kRun) {
+            if ((e = E.run(&launches)) || (e = E.pull_ctl())) return e;
+            c.launches += launches;
+            launches = 0;
+            continue;
+        }
+        info->escalations++;
+        bool stop = false;
+        if (h.reason == kBiSave) { // :133
+            v_copy(c, n, (const T*)E.x, sv);
+        } else if (h.reason == kBiStag) { // :144-162
+            true_res();
+            if (h.resRel < P.relTol || h.resAbs < P.absTol) {
+                stop = true;
+            } else if (h.stagStep >= kMaxStagNum) {
+                h.code = kErrStag;
+                stop = true;
+            } else {
+                v_set(c, n, 0.0, E.pj);
+                ++h.stagStep;
+            }
+        } else if (h.reason == kBiCheck) { // :164-175
+            true_res();
+            if (h.resRel < P.relTol || h.resAbs < P.absTol) {
+                stop = true;
+            } else if (h.moreStep >= P.restart) {
+                h.code = kErrTolSmall;
+                stop = true;
+            } else {
+                v_set(c, n, 0.0, E.pj);
+                ++h.moreStep;
+            }
+        }
+        if (stop) { // rec(numIter, resAbs) and leave the loop (:176-177)
+            patches.push_back({h.numIter, h.resAbs});
+            h.status = kDone;
+            if ((e = E.push_ctl())) return e;
+            break;
+        }
+        h.status = kRun;
+        if ((e = E.push_ctl()) || (e = E.launch_resume()) || (e = E.pull_ctl())) return e;
+        if (guard > P.maxIter + 64) return kErrCuda; // cannot happen: each pass advances
+    }
+    info->numIter = h.numIter;
+    info->code = h.code;
+    if (!(h.numIter == P.minIter && h.numIter == P.maxIter)) {
+        info->norm2 = h.resAbs;
+        v_norminf(c, n, (const T*)E.rj, c.dslot + SL_T2);
+        info->normInf = fetch(c.dslot + SL_T2);
+    }
+    v_copy(c, n, (const T*)E.x, x);
+    if (h.numIter > P.savIter) v_copy(c, n, (const T*)sv, x);
+    // the device recorded scaled entries at histOff + k; the host's through rec()
+    const uint32_t len = std::min<uint32_t>(histOff + h.numIter + 1, dhistCap);
+    std::vector<double> dh(len, kNaN);
+    FB_CUDA(cudaMemcpyAsync(dh.data(), dhist, (size_t)len * 8, cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    if (hist.size() < len) hist.resize(len, kNaN);
+    for (uint32_t k = histOff; k < len; ++k)
+        if (std::isfinite(dh[k])) hist[k] = dh[k];
+    for (auto& pt : patches) rec(pt.first, pt.second);
     return kOk;
 }
 

@@ -24,10 +24,10 @@ __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restri
                                                  T* __restrict__ y)
 {
     if (L == 1) { // thread per row: short rows (stencils)
-        for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.nrow;
-             r += (size_t)gridDim.x * blockDim.x) {
-            y[r] = row_apply<T, PAT>(A, r, [&](uint32_t j) { return x[j]; });
-        }
+        auto xv = [&](uint32_t j) { return x[j]; };
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
+        for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.nrow; r += stride)
+            y[r] = row_apply<T, PAT>(A, r, xv);
         return;
     }
     const int lane = threadIdx.x & (L - 1);

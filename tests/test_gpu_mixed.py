@@ -189,3 +189,19 @@ def test_mixed_precision_rejected_for_stationary_solvers(gpu):
     s.SetPrecision(capi.MIXED_RELIABLE)
     with pytest.raises(capi.FaspError):
         s.Setup(gpu.MAT(A))
+
+
+def test_reliable_stops_below_attainable_accuracy(gpu):
+    """A start already at the rounding floor (x0 = x*): the relative target 1e-10 of a
+    residual that is itself rounding noise cannot be met; the FP64 refreshes stop gaining
+    and the solve ends with ERROR_SOLVER_TOLSMALL long before maxIter."""
+    from faspxx_b200 import capi
+    A = P.poisson3d(24)
+    xs = np.random.default_rng(9).uniform(0, 1, A.nrow)
+    b = A.matvec(xs)
+    s = _solver(gpu, A, capi.MIXED_RELIABLE, relTol=1e-10, maxIter=5000)
+    x = xs.copy()
+    code = s.Solve(b, x)
+    assert code in (0, -34), code
+    assert s.GetIterations() < 1000
+    assert np.max(np.abs(x - xs)) < 1e-10

@@ -30,8 +30,11 @@ RUNS = json.load(open(os.path.join(GOLD, "reference_runs.json")))
 ARR = np.load(os.path.join(GOLD, "reference_runs.npz"))
 CASES = {c["name"]: c for c in G.solver_cases()}
 
-# stopping test at the rounding floor: relTol 1e-17 (see tests/golden/cases.py)
-FLOOR = {"fdm_cg_tolsmall": 8, "fdm_bicgstab_tolsmall": 12}
+# stopping test at the rounding floor: relTol 1e-17 (see tests/golden/cases.py). The run
+# ends in rounding noise: converged, ERROR_SOLVER_TOLSMALL after the false-convergence
+# restarts, or (BiCGStab) the breakdown test |(ptmp, r0*)| <= 1e-40 once the residual of this
+# 100-unknown system has reached zero (ERROR_DIVIDE_ZERO); the true residual is checked.
+FLOOR = {"fdm_cg_tolsmall": (0, -34), "fdm_bicgstab_tolsmall": (0, -34, -18)}
 # BiCGStab on fem_small from x0 = 1, b = 0: the residual norm oscillates by orders of
 # magnitude near the threshold; two reruns of the reference with reordered sums differ too
 ERRATIC = {"fem_bicgstab": 3, "fem_bicgstab_jac": 3}
@@ -173,8 +176,7 @@ def _check_case(gpu, oracle, name, engine="graph"):
         ref = po.solve(b, x0)
         assert ref.code == meta["code"] and ref.iters == meta["iters"]  # oracle pinned
         if name in FLOOR:
-            # converged exactly at the floor, or ERROR_SOLVER_TOLSMALL one restart later
-            assert code in (0, -34), (key, code)
+            assert code in FLOOR[name], (key, code)
         else:
             assert code == meta["code"], (key, code, meta["code"])
         it = s.GetIterations()
