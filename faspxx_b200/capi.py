@@ -38,7 +38,7 @@ class Config(C.Structure):
                 ("leftPrecond", C.c_int), ("precision", C.c_int), ("orth", C.c_int),
                 ("innerRelTol", C.c_double), ("innerMaxIter", C.c_uint32),
                 ("maxOuter", C.c_uint32), ("useGraph", C.c_int), ("persistent", C.c_int),
-                ("overlapLaunch", C.c_int)]
+                ("overlapLaunch", C.c_int), ("fp32Recurrence", C.c_int)]
 
 
 class Info(C.Structure):

@@ -148,6 +148,7 @@ void fasp_gpu_default_config(fasp_gpu_config* cfg, int alg)
     cfg->useGraph = 1;
     cfg->persistent = 0;
     cfg->overlapLaunch = 1;
+    cfg->fp32Recurrence = 1;
 }
 
 // ---- memory ---------------------------------------------------------------------------

@@ -284,7 +284,13 @@ struct V16<double> {
     enum { W = 2 };
 };
 
-template <typename T, int L>
+// REC = 0: q = A p with p = z + beta p_old formed on the fly for every gathered entry (the
+// reference's order: XPAY, then Apply); p is double-buffered.
+// REC = 1 (FP32 iterations of the mixed-precision solves): the recurrence
+// q = A p = A z + beta q_old, so the SpMV gathers z alone and p, q update in place for the
+// owned row (half the gathers). Its rounding differs from A p by a term that beta < 1 damps;
+// the FP64 refreshes of reliable updates correct the residual it feeds.
+template <typename T, int L, int REC>
 __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
                                                   CGCtl* c, Scratch s)
@@ -301,17 +307,31 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
     T acc = T(0);
-    if (L == 1) { // thread per row
-        auto pv = [&](uint32_t j) { return mode ? fma(beta, pOld[j], z[j]) : z[j]; };
-        const size_t stride = (size_t)gridDim.x * blockDim.x;
-        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += stride) {
-            const T sum = row_apply<T, false>(A, row, pv);
-            const T pi = pv((uint32_t)row);
+    // the owned row's p and q from its product `sum`
+    auto own = [&](size_t row, T sum) {
+        const T zi = z[row];
+        if (REC) {
+            const T pi = mode ? fma(beta, P0[row], zi) : zi;
+            const T qi = mode ? fma(beta, q[row], sum) : sum;
+            P0[row] = pi;
+            q[row] = qi;
+            acc = fma(qi, pi, acc);
+        } else {
+            const T pi = mode ? fma(beta, pOld[row], zi) : zi;
             pNew[row] = pi;
             q[row] = sum;
             acc = fma(sum, pi, acc);
         }
+    };
+    auto gv = [&](uint32_t j) {
+        if (REC) return z[j];
+        return mode ? fma(beta, pOld[j], z[j]) : z[j];
+    };
+    if (L == 1) { // thread per row
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += stride)
+            own(row, row_apply<T, false>(A, row, gv));
     }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
@@ -323,24 +343,15 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
         T sum = T(0);
         if (row < A.nrow) {
             const uint32_t b = A.rowPtr[row], e = A.rowPtr[row + 1];
-            for (uint32_t k = b + lane; k < e; k += L) {
-                const uint32_t j = A.colInd[k];
-                const T pj = mode ? fma(beta, pOld[j], z[j]) : z[j];
-                sum = fma(A.val[k], pj, sum);
-            }
+            for (uint32_t k = b + lane; k < e; k += L) sum = fma(A.val[k], gv(A.colInd[k]), sum);
         }
         sum = group_sum<L>(sum);
-        if (lane == 0 && row < A.nrow) {
-            const T pi = mode ? fma(beta, pOld[row], z[row]) : z[row];
-            pNew[row] = pi;
-            q[row] = sum;
-            acc = fma(sum, pi, acc);
-        }
+        if (lane == 0 && row < A.nrow) own(row, sum);
     }
     double a[1] = {(double)acc};
     const int ops[1] = {kSum};
     grid_reduce<1>(a, ops, s, [=] __device__(const double* t) {
-        c->par = par ^ 1;
+        if (!REC) c->par = par ^ 1;
         if (!c->bench) cg_after_spmv(c, t[0]);
     });
 }
@@ -720,14 +731,21 @@ void CGEngine<T>::launch_spmv_kernel()
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red);
     };
-    switch (A->lanes) {
-        case 1: go(cg_spmv<T, 1>); break;
-        case 2: go(cg_spmv<T, 2>); break;
-        case 4: go(cg_spmv<T, 4>); break;
-        case 8: go(cg_spmv<T, 8>); break;
-        case 16: go(cg_spmv<T, 16>); break;
-        default: go(cg_spmv<T, 32>); break;
+#define CG_SPMV_LANES(RR)                                                                  \
+    switch (A->lanes) {                                                                    \
+        case 1: go(cg_spmv<T, 1, RR>); break;                                              \
+        case 2: go(cg_spmv<T, 2, RR>); break;                                              \
+        case 4: go(cg_spmv<T, 4, RR>); break;                                              \
+        case 8: go(cg_spmv<T, 8, RR>); break;                                              \
+        case 16: go(cg_spmv<T, 16, RR>); break;                                            \
+        default: go(cg_spmv<T, 32, RR>); break;                                            \
     }
+    if (recurrence) {
+        CG_SPMV_LANES(1)
+    } else {
+        CG_SPMV_LANES(0)
+    }
+#undef CG_SPMV_LANES
 }
 
 template <typename T>

@@ -73,6 +73,7 @@ struct CGEngine {
     bool       useGraph = true;
     bool       capturing = false;
     bool       pdl = true;      // programmatic dependent launch of the iteration kernels
+    bool       recurrence = false; // q = A z + beta q_old (FP32 engines; p single-buffered)
     uint32_t   n = 0;
     // persistent engine: one cooperative launch runs the iterations
     bool       wantPersistent = true; // set before init

@@ -220,6 +220,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 cg32 = new CGEngine<float>();
                 cg32->wantPersistent = cfg.persistent != 0;
                 cg32->pdl = cfg.overlapLaunch != 0;
+                cg32->recurrence = cfg.fp32Recurrence != 0;
                 if ((e = cg32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
             }
             break;

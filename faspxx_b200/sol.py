@@ -237,6 +237,9 @@ class SOL:
     def SetOverlapLaunch(self, flag: bool):
         self.cfg.overlapLaunch = 1 if flag else 0
 
+    def SetFP32Recurrence(self, flag: bool):
+        self.cfg.fp32Recurrence = 1 if flag else 0
+
     def SetUseGraph(self, flag: bool):
         self.cfg.useGraph = 1 if flag else 0
 

@@ -89,6 +89,9 @@ typedef struct {
     int             overlapLaunch; /* 1 (default): the CG iteration kernels use programmatic
                                     dependent launch, each one's launch overlapping its
                                     predecessor's reduction tail */
+    int             fp32Recurrence; /* MIXED, MIXED_RELIABLE CG: 1 (default) = the FP32
+                                    iterations form q = A p as A z + beta q_old (the SpMV
+                                    gathers one vector); 0 = as the reference, A (z + beta p) */
 } fasp_gpu_config;
 
 /* Outcome of one Solve. */

@@ -208,6 +208,7 @@ public:
     void SetUseGraph(bool on) { cfg_.useGraph = on ? 1 : 0; dirty_ = true; }
     void SetPersistent(bool on) { cfg_.persistent = on ? 1 : 0; dirty_ = true; }
     void SetOverlapLaunch(bool on) { cfg_.overlapLaunch = on ? 1 : 0; dirty_ = true; }
+    void SetFP32Recurrence(bool on) { cfg_.fp32Recurrence = on ? 1 : 0; dirty_ = true; }
     const fasp_gpu_config& Config() const { return cfg_; }
     /* SOL::SetupPCD (SOL.cxx:249): Identity or Jacobi */
     virtual void SetupPCD(SOL& pc) { pc.AsPreconditionerOf(cfg_); dirty_ = true; }

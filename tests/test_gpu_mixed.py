@@ -205,3 +205,32 @@ def test_reliable_stops_below_attainable_accuracy(gpu):
     assert code in (0, -34), code
     assert s.GetIterations() < 1000
     assert np.max(np.abs(x - xs)) < 1e-10
+
+
+@pytest.mark.parametrize("rec", [True, False])
+@pytest.mark.parametrize("name", ["poisson3d_32", "vardiff3d_24"])
+def test_reliable_q_recurrence_and_reference_form(gpu, name, rec):
+    """The FP32 iterations reach the FP64 tolerance in the FP64 iteration count (+5%) both
+    with the q = A z + beta q_old recurrence (default) and with the reference's A (z + beta
+    p) form."""
+    from faspxx_b200 import capi
+    A = _problems()[name]
+    b = A.matvec(np.random.default_rng(21).uniform(0.0, 1.0, A.nrow))
+    ref = _solver(gpu, A, capi.FP64)
+    xr = np.zeros(A.nrow)
+    assert ref.Solve(b, xr) == 0
+    s = gpu.CG()
+    s.SetMaxIter(2000)
+    s.SetRelTol(1e-8)
+    s.SetAbsTol(0.0)
+    pc = gpu.Jacobi()
+    pc.SetMaxIter(1)
+    pc.SetMinIter(1)
+    s.SetupPCD(pc)
+    s.SetPrecision(capi.MIXED_RELIABLE)
+    s.SetFP32Recurrence(rec)
+    s.Setup(gpu.MAT(A))
+    x = np.zeros(A.nrow)
+    assert s.Solve(b, x) == 0
+    assert np.linalg.norm(b - A.matvec(x)) < 1e-8 * np.linalg.norm(b)
+    assert s.GetIterations() <= ref.GetIterations() * 1.05 + 2
