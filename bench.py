@@ -359,7 +359,8 @@ def run_ours(args):
     # per row (the class table stays in L1/L2, the stencil travels as kernel parameters)
     mat32 = 2 * n if rc_on else 8 * nnz + 4 * (n + 1)
     mat64 = 2 * n if rc_on else 12 * nnz + 4 * (n + 1)
-    b_spmv32 = mat32 + 4 * n * 4                     # read z,p_old write p,q
+    # FP32 iterations use q = A z + beta q_old: read z (gathered), p, q; write p, q
+    b_spmv32 = mat32 + 4 * n * 5
     b_upd32 = 4 * n * 5 + 4 * n * 3                 # read p,x,r,q,dinv write x,r,z
     b_spmv64 = mat64 + 8 * n * 4
     b_upd64 = 8 * n * 5 + 8 * n * 3
@@ -381,8 +382,8 @@ def run_ours(args):
         # the dominant kernel of the FP32 iteration: the larger of the two fused kernels
         if km[0] >= km[1]:
             form = {0: "csr", 1: "rowclass", 2: "stencil"}[rc_mode]
-            name = (f"cg_spmv<float> (SpMV + p update + (Ap,p), FP32 CG iteration, {form} "
-                    "matrix form)")
+            name = (f"cg_spmv<float> (w = A z, p = z + beta p, q = w + beta q, (q,p); FP32 CG "
+                    f"iteration, {form} matrix form)")
             byt, ms_k = b_spmv32, km[0]
             key = f"cg_spmv<float>/{form}"
         else:

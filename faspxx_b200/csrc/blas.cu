@@ -224,8 +224,9 @@ constexpr int KC = 8;
 // dres[j] = (V_j, w), j in [j0, j0+k)
 template <typename T>
 __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
-                           const T* __restrict__ w, Scratch s, double* dres)
+                           const T* __restrict__ w, Scratch s, double* dres, const int* stop)
 {
+    if (stop && *stop) return;
     T t[KC];
     double acc[KC];
     int ops[KC];
@@ -252,8 +253,9 @@ __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld
 template <typename T>
 __global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
                             const double* __restrict__ h, double sign, T* __restrict__ w,
-                            Scratch s, double* dnorm)
+                            Scratch s, double* dnorm, const int* stop)
 {
+    if (stop && *stop) return;
     T hj[KC];
 #pragma unroll
     for (int j = 0; j < KC; ++j) hj[j] = j < k ? (T)(sign * h[j]) : T(0);
@@ -273,13 +275,14 @@ __global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t l
 }
 
 template <typename T>
-int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres)
+int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres,
+               const int* stop)
 {
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         ++c.launches;
         k_multidot<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, kk, V + j0 * ld, ld, w,
-                                                                   c.red, dres + j0);
+                                                                   c.red, dres + j0, stop);
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
@@ -287,14 +290,14 @@ int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, dou
 
 template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
-                double sign, T* w, double* dnorm)
+                double sign, T* w, double* dnorm, const int* stop)
 {
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         const bool last = j0 + KC >= k;
         ++c.launches;
         k_multiaxpy<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
-            n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr);
+            n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
@@ -313,9 +316,10 @@ int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* 
     template int v_copy<T>(Ctx&, uint32_t, const T*, T*);                                 \
     template int v_pmult<T>(Ctx&, uint32_t, const T*, T*);                                \
     template int v_add<T>(Ctx&, uint32_t, const T*, T*);                                  \
-    template int v_multidot<T>(Ctx&, uint32_t, int, const T*, size_t, const T*, double*); \
+    template int v_multidot<T>(Ctx&, uint32_t, int, const T*, size_t, const T*, double*,  \
+                               const int*);                                               \
     template int v_multiaxpy<T>(Ctx&, uint32_t, int, const T*, size_t, const double*,     \
-                                double, T*, double*);
+                                double, T*, double*, const int*);
 FB_VEC_INSTANTIATE(double)
 FB_VEC_INSTANTIATE(float)
 #undef FB_VEC_INSTANTIATE

@@ -196,12 +196,14 @@ template <typename T> int v_add(Ctx& c, uint32_t n, const T* d, T* x);          
 int v_recip_scale(Ctx& c, uint32_t n, double w, const double* d, double* out); // out = w*(1/d)
 // Classical Gram-Schmidt blocks over a basis stored at V + j*ld:
 // dres[j] = (V_j, w) for j < k, in one pass over w;
+// A non-null stop (device flag) turns the launches into no-ops once it is set.
 template <typename T>
-int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres);
+int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres,
+               const int* stop = nullptr);
 // w -= sign * sum_j h[j] V_j (h on the device); dnorm (nullable) receives ||w_new||.
 template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
-                double sign, T* w, double* dnorm);
+                double sign, T* w, double* dnorm, const int* stop = nullptr);
 
 // ---- sparse kernels (spmv.cu) ---------------------------------------------------------
 int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,

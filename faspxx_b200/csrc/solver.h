@@ -17,6 +17,19 @@ struct fasp_gpu_mat_s {
 
 namespace fb {
 
+// The in-cycle state of a GMRES restart cycle run without host round trips: k_gmres_givens
+// updates it after every Arnoldi step and sets stop (1: breakdown, 2: converged); the other
+// step kernels return at once when it is set.
+struct GmCtl {
+    int      stop;
+    unsigned count;     // steps of this cycle done, a breakdown step included
+    unsigned numIter, minIter;
+    double   resAbs, denAbs, relTol, absTol;
+    double*  hist;
+    unsigned histCap, histOffset;
+    double   histScale;
+};
+
 // The preconditioner of a solver: Identity (Iter.cxx:16-20) or Jacobi (Iter.cxx:29-112).
 struct Pcd {
     int             type = 0;    // 0 identity, 1 Jacobi
@@ -65,6 +78,8 @@ struct SolverImpl {
     uint32_t        histOff = 0;
     double          histScale = 1.0;
     double*         gm = nullptr;   // device Hessenberg block: hh, hcos, hsin, var, dots
+    GmCtl*          gmc = nullptr;  // device in-cycle state, and its pinned host copy
+    GmCtl*          hgmc = nullptr;
     uint32_t        maxRestart = 0, minRestart = 0, restart = 0;
     // MG (identity transfers): per level smoother and coarse solver, coarse b and x
     std::vector<Pcd> mgSmooth, mgCoarse;
@@ -107,6 +122,7 @@ struct SolverImpl {
                     Space<T> S, bool flexible);
     template <typename T>
     int gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P, Space<T> S);
+    bool gm_device_cycles(bool flexible) const;
     // FP64 iterative refinement around FP32 inner BiCGStab / GMRES / FGMRES solves
     int refine(const double* b, double* x, fasp_gpu_info* info);
     Space<double> sp64() { return Space<double>{&w, V, Z}; }

@@ -286,6 +286,11 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             const size_t gmSize = (m + 1) * m + (m + 1) + m + (m + 1) + 2 * (m + 1) + 4;
             if (cudaMalloc(&gm, gmSize * 8) != cudaSuccess) return kErrAlloc;
             cudaMemset(gm, 0, gmSize * 8);
+            if (cudaMalloc(&gmc, sizeof(GmCtl)) != cudaSuccess ||
+                cudaMallocHost(&hgmc, sizeof(GmCtl)) != cudaSuccess)
+                return kErrAlloc;
+            dhistCap = cfg.prm.maxIter + 2;
+            if (cudaMalloc(&dhist, (size_t)dhistCap * 8) != cudaSuccess) return kErrAlloc;
             break;
         }
         case FASP_GPU_MG: {
@@ -344,6 +349,10 @@ void SolverImpl::destroy()
     cudaFree(V);
     cudaFree(Z);
     cudaFree(gm);
+    cudaFree(gmc);
+    if (hgmc) cudaFreeHost(hgmc);
+    gmc = nullptr;
+    hgmc = nullptr;
     cudaFree(safe);
     cudaFree(dhist);
     cudaFree(hostB);
@@ -1104,16 +1113,23 @@ static GmLayout gm_layout(double* gm, size_t m)
 // GMRES.cxx:168-203 after the dots: hh[j][c1] (CGS2: h1+h2), t = ||w||, then the previous
 // rotations, the new rotation and the updated residual estimate |var[count]|. out[1] = 0
 // when t is not > SMALL_DBL (the reference leaves the restart cycle before rotating).
-__global__ void k_gmres_givens(GmLayout L, int count, int c1, int cgs, const double* tnorm)
+__global__ void k_gmres_givens(GmLayout L, int count, int c1, int cgs, const double* tnorm,
+                               GmCtl* g)
 {
+    if (g && g->stop) return;
     const size_t m = L.m;
 #define HH(i, j) L.hh[(size_t)(i) * m + (j)]
     if (cgs)
         for (int j = 0; j < count; ++j) HH(j, c1) = L.h1[j] + L.h2[j];
     double t = *tnorm;
     HH(count, c1) = t;
+    if (g) { // ++numIter at the top of the step (GMRES.cxx:162)
+        g->numIter += 1;
+        g->count = count;
+    }
     if (!(fabs(t) > kSmallDbl)) {
         L.out[1] = 0.0;
+        if (g) g->stop = 1;
         return;
     }
     L.out[1] = 1.0;
@@ -1132,6 +1148,14 @@ __global__ void k_gmres_givens(GmLayout L, int count, int c1, int cgs, const dou
     L.var[count] = -L.hsin[c1] * L.var[c1];
     L.var[c1] = L.hcos[c1] * L.var[c1];
     L.out[0] = fabs(L.var[count]);
+    if (g) { // GMRES.cxx:205-209: the estimate, its record and the in-cycle stop test
+        const double resAbs = L.out[0];
+        g->resAbs = resAbs;
+        const unsigned k = g->numIter + g->histOffset;
+        if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;
+        if ((resAbs < g->absTol || resAbs / g->denAbs < g->relTol) && g->numIter > g->minIter)
+            g->stop = 2;
+    }
 #undef HH
 }
 
@@ -1173,9 +1197,163 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, co
         v_multiaxpy(c, n, count, V, ld, L.h2, 1.0, wv, tn);
     }
     ++c.launches;
-    k_gmres_givens<<<1, 1, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn);
+    k_gmres_givens<<<1, 1, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn,
+                                          nullptr);
     FB_CUDA(cudaGetLastError());
     v_scale(c, n, Scal::dinv(tn), wv);
+    return kOk;
+}
+
+// ---- restart cycles without host round trips (Identity or one Jacobi sweep, CGS2) -------
+
+bool SolverImpl::gm_device_cycles(bool flexible) const
+{
+    // FGMRES warm-starts its preconditioner from the previous basis Z; MGS keeps the
+    // reference's per-vector op sequence with a host-read scalar per step
+    return !flexible && gmc && dhist && A->val && cfg.orth != FASP_GPU_ORTH_MGS &&
+           (pcd.type == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
+}
+
+// The preconditioned product of an Arnoldi step: mode 0 y = A v (Identity), 1 y = A (D v)
+// (right Jacobi from zero: the sweep is diagInv .* v), 2 y = D (A v) (left Jacobi).
+template <typename T, int L, int MODE>
+__global__ void __launch_bounds__(kBlock) k_gm_apply(CSRView<T> A, const T* __restrict__ v,
+                                                     const T* __restrict__ dinv,
+                                                     T* __restrict__ y, const int* stop)
+{
+    if (*stop) return;
+    auto xv = [&](uint32_t j) { return MODE == 1 ? v[j] * dinv[j] : v[j]; };
+    auto out = [&](size_t row, T sum) { y[row] = MODE == 2 ? sum * dinv[row] : sum; };
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x)
+            out(row, row_apply<T, false>(A, row, xv));
+        return;
+    }
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t row = base + sub;
+        T sum = T(0);
+        if (row < A.nrow)
+            for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
+                sum = fma(A.val[k], xv(A.colInd[k]), sum);
+        sum = group_sum<L>(sum);
+        if (lane == 0 && row < A.nrow) out(row, sum);
+    }
+}
+
+// w *= 1 / t (Scale by a device scalar, as v_scale(Scal::dinv(t)))
+template <typename T>
+__global__ void k_gm_scale(uint32_t n, const double* __restrict__ tn, T* __restrict__ w,
+                           const int* stop)
+{
+    if (*stop) return;
+    const T inv = (T)(1.0 / *tn);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        w[i] *= inv;
+}
+
+template <typename T, int MODE>
+static void gm_apply_launch(Ctx& c, const Mat& A, CSRView<T> V, const T* v, const T* dinv,
+                            T* y, const int* stop)
+{
+    const int need = c.grid((long long)A.nrow * A.lanes, kBlock);
+    auto go = [&](auto kern) {
+        kern<<<std::min(need, resident_grid(c, (const void*)kern, kBlock)), kBlock, 0,
+               c.stream>>>(V, v, dinv, y, stop);
+    };
+    switch (A.lanes) {
+        case 1: go(k_gm_apply<T, 1, MODE>); break;
+        case 2: go(k_gm_apply<T, 2, MODE>); break;
+        case 4: go(k_gm_apply<T, 4, MODE>); break;
+        case 8: go(k_gm_apply<T, 8, MODE>); break;
+        case 16: go(k_gm_apply<T, 16, MODE>); break;
+        default: go(k_gm_apply<T, 32, MODE>); break;
+    }
+}
+
+template <typename T>
+static CSRView<T> gm_view(const Mat& A);
+template <>
+CSRView<double> gm_view<double>(const Mat& A) { return A.v64(); }
+template <>
+CSRView<float> gm_view<float>(const Mat& A) { return A.v32(); }
+
+// Enqueues up to `steps` Arnoldi steps of one restart cycle (GMRES.cxx:160-210 /
+// :371-402) with no host synchronisation, then reads the cycle's outcome: count, numIter,
+// the last estimate, and merges the device's history records. left: GMRES::LSolve.
+template <typename T>
+static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t steps, bool left,
+                           uint32_t& count, uint32_t& numIter, double& resAbs, double denAbs,
+                           const fasp_gpu_params& P, int& stopped)
+{
+    Ctx& c = S.c;
+    const uint32_t n = S.n;
+    const size_t ld = n;
+    GmCtl& h = *S.hgmc;
+    const uint32_t iter0 = numIter;
+    std::memset(&h, 0, sizeof(GmCtl));
+    h.numIter = numIter;
+    h.minIter = P.minIter;
+    h.resAbs = resAbs;
+    h.denAbs = denAbs;
+    h.relTol = P.relTol;
+    h.absTol = P.absTol;
+    h.hist = S.dhist;
+    h.histCap = S.dhistCap;
+    h.histOffset = S.histOff;
+    h.histScale = S.histScale;
+    FB_CUDA(cudaMemcpyAsync(S.gmc, &h, sizeof(GmCtl), cudaMemcpyHostToDevice, c.stream));
+    const int* stop = &S.gmc->stop;
+    const CSRView<T> AV = gm_view<T>(*S.A);
+    const T* dinv;
+    if constexpr (std::is_same<T, float>::value)
+        dinv = S.pcd.dinv32;
+    else
+        dinv = S.pcd.dinv;
+    const int mode = S.pcd.type == 0 ? 0 : (left ? 2 : 1);
+    double* tn = c.dslot + SL_T5;
+    for (uint32_t k = 1; k <= steps; ++k) {
+        const T* vin = V + (k - 1) * ld;
+        T* vnew = V + k * ld;
+        if (mode == 0)
+            gm_apply_launch<T, 0>(c, *S.A, AV, vin, dinv, vnew, stop);
+        else if (mode == 1)
+            gm_apply_launch<T, 1>(c, *S.A, AV, vin, dinv, vnew, stop);
+        else
+            gm_apply_launch<T, 2>(c, *S.A, AV, vin, dinv, vnew, stop);
+        v_multidot(c, n, (int)k, (const T*)V, ld, (const T*)vnew, L.h1, stop);
+        v_multiaxpy(c, n, (int)k, (const T*)V, ld, L.h1, 1.0, vnew, nullptr, stop);
+        v_multidot(c, n, (int)k, (const T*)V, ld, (const T*)vnew, L.h2, stop);
+        v_multiaxpy(c, n, (int)k, (const T*)V, ld, L.h2, 1.0, vnew, tn, stop);
+        k_gmres_givens<<<1, 1, 0, c.stream>>>(L, (int)k, (int)k - 1, 1, tn, S.gmc);
+        k_gm_scale<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, tn, vnew, stop);
+        c.launches += 3;
+    }
+    FB_CUDA(cudaGetLastError());
+    FB_CUDA(cudaMemcpyAsync(&h, S.gmc, sizeof(GmCtl), cudaMemcpyDeviceToHost, c.stream));
+    const uint32_t off = S.histOff + iter0 + 1;
+    const uint32_t cnt = std::min<uint32_t>(steps, S.dhistCap > off ? S.dhistCap - off : 0);
+    std::vector<double> dh(cnt);
+    if (cnt)
+        FB_CUDA(cudaMemcpyAsync(dh.data(), S.dhist + off, (size_t)cnt * 8,
+                                cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    count = h.count;
+    numIter = h.numIter;
+    resAbs = h.resAbs;
+    stopped = h.stop;
+    for (uint32_t k = 0; k < cnt && iter0 + 1 + k <= numIter; ++k)
+        if (std::isfinite(dh[k])) {
+            const uint32_t g = off + k;
+            if (g >= S.hist.size()) S.hist.resize((size_t)g + 1, kNaN);
+            S.hist[g] = dh[k];
+        }
     return kOk;
 }
 
@@ -1211,6 +1389,11 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
     double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, resAbsOld = 1.0;
     uint32_t count = 1, count_1 = 2, numIter = 0;
 
+    const bool devCycle = gm_device_cycles(flexible);
+    if (devCycle) {
+        ++c.launches;
+        k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    }
     v_copy(c, n, x, sv);
     apply_residual(c, *A, b, x, V);
     v_norm2(c, n, V, d + SL_T1);
@@ -1230,7 +1413,19 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
         v_scale(c, n, Scal::h(1 / resAbs), V);
 
         count = 0;
-        while (count < restart && numIter < P.maxIter) {
+        if (devCycle) { // the whole cycle on the device, one synchronisation
+            const uint32_t steps = std::min<uint32_t>(restart, P.maxIter - numIter);
+            int stopped = 0;
+            if ((e = gm_cycle_device<T>(*this, L, V, steps, false, count, numIter, resAbs, denAbs,
+                                        P, stopped)))
+                return e;
+            count_1 = count - 1;
+            if (!(stopped == 1 && count == 1)) { // a breakdown step updates nothing
+                resRel = resAbs / denAbs;
+                resAbsOld = resAbs;
+            }
+        }
+        while (!devCycle && count < restart && numIter < P.maxIter) {
             ++numIter;
             count_1 = count++;
             T* vnew = V + count * ld;
@@ -1310,6 +1505,11 @@ int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu
     double resAbs = 1.0, resRel = 1.0, denAbs = 1.0, resAbsOld = 1.0;
     uint32_t count = 1, count_1 = 2, numIter = 0;
 
+    const bool devCycle = gm_device_cycles(false);
+    if (devCycle) {
+        ++c.launches;
+        k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    }
     v_copy(c, n, x, sv);
     apply_residual(c, *A, b, x, tmp);
     v_norm2(c, n, tmp, d + SL_T1);
@@ -1333,7 +1533,19 @@ int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu
         v_scale(c, n, Scal::h(1 / resAbs), V);
 
         count = 0;
-        while (count < restart && numIter < P.maxIter) {
+        if (devCycle) { // the whole cycle on the device, one synchronisation
+            const uint32_t steps = std::min<uint32_t>(restart, P.maxIter - numIter);
+            int stopped = 0;
+            if ((e = gm_cycle_device<T>(*this, L, V, steps, true, count, numIter, resAbs, denAbs,
+                                        P, stopped)))
+                return e;
+            count_1 = count - 1;
+            if (!(stopped == 1 && count == 1)) {
+                resAbsOld = resAbs;
+                resRel = resAbs / denAbs;
+            }
+        }
+        while (!devCycle && count < restart && numIter < P.maxIter) {
             ++numIter;
             count_1 = count++;
             T* vnew = V + count * ld;
