@@ -80,9 +80,10 @@ __device__ void cg_after_spmv(CGCtl* c, double tmpb)
 {
     c->numIter += 1;
     c->tmpb = tmpb;
-    if (fabs(tmpb) > kCloseZero * kCloseZero)
+    if (fabs(tmpb) > kCloseZero * kCloseZero) {
         c->alpha = c->tmpa / tmpb;
-    else if (c->inner)
+        c->xpend = 1;
+    } else if (c->inner)
         cg_done(c, kErrDivZero);
     else {
         const double red[5] = {0, 0, 0, 0, 0};
@@ -165,6 +166,7 @@ __device__ void cg_after_refresh(CGCtl* c, const double* t)
     c->res64 = rn;
     c->refreshes += 1;
     c->reason = kNoReason;
+    c->xpend = 0; // the fold applied it
     const bool conv = rn / c->den64 < c->relTol || rn < c->absTol;
     // three refreshes in a row without real progress: the tolerance is below what FP32
     // iterations with FP64 refreshes attain here (ERROR_SOLVER_TOLSMALL)
@@ -188,13 +190,18 @@ __device__ void cg_after_refresh(CGCtl* c, const double* t)
 }
 
 // Reliable update, part 1 (in the cg_spmv slot): x64 += s x32, x32 = 0.
-__device__ __forceinline__ void cg_refresh_fold(uint32_t n, float* x32, const CGCtl* c)
+// A lean engine first applies the pending x += alpha p of the last iteration.
+__device__ __forceinline__ void cg_refresh_fold(uint32_t n, float* x32, const float* p,
+                                                const CGCtl* c)
 {
     double* x64 = c->rx;
     const double s = c->histScale;
+    const float alpha = (float)c->alpha;
+    const bool pend = p && c->xpend;
     GRID_STRIDE(i, n)
     {
-        x64[i] = fma(s, (double)x32[i], x64[i]);
+        const float xi = pend ? fmaf(alpha, p[i], x32[i]) : x32[i];
+        x64[i] = fma(s, (double)xi, x64[i]);
         x32[i] = 0.0f;
     }
 }
@@ -291,7 +298,8 @@ struct V16<double> {
 // owned row (half the gathers). Its rounding differs from A p by a term that beta < 1 damps;
 // the FP64 refreshes of reliable updates correct the residual it feeds.
 template <typename T, int L, int REC>
-__global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restrict__ z,
+__global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))) cg_spmv(CSRView<T> A,
+                                                                     const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
                                                   CGCtl* c, Scratch s)
 {
@@ -299,10 +307,12 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     pdl_release();
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
-            if (c->status == kRefresh) cg_refresh_fold(A.nrow, x, c);
+            if (c->status == kRefresh) cg_refresh_fold(A.nrow, x, REC ? P0 : nullptr, c);
         return;
     }
     const int mode = c->pmode, par = c->par;
+    const bool xpend = REC && c->xpend;
+    const T alphaPrev = (T)c->alpha;
     const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
@@ -311,7 +321,9 @@ __global__ void __launch_bounds__(kBlock) cg_spmv(CSRView<T> A, const T* __restr
     auto own = [&](size_t row, T sum) {
         const T zi = z[row];
         if (REC) {
-            const T pi = mode ? fma(beta, P0[row], zi) : zi;
+            const T po = P0[row];
+            if (xpend) x[row] = fma(alphaPrev, po, x[row]); // the last iteration's x update
+            const T pi = mode ? fma(beta, po, zi) : zi;
             const T qi = mode ? fma(beta, q[row], sum) : sum;
             P0[row] = pi;
             q[row] = qi;
@@ -448,6 +460,63 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
     });
 }
 
+// The lean FP32 update (engines with the recurrence): r -= alpha q, z = D r and the two sums
+// (r,r), (z,r) that the FP32 loop reads; x is updated by the next cg_spmv.
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __restrict__ r,
+                                                         T* __restrict__ z,
+                                                         const T* __restrict__ q,
+                                                         const T* __restrict__ dinv, CGCtl* c,
+                                                         Scratch s, CSRView<T> A)
+{
+    pdl_wait();
+    pdl_release();
+    if (c->status != kRun) {
+        if constexpr (std::is_same<T, float>::value)
+            if (c->status == kRefresh)
+                cg_refresh_residual<JAC>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd, A.cls,
+                                                     A.coff, A.cdelta, A.mask},
+                                         r, z, dinv, c, s);
+        return;
+    }
+    const T alpha = (T)c->alpha;
+    T rr = 0, zr = 0;
+    using V = typename V16<T>::t;
+    constexpr int W = V16<T>::W;
+    const size_t nv = n / W;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i < nv; i += stride) {
+        T ra[W], qa[W], da[W];
+        *(V*)ra = ((const V*)r)[i];
+        *(V*)qa = ((const V*)q)[i];
+        if (JAC) *(V*)da = ((const V*)dinv)[i];
+#pragma unroll
+        for (int u = 0; u < W; ++u) {
+            ra[u] = fma(-alpha, qa[u], ra[u]);
+            qa[u] = JAC ? da[u] * ra[u] : ra[u]; // z in q's registers
+            rr = fma(ra[u], ra[u], rr);
+            zr = fma(qa[u], ra[u], zr);
+        }
+        ((V*)r)[i] = *(V*)ra;
+        if (JAC) ((V*)z)[i] = *(V*)qa;
+    }
+    for (size_t i = nv * W + tid; i < n; i += stride) {
+        const T ri = fma(-alpha, q[i], r[i]);
+        const T zi = JAC ? dinv[i] * ri : ri;
+        r[i] = ri;
+        if (JAC) z[i] = zi;
+        rr = fma(ri, ri, rr);
+        zr = fma(zi, ri, zr);
+    }
+    double a[2] = {(double)rr, (double)zr};
+    const int ops[2] = {kSum, kSum};
+    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+        const double red[5] = {t[0], t[1], 0.0, 0.0, 0.0};
+        if (!c->bench) cg_checks(c, red, 0);
+    });
+}
+
 // Start of CG::Solve after rk = b - A x (CG.cxx:69-79): z = B(r), tmpa = (z, r), p = z.
 template <typename T, int JAC>
 __global__ void __launch_bounds__(kBlock) cg_start(uint32_t n, const T* __restrict__ r,
@@ -481,6 +550,7 @@ __global__ void __launch_bounds__(kBlock) cg_start(uint32_t n, const T* __restri
         c->ratio = 0.0;
         c->resAbsOld = 1.0;
         c->alpha = 0.0;
+        c->xpend = 0;
         cg_looptop(c, t[0]);
     });
 }
@@ -576,13 +646,8 @@ template <int NV>
 __device__ __forceinline__ void all_reduce_partials(const Scratch s, const int (&slot)[NV],
                                                     const int (&ops)[NV], double (&tot)[NV])
 {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double t = red_ident(ops[k]);
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-            t = red_apply(t, __ldcg(&s.partials[slot[k] * kMaxGrid + b]), ops[k]);
-        tot[k] = t;
-    }
+    // the slots are consecutive (0..4, or the single phase-1 slot)
+    sum_partials<NV>(s.partials + slot[0] * kMaxGrid, ops, tot);
     block_reduce<NV>(tot, ops);
 }
 
@@ -757,10 +822,31 @@ void CGEngine<T>::launch_update_kernel()
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
     };
+    if (lean()) {
+        auto gl = [&](auto kern, T* zz) {
+            const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
+            launch_overlapped(kern, g, c->stream, pdl, n, r, zz, q, dinv, ctl, c->red, V);
+        };
+        if (jacobi)
+            gl(cg_update_lean<T, 1>, z);
+        else
+            gl(cg_update_lean<T, 0>, r);
+        return;
+    }
     if (jacobi)
         go(cg_update<T, 1>, z);
     else
         go(cg_update<T, 0>, r);
+}
+
+template <typename T>
+int CGEngine<T>::apply_pending_x()
+{
+    if (!lean() || !hctl->xpend) return kOk;
+    hctl->xpend = 0;
+    int e = v_axpy(*c, n, Scal::h(hctl->alpha), (const T*)P0, x);
+    if (e) return e;
+    return push_ctl();
 }
 
 template <typename T>

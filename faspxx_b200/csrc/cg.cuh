@@ -24,6 +24,7 @@ struct CGCtl {
     int      pmode;     // 0: p = z (first iteration or restart), 1: p = z + beta p
     int      par;       // which of the two p buffers holds the current direction
     int      pzero;     // the host zeroed p (a restart): next p = z
+    int      xpend;     // lean FP32 engine: x += alpha p of the last iteration not yet applied
     int      inner;     // 1: inner solve of mixed refinement (plain relative stop)
     int      reliable;  // 1 (with inner): FP32 iterations with FP64 reliable updates
     int      bench;     // 1: kernel timing, the finalize steps do nothing
@@ -74,6 +75,11 @@ struct CGEngine {
     bool       capturing = false;
     bool       pdl = true;      // programmatic dependent launch of the iteration kernels
     bool       recurrence = false; // q = A z + beta q_old (FP32 engines; p single-buffered)
+    // with the recurrence (not persistent): x += alpha p is applied by the next cg_spmv for
+    // its own rows and cg_update keeps to r, z and two sums (the FP32 loop reads no others)
+    bool       lean() const { return recurrence && !persistent; }
+    // applies a pending x += alpha p (host side, after the device loop stopped)
+    int        apply_pending_x();
     uint32_t   n = 0;
     // persistent engine: one cooperative launch runs the iterations
     bool       wantPersistent = true; // set before init

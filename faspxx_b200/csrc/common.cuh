@@ -61,6 +61,35 @@ __device__ __forceinline__ void block_reduce(double (&acc)[NV], const int (&ops)
     __syncthreads();
 }
 
+// One thread's share of the partials of every block: value k of block b sits at
+// partials[k * kMaxGrid + b]; the thread sums blocks threadIdx.x, +blockDim.x, ... in that
+// order. The loads of U consecutive block indices (all NV values) are issued before their
+// adds, so the last block waits for about gridDim / (blockDim U) L2 round trips instead of
+// one per block index and value.
+template <int NV>
+__device__ __forceinline__ void sum_partials(const double* partials, const int (&ops)[NV],
+                                             double (&tot)[NV])
+{
+    constexpr int U = NV >= 8 ? 1 : 8 / NV;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) tot[k] = red_ident(ops[k]);
+    const int nb = (int)gridDim.x, bd = (int)blockDim.x;
+    for (int b0 = threadIdx.x; b0 < nb; b0 += U * bd) {
+        double v[U][NV];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u * bd;
+#pragma unroll
+            for (int k = 0; k < NV; ++k)
+                v[u][k] = b < nb ? __ldcg(&partials[k * kMaxGrid + b]) : red_ident(ops[k]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) tot[k] = red_apply(tot[k], v[u][k], ops[k]);
+    }
+}
+
 // Grid-wide deterministic reduction. Every thread of every block must call it (after its
 // grid-stride work). The last block runs fin(totals) on thread 0. Returns nothing useful to
 // other threads.
@@ -81,13 +110,7 @@ __device__ __forceinline__ void grid_reduce(double (&acc)[NV], const int (&ops)[
     if (!amLast) return;
     __threadfence();
     double tot[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        double t = red_ident(ops[k]);
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
-            t = red_apply(t, __ldcg(&s.partials[k * kMaxGrid + b]), ops[k]);
-        tot[k] = t;
-    }
+    sum_partials<NV>(s.partials, ops, tot);
     block_reduce<NV>(tot, ops);
     if (threadIdx.x == 0) {
         *s.ticket = 0;

@@ -688,7 +688,7 @@ int SolverImpl::cg_mixed(const double* b, double* x, fasp_gpu_info* info)
         c.launches += gl;
         const uint32_t it = h.numIter;
         total += it;
-        if ((e = update_from32(c, n, rn, E.x, x64))) return e;
+        if ((e = E.apply_pending_x()) || (e = update_from32(c, n, rn, E.x, x64))) return e;
         ++outer;
         if (it == 0) {
             code = h.code ? h.code : kErrMaxIt;
@@ -801,7 +801,9 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
             }
             // a host refresh: the stop test or delta reached (persistent engine), or the end
             // of the FP32 run (maxIter, breakdown)
-            if ((e = update_from32(c, n, s, E.x, x64)) || (e = set32(c, n, E.x))) return e;
+            if ((e = E.apply_pending_x()) || (e = update_from32(c, n, s, E.x, x64)) ||
+                (e = set32(c, n, E.x)))
+                return e;
             if ((e = true_res(&rn))) return e;
             ++hostRefreshes;
             patches.push_back({h.numIter, rn});
