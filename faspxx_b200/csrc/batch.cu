@@ -198,6 +198,289 @@ __global__ void __launch_bounds__(512) batch_pcg(BatchArgs<T> a)
     }
 }
 
+// Mixed precision with reliable updates, block-local: the CG iterations run in FP32 on the
+// system scaled by s = ||b|| (x0 = 0), and whenever a right-hand side's recursive residual
+// meets the stop test or has fallen by delta since its last refresh, the block refreshes
+// every active right-hand side in FP64 (the block owns the whole system, so this needs only
+// __syncthreads): x64 += s x32, x32 = 0, r = b - A x64 in FP64 with the FP64 values, r32 =
+// r / s, z32 = diagInv .* r32. The stop test is applied to the FP64 residual; otherwise CG
+// goes on with the same p and beta = (z, r)_refreshed / (z, r)_old.
+struct BatchRel {
+    const double* val64;
+    const double* b64;
+    double*       x64;
+    double        delta;
+};
+
+template <int NR>
+__global__ void __launch_bounds__(512) batch_pcg_rel(BatchArgs<float> a, BatchRel f)
+{
+    // per right-hand side scalars, uniform across the block: thread 0 updates them after
+    // each block reduction, the others read them after the barrier
+    struct Rhs {
+        double rz, rzold, beta, rmax, res, true0, prev, sc, pq;
+        float  alpha;
+        int    active, fresh, stall, trig;
+    };
+    __shared__ Rhs st[kMaxRhs];
+    __shared__ unsigned item;
+    __shared__ double sh[3 * kMaxRhs];
+    __shared__ int nact, refresh;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item = atomicAdd(a.queue, 1u);
+        __syncthreads();
+        if (item >= a.count) return;
+        const uint32_t sys = a.order[item];
+        const uint32_t r0 = a.sysRow[sys], r1 = a.sysRow[sys + 1];
+        const size_t N = a.N;
+        // ||b|| per right-hand side (FP64), the scale s
+        {
+            double bb[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) bb[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const double bi = f.b64[k * N + i];
+                    bb[k] = fma(bi, bi, bb[k]);
+                }
+            bsum<NR>(bb);
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const double nb = sqrt(bb[k]);
+                    st[k].true0 = nb;
+                    st[k].prev = nb;
+                    st[k].sc = nb > 0.0 ? nb : 1.0;
+                    st[k].active = nb > 0.0;
+                    st[k].fresh = 1; // the next p is z (first iteration, or after a restart)
+                    st[k].stall = 0;
+                    st[k].beta = 0.0;
+                }
+            __syncthreads();
+        }
+        // start: x = 0, r32 = b / s, z32 = diagInv .* r32, (r,r), (z,r)
+        {
+            double acc[2 * NR];
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const float d = a.dinv[i];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    const size_t o = k * N + i;
+                    f.x64[o] = 0.0;
+                    const float ri = (float)(f.b64[o] / st[k].sc);
+                    const float zi = d * ri;
+                    a.x[o] = 0.0f;
+                    a.r[o] = ri;
+                    a.z[o] = zi;
+                    acc[k] += (double)ri * ri;
+                    acc[NR + k] += (double)zi * ri;
+                }
+            }
+            bsum<2 * NR>(acc);
+            if (threadIdx.x == 0) {
+                int na = 0;
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    st[k].rz = acc[NR + k];
+                    st[k].res = sqrt(acc[k]);
+                    st[k].rmax = st[k].res;
+                    na += st[k].active;
+                }
+                nact = na;
+            }
+            __syncthreads();
+        }
+        uint32_t it = 0;
+        int par = 0;
+        while (nact > 0 && it < a.maxIter) {
+            ++it;
+            const float* pOld = par ? a.p1 : a.p0;
+            float* pNew = par ? a.p0 : a.p1;
+            int act[NR], fr[NR];
+            float bt[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                act[k] = st[k].active;
+                fr[k] = st[k].fresh;
+                bt[k] = (float)st[k].beta;
+            }
+            // pass 1: q = A p with p = z + beta p_old on the fly, (q, p)
+            double pq[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) pq[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const uint32_t kb = a.rowPtr[i], ke = a.rowPtr[i + 1];
+                float s[NR];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) s[k] = 0.f;
+                for (uint32_t e = kb; e < ke; ++e) {
+                    const uint32_t j = __ldg(a.colInd + e);
+                    const float v = __ldg(a.val + e);
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) {
+                        if (!act[k]) continue;
+                        const size_t o = k * N + j;
+                        const float pj = fr[k] ? a.z[o] : fmaf(bt[k], pOld[o], a.z[o]);
+                        s[k] = fmaf(v, pj, s[k]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    if (!act[k]) continue;
+                    const size_t o = k * N + i;
+                    const float pi = fr[k] ? a.z[o] : fmaf(bt[k], pOld[o], a.z[o]);
+                    pNew[o] = pi;
+                    a.q[o] = s[k];
+                    pq[k] += (double)s[k] * pi;
+                }
+            }
+            bsum<NR>(pq);
+            if (threadIdx.x == 0)
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    st[k].alpha = st[k].active && pq[k] != 0.0 ? (float)(st[k].rz / pq[k]) : 0.f;
+                    st[k].fresh = 0;
+                }
+            __syncthreads();
+            // pass 2: x += alpha p, r -= alpha q, z = diagInv .* r; (r,r), (z,r)
+            float al[NR];
+#pragma unroll
+            for (int k = 0; k < NR; ++k) al[k] = st[k].alpha;
+            double red[2 * NR];
+#pragma unroll
+            for (int k = 0; k < 2 * NR; ++k) red[k] = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                const float d = a.dinv[i];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    if (!act[k]) continue;
+                    const size_t o = k * N + i;
+                    const float xi = fmaf(al[k], pNew[o], a.x[o]);
+                    const float ri = fmaf(-al[k], a.q[o], a.r[o]);
+                    const float zi = d * ri;
+                    a.x[o] = xi;
+                    a.r[o] = ri;
+                    a.z[o] = zi;
+                    red[k] += (double)ri * ri;
+                    red[NR + k] += (double)zi * ri;
+                }
+            }
+            bsum<2 * NR>(red);
+            if (threadIdx.x == 0) {
+                int rf = 0;
+#pragma unroll
+                for (int k = 0; k < NR; ++k) {
+                    st[k].trig = 0;
+                    if (!st[k].active) continue;
+                    const double res = sqrt(red[k]);
+                    st[k].res = res;
+                    if (res > st[k].rmax) st[k].rmax = res;
+                    st[k].rzold = st[k].rz;
+                    if (res < a.relTol || res < f.delta * st[k].rmax || !(red[k] == red[k])) {
+                        rf = 1;
+                        st[k].trig = 1;
+                    } else {
+                        st[k].beta = red[NR + k] / st[k].rz;
+                        st[k].rz = red[NR + k];
+                    }
+                }
+                refresh = rf;
+            }
+            __syncthreads();
+            if (refresh) { // block-uniform
+                // 1. x64 += s x32, x32 = 0
+                for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) {
+                        if (!act[k]) continue;
+                        const size_t o = k * N + i;
+                        f.x64[o] = fma(st[k].sc, (double)a.x[o], f.x64[o]);
+                        a.x[o] = 0.0f;
+                    }
+                __syncthreads();
+                // 2. r = b - A x64 in FP64; r32 = r / s; z32 = diagInv .* r32
+                double rr[3 * NR];
+#pragma unroll
+                for (int k = 0; k < 3 * NR; ++k) rr[k] = 0.0;
+                for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                    const float d = a.dinv[i];
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) {
+                        if (!act[k]) continue;
+                        double sum = 0.0;
+                        for (uint32_t e = a.rowPtr[i]; e < a.rowPtr[i + 1]; ++e)
+                            sum = fma(f.val64[e], f.x64[k * N + a.colInd[e]], sum);
+                        const size_t o = k * N + i;
+                        const double ri = f.b64[o] - sum;
+                        const float r32 = (float)(ri / st[k].sc);
+                        const float z32 = d * r32;
+                        a.r[o] = r32;
+                        a.z[o] = z32;
+                        rr[k] = fma(ri, ri, rr[k]);
+                        rr[NR + k] += (double)r32 * r32;
+                        rr[2 * NR + k] += (double)z32 * r32;
+                    }
+                }
+                bsum<3 * NR>(rr);
+                if (threadIdx.x == 0)
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) {
+                        if (!st[k].active) continue;
+                        const double tr = sqrt(rr[k]);
+                        // three refreshes of its own in a row gaining less than sqrt(delta):
+                        // the tolerance is below what the FP32 iterations attain here (a
+                        // refresh another right-hand side asked for is not counted)
+                        if (st[k].trig) {
+                            st[k].stall = tr > sqrt(f.delta) * st[k].prev ? st[k].stall + 1 : 0;
+                            st[k].prev = tr;
+                        }
+                        if (tr < a.relTol * st[k].true0 || !(tr == tr) || st[k].stall >= 3) {
+                            st[k].active = 0;
+                            st[k].res = tr / st[k].sc;
+                        } else {
+                            const double rs = sqrt(rr[NR + k]);
+                            // a refreshed residual far above the recursive one: p = z
+                            if (rs > 4.0 * st[k].res) st[k].fresh = 1;
+                            // beta from the refreshed residual and the (z, r) of the previous
+                            // iteration
+                            st[k].beta = rr[2 * NR + k] / st[k].rzold;
+                            st[k].rz = rr[2 * NR + k];
+                            st[k].rmax = rs;
+                            st[k].res = rs;
+                        }
+                    }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                int na = 0;
+#pragma unroll
+                for (int k = 0; k < NR; ++k) na += st[k].active;
+                nact = na;
+            }
+            __syncthreads();
+            par ^= 1;
+        }
+        // right-hand sides still active at maxIter: fold the FP32 correction
+        for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+#pragma unroll
+            for (int k = 0; k < NR; ++k) {
+                if (!st[k].active) continue;
+                const size_t o = k * N + i;
+                f.x64[o] = fma(st[k].sc, (double)a.x[o], f.x64[o]);
+            }
+        if (threadIdx.x < NR) {
+            const int k = threadIdx.x;
+            a.iters[(size_t)sys * a.nrhs + k] += it;
+            a.resRel[(size_t)sys * a.nrhs + k] =
+                st[k].true0 > 0 ? st[k].res * st[k].sc / st[k].true0 : 0.0;
+        }
+    }
+}
+
 // FP64 residual of every system and right-hand side, r64 = b - A x (the outer step of the
 // mixed solve), with ||r|| per (system, rhs) and the FP32 right-hand side r / ||r||.
 __global__ void __launch_bounds__(256) batch_residual(uint32_t count, uint32_t nrhs, uint32_t N,
@@ -435,6 +718,21 @@ int fasp_gpu_batch_solve(fasp_gpu_batch h, const double* b, double* x, double re
                             B.dinv, b, x, B.r64, B.z64, B.p0, B.p1, B.q64, B.iters, B.resRel,
                             relTol, maxIter, B.queue};
         e = launch_batch<double>(B, a);
+    } else if (precision == FASP_GPU_MIXED_RELIABLE) {
+        BatchArgs<float> a{cnt, nr, N, B.sysRow, B.order, B.M.rowPtr, B.M.colInd, B.M.val32,
+                           B.dinv32, nullptr, B.x32, B.r32, B.z32, B.p032, B.p132, B.q32,
+                           B.iters, B.resRel, relTol, maxIter, B.queue};
+        const BatchRel f{B.M.val, b, x, innerRelTol > 0 && innerRelTol < 1 ? innerRelTol : 1e-2};
+        const int grid = B.c.nsm * B.blocksPerSM;
+        cudaMemsetAsync(B.queue, 0, sizeof(unsigned), B.c.stream);
+        switch (nr) {
+            case 1: batch_pcg_rel<1><<<grid, B.block, 0, B.c.stream>>>(a, f); break;
+            case 2: batch_pcg_rel<2><<<grid, B.block, 0, B.c.stream>>>(a, f); break;
+            case 3: batch_pcg_rel<3><<<grid, B.block, 0, B.c.stream>>>(a, f); break;
+            default: batch_pcg_rel<4><<<grid, B.block, 0, B.c.stream>>>(a, f); break;
+        }
+        B.c.launches += 1;
+        if (cudaGetLastError() != cudaSuccess) e = kErrCuda;
     } else {
         // FP64 refinement around FP32 inner solves, x0 = 0
         cudaMemsetAsync(x, 0, vN * 8, B.c.stream);

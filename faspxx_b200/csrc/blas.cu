@@ -5,8 +5,10 @@
 // scalar, so a following kernel can consume it without a host round trip. Sums use FMA and
 // a different association than the reference's 4 interleaved partial sums (VEC.cxx:424-485);
 // results agree to rounding, not bit for bit.
+#include <cstdint>
 #include <map>
 #include <mutex>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -217,16 +219,39 @@ int v_copy(Ctx& c, uint32_t n, const T* src, T* dst)
 
 // ---- classical Gram-Schmidt building blocks ------------------------------------------
 // V holds basis vectors at V + j*ld. KC vectors are handled per launch; the coefficients
-// h stay FP64 for either vector type.
+// h stay FP64 for either vector type. When V, w and the stride allow it (16-byte aligned
+// vectors, ld a multiple of the vector width), each thread reads 16-byte vectors of
+// consecutive elements (VEC = 1), which keeps more bytes in flight per thread; the few
+// elements past the last full vector are read one by one.
 
 constexpr int KC = 8;
 
-// dres[j] = (V_j, w), j in [j0, j0+k)
 template <typename T>
+struct Vec16 {
+    typedef typename std::conditional<sizeof(T) == 8, double2, float4>::type type;
+    static constexpr int W = 16 / (int)sizeof(T);
+};
+
+// Grid of the Gram-Schmidt kernels (one grid for all three, so the fused kernel maps
+// elements to threads exactly as the separate ones): 4 blocks per SM -- each thread keeps
+// several 16-byte loads per vector in flight, and the grid reduction sums fewer partials.
+static int mgrid(const Ctx& c, uint32_t n) { return c.grid(n, kBlock, 4); }
+
+template <typename T>
+static bool vec_ok(const T* V, size_t ld, const T* w)
+{
+    return ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15) == 0 &&
+           ld % Vec16<T>::W == 0;
+}
+
+// dres[j] = (V_j, w), j in [j0, j0+k)
+template <typename T, int VEC>
 __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
                            const T* __restrict__ w, Scratch s, double* dres, const int* stop)
 {
     if (stop && *stop) return;
+    using VT = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
     T t[KC];
     double acc[KC];
     int ops[KC];
@@ -235,8 +260,26 @@ __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld
         t[j] = T(0);
         ops[j] = kSum;
     }
-    GRID_STRIDE(i, n)
-    {
+    size_t i0 = 0;
+    if (VEC) {
+        const size_t nv = n / W;
+        GRID_STRIDE(iv, nv)
+        {
+            T wv[W];
+            *(VT*)wv = ((const VT*)w)[iv];
+#pragma unroll
+            for (int j = 0; j < KC; ++j)
+                if (j < k) {
+                    T vv[W];
+                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+#pragma unroll
+                    for (int u = 0; u < W; ++u) t[j] = fma(vv[u], wv[u], t[j]);
+                }
+        }
+        i0 = nv * W;
+    }
+    for (size_t i = i0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
         const T wi = w[i];
 #pragma unroll
         for (int j = 0; j < KC; ++j)
@@ -250,18 +293,41 @@ __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld
 }
 
 // w -= sign * sum_j h[j] V_j; with dnorm != null also ||w_new|| -> *dnorm.
-template <typename T>
+template <typename T, int VEC>
 __global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
                             const double* __restrict__ h, double sign, T* __restrict__ w,
                             Scratch s, double* dnorm, const int* stop)
 {
     if (stop && *stop) return;
+    using VT = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
     T hj[KC];
 #pragma unroll
     for (int j = 0; j < KC; ++j) hj[j] = j < k ? (T)(sign * h[j]) : T(0);
     T t = T(0);
-    GRID_STRIDE(i, n)
-    {
+    size_t i0 = 0;
+    if (VEC) {
+        const size_t nv = n / W;
+        GRID_STRIDE(iv, nv)
+        {
+            T wv[W];
+            *(VT*)wv = ((const VT*)w)[iv];
+#pragma unroll
+            for (int j = 0; j < KC; ++j)
+                if (j < k) {
+                    T vv[W];
+                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+#pragma unroll
+                    for (int u = 0; u < W; ++u) wv[u] = fma(-hj[j], vv[u], wv[u]);
+                }
+            ((VT*)w)[iv] = *(VT*)wv;
+#pragma unroll
+            for (int u = 0; u < W; ++u) t = fma(wv[u], wv[u], t);
+        }
+        i0 = nv * W;
+    }
+    for (size_t i = i0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
         T wi = w[i];
 #pragma unroll
         for (int j = 0; j < KC; ++j)
@@ -274,15 +340,95 @@ __global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t l
     if (dnorm) grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dnorm = sqrt(v[0]); });
 }
 
+// CGS2's second projection and its re-orthogonalisation dots in one pass over the basis,
+// for k <= KF<T> vectors (16 FP32, 8 FP64: what fits in registers): w -= sum_j h[j] V_j,
+// then dres[j] = (V_j, w_new). Each element's
+// FMA sequence, each thread's elements (the same grid and mapping as k_multidot) and the
+// reduction order equal those of k_multiaxpy followed by k_multidot, so the results are
+// bit-identical to the two passes; V is read once instead of twice.
+template <typename T>
+__host__ __device__ constexpr int kf() { return sizeof(T) == 8 ? 8 : 16; }
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kBlock, 3)
+k_multiaxpy_dot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
+                const double* __restrict__ h, T* __restrict__ w, Scratch s, double* dres,
+                const int* stop)
+{
+    if (stop && *stop) return;
+    constexpr int KF_ = kf<T>();
+    using VT = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    __shared__ T hs[KF_];
+    if (threadIdx.x < KF_) hs[threadIdx.x] = (int)threadIdx.x < k ? (T)(1.0 * h[threadIdx.x]) : T(0);
+    __syncthreads();
+    T t[KF_];
+#pragma unroll
+    for (int j = 0; j < KF_; ++j) t[j] = T(0);
+    size_t i0 = 0;
+    if (VEC) {
+        const size_t nv = n / W;
+        GRID_STRIDE(iv, nv)
+        {
+            T wv[W];
+            *(VT*)wv = ((const VT*)w)[iv];
+#pragma unroll
+            for (int j = 0; j < KF_; ++j)
+                if (j < k) {
+                    T vv[W];
+                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+#pragma unroll
+                    for (int u = 0; u < W; ++u) wv[u] = fma(-hs[j], vv[u], wv[u]);
+                }
+            ((VT*)w)[iv] = *(VT*)wv;
+#pragma unroll
+            for (int j = 0; j < KF_; ++j)
+                if (j < k) {
+                    T vv[W];
+                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+#pragma unroll
+                    for (int u = 0; u < W; ++u) t[j] = fma(vv[u], wv[u], t[j]);
+                }
+        }
+        i0 = nv * W;
+    }
+    for (size_t i = i0 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        T wi = w[i];
+#pragma unroll
+        for (int j = 0; j < KF_; ++j)
+            if (j < k) wi = fma(-hs[j], V[j * ld + i], wi);
+        w[i] = wi;
+#pragma unroll
+        for (int j = 0; j < KF_; ++j)
+            if (j < k) t[j] = fma(V[j * ld + i], wi, t[j]);
+    }
+    double acc[KF_];
+    int ops[KF_];
+#pragma unroll
+    for (int j = 0; j < KF_; ++j) {
+        acc[j] = (double)t[j];
+        ops[j] = kSum;
+    }
+    grid_reduce<KF_>(acc, ops, s, [=] __device__(const double* v) {
+        for (int j = 0; j < k; ++j) dres[j] = v[j];
+    });
+}
+
 template <typename T>
 int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres,
                const int* stop)
 {
+    const bool vec = vec_ok(V, ld, w);
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         ++c.launches;
-        k_multidot<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, kk, V + j0 * ld, ld, w,
-                                                                   c.red, dres + j0, stop);
+        if (vec)
+            k_multidot<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                n, kk, V + j0 * ld, ld, w, c.red, dres + j0, stop);
+        else
+            k_multidot<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                n, kk, V + j0 * ld, ld, w, c.red, dres + j0, stop);
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
@@ -292,14 +438,38 @@ template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
                 double sign, T* w, double* dnorm, const int* stop)
 {
+    const bool vec = vec_ok(V, ld, (const T*)w);
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         const bool last = j0 + KC >= k;
         ++c.launches;
-        k_multiaxpy<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
-            n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
+        if (vec)
+            k_multiaxpy<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
+        else
+            k_multiaxpy<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
         FB_CUDA(cudaGetLastError());
     }
+    return kOk;
+}
+
+template <typename T>
+int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h, T* w,
+                    double* dres, const int* stop)
+{
+    if (k > kf<T>()) {
+        int e = v_multiaxpy(c, n, k, V, ld, h, 1.0, w, (double*)nullptr, stop);
+        return e ? e : v_multidot(c, n, k, V, ld, (const T*)w, dres, stop);
+    }
+    ++c.launches;
+    if (vec_ok(V, ld, (const T*)w))
+        k_multiaxpy_dot<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, k, V, ld, h, w, c.red,
+                                                                    dres, stop);
+    else
+        k_multiaxpy_dot<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, k, V, ld, h, w, c.red,
+                                                                    dres, stop);
+    FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
@@ -319,7 +489,9 @@ int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* 
     template int v_multidot<T>(Ctx&, uint32_t, int, const T*, size_t, const T*, double*,  \
                                const int*);                                               \
     template int v_multiaxpy<T>(Ctx&, uint32_t, int, const T*, size_t, const double*,     \
-                                double, T*, double*, const int*);
+                                double, T*, double*, const int*);                         \
+    template int v_multiaxpy_dot<T>(Ctx&, uint32_t, int, const T*, size_t, const double*, \
+                                    T*, double*, const int*);
 FB_VEC_INSTANTIATE(double)
 FB_VEC_INSTANTIATE(float)
 #undef FB_VEC_INSTANTIATE

@@ -14,7 +14,7 @@
 namespace fb {
 
 constexpr int kBlock = 256;          // threads per block for vector kernels
-constexpr int kMaxRedValues = 8;     // values one fused reduction may carry
+constexpr int kMaxRedValues = 16;    // values one fused reduction may carry
 constexpr int kMaxGrid = 148 * 16;   // upper bound of any reducing grid (partials sizing)
 
 struct Scratch {

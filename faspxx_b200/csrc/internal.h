@@ -204,6 +204,11 @@ int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, dou
 template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
                 double sign, T* w, double* dnorm, const int* stop = nullptr);
+// w -= sum_j h[j] V_j then dres[j] = (V_j, w), in one pass for k <= 16 (FP32) or 8 (FP64)
+// (bit-identical to v_multiaxpy followed by v_multidot, which it falls back to above)
+template <typename T>
+int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h, T* w,
+                    double* dres, const int* stop = nullptr);
 
 // ---- sparse kernels (spmv.cu) ---------------------------------------------------------
 int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,

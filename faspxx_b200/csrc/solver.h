@@ -81,6 +81,7 @@ struct SolverImpl {
     GmCtl*          gmc = nullptr;  // device in-cycle state, and its pinned host copy
     GmCtl*          hgmc = nullptr;
     uint32_t        maxRestart = 0, minRestart = 0, restart = 0;
+    size_t          ldV = 0;        // stride of the GMRES/FGMRES bases (n padded to 32)
     // MG (identity transfers): per level smoother and coarse solver, coarse b and x
     std::vector<Pcd> mgSmooth, mgCoarse;
     std::vector<double*> mgB, mgX;

@@ -261,11 +261,12 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             else if (restart < minRestart)
                 restart = minRestart;
             if (maxRestart == 0 || restart == 0) return kErrInputPar;
+            ldV = ((size_t)n + 31) & ~(size_t)31; // every basis vector 256-byte aligned
             if (cfg.precision == FASP_GPU_MIXED) {
                 // FP64 outer residual; FP32 wk tmp safe + b, e and the FP32 bases
                 if ((e = alloc_vecs(w, 1, n)) || (e = alloc_vecs(w32, 5, n))) return e;
                 if ((e = Ah->M.ensure32(c.stream))) return e;
-                const size_t vb = (size_t)(maxRestart + 1) * n * 4;
+                const size_t vb = (size_t)(maxRestart + 1) * ldV * 4;
                 if (cudaMalloc(&V32, vb + 16) != cudaSuccess) return kErrAlloc;
                 cudaMemset(V32, 0, vb);
                 if (alg == FASP_GPU_FGMRES) {
@@ -274,7 +275,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 }
             } else {
                 if ((e = alloc_vecs(w, 3, n))) return e; // wk tmp safe
-                const size_t vb = (size_t)(maxRestart + 1) * n * 8;
+                const size_t vb = (size_t)(maxRestart + 1) * ldV * 8;
                 if (cudaMalloc(&V, vb + 16) != cudaSuccess) return kErrAlloc;
                 cudaMemset(V, 0, vb);
                 if (alg == FASP_GPU_FGMRES) {
@@ -328,7 +329,7 @@ void SolverImpl::clean()
             restart = maxRestart;
         else if (restart < minRestart)
             restart = minRestart;
-        const size_t vb = (size_t)(maxRestart + 1) * n * 8;
+        const size_t vb = (size_t)(maxRestart + 1) * ldV * 8;
         if (V) cudaMemsetAsync(V, 0, vb, c.stream);
         if (Z) cudaMemsetAsync(Z, 0, vb, c.stream);
         if (V32) cudaMemsetAsync(V32, 0, vb / 2, c.stream);
@@ -1115,48 +1116,72 @@ static GmLayout gm_layout(double* gm, size_t m)
 // GMRES.cxx:168-203 after the dots: hh[j][c1] (CGS2: h1+h2), t = ||w||, then the previous
 // rotations, the new rotation and the updated residual estimate |var[count]|. out[1] = 0
 // when t is not > SMALL_DBL (the reference leaves the restart cycle before rotating).
-__global__ void k_gmres_givens(GmLayout L, int count, int c1, int cgs, const double* tnorm,
-                               GmCtl* g)
+constexpr int kGmShared = 512; // Hessenberg columns up to this length are staged in shared memory
+
+__global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int c1, int cgs,
+                                                      const double* tnorm, GmCtl* g)
 {
     if (g && g->stop) return;
     const size_t m = L.m;
 #define HH(i, j) L.hh[(size_t)(i) * m + (j)]
-    if (cgs)
-        for (int j = 0; j < count; ++j) HH(j, c1) = L.h1[j] + L.h2[j];
-    double t = *tnorm;
-    HH(count, c1) = t;
-    if (g) { // ++numIter at the top of the step (GMRES.cxx:162)
-        g->numIter += 1;
-        g->count = count;
+    // the column c1 and the previous rotations, loaded by all threads; one thread then runs
+    // the reference's serial sequence on shared memory, with the same operations and order
+    __shared__ double col[kGmShared + 1], sn[kGmShared], cs[kGmShared];
+    const bool sh = count <= kGmShared;
+    if (sh) {
+        for (int j = threadIdx.x; j < count; j += blockDim.x) {
+            col[j] = cgs ? L.h1[j] + L.h2[j] : HH(j, c1);
+            sn[j] = L.hsin[j];
+            cs[j] = L.hcos[j];
+        }
+        __syncthreads();
     }
-    if (!(fabs(t) > kSmallDbl)) {
-        L.out[1] = 0.0;
-        if (g) g->stop = 1;
-        return;
+    if (threadIdx.x == 0) {
+        if (!sh && cgs)
+            for (int j = 0; j < count; ++j) HH(j, c1) = L.h1[j] + L.h2[j];
+        auto C = [&](int j) -> double& { return sh ? col[j] : HH(j, c1); };
+        auto S = [&](int j) { return sh ? sn[j] : L.hsin[j]; };
+        auto K = [&](int j) { return sh ? cs[j] : L.hcos[j]; };
+        double t = *tnorm;
+        C(count) = t;
+        if (g) { // ++numIter at the top of the step (GMRES.cxx:162)
+            g->numIter += 1;
+            g->count = count;
+        }
+        if (!(fabs(t) > kSmallDbl)) {
+            L.out[1] = 0.0;
+            if (g) g->stop = 1;
+        } else {
+            L.out[1] = 1.0;
+            for (int j = 1; j < count; ++j) {
+                t = C(j - 1);
+                C(j - 1) = S(j - 1) * C(j) + K(j - 1) * t;
+                C(j) = -S(j - 1) * t + K(j - 1) * C(j);
+            }
+            t = C(count) * C(count);
+            t += C(c1) * C(c1);
+            t = sqrt(t);
+            const double gamma = t > kSmallDbl ? t : kSmallDbl;
+            L.hcos[c1] = C(c1) / gamma;
+            L.hsin[c1] = C(count) / gamma;
+            C(c1) = L.hsin[c1] * C(count) + L.hcos[c1] * C(c1);
+            L.var[count] = -L.hsin[c1] * L.var[c1];
+            L.var[c1] = L.hcos[c1] * L.var[c1];
+            L.out[0] = fabs(L.var[count]);
+            if (g) { // GMRES.cxx:205-209: the estimate, its record and the in-cycle stop test
+                const double resAbs = L.out[0];
+                g->resAbs = resAbs;
+                const unsigned k = g->numIter + g->histOffset;
+                if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;
+                if ((resAbs < g->absTol || resAbs / g->denAbs < g->relTol) &&
+                    g->numIter > g->minIter)
+                    g->stop = 2;
+            }
+        }
     }
-    L.out[1] = 1.0;
-    for (int j = 1; j < count; ++j) {
-        t = HH(j - 1, c1);
-        HH(j - 1, c1) = L.hsin[j - 1] * HH(j, c1) + L.hcos[j - 1] * t;
-        HH(j, c1) = -L.hsin[j - 1] * t + L.hcos[j - 1] * HH(j, c1);
-    }
-    t = HH(count, c1) * HH(count, c1);
-    t += HH(c1, c1) * HH(c1, c1);
-    t = sqrt(t);
-    const double gamma = t > kSmallDbl ? t : kSmallDbl;
-    L.hcos[c1] = HH(c1, c1) / gamma;
-    L.hsin[c1] = HH(count, c1) / gamma;
-    HH(c1, c1) = L.hsin[c1] * HH(count, c1) + L.hcos[c1] * HH(c1, c1);
-    L.var[count] = -L.hsin[c1] * L.var[c1];
-    L.var[c1] = L.hcos[c1] * L.var[c1];
-    L.out[0] = fabs(L.var[count]);
-    if (g) { // GMRES.cxx:205-209: the estimate, its record and the in-cycle stop test
-        const double resAbs = L.out[0];
-        g->resAbs = resAbs;
-        const unsigned k = g->numIter + g->histOffset;
-        if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;
-        if ((resAbs < g->absTol || resAbs / g->denAbs < g->relTol) && g->numIter > g->minIter)
-            g->stop = 2;
+    if (sh) {
+        __syncthreads();
+        for (int j = threadIdx.x; j <= count; j += blockDim.x) HH(j, c1) = col[j];
     }
 #undef HH
 }
@@ -1183,7 +1208,7 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, co
 {
     Ctx& c = S.c;
     const uint32_t n = S.n;
-    const size_t ld = n;
+    const size_t ld = S.ldV;
     double* tn = c.dslot + SL_T5;
     if (S.cfg.orth == FASP_GPU_ORTH_MGS) { // GMRES.cxx:169-172
         for (int j = 0; j < count; ++j) {
@@ -1194,13 +1219,12 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, co
         v_norm2(c, n, (const T*)wv, tn);
     } else { // CGS2: two fused multi-dot / multi-AXPY passes
         v_multidot(c, n, count, V, ld, (const T*)wv, L.h1);
-        v_multiaxpy(c, n, count, V, ld, L.h1, 1.0, wv, nullptr);
-        v_multidot(c, n, count, V, ld, (const T*)wv, L.h2);
+        v_multiaxpy_dot(c, n, count, V, ld, L.h1, wv, L.h2);
         v_multiaxpy(c, n, count, V, ld, L.h2, 1.0, wv, tn);
     }
     ++c.launches;
-    k_gmres_givens<<<1, 1, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn,
-                                          nullptr);
+    k_gmres_givens<<<1, 128, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn,
+                                            nullptr);
     FB_CUDA(cudaGetLastError());
     v_scale(c, n, Scal::dinv(tn), wv);
     return kOk;
@@ -1296,7 +1320,7 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
 {
     Ctx& c = S.c;
     const uint32_t n = S.n;
-    const size_t ld = n;
+    const size_t ld = S.ldV;
     GmCtl& h = *S.hgmc;
     const uint32_t iter0 = numIter;
     std::memset(&h, 0, sizeof(GmCtl));
@@ -1330,10 +1354,9 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
         else
             gm_apply_launch<T, 2>(c, *S.A, AV, vin, dinv, vnew, stop);
         v_multidot(c, n, (int)k, (const T*)V, ld, (const T*)vnew, L.h1, stop);
-        v_multiaxpy(c, n, (int)k, (const T*)V, ld, L.h1, 1.0, vnew, nullptr, stop);
-        v_multidot(c, n, (int)k, (const T*)V, ld, (const T*)vnew, L.h2, stop);
+        v_multiaxpy_dot(c, n, (int)k, (const T*)V, ld, L.h1, vnew, L.h2, stop);
         v_multiaxpy(c, n, (int)k, (const T*)V, ld, L.h2, 1.0, vnew, tn, stop);
-        k_gmres_givens<<<1, 1, 0, c.stream>>>(L, (int)k, (int)k - 1, 1, tn, S.gmc);
+        k_gmres_givens<<<1, 128, 0, c.stream>>>(L, (int)k, (int)k - 1, 1, tn, S.gmc);
         k_gm_scale<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, tn, vnew, stop);
         c.launches += 3;
     }
@@ -1383,7 +1406,7 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
     std::vector<T*>& w = *S.w;
     T *wk = w[0], *tmp = w[1], *sv = w[2];
     T *V = S.V, *Z = S.Z;
-    const size_t ld = n;
+    const size_t ld = ldV;
     const GmLayout L = gm_layout(gm, maxRestart);
     double* d = c.dslot;
     int err = kOk, e;
@@ -1499,7 +1522,7 @@ int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu
     std::vector<T*>& w = *S.w;
     T *wk = w[0], *tmp = w[1], *sv = w[2];
     T *V = S.V;
-    const size_t ld = n;
+    const size_t ld = ldV;
     const GmLayout L = gm_layout(gm, maxRestart);
     double* d = c.dslot;
     int err = kOk, e;

@@ -243,7 +243,9 @@ int fasp_gpu_batch_create(uint32_t count, const uint32_t* sysRow, uint32_t nnz,
  * per SM; the autotuner in the Python/C++ layers times the choices. */
 int fasp_gpu_batch_set_shape(fasp_gpu_batch bt, int block, int blocksPerSM);
 /* Solves all systems from x0 = 0 to ||r|| < relTol ||b|| per right-hand side (device b, x).
- * precision FASP_GPU_MIXED runs FP32 inner CG to innerRelTol inside FP64 refinement.
+ * precision FASP_GPU_MIXED runs FP32 inner CG to innerRelTol inside FP64 refinement;
+ * FASP_GPU_MIXED_RELIABLE runs FP32 CG iterations with block-local FP64 reliable updates
+ * (innerRelTol = the refresh factor, default 1e-2), the FP64 iteration count.
  * iters (host, count*nrhs, may be NULL): iterations per right-hand side; resRel (host,
  * may be NULL): final relative residual per right-hand side. */
 int fasp_gpu_batch_solve(fasp_gpu_batch bt, const double* b, double* x, double relTol,

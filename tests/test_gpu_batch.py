@@ -62,6 +62,25 @@ def test_batch_mixed_reaches_fp64_residual(batch):
             assert res <= 1e-8, (k, j, res)
 
 
+def test_batch_reliable_updates_reach_fp64_residual_in_fp64_iterations(batch):
+    """FP32 iterations with block-local FP64 reliable updates: every system and right-hand
+    side reaches the FP64 relative residual 1e-8, in the FP64 iteration count (+5% +2)."""
+    from faspxx_b200 import capi
+    B, mats, b, P = batch
+    x64, it64, _, _ = B.solve(b, relTol=1e-8, precision=capi.FP64)
+    x, it, rr, ms = B.solve(b, relTol=1e-8, precision=capi.MIXED_RELIABLE, innerRelTol=1e-2)
+    assert np.all(rr <= 1e-8)
+    for k, m in enumerate(mats):
+        r0, r1 = int(B.sys_row[k]), int(B.sys_row[k + 1])
+        for j in range(4):
+            bj = b[j, r0:r1]
+            res = np.linalg.norm(bj - m.matvec(x[j, r0:r1])) / np.linalg.norm(bj)
+            assert res <= 1e-8, (k, j, res)
+    assert it.sum() <= it64.sum() * 1.05 + 2 * it.size
+    x2 = B.solve(b, relTol=1e-8, precision=capi.MIXED_RELIABLE, innerRelTol=1e-2)[0]
+    assert np.array_equal(x, x2)
+
+
 def test_batch_autotune_and_repeatability(batch):
     B, mats, b, P = batch
     shape, ms = B.autotune(b)
