@@ -233,9 +233,10 @@ struct Vec16 {
 };
 
 // Grid of the Gram-Schmidt kernels (one grid for all three, so the fused kernel maps
-// elements to threads exactly as the separate ones): 4 blocks per SM -- each thread keeps
-// several 16-byte loads per vector in flight, and the grid reduction sums fewer partials.
-static int mgrid(const Ctx& c, uint32_t n) { return c.grid(n, kBlock, 4); }
+// elements to threads exactly as the separate ones): 3 blocks per SM, all resident at once
+// (each kernel is compiled for 3 blocks of kBlock threads) -- one wave, each thread keeping
+// several 16-byte loads per vector in flight, and few partials for the grid reduction.
+static int mgrid(const Ctx& c, uint32_t n) { return c.grid(n, kBlock, 3); }
 
 template <typename T>
 static bool vec_ok(const T* V, size_t ld, const T* w)
@@ -246,7 +247,8 @@ static bool vec_ok(const T* V, size_t ld, const T* w)
 
 // dres[j] = (V_j, w), j in [j0, j0+k)
 template <typename T, int VEC>
-__global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
+__global__ void __launch_bounds__(kBlock, 3)
+k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
                            const T* __restrict__ w, Scratch s, double* dres, const int* stop)
 {
     if (stop && *stop) return;
@@ -294,7 +296,8 @@ __global__ void k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld
 
 // w -= sign * sum_j h[j] V_j; with dnorm != null also ||w_new|| -> *dnorm.
 template <typename T, int VEC>
-__global__ void k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
+__global__ void __launch_bounds__(kBlock, 3)
+k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
                             const double* __restrict__ h, double sign, T* __restrict__ w,
                             Scratch s, double* dnorm, const int* stop)
 {

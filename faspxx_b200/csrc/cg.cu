@@ -263,9 +263,11 @@ __device__ __noinline__ void cg_refresh_residual(RefreshView A, float* r32, floa
         const float r32i = (float)(ri * inv);
         r32[row] = r32i;
         float zi = r32i;
-        if (JAC) {
+        if (JAC == 1) {
             zi = dinv32[row] * r32i;
             z32[row] = zi;
+        } else if (JAC == 2) {
+            zi = (float)c->zc * r32i;
         }
         rr64 = fma(ri, ri, rr64);
         rr = fmaf(r32i, r32i, rr);
@@ -297,7 +299,7 @@ struct V16<double> {
 // q = A p = A z + beta q_old, so the SpMV gathers z alone and p, q update in place for the
 // owned row (half the gathers). Its rounding differs from A p by a term that beta < 1 damps;
 // the FP64 refreshes of reliable updates correct the residual it feeds.
-template <typename T, int L, int REC>
+template <typename T, int L, int REC, int JZ>
 __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))) cg_spmv(CSRView<T> A,
                                                                      const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
@@ -313,13 +315,16 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
     const int mode = c->pmode, par = c->par;
     const bool xpend = REC && c->xpend;
     const T alphaPrev = (T)c->alpha;
+    const T zc = (T)c->zc;
+    // JZ = 2: z = zc r is formed here from r (passed as z), never stored
+    auto zat = [&](size_t j) { return JZ == 2 ? zc * z[j] : z[j]; };
     const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
     T acc = T(0);
     // the owned row's p and q from its product `sum`
     auto own = [&](size_t row, T sum) {
-        const T zi = z[row];
+        const T zi = zat(row);
         if (REC) {
             const T po = P0[row];
             if (xpend) x[row] = fma(alphaPrev, po, x[row]); // the last iteration's x update
@@ -336,8 +341,8 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
         }
     };
     auto gv = [&](uint32_t j) {
-        if (REC) return z[j];
-        return mode ? fma(beta, pOld[j], z[j]) : z[j];
+        if (REC) return zat(j);
+        return mode ? fma(beta, pOld[j], zat(j)) : zat(j);
     };
     if (L == 1) { // thread per row
         const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -387,12 +392,13 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
         return;
     }
     const T alpha = (T)c->alpha;
+    const T zc = (T)c->zc;
     const T* __restrict__ p = c->par ? P1 : P0;
     T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
     auto one = [&](T pi, T& xi, T& ri, T qi, T di, T& zi) {
         xi = fma(alpha, pi, xi);
         ri = fma(-alpha, qi, ri);
-        zi = JAC ? di * ri : ri;
+        zi = JAC == 1 ? di * ri : (JAC == 2 ? zc * ri : ri);
         rr = fma(ri, ri, rr);
         zr = fma(zi, ri, zr);
         xx = fma(xi, xi, xx);
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
             *(V*)xa[h] = ((const V*)x)[k];
             *(V*)ra[h] = ((const V*)r)[k];
             *(V*)qa[h] = ((const V*)q)[k];
-            if (JAC) *(V*)da[h] = ((const V*)dinv)[k];
+            if (JAC == 1) *(V*)da[h] = ((const V*)dinv)[k];
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
@@ -427,10 +433,11 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
             // z overwrites q's registers: q is dead once r is updated
 #pragma unroll
             for (int u = 0; u < W; ++u)
-                one(pa[h][u], xa[h][u], ra[h][u], qa[h][u], JAC ? da[h][u] : T(0), qa[h][u]);
+                one(pa[h][u], xa[h][u], ra[h][u], qa[h][u], JAC == 1 ? da[h][u] : T(0),
+                    qa[h][u]);
             ((V*)x)[k] = *(V*)xa[h];
             ((V*)r)[k] = *(V*)ra[h];
-            if (JAC) ((V*)z)[k] = *(V*)qa[h];
+            if (JAC == 1) ((V*)z)[k] = *(V*)qa[h];
         }
     }
     for (; i < nv; i += stride) {
@@ -439,19 +446,20 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
         *(V*)xa = ((const V*)x)[i];
         *(V*)ra = ((const V*)r)[i];
         *(V*)qa = ((const V*)q)[i];
-        if (JAC) *(V*)da = ((const V*)dinv)[i];
+        if (JAC == 1) *(V*)da = ((const V*)dinv)[i];
 #pragma unroll
-        for (int u = 0; u < W; ++u) one(pa[u], xa[u], ra[u], qa[u], JAC ? da[u] : T(0), qa[u]);
+        for (int u = 0; u < W; ++u)
+            one(pa[u], xa[u], ra[u], qa[u], JAC == 1 ? da[u] : T(0), qa[u]);
         ((V*)x)[i] = *(V*)xa;
         ((V*)r)[i] = *(V*)ra;
-        if (JAC) ((V*)z)[i] = *(V*)qa;
+        if (JAC == 1) ((V*)z)[i] = *(V*)qa;
     }
     for (size_t i = nv * W + tid; i < n; i += stride) {
         T xi = x[i], ri = r[i], zi;
-        one(p[i], xi, ri, q[i], JAC ? dinv[i] : T(0), zi);
+        one(p[i], xi, ri, q[i], JAC == 1 ? dinv[i] : T(0), zi);
         x[i] = xi;
         r[i] = ri;
-        if (JAC) z[i] = zi;
+        if (JAC == 1) z[i] = zi;
     }
     double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
     const int ops[5] = {kSum, kSum, kSum, kMax, kSum};
@@ -480,6 +488,7 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
         return;
     }
     const T alpha = (T)c->alpha;
+    const T zc = (T)c->zc;
     T rr = 0, zr = 0;
     using V = typename V16<T>::t;
     constexpr int W = V16<T>::W;
@@ -490,22 +499,22 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
         T ra[W], qa[W], da[W];
         *(V*)ra = ((const V*)r)[i];
         *(V*)qa = ((const V*)q)[i];
-        if (JAC) *(V*)da = ((const V*)dinv)[i];
+        if (JAC == 1) *(V*)da = ((const V*)dinv)[i];
 #pragma unroll
         for (int u = 0; u < W; ++u) {
             ra[u] = fma(-alpha, qa[u], ra[u]);
-            qa[u] = JAC ? da[u] * ra[u] : ra[u]; // z in q's registers
+            qa[u] = JAC == 1 ? da[u] * ra[u] : (JAC == 2 ? zc * ra[u] : ra[u]); // z in q's regs
             rr = fma(ra[u], ra[u], rr);
             zr = fma(qa[u], ra[u], zr);
         }
         ((V*)r)[i] = *(V*)ra;
-        if (JAC) ((V*)z)[i] = *(V*)qa;
+        if (JAC == 1) ((V*)z)[i] = *(V*)qa;
     }
     for (size_t i = nv * W + tid; i < n; i += stride) {
         const T ri = fma(-alpha, q[i], r[i]);
-        const T zi = JAC ? dinv[i] * ri : ri;
+        const T zi = JAC == 1 ? dinv[i] * ri : (JAC == 2 ? zc * ri : ri);
         r[i] = ri;
-        if (JAC) z[i] = zi;
+        if (JAC == 1) z[i] = zi;
         rr = fma(ri, ri, rr);
         zr = fma(zi, ri, zr);
     }
@@ -524,13 +533,16 @@ __global__ void __launch_bounds__(kBlock) cg_start(uint32_t n, const T* __restri
                                                    CGCtl* c, Scratch s)
 {
     T rr = 0, zr = 0;
+    const T zc = (T)c->zc;
     GRID_STRIDE(i, n)
     {
         const T ri = r[i];
         T zi = ri;
-        if (JAC) {
+        if (JAC == 1) {
             zi = dinv[i] * ri;
             z[i] = zi;
+        } else if (JAC == 2) {
+            zi = zc * ri;
         }
         rr = fma(ri, ri, rr);
         zr = fma(zi, ri, zr);
@@ -564,13 +576,16 @@ __global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restr
                                                     Scratch s)
 {
     T rr = 0, zr = 0;
+    const T zc = (T)c->zc;
     GRID_STRIDE(i, n)
     {
         const T ri = r[i];
         T zi = ri;
-        if (JAC) {
+        if (JAC == 1) {
             zi = dinv[i] * ri;
             z[i] = zi;
+        } else if (JAC == 2) {
+            zi = zc * ri;
         }
         rr = fma(ri, ri, rr);
         zr = fma(zi, ri, zr);
@@ -791,24 +806,29 @@ void CGEngine<T>::launch_spmv_kernel()
 {
     const CSRView<T> V = view_of<T>(*A);
     const int need = spmv_grid_cg(*c, A->nrow, A->lanes);
-    const T* zz = jacobi ? z : r;
+    const int jm = jmode();
+    const T* zz = jm == 1 ? z : r;
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red);
     };
-#define CG_SPMV_LANES(RR)                                                                  \
+#define CG_SPMV_LANES(RR, JJ)                                                              \
     switch (A->lanes) {                                                                    \
-        case 1: go(cg_spmv<T, 1, RR>); break;                                              \
-        case 2: go(cg_spmv<T, 2, RR>); break;                                              \
-        case 4: go(cg_spmv<T, 4, RR>); break;                                              \
-        case 8: go(cg_spmv<T, 8, RR>); break;                                              \
-        case 16: go(cg_spmv<T, 16, RR>); break;                                            \
-        default: go(cg_spmv<T, 32, RR>); break;                                            \
+        case 1: go(cg_spmv<T, 1, RR, JJ>); break;                                          \
+        case 2: go(cg_spmv<T, 2, RR, JJ>); break;                                          \
+        case 4: go(cg_spmv<T, 4, RR, JJ>); break;                                          \
+        case 8: go(cg_spmv<T, 8, RR, JJ>); break;                                          \
+        case 16: go(cg_spmv<T, 16, RR, JJ>); break;                                        \
+        default: go(cg_spmv<T, 32, RR, JJ>); break;                                        \
     }
-    if (recurrence) {
-        CG_SPMV_LANES(1)
+    if (recurrence && jm == 2) {
+        CG_SPMV_LANES(1, 2)
+    } else if (recurrence) {
+        CG_SPMV_LANES(1, 0)
+    } else if (jm == 2) {
+        CG_SPMV_LANES(0, 2)
     } else {
-        CG_SPMV_LANES(0)
+        CG_SPMV_LANES(0, 0)
     }
 #undef CG_SPMV_LANES
 }
@@ -822,18 +842,23 @@ void CGEngine<T>::launch_update_kernel()
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
     };
+    const int jm = jmode();
     if (lean()) {
         auto gl = [&](auto kern, T* zz) {
             const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
             launch_overlapped(kern, g, c->stream, pdl, n, r, zz, q, dinv, ctl, c->red, V);
         };
-        if (jacobi)
+        if (jm == 2)
+            gl(cg_update_lean<T, 2>, r);
+        else if (jm == 1)
             gl(cg_update_lean<T, 1>, z);
         else
             gl(cg_update_lean<T, 0>, r);
         return;
     }
-    if (jacobi)
+    if (jm == 2)
+        go(cg_update<T, 2>, r);
+    else if (jm == 1)
         go(cg_update<T, 1>, z);
     else
         go(cg_update<T, 0>, r);
@@ -864,7 +889,10 @@ int CGEngine<T>::launch_init()
 {
     const int g2 = c->grid(n, kBlock);
     ++c->launches;
-    if (jacobi)
+    const int jm = persistent ? jacobi : jmode();
+    if (jm == 2)
+        cg_start<T, 2><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
+    else if (jm == 1)
         cg_start<T, 1><<<g2, kBlock, 0, c->stream>>>(n, r, z, dinv, ctl, c->red);
     else
         cg_start<T, 0><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
@@ -877,7 +905,10 @@ int CGEngine<T>::launch_resume()
 {
     const int g2 = c->grid(n, kBlock);
     ++c->launches;
-    if (jacobi)
+    const int jm = persistent ? jacobi : jmode();
+    if (jm == 2)
+        cg_resume<T, 2><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
+    else if (jm == 1)
         cg_resume<T, 1><<<g2, kBlock, 0, c->stream>>>(n, r, z, dinv, ctl, c->red);
     else
         cg_resume<T, 0><<<g2, kBlock, 0, c->stream>>>(n, r, r, dinv, ctl, c->red);
@@ -888,6 +919,7 @@ int CGEngine<T>::launch_resume()
 template <typename T>
 int CGEngine<T>::push_ctl()
 {
+    hctl->zc = zc;
     FB_CUDA(cudaMemcpyAsync(ctl, hctl, sizeof(CGCtl), cudaMemcpyHostToDevice, c->stream));
     return kOk;
 }

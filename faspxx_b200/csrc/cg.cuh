@@ -25,6 +25,7 @@ struct CGCtl {
     int      par;       // which of the two p buffers holds the current direction
     int      pzero;     // the host zeroed p (a restart): next p = z
     int      xpend;     // lean FP32 engine: x += alpha p of the last iteration not yet applied
+    double   zc;        // the constant diagInv when the Jacobi diagonal is one value (z = zc r)
     int      inner;     // 1: inner solve of mixed refinement (plain relative stop)
     int      reliable;  // 1 (with inner): FP32 iterations with FP64 reliable updates
     int      bench;     // 1: kernel timing, the finalize steps do nothing
@@ -65,6 +66,11 @@ struct CGEngine {
     const Mat* A = nullptr;
     int        jacobi = 0;
     const T*   dinv = nullptr;
+    // a constant diagInv (every diagonal entry equal): z = zc r is formed where it is used
+    // and never stored, with the same values as the stored z (graph and plain engines)
+    bool       constDiag = false;
+    double     zc = 0.0;
+    int        jmode() const { return !jacobi ? 0 : (constDiag && !wantPersistent ? 2 : 1); }
     T *x = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *P0 = nullptr, *P1 = nullptr;
     CGCtl*     ctl = nullptr;    // device
     CGCtl*     hctl = nullptr;   // pinned host copy

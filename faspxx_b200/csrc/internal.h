@@ -128,6 +128,8 @@ struct Mat {
     float*    val32 = nullptr;   // FP32 copy for the mixed-precision inner solves (lazy)
     double*   diag = nullptr;    // GetDiag (1 for pattern-only)
     int       lanes = 8;         // lanes per row of the SpMV (autotuned or from row lengths)
+    bool      diagConst = false; // every row stores a diagonal entry, all with one value
+    double    diagValue = 0.0;
     uint32_t  maxRowLen = 0;
     double    meanRowLen = 0;
     int       dev = 0;

@@ -212,6 +212,9 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 cg64 = new CGEngine<double>();
                 cg64->wantPersistent = cfg.persistent != 0;
                 cg64->pdl = cfg.overlapLaunch != 0;
+                // Jacobi::Setup's diagInv = (1 / diag) * weight, one value for all rows
+                cg64->constDiag = cfg.pcd == 1 && A->diagConst;
+                cg64->zc = (1.0 / A->diagValue) * pcd.weight;
                 if ((e = cg64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
             }
             if (cfg.precision == FASP_GPU_MIXED || cfg.precision == FASP_GPU_MIXED_RELIABLE) {
@@ -221,6 +224,8 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 cg32->wantPersistent = cfg.persistent != 0;
                 cg32->pdl = cfg.overlapLaunch != 0;
                 cg32->recurrence = cfg.fp32Recurrence != 0;
+                cg32->constDiag = cfg.pcd == 1 && A->diagConst;
+                cg32->zc = (1.0 / A->diagValue) * pcd.weight;
                 if ((e = cg32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
             }
             break;
@@ -1234,9 +1239,10 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, co
 
 bool SolverImpl::gm_device_cycles(bool flexible) const
 {
-    // FGMRES warm-starts its preconditioner from the previous basis Z; MGS keeps the
-    // reference's per-vector op sequence with a host-read scalar per step
-    return !flexible && gmc && dhist && A->val && cfg.orth != FASP_GPU_ORTH_MGS &&
+    // Identity or one Jacobi sweep (from zero for GMRES, from the warm start Z_j for
+    // FGMRES); MGS keeps the reference's per-vector op sequence with a host-read scalar
+    (void)flexible;
+    return gmc && dhist && A->val && cfg.orth != FASP_GPU_ORTH_MGS &&
            (pcd.type == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
 }
 
@@ -1284,6 +1290,108 @@ __global__ void k_gm_scale(uint32_t n, const double* __restrict__ tn, T* __restr
         w[i] *= inv;
 }
 
+// FGMRES with one Jacobi sweep from the warm start Z_j (Jacobi::Solve with minIter =
+// maxIter = 1, Iter.cxx:56-112, as FGMRES.cxx:158-159 calls it): NormInf(Z_j) for the
+// residual's shortcut, then t = Z_j + diagInv .* (V_j - A Z_j) into a work vector; the
+// step's product A t stores t back into Z_j (k_fg_apply), so every gather reads the old Z_j.
+template <typename T>
+__global__ void k_fg_norminf(uint32_t n, const T* __restrict__ z, Scratch s, double* dres,
+                             const int* stop)
+{
+    if (*stop) return;
+    T m = T(0);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(z[i]));
+    double acc[1] = {(double)m};
+    const int ops[1] = {kMax};
+    grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dres = t[0]; });
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kBlock) k_fg_sweep(CSRView<T> A, const T* __restrict__ v,
+                                                     const T* __restrict__ zj,
+                                                     const T* __restrict__ dinv,
+                                                     const double* __restrict__ zinf,
+                                                     T* __restrict__ t, const int* stop)
+{
+    if (*stop) return;
+    const bool shortcut = *zinf < kCloseZero; // MAT::Residual (MAT.cxx:459-462)
+    auto xv = [&](uint32_t j) { return zj[j]; };
+    auto out = [&](size_t row, T sum) {
+        const T work = v[row] - sum;
+        t[row] = zj[row] + work * dinv[row];
+    };
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x)
+            out(row, shortcut ? T(0) : row_apply<T, false>(A, row, xv));
+        return;
+    }
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t row = base + sub;
+        T sum = T(0);
+        if (row < A.nrow && !shortcut)
+            for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
+                sum = fma(A.val[k], xv(A.colInd[k]), sum);
+        sum = group_sum<L>(sum);
+        if (lane == 0 && row < A.nrow) out(row, sum);
+    }
+}
+
+// y = A t and z = t (the preconditioned basis vector Z_j of FGMRES, FGMRES.cxx:159-160)
+template <typename T, int L>
+__global__ void __launch_bounds__(kBlock) k_fg_apply(CSRView<T> A, const T* __restrict__ t,
+                                                     T* __restrict__ z, T* __restrict__ y,
+                                                     const int* stop)
+{
+    if (*stop) return;
+    auto xv = [&](uint32_t j) { return t[j]; };
+    if (L == 1) {
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += (size_t)gridDim.x * blockDim.x) {
+            y[row] = row_apply<T, false>(A, row, xv);
+            z[row] = t[row];
+        }
+        return;
+    }
+    const int lane = threadIdx.x & (L - 1);
+    const size_t warpRows = 32 / L;
+    const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+    const size_t sub = (threadIdx.x & 31) / L;
+    for (size_t base = gw * warpRows; base < A.nrow; base += nwarps * warpRows) {
+        const size_t row = base + sub;
+        T sum = T(0);
+        if (row < A.nrow)
+            for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
+                sum = fma(A.val[k], xv(A.colInd[k]), sum);
+        sum = group_sum<L>(sum);
+        if (lane == 0 && row < A.nrow) {
+            y[row] = sum;
+            z[row] = t[row];
+        }
+    }
+}
+
+template <typename T, typename F>
+static void lanes_launch(Ctx& c, const Mat& A, F&& go)
+{
+    switch (A.lanes) {
+        case 1: go(std::integral_constant<int, 1>()); break;
+        case 2: go(std::integral_constant<int, 2>()); break;
+        case 4: go(std::integral_constant<int, 4>()); break;
+        case 8: go(std::integral_constant<int, 8>()); break;
+        case 16: go(std::integral_constant<int, 16>()); break;
+        default: go(std::integral_constant<int, 32>()); break;
+    }
+}
+
 template <typename T, int MODE>
 static void gm_apply_launch(Ctx& c, const Mat& A, CSRView<T> V, const T* v, const T* dinv,
                             T* y, const int* stop)
@@ -1316,7 +1424,8 @@ CSRView<float> gm_view<float>(const Mat& A) { return A.v32(); }
 template <typename T>
 static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t steps, bool left,
                            uint32_t& count, uint32_t& numIter, double& resAbs, double denAbs,
-                           const fasp_gpu_params& P, int& stopped)
+                           const fasp_gpu_params& P, int& stopped, T* Z = nullptr,
+                           T* tmp = nullptr)
 {
     Ctx& c = S.c;
     const uint32_t n = S.n;
@@ -1344,10 +1453,31 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
         dinv = S.pcd.dinv;
     const int mode = S.pcd.type == 0 ? 0 : (left ? 2 : 1);
     double* tn = c.dslot + SL_T5;
+    const int needS = c.grid((long long)n * S.A->lanes, kBlock);
     for (uint32_t k = 1; k <= steps; ++k) {
         const T* vin = V + (k - 1) * ld;
         T* vnew = V + k * ld;
-        if (mode == 0)
+        if (Z) { // FGMRES: Z_{k-1} = P(V_{k-1}) from its warm start, then A Z_{k-1}
+            T* zj = Z + (k - 1) * ld;
+            const T* t = vin;
+            if (S.pcd.type != 0) {
+                k_fg_norminf<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
+                    n, (const T*)zj, c.red, c.dslot + SL_T6, stop);
+                lanes_launch<T>(c, *S.A, [&](auto LL) {
+                    auto kern = k_fg_sweep<T, decltype(LL)::value>;
+                    kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock)), kBlock,
+                           0, c.stream>>>(AV, vin, (const T*)zj, dinv, c.dslot + SL_T6, tmp,
+                                          stop);
+                });
+                t = tmp;
+                c.launches += 2;
+            }
+            lanes_launch<T>(c, *S.A, [&](auto LL) {
+                auto kern = k_fg_apply<T, decltype(LL)::value>;
+                kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock)), kBlock, 0,
+                       c.stream>>>(AV, t, zj, vnew, stop);
+            });
+        } else if (mode == 0)
             gm_apply_launch<T, 0>(c, *S.A, AV, vin, dinv, vnew, stop);
         else if (mode == 1)
             gm_apply_launch<T, 1>(c, *S.A, AV, vin, dinv, vnew, stop);
@@ -1442,7 +1572,7 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
             const uint32_t steps = std::min<uint32_t>(restart, P.maxIter - numIter);
             int stopped = 0;
             if ((e = gm_cycle_device<T>(*this, L, V, steps, false, count, numIter, resAbs, denAbs,
-                                        P, stopped)))
+                                        P, stopped, flexible ? Z : nullptr, tmp)))
                 return e;
             count_1 = count - 1;
             if (!(stopped == 1 && count == 1)) { // a breakdown step updates nothing

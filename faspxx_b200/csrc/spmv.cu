@@ -430,14 +430,35 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
         nrow, T.rowPtr, T.colInd, T.val, T.diagPtr, T.diag);
     FB_CUDA(cudaGetLastError());
     T.lanes = lanes_for(T.meanRowLen);
-    if (values && T.lanes == 1) {
-        std::vector<double> hv;
-        const double* cv = values;
-        if (!hostPtrs) {
-            hv.resize(nnz);
-            FB_CUDA(cudaMemcpy(hv.data(), values, (size_t)nnz * 8, cudaMemcpyDeviceToHost));
-            cv = hv.data();
+    std::vector<double> hv;
+    const double* cv = values;
+    if (values && !hostPtrs) {
+        hv.resize(nnz);
+        FB_CUDA(cudaMemcpy(hv.data(), values, (size_t)nnz * 8, cudaMemcpyDeviceToHost));
+        cv = hv.data();
+    }
+    if (values && nrow == mcol && nrow > 0) { // one diagonal value (bitwise) in every row?
+        bool same = true, first = true;
+        double d0 = 0.0;
+        for (uint32_t r = 0; r < nrow && same; ++r) {
+            bool found = false;
+            for (uint32_t k = crp[r]; k < crp[r + 1]; ++k)
+                if (cci[k] == r) {
+                    found = true;
+                    if (first) {
+                        d0 = cv[k];
+                        first = false;
+                    } else if (std::memcmp(&cv[k], &d0, 8) != 0) {
+                        same = false;
+                    }
+                    break;
+                }
+            same = same && found;
         }
+        T.diagConst = same && d0 != 0.0;
+        T.diagValue = d0;
+    }
+    if (values && T.lanes == 1) {
         RowClasses R;
         if (build_row_classes(nrow, crp, cci, cv, R) && (e = upload_row_classes(T, R, s))) {
             m_free(T);
