@@ -78,6 +78,25 @@ static Ctx* vec_ctx(int* err)
     return c;
 }
 
+// A handle whose matrix is built by `build` on the handle's own stream.
+template <typename F>
+static int mat_build(fasp_gpu_mat* out, F build)
+{
+    if (!out) return kErrInputPar;
+    *out = nullptr;
+    fasp_gpu_mat h = new (std::nothrow) fasp_gpu_mat_s();
+    if (!h) return kErrAlloc;
+    int e = h->c.init(g_device);
+    if (!e) e = build(h);
+    if (e) {
+        h->c.destroy();
+        delete h;
+        return e;
+    }
+    *out = h;
+    return kOk;
+}
+
 extern "C" {
 
 int fasp_gpu_abi_version(void) { return FASP_GPU_ABI_VERSION; }
@@ -235,6 +254,25 @@ int fasp_gpu_mat_create_device(uint32_t nrow, uint32_t mcol, uint32_t nnz,
                                const double* values, fasp_gpu_mat* out)
 {
     return mat_create(nrow, mcol, nnz, rowPtr, colInd, values, false, out);
+}
+
+int fasp_gpu_mat_create_coo(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+                            const uint32_t* colInd, const double* values, int onDevice,
+                            fasp_gpu_mat* out)
+{
+    return mat_build(out, [&](fasp_gpu_mat h) {
+        return m_from_coo(h->c, nrow, mcol, nnz, rowInd, colInd, values, onDevice != 0, h->M);
+    });
+}
+
+int fasp_gpu_mat_create_csr_raw(uint32_t nrow, uint32_t mcol, uint32_t nnz,
+                                const uint32_t* rowPtr, const uint32_t* colInd,
+                                const double* values, int onDevice, fasp_gpu_mat* out)
+{
+    return mat_build(out, [&](fasp_gpu_mat h) {
+        return m_from_csr_raw(h->c, nrow, mcol, nnz, rowPtr, colInd, values, onDevice != 0,
+                              h->M);
+    });
 }
 
 int fasp_gpu_mat_destroy(fasp_gpu_mat A)

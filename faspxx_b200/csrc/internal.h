@@ -216,6 +216,12 @@ int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const doub
 int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
              const uint32_t* colInd, const double* values, bool hostPtrs, cudaStream_t s);
 void m_free(Mat& M);
+// ReadMat's conversions on the device (ingest.cu): MTXtoMAT of 0-based triplets, and
+// ReadCSR's shift + SortCSRRow + CSRtoMAT of raw CSR arrays (0- or 1-based).
+int m_from_coo(Ctx& c, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+               const uint32_t* colInd, const double* values, bool onDevice, Mat& M);
+int m_from_csr_raw(Ctx& c, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
+                   const uint32_t* colInd, const double* values, bool onDevice, Mat& M);
 int m_spmv(Ctx& c, const Mat& A, const double* x, double* y);           // y = A x
 int m_spmv32(Ctx& c, const Mat& A, const float* x, float* y);
 inline int m_spmv(Ctx& c, const Mat& A, const float* x, float* y) { return m_spmv32(c, A, x, y); }

@@ -168,6 +168,35 @@ def batch_systems(count: int = 4096, mlo: int = 16, mhi: int = 128, nrhs: int = 
     return ms, sig, rhs
 
 
+def read_csr_raw(path: str):
+    """The arrays ReadCSR (src/ReadData.cxx:221-358) reads from a text CSR file, before any
+    conversion: n, then rowPtr[n + 1], colInd[nnz], values[nnz] as stored in the file
+    (0- or 1-based, each row's entries in file order). Returns (n, rowPtr, colInd, values)."""
+    with open(path) as f:
+        tok = f.read().split()
+    n = int(tok[0])
+    rp = np.array(tok[1:n + 2], dtype=np.int64)
+    nnz = int(rp[n] - rp[0])
+    ci = np.array(tok[n + 2:n + 2 + nnz], dtype=np.int64)
+    va = np.array(tok[n + 2 + nnz:n + 2 + 2 * nnz], dtype=np.float64)
+    return n, rp.astype(np.uint32), ci.astype(np.uint32), va
+
+
+def read_mtx_raw(path: str):
+    """The triplets ReadMTX (src/ReadData.cxx:98-218) reads from a MatrixMarket file: lines
+    starting with '%' skipped, then 'nrow mcol nnz', then nnz lines 'i j value' with 1-based
+    indices, returned 0-based in file order: (nrow, mcol, rowInd, colInd, values)."""
+    with open(path) as f:
+        lines = [ln for ln in f if not ln.startswith("%")]
+    tok = " ".join(lines).split()
+    nrow, mcol, nnz = int(tok[0]), int(tok[1]), int(tok[2])
+    t = np.array(tok[3:3 + 3 * nnz], dtype=object).reshape(nnz, 3)
+    ri = t[:, 0].astype(np.int64) - 1
+    ci = t[:, 1].astype(np.int64) - 1
+    va = t[:, 2].astype(np.float64)
+    return nrow, mcol, ri.astype(np.uint32), ci.astype(np.uint32), va
+
+
 def read_csr_text(path: str) -> CSRMatrix:
     """FASP++ ReadMat of a text CSR file (src/ReadData.cxx:221-446): n, then n+1 row
     pointers, nnz column indices and nnz values; 1-based indices are shifted to 0-based,

@@ -114,6 +114,37 @@ class MAT:
         check(lib.fasp_gpu_mat_info(self.h, C.byref(n), C.byref(m), C.byref(z)), "info")
         self.nrow, self.mcol, self.nnz = n.value, m.value, z.value
 
+    @classmethod
+    def FromCOO(cls, nrow: int, mcol: int, rowInd, colInd, values) -> "MAT":
+        """MTXtoMAT (src/MATUtil.cxx:416-436) on the GPU: 0-based triplets in any order,
+        duplicates kept, rows sorted stably by column, missing diagonals stored as 0.0.
+        The arrays are host NumPy arrays, or DVec-like objects with a device ``ptr``
+        (row and column indices as uint32, values as float64)."""
+        return cls._ingest(lib.fasp_gpu_mat_create_coo, "MTXtoMAT", nrow, mcol, _count(values),
+                           rowInd, colInd, values)
+
+    @classmethod
+    def FromCSRRaw(cls, nrow: int, rowPtr, colInd, values, mcol: int | None = None) -> "MAT":
+        """ReadMat's .csr conversions (src/ReadData.cxx:350-353,376-400) on the GPU: raw
+        CSR arrays, 0- or 1-based, rows in any column order."""
+        return cls._ingest(lib.fasp_gpu_mat_create_csr_raw, "ReadCSR", nrow,
+                           nrow if mcol is None else mcol, _count(values), rowPtr, colInd,
+                           values)
+
+    @classmethod
+    def _ingest(cls, fn, where, nrow, mcol, nnz, a, b, v) -> "MAT":
+        capi.init()
+        dev = hasattr(v, "ptr")
+        if dev:
+            ptrs = [x.ptr for x in (a, b, v)]
+        else:
+            keep = [np.ascontiguousarray(a, np.uint32), np.ascontiguousarray(b, np.uint32),
+                    np.ascontiguousarray(v, np.float64)]
+            ptrs = [x.ctypes.data for x in keep]
+        h = C.c_void_p()
+        check(fn(nrow, mcol, nnz, *ptrs, 1 if dev else 0, C.byref(h)), where)
+        return cls(_handle=h)
+
     def GetRowSize(self) -> int:
         return self.nrow
 
@@ -178,6 +209,25 @@ class MAT:
         if getattr(self, "h", None):
             lib.fasp_gpu_mat_destroy(self.h)
             self.h = None
+
+
+def _count(a) -> int:
+    return int(a.n) if hasattr(a, "ptr") else len(a)
+
+
+def ReadMat(path: str) -> MAT:
+    """ReadMat (src/ReadData.cxx:361-446): a .csr or .mtx file by its extension. The text
+    is parsed on the host (read_csr_raw / read_mtx_raw); sorting, the 1-based shift and
+    the diagonal insertion run on the GPU. Unknown extension: ERROR_INPUT_FILE (-11)."""
+    from .problems import read_csr_raw, read_mtx_raw
+    ext = path[-3:].lower() if len(path) > 4 else ""
+    if ext == "csr":
+        n, rp, ci, va = read_csr_raw(path)
+        return MAT.FromCSRRaw(n, rp, ci, va)
+    if ext == "mtx":
+        nrow, mcol, ri, ci, va = read_mtx_raw(path)
+        return MAT.FromCOO(nrow, mcol, ri, ci, va)
+    raise capi.FaspError(-11, "ReadMat")
 
 
 class SOL:

@@ -134,6 +134,27 @@ int fasp_gpu_mat_create(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32
 int fasp_gpu_mat_create_device(uint32_t nrow, uint32_t mcol, uint32_t nnz,
                                const uint32_t* rowPtr, const uint32_t* colInd,
                                const double* values, fasp_gpu_mat* out);
+/* ReadMat (src/ReadData.cxx:361-446) after its readers, on the device: the arrays that
+ * ReadMTX (ReadData.cxx:98-218) returns -- 0-based row and column indices of nnz entries in
+ * any order -- converted as MTXtoMAT does (src/MATUtil.cxx:416-436): rows counted and
+ * scattered (MTXtoCSR, :252-300), each row sorted by column with equal columns kept in
+ * input order (SortCSRRow, :439-476; duplicates are kept, not summed), and an explicit 0.0
+ * diagonal inserted in rows without one (CSRtoMAT, :303-413). onDevice != 0: the three
+ * arrays are device memory; otherwise host memory. ERROR_MAT_DATA for an index out of
+ * range or a row >= mcol without a diagonal (the reference's MTXtoMAT leaves the MAT empty
+ * and returns SUCCESS there); ERROR_MAT_SIZE for a zero size. */
+int fasp_gpu_mat_create_coo(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+                            const uint32_t* colInd, const double* values, int onDevice,
+                            fasp_gpu_mat* out);
+/* The .csr branch of ReadMat on the device: the arrays ReadCSR (ReadData.cxx:221-358)
+ * reads -- rowPtr[nrow + 1], colInd[nnz], values[nnz], 0-based or 1-based (rowPtr[0] == 1;
+ * shifted as ReadData.cxx:350-353 does) with rows in any column order -- then SortCSRRow
+ * and CSRtoMAT as above. ReadCSR's files are square: pass mcol = nrow for them.
+ * ERROR_MAT_DATA when rowPtr[0] is neither 0 nor 1, rowPtr is not monotone,
+ * rowPtr[nrow] - rowPtr[0] != nnz, or a column is out of range. */
+int fasp_gpu_mat_create_csr_raw(uint32_t nrow, uint32_t mcol, uint32_t nnz,
+                                const uint32_t* rowPtr, const uint32_t* colInd,
+                                const double* values, int onDevice, fasp_gpu_mat* out);
 int fasp_gpu_mat_destroy(fasp_gpu_mat A);
 /* GetRowSize / GetColSize / GetNNZ (LOP.hxx:50-53, MAT.hxx:113) */
 int fasp_gpu_mat_info(fasp_gpu_mat A, uint32_t* nrow, uint32_t* mcol, uint32_t* nnz);

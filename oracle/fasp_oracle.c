@@ -235,6 +235,143 @@ void orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* r
 }
 
 /* ------------------------------------------------------------------------------------
+ * ReadMat's conversions (src/ReadData.cxx:361-446, src/MATUtil.cxx:110-476)
+ * ---------------------------------------------------------------------------------- */
+
+#define ERROR_MAT_DATA -17
+
+/* CheckCSR, MATUtil.cxx:110-174 (the array-size checks hold by construction here). */
+static int check_csr(uint32_t row, uint32_t col, uint32_t nnz, const uint32_t* colInd,
+                     const uint32_t* rowPtr)
+{
+    if (row == 0 || col == 0 || nnz == 0) return SUCCESS;
+    if (nnz != rowPtr[row] - rowPtr[0]) return ERROR_MAT_DATA;
+    for (uint32_t j = 0; j < row; ++j)
+        if (rowPtr[j] > rowPtr[j + 1]) return ERROR_MAT_DATA;
+    for (uint32_t j = 0; j < row; ++j)
+        for (uint32_t k = rowPtr[j]; k < rowPtr[j + 1]; ++k)
+            if (colInd[k] >= col) return ERROR_MAT_DATA;
+    return SUCCESS;
+}
+
+/* SortCSRRow, MATUtil.cxx:439-476: a stable insertion sort of each row by column (the
+ * reference's unsigned inner index is signed here; it wraps when an entry of row 0 moves
+ * to the front). */
+static void sort_rows(uint32_t row, const uint32_t* rowPtr, uint32_t* colInd, double* values)
+{
+    for (uint32_t j = 0; j < row; ++j) {
+        const int64_t begin = rowPtr[j], end = rowPtr[j + 1];
+        for (int64_t k = begin + 1; k < end; ++k) {
+            const uint32_t index = colInd[k];
+            const double data = values[k];
+            int64_t l = k - 1;
+            for (; l >= begin && index < colInd[l]; --l) {
+                colInd[l + 1] = colInd[l];
+                values[l + 1] = values[l];
+            }
+            colInd[l + 1] = index;
+            values[l + 1] = data;
+        }
+    }
+}
+
+/* CSRtoMAT, MATUtil.cxx:303-413: rows without a diagonal entry get 0.0 after their
+ * entries of smaller column; then CheckCSR. Output arrays hold nnz + row entries.
+ * Returns the code; *nnzOut = 0 when the check fails (the MAT is not set). */
+static int csr_to_mat(uint32_t row, uint32_t col, uint32_t nnz, const double* values,
+                      const uint32_t* colInd, const uint32_t* rowPtr, uint32_t* nnzOut,
+                      uint32_t* rpOut, uint32_t* ciOut, double* vaOut)
+{
+    uint32_t count = 0, added = 0;
+    rpOut[0] = 0;
+    for (uint32_t i = 0; i < row; ++i) {
+        const uint32_t begin = rowPtr[i], end = rowPtr[i + 1];
+        int found = 0;
+        for (uint32_t k = begin; k < end; ++k)
+            if (colInd[k] == i) {
+                found = 1;
+                break;
+            }
+        uint32_t k = begin;
+        if (!found) {
+            for (; k < end && colInd[k] < i; ++k) {
+                vaOut[count] = values[k];
+                ciOut[count++] = colInd[k];
+            }
+            vaOut[count] = 0.0;
+            ciOut[count++] = i;
+            ++added;
+        }
+        for (; k < end; ++k) {
+            vaOut[count] = values[k];
+            ciOut[count++] = colInd[k];
+        }
+        rpOut[i + 1] = rowPtr[i + 1] + added;
+    }
+    *nnzOut = 0;
+    const int code = check_csr(row, col, nnz + added, ciOut, rpOut);
+    if (code == SUCCESS) *nnzOut = nnz + added;
+    return code;
+}
+
+int orc_mtx_to_mat(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+                   const uint32_t* colInd, const double* values, uint32_t* nnzOut,
+                   uint32_t* rowPtr, uint32_t* colIndOut, double* valuesOut)
+{
+    *nnzOut = 0;
+    for (uint32_t j = 0; j < nnz; ++j)
+        if (rowInd[j] >= nrow) return ERROR_MAT_DATA; /* the reference writes out of bounds */
+    /* MTXtoCSR, MATUtil.cxx:252-300: count, prefix, scatter in input order, shift back */
+    uint32_t* rp = (uint32_t*)calloc((size_t)nrow + 1, 4);
+    uint32_t* ci = (uint32_t*)malloc((size_t)nnz * 4 + 4);
+    double* va = (double*)malloc((size_t)nnz * 8 + 8);
+    for (uint32_t j = 0; j < nnz; ++j) ++rp[rowInd[j] + 1];
+    for (uint32_t i = 1; i < nrow; ++i) rp[i] += rp[i - 1];
+    for (uint32_t j = 0; j < nnz; ++j) {
+        const uint32_t p = rp[rowInd[j]]++;
+        ci[p] = colInd[j];
+        va[p] = values[j];
+    }
+    for (uint32_t i = nrow; i > 0; --i) rp[i] = rp[i - 1];
+    rp[0] = 0;
+    sort_rows(nrow, rp, ci, va);
+    /* MTXtoMAT (MATUtil.cxx:416-436) ignores the codes of its three steps */
+    csr_to_mat(nrow, mcol, nnz, va, ci, rp, nnzOut, rowPtr, colIndOut, valuesOut);
+    free(rp);
+    free(ci);
+    free(va);
+    return SUCCESS;
+}
+
+int orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr, const uint32_t* colInd,
+                   const double* values, uint32_t* nnzOut, uint32_t* rowPtrOut,
+                   uint32_t* colIndOut, double* valuesOut)
+{
+    *nnzOut = 0;
+    uint32_t* rp = (uint32_t*)malloc(((size_t)nrow + 1) * 4);
+    uint32_t* ci = (uint32_t*)malloc((size_t)nnz * 4 + 4);
+    double* va = (double*)malloc((size_t)nnz * 8 + 8);
+    memcpy(rp, rowPtr, ((size_t)nrow + 1) * 4);
+    memcpy(ci, colInd, (size_t)nnz * 4);
+    memcpy(va, values, (size_t)nnz * 8);
+    if (rp[0] == 1) { /* ReadCSR, ReadData.cxx:350-353 */
+        for (uint32_t i = 0; i <= nrow; ++i) rp[i]--;
+        for (uint32_t k = 0; k < nnz; ++k) ci[k]--;
+    }
+    /* ReadMat's .csr branch (ReadData.cxx:376-400): SortCSRRow, then CSRtoMAT; the sort's
+     * check runs first here so that a bad rowPtr is never followed */
+    int code = (rp[0] == 0) ? check_csr(nrow, nrow, nnz, ci, rp) : ERROR_MAT_DATA;
+    if (code == SUCCESS) {
+        sort_rows(nrow, rp, ci, va);
+        code = csr_to_mat(nrow, nrow, nnz, va, ci, rp, nnzOut, rowPtrOut, colIndOut, valuesOut);
+    }
+    free(rp);
+    free(ci);
+    free(va);
+    return code;
+}
+
+/* ------------------------------------------------------------------------------------
  * Solver objects (src/SOL.hxx, CG.cxx, BiCGStab.cxx, GMRES.cxx, FGMRES.cxx, Iter.cxx,
  * MG.cxx)
  * ---------------------------------------------------------------------------------- */

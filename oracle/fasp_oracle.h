@@ -91,6 +91,25 @@ void   orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
 void   orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
                    uint32_t* diagPtr);
 
+/* ReadMat's conversions (src/ReadData.cxx:361-446). Outputs hold nrow + 1, nnz + nrow and
+ * nnz + nrow entries; *nnzOut = the nnz of the resulting MAT, 0 when it is left empty.
+ * orc_mtx_to_mat: MTXtoMAT (src/MATUtil.cxx:416-436) of ReadMTX's 0-based triplets;
+ *   returns MTXtoMAT's code, which is SUCCESS even when CSRtoMAT's check fails.
+ * orc_csr_to_mat: ReadCSR's 1-based shift (ReadData.cxx:350-353), SortCSRRow and
+ *   CSRtoMAT (ReadData.cxx:376-400) of a square matrix's raw CSR arrays; returns the code.
+ * The reference library returns ORC_REF_UNDEFINED, without calling the reference, for
+ * inputs on which the reference reads or writes out of bounds: a row index >= nrow; an
+ * entry of row 0 that sorts before the row's first entry (SortCSRRow's unsigned index
+ * wraps, MATUtil.cxx:459); an empty first row without a diagonal (CSRtoMAT reads
+ * colInd[-1], :369). */
+#define ORC_REF_UNDEFINED (-1000)
+int    orc_mtx_to_mat(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+                      const uint32_t* colInd, const double* values, uint32_t* nnzOut,
+                      uint32_t* rowPtr, uint32_t* colIndOut, double* valuesOut);
+int    orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr,
+                      const uint32_t* colInd, const double* values, uint32_t* nnzOut,
+                      uint32_t* rowPtrOut, uint32_t* colIndOut, double* valuesOut);
+
 /* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
 int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
                        uint32_t* colInd, double* values);

@@ -85,6 +85,10 @@ def load(kind: str = "port") -> C.CDLL:
     lib.orc_transpose.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p, C.c_void_p,
                                   _u32p, _u32p, C.c_void_p, C.c_void_p]
     lib.orc_diagptr.argtypes = [C.c_uint32, _u32p, _u32p, _u32p]
+    lib.orc_mtx_to_mat.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p,
+                                   C.POINTER(C.c_uint32), _u32p, _u32p, _f64p]
+    lib.orc_csr_to_mat.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p,
+                                   C.POINTER(C.c_uint32), _u32p, _u32p, _f64p]
     _LIBS[kind] = lib
     return lib
 
@@ -208,3 +212,37 @@ def transpose(kind, mat):
     lib.orc_transpose(mat.nrow, mat.mcol, nnz, mat.rowPtr, mat.colInd, _vptr(mat.values),
                       trp, tci, _vptr(tva), tdp.ctypes.data_as(C.c_void_p))
     return trp, tci, tva, tdp
+
+
+# ORC_REF_UNDEFINED (fasp_oracle.h): the reference indexes out of bounds on this input.
+REF_UNDEFINED = -1000
+
+
+def _converted(code, nnz_out, rp, ci, va):
+    n = nnz_out.value
+    return code, (rp, ci[:n].copy(), va[:n].copy()) if n else None
+
+
+def mtx_to_mat(kind, nrow, mcol, rowInd, colInd, values):
+    """MTXtoMAT of 0-based triplets: (code, (rowPtr, colInd, values) or None if empty)."""
+    ri = np.ascontiguousarray(rowInd, np.uint32)
+    ci = np.ascontiguousarray(colInd, np.uint32)
+    va = np.ascontiguousarray(values, np.float64)
+    cap = len(ci) + nrow
+    rp_o, ci_o, va_o = np.zeros(nrow + 1, np.uint32), np.empty(cap, np.uint32), np.empty(cap)
+    z = C.c_uint32()
+    code = load(kind).orc_mtx_to_mat(nrow, mcol, len(ci), ri, ci, va, C.byref(z), rp_o, ci_o,
+                                     va_o)
+    return _converted(code, z, rp_o, ci_o, va_o)
+
+
+def csr_to_mat(kind, nrow, rowPtr, colInd, values):
+    """ReadMat's .csr conversions of raw (0- or 1-based) CSR arrays: (code, arrays or None)."""
+    rp = np.ascontiguousarray(rowPtr, np.uint32)
+    ci = np.ascontiguousarray(colInd, np.uint32)
+    va = np.ascontiguousarray(values, np.float64)
+    cap = len(ci) + nrow
+    rp_o, ci_o, va_o = np.zeros(nrow + 1, np.uint32), np.empty(cap, np.uint32), np.empty(cap)
+    z = C.c_uint32()
+    code = load(kind).orc_csr_to_mat(nrow, len(ci), rp, ci, va, C.byref(z), rp_o, ci_o, va_o)
+    return _converted(code, z, rp_o, ci_o, va_o)

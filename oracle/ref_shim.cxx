@@ -24,6 +24,7 @@
 #include "GMRES.hxx"
 #include "Iter.hxx"
 #include "MAT.hxx"
+#include "MATUtil.hxx"
 #include "MG.hxx"
 #include "ReadData.hxx"
 #include "VEC.hxx"
@@ -348,6 +349,87 @@ void orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
                 break;
             }
     }
+}
+
+/* The MAT's arrays; *nnzOut = 0 for an empty MAT. */
+static void copy_mat(const MAT& A, uint32_t* nnzOut, uint32_t* rowPtr, uint32_t* colInd,
+                     double* values)
+{
+    *nnzOut = A.GetNNZ();
+    if (*nnzOut == 0) return;
+    int* rp = A.GetRowPtr();
+    int* ci = A.GetColInd();
+    double* va = A.GetValues();
+    for (uint32_t i = 0; i <= A.GetRowSize(); ++i) rowPtr[i] = (uint32_t)rp[i];
+    for (uint32_t k = 0; k < *nnzOut; ++k) {
+        colInd[k] = (uint32_t)ci[k];
+        values[k] = va[k];
+    }
+    delete[] rp;
+    delete[] ci;
+    delete[] va;
+}
+
+/* Inputs on which SortCSRRow or CSRtoMAT index out of bounds (fasp_oracle.h): rp is the
+ * 0-based row pointer of the rows as they reach SortCSRRow. */
+static bool row0_undefined(const std::vector<USI>& rp, const std::vector<USI>& ci)
+{
+    if (rp.size() < 2) return false;
+    if (rp[1] == rp[0]) return true; /* empty first row: CSRtoMAT reads colInd[end - 1] */
+    for (USI k = rp[0] + 1; k < rp[1]; ++k)
+        if (ci[k] < ci[rp[0]]) return true; /* SortCSRRow moves it to position 0 */
+    return false;
+}
+
+int orc_mtx_to_mat(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowInd,
+                   const uint32_t* colInd, const double* values, uint32_t* nnzOut,
+                   uint32_t* rowPtr, uint32_t* colIndOut, double* valuesOut)
+{
+    *nnzOut = 0;
+    std::vector<USI> ri(rowInd, rowInd + nnz), ci(colInd, colInd + nnz);
+    std::vector<DBL> va(values, values + nnz);
+    /* the first row as MTXtoCSR's stable scatter hands it to SortCSRRow */
+    std::vector<USI> rp0{0, 0}, ci0;
+    for (uint32_t j = 0; j < nnz; ++j) {
+        if (ri[j] >= nrow) return ORC_REF_UNDEFINED;
+        if (ri[j] == 0) ci0.push_back(ci[j]);
+    }
+    rp0[1] = (USI)ci0.size();
+    if (row0_undefined(rp0, ci0)) return ORC_REF_UNDEFINED;
+    MAT A;
+    std::ostringstream sink;
+    std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
+    const FaspRetCode code = MTXtoMAT(nrow, mcol, nnz, ri, ci, va, A);
+    std::cout.rdbuf(old);
+    copy_mat(A, nnzOut, rowPtr, colIndOut, valuesOut);
+    return static_cast<int>(code);
+}
+
+int orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr, const uint32_t* colInd,
+                   const double* values, uint32_t* nnzOut, uint32_t* rowPtrOut,
+                   uint32_t* colIndOut, double* valuesOut)
+{
+    *nnzOut = 0;
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    std::vector<DBL> va(values, values + nnz);
+    USI row = nrow, col = nrow, nz = nnz;
+    if (rp[0] == 1) { /* ReadCSR's shift, ReadData.cxx:350-353 */
+        for (auto& v : rp) --v;
+        for (auto& v : ci) --v;
+    }
+    /* SortCSRRow sorts before it checks: only well-formed row pointers reach it */
+    if (rp[0] != 0 || rp[nrow] != nnz) return ORC_REF_UNDEFINED;
+    for (uint32_t i = 0; i < nrow; ++i)
+        if (rp[i] > rp[i + 1]) return ORC_REF_UNDEFINED;
+    if (row0_undefined(rp, ci)) return ORC_REF_UNDEFINED;
+    MAT A;
+    std::ostringstream sink;
+    std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
+    FaspRetCode code = SortCSRRow(row, col, nz, rp, ci, va); /* ReadData.cxx:376-400 */
+    if (code >= 0) code = CSRtoMAT(row, col, nz, va, ci, rp, A);
+    std::cout.rdbuf(old);
+    copy_mat(A, nnzOut, rowPtrOut, colIndOut, valuesOut);
+    return static_cast<int>(code);
 }
 
 /* ReadMat (src/ReadData.cxx:361-446) of a .csr/.mtx file: call once with NULL arrays to

@@ -151,3 +151,43 @@ def solver_cases():
 def transpose_cases():
     return [("fdm_10X10", matrix("fdm_10X10")), ("fem_small", matrix("fem_small")),
             ("convdiff_pe10", matrix("convdiff_pe10")), ("jacobi3", matrix("jacobi3"))]
+
+
+# ---- ReadMat conversions (reference_ingest.npz / .json, written by make_golden.py) ----------
+
+_INGEST: dict = {}
+
+
+def ingest_cases() -> dict:
+    """name -> dict(kind, nrow, mcol, code, nnz, inputs=(a, b, values), expected=(rowPtr,
+    colInd, values) or None when the reference leaves the MAT empty)."""
+    if _INGEST:
+        return _INGEST
+    import json
+    meta = json.load(open(os.path.join(HERE, "reference_ingest.json")))
+    z = np.load(os.path.join(HERE, "reference_ingest.npz"))
+    for name, m in meta.items():
+        d = dict(m)
+        d["inputs"] = (z[name + "__in0"], z[name + "__in1"], z[name + "__in2"])
+        d["expected"] = ((z[name + "__rowPtr"], z[name + "__colInd"], z[name + "__values"])
+                         if m["nnz"] else None)
+        _INGEST[name] = d
+    return _INGEST
+
+
+def write_mtx(path: str, nrow: int, mcol: int, ri, ci, va) -> None:
+    """MatrixMarket text of 0-based triplets (1-based in the file), values in repr form."""
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{nrow} {mcol} {len(va)}\n")
+        for i, j, v in zip(ri, ci, va):
+            f.write(f"{int(i) + 1} {int(j) + 1} {float(v)!r}\n")
+
+
+def write_csr(path: str, n: int, rp, ci, va) -> None:
+    """The text CSR layout ReadCSR reads: n, rowPtr, colInd, values, one number per line."""
+    with open(path, "w") as f:
+        f.write(f"{n}\n")
+        for a in (rp, ci):
+            f.write("".join(f"{int(x)}\n" for x in a))
+        f.write("".join(f"{float(x)!r}\n" for x in va))

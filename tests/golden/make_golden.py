@@ -11,9 +11,13 @@ Run in a container that has the reference tree (default /root/reference) after
 * ``reference_runs.npz`` + ``reference_runs.json`` -- outputs of the compiled reference
   (oracle/_ref/liboracle_ref.so) for every solver configuration the tests replay: return
   code, iteration count, norms, the solution x and the printed residual history;
-* ``reference_transpose.npz`` -- MAT::TransInPlace results, the bit-exact target for CSC.
+* ``reference_transpose.npz`` -- MAT::TransInPlace results, the bit-exact target for CSC;
+* ``reference_ingest.npz`` + ``reference_ingest.json`` -- ReadMat's conversions run by the
+  reference (MTXtoMAT; ReadCSR's shift + SortCSRRow + CSRtoMAT) on the bundled data/*.csr
+  and data/nos7.mtx arrays and on seeded synthetic inputs: shuffled entries, duplicates,
+  missing and empty-row diagonals, long rows, rectangular and invalid matrices.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [--ingest-only]
 """
 from __future__ import annotations
 
@@ -89,5 +93,154 @@ def main(ref_root: str) -> None:
     print("wrote", len(runs_meta), "solver runs and", len(G.transpose_cases()), "transposes")
 
 
+def _front_row0(ri, ci, order):
+    """Reorders the entries so that row 0's first entry has its smallest column: the
+    reference's SortCSRRow indexes out of bounds when an entry moves to the front of row 0."""
+    order = list(order)
+    pos = [k for k, j in enumerate(order) if ri[j] == 0]
+    if pos:
+        best = min(pos, key=lambda k: (ci[order[k]], k))
+        order[pos[0]], order[best] = order[best], order[pos[0]]
+    return np.array(order, dtype=np.int64)
+
+
+def _coo(A: P.CSRMatrix):
+    rows = np.repeat(np.arange(A.nrow, dtype=np.int64), np.diff(A.rowPtr.astype(np.int64)))
+    return rows, A.colInd.astype(np.int64), A.values.copy()
+
+
+def _random_coo(rng, nrow, mcol, per_row, dup=0.1, drop_diag=0.2, empty=0.05):
+    """Random entries per row, some duplicated (same column, new value), some rows without
+    their diagonal, some rows empty (never row 0)."""
+    ri, ci = [], []
+    for r in range(nrow):
+        if r > 0 and rng.random() < empty:
+            continue
+        k = int(rng.integers(1, per_row + 1))
+        cols = list(rng.choice(mcol, size=min(k, mcol), replace=False))
+        if r < mcol:
+            if rng.random() < drop_diag:
+                cols = [c for c in cols if c != r] or [(r + 1) % mcol]
+            elif r not in cols:
+                cols.append(r)
+        cols += [c for c in cols if rng.random() < dup]
+        ri += [r] * len(cols)
+        ci += cols
+    ri, ci = np.array(ri, np.int64), np.array(ci, np.int64)
+    va = rng.standard_normal(len(ri))
+    return ri, ci, va
+
+
+def ingest_cases(ref_root: str):
+    """(name, kind, nrow, mcol, arrays) of every ingestion case; arrays are the reader's
+    output: (rowInd, colInd, values) for "mtx", (rowPtr, colInd, values) for "csr"."""
+    rng = np.random.default_rng(2024)
+    out = []
+    nr, mc, ri, ci, va = P.read_mtx_raw(os.path.join(ref_root, "data", "nos7.mtx"))
+    out.append(("nos7_mtx", "mtx", nr, mc, (ri, ci, va)))
+    for name in ("fdm_10X10", "fem_small"):
+        n, rp, ci, va = P.read_csr_raw(os.path.join(ref_root, "data", name + ".csr"))
+        out.append((name + "_csr", "csr", n, n, (rp, ci, va)))
+    # a stencil matrix with its triplets in random order
+    r, c, v = _coo(P.poisson2d(12))
+    o = _front_row0(r, c, rng.permutation(len(r)))
+    out.append(("poisson2d_shuffled_mtx", "mtx", 144, 144, (r[o], c[o], v[o])))
+    # duplicates, missing diagonals, empty rows
+    r, c, v = _random_coo(rng, 60, 60, 6)
+    o = _front_row0(r, c, rng.permutation(len(r)))
+    out.append(("random_dup_mtx", "mtx", 60, 60, (r[o], c[o], v[o])))
+    # wide: every row can take its diagonal
+    r, c, v = _random_coo(rng, 30, 47, 8)
+    o = _front_row0(r, c, rng.permutation(len(r)))
+    out.append(("wide_mtx", "mtx", 30, 47, (r[o], c[o], v[o])))
+    # tall: rows >= mcol have no diagonal place, CSRtoMAT's check fails (MAT left empty)
+    r, c, v = _random_coo(rng, 40, 30, 5)
+    o = _front_row0(r, c, rng.permutation(len(r)))
+    out.append(("tall_mtx", "mtx", 40, 30, (r[o], c[o], v[o])))
+    # a column out of range: CheckCSR fails (MAT left empty)
+    r, c, v = _random_coo(rng, 20, 20, 4)
+    c = c.copy()
+    c[len(c) // 2] = 20
+    o = _front_row0(r, c, np.arange(len(r)))
+    out.append(("badcol_mtx", "mtx", 20, 20, (r[o], c[o], v[o])))
+    # long rows: 33..4096 (one block per row), > 4096 (merge passes), duplicates included
+    lens = [3, 40, 700, 4096, 4097, 8300, 5, 1, 900]
+    ri, ci = [], []
+    for row, k in enumerate(lens):
+        cols = rng.integers(0, 5000, size=k)
+        if row == 0:
+            cols[0] = cols.min()
+        ri += [row] * k
+        ci += list(cols)
+    ri, ci = np.array(ri, np.int64), np.array(ci, np.int64)
+    va = rng.integers(-64, 65, size=len(ri)) / 8.0  # short fixtures: few distinct values
+    o = rng.permutation(len(ri))
+    o = _front_row0(ri, ci, o)
+    out.append(("long_rows_mtx", "mtx", len(lens), 5000, (ri[o], ci[o], va[o])))
+    # raw CSR: rows shuffled in place, 0-based and 1-based, missing diagonals, duplicates
+    for base, name in ((0, "shuffled0_csr"), (1, "dup1_csr")):
+        if base == 0:
+            A = P.poisson3d(5)
+            r, c, v = _coo(A)
+        else:
+            r, c, v = _random_coo(rng, 50, 50, 7)
+            o = np.lexsort((rng.random(len(r)), r))
+            r, c, v = r[o], c[o], v[o]
+        n = int(r.max()) + 1 if base == 0 else 50
+        rp = np.zeros(n + 1, np.int64)
+        np.cumsum(np.bincount(r, minlength=n), out=rp[1:])
+        c, v = c.copy(), v.copy()
+        for i in range(n):
+            seg = np.arange(rp[i], rp[i + 1])
+            perm = rng.permutation(seg)
+            if i == 0 and len(perm):
+                k = int(np.argmin(c[perm]))
+                perm[0], perm[k] = perm[k], perm[0]
+            c[seg], v[seg] = c[perm], v[perm]
+        out.append((name, "csr", n, n, (rp + base, c + base, v)))
+    return out
+
+
+def make_ingest(ref_root: str) -> None:
+    O.build(ref=True)
+    meta, arr = {}, {}
+    for name, kind, nrow, mcol, (a, b, v) in ingest_cases(ref_root):
+        if kind == "mtx":
+            code, res = O.mtx_to_mat("ref", nrow, mcol, a, b, v)
+        else:
+            code, res = O.csr_to_mat("ref", nrow, a, b, v)
+        assert code != O.REF_UNDEFINED, name
+        meta[name] = dict(kind=kind, nrow=int(nrow), mcol=int(mcol), code=int(code),
+                          nnz=0 if res is None else int(len(res[1])))
+        arr[name + "__in0"] = np.asarray(a, np.uint32)
+        arr[name + "__in1"] = np.asarray(b, np.uint32)
+        arr[name + "__in2"] = np.asarray(v, np.float64)
+        if res is not None:
+            arr[name + "__rowPtr"], arr[name + "__colInd"], arr[name + "__values"] = res
+    # the file reader itself on the bundled MatrixMarket file (ReadMat end to end)
+    A = P.read_mtx_raw(os.path.join(ref_root, "data", "nos7.mtx"))
+    code, res = O.mtx_to_mat("ref", *A)
+    lib = O.load("ref")
+    nrow, nnz = C.c_uint32(), C.c_uint32()
+    lib.orc_ref_readmat.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
+    path = os.path.join(ref_root, "data", "nos7.mtx").encode()
+    assert lib.orc_ref_readmat(path, C.byref(nrow), C.byref(nnz), None, None, None) == 0
+    rp = np.empty(nrow.value + 1, np.uint32)
+    ci = np.empty(nnz.value, np.uint32)
+    va = np.empty(nnz.value, np.float64)
+    lib.orc_ref_readmat(path, C.byref(nrow), C.byref(nnz), rp.ctypes.data, ci.ctypes.data,
+                        va.ctypes.data)
+    assert np.array_equal(rp, res[0]) and np.array_equal(ci, res[1]) and np.array_equal(va, res[2])
+    np.savez_compressed(os.path.join(HERE, "reference_ingest.npz"), **arr)
+    with open(os.path.join(HERE, "reference_ingest.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", len(meta), "ingestion cases")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    root = args[0] if args else "/root/reference"
+    if "--ingest-only" not in sys.argv:
+        main(root)
+    make_ingest(root)
