@@ -74,7 +74,11 @@ def profile_traffic(key: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a timed region.
+
+    nvidia-smi's start-up (NVML initialisation, device attach) disturbs GPU work that runs
+    at the same moment, so __enter__ waits for its first sample before the timed region
+    starts; samples from before the region are dropped when later ones exist."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -83,8 +87,17 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.rows = []
+        self.first = 0
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -92,27 +105,33 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        t0 = time.perf_counter()
+        while not self.rows and time.perf_counter() - t0 < 5.0:
+            time.sleep(0.01)
+        time.sleep(0.05)
+        self.first = len(self.rows)
         return self
 
     def __exit__(self, *exc):
-        self.rows = []
         if self.proc is None:
             return False
+        time.sleep(0.25)  # at least one sample ends inside or right after the region
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-            out = ""
-        for line in out.strip().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+        self.thread.join(timeout=5)
         return False
 
     def summary(self):
-        if not getattr(self, "rows", None):
+        rows = self.rows[self.first:] or self.rows
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        self.rows = rows
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         smax = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
         loaded = [s for s in sm if s > 0.5 * smax] or sm

@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
     }
     double a[3] = {(double)a0, (double)a1, (double)a2};
     const int ops[3] = {kSum, kSum, kSum};
-    grid_reduce<3>(a, ops, s, [=] __device__(const double* t) {
-        if (!c->bench) bi_after_p(c, t);
+    grid_reduce_ctl<3>(a, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
+        if (!cs->bench) bi_after_p(cs, t);
     });
 }
 
@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
     }
     double a[2] = {(double)a0, (double)a1};
     const int ops[2] = {kSum, kSum};
-    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
-        if (!c->bench) c->omega = t[0] / t[1];
+    grid_reduce_ctl<2>(a, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
+        if (!cs->bench) cs->omega = t[0] / t[1];
     });
 }
 
@@ -239,8 +239,8 @@ __global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T*
     }
     double a[5] = {(double)rr, (double)rr0, (double)xm, (double)pp, (double)xx};
     const int ops[5] = {kSum, kSum, kMax, kSum, kSum};
-    grid_reduce<5>(a, ops, s, [=] __device__(const double* t) {
-        if (!c->bench) bi_checks(c, t, 0);
+    grid_reduce_ctl<5>(a, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
+        if (!cs->bench) bi_checks(cs, t, 0);
     });
 }
 
@@ -274,11 +274,11 @@ __global__ void __launch_bounds__(kBlock) bi_resume(uint32_t n, const T* __restr
     }
     double a[2] = {(double)rr, (double)rr0};
     const int ops[2] = {kSum, kSum};
-    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
-        const double red[5] = {t[0], t[1], c->red[2], c->red[3], c->red[4]};
-        c->status = kRun;
-        c->reason = kBiNone;
-        bi_checks(c, red, c->phase);
+    grid_reduce_ctl<2>(a, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
+        const double red[5] = {t[0], t[1], cs->red[2], cs->red[3], cs->red[4]};
+        cs->status = kRun;
+        cs->reason = kBiNone;
+        bi_checks(cs, red, cs->phase);
     });
 }
 

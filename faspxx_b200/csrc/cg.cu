@@ -275,7 +275,9 @@ __device__ __noinline__ void cg_refresh_residual(RefreshView A, float* r32, floa
     }
     double a[3] = {rr64, (double)rr, (double)zr};
     const int ops[3] = {kSum, kSum, kSum};
-    grid_reduce<3>(a, ops, s, [=] __device__(const double* t) { cg_after_refresh(c, t); });
+    grid_reduce_ctl<3>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+        cg_after_refresh(cs, t);
+    });
 }
 
 // ---- kernels ---------------------------------------------------------------------------
@@ -340,15 +342,35 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
             acc = fma(sum, pi, acc);
         }
     };
+    // REC with JZ = 2: the gathers read r itself and the row's sum is scaled once,
+    // A z = zc (A r), instead of forming zc r_j for every gathered entry
     auto gv = [&](uint32_t j) {
-        if (REC) return zat(j);
+        if (REC) return JZ == 2 ? z[j] : zat(j);
         return mode ? fma(beta, pOld[j], zat(j)) : zat(j);
     };
-    if (L == 1) { // thread per row
+    auto ownr = [&](size_t row, T sum) { own(row, (REC && JZ == 2) ? zc * sum : sum); };
+    if (L == 1 && REC && A.mask && A.ulen <= 8) {
+        // stencil masks of at most 8 offsets (the 5- and 7-point stencils): 32-bit row
+        // indices, each gather one signed offset from the row's own address, and no
+        // offset-count tests (the mask has no bits at or above ulen)
+        const uint32_t n32 = A.nrow, stride = gridDim.x * blockDim.x;
+        for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n32; row += stride) {
+            const uint32_t m = __ldcs(A.mask + row);
+            const T* zr = z + row;
+            T xs[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) xs[k] = ((m >> k) & 1u) ? zr[A.udelta[k]] : T(0);
+            T sum = T(0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if ((m >> k) & 1u) sum = fma(A.uval[k], xs[k], sum);
+            ownr(row, sum);
+        }
+    } else if (L == 1) { // thread per row
         const size_t stride = (size_t)gridDim.x * blockDim.x;
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += stride)
-            own(row, row_apply<T, false>(A, row, gv));
+            ownr(row, row_apply<T, false>(A, row, gv));
     }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
@@ -363,13 +385,13 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
             for (uint32_t k = b + lane; k < e; k += L) sum = fma(A.val[k], gv(A.colInd[k]), sum);
         }
         sum = group_sum<L>(sum);
-        if (lane == 0 && row < A.nrow) own(row, sum);
+        if (lane == 0 && row < A.nrow) ownr(row, sum);
     }
     double a[1] = {(double)acc};
     const int ops[1] = {kSum};
-    grid_reduce<1>(a, ops, s, [=] __device__(const double* t) {
-        if (!REC) c->par = par ^ 1;
-        if (!c->bench) cg_after_spmv(c, t[0]);
+    grid_reduce_ctl<1>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+        if (!REC) cs->par = par ^ 1;
+        if (!cs->bench) cg_after_spmv(cs, t[0]);
     });
 }
 
@@ -463,8 +485,8 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
     }
     double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
     const int ops[5] = {kSum, kSum, kSum, kMax, kSum};
-    grid_reduce<5>(a, ops, s, [=] __device__(const double* t) {
-        if (!c->bench) cg_checks(c, t, 0);
+    grid_reduce_ctl<5>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+        if (!cs->bench) cg_checks(cs, t, 0);
     });
 }
 
@@ -520,9 +542,9 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
     }
     double a[2] = {(double)rr, (double)zr};
     const int ops[2] = {kSum, kSum};
-    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
+    grid_reduce_ctl<2>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
         const double red[5] = {t[0], t[1], 0.0, 0.0, 0.0};
-        if (!c->bench) cg_checks(c, red, 0);
+        if (!cs->bench) cg_checks(cs, red, 0);
     });
 }
 
@@ -549,21 +571,21 @@ __global__ void __launch_bounds__(kBlock) cg_start(uint32_t n, const T* __restri
     }
     double a[2] = {(double)rr, (double)zr};
     const int ops[2] = {kSum, kSum};
-    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
-        c->status = kRun;
-        c->numIter = 0;
-        c->code = kOk;
-        c->tmpa = t[1];
-        c->pmode = 0;
-        c->pzero = 0;
-        c->resAbs = 1.0;
-        c->resRel = 1.0;
-        c->denAbs = 1.0;
-        c->ratio = 0.0;
-        c->resAbsOld = 1.0;
-        c->alpha = 0.0;
-        c->xpend = 0;
-        cg_looptop(c, t[0]);
+    grid_reduce_ctl<2>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+        cs->status = kRun;
+        cs->numIter = 0;
+        cs->code = kOk;
+        cs->tmpa = t[1];
+        cs->pmode = 0;
+        cs->pzero = 0;
+        cs->resAbs = 1.0;
+        cs->resRel = 1.0;
+        cs->denAbs = 1.0;
+        cs->ratio = 0.0;
+        cs->resAbsOld = 1.0;
+        cs->alpha = 0.0;
+        cs->xpend = 0;
+        cg_looptop(cs, t[0]);
     });
 }
 
@@ -592,11 +614,11 @@ __global__ void __launch_bounds__(kBlock) cg_resume(uint32_t n, const T* __restr
     }
     double a[2] = {(double)rr, (double)zr};
     const int ops[2] = {kSum, kSum};
-    grid_reduce<2>(a, ops, s, [=] __device__(const double* t) {
-        const double red[5] = {t[0], t[1], c->red[2], c->red[3], c->red[4]};
-        c->status = kRun;
-        c->reason = kNoReason;
-        cg_checks(c, red, c->phase);
+    grid_reduce_ctl<2>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+        const double red[5] = {t[0], t[1], cs->red[2], cs->red[3], cs->red[4]};
+        cs->status = kRun;
+        cs->reason = kNoReason;
+        cg_checks(cs, red, cs->phase);
     });
 }
 
