@@ -184,6 +184,9 @@ __device__ void cg_after_refresh(CGCtl* c, const double* t)
     // p would swamp it, so the direction restarts from z (p = z).
     if (rn / c->histScale > 4.0 * c->resAbs) c->pzero = 1;
     c->rmax = sqrt(t[1]);
+    // one-reduction engines refresh in the cg_spmv slot: the cg_update slot that follows has
+    // nothing to update
+    if (c->onered) c->skipUpd = c->numIter + 1;
     const double red[5] = {t[1], t[2], 0.0, 0.0, 0.0};
     cg_checks(c, red, 1);
     cg_rec(c, c->numIter, rn / c->histScale);
@@ -297,21 +300,35 @@ struct V16<double> {
 
 // REC = 0: q = A p with p = z + beta p_old formed on the fly for every gathered entry (the
 // reference's order: XPAY, then Apply); p is double-buffered.
+// REC = 2: REC = 1 with one reduction per iteration (CGCtl::onered; z is r or zc r).
 // REC = 1 (FP32 iterations of the mixed-precision solves): the recurrence
 // q = A p = A z + beta q_old, so the SpMV gathers z alone and p, q update in place for the
 // owned row (half the gathers). Its rounding differs from A p by a term that beta < 1 damps;
 // the FP64 refreshes of reliable updates correct the residual it feeds.
+// Blocks per SM: FP32 6 (40 registers), one-reduction FP32 5 (its extra sums spill under
+// 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4.
 template <typename T, int L, int REC, int JZ>
-__global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))) cg_spmv(CSRView<T> A,
+__global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC == 2 ? 5 : 6) : 5)))
+    cg_spmv(CSRView<T> A,
                                                                      const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
                                                   CGCtl* c, Scratch s)
 {
+    static_assert(REC != 2 || JZ != 1, "one-reduction iterations need z = r or z = zc r");
+    constexpr bool ONE = REC == 2;
     pdl_wait();
     pdl_release();
     if (c->status != kRun) {
-        if constexpr (std::is_same<T, float>::value)
-            if (c->status == kRefresh) cg_refresh_fold(A.nrow, x, REC ? P0 : nullptr, c);
+        if constexpr (std::is_same<T, float>::value) {
+            if (c->status == kRefresh) {
+                if constexpr (ONE) // the cg_update slot folded x: the FP64 residual comes here
+                    cg_refresh_residual<JZ>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd,
+                                                        A.cls, A.coff, A.cdelta, A.mask},
+                                            const_cast<T*>(z), nullptr, nullptr, c, s);
+                else
+                    cg_refresh_fold(A.nrow, x, REC ? P0 : nullptr, c);
+            }
+        }
         return;
     }
     const int mode = c->pmode, par = c->par;
@@ -323,10 +340,11 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
     const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
-    T acc = T(0);
+    T acc = T(0), rr = T(0), rq = T(0), qq = T(0);
     // the owned row's p and q from its product `sum`
     auto own = [&](size_t row, T sum) {
-        const T zi = zat(row);
+        const T zraw = z[row];
+        const T zi = JZ == 2 ? zc * zraw : zraw;
         if (REC) {
             const T po = P0[row];
             if (xpend) x[row] = fma(alphaPrev, po, x[row]); // the last iteration's x update
@@ -335,6 +353,11 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
             P0[row] = pi;
             q[row] = qi;
             acc = fma(qi, pi, acc);
+            if (ONE) { // zraw is r
+                rr = fma(zraw, zraw, rr);
+                rq = fma(zraw, qi, rq);
+                qq = fma(qi, qi, qq);
+            }
         } else {
             const T pi = mode ? fma(beta, pOld[row], zi) : zi;
             pNew[row] = pi;
@@ -355,7 +378,7 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
         // offset-count tests (the mask has no bits at or above ulen)
         const uint32_t n32 = A.nrow, stride = gridDim.x * blockDim.x;
         for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n32; row += stride) {
-            const uint32_t m = __ldcs(A.mask + row);
+            const uint32_t m = __ldg(A.mask + row); // kept in L2: the FP32 working set fits
             const T* zr = z + row;
             T xs[8];
 #pragma unroll
@@ -387,12 +410,31 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? 6 : 5))
         sum = group_sum<L>(sum);
         if (lane == 0 && row < A.nrow) ownr(row, sum);
     }
-    double a[1] = {(double)acc};
-    const int ops[1] = {kSum};
-    grid_reduce_ctl<1>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
-        if (!REC) cs->par = par ^ 1;
-        if (!cs->bench) cg_after_spmv(cs, t[0]);
-    });
+    if constexpr (ONE) {
+        double a[4] = {(double)acc, (double)rr, (double)rq, (double)qq};
+        const int ops[4] = {kSum, kSum, kSum, kSum};
+        grid_reduce_ctl<4>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+            if (cs->bench) return;
+            // alpha from (r,z) of this r (not the value carried from the last iteration),
+            // then the update's checks on the residual that cg_update will form
+            const double f = JZ == 2 ? cs->zc : 1.0;
+            cs->tmpa = f * t[1];
+            cg_after_spmv(cs, t[0]);
+            if (cs->status != kRun) return;
+            const double al = cs->alpha;
+            double rn = t[1] - 2.0 * al * t[2] + al * al * t[3];
+            if (rn < 0.0) rn = 0.0;
+            const double red[5] = {rn, f * rn, 0.0, 0.0, 0.0};
+            cg_checks(cs, red, 0);
+        });
+    } else {
+        double a[1] = {(double)acc};
+        const int ops[1] = {kSum};
+        grid_reduce_ctl<1>(a, ops, s, c, [=] __device__(CGCtl* cs, const double* t) {
+            if (!REC) cs->par = par ^ 1;
+            if (!cs->bench) cg_after_spmv(cs, t[0]);
+        });
+    }
 }
 
 template <typename T, int JAC>
@@ -517,11 +559,10 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
     const size_t nv = n / W;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = tid; i < nv; i += stride) {
-        T ra[W], qa[W], da[W];
-        *(V*)ra = ((const V*)r)[i];
-        *(V*)qa = ((const V*)q)[i];
-        if (JAC == 1) *(V*)da = ((const V*)dinv)[i];
+    // two grid-stride steps per pass with all loads issued first (more bytes in flight per
+    // thread on the small grid), then the single-step remainder; same order of sums
+    size_t i = tid;
+    auto step = [&](T (&ra)[W], T (&qa)[W], const T (&da)[W], size_t k) {
 #pragma unroll
         for (int u = 0; u < W; ++u) {
             ra[u] = fma(-alpha, qa[u], ra[u]);
@@ -529,8 +570,26 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
             rr = fma(ra[u], ra[u], rr);
             zr = fma(qa[u], ra[u], zr);
         }
-        ((V*)r)[i] = *(V*)ra;
-        if (JAC == 1) ((V*)z)[i] = *(V*)qa;
+        ((V*)r)[k] = *(V*)ra;
+        if (JAC == 1) ((V*)z)[k] = *(V*)qa;
+    };
+    for (; i + stride < nv; i += 2 * stride) {
+        T ra[2][W], qa[2][W], da[2][W];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            *(V*)ra[h] = ((const V*)r)[i + h * stride];
+            *(V*)qa[h] = ((const V*)q)[i + h * stride];
+            if (JAC == 1) *(V*)da[h] = ((const V*)dinv)[i + h * stride];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) step(ra[h], qa[h], da[h], i + h * stride);
+    }
+    for (; i < nv; i += stride) {
+        T ra[W], qa[W], da[W];
+        *(V*)ra = ((const V*)r)[i];
+        *(V*)qa = ((const V*)q)[i];
+        if (JAC == 1) *(V*)da = ((const V*)dinv)[i];
+        step(ra, qa, da, i);
     }
     for (size_t i = nv * W + tid; i < n; i += stride) {
         const T ri = fma(-alpha, q[i], r[i]);
@@ -546,6 +605,54 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
         const double red[5] = {t[0], t[1], 0.0, 0.0, 0.0};
         if (!cs->bench) cg_checks(cs, red, 0);
     });
+}
+
+// The update of one-reduction engines: r -= alpha q, no sums (cg_spmv ran the checks). In a
+// refresh it folds x (the FP64 residual follows in the next cg_spmv slot).
+template <typename T>
+__global__ void __launch_bounds__(kBlock, 4) cg_update_r(uint32_t n, T* __restrict__ r,
+                                                      const T* __restrict__ q, T* x,
+                                                      const T* P0, CGCtl* c)
+{
+    pdl_wait();
+    pdl_release();
+    const int st = c->status;
+    if (st != kRun) {
+        if constexpr (std::is_same<T, float>::value)
+            if (st == kRefresh) cg_refresh_fold(n, x, P0, c);
+        return;
+    }
+    if (c->skipUpd == c->numIter + 1) return;
+    const T alpha = (T)c->alpha;
+    using V = typename V16<T>::t;
+    constexpr int W = V16<T>::W;
+    const size_t nv = n / W;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i = tid;
+    for (; i + stride < nv; i += 2 * stride) {
+        T ra[2][W], qa[2][W];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            *(V*)ra[h] = ((const V*)r)[i + h * stride];
+            *(V*)qa[h] = ((const V*)q)[i + h * stride];
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+            for (int u = 0; u < W; ++u) ra[h][u] = fma(-alpha, qa[h][u], ra[h][u]);
+            ((V*)r)[i + h * stride] = *(V*)ra[h];
+        }
+    }
+    for (; i < nv; i += stride) {
+        T ra[W], qa[W];
+        *(V*)ra = ((const V*)r)[i];
+        *(V*)qa = ((const V*)q)[i];
+#pragma unroll
+        for (int u = 0; u < W; ++u) ra[u] = fma(-alpha, qa[u], ra[u]);
+        ((V*)r)[i] = *(V*)ra;
+    }
+    for (size_t k = nv * W + tid; k < n; k += stride) r[k] = fma(-alpha, q[k], r[k]);
 }
 
 // Start of CG::Solve after rk = b - A x (CG.cxx:69-79): z = B(r), tmpa = (z, r), p = z.
@@ -843,7 +950,11 @@ void CGEngine<T>::launch_spmv_kernel()
         case 16: go(cg_spmv<T, 16, RR, JJ>); break;                                        \
         default: go(cg_spmv<T, 32, RR, JJ>); break;                                        \
     }
-    if (recurrence && jm == 2) {
+    if (onered() && jm == 2) {
+        CG_SPMV_LANES(2, 2)
+    } else if (onered()) {
+        CG_SPMV_LANES(2, 0)
+    } else if (recurrence && jm == 2) {
         CG_SPMV_LANES(1, 2)
     } else if (recurrence) {
         CG_SPMV_LANES(1, 0)
@@ -865,6 +976,12 @@ void CGEngine<T>::launch_update_kernel()
         launch_overlapped(kern, g, c->stream, pdl, n, x, r, zz, P0, P1, q, dinv, ctl, c->red, V);
     };
     const int jm = jmode();
+    if (onered()) {
+        const int g = std::min(need, resident_grid(*c, (const void*)cg_update_r<T>, kBlock));
+        launch_overlapped(cg_update_r<T>, g, c->stream, pdl, n, r, (const T*)q, x,
+                          (const T*)P0, ctl);
+        return;
+    }
     if (lean()) {
         auto gl = [&](auto kern, T* zz) {
             const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
@@ -942,6 +1059,7 @@ template <typename T>
 int CGEngine<T>::push_ctl()
 {
     hctl->zc = zc;
+    hctl->onered = onered() ? 1 : 0;
     FB_CUDA(cudaMemcpyAsync(ctl, hctl, sizeof(CGCtl), cudaMemcpyHostToDevice, c->stream));
     return kOk;
 }

@@ -25,6 +25,12 @@ struct CGCtl {
     int      par;       // which of the two p buffers holds the current direction
     int      pzero;     // the host zeroed p (a restart): next p = z
     int      xpend;     // lean FP32 engine: x += alpha p of the last iteration not yet applied
+    // one reduction per iteration (FP32 engines with the recurrence and z = zc r or z = r):
+    // cg_spmv also sums (r,r), (r,q), (q,q) and runs the checks of the update on
+    // (r - alpha q, r - alpha q) = (r,r) - 2 alpha (r,q) + alpha^2 (q,q); cg_update only
+    // updates r, and skips the slot after a refresh (skipUpd == numIter + 1)
+    int      onered;
+    unsigned skipUpd;
     double   zc;        // the constant diagInv when the Jacobi diagonal is one value (z = zc r)
     int      inner;     // 1: inner solve of mixed refinement (plain relative stop)
     int      reliable;  // 1 (with inner): FP32 iterations with FP64 reliable updates
@@ -84,6 +90,11 @@ struct CGEngine {
     // with the recurrence (not persistent): x += alpha p is applied by the next cg_spmv for
     // its own rows and cg_update keeps to r, z and two sums (the FP32 loop reads no others)
     bool       lean() const { return recurrence && !persistent; }
+    // one grid reduction per iteration (see CGCtl::onered)
+    bool       onered() const
+    {
+        return lean() && sizeof(T) == 4 && (jmode() == 2 || jmode() == 0);
+    }
     // applies a pending x += alpha p (host side, after the device loop stopped)
     int        apply_pending_x();
     uint32_t   n = 0;

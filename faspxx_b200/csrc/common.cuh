@@ -91,14 +91,19 @@ __device__ __forceinline__ void sum_partials(const double* partials, const int (
 }
 
 // Called by thread 0 of every block after its partials are written: true in exactly one
-// block, the last to arrive, when every block's partials are visible; that block returns
-// the counter to 0. (Counting in per-group counters first, to spread the atomics over
-// several addresses, measured slower on B200: the completing block pays two dependent
-// atomics and a fence instead of one atomic.)
+// block, the last to arrive, which returns the counter to 0. The ticket is one acq_rel
+// atomic: its release half publishes this block's partials, and in the last block its
+// acquire half (with the __syncthreads that follows in the caller) orders the partial
+// loads after every block's release -- no separate fences (the last block's full fence
+// cost ~0.35 us per reduction on B200). Counting in per-group counters first, to spread
+// the atomics over several addresses, measured slower: the completing block pays two
+// dependent atomics instead of one.
 __device__ __forceinline__ bool last_block_ticket(unsigned* ticket)
 {
-    __threadfence();
-    if (atomicAdd(ticket, 1u) != gridDim.x - 1) return false;
+    unsigned prev;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(ticket)
+                 : "memory");
+    if (prev != gridDim.x - 1) return false;
     *ticket = 0;
     return true;
 }
@@ -119,7 +124,6 @@ __device__ __forceinline__ void grid_reduce(double (&acc)[NV], const int (&ops)[
     }
     __syncthreads();
     if (!amLast) return;
-    __threadfence();
     double tot[NV];
     sum_partials<NV>(s.partials, ops, tot);
     block_reduce<NV>(tot, ops);
@@ -150,7 +154,6 @@ __device__ __forceinline__ void grid_reduce_ctl(double (&acc)[NV], const int (&o
     }
     __syncthreads();
     if (!amLast) return;
-    __threadfence();
     uint32_t* g = reinterpret_cast<uint32_t*>(gctl);
     for (int w = threadIdx.x; w < kWords; w += blockDim.x) sc[w] = __ldcg(g + w);
     double tot[NV];
