@@ -381,9 +381,11 @@ def run_ours(args):
     # per row (the class table stays in L1/L2, the stencil travels as kernel parameters)
     mat32 = 2 * n if rc_on else 8 * nnz + 4 * (n + 1)
     mat64 = 2 * n if rc_on else 12 * nnz + 4 * (n + 1)
-    # FP32 iterations use q = A z + beta q_old: read z (gathered), p, q; write p, q
-    b_spmv32 = mat32 + 4 * n * 5
-    b_upd32 = 4 * n * 5 + 4 * n * 3                 # read p,x,r,q,dinv write x,r,z
+    # FP32 iterations on this matrix (one Jacobi diagonal value) run the one-reduction
+    # engine: cg_spmv reads r (gathered), p, q, x and writes p, q, x (x += alpha p of the
+    # last iteration); cg_update_r reads r, q and writes r
+    b_spmv32 = mat32 + 4 * n * 7
+    b_upd32 = 4 * n * 3
     b_spmv64 = mat64 + 8 * n * 4
     b_upd64 = 8 * n * 5 + 8 * n * 3
     b_apply = mat64 + 16 * n
@@ -404,15 +406,15 @@ def run_ours(args):
         # the dominant kernel of the FP32 iteration: the larger of the two fused kernels
         if km[0] >= km[1]:
             form = {0: "csr", 1: "rowclass", 2: "stencil"}[rc_mode]
-            name = (f"cg_spmv<float> (w = A z, p = z + beta p, q = w + beta q, (q,p); FP32 CG "
-                    f"iteration, {form} matrix form)")
+            name = (f"cg_spmv<float> (w = A r, p = zc r + beta p, q = zc w + beta q, "
+                    f"x += alpha p_old, (p,q), (r,r), (r,q), (q,q); FP32 CG iteration, {form} "
+                    f"matrix form)")
             byt, ms_k = b_spmv32, km[0]
             key = f"cg_spmv<float>/{form}"
         else:
-            name = ("cg_update<float,1> (x += alpha p, r -= alpha Ap, z = D^-1 r and five "
-                    "reductions, FP32 CG iteration)")
+            name = "cg_update_r<float> (r -= alpha q, FP32 CG iteration, no reduction)"
             byt, ms_k = b_upd32, km[1]
-            key = "cg_update<float,1>"
+            key = "cg_update_r<float>"
         ach = gbs(byt, ms_k)
         roofline = {"kernel": name,
                     "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
