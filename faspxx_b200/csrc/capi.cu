@@ -275,6 +275,15 @@ int fasp_gpu_mat_create_csr_raw(uint32_t nrow, uint32_t mcol, uint32_t nnz,
     });
 }
 
+int fasp_gpu_mat_create_stencil(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
+                                const int32_t* dx, const int32_t* dy, const int32_t* dz,
+                                const double* coef, fasp_gpu_mat* out)
+{
+    return mat_build(out, [&](fasp_gpu_mat h) {
+        return m_create_stencil(h->M, nx, ny, nz, npts, dx, dy, dz, coef, h->c.stream);
+    });
+}
+
 int fasp_gpu_mat_destroy(fasp_gpu_mat A)
 {
     if (!A) return kOk;
@@ -300,6 +309,24 @@ int fasp_gpu_mat_download(fasp_gpu_mat A, uint32_t* rowPtr, uint32_t* colInd, do
 {
     if (!A) return kErrInputPar;
     const Mat& M = A->M;
+    if (M.grid) { // no stored matrix: the CSR arrays it applies, generated on the host
+        std::vector<uint32_t> rp, ci;
+        std::vector<double> va;
+        m_grid_csr(M, rp, ci, va);
+        if (rowPtr) std::memcpy(rowPtr, rp.data(), rp.size() * 4);
+        if (colInd) std::memcpy(colInd, ci.data(), ci.size() * 4);
+        if (values) std::memcpy(values, va.data(), va.size() * 8);
+        if (diagPtr)
+            for (uint32_t i = 0; i < M.nrow; ++i) {
+                diagPtr[i] = 0;
+                for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+                    if (ci[k] == i) {
+                        diagPtr[i] = k;
+                        break;
+                    }
+            }
+        return kOk;
+    }
     if (rowPtr) FB_CUDA(cudaMemcpy(rowPtr, M.rowPtr, ((size_t)M.nrow + 1) * 4, cudaMemcpyDeviceToHost));
     if (colInd) FB_CUDA(cudaMemcpy(colInd, M.colInd, (size_t)M.nnz * 4, cudaMemcpyDeviceToHost));
     if (values && M.val) FB_CUDA(cudaMemcpy(values, M.val, (size_t)M.nnz * 8, cudaMemcpyDeviceToHost));
@@ -358,6 +385,7 @@ int fasp_gpu_mat_autotune(fasp_gpu_mat A, int* lanes)
 int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes)
 {
     if (!A || lanes < 1 || lanes > 32 || (lanes & (lanes - 1))) return kErrInputPar;
+    if (A->M.grid && lanes != 1) return kErrInputPar; // grid operators: thread per row
     A->M.lanes = lanes;
     return kOk;
 }
@@ -365,6 +393,7 @@ int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes)
 int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode)
 {
     if (!A || mode < 0 || mode > 2) return kErrInputPar;
+    if (A->M.grid) return kOk; // a grid operator has no stored form to choose
     A->M.rcOn = mode >= 1 && A->M.rcCls != nullptr;
     A->M.skOn = mode == 2;
     return kOk;
@@ -375,10 +404,10 @@ int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uin
 {
     if (!A) return kErrInputPar;
     const Mat& M = A->M;
-    if (mode) *mode = !M.rcOn ? 0 : (M.skOn && M.skMask ? 2 : 1);
+    if (mode) *mode = M.grid ? 3 : (!M.rcOn ? 0 : (M.skOn && M.skMask ? 2 : 1));
     if (classes) *classes = M.rcClasses;
     if (entries) *entries = M.rcEntries;
-    if (stencil) *stencil = M.skMask ? M.skLen : 0;
+    if (stencil) *stencil = (M.skMask || M.grid) ? M.skLen : 0;
     return kOk;
 }
 

@@ -219,7 +219,39 @@ struct RefreshView {
     const uint32_t* coff;
     const int32_t*  cdelta;
     const uint16_t* mask;
+    // structured-grid form (see CSRView)
+    uint32_t        gnx, gny, gnz, gnxy, gmx, gmxy;
+    uint8_t         gsx[2], gsxy[2];
+    uint16_t        glo[12], ghi[12];
 };
+
+__device__ __forceinline__ RefreshView refresh_view(const CSRView<float>& A)
+{
+    RefreshView R;
+    R.nrow = A.nrow;
+    R.ulen = A.ulen;
+    R.rowPtr = A.rowPtr;
+    R.colInd = A.colInd;
+    R.cls = A.cls;
+    R.coff = A.coff;
+    R.cdelta = A.cdelta;
+    R.mask = A.mask;
+    R.gnx = A.gnx;
+    R.gny = A.gny;
+    R.gnz = A.gnz;
+    R.gnxy = A.gnxy;
+    R.gmx = A.gmx;
+    R.gmxy = A.gmxy;
+    for (int k = 0; k < 2; ++k) {
+        R.gsx[k] = A.gsx[k];
+        R.gsxy[k] = A.gsxy[k];
+    }
+    for (int k = 0; k < 12; ++k) {
+        R.glo[k] = A.glo[k];
+        R.ghi[k] = A.ghi[k];
+    }
+    return R;
+}
 
 // Row `row` of the FP64 matrix: the same storage form and entry order as row_apply.
 template <typename XV>
@@ -227,8 +259,8 @@ __device__ __forceinline__ double row_fp64(const RefreshView& A, const CGCtl* c,
                                            XV xv)
 {
     double s = 0.0;
-    if (A.mask) {
-        const uint32_t m = __ldcs(A.mask + row);
+    if (A.mask || A.gnz) {
+        const uint32_t m = A.gnz ? grid_mask(A, (uint32_t)row) : (uint32_t)__ldcs(A.mask + row);
         for (uint32_t k = 0; k < A.ulen; ++k)
             if ((m >> k) & 1u)
                 s = fma(c->skval[k], xv((uint32_t)((long long)row + c->skdelta[k])), s);
@@ -322,8 +354,7 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC ==
         if constexpr (std::is_same<T, float>::value) {
             if (c->status == kRefresh) {
                 if constexpr (ONE) // the cg_update slot folded x: the FP64 residual comes here
-                    cg_refresh_residual<JZ>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd,
-                                                        A.cls, A.coff, A.cdelta, A.mask},
+                    cg_refresh_residual<JZ>(refresh_view(A),
                                             const_cast<T*>(z), nullptr, nullptr, c, s);
                 else
                     cg_refresh_fold(A.nrow, x, REC ? P0 : nullptr, c);
@@ -372,13 +403,14 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC ==
         return mode ? fma(beta, pOld[j], zat(j)) : zat(j);
     };
     auto ownr = [&](size_t row, T sum) { own(row, (REC && JZ == 2) ? zc * sum : sum); };
-    if (L == 1 && REC && A.mask && A.ulen <= 8) {
+    if (L == 1 && REC && (A.mask || A.gnz) && A.ulen <= 8) {
         // stencil masks of at most 8 offsets (the 5- and 7-point stencils): 32-bit row
         // indices, each gather one signed offset from the row's own address, and no
         // offset-count tests (the mask has no bits at or above ulen)
         const uint32_t n32 = A.nrow, stride = gridDim.x * blockDim.x;
         for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n32; row += stride) {
-            const uint32_t m = __ldg(A.mask + row); // kept in L2: the FP32 working set fits
+            // masks kept in L2 (the FP32 working set fits), or computed (grid operators)
+            const uint32_t m = A.gnz ? grid_mask(A, row) : (uint32_t)__ldg(A.mask + row);
             const T* zr = z + row;
             T xs[8];
 #pragma unroll
@@ -450,8 +482,7 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update(uint32_t n, T* __restrict
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
             if (c->status == kRefresh)
-                cg_refresh_residual<JAC>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd, A.cls,
-                                                     A.coff, A.cdelta, A.mask},
+                cg_refresh_residual<JAC>(refresh_view(A),
                                          r, z, dinv, c, s);
         return;
     }
@@ -546,8 +577,7 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_lean(uint32_t n, T* __res
     if (c->status != kRun) {
         if constexpr (std::is_same<T, float>::value)
             if (c->status == kRefresh)
-                cg_refresh_residual<JAC>(RefreshView{A.nrow, A.ulen, A.rowPtr, A.colInd, A.cls,
-                                                     A.coff, A.cdelta, A.mask},
+                cg_refresh_residual<JAC>(refresh_view(A),
                                          r, z, dinv, c, s);
         return;
     }

@@ -198,7 +198,59 @@ struct CSRView {
     uint32_t        ulen;
     int32_t         udelta[kMaxStencil];
     T               uval[kMaxStencil];
+    // Structured-grid form (a matrix-free operator, no stored matrix; gnz == 0: not one).
+    // Row i is the grid point (ix, iy, iz), i = ix + nx (iy + ny iz); its entries are the
+    // stencil list above truncated at the faces, and its mask is computed from the
+    // coordinates: in dimension d, with t = min(coordinate, 3) and u = min(extent - 1 -
+    // coordinate, 3), the offsets present are glo[4d + t] & ghi[4d + u] (every offset
+    // reaches at most 3 points in each dimension). Division by nx and nx ny uses
+    // multiply-high with precomputed constants (FastDiv).
+    uint32_t        gnx, gny, gnz, gnxy;
+    uint32_t        gmx, gmxy;      // FastDiv multipliers for nx and nx ny
+    uint8_t         gsx[2], gsxy[2]; // and their shifts
+    uint16_t        glo[12], ghi[12];
 };
+
+// Division of a 32-bit unsigned n by a divisor fixed at launch (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994, Figure 4.1): with
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, t = mulhi(m, n),
+// n / d = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0) for every n < 2^32.
+struct FastDiv {
+    uint32_t m;
+    uint8_t  s1, s2;
+    static FastDiv make(uint32_t d)
+    {
+        uint32_t l = 0;
+        while (l < 32 && (1ull << l) < d) ++l;
+        FastDiv f;
+        f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+        f.s1 = (uint8_t)(l < 1 ? l : 1);
+        f.s2 = (uint8_t)(l > 1 ? l - 1 : 0);
+        return f;
+    }
+};
+
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, uint32_t m, uint32_t s1, uint32_t s2)
+{
+    const uint32_t t = __umulhi(m, n);
+    return (t + ((n - t) >> s1)) >> s2;
+}
+
+// The stencil mask of grid row `row` (structured-grid form); V is any view with the g*
+// fields of CSRView.
+template <typename V>
+__device__ __forceinline__ uint32_t grid_mask(const V& A, uint32_t row)
+{
+    const uint32_t iz = fast_div(row, A.gmxy, A.gsxy[0], A.gsxy[1]);
+    const uint32_t rem = row - iz * A.gnxy;
+    const uint32_t iy = fast_div(rem, A.gmx, A.gsx[0], A.gsx[1]);
+    const uint32_t ix = rem - iy * A.gnx;
+    auto dim = [&](int d, uint32_t c, uint32_t N) {
+        const uint32_t t = c < 3u ? c : 3u, u = N - 1u - c < 3u ? N - 1u - c : 3u;
+        return (uint32_t)A.glo[4 * d + t] & (uint32_t)A.ghi[4 * d + u];
+    };
+    return dim(0, ix, A.gnx) & dim(1, iy, A.gny) & dim(2, iz, A.gnz);
+}
 
 // The matrix is streamed once per SpMV: evict-first loads keep it from displacing the
 // vectors, which are reused every iteration and fit in the 126 MB L2 at the benchmark sizes.
@@ -238,8 +290,8 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, uint32_t b, uint32_t e
 template <typename T, bool PAT, typename XV>
 __device__ __forceinline__ T row_apply(const CSRView<T>& A, size_t row, XV xv)
 {
-    if (!PAT && A.mask) {
-        const uint32_t m = __ldcs(A.mask + row);
+    if (!PAT && (A.mask || A.gnz)) {
+        const uint32_t m = A.gnz ? grid_mask(A, (uint32_t)row) : (uint32_t)__ldcs(A.mask + row);
         T s = T(0);
         // chunks of 8 offsets: a 7-point row issues all its gathers before the first FMA
         // (loading every offset at a clamped index instead, so that the gathers need not

@@ -147,6 +147,11 @@ struct Mat {
     uint32_t  skLen = 0;
     int32_t   skDelta[kMaxStencil] = {};
     double    skVal[kMaxStencil] = {};
+    // structured-grid (matrix-free) operator: no CSR arrays; the stencil is skLen / skDelta /
+    // skVal (flattened offsets, ascending) with per-dimension offsets gd[3][k]
+    bool      grid = false;
+    uint32_t  gdim[3] = {0, 0, 0};
+    int8_t    gd[3][kMaxStencil] = {};
     template <typename T>
     CSRView<T> view(const T* v, const T* cv) const
     {
@@ -157,6 +162,35 @@ struct Mat {
         V.rowPtr = rowPtr;
         V.colInd = colInd;
         V.val = v;
+        if (grid) {
+            V.ulen = skLen;
+            for (uint32_t u = 0; u < skLen; ++u) {
+                V.udelta[u] = skDelta[u];
+                V.uval[u] = (T)skVal[u];
+            }
+            V.gnx = gdim[0];
+            V.gny = gdim[1];
+            V.gnz = gdim[2];
+            V.gnxy = gdim[0] * gdim[1];
+            const FastDiv fx = FastDiv::make(gdim[0]), fxy = FastDiv::make(V.gnxy);
+            V.gmx = fx.m;
+            V.gsx[0] = fx.s1;
+            V.gsx[1] = fx.s2;
+            V.gmxy = fxy.m;
+            V.gsxy[0] = fxy.s1;
+            V.gsxy[1] = fxy.s2;
+            for (int d = 0; d < 3; ++d)
+                for (int t = 0; t < 4; ++t) {
+                    uint32_t lo = 0, hi = 0;
+                    for (uint32_t u = 0; u < skLen; ++u) {
+                        if (gd[d][u] >= -t) lo |= 1u << u;
+                        if (gd[d][u] <= t) hi |= 1u << u;
+                    }
+                    V.glo[4 * d + t] = (uint16_t)lo;
+                    V.ghi[4 * d + t] = (uint16_t)hi;
+                }
+            return V;
+        }
         if (rcOn && rcCls && v && cv) {
             V.cls = rcCls;
             V.coff = rcOff;
@@ -215,6 +249,14 @@ int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const doub
 // ---- sparse kernels (spmv.cu) ---------------------------------------------------------
 int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
              const uint32_t* colInd, const double* values, bool hostPtrs, cudaStream_t s);
+// A structured-grid operator (no stored matrix): nx x ny x nz points, npts stencil points
+// (dx, dy, dz) with coefficients, truncated at the faces (spmv.cu).
+int m_create_stencil(Mat& M, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
+                     const int32_t* dx, const int32_t* dy, const int32_t* dz, const double* coef,
+                     cudaStream_t s);
+// The CSR arrays of a grid operator, generated on the host (downloads and tests).
+void m_grid_csr(const Mat& M, std::vector<uint32_t>& rowPtr, std::vector<uint32_t>& colInd,
+                std::vector<double>& values);
 void m_free(Mat& M);
 // ReadMat's conversions on the device (ingest.cu): MTXtoMAT of 0-based triplets, and
 // ReadCSR's shift + SortCSRRow + CSRtoMAT of raw CSR arrays (0- or 1-based).

@@ -239,7 +239,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 return e;
             }
             // Identity or one Jacobi sweep from zero: the device-driven engine
-            const bool fusable = A->val && (cfg.pcd == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
+            const bool fusable = (A->val || A->grid) && (cfg.pcd == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
             if (fusable) {
                 dhistCap = cfg.prm.maxIter + 2;
                 if (cudaMalloc(&dhist, (size_t)dhistCap * 8) != cudaSuccess) return kErrAlloc;
@@ -1242,7 +1242,7 @@ bool SolverImpl::gm_device_cycles(bool flexible) const
     // Identity or one Jacobi sweep (from zero for GMRES, from the warm start Z_j for
     // FGMRES); MGS keeps the reference's per-vector op sequence with a host-read scalar
     (void)flexible;
-    return gmc && dhist && A->val && cfg.orth != FASP_GPU_ORTH_MGS &&
+    return gmc && dhist && (A->val || A->grid) && cfg.orth != FASP_GPU_ORTH_MGS &&
            (pcd.type == 0 || (pcd.pure() && pcd.prm.maxIter == 1));
 }
 

@@ -8,6 +8,7 @@
 // nearby columns, so x stays cache resident). L = 1 is the scalar thread-per-row kernel and
 // L = 32 the warp-per-row vector kernel; L is chosen from the mean row length or timed.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <unordered_map>
@@ -107,7 +108,7 @@ static int launch_spmv(Ctx& c, CSRView<T> A, int L, const T* x, T* y)
 {
     if (A.nrow == 0) return kOk;
     const int need = spmv_grid(c, A.nrow, L);
-    const bool pat = A.val == nullptr;
+    const bool pat = A.val == nullptr && !A.gnz;
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
         kern<<<g, kBlock, 0, c.stream>>>(A, x, y);
@@ -149,7 +150,7 @@ static int residual_t(Ctx& c, const Mat& A, CSRView<T> V, const T* b, const T* x
                       const double* xinf)
 {
     if (A.nrow == 0) return kOk;
-    if (!V.val) return kErrMatData; // MAT::Residual reads values (MAT.cxx:466)
+    if (!V.val && !V.gnz) return kErrMatData; // MAT::Residual reads values (MAT.cxx:466)
     if (!xinf) {
         double* slot = c.dslot + kSlotResidualXinf;
         int e = v_norminf(c, A.mcol, x, slot);
@@ -183,7 +184,7 @@ int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r
 int m_residual(Ctx& c, const Mat& A, const float* b, const float* x, float* r,
                const double* xinf)
 {
-    if (!A.val) return kErrMatData;
+    if (!A.val && !A.grid) return kErrMatData;
     return residual_t<float>(c, A, A.v32(), b, x, r, xinf);
 }
 
@@ -585,8 +586,23 @@ __global__ void k_sort_gather(uint32_t m, const uint32_t* __restrict__ tRowPtr,
     }
 }
 
+// The transpose of a grid operator is the grid operator with every offset negated (the
+// same coefficients), in ascending order of the negated flattened offsets.
+static int grid_transpose(Ctx& c, const Mat& A, Mat& T)
+{
+    std::vector<int32_t> dx(A.skLen), dy(A.skLen), dz(A.skLen);
+    for (uint32_t k = 0; k < A.skLen; ++k) {
+        dx[k] = -A.gd[0][k];
+        dy[k] = -A.gd[1][k];
+        dz[k] = -A.gd[2][k];
+    }
+    return m_create_stencil(T, A.gdim[0], A.gdim[1], A.gdim[2], A.skLen, dx.data(), dy.data(),
+                            dz.data(), A.skVal, c.stream);
+}
+
 int m_transpose(Ctx& c, const Mat& A, Mat& T)
 {
+    if (A.grid) return grid_transpose(c, A, T);
     const uint32_t m = A.mcol, n = A.nrow, nnz = A.nnz;
     Mat R;
     R.nrow = m;
@@ -640,6 +656,7 @@ int m_transpose(Ctx& c, const Mat& A, Mat& T)
 // ---- autotuner: time each lanes-per-row choice on this matrix ---------------------------
 int m_autotune(Ctx& c, Mat& A)
 {
+    if (A.grid) return kOk; // grid operators run thread per row (lanes = 1) only
     double *x = nullptr, *y = nullptr;
     int e;
     if ((e = dmalloc((void**)&x, (size_t)A.mcol * 8)) || (e = dmalloc((void**)&y, (size_t)A.nrow * 8))) {
@@ -692,10 +709,130 @@ __global__ void k_sampled_outer(CSRView<double> A, const double* __restrict__ la
 int m_sampled_outer(Ctx& c, const Mat& A, const double* lam, const double* x, double scale,
                     double* dA)
 {
+    if (A.grid) return kErrInputPar; // no stored entries to differentiate
     const int g = std::max(1, std::min(ceil_div(A.nrow, kBlock), c.nsm * 8));
     k_sampled_outer<<<g, kBlock, 0, c.stream>>>(A.v64(), lam, x, scale, dA);
     FB_CUDA(cudaGetLastError());
     return kOk;
+}
+
+// ---- structured-grid (matrix-free) operators --------------------------------------------
+// The GPU counterpart of the reference's matrix-free LOP example (example/TestMatFree.cxx:
+// 26-176): y = A x on an nx x ny x nz grid with a constant-coefficient stencil, Dirichlet
+// truncation at the faces, without any stored matrix. Rows are grid points in x-fastest
+// order; a row's entries are the stencil points inside the grid in ascending column order,
+// so every kernel computes exactly what it computes on the assembled CSR matrix.
+
+__global__ void k_fill_const(uint32_t n, double v, double* __restrict__ y)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        y[i] = v;
+}
+
+int m_create_stencil(Mat& M, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
+                     const int32_t* dx, const int32_t* dy, const int32_t* dz, const double* coef,
+                     cudaStream_t s)
+{
+    if (!dx || !dy || !dz || !coef) return kErrInputPar;
+    if (nx == 0 || ny == 0 || nz == 0) return kErrMatSize;
+    const uint64_t n64 = (uint64_t)nx * ny * nz;
+    if (n64 > 0xffffffffull || (uint64_t)nx * ny > 0xffffffffull) return kErrMatSize;
+    if (npts == 0 || npts > (uint32_t)kMaxStencil) return kErrInputPar;
+    struct Pt {
+        int64_t flat;
+        int32_t d[3];
+        double  v;
+    };
+    std::vector<Pt> pts(npts);
+    for (uint32_t k = 0; k < npts; ++k) {
+        const int32_t d[3] = {dx[k], dy[k], dz[k]};
+        for (int a = 0; a < 3; ++a)
+            if (d[a] < -3 || d[a] > 3) return kErrInputPar; // reach of at most 3 points
+        pts[k] = Pt{(int64_t)d[0] + (int64_t)nx * ((int64_t)d[1] + (int64_t)ny * d[2]),
+                    {d[0], d[1], d[2]}, coef[k]};
+    }
+    // points that reach past the grid in some dimension are never inside it: dropped (in a
+    // grid one point thick, such points could share a flattened offset with real ones)
+    const uint32_t ext[3] = {nx, ny, nz};
+    pts.erase(std::remove_if(pts.begin(), pts.end(),
+                             [&](const Pt& p) {
+                                 for (int a = 0; a < 3; ++a)
+                                     if ((uint32_t)std::abs(p.d[a]) >= ext[a]) return true;
+                                 return false;
+                             }),
+              pts.end());
+    npts = (uint32_t)pts.size();
+    // a present neighbour (ix + dx, iy + dy, iz + dz) is column row + flat, so ascending
+    // flattened offset is the CSR column order of every row
+    std::sort(pts.begin(), pts.end(), [](const Pt& a, const Pt& b) { return a.flat < b.flat; });
+    for (uint32_t k = 1; k < npts; ++k)
+        if (pts[k].flat == pts[k - 1].flat) return kErrInputPar;
+    Mat T;
+    T.grid = true;
+    T.nrow = T.mcol = (uint32_t)n64;
+    T.gdim[0] = nx;
+    T.gdim[1] = ny;
+    T.gdim[2] = nz;
+    T.skLen = npts;
+    uint64_t nnz = 0;
+    double diagv = 0.0;
+    bool hasDiag = false;
+    for (uint32_t k = 0; k < npts; ++k) {
+        T.skDelta[k] = (int32_t)pts[k].flat;
+        T.skVal[k] = pts[k].v;
+        uint64_t cnt = 1;
+        for (int a = 0; a < 3; ++a) {
+            T.gd[a][k] = (int8_t)pts[k].d[a];
+            const uint32_t r = (uint32_t)std::abs(pts[k].d[a]);
+            cnt *= r < ext[a] ? ext[a] - r : 0;
+        }
+        nnz += cnt;
+        if (pts[k].flat == 0) {
+            hasDiag = true;
+            diagv = pts[k].v;
+        }
+    }
+    if (nnz > 0xffffffffull) return kErrMatSize;
+    T.nnz = (uint32_t)nnz;
+    T.lanes = 1;
+    T.maxRowLen = npts;
+    T.meanRowLen = (double)nnz / (double)n64;
+    T.diagConst = hasDiag && diagv != 0.0;
+    T.diagValue = diagv;
+    cudaGetDevice(&T.dev);
+    int e;
+    if ((e = dmalloc((void**)&T.diag, (size_t)T.nrow * 8))) return e;
+    k_fill_const<<<std::max(1, std::min(ceil_div(T.nrow, kBlock), 148 * 8)), kBlock, 0, s>>>(
+        T.nrow, diagv, T.diag);
+    FB_CUDA(cudaGetLastError());
+    FB_CUDA(cudaStreamSynchronize(s));
+    M = T;
+    return kOk;
+}
+
+void m_grid_csr(const Mat& M, std::vector<uint32_t>& rowPtr, std::vector<uint32_t>& colInd,
+                std::vector<double>& values)
+{
+    const uint32_t nx = M.gdim[0], ny = M.gdim[1], nz = M.gdim[2];
+    rowPtr.assign((size_t)M.nrow + 1, 0);
+    colInd.clear();
+    values.clear();
+    colInd.reserve(M.nnz);
+    values.reserve(M.nnz);
+    uint32_t row = 0;
+    for (uint32_t iz = 0; iz < nz; ++iz)
+        for (uint32_t iy = 0; iy < ny; ++iy)
+            for (uint32_t ix = 0; ix < nx; ++ix, ++row) {
+                for (uint32_t k = 0; k < M.skLen; ++k) {
+                    const int64_t jx = (int64_t)ix + M.gd[0][k], jy = (int64_t)iy + M.gd[1][k],
+                                  jz = (int64_t)iz + M.gd[2][k];
+                    if (jx < 0 || jy < 0 || jz < 0 || jx >= nx || jy >= ny || jz >= nz) continue;
+                    colInd.push_back((uint32_t)((int64_t)row + M.skDelta[k]));
+                    values.push_back(M.skVal[k]);
+                }
+                rowPtr[(size_t)row + 1] = (uint32_t)colInd.size();
+            }
 }
 
 } // namespace fb

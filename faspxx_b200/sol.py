@@ -132,6 +132,25 @@ class MAT:
                            values)
 
     @classmethod
+    def Stencil(cls, shape, points) -> "MAT":
+        """A matrix-free operator on a structured grid (the GPU form of the reference's
+        matrix-free LOP, example/TestMatFree.cxx:26-176): shape = (nx,), (nx, ny) or
+        (nx, ny, nz); points = [((dx, dy, dz), coef), ...] (shorter offset tuples are
+        padded with 0). Row ix + nx (iy + ny iz); the stencil is truncated at the faces."""
+        capi.init()
+        dims = list(shape) + [1] * (3 - len(shape))
+        off = [tuple(list(o) + [0] * (3 - len(o))) for o, _ in points]
+        dx = np.array([o[0] for o in off], np.int32)
+        dy = np.array([o[1] for o in off], np.int32)
+        dz = np.array([o[2] for o in off], np.int32)
+        cf = np.array([c for _, c in points], np.float64)
+        h = C.c_void_p()
+        check(lib.fasp_gpu_mat_create_stencil(dims[0], dims[1], dims[2], len(cf),
+                                              dx.ctypes.data, dy.ctypes.data, dz.ctypes.data,
+                                              cf.ctypes.data, C.byref(h)), "MatFree")
+        return cls(_handle=h)
+
+    @classmethod
     def _ingest(cls, fn, where, nrow, mcol, nnz, a, b, v) -> "MAT":
         capi.init()
         dev = hasattr(v, "ptr")

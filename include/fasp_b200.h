@@ -155,6 +155,21 @@ int fasp_gpu_mat_create_coo(uint32_t nrow, uint32_t mcol, uint32_t nnz, const ui
 int fasp_gpu_mat_create_csr_raw(uint32_t nrow, uint32_t mcol, uint32_t nnz,
                                 const uint32_t* rowPtr, const uint32_t* colInd,
                                 const double* values, int onDevice, fasp_gpu_mat* out);
+/* A matrix-free operator (the LOP of example/TestMatFree.cxx:26-39, applied as in its
+ * MatFree::Apply, :97-176, generalised): y = A x on an nx x ny x nz grid (ny = nz = 1 for
+ * 1D, nz = 1 for 2D), point (ix, iy, iz) being row ix + nx (iy + ny iz), with the
+ * constant-coefficient stencil sum_k coef[k] x(ix + dx[k], iy + dy[k], iz + dz[k]) over the
+ * stencil points inside the grid (Dirichlet truncation at the faces). Nothing is stored:
+ * kernels compute each row's points from its coordinates. Every operation gives the same
+ * results as on the assembled CSR matrix (entries in ascending column order); a grid
+ * operator is accepted wherever a matrix is, except the sampled outer product (no stored
+ * entries, ERROR_INPUT_PAR) and SpMV lanes other than 1. npts <= 16, |dx|,|dy|,|dz| <= 3,
+ * no two points at the same offset (ERROR_INPUT_PAR); points that reach past the grid in
+ * some dimension (|dx| >= nx, ...) have no entries and are dropped; the diagonal (Jacobi) is the
+ * coefficient of (0,0,0), 0 when absent. Download returns the CSR arrays it applies. */
+int fasp_gpu_mat_create_stencil(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
+                                const int32_t* dx, const int32_t* dy, const int32_t* dz,
+                                const double* coef, fasp_gpu_mat* out);
 int fasp_gpu_mat_destroy(fasp_gpu_mat A);
 /* GetRowSize / GetColSize / GetNNZ (LOP.hxx:50-53, MAT.hxx:113) */
 int fasp_gpu_mat_info(fasp_gpu_mat A, uint32_t* nrow, uint32_t* mcol, uint32_t* nnz);

@@ -43,3 +43,12 @@ g++ -std=c++17 -O2 -ffp-contract=off -fPIC -shared -w -I"$TMP" -I"$HERE" \
     $SRCS "$HERE/ref_shim.cxx" -o "$OUT/liboracle_ref.so.tmp"
 mv "$OUT/liboracle_ref.so.tmp" "$OUT/liboracle_ref.so"
 echo "built $OUT/liboracle_ref.so"
+# The reference's own matrix-free example (example/TestMatFree.cxx, with its Poisson2D.hxx),
+# built from the same patched sources; tests/golden/make_golden.py records what it prints.
+if [ -f "$REF/example/TestMatFree.cxx" ]; then
+    cp "$REF/example/TestMatFree.cxx" "$REF/example/Poisson2D.hxx" "$TMP"/
+    g++ -std=c++17 -O2 -ffp-contract=off -w -I"$TMP" $SRCS "$TMP/Timing.cxx" \
+        "$TMP/TestMatFree.cxx" -o "$OUT/test_matfree.tmp"
+    mv "$OUT/test_matfree.tmp" "$OUT/test_matfree"
+    echo "built $OUT/test_matfree"
+fi

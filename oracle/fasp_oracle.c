@@ -1258,3 +1258,25 @@ void orc_destroy(void* hv)
     free(h->mat.rowPtr); free(h->mat.colInd); free(h->mat.diagPtr); free(h->mat.values);
     free(h);
 }
+
+/* ------------------------------------------------------------------------------------
+ * The reference's matrix-free example problem (example/TestMatFree.cxx:41-85 with
+ * example/Poisson2D.hxx, TEST_PROBLEM 1): the right-hand side AssembleRHS builds on the
+ * (dim-1) x (dim-1) interior grid, h = 1/dim, point (k, j) at index (k-1)(dim-1) + j-1.
+ * u = sin(pi x) sin(pi y) vanishes on the boundary, so every point gets h^2 Load(k h, j h)
+ * (the boundary terms the example adds are 0.0 there); Load is evaluated in the example's
+ * operation order with the C library's sin.
+ * ---------------------------------------------------------------------------------- */
+void orc_matfree_rhs(int dim, double* b)
+{
+    const double pi = 3.14159265358979323846264338327950288;
+    const double h = 1.0 / dim;
+    const double h2 = h * h;
+    const int dim1 = dim - 1;
+    for (int k = 1; k <= dim1; ++k)
+        for (int j = 1; j <= dim1; ++j) {
+            const double x = k * h, y = j * h;
+            const double load = 2 * pi * pi * sin(pi * x) * sin(pi * y);
+            b[(size_t)(k - 1) * dim1 + (j - 1)] = h2 * load;
+        }
+}

@@ -110,6 +110,10 @@ int    orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr,
                       const uint32_t* colInd, const double* values, uint32_t* nnzOut,
                       uint32_t* rowPtrOut, uint32_t* colIndOut, double* valuesOut);
 
+/* The right-hand side of the reference's matrix-free example (example/TestMatFree.cxx:41-85,
+ * Poisson2D.hxx TEST_PROBLEM 1) on the (dim-1)^2 interior grid. Port library only. */
+void   orc_matfree_rhs(int dim, double* b);
+
 /* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
 int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
                        uint32_t* colInd, double* values);

@@ -246,3 +246,12 @@ def csr_to_mat(kind, nrow, rowPtr, colInd, values):
     z = C.c_uint32()
     code = load(kind).orc_csr_to_mat(nrow, len(ci), rp, ci, va, C.byref(z), rp_o, ci_o, va_o)
     return _converted(code, z, rp_o, ci_o, va_o)
+
+
+def matfree_rhs(dim: int) -> np.ndarray:
+    """The right-hand side of the reference's matrix-free example at mesh `dim` (port)."""
+    lib = load("port")
+    lib.orc_matfree_rhs.argtypes = [C.c_int, _f64p]
+    b = np.empty((dim - 1) ** 2)
+    lib.orc_matfree_rhs(dim, b)
+    return b

@@ -17,7 +17,10 @@ Run in a container that has the reference tree (default /root/reference) after
   and data/nos7.mtx arrays and on seeded synthetic inputs: shuffled entries, duplicates,
   missing and empty-row diagonals, long rows, rectangular and invalid matrices.
 
-    python tests/golden/make_golden.py [/path/to/reference] [--ingest-only]
+* ``reference_matfree.json`` -- what the reference's matrix-free example prints
+  (example/TestMatFree.cxx, built from the reference sources by oracle/build_ref.sh).
+
+    python tests/golden/make_golden.py [/path/to/reference] [--ingest-only | --matfree-only]
 """
 from __future__ import annotations
 
@@ -238,9 +241,33 @@ def make_ingest(ref_root: str) -> None:
     print("wrote", len(meta), "ingestion cases")
 
 
+def make_matfree() -> None:
+    """What the reference's matrix-free example prints (example/TestMatFree.cxx, built from
+    the reference sources into oracle/_ref/test_matfree by build_ref.sh): per mesh dim
+    (16, 32, ..., 512), the CG iteration count, the final residual norms and the L2 error."""
+    import re
+    import subprocess
+    import tempfile
+    O.build(ref=True)
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_matfree")
+    with tempfile.TemporaryDirectory() as d:
+        out = subprocess.run([exe], cwd=d, capture_output=True, text=True, check=True).stdout
+    runs = {}
+    for block in out.split("dim = ")[1:]:
+        dim = int(block.split(",")[0])
+        get = lambda key: re.search(key + r"\s*:\s*([-+0-9.eE]+)", block).group(1)  # noqa: E731
+        runs[str(dim)] = dict(iters=int(get("NumIter")), norm2=get("Norm2"),
+                              normInf=get("NormInf"), l2err=get("Error in L2-norm"))
+    with open(os.path.join(HERE, "reference_matfree.json"), "w") as f:
+        json.dump(runs, f, indent=1)
+    print("wrote", len(runs), "matrix-free runs")
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     root = args[0] if args else "/root/reference"
-    if "--ingest-only" not in sys.argv:
+    if "--ingest-only" not in sys.argv and "--matfree-only" not in sys.argv:
         main(root)
-    make_ingest(root)
+    if "--matfree-only" not in sys.argv:
+        make_ingest(root)
+    make_matfree()
