@@ -806,6 +806,74 @@ def run_pcg2d(args):
     return 0
 
 
+def run_matfree(args):
+    """The reference's matrix-free example (example/TestMatFree.cxx:178-255): CG without a
+    preconditioner on the 2D 5-point operator of the (dim-1)^2 interior grid, dim = 16 ...
+    512, relTol 1e-8, absTol 1e-12, x0 = 0.25, its right-hand side (u = sin(pi x) sin(pi y)).
+    GPU: the matrix-free grid operator (no stored matrix) and, at dim 512, the stored CSR
+    matrix in its stencil-mask form. CPU: the reference example itself (built from the
+    reference sources into oracle/_ref), its own wall-clock timing of each CG solve."""
+    import re
+    from faspxx_b200 import capi, problems as P, sol
+    from oracle import oracle as O
+    capi.init(0)
+    five = [((0, -1), -1.0), ((-1, 0), -1.0), ((0, 0), 4.0), ((1, 0), -1.0), ((0, 1), -1.0)]
+    res = {}
+    for dim in (16, 32, 64, 128, 256, 512):
+        n = (dim - 1) ** 2
+        b = sol.DVec.from_numpy(O.matfree_rhs(dim))
+        x = sol.DVec(n)
+        x0 = np.full(n, 0.25)
+        forms = [("grid", sol.MAT.Stencil((dim - 1, dim - 1), five))]
+        if dim == 512:
+            forms.append(("stored", sol.MAT(P.poisson2d(dim - 1))))
+        for form, M in forms:
+            s = sol.configure("cg", maxIter=10000, restart=20, relTol=1e-8, absTol=1e-12)
+            s.Setup(M)
+            ts = []
+            for i in range(args.warmup + args.steps):
+                x.set(x0)
+                if s.Solve(b, x) != 0:
+                    raise RuntimeError("matrix-free CG failed")
+                if i >= args.warmup:
+                    ts.append(s.LastTimeMs())
+            h = 1.0 / dim
+            k = np.arange(1, dim)
+            u = np.outer(np.sin(np.pi * k * h), np.sin(np.pi * k * h)).ravel()
+            err = float(np.sqrt(np.sum((x.numpy() - u) ** 2) * h * h))
+            key = str(dim) if form == "grid" else f"{dim}_stored_matrix"
+            res[key] = {"ms": round(statistics.mean(ts), 4), "iters": s.GetIterations(),
+                        "norm2": s.GetNorm2(), "l2_error": err}
+    cpu = None
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref",
+                       "test_matfree")
+    if not args.no_cpu_baseline and os.path.exists(exe):
+        import tempfile
+        with tempfile.TemporaryDirectory() as d:
+            out = subprocess.run([exe], cwd=d, capture_output=True, text=True,
+                                 timeout=600).stdout
+        cpu = {}
+        for block in out.split("dim = ")[1:]:
+            dim = int(block.split(",")[0])
+            cpu[str(dim)] = {"ms": float(re.search(r"costs\s+([0-9.eE+-]+)ms", block).group(1)),
+                             "iters": int(re.search(r"NumIter\s*:\s*(\d+)", block).group(1))}
+    line = {"metric": "Time of the matrix-free CG solve, reference example TestMatFree "
+                      "(2D Poisson, dim 512: n = 261,121)",
+            "value": res["512"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "dtype": "f64",
+            "data": "the example's own right-hand side",
+            "config": {"workload": "example/TestMatFree.cxx: 5-point operator on the "
+                                   "(dim-1)^2 interior grid, CG without preconditioner, "
+                                   "rtol 1e-8, atol 1e-12, x0 = 0.25, dim 16..512"},
+            "results": res,
+            "cpu_baseline": None if not cpu else {
+                "value": cpu["512"]["ms"], "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": "the reference example's own timing of each CG solve",
+                "per_dim": cpu}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -824,7 +892,7 @@ def main():
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
                          "one 60-iteration BiCGStab and GMRES(30) solve (krylov96)")
     ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",
-                                           "pcg2d256"], default="poisson128")
+                                           "pcg2d256", "matfree"], default="poisson128")
     ap.add_argument("--fd-dirs", type=int, default=32)
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-sample", type=int, default=256)
@@ -840,6 +908,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "pcg2d256":
         return run_pcg2d(args)
+    if args.workload == "matfree":
+        return run_matfree(args)
     return run_ours(args)
 
 
