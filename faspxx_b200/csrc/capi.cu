@@ -284,6 +284,12 @@ int fasp_gpu_mat_create_stencil(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t 
     });
 }
 
+int fasp_gpu_mat_mult(fasp_gpu_mat L, fasp_gpu_mat R, fasp_gpu_mat* out)
+{
+    if (!L || !R) return kErrInputPar;
+    return mat_build(out, [&](fasp_gpu_mat h) { return m_mult(h->c, L->M, R->M, h->M); });
+}
+
 int fasp_gpu_mat_destroy(fasp_gpu_mat A)
 {
     if (!A) return kOk;

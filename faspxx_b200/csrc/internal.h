@@ -254,6 +254,8 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
 int m_create_stencil(Mat& M, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
                      const int32_t* dx, const int32_t* dy, const int32_t* dz, const double* coef,
                      cudaStream_t s);
+// C = L R exactly as MAT::Mult (src/MAT.cxx:715-800) forms it (spgemm.cu).
+int m_mult(Ctx& c, const Mat& L, const Mat& R, Mat& C);
 // The CSR arrays of a grid operator, generated on the host (downloads and tests).
 void m_grid_csr(const Mat& M, std::vector<uint32_t>& rowPtr, std::vector<uint32_t>& colInd,
                 std::vector<double>& values);

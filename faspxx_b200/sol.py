@@ -193,6 +193,12 @@ class MAT:
                                              C.byref(st)), "RowClassInfo")
         return mode.value, k.value, e.value, st.value
 
+    def Mult(self, R: "MAT") -> "MAT":
+        """MAT::Mult (src/MAT.cxx:715-800): self * R as a new matrix, computed on the GPU."""
+        h = C.c_void_p()
+        check(lib.fasp_gpu_mat_mult(self.h, R.h, C.byref(h)), "Mult")
+        return MAT(_handle=h)
+
     def Transpose(self) -> "MAT":
         """MAT::TransInPlace into a new matrix (the original stays)."""
         h = C.c_void_p()

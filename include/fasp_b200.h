@@ -170,6 +170,13 @@ int fasp_gpu_mat_create_csr_raw(uint32_t nrow, uint32_t mcol, uint32_t nnz,
 int fasp_gpu_mat_create_stencil(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npts,
                                 const int32_t* dx, const int32_t* dy, const int32_t* dz,
                                 const double* coef, fasp_gpu_mat* out);
+/* MAT::Mult (MAT.cxx:715-800): *out = L R on the device, with MAT::Mult's exact result --
+ * the columns of each row in the order in which the loop over L's row and R's rows first
+ * meets them (rows are not sorted), each entry 0 + the products of that column added in the
+ * same loop order. ERROR_MAT_NONMATCH (-16) unless L's columns = R's rows; ERROR_INPUT_PAR
+ * for a pattern-only matrix or a grid operator (no stored values); ERROR_MAT_SIZE when the
+ * product has no entries or more than 2^32 - 1 intermediate products. */
+int fasp_gpu_mat_mult(fasp_gpu_mat L, fasp_gpu_mat R, fasp_gpu_mat* out);
 int fasp_gpu_mat_destroy(fasp_gpu_mat A);
 /* GetRowSize / GetColSize / GetNNZ (LOP.hxx:50-53, MAT.hxx:113) */
 int fasp_gpu_mat_info(fasp_gpu_mat A, uint32_t* nrow, uint32_t* mcol, uint32_t* nnz);

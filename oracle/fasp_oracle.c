@@ -1280,3 +1280,50 @@ void orc_matfree_rhs(int dim, double* b)
             b[(size_t)(k - 1) * dim1 + (j - 1)] = h2 * load;
         }
 }
+
+/* ------------------------------------------------------------------------------------
+ * MAT::Mult, src/MAT.cxx:715-800: C = L R. The columns of row i of C are listed in the
+ * order in which the loop over L's row i (k ascending) and R's row colInd[k] (l ascending)
+ * first meets them; C(i,c) = 0 + each matching L(i,k) R(k,l) in that loop order. (The
+ * reference finds a column by a linear search of the row's list; a column-to-slot table
+ * gives the same list and the same additions in the same order.)
+ * ---------------------------------------------------------------------------------- */
+int orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_t* cil,
+                 const double* val, uint32_t mr, const uint32_t* rpr, const uint32_t* cir,
+                 const double* var, uint32_t cap, uint32_t* nnzC, uint32_t* rpC,
+                 uint32_t* ciC, double* vaC)
+{
+    (void)ml;
+    uint32_t* slot = (uint32_t*)malloc((size_t)(mr ? mr : 1) * sizeof(uint32_t));
+    for (uint32_t c = 0; c < mr; ++c) slot[c] = 0xffffffffu;
+    uint32_t count = 0;
+    int fits = 1;
+    rpC[0] = 0;
+    for (uint32_t i = 0; i < nl; ++i) {
+        const uint32_t start = count;
+        for (uint32_t k = rpl[i]; k < rpl[i + 1]; ++k)
+            for (uint32_t l = rpr[cil[k]]; l < rpr[cil[k] + 1]; ++l) {
+                const uint32_t c = cir[l];
+                if (slot[c] == 0xffffffffu) {
+                    slot[c] = count;
+                    if (count < cap) {
+                        ciC[count] = c;
+                        vaC[count] = 0.0;
+                    } else {
+                        fits = 0;
+                    }
+                    ++count;
+                }
+                if (fits) vaC[slot[c]] += val[k] * var[l];
+            }
+        for (uint32_t q = start; q < count && q < cap; ++q) slot[ciC[q]] = 0xffffffffu;
+        if (!fits) /* keep counting: reset the table from R's rows again */
+            for (uint32_t k = rpl[i]; k < rpl[i + 1]; ++k)
+                for (uint32_t l = rpr[cil[k]]; l < rpr[cil[k] + 1]; ++l) slot[cir[l]] = 0xffffffffu;
+        rpC[i + 1] = count;
+    }
+    free(slot);
+    *nnzC = count;
+    return fits ? 0 : -1;
+}
+

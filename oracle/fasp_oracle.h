@@ -114,6 +114,14 @@ int    orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr,
  * Poisson2D.hxx TEST_PROBLEM 1) on the (dim-1)^2 interior grid. Port library only. */
 void   orc_matfree_rhs(int dim, double* b);
 
+/* MAT::Mult (src/MAT.cxx:715-800): C = L R (L: nl x ml, R: ml x mr). cap = capacity of
+ * ciC/vaC in entries; rpC holds nl + 1. Returns 0, or -1 when cap is too small (*nnzC is
+ * then the size needed). */
+int    orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_t* cil,
+                    const double* val, uint32_t mr, const uint32_t* rpr, const uint32_t* cir,
+                    const double* var, uint32_t cap, uint32_t* nnzC, uint32_t* rpC,
+                    uint32_t* ciC, double* vaC);
+
 /* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
 int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
                        uint32_t* colInd, double* values);

@@ -255,3 +255,24 @@ def matfree_rhs(dim: int) -> np.ndarray:
     b = np.empty((dim - 1) ** 2)
     lib.orc_matfree_rhs(dim, b)
     return b
+
+
+def mat_mult(kind, L, R):
+    """MAT::Mult: (rowPtr, colInd, values) of L R (CSRMatrix-like L and R)."""
+    lib = load(kind)
+    lib.orc_mat_mult.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p, C.c_uint32,
+                                 _u32p, _u32p, _f64p, C.c_uint32, C.POINTER(C.c_uint32),
+                                 _u32p, _u32p, _f64p]
+    lrp, lci = np.ascontiguousarray(L.rowPtr, np.uint32), np.ascontiguousarray(L.colInd, np.uint32)
+    rrp, rci = np.ascontiguousarray(R.rowPtr, np.uint32), np.ascontiguousarray(R.colInd, np.uint32)
+    lva, rva = np.ascontiguousarray(L.values, np.float64), np.ascontiguousarray(R.values, np.float64)
+    rlen = np.diff(rrp.astype(np.int64))
+    cap = int(rlen[lci].sum()) if len(lci) else 0
+    rp = np.zeros(L.nrow + 1, np.uint32)
+    ci = np.empty(max(cap, 1), np.uint32)
+    va = np.empty(max(cap, 1), np.float64)
+    z = C.c_uint32()
+    code = lib.orc_mat_mult(L.nrow, L.mcol, lrp, lci, lva, R.mcol, rrp, rci, rva, cap,
+                            C.byref(z), rp, ci, va)
+    assert code == 0
+    return rp, ci[:z.value].copy(), va[:z.value].copy()

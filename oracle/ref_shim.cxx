@@ -432,6 +432,33 @@ int orc_csr_to_mat(uint32_t nrow, uint32_t nnz, const uint32_t* rowPtr, const ui
     return static_cast<int>(code);
 }
 
+int orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_t* cil,
+                 const double* val, uint32_t mr, const uint32_t* rpr, const uint32_t* cir,
+                 const double* var, uint32_t cap, uint32_t* nnzC, uint32_t* rpC,
+                 uint32_t* ciC, double* vaC)
+{
+    std::vector<USI> lrp(rpl, rpl + nl + 1), lci(cil, cil + rpl[nl]);
+    std::vector<DBL> lva(val, val + rpl[nl]);
+    std::vector<USI> rrp(rpr, rpr + ml + 1), rci(cir, cir + rpr[ml]);
+    std::vector<DBL> rva(var, var + rpr[ml]);
+    MAT L(nl, ml, rpl[nl], lva, lci, lrp), R(ml, mr, rpr[ml], rva, rci, rrp), C;
+    C.Mult(L, R);
+    *nnzC = C.GetNNZ();
+    if (*nnzC > cap) return -1;
+    int* rp = C.GetRowPtr();
+    int* ci = C.GetColInd();
+    double* va = C.GetValues();
+    for (uint32_t i = 0; i <= nl; ++i) rpC[i] = (uint32_t)rp[i];
+    for (uint32_t k = 0; k < *nnzC; ++k) {
+        ciC[k] = (uint32_t)ci[k];
+        vaC[k] = va[k];
+    }
+    delete[] rp;
+    delete[] ci;
+    delete[] va;
+    return 0;
+}
+
 /* ReadMat (src/ReadData.cxx:361-446) of a .csr/.mtx file: call once with NULL arrays to
  * get nrow and nnz, then with arrays of those sizes. Returns the FaspRetCode. */
 int orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,

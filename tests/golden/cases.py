@@ -191,3 +191,23 @@ def write_csr(path: str, n: int, rp, ci, va) -> None:
         for a in (rp, ci):
             f.write("".join(f"{int(x)}\n" for x in a))
         f.write("".join(f"{float(x)!r}\n" for x in va))
+
+
+# ---- MAT::Mult (reference_mult.npz / .json, written by make_golden.py) ---------------------
+
+def mult_cases() -> dict:
+    """name -> (L, R, (rowPtr, colInd, values) of the reference's L R)."""
+    import json
+    from faspxx_b200 import problems as P
+    meta = json.load(open(os.path.join(HERE, "reference_mult.json")))
+    z = np.load(os.path.join(HERE, "reference_mult.npz"))
+    out = {}
+    for name in sorted({k.split("__")[0] for k in meta}):
+        mats = []
+        for tag in ("L", "R"):
+            nr, nc = meta[f"{name}__{tag}"]
+            mats.append(P.CSRMatrix(nr, nc, z[f"{name}__{tag}_rowPtr"],
+                                    z[f"{name}__{tag}_colInd"], z[f"{name}__{tag}_values"]))
+        out[name] = (mats[0], mats[1], (z[name + "__C_rowPtr"], z[name + "__C_colInd"],
+                                        z[name + "__C_values"]))
+    return out

@@ -20,7 +20,11 @@ Run in a container that has the reference tree (default /root/reference) after
 * ``reference_matfree.json`` -- what the reference's matrix-free example prints
   (example/TestMatFree.cxx, built from the reference sources by oracle/build_ref.sh).
 
-    python tests/golden/make_golden.py [/path/to/reference] [--ingest-only | --matfree-only]
+* ``reference_mult.npz`` + ``reference_mult.json`` -- MAT::Mult products computed by the
+  reference (stencil squares, rectangular random factors, an interpolation product).
+
+    python tests/golden/make_golden.py [/path/to/reference]
+                                       [--ingest-only | --matfree-only | --mult-only]
 """
 from __future__ import annotations
 
@@ -263,11 +267,78 @@ def make_matfree() -> None:
     print("wrote", len(runs), "matrix-free runs")
 
 
+def mult_cases():
+    """(name, L, R) of the MAT::Mult fixtures: stencil products, rectangular random factors
+    with unsorted rows, duplicate columns and empty rows, and a Galerkin triple product."""
+    rng = np.random.default_rng(77)
+
+    def rand(n, m, per_row, empty=0.1):
+        rp, ci, va = [0], [], []
+        for i in range(n):
+            if rng.random() >= empty:
+                k = int(rng.integers(1, per_row + 1))
+                cols = list(rng.integers(0, m, size=k))   # unsorted, may repeat
+                ci += cols
+                va += list(rng.integers(-8, 9, size=k) / 4.0 + rng.standard_normal(k) * 1e-3)
+            rp.append(len(ci))
+        return P.CSRMatrix(n, m, np.array(rp, np.uint32), np.array(ci, np.uint32),
+                           np.array(va, np.float64))
+
+    def interp1d(nf):
+        nc = (nf - 1) // 2
+        rp, ci, va = [0], [], []
+        for i in range(nf):
+            if i % 2 == 1:
+                ci.append((i - 1) // 2)
+                va.append(1.0)
+            else:
+                if i // 2 - 1 >= 0:
+                    ci.append(i // 2 - 1)
+                    va.append(0.5)
+                if i // 2 < nc:
+                    ci.append(i // 2)
+                    va.append(0.5)
+            rp.append(len(ci))
+        return P.CSRMatrix(nf, nc, np.array(rp, np.uint32), np.array(ci, np.uint32),
+                           np.array(va, np.float64))
+
+    A = P.poisson2d(6)
+    out = [("poisson2d_squared", A, A),
+           ("random_rect", rand(20, 15, 5), rand(15, 25, 6)),
+           ("random_dense_rows", rand(12, 40, 30, 0.0), rand(40, 9, 4))]
+    Pm = interp1d(15)
+    A1 = P.poisson2d(15, 1)
+    Rt = P.CSRMatrix(Pm.mcol, Pm.nrow, *O.transpose("ref", Pm)[:3])
+    out.append(("interp_R_times_A", Rt, A1))
+    return out
+
+
+def make_mult() -> None:
+    O.build(ref=True)
+    arr, meta = {}, {}
+    for name, L, R in mult_cases():
+        rp, ci, va = O.mat_mult("ref", L, R)
+        for tag, M in (("L", L), ("R", R)):
+            arr[f"{name}__{tag}_rowPtr"] = M.rowPtr
+            arr[f"{name}__{tag}_colInd"] = M.colInd
+            arr[f"{name}__{tag}_values"] = M.values
+            meta[f"{name}__{tag}"] = [int(M.nrow), int(M.mcol)]
+        arr[name + "__C_rowPtr"], arr[name + "__C_colInd"], arr[name + "__C_values"] = rp, ci, va
+    np.savez_compressed(os.path.join(HERE, "reference_mult.npz"), **arr)
+    with open(os.path.join(HERE, "reference_mult.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", len(meta) // 2, "MAT::Mult cases")
+
+
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     root = args[0] if args else "/root/reference"
+    if "--mult-only" in sys.argv:
+        make_mult()
+        sys.exit(0)
     if "--ingest-only" not in sys.argv and "--matfree-only" not in sys.argv:
         main(root)
     if "--matfree-only" not in sys.argv:
         make_ingest(root)
     make_matfree()
+    make_mult()
