@@ -92,6 +92,7 @@ SIGNATURES = {
     "fasp_gpu_vec_dot_noalloc": (_i, [_u32, _vp, _vp, _P(_d)]),
     "fasp_gpu_solver_create": (_i, [_P(Config), _P(_vp)]),
     "fasp_gpu_solver_setup": (_i, [_vp, _vp]),
+    "fasp_gpu_solver_set_mg_transfer": (_i, [_vp, _u32, _vp, _vp, _vp]),
     "fasp_gpu_solver_solve": (_i, [_vp, _vp, _vp, _P(Info)]),
     "fasp_gpu_solver_solve_host": (_i, [_vp, _vp, _vp, _P(Info)]),
     "fasp_gpu_solver_history": (_i, [_vp, _vp, _u32, _P(_u32)]),

@@ -535,6 +535,18 @@ int fasp_gpu_solver_setup(fasp_gpu_solver s, fasp_gpu_mat A)
     return s->s.setup(A);
 }
 
+int fasp_gpu_solver_set_mg_transfer(fasp_gpu_solver s, uint32_t level, fasp_gpu_mat P,
+                                    fasp_gpu_mat R, fasp_gpu_mat Ac)
+{
+    if (!s || !P || level > 64) return kErrInputPar;
+    auto& in = s->s.mgIn;
+    if (in.size() <= level) in.resize(level + 1);
+    in[level].P = P;
+    in[level].R = R;
+    in[level].Ac = Ac;
+    return kOk;
+}
+
 int fasp_gpu_solver_solve(fasp_gpu_solver s, const double* b, double* x, fasp_gpu_info* info)
 {
     if (!s || !b || !x) return kErrInputPar;

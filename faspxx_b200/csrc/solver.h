@@ -86,6 +86,19 @@ struct SolverImpl {
     std::vector<Pcd> mgSmooth, mgCoarse;
     std::vector<double*> mgB, mgX;
     int             mgLevel = -1;
+    // MG with transfer operators: what the caller set per coarse level (borrowed handles,
+    // kept across Setup calls), and what Setup resolved: the level operators A_0 .. A_L,
+    // P_l, R_l, the restrictions and Galerkin operators it formed itself (owned), and a
+    // residual vector per level below the finest
+    struct MgIn {
+        fasp_gpu_mat P = nullptr, R = nullptr, Ac = nullptr;
+    };
+    std::vector<MgIn>        mgIn;
+    std::vector<const Mat*>  mgA, mgP, mgR;
+    std::vector<Mat*>        mgOwn;
+    std::vector<double*>     mgRes;
+    int  mg_setup_transfers();
+    void mg_cycle_transfer(const double* b, double* x);
     // device-driven CG
     CGEngine<double>* cg64 = nullptr;
     CGEngine<float>*  cg32 = nullptr;

@@ -300,6 +300,11 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             break;
         }
         case FASP_GPU_MG: {
+            if (!mgIn.empty()) {
+                if ((e = alloc_vecs(w, 1, n))) return e; // r
+                if ((e = mg_setup_transfers())) return e;
+                break;
+            }
             // MG::SetupALL + SetupLevel with identity transfers (MG.cxx:26-79)
             if ((e = alloc_vecs(w, 1, n))) return e; // r
             const uint32_t L = cfg.mgLevels;
@@ -369,6 +374,16 @@ void SolverImpl::destroy()
     for (auto& p : mgCoarse) p.destroy();
     for (double* p : mgB) cudaFree(p);
     for (double* p : mgX) cudaFree(p);
+    for (double* p : mgRes) cudaFree(p);
+    mgRes.clear();
+    for (Mat* m : mgOwn) {
+        m_free(*m);
+        delete m;
+    }
+    mgOwn.clear();
+    mgA.clear();
+    mgP.clear();
+    mgR.clear();
     mgSmooth.clear();
     mgCoarse.clear();
     mgB.clear();
@@ -1797,6 +1812,103 @@ void SolverImpl::mg_cycle(const double* b, double* x)
     }
 }
 
+// ---- MG with transfer operators (no reference counterpart) -------------------------------
+// The reference's MG cycle (MG.cxx:105-152) with what its identity-transfer setup leaves
+// out: level l's residual uses its own operator A_l (the reference always uses the top-level
+// A, MG.cxx:119), the residual is restricted by R_l and the correction prolongated by P_l
+// (the reference stores one operator for both, MG.cxx:42-43). The smoother of level l runs
+// on A_l and the coarse solver on A_{l+1}. Missing restrictions are P_l's exact transpose;
+// missing coarse operators the Galerkin products R_l (A_l P_l), formed with MAT::Mult.
+
+int SolverImpl::mg_setup_transfers()
+{
+    const uint32_t L = cfg.mgLevels;
+    if (L == 0 || mgIn.size() != L) return kErrInputPar;
+    int e;
+    mgA.assign(1, A);
+    mgP.clear();
+    mgR.clear();
+    auto own = [&]() {
+        Mat* m = new Mat();
+        mgOwn.push_back(m);
+        return m;
+    };
+    for (uint32_t l = 0; l < L; ++l) {
+        if (!mgIn[l].P) return kErrInputPar;
+        const Mat* Al = mgA[l];
+        const Mat* P = &mgIn[l].P->M;
+        if (P->nrow != Al->nrow) return kErrNonmatch;
+        const uint32_t nc = P->mcol;
+        const Mat* R = nullptr;
+        if (mgIn[l].R) {
+            R = &mgIn[l].R->M;
+        } else {
+            Mat* T = own();
+            if ((e = m_transpose(c, *P, *T))) return e;
+            R = T;
+        }
+        if (R->nrow != nc || R->mcol != Al->nrow) return kErrNonmatch;
+        const Mat* Ac = nullptr;
+        if (mgIn[l].Ac) {
+            Ac = &mgIn[l].Ac->M;
+        } else {
+            Mat AP;
+            if ((e = m_mult(c, *Al, *P, AP))) return e;
+            Mat* G = own();
+            e = m_mult(c, *R, AP, *G);
+            m_free(AP);
+            if (e) return e;
+            Ac = G;
+        }
+        if (Ac->nrow != nc || Ac->mcol != nc) return kErrNonmatch;
+        mgA.push_back(Ac);
+        mgP.push_back(P);
+        mgR.push_back(R);
+    }
+    mgSmooth.resize(L);
+    mgCoarse.resize(L);
+    for (uint32_t l = 0; l < L; ++l) {
+        if ((e = mgSmooth[l].setup(c, mgA[l], 1, cfg.mgSmoothWeight, cfg.mgSmoothPrm)))
+            return e;
+        if ((e = mgCoarse[l].setup(c, mgA[l + 1], 1, cfg.mgCoarseWeight, cfg.mgCoarsePrm)))
+            return e;
+        std::vector<double*> v;
+        if ((e = alloc_vecs(v, 2, mgA[l + 1]->nrow))) return e;
+        mgB.push_back(v[0]);
+        mgX.push_back(v[1]);
+        std::vector<double*> r;
+        if (l > 0) {
+            if ((e = alloc_vecs(r, 1, mgA[l]->nrow))) return e;
+            mgRes.push_back(r[0]);
+        } else {
+            mgRes.push_back(nullptr); // level 0 uses the solver's residual vector
+        }
+    }
+    return kOk;
+}
+
+void SolverImpl::mg_cycle_transfer(const double* b, double* x)
+{
+    const uint32_t NL = (uint32_t)mgP.size();
+    ++mgLevel;
+    if ((uint32_t)mgLevel == NL) return;
+    const uint32_t l = (uint32_t)mgLevel;
+    const Mat& Al = *mgA[l];
+    double* r = l == 0 ? w[0] : mgRes[l];
+    mgSmooth[l].solve(c, b, x);                        // pre-smoothing on A_l
+    m_residual(c, Al, b, x, r, nullptr);               // r = b - A_l x
+    m_spmv(c, *mgR[l], r, mgB[l]);                     // b_{l+1} = R_l r
+    v_set(c, mgA[l + 1]->nrow, 0.0, mgX[l]);
+    if (l + 1 == NL)
+        mgCoarse[l].solve(c, mgB[l], mgX[l]);          // coarsest: on A_{l+1}
+    else
+        for (uint32_t i = 0; i < cfg.mgCycles; ++i) mg_cycle_transfer(mgB[l], mgX[l]);
+    m_spmv(c, *mgP[l], mgX[l], r);                     // P_l e_{l+1}
+    v_axpy(c, Al.nrow, Scal::h(1.0), r, x);
+    mgSmooth[l].solve(c, b, x);                        // post-smoothing
+    --mgLevel;
+}
+
 int SolverImpl::mg(const double* b, double* x, fasp_gpu_info* info)
 {
     const fasp_gpu_params& P = cfg.prm;
@@ -1815,7 +1927,10 @@ int SolverImpl::mg(const double* b, double* x, fasp_gpu_info* info)
             rec(numIter, resAbs);
             if (resRel < P.relTol || resAbs < P.absTol) break;
         }
-        mg_cycle(b, x);
+        if (mgP.empty())
+            mg_cycle(b, x);
+        else
+            mg_cycle_transfer(b, x);
         ++numIter;
     }
     info->numIter = numIter;

@@ -348,6 +348,11 @@ class SOL:
         h = C.c_void_p()
         check(lib.fasp_gpu_solver_create(C.byref(self.cfg), C.byref(h)), "solver_create")
         self.h = h
+        for level, (P, R, Ac) in sorted(getattr(self, "transfers", {}).items()):
+            check(lib.fasp_gpu_solver_set_mg_transfer(self.h, level, P.h,
+                                                      None if R is None else R.h,
+                                                      None if Ac is None else Ac.h),
+                  "set_mg_transfer")
         check(lib.fasp_gpu_solver_setup(self.h, self.A.h), "Setup")
         self._built = self._key()
 
@@ -459,8 +464,18 @@ class Jacobi(SOL):
 
 
 class MG(SOL):
-    """Abstract MG with identity transfers and Jacobi smoothers/coarse solvers (MG.hxx)."""
+    """Abstract MG with identity transfers and Jacobi smoothers/coarse solvers (MG.hxx), or,
+    with SetTransfer for every coarse level, MG with restriction/prolongation operators and
+    per-level operators (a B200 extension; see fasp_gpu_solver_set_mg_transfer)."""
     ALG = capi.MG
+
+    def SetTransfer(self, level: int, P: MAT, R: MAT | None = None, Ac: MAT | None = None):
+        """Level `level` (0 = finest): prolongation P from level+1, restriction R (None: P's
+        transpose) and coarse operator Ac (None: the Galerkin product R A P on the GPU)."""
+        if not hasattr(self, "transfers"):
+            self.transfers = {}
+        self.transfers[int(level)] = (P, R, Ac)
+        self._built = None
 
     def SetupALL(self, A: MAT, numLevels: int):
         self.cfg.mgLevels = int(numLevels)

@@ -246,6 +246,20 @@ int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out);
 /* Setup(const LOP& A): binds A (the caller keeps it alive, as SOL keeps a raw pointer,
  * SOL.hxx:28), builds the preconditioner (Jacobi::Setup, Iter.cxx:29-53) and work space. */
 int fasp_gpu_solver_setup(fasp_gpu_solver s, fasp_gpu_mat A);
+/* MG with transfer operators (no reference counterpart: the reference's MG::SetupLevel
+ * stores one operator as both restriction and prolongation, MG.cxx:42-43, and every level's
+ * residual uses the top-level matrix, MG.cxx:119, so only identity transfers work there).
+ * Call before fasp_gpu_solver_setup for every coarse level l = 0 .. mgLevels - 1 (level 0
+ * is the Setup matrix): P = prolongation from level l+1 to level l (n_l x n_{l+1}); R =
+ * restriction (n_{l+1} x n_l), NULL for the exact transpose of P; Ac = the level-(l+1)
+ * operator, NULL for the Galerkin product R (A_l P) formed with MAT::Mult on the GPU. The
+ * cycle is the reference's (pre-smoothing, residual, restriction, coarse solve or the next
+ * level's cycles, prolongation, correction, post-smoothing) with level l's smoother on A_l,
+ * the coarse solver on A_mgLevels and each residual on its own level's operator. Handles
+ * are borrowed: keep them alive while the solver uses them. Setup returns ERROR_INPUT_PAR
+ * when a level is missing and ERROR_MAT_NONMATCH for inconsistent sizes. */
+int fasp_gpu_solver_set_mg_transfer(fasp_gpu_solver s, uint32_t level, fasp_gpu_mat P,
+                                    fasp_gpu_mat R, fasp_gpu_mat Ac);
 /* Solve(b, x) on DEVICE vectors: x is the initial guess in, the solution out. */
 int fasp_gpu_solver_solve(fasp_gpu_solver s, const double* b, double* x, fasp_gpu_info* info);
 /* Solve(b, x) on HOST vectors: copies in, solves, copies out (end-to-end path). */

@@ -407,6 +407,12 @@ struct osol {
     double**  lx;
     double*   mgr;
     int       level;
+    /* MG with transfer operators (orc_mg_set_level): lA[l] = A_{l+1}, lP[l], lR[l], and the
+     * residual vector lr[l] of level l >= 1 */
+    omat_t**  lA;
+    omat_t**  lP;
+    omat_t**  lR;
+    double**  lr;
 };
 
 typedef struct {
@@ -952,6 +958,29 @@ static void mg_cycle(osol_t* s, const double* b, double* x)
 {
     const omat_t* A = s->A;
     const uint32_t n = s->len;
+    if (s->lP) {
+        /* with transfer operators: the same cycle, level l's residual with A_l, restriction
+         * R_l, prolongation P_l (the B200 library's fasp_gpu_solver_set_mg_transfer) */
+        ++s->level;
+        if ((uint32_t)s->level == s->numLevels) return;
+        const uint32_t l = (uint32_t)s->level;
+        const omat_t* Al = l == 0 ? A : s->lA[l - 1];
+        double* r = l == 0 ? s->mgr : s->lr[l];
+        const omat_t *R = s->lR[l], *P = s->lP[l];
+        sol_solve(s->smoothers[l], b, x);
+        orc_residual(Al->nrow, Al->mcol, Al->rowPtr, Al->colInd, Al->values, b, x, r);
+        orc_spmv(R->nrow, R->rowPtr, R->colInd, R->values, r, s->lb[l]);
+        v_set(s->lA[l]->nrow, 0.0, s->lx[l]);
+        if (l + 1 == s->numLevels)
+            sol_solve(s->coarse[l], s->lb[l], s->lx[l]);
+        else
+            for (uint32_t i = 0; i < s->numCycles[l]; ++i) mg_cycle(s, s->lb[l], s->lx[l]);
+        orc_spmv(P->nrow, P->rowPtr, P->colInd, P->values, s->lx[l], r);
+        v_axpy(Al->nrow, 1.0, r, x);
+        sol_solve(s->smoothers[l], b, x);
+        --s->level;
+        return;
+    }
     if (s->numLevels > 0) {
         ++s->level;
         if ((uint32_t)s->level - s->numLevels == 0) return;
@@ -1072,9 +1101,24 @@ static osol_t* new_jacobi(const orc_params_t* prm, double weight, const omat_t* 
     return s;
 }
 
+static void omat_free(omat_t* m)
+{
+    if (!m) return;
+    free(m->rowPtr); free(m->colInd); free(m->diagPtr); free(m->values);
+    free(m);
+}
+
 static void free_sol(osol_t* s)
 {
     if (!s) return;
+    if (s->lP)
+        for (uint32_t l = 0; l < s->numLevels; ++l) {
+            omat_free(s->lA[l]);
+            omat_free(s->lP[l]);
+            omat_free(s->lR[l]);
+            free(s->lr[l]);
+        }
+    free(s->lA); free(s->lP); free(s->lR); free(s->lr);
     free(s->diagInv); free(s->work);
     free(s->rk); free(s->pk); free(s->zk); free(s->ax); free(s->safe);
     free(s->r0star); free(s->tmp); free(s->apj); free(s->asj); free(s->sj);
@@ -1325,5 +1369,65 @@ int orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_t* 
     free(slot);
     *nnzC = count;
     return fits ? 0 : -1;
+}
+
+static omat_t* omat_copy(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rp,
+                         const uint32_t* ci, const double* va)
+{
+    omat_t* m = (omat_t*)calloc(1, sizeof(omat_t));
+    m->nrow = nrow;
+    m->mcol = mcol;
+    m->nnz = nnz;
+    m->rowPtr = (uint32_t*)malloc(((size_t)nrow + 1) * sizeof(uint32_t));
+    m->colInd = (uint32_t*)malloc(((size_t)nnz + 1) * sizeof(uint32_t));
+    m->diagPtr = (uint32_t*)malloc(((size_t)nrow + 1) * sizeof(uint32_t));
+    m->values = (double*)malloc(((size_t)nnz + 1) * sizeof(double));
+    memcpy(m->rowPtr, rp, ((size_t)nrow + 1) * sizeof(uint32_t));
+    memcpy(m->colInd, ci, (size_t)nnz * sizeof(uint32_t));
+    memcpy(m->values, va, (size_t)nnz * sizeof(double));
+    orc_diagptr(nrow, m->rowPtr, m->colInd, m->diagPtr);
+    return m;
+}
+
+int orc_mg_set_level(void* hv, uint32_t level,
+                     uint32_t pn, uint32_t pm, uint32_t pnnz, const uint32_t* prp,
+                     const uint32_t* pci, const double* pva,
+                     uint32_t rn, uint32_t rm, uint32_t rnnz, const uint32_t* rrp,
+                     const uint32_t* rci, const double* rva,
+                     uint32_t an, uint32_t annz, const uint32_t* arp, const uint32_t* aci,
+                     const double* ava)
+{
+    ohandle_t* h = (ohandle_t*)hv;
+    osol_t* s = h ? h->sol : NULL;
+    if (!s || s->alg != ORC_MG || level >= s->numLevels) return ERROR_INPUT_PAR;
+    const uint32_t L = s->numLevels;
+    if (!s->lP) {
+        s->lA = (omat_t**)calloc(L, sizeof(omat_t*));
+        s->lP = (omat_t**)calloc(L, sizeof(omat_t*));
+        s->lR = (omat_t**)calloc(L, sizeof(omat_t*));
+        s->lr = (double**)calloc(L, sizeof(double*));
+    }
+    omat_free(s->lA[level]);
+    omat_free(s->lP[level]);
+    omat_free(s->lR[level]);
+    s->lP[level] = omat_copy(pn, pm, pnnz, prp, pci, pva);
+    s->lR[level] = omat_copy(rn, rm, rnnz, rrp, rci, rva);
+    s->lA[level] = omat_copy(an, an, annz, arp, aci, ava);
+    /* the coarse solver of this level and the smoother of the next one run on A_{level+1} */
+    osol_t* old = s->coarse[level];
+    s->coarse[level] = new_jacobi(&old->prm, old->weight, s->lA[level]);
+    free_sol(old);
+    if (level + 1 < L) {
+        old = s->smoothers[level + 1];
+        s->smoothers[level + 1] = new_jacobi(&old->prm, old->weight, s->lA[level]);
+        free_sol(old);
+        free(s->lr[level + 1]);
+        s->lr[level + 1] = dalloc(an);
+    }
+    free(s->lb[level]);
+    free(s->lx[level]);
+    s->lb[level] = dalloc(an);
+    s->lx[level] = dalloc(an);
+    return SUCCESS;
 }
 

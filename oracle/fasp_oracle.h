@@ -122,6 +122,20 @@ int    orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_
                     const double* var, uint32_t cap, uint32_t* nnzC, uint32_t* rpC,
                     uint32_t* ciC, double* vaC);
 
+/* Port library only: MG with transfer operators (the B200 library's
+ * fasp_gpu_solver_set_mg_transfer) on a handle made by orc_create with alg ORC_MG: level l
+ * gets prolongation P (n_l x n_{l+1}), restriction R (n_{l+1} x n_l) and the operator
+ * A_{l+1} (an x an). MG::MGCycle (src/MG.cxx:105-152) then runs with level l's residual
+ * on A_l, R and P as the transfers, the smoother of level l on A_l and the coarse solver
+ * on A_{l+1}. Every coarse level must be set before orc_solve. */
+int    orc_mg_set_level(void* h, uint32_t level,
+                        uint32_t pn, uint32_t pm, uint32_t pnnz, const uint32_t* prp,
+                        const uint32_t* pci, const double* pva,
+                        uint32_t rn, uint32_t rm, uint32_t rnnz, const uint32_t* rrp,
+                        const uint32_t* rci, const double* rva,
+                        uint32_t an, uint32_t annz, const uint32_t* arp, const uint32_t* aci,
+                        const double* ava);
+
 /* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
 int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
                        uint32_t* colInd, double* values);

@@ -157,6 +157,23 @@ class Solver:
                                   self.histCap)
         return Result(code, x, it.value, n2.value, ni.value, hist[: it.value + 1].copy())
 
+    def set_mg_level(self, level, P, R, Ac):
+        """MG with transfer operators (port library): level's P, R and coarse operator."""
+        self.lib.orc_mg_set_level.argtypes = [C.c_void_p, C.c_uint32] + \
+            [C.c_uint32, C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p] * 2 + \
+            [C.c_uint32, C.c_uint32, _u32p, _u32p, _f64p]
+        mats = []
+        for M in (P, R, Ac):
+            mats.append((np.ascontiguousarray(M.rowPtr, np.uint32),
+                         np.ascontiguousarray(M.colInd, np.uint32),
+                         np.ascontiguousarray(M.values, np.float64)))
+        self._keep = self._keep + tuple(mats)
+        (prp, pci, pva), (rrp, rci, rva), (arp, aci, ava) = mats
+        code = self.lib.orc_mg_set_level(self.h, level, P.nrow, P.mcol, len(pci), prp, pci, pva,
+                                         R.nrow, R.mcol, len(rci), rrp, rci, rva,
+                                         Ac.nrow, len(aci), arp, aci, ava)
+        assert code == 0, code
+
     def clean(self):
         self.lib.orc_clean(self.h)
 
