@@ -68,6 +68,7 @@ SIGNATURES = {
     "fasp_gpu_mat_create_csr_raw": (_i, [_u32, _u32, _u32, _vp, _vp, _vp, _i, _P(_vp)]),
     "fasp_gpu_mat_create_stencil": (_i, [_u32, _u32, _u32, _u32, _vp, _vp, _vp, _vp, _P(_vp)]),
     "fasp_gpu_mat_mult": (_i, [_vp, _vp, _P(_vp)]),
+    "fasp_gpu_mat_add": (_i, [C.c_double, _vp, C.c_double, _vp, _P(_vp)]),
     "fasp_gpu_mat_destroy": (_i, [_vp]),
     "fasp_gpu_mat_info": (_i, [_vp, _P(_u32), _P(_u32), _P(_u32)]),
     "fasp_gpu_mat_download": (_i, [_vp, _vp, _vp, _vp, _vp]),

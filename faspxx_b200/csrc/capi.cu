@@ -290,6 +290,12 @@ int fasp_gpu_mat_mult(fasp_gpu_mat L, fasp_gpu_mat R, fasp_gpu_mat* out)
     return mat_build(out, [&](fasp_gpu_mat h) { return m_mult(h->c, L->M, R->M, h->M); });
 }
 
+int fasp_gpu_mat_add(double a, fasp_gpu_mat A, double b, fasp_gpu_mat B, fasp_gpu_mat* out)
+{
+    if (!A || !B) return kErrInputPar;
+    return mat_build(out, [&](fasp_gpu_mat h) { return m_add(h->c, a, A->M, b, B->M, h->M); });
+}
+
 int fasp_gpu_mat_destroy(fasp_gpu_mat A)
 {
     if (!A) return kOk;

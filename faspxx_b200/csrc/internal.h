@@ -256,6 +256,8 @@ int m_create_stencil(Mat& M, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t npt
                      cudaStream_t s);
 // C = L R exactly as MAT::Mult (src/MAT.cxx:715-800) forms it (spgemm.cu).
 int m_mult(Ctx& c, const Mat& L, const Mat& R, Mat& C);
+// C = a A + b B exactly as MAT::Add (src/MAT.cxx:652-713) forms it (spgemm.cu).
+int m_add(Ctx& c, double a, const Mat& A, double b, const Mat& B, Mat& C);
 // The CSR arrays of a grid operator, generated on the host (downloads and tests).
 void m_grid_csr(const Mat& M, std::vector<uint32_t>& rowPtr, std::vector<uint32_t>& colInd,
                 std::vector<double>& values);

@@ -1,4 +1,4 @@
-// spgemm.cu -- the sparse matrix product C = L R on the device, MAT::Mult
+// spgemm.cu -- sparse matrix algebra on the device: the product C = L R, MAT::Mult
 // (src/MAT.cxx:715-800) with its exact result:
 //   * the columns of row i of C appear in the order in which the loop over L's row i
 //     (entries k in CSR order) and, for each, R's row colInd[k] (entries l in CSR order)
@@ -10,7 +10,7 @@
 // sorted (equal columns become adjacent, in loop order), each run of one column is summed in
 // order and remembered by its first position, and a second sort by first position restores
 // MAT::Mult's column order. Products are computed and stored before they are added, so no
-// multiply-add is fused.
+// multiply-add is fused. Further down: the sum C = a A + b B, MAT::Add.
 #include "segsort.cuh"
 
 namespace fb {
@@ -165,6 +165,114 @@ int m_mult(Ctx& c, const Mat& L, const Mat& R, Mat& C)
     FB_CUDA(cudaGetLastError());
     FB_CUDA(cudaStreamSynchronize(s));
     return m_upload(C, n, R.mcol, nnzC, crp, cci, cva, false, s);
+}
+
+namespace {
+
+// ---- MAT::Add (src/MAT.cxx:652-713): C = a A + b B -------------------------------------------
+// Row i of C: A's entries in order as a A(i,k); then each entry of B's row in order is added
+// to the first entry of A's row with its column -- or to the first of B's entries already
+// appended to this row, the one extra slot MAT::Add's search window reaches -- else appended
+// as b B(i,k); finally each row sorted by column, stably (SortCSRRow). Products and sums are
+// rounded separately as the reference rounds them.
+
+__global__ void k_add_rows(uint32_t n, double a, double b, const uint32_t* __restrict__ arp,
+                           const uint32_t* __restrict__ aci, const double* __restrict__ ava,
+                           const uint32_t* __restrict__ brp, const uint32_t* __restrict__ bci,
+                           const double* __restrict__ bva, uint32_t* __restrict__ tci,
+                           double* __restrict__ tva, uint32_t* __restrict__ nout)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t base = (size_t)arp[i] + brp[i];
+        const uint32_t c1 = arp[i + 1] - arp[i];
+        uint32_t cnt = 0;
+        for (uint32_t k = arp[i]; k < arp[i + 1]; ++k, ++cnt) {
+            tci[base + cnt] = aci[k];
+            tva[base + cnt] = __dmul_rn(a, ava[k]);
+        }
+        for (uint32_t k = brp[i]; k < brp[i + 1]; ++k) {
+            const uint32_t col = bci[k];
+            const double v = __dmul_rn(b, bva[k]);
+            const uint32_t window = cnt > c1 ? c1 + 1 : c1;
+            uint32_t l = 0;
+            for (; l < window; ++l)
+                if (tci[base + l] == col) break;
+            if (l < window) {
+                tva[base + l] = __dadd_rn(tva[base + l], v);
+            } else {
+                tci[base + cnt] = col;
+                tva[base + cnt] = v;
+                ++cnt;
+            }
+        }
+        nout[i] = cnt;
+    }
+}
+
+__global__ void k_add_keys(uint32_t n, const uint32_t* __restrict__ arp,
+                           const uint32_t* __restrict__ brp, const uint32_t* __restrict__ crp,
+                           const uint32_t* __restrict__ tci, uint64_t* __restrict__ keys)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t base = (size_t)arp[i] + brp[i];
+        for (uint32_t q = crp[i]; q < crp[i + 1]; ++q) {
+            const uint32_t p = q - crp[i];
+            keys[q] = (uint64_t)tci[base + p] << 32 | p;
+        }
+    }
+}
+
+__global__ void k_add_out(uint32_t n, const uint32_t* __restrict__ arp,
+                          const uint32_t* __restrict__ brp, const uint32_t* __restrict__ crp,
+                          const uint64_t* __restrict__ keys, const double* __restrict__ tva,
+                          uint32_t* __restrict__ cci, double* __restrict__ cva)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t base = (size_t)arp[i] + brp[i];
+        for (uint32_t q = crp[i]; q < crp[i + 1]; ++q) {
+            cci[q] = (uint32_t)(keys[q] >> 32);
+            cva[q] = tva[base + (uint32_t)keys[q]];
+        }
+    }
+}
+
+} // namespace
+
+int m_add(Ctx& c, double a, const Mat& A, double b, const Mat& B, Mat& C)
+{
+    if (A.grid || B.grid || !A.val || !B.val) return kErrInputPar;
+    if (A.nrow != B.nrow || A.mcol != B.mcol) return kErrNonmatch;
+    const uint64_t cap = (uint64_t)A.nnz + B.nnz;
+    if (cap > 0xffffffffull) return kErrMatSize;
+    cudaStream_t s = c.stream;
+    const uint32_t n = A.nrow;
+    Tmp t;
+    int e;
+    uint32_t *tci = nullptr, *nout = nullptr, *crp = nullptr, *tiles = nullptr, *cci = nullptr;
+    double *tva = nullptr, *cva = nullptr;
+    uint64_t* keys = nullptr;
+    if ((e = t.get(&tci, cap)) || (e = t.get(&tva, cap)) || (e = t.get(&nout, n)) ||
+        (e = t.get(&crp, (size_t)n + 1)) || (e = t.get(&tiles, (n + (size_t)kTile - 1) / kTile)))
+        return e;
+    const int g = grid_for(n, 256);
+    k_add_rows<<<g, 256, 0, s>>>(n, a, b, A.rowPtr, A.colInd, A.val, B.rowPtr, B.colInd, B.val,
+                                 tci, tva, nout);
+    FB_CUDA(cudaGetLastError());
+    if ((e = scan_counts(s, n, nout, crp, tiles))) return e;
+    uint32_t nnzC = 0;
+    FB_CUDA(cudaMemcpyAsync(&nnzC, crp + n, 4, cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    if ((e = t.get(&keys, nnzC)) || (e = t.get(&cci, nnzC)) || (e = t.get(&cva, nnzC))) return e;
+    k_add_keys<<<g, 256, 0, s>>>(n, A.rowPtr, B.rowPtr, crp, tci, keys);
+    FB_CUDA(cudaGetLastError());
+    if ((e = sort_row_keys(c, t, n, crp, keys, nnzC))) return e;
+    k_add_out<<<g, 256, 0, s>>>(n, A.rowPtr, B.rowPtr, crp, keys, tva, cci, cva);
+    FB_CUDA(cudaGetLastError());
+    FB_CUDA(cudaStreamSynchronize(s));
+    return m_upload(C, n, A.mcol, nnzC, crp, cci, cva, false, s);
 }
 
 } // namespace fb

@@ -199,6 +199,13 @@ class MAT:
         check(lib.fasp_gpu_mat_mult(self.h, R.h, C.byref(h)), "Mult")
         return MAT(_handle=h)
 
+    @staticmethod
+    def Add(a: float, A: "MAT", b: float, B: "MAT") -> "MAT":
+        """MAT::Add (src/MAT.cxx:652-713): a A + b B as a new matrix, computed on the GPU."""
+        h = C.c_void_p()
+        check(lib.fasp_gpu_mat_add(a, A.h, b, B.h, C.byref(h)), "Add")
+        return MAT(_handle=h)
+
     def Transpose(self) -> "MAT":
         """MAT::TransInPlace into a new matrix (the original stays)."""
         h = C.c_void_p()

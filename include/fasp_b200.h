@@ -177,6 +177,13 @@ int fasp_gpu_mat_create_stencil(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t 
  * for a pattern-only matrix or a grid operator (no stored values); ERROR_MAT_SIZE when the
  * product has no entries or more than 2^32 - 1 intermediate products. */
 int fasp_gpu_mat_mult(fasp_gpu_mat L, fasp_gpu_mat R, fasp_gpu_mat* out);
+/* MAT::Add (MAT.cxx:652-713): *out = a A + b B on the device, with MAT::Add's exact result
+ * -- each row: A's entries as a A(i,k), then every entry of B's row added (b B(i,k)) to the
+ * first of A's entries with its column, or to the first of B's entries already appended to
+ * the row (the reference's search window), else appended; then the row sorted by column,
+ * stably (SortCSRRow). ERROR_MAT_NONMATCH for different sizes; ERROR_INPUT_PAR for a
+ * pattern-only matrix or a grid operator. */
+int fasp_gpu_mat_add(double a, fasp_gpu_mat A, double b, fasp_gpu_mat B, fasp_gpu_mat* out);
 int fasp_gpu_mat_destroy(fasp_gpu_mat A);
 /* GetRowSize / GetColSize / GetNNZ (LOP.hxx:50-53, MAT.hxx:113) */
 int fasp_gpu_mat_info(fasp_gpu_mat A, uint32_t* nrow, uint32_t* mcol, uint32_t* nnz);

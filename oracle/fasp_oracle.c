@@ -1431,3 +1431,41 @@ int orc_mg_set_level(void* hv, uint32_t level,
     return SUCCESS;
 }
 
+/* MAT::Add, src/MAT.cxx:652-713: C = a A + b B. Row i: A's entries as a*A(i,k); each entry
+ * of B's row (in order) is added to the first entry of the row so far with its column among
+ * A's entries and the first appended B entry (the reference searches countrow + 1 slots), or
+ * appended as b*B(i,k); then SortCSRRow. Outputs hold nnz(A) + nnz(B) entries. */
+int orc_mat_add(uint32_t n, uint32_t m, double a, const uint32_t* arp, const uint32_t* aci,
+                const double* ava, double b, const uint32_t* brp, const uint32_t* bci,
+                const double* bva, uint32_t* nnzC, uint32_t* rpC, uint32_t* ciC, double* vaC)
+{
+    (void)m;
+    uint32_t count = 0;
+    rpC[0] = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t start = count, c1 = arp[i + 1] - arp[i];
+        for (uint32_t k = arp[i]; k < arp[i + 1]; ++k) {
+            ciC[count] = aci[k];
+            vaC[count] = a * ava[k];
+            ++count;
+        }
+        for (uint32_t k = brp[i]; k < brp[i + 1]; ++k) {
+            const uint32_t window = (count - start > c1) ? c1 + 1 : c1;
+            uint32_t l = 0;
+            for (; l < window; ++l)
+                if (ciC[start + l] == bci[k]) break;
+            if (l < window) {
+                vaC[start + l] = vaC[start + l] + b * bva[k];
+            } else {
+                ciC[count] = bci[k];
+                vaC[count] = b * bva[k];
+                ++count;
+            }
+        }
+        rpC[i + 1] = count;
+    }
+    sort_rows(n, rpC, ciC, vaC);
+    *nnzC = count;
+    return SUCCESS;
+}
+

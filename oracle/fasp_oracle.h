@@ -136,6 +136,15 @@ int    orc_mg_set_level(void* h, uint32_t level,
                         uint32_t an, uint32_t annz, const uint32_t* arp, const uint32_t* aci,
                         const double* ava);
 
+/* MAT::Add (src/MAT.cxx:652-713): C = a A + b B (n x m each); outputs hold nnz(A) + nnz(B)
+ * entries and n + 1 row pointers. The reference library returns ORC_REF_UNDEFINED, without
+ * calling the reference, when the sort of a row 0 would move an entry to the front
+ * (SortCSRRow's unsigned index wraps). */
+int    orc_mat_add(uint32_t n, uint32_t m, double a, const uint32_t* arp, const uint32_t* aci,
+                   const double* ava, double b, const uint32_t* brp, const uint32_t* bci,
+                   const double* bva, uint32_t* nnzC, uint32_t* rpC, uint32_t* ciC,
+                   double* vaC);
+
 /* Reference library only (_ref/liboracle_ref.so): ReadMat of a .csr/.mtx file. */
 int    orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,
                        uint32_t* colInd, double* values);

@@ -293,3 +293,21 @@ def mat_mult(kind, L, R):
                             C.byref(z), rp, ci, va)
     assert code == 0
     return rp, ci[:z.value].copy(), va[:z.value].copy()
+
+
+def mat_add(kind, a, A, b, B):
+    """MAT::Add: (code, (rowPtr, colInd, values)) of a A + b B."""
+    lib = load(kind)
+    lib.orc_mat_add.argtypes = [C.c_uint32, C.c_uint32, C.c_double, _u32p, _u32p, _f64p,
+                                C.c_double, _u32p, _u32p, _f64p, C.POINTER(C.c_uint32),
+                                _u32p, _u32p, _f64p]
+    arrs = [np.ascontiguousarray(x, t) for x, t in
+            ((A.rowPtr, np.uint32), (A.colInd, np.uint32), (A.values, np.float64),
+             (B.rowPtr, np.uint32), (B.colInd, np.uint32), (B.values, np.float64))]
+    cap = len(arrs[1]) + len(arrs[4])
+    rp = np.zeros(A.nrow + 1, np.uint32)
+    ci, va = np.empty(max(cap, 1), np.uint32), np.empty(max(cap, 1), np.float64)
+    z = C.c_uint32()
+    code = lib.orc_mat_add(A.nrow, A.mcol, a, arrs[0], arrs[1], arrs[2], b, arrs[3], arrs[4],
+                           arrs[5], C.byref(z), rp, ci, va)
+    return code, (rp, ci[:z.value].copy(), va[:z.value].copy())

@@ -459,6 +459,32 @@ int orc_mat_mult(uint32_t nl, uint32_t ml, const uint32_t* rpl, const uint32_t* 
     return 0;
 }
 
+int orc_mat_add(uint32_t n, uint32_t m, double a, const uint32_t* arp, const uint32_t* aci,
+                const double* ava, double b, const uint32_t* brp, const uint32_t* bci,
+                const double* bva, uint32_t* nnzC, uint32_t* rpC, uint32_t* ciC, double* vaC)
+{
+    /* row 0 as MAT::Add builds it before sorting: A's columns, then B's unmatched ones */
+    std::vector<USI> row0(aci, aci + arp[1]);
+    for (uint32_t k = brp[0]; k < brp[1]; ++k) {
+        bool hit = false;
+        for (USI c : row0) hit = hit || c == bci[k];
+        if (!hit) row0.push_back(bci[k]);
+    }
+    std::vector<USI> rp0{0, (USI)row0.size()};
+    if (!row0.empty() && row0_undefined(rp0, row0)) return ORC_REF_UNDEFINED;
+    std::vector<USI> arpv(arp, arp + n + 1), aciv(aci, aci + arp[n]);
+    std::vector<DBL> avav(ava, ava + arp[n]);
+    std::vector<USI> brpv(brp, brp + n + 1), bciv(bci, bci + brp[n]);
+    std::vector<DBL> bvav(bva, bva + brp[n]);
+    MAT A(n, m, arp[n], avav, aciv, arpv), B(n, m, brp[n], bvav, bciv, brpv), C;
+    std::ostringstream sink;
+    std::streambuf* old = std::cout.rdbuf(sink.rdbuf());
+    C.Add(a, A, b, B);
+    std::cout.rdbuf(old);
+    copy_mat(C, nnzC, rpC, ciC, vaC);
+    return 0;
+}
+
 /* ReadMat (src/ReadData.cxx:361-446) of a .csr/.mtx file: call once with NULL arrays to
  * get nrow and nnz, then with arrays of those sizes. Returns the FaspRetCode. */
 int orc_ref_readmat(const char* path, uint32_t* nrow, uint32_t* nnz, uint32_t* rowPtr,

@@ -202,7 +202,7 @@ def mult_cases() -> dict:
     meta = json.load(open(os.path.join(HERE, "reference_mult.json")))
     z = np.load(os.path.join(HERE, "reference_mult.npz"))
     out = {}
-    for name in sorted({k.split("__")[0] for k in meta}):
+    for name in sorted({k.split("__")[0] for k in meta if not k.startswith("add_")}):
         mats = []
         for tag in ("L", "R"):
             nr, nc = meta[f"{name}__{tag}"]
@@ -210,4 +210,22 @@ def mult_cases() -> dict:
                                     z[f"{name}__{tag}_colInd"], z[f"{name}__{tag}_values"]))
         out[name] = (mats[0], mats[1], (z[name + "__C_rowPtr"], z[name + "__C_colInd"],
                                         z[name + "__C_values"]))
+    return out
+
+
+def add_cases() -> dict:
+    """name -> (a, A, b, B, (rowPtr, colInd, values) of the reference's a A + b B)."""
+    import json
+    from faspxx_b200 import problems as P
+    meta = json.load(open(os.path.join(HERE, "reference_mult.json")))
+    z = np.load(os.path.join(HERE, "reference_mult.npz"))
+    out = {}
+    for key, m in meta.items():
+        if not key.startswith("add_"):
+            continue
+        nr, nc = m["shape"]
+        A, B = (P.CSRMatrix(nr, nc, z[f"{key}__{t}_rowPtr"], z[f"{key}__{t}_colInd"],
+                            z[f"{key}__{t}_values"]) for t in ("A", "B"))
+        out[key[4:]] = (m["a"], A, m["b"], B, (z[key + "__C_rowPtr"], z[key + "__C_colInd"],
+                                                  z[key + "__C_values"]))
     return out

@@ -20,8 +20,9 @@ Run in a container that has the reference tree (default /root/reference) after
 * ``reference_matfree.json`` -- what the reference's matrix-free example prints
   (example/TestMatFree.cxx, built from the reference sources by oracle/build_ref.sh).
 
-* ``reference_mult.npz`` + ``reference_mult.json`` -- MAT::Mult products computed by the
-  reference (stencil squares, rectangular random factors, an interpolation product).
+* ``reference_mult.npz`` + ``reference_mult.json`` -- MAT::Mult products and MAT::Add sums
+  computed by the reference (stencil squares, rectangular random factors, an interpolation
+  product; stencil plus diagonal, unsorted random rows, repeated appended columns).
 
     python tests/golden/make_golden.py [/path/to/reference]
                                        [--ingest-only | --matfree-only | --mult-only]
@@ -313,6 +314,42 @@ def mult_cases():
     return out
 
 
+def add_cases():
+    """(name, a, A, b, B) of the MAT::Add fixtures: a stencil plus a shifted diagonal, random
+    unsorted rows with repeated columns (row 0 starts with its smallest column: the
+    reference's SortCSRRow cannot move an entry to the front of row 0), and B entries that
+    repeat a column first appended from B (the one extra slot MAT::Add searches)."""
+    rng = np.random.default_rng(91)
+
+    def rand(n, m, per):
+        rp, ci, va = [0], [], []
+        for i in range(n):
+            k = int(rng.integers(1, per + 1))
+            cols = [0] if i == 0 else []
+            cols += list(rng.integers(1 if i == 0 else 0, m, size=k))
+            ci += cols
+            va += list(rng.integers(-8, 9, size=len(cols)) / 8.0 + rng.standard_normal(len(cols)) * 1e-3)
+            rp.append(len(ci))
+        return P.CSRMatrix(n, m, np.array(rp, np.uint32), np.array(ci, np.uint32),
+                           np.array(va, np.float64))
+
+    A = P.poisson2d(6)
+    D = P.CSRMatrix(36, 36, np.arange(37, dtype=np.uint32), np.arange(36, dtype=np.uint32),
+                    np.linspace(0.5, 2.0, 36))
+    # B rows that append a new column and then repeat it
+    B3rp, B3ci, B3va = [0], [], []
+    for i in range(36):
+        cols = [0, (i + 7) % 36, (i + 7) % 36, (i + 9) % 36, (i + 7) % 36]
+        B3ci += cols
+        B3va += [0.25, 1.5, -0.75, 2.0, 0.125]
+        B3rp.append(len(B3ci))
+    B3 = P.CSRMatrix(36, 36, np.array(B3rp, np.uint32), np.array(B3ci, np.uint32),
+                     np.array(B3va, np.float64))
+    return [("stencil_plus_diag", 1.0, A, 0.5, D),
+            ("random_unsorted", 0.5, rand(30, 20, 6), -1.25, rand(30, 20, 6)),
+            ("repeated_appends", 2.0, A, -1.0, B3)]
+
+
 def make_mult() -> None:
     O.build(ref=True)
     arr, meta = {}, {}
@@ -324,10 +361,20 @@ def make_mult() -> None:
             arr[f"{name}__{tag}_values"] = M.values
             meta[f"{name}__{tag}"] = [int(M.nrow), int(M.mcol)]
         arr[name + "__C_rowPtr"], arr[name + "__C_colInd"], arr[name + "__C_values"] = rp, ci, va
+    for name, a, A, b, B in add_cases():
+        code, (rp, ci, va) = O.mat_add("ref", a, A, b, B)
+        assert code == 0, name
+        for tag, M in (("A", A), ("B", B)):
+            arr[f"add_{name}__{tag}_rowPtr"] = M.rowPtr
+            arr[f"add_{name}__{tag}_colInd"] = M.colInd
+            arr[f"add_{name}__{tag}_values"] = M.values
+        meta[f"add_{name}"] = {"a": a, "b": b, "shape": [int(A.nrow), int(A.mcol)]}
+        arr[f"add_{name}__C_rowPtr"], arr[f"add_{name}__C_colInd"] = rp, ci
+        arr[f"add_{name}__C_values"] = va
     np.savez_compressed(os.path.join(HERE, "reference_mult.npz"), **arr)
     with open(os.path.join(HERE, "reference_mult.json"), "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)
-    print("wrote", len(meta) // 2, "MAT::Mult cases")
+    print("wrote", len(mult_cases()), "MAT::Mult and", len(add_cases()), "MAT::Add cases")
 
 
 if __name__ == "__main__":

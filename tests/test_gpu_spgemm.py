@@ -133,3 +133,30 @@ def test_errors(gpu):
     with pytest.raises(capi.FaspError) as e:
         gpu.MAT(P.CSRMatrix(pat.nrow, pat.mcol, pat.rowPtr, pat.colInd, None)).Mult(A)
     assert e.value.code == -12
+
+
+ADD = G.add_cases()
+
+
+@pytest.mark.parametrize("name", sorted(ADD))
+def test_add_matches_reference(gpu, name):
+    a, A, b, B, want = ADD[name]
+    _same(gpu.MAT.Add(a, gpu.MAT(A), b, gpu.MAT(B)), want)
+
+
+def test_add_at_size_against_oracle(gpu, O):
+    A = P.poisson3d(24)
+    rng = np.random.default_rng(11)
+    B = _random(rng, A.nrow, A.mcol, 1, 5)
+    # row 0 of B starts with column 0 (the reference's sort cannot front-load row 0)
+    B.colInd[B.rowPtr[0]] = 0
+    code, want = O.mat_add("port", 0.75, A, -2.5, B)
+    assert code == 0
+    _same(gpu.MAT.Add(0.75, gpu.MAT(A), -2.5, gpu.MAT(B)), want)
+
+
+def test_add_errors(gpu):
+    from faspxx_b200 import capi
+    with pytest.raises(capi.FaspError) as e:
+        gpu.MAT.Add(1.0, gpu.MAT(P.poisson2d(5)), 1.0, gpu.MAT(P.poisson2d(6)))
+    assert e.value.code == -16

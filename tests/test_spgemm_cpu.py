@@ -40,3 +40,25 @@ def test_products_are_unsorted_and_complete():
                 C[i, ci[rp[i]:rp[i + 1]]] = va[rp[i]:rp[i + 1]]
             assert np.allclose(C, dense, rtol=1e-13, atol=1e-12)
     assert unsorted > 0
+
+
+ADD = G.add_cases()
+
+
+@pytest.mark.parametrize("name", sorted(ADD))
+def test_add_restatement_matches_reference(O, name):
+    a, A, b, B, want = ADD[name]
+    code, got = O.mat_add("port", a, A, b, B)
+    assert code == 0
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+
+
+def test_add_fixture_repeats_an_appended_column():
+    """repeated_appends: each row of B is [0, i+7, i+7, i+9, i+7]. Column 0 is appended first
+    and takes the one extra slot MAT::Add searches besides A's entries, so the later repeats
+    of column i+7 find no match and stay separate entries (sorted together)."""
+    a, A, b, B, (rp, ci, va) = ADD["repeated_appends"]
+    row = 20
+    seg = ci[rp[row]:rp[row + 1]]
+    assert np.count_nonzero(seg == row + 7) == 3 and np.count_nonzero(seg == 0) == 1
