@@ -31,8 +31,10 @@ struct GmCtl {
 };
 
 // The preconditioner of a solver: Identity (Iter.cxx:16-20) or Jacobi (Iter.cxx:29-112).
+struct SolverImpl;
+
 struct Pcd {
-    int             type = 0;    // 0 identity, 1 Jacobi
+    int             type = 0;    // 0 identity, 1 Jacobi, 2 MG (one MG solve, prm its SOLParams)
     fasp_gpu_params prm{};
     double          weight = 1.0;
     const Mat*      A = nullptr;
@@ -41,6 +43,7 @@ struct Pcd {
     double*         work = nullptr;
     float*          work32 = nullptr; // FP32 sweeps of mixed-precision inner solves (lazy)
     uint32_t        numIter = 0;
+    SolverImpl*     mg = nullptr;     // type 2: the MG solver it runs (owned)
     bool pure() const { return type == 1 && prm.minIter == prm.maxIter; }
     int  setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p);
     void destroy();

@@ -10,6 +10,8 @@
 #include <limits>
 #include <type_traits>
 
+#include <new>
+
 #include "solver.h"
 
 namespace fb {
@@ -80,8 +82,16 @@ int Pcd::setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p)
     return to32(c, M->nrow, dinv, dinv32);
 }
 
+// type 2 (MG preconditioner): one MG::Solve on the preconditioner's own solver object
+static int pcd_mg_apply(SolverImpl* s, const double* b, double* x);
+static void pcd_mg_free(SolverImpl* s);
+
 void Pcd::destroy()
 {
+    if (mg) {
+        pcd_mg_free(mg);
+        mg = nullptr;
+    }
     cudaFree(dinv);
     cudaFree(dinv32);
     cudaFree(work);
@@ -99,6 +109,12 @@ int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm
 {
     const uint32_t n = A->nrow;
     if (type == 0) return v_copy(c, n, b, x);
+    if (type == 2) {
+        if constexpr (std::is_same<T, float>::value)
+            return kErrPcdType; // FP32 inner solves have no MG preconditioner
+        else
+            return pcd_mg_apply(mg, b, x);
+    }
     T* work;
     const T* dinv;
     if constexpr (std::is_same<T, float>::value) {
@@ -200,8 +216,28 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
         FB_CUDA(cudaStreamSynchronize(c.stream));
         return kOk;
     }
-    if (cfg.pcd != 0 && cfg.pcd != 1) return kErrPcdType;
-    if ((e = pcd.setup(c, A, cfg.pcd, cfg.pcdWeight, cfg.pcdPrm))) return e;
+    if (cfg.pcd < 0 || cfg.pcd > 2) return kErrPcdType;
+    if (cfg.pcd == 2) {
+        // MG as the preconditioner (SOL::SetupPCD with an MG object, SOL.cxx:249): an MG
+        // solver on the same matrix and stream, with this solver's MG settings and the
+        // preconditioner's SOLParams (pcdPrm), transfers included when set
+        if (cfg.precision != FASP_GPU_FP64) return kErrPcdType;
+        SolverImpl* m = new (std::nothrow) SolverImpl();
+        if (!m) return kErrAlloc;
+        m->cfg = cfg;
+        m->cfg.alg = FASP_GPU_MG;
+        m->cfg.prm = cfg.pcdPrm;
+        m->cfg.pcd = 0;
+        m->c = c; // shares the stream and reduction scratch (never destroyed by m)
+        m->mgIn = mgIn;
+        pcd.type = 2;
+        pcd.A = A;
+        pcd.prm = cfg.pcdPrm;
+        pcd.mg = m;
+        if ((e = m->setup(Mh))) return e;
+    } else if ((e = pcd.setup(c, A, cfg.pcd, cfg.pcdWeight, cfg.pcdPrm))) {
+        return e;
+    }
     switch (alg) {
         case FASP_GPU_CG: {
             if ((e = alloc_vecs(w, 5, n))) return e; // rk pk zk ax safe
@@ -1810,6 +1846,18 @@ void SolverImpl::mg_cycle(const double* b, double* x)
     } else {
         v_copy(c, n, b, x);
     }
+}
+
+static int pcd_mg_apply(SolverImpl* s, const double* b, double* x)
+{
+    fasp_gpu_info info{};
+    return s->mg(b, x, &info);
+}
+
+static void pcd_mg_free(SolverImpl* s)
+{
+    s->destroy();
+    delete s;
 }
 
 // ---- MG with transfer operators (no reference counterpart) -------------------------------

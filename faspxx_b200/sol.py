@@ -335,6 +335,18 @@ class SOL:
                                           pc.cfg.prm.relTol, pc.cfg.prm.absTol)
         elif isinstance(pc, Identity):
             self.cfg.pcd = 0
+        elif isinstance(pc, MG):
+            # MG as the preconditioner: its SOLParams, levels, cycles, smoother and coarse
+            # solver settings and transfer operators
+            self.cfg.pcd = 2
+            p = pc.cfg.prm
+            self.cfg.pcdPrm = capi.Params(p.maxIter, p.minIter, p.savIter, p.restart, p.relTol,
+                                          p.absTol)
+            for f in ("mgLevels", "mgCycles", "mgSmoothWeight", "mgCoarseWeight",
+                      "mgSmoothPrm", "mgCoarsePrm"):
+                setattr(self.cfg, f, getattr(pc.cfg, f))
+            self.transfers = dict(getattr(pc, "transfers", {}))
+            self._built = None
         else:
             raise capi.FaspError(-31, "SetupPCD")
 
@@ -533,6 +545,22 @@ def configure(alg: str, maxIter=1, minIter=0, savIter=100000, restart=30, relTol
                         setattr(s.cfg, name + "Weight", v)
                     else:
                         setattr(prm, k, v)
+    if pcd == "mg":
+        m = MG()
+        m.cfg.mgLevels, m.cfg.mgCycles = mgLevels, mgCycles
+        for name, spec in (("mgSmooth", mgSmooth), ("mgCoarse", mgCoarse)):
+            if spec:
+                prm = getattr(m.cfg, name + "Prm")
+                for k, v in spec.items():
+                    if k == "weight":
+                        setattr(m.cfg, name + "Weight", v)
+                    else:
+                        setattr(prm, k, v)
+        m.SetMaxIter(pcdIter)
+        m.SetMinIter(pcdIter if pcdMinIter is None else pcdMinIter)
+        m.SetRelTol(pcdRelTol)
+        m.SetAbsTol(pcdAbsTol)
+        s.SetupPCD(m)
     if pcd == "jacobi":
         p = Jacobi(pcdWeight)
         p.SetMaxIter(pcdIter)

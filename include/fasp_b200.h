@@ -66,7 +66,9 @@ typedef struct {
     fasp_gpu_params prm;        /* SOL::Set{Max,Min,Sav}Iter, SetRestart, SetRelTol, ... */
     double          weight;     /* Jacobi::SetWeight when alg == FASP_GPU_JACOBI */
     uint32_t        maxRestart, minRestart; /* GMRES/FGMRES::SetMaxMinRestart; 0,0 = 30,10 */
-    int             pcd;        /* preconditioner: 0 Identity, 1 Jacobi */
+    int             pcd;        /* preconditioner: 0 Identity, 1 Jacobi, 2 MG (an MG solve with
+                                   SOLParams pcdPrm and the mg* settings below, plus any
+                                   fasp_gpu_solver_set_mg_transfer levels; FP64 only) */
     double          pcdWeight;  /* its Jacobi weight */
     fasp_gpu_params pcdPrm;     /* its SOLParams (maxIter = minIter = sweeps in the examples) */
     uint32_t        mgLevels, mgCycles; /* MG::SetupALL levels, MG::SetNumCycles */
@@ -257,7 +259,7 @@ int fasp_gpu_solver_setup(fasp_gpu_solver s, fasp_gpu_mat A);
  * stores one operator as both restriction and prolongation, MG.cxx:42-43, and every level's
  * residual uses the top-level matrix, MG.cxx:119, so only identity transfers work there).
  * Call before fasp_gpu_solver_setup for every coarse level l = 0 .. mgLevels - 1 (level 0
- * is the Setup matrix): P = prolongation from level l+1 to level l (n_l x n_{l+1}); R =
+ * is the Setup matrix; with pcd = 2 the levels belong to the MG preconditioner): P = prolongation from level l+1 to level l (n_l x n_{l+1}); R =
  * restriction (n_{l+1} x n_l), NULL for the exact transpose of P; Ac = the level-(l+1)
  * operator, NULL for the Galerkin product R (A_l P) formed with MAT::Mult on the GPU. The
  * cycle is the reference's (pre-smoothing, residual, restriction, coarse solve or the next

@@ -1166,6 +1166,32 @@ static void gmres_setup(osol_t* s, uint32_t maxR, uint32_t minR, int flexible)
         s->restart = s->minRestart;
 }
 
+/* MG::SetupALL (MG.cxx:54-79) + SetupLevel (:26-51) as in TestMG.cxx:80-97: identity
+ * transfers, Jacobi smoothers and coarse solvers; prm = the MG object's SOLParams. */
+static osol_t* new_mg(const orc_config_t* cfg, const orc_params_t* prm, const omat_t* M)
+{
+    const uint32_t n = M->mcol;
+    osol_t* s = new_sol(ORC_MG, prm, M);
+    const uint32_t L = cfg->mgLevels;
+    s->numLevels = L;
+    s->mgr = dalloc(n);
+    if (L) {
+        s->numCycles = (uint32_t*)calloc(L, sizeof(uint32_t));
+        s->smoothers = (osol_t**)calloc(L, sizeof(osol_t*));
+        s->coarse = (osol_t**)calloc(L, sizeof(osol_t*));
+        s->lb = (double**)calloc(L, sizeof(double*));
+        s->lx = (double**)calloc(L, sizeof(double*));
+        for (uint32_t l = 0; l < L; ++l) {
+            s->numCycles[l] = cfg->mgCycles;
+            s->smoothers[l] = new_jacobi(&cfg->mgSmoothPrm, cfg->mgSmoothWeight, M);
+            s->coarse[l] = new_jacobi(&cfg->mgCoarsePrm, cfg->mgCoarseWeight, M);
+            s->lb[l] = dalloc(n);
+            s->lx[l] = dalloc(n);
+        }
+    }
+    return s;
+}
+
 void* orc_create(const orc_config_t* cfg, uint32_t nrow, uint32_t mcol, uint32_t nnz,
                  const uint32_t* rowPtr, const uint32_t* colInd, const double* values)
 {
@@ -1189,6 +1215,8 @@ void* orc_create(const orc_config_t* cfg, uint32_t nrow, uint32_t mcol, uint32_t
     const uint32_t n = mcol;
     if (cfg->pcd == 1)
         h->pcd = new_jacobi(&cfg->pcdPrm, cfg->pcdWeight, M);
+    else if (cfg->pcd == 2) /* an MG object as the preconditioner (SOL::SetupPCD) */
+        h->pcd = new_mg(cfg, &cfg->pcdPrm, M);
     else
         h->pcd = new_sol(ORC_IDENTITY, &cfg->pcdPrm, M);
 
@@ -1222,28 +1250,9 @@ void* orc_create(const orc_config_t* cfg, uint32_t nrow, uint32_t mcol, uint32_t
         case ORC_JACOBI:
             s = new_jacobi(&cfg->prm, cfg->weight, M);
             break;
-        case ORC_MG: {
-            /* MG::SetupALL (MG.cxx:54-79) + SetupLevel (:26-51) as in TestMG.cxx:80-97 */
-            s = new_sol(ORC_MG, &cfg->prm, M);
-            const uint32_t L = cfg->mgLevels;
-            s->numLevels = L;
-            s->mgr = dalloc(n);
-            if (L) {
-                s->numCycles = (uint32_t*)calloc(L, sizeof(uint32_t));
-                s->smoothers = (osol_t**)calloc(L, sizeof(osol_t*));
-                s->coarse = (osol_t**)calloc(L, sizeof(osol_t*));
-                s->lb = (double**)calloc(L, sizeof(double*));
-                s->lx = (double**)calloc(L, sizeof(double*));
-                for (uint32_t l = 0; l < L; ++l) {
-                    s->numCycles[l] = cfg->mgCycles;
-                    s->smoothers[l] = new_jacobi(&cfg->mgSmoothPrm, cfg->mgSmoothWeight, M);
-                    s->coarse[l] = new_jacobi(&cfg->mgCoarsePrm, cfg->mgCoarseWeight, M);
-                    s->lb[l] = dalloc(n);
-                    s->lx[l] = dalloc(n);
-                }
-            }
+        case ORC_MG:
+            s = new_mg(cfg, &cfg->prm, M);
             break;
-        }
         default:
             break;
     }
@@ -1399,6 +1408,7 @@ int orc_mg_set_level(void* hv, uint32_t level,
 {
     ohandle_t* h = (ohandle_t*)hv;
     osol_t* s = h ? h->sol : NULL;
+    if (s && s->alg != ORC_MG) s = h->pcd; /* the MG preconditioner of a Krylov solver */
     if (!s || s->alg != ORC_MG || level >= s->numLevels) return ERROR_INPUT_PAR;
     const uint32_t L = s->numLevels;
     if (!s->lP) {

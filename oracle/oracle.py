@@ -117,7 +117,7 @@ def make_config(lib, alg: str, maxIter=1, minIter=0, savIter=100000, restart=30,
     cfg.prm.restart, cfg.prm.relTol, cfg.prm.absTol = restart, relTol, absTol
     cfg.weight = weight
     cfg.maxRestart, cfg.minRestart = maxRestart, minRestart
-    cfg.pcd = 1 if pcd == "jacobi" else 0
+    cfg.pcd = {"jacobi": 1, "mg": 2}.get(pcd, 0)
     cfg.pcdWeight = pcdWeight
     cfg.pcdPrm.maxIter = pcdIter
     cfg.pcdPrm.minIter = pcdIter if pcdMinIter is None else pcdMinIter
