@@ -874,6 +874,100 @@ def run_matfree(args):
     return 0
 
 
+def _interp_trilinear(nf: int):
+    """Trilinear prolongation from the ((nf-1)/2)^3 grid to nf^3 (x fastest), as CSR arrays."""
+    import scipy.sparse as sp
+    nc = (nf - 1) // 2
+    rows, cols, vals = [], [], []
+    for i in range(nf):
+        if i % 2 == 1:
+            rows.append(i), cols.append((i - 1) // 2), vals.append(1.0)
+        else:
+            if i // 2 - 1 >= 0:
+                rows.append(i), cols.append(i // 2 - 1), vals.append(0.5)
+            if i // 2 < nc:
+                rows.append(i), cols.append(i // 2), vals.append(0.5)
+    p1 = sp.csr_matrix((vals, (rows, cols)), shape=(nf, nc))
+    p3 = sp.kron(p1, sp.kron(p1, p1, format="csr"), format="csr")
+    p3.sort_indices()
+    return p3
+
+
+def run_mg(args):
+    """Geometric multigrid on the 3D 7-point Poisson matrix at 127^3 (n = 2,048,383): the
+    headline's system at the nearest size that coarsens to a point (127 -> 63 -> 31 -> 15 ->
+    7 -> 3), trilinear prolongation, restriction = its transpose and Galerkin coarse
+    operators formed on the GPU (MAT::Mult), Jacobi V(2,2) cycles with 40 sweeps on 3^3.
+    Reported: the setup (transposes and Galerkin products), MG-preconditioned CG and plain MG
+    to rtol 1e-8, against Jacobi-PCG in FP64 and in mixed precision on the same system."""
+    from faspxx_b200 import capi, problems as P, sol
+    capi.init(0)
+    nf = 127
+    A = P.poisson3d(nf)
+    xs = P.seeded_uniform(A.nrow, 42)
+    b = A.matvec(xs)
+    M = sol.MAT(A)
+    Ps, keep = [], []
+    f = nf
+    t0 = time.perf_counter()
+    while f > 3:
+        p3 = _interp_trilinear(f)
+        Ps.append(sol.MAT(P.CSRMatrix(p3.shape[0], p3.shape[1], p3.indptr.astype(np.uint32),
+                                      p3.indices.astype(np.uint32), p3.data.astype(np.float64))))
+        f = (f - 1) // 2
+    build_s = time.perf_counter() - t0
+    L = len(Ps)
+    mgkw = dict(mgLevels=L, mgCycles=1, mgSmooth=dict(maxIter=2, minIter=2, weight=2.0 / 3.0),
+                mgCoarse=dict(maxIter=40, minIter=40, weight=2.0 / 3.0))
+    db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
+    flush = sol.DVec(32 << 20)
+    res = {}
+    configs = [("mg_pcg", sol.configure("cg", maxIter=200, relTol=1e-8, absTol=0.0, pcd="mg",
+                                        pcdIter=1, **mgkw)),
+               ("mg", sol.configure("mg", maxIter=200, relTol=1e-8, absTol=0.0, **mgkw)),
+               ("jacobi_pcg_fp64", sol.configure("cg", maxIter=2000, relTol=1e-8, absTol=0.0,
+                                                 pcd="jacobi", pcdIter=1)),
+               ("jacobi_pcg_mixed", sol.configure("cg", maxIter=2000, relTol=1e-8, absTol=0.0,
+                                                  pcd="jacobi", pcdIter=1))]
+    configs[3][1].SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-2)
+    for name, s in configs:
+        if name.startswith("mg"):
+            s.transfers = {l: (Ps[l], None, None) for l in range(L)}
+        lib = capi.lib
+        lib.fasp_gpu_synchronize()
+        t0 = time.perf_counter()
+        s.Setup(M)
+        lib.fasp_gpu_synchronize()
+        setup_ms = (time.perf_counter() - t0) * 1e3
+        ms, code = _time_solve(s, db, dx, args.steps, flush=flush)
+        x = dx.numpy()
+        res[name] = {"ms": round(ms, 3), "setup_ms": round(setup_ms, 1), "code": code,
+                     "iters": s.GetIterations(),
+                     "rel_residual": float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b))}
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        kind = "ref" if os.path.exists(O.REF_SO) else "port"
+        per_iter, _ = reference_sample(A, b, args.ref_sample, kind)
+        cpu = {"value": round(per_iter * res["jacobi_pcg_fp64"]["iters"], 1), "unit": "ms",
+               "cores": 1, "kind": "reference" if kind == "ref" else "port",
+               "sample": f"{args.ref_sample} Jacobi-PCG iterations of the reference on this "
+                         "system, scaled by the FP64 iteration count (the reference's MG "
+                         "cannot use transfer operators)"}
+    line = {"metric": "Time to rtol 1e-8, 3D Poisson 127^3: MG-preconditioned CG (V(2,2), "
+                      "Galerkin hierarchy formed on the GPU)",
+            "value": res["mg_pcg"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": 2, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D 7-point 127^3 (n=2048383), b=A x*, x*~U[0,1), x0=0; "
+                                   f"{L} coarse levels, trilinear P, R = P^T, Galerkin "
+                                   "R A P, Jacobi 2/3 V(2,2), 40 sweeps on 3^3",
+                       "l2": "L2 flushed between timed solves",
+                       "prolongations_built_on_host_s": round(build_s, 2)},
+            "results": res, "cpu_baseline": cpu}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -892,7 +986,8 @@ def main():
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
                          "one 60-iteration BiCGStab and GMRES(30) solve (krylov96)")
     ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",
-                                           "pcg2d256", "matfree"], default="poisson128")
+                                           "pcg2d256", "matfree", "mg127"],
+                    default="poisson128")
     ap.add_argument("--fd-dirs", type=int, default=32)
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--batch-sample", type=int, default=256)
@@ -910,6 +1005,8 @@ def main():
         return run_pcg2d(args)
     if args.workload == "matfree":
         return run_matfree(args)
+    if args.workload == "mg127":
+        return run_mg(args)
     return run_ours(args)
 
 

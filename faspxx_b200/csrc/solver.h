@@ -102,6 +102,16 @@ struct SolverImpl {
     std::vector<double*>     mgRes;
     int  mg_setup_transfers();
     void mg_cycle_transfer(const double* b, double* x);
+    // MG as a preconditioner: when no step of its solve reads a norm on the host (minIter =
+    // maxIter for the MG object, its smoothers and its coarse solver), the whole solve is a
+    // fixed kernel sequence; it is captured once per (b, x) pair and replayed as a graph
+    struct MgGraph {
+        const double*   b;
+        double*         x;
+        cudaGraphExec_t exec;
+    };
+    std::vector<MgGraph> mgGraphs;
+    bool capturing = false;
     // device-driven CG
     CGEngine<double>* cg64 = nullptr;
     CGEngine<float>*  cg32 = nullptr;

@@ -1851,11 +1851,39 @@ void SolverImpl::mg_cycle(const double* b, double* x)
 static int pcd_mg_apply(SolverImpl* s, const double* b, double* x)
 {
     fasp_gpu_info info{};
-    return s->mg(b, x, &info);
+    const fasp_gpu_config& k = s->cfg;
+    const bool fixed = k.prm.minIter == k.prm.maxIter && k.mgSmoothPrm.minIter == k.mgSmoothPrm.maxIter &&
+                       k.mgCoarsePrm.minIter == k.mgCoarsePrm.maxIter;
+    if (!fixed) return s->mg(b, x, &info);
+    for (const auto& g : s->mgGraphs)
+        if (g.b == b && g.x == x) {
+            FB_CUDA(cudaGraphLaunch(g.exec, s->c.stream));
+            return kOk;
+        }
+    cudaStream_t st = s->c.stream;
+    FB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    s->capturing = true;
+    const int e = s->mg(b, x, &info);
+    s->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (!e && ce == cudaSuccess && graph &&
+        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        s->mgGraphs.push_back({b, x, exec});
+        FB_CUDA(cudaGraphLaunch(exec, st));
+        return kOk;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return e ? e : kErrCuda;
 }
 
 static void pcd_mg_free(SolverImpl* s)
 {
+    for (auto& g : s->mgGraphs) cudaGraphExecDestroy(g.exec);
+    s->mgGraphs.clear();
     s->destroy();
     delete s;
 }
@@ -1991,7 +2019,7 @@ int SolverImpl::mg(const double* b, double* x, fasp_gpu_info* info)
         info->normInf = fetch(d + SL_T2);
         rec(numIter, resAbs);
     }
-    FB_CUDA(cudaStreamSynchronize(c.stream));
+    if (!capturing) FB_CUDA(cudaStreamSynchronize(c.stream));
     return kOk;
 }
 
