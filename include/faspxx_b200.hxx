@@ -10,8 +10,11 @@
  *   LOP    linear operator base (src/LOP.hxx:22-66)
  *   MAT    CSRx matrix (src/MAT.hxx:39-213), uploaded once at construction
  *   SOL    solver base (src/SOL.hxx:24-126) with SOLParams setters and getters
- *   CG, BiCGStab, GMRES, FGMRES, Jacobi, Identity, MG<MAT>   (src/*.hxx)
+ *   CG, BiCGStab, GMRES, FGMRES, Jacobi, Identity, MG<MAT>   (src/CG.hxx and the others)
  *   Krylov(A, b, x, pcd, params)                             (src/Krylov.cxx:16-53)
+ *   ReadMat(file, MAT&)                                      (src/ReadData.cxx:361-446)
+ *   StencilLOP  matrix-free grid operator, the GPU form of a user LOP such as the one of
+ *               example/TestMatFree.cxx:26-176 (no reference class of this name)
  *
  * Differences a caller sees: operators must be MAT (a host-side user LOP cannot be applied
  * on the GPU, so Setup returns ERROR_SOLVER_TYPE for it); Solve blocks until the device is
@@ -23,7 +26,9 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdint>
+#include <fstream>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "fasp_b200.h"
@@ -118,6 +123,14 @@ class MAT : public LOP {
     fasp_gpu_mat h_ = nullptr;
     USI          nnz_ = 0;
     int          err_ = 0;
+    void adopt(int e, fasp_gpu_mat h)
+    {
+        err_ = e;
+        if (e) return;
+        if (h_) fasp_gpu_mat_destroy(h_);
+        h_ = h;
+        fasp_gpu_mat_info(h_, &nrow, &mcol, &nnz_);
+    }
     void create(USI n, USI m, USI nnz, const DBL* v, const USI* ci, const USI* rp)
     {
         nrow = n; mcol = m; nnz_ = nnz;
@@ -158,6 +171,39 @@ public:
     /* B200 option: matrix form of the SpMV kernels, 0 CSR, 1 row classes, 2 row classes
      * with stencil masks (bit-identical results; set before a solver's Setup) */
     void SetRowClass(int mode) { fasp_gpu_mat_set_rowclass(h_, mode); }
+    /* MAT::Mult (MAT.cxx:715-800): *this = matl * matr, formed on the GPU */
+    void Mult(const MAT& matl, const MAT& matr)
+    {
+        fasp_gpu_mat h = nullptr;
+        const int e = fasp_gpu_mat_mult(matl.h_, matr.h_, &h);
+        adopt(e, h);
+    }
+    /* MAT::Add (MAT.cxx:652-713): *this = a * mat1 + b * mat2, formed on the GPU */
+    void Add(const DBL a, const MAT& mat1, const DBL b, const MAT& mat2)
+    {
+        fasp_gpu_mat h = nullptr;
+        const int e = fasp_gpu_mat_add(a, mat1.h_, b, mat2.h_, &h);
+        adopt(e, h);
+    }
+    /* MTXtoMAT / ReadCSR's conversions on the GPU from the readers' arrays (see ReadMat) */
+    int FromCOO(USI n, USI m, const std::vector<USI>& rowInd, const std::vector<USI>& colInd,
+                const std::vector<DBL>& values)
+    {
+        fasp_gpu_mat h = nullptr;
+        const int e = fasp_gpu_mat_create_coo(n, m, (USI)values.size(), rowInd.data(),
+                                              colInd.data(), values.data(), 0, &h);
+        adopt(e, h);
+        return e;
+    }
+    int FromCSRRaw(USI n, const std::vector<USI>& rowPtr, const std::vector<USI>& colInd,
+                   const std::vector<DBL>& values)
+    {
+        fasp_gpu_mat h = nullptr;
+        const int e = fasp_gpu_mat_create_csr_raw(n, n, (USI)values.size(), rowPtr.data(),
+                                                  colInd.data(), values.data(), 0, &h);
+        adopt(e, h);
+        return e;
+    }
     /* MAT::TransInPlace (MAT.cxx:479-538) */
     void TransInPlace()
     {
@@ -170,6 +216,73 @@ public:
     }
 };
 
+/* Matrix-free operator on an nx x ny x nz grid (nz = 1: 2D, ny = nz = 1: 1D): a
+ * constant-coefficient stencil of up to 16 points (dx, dy, dz in -3..3) truncated at the
+ * faces, row ix + nx (iy + ny iz), nothing stored -- what a user LOP like the one of
+ * example/TestMatFree.cxx computes, in a form the GPU applies (fasp_gpu_mat_create_stencil). */
+class StencilLOP : public LOP {
+    fasp_gpu_mat h_ = nullptr;
+    int          err_ = 0;
+public:
+    StencilLOP(USI nx, USI ny, USI nz, const std::vector<int32_t>& dx,
+               const std::vector<int32_t>& dy, const std::vector<int32_t>& dz,
+               const std::vector<DBL>& coef)
+    {
+        nrow = mcol = nx * ny * nz;
+        err_ = fasp_gpu_mat_create_stencil(nx, ny, nz, (USI)coef.size(), dx.data(), dy.data(),
+                                           dz.data(), coef.data(), &h_);
+    }
+    StencilLOP(const StencilLOP&) = delete;
+    StencilLOP& operator=(const StencilLOP&) = delete;
+    ~StencilLOP() override { if (h_) fasp_gpu_mat_destroy(h_); }
+    int Status() const { return err_; }
+    fasp_gpu_mat Device() const override { return h_; }
+    void Apply(const DVEC& v, DVEC& w) const { fasp_gpu_mat_apply(h_, v.data(), w.data()); }
+};
+
+/* ReadMat (src/ReadData.cxx:361-446): a .csr or .mtx file by its extension. The text is
+ * read here on the host as ReadCSR / ReadMTX read it; the conversions (the 1-based shift,
+ * the row sorts, the zero diagonals) run on the GPU. */
+inline FaspRetCode ReadMat(const char* fileName, MAT& dst)
+{
+    const std::string f(fileName);
+    if (f.size() <= 4) return ERROR_INPUT_FILE;
+    std::string ext = f.substr(f.size() - 3);
+    for (char& ch : ext) ch = (char)std::tolower((unsigned char)ch);
+    std::ifstream in(fileName);
+    if (!in.is_open()) return ERROR_OPEN_FILE;
+    if (ext == "csr") {
+        USI n = 0;
+        if (!(in >> n) || n == 0) return ERROR_INPUT_PAR;
+        std::vector<USI> rp(n + 1);
+        for (auto& v : rp)
+            if (!(in >> v)) return ERROR_INPUT_FILE;
+        const USI nnz = rp[n] - rp[0];
+        std::vector<USI> ci(nnz);
+        std::vector<DBL> va(nnz);
+        for (auto& v : ci)
+            if (!(in >> v)) return ERROR_INPUT_FILE;
+        for (auto& v : va)
+            if (!(in >> v)) return ERROR_INPUT_FILE;
+        return (FaspRetCode)dst.FromCSRRaw(n, rp, ci, va);
+    }
+    if (ext == "mtx") {
+        std::string line;
+        while (in.peek() == '%' && std::getline(in, line)) {}
+        USI n = 0, m = 0, nnz = 0;
+        if (!(in >> n >> m >> nnz)) return ERROR_INPUT_FILE;
+        std::vector<USI> ri(nnz), ci(nnz);
+        std::vector<DBL> va(nnz);
+        for (USI k = 0; k < nnz; ++k) {
+            if (!(in >> ri[k] >> ci[k] >> va[k])) return ERROR_INPUT_FILE;
+            --ri[k];
+            --ci[k];
+        }
+        return (FaspRetCode)dst.FromCOO(n, m, ri, ci, va);
+    }
+    return ERROR_INPUT_FILE;
+}
+
 /* Solver base (src/SOL.hxx:24-126). */
 class SOL {
 protected:
@@ -178,7 +291,10 @@ protected:
     fasp_gpu_solver h_ = nullptr;
     fasp_gpu_info   info_{};
     bool            dirty_ = true;
+    const SOL*      pcdObj_ = nullptr; /* the preconditioner object given to SetupPCD */
     explicit SOL(int alg) { fasp_gpu_default_config(&cfg_, alg); info_.norm2 = info_.normInf = 1e60; }
+    /* MG transfer levels of this solver, or of the MG object that preconditions it */
+    virtual int SetTransfers(fasp_gpu_solver) const { return SUCCESS; }
     int build()
     {
         if (!A || !A->Device()) return ERROR_SOLVER_TYPE;
@@ -186,6 +302,8 @@ protected:
         if (h_) fasp_gpu_solver_destroy(h_);
         h_ = nullptr;
         int e = fasp_gpu_solver_create(&cfg_, &h_);
+        if (!e) e = SetTransfers(h_);
+        if (!e && pcdObj_) e = pcdObj_->SetTransfers(h_);
         if (!e) e = fasp_gpu_solver_setup(h_, A->Device());
         dirty_ = e != 0;
         return e;
@@ -210,8 +328,13 @@ public:
     void SetOverlapLaunch(bool on) { cfg_.overlapLaunch = on ? 1 : 0; dirty_ = true; }
     void SetFP32Recurrence(bool on) { cfg_.fp32Recurrence = on ? 1 : 0; dirty_ = true; }
     const fasp_gpu_config& Config() const { return cfg_; }
-    /* SOL::SetupPCD (SOL.cxx:249): Identity or Jacobi */
-    virtual void SetupPCD(SOL& pc) { pc.AsPreconditionerOf(cfg_); dirty_ = true; }
+    /* SOL::SetupPCD (SOL.cxx:249): Identity, Jacobi or MG */
+    virtual void SetupPCD(SOL& pc)
+    {
+        pc.AsPreconditionerOf(cfg_);
+        pcdObj_ = &pc;
+        dirty_ = true;
+    }
     virtual void AsPreconditionerOf(fasp_gpu_config& c) const { c.pcd = 0; }
     virtual FaspRetCode Setup(const LOP& op)
     {
@@ -277,6 +400,7 @@ public:
     Jacobi() : SOL(FASP_GPU_JACOBI) {}
     explicit Jacobi(DBL weight) : SOL(FASP_GPU_JACOBI) { cfg_.weight = weight; }
     void SetWeight(const DBL w) { cfg_.weight = w; dirty_ = true; }
+    using SOL::Setup;
     FaspRetCode Setup(const MAT& M) { return SOL::Setup(M); }
     void AsPreconditionerOf(fasp_gpu_config& c) const override
     {
@@ -286,11 +410,53 @@ public:
     }
 };
 
-/* Abstract MG with identity transfers and Jacobi level solvers (src/MG.hxx:44-106). */
+/* Abstract MG with identity transfers and Jacobi level solvers (src/MG.hxx:44-106), or,
+ * with SetTransfer for every coarse level, MG with restriction/prolongation operators and
+ * per-level operators (B200; fasp_gpu_solver_set_mg_transfer). As the preconditioner of a
+ * Krylov solver (SetupPCD) it runs one MG solve with its own SOLParams. */
 template <class TTT>
 class MG : public SOL {
+    struct Level {
+        const MAT* P;
+        const MAT* R;
+        const MAT* Ac;
+    };
+    std::vector<Level> levels_;
+    int SetTransfers(fasp_gpu_solver h) const override
+    {
+        for (size_t l = 0; l < levels_.size(); ++l) {
+            const Level& v = levels_[l];
+            if (!v.P) continue;
+            const int e = fasp_gpu_solver_set_mg_transfer(h, (uint32_t)l, v.P->Device(),
+                                                          v.R ? v.R->Device() : nullptr,
+                                                          v.Ac ? v.Ac->Device() : nullptr);
+            if (e) return e;
+        }
+        return SUCCESS;
+    }
 public:
     MG() : SOL(FASP_GPU_MG) {}
+    /* level `level` (0 = finest): prolongation P from level+1, restriction R (nullptr: the
+     * transpose of P), coarse operator Ac (nullptr: the Galerkin product R A P) */
+    void SetTransfer(USI level, const MAT& P, const MAT* R = nullptr, const MAT* Ac = nullptr)
+    {
+        if (levels_.size() <= level) levels_.resize(level + 1, Level{nullptr, nullptr, nullptr});
+        levels_[level] = Level{&P, R, Ac};
+        dirty_ = true;
+    }
+    void AsPreconditionerOf(fasp_gpu_config& c) const override
+    {
+        c.pcd = 2;
+        c.pcdPrm = cfg_.prm;
+        c.mgLevels = cfg_.mgLevels;
+        c.mgCycles = cfg_.mgCycles;
+        c.mgSmoothWeight = cfg_.mgSmoothWeight;
+        c.mgSmoothPrm = cfg_.mgSmoothPrm;
+        c.mgCoarseWeight = cfg_.mgCoarseWeight;
+        c.mgCoarsePrm = cfg_.mgCoarsePrm;
+    }
+    /* the numLevels of SetupALL without binding a matrix (for a preconditioner) */
+    void SetNumLevels(USI numLevels) { cfg_.mgLevels = numLevels; dirty_ = true; }
     FaspRetCode SetupALL(const TTT& M, const USI numLevels)
     {
         cfg_.mgLevels = numLevels;

@@ -45,3 +45,34 @@ def test_driver_runs_on_gpu():
     for name, code, err in rows[1:]:
         assert code == "0", name
         assert float(err) < 1e-5, (name, err)
+
+
+FEATURES = os.path.join(ROOT, "faspxx_b200", "examples", "test_features.cxx")
+
+
+def _compile_features(out):
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", f"-I{INC}", FEATURES, "-o", out,
+                    f"-L{LIBDIR}", "-l:libfasp_b200.so", f"-Wl,-rpath,{LIBDIR}"], check=True)
+
+
+def test_feature_driver_compiles():
+    with tempfile.TemporaryDirectory() as d:
+        _compile_features(os.path.join(d, "f"))
+
+
+@pytest.mark.gpu
+def test_feature_driver_runs_on_gpu():
+    """StencilLOP (the matrix-free example at dim 64: 121 CG iterations and the L2 error the
+    reference prints, 1.0041e-04), MAT::Mult/Add, ReadMat of a MatrixMarket file, and
+    MG-preconditioned CG through the façade."""
+    with tempfile.TemporaryDirectory() as d:
+        exe = os.path.join(d, "f")
+        _compile_features(exe)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True, cwd=d).stdout
+    r = {l.split()[0]: l.split()[1:] for l in out.strip().splitlines()}
+    assert r["matfree_cg"][0] == "0" and abs(int(r["matfree_cg"][1]) - 121) <= 1
+    assert abs(float(r["matfree_cg"][2]) - 1.0041e-04) <= 2e-8
+    assert r["mult"] == ["0", "352", "36"]  # the 13-point square of the 5-point stencil
+    assert r["add"] == ["0", "156", "36"]   # 2A - A keeps A's pattern
+    assert r["readmat"] == ["0", "3", "5"]  # every row has its diagonal: nothing inserted
+    assert r["mg_pcg"][0] == "0" and int(r["mg_pcg"][1]) <= 12
