@@ -330,6 +330,23 @@ struct V16<double> {
     enum { W = 2 };
 };
 
+// Component j of a float4 (j a constant after unrolling).
+__device__ __forceinline__ float f4c(const float4& v, int j)
+{
+    return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+
+// Elements s .. s+3 of the eight-element run (a, b); s is the same on every thread.
+__device__ __forceinline__ float4 f4shift(const float4& a, const float4& b, int s)
+{
+    switch (s) {
+        case 0: return a;
+        case 1: return make_float4(a.y, a.z, a.w, b.x);
+        case 2: return make_float4(a.z, a.w, b.x, b.y);
+        default: return make_float4(a.w, b.x, b.y, b.z);
+    }
+}
+
 // REC = 0: q = A p with p = z + beta p_old formed on the fly for every gathered entry (the
 // reference's order: XPAY, then Apply); p is double-buffered.
 // REC = 2: REC = 1 with one reduction per iteration (CGCtl::onered; z is r or zc r).
@@ -339,8 +356,11 @@ struct V16<double> {
 // the FP64 refreshes of reliable updates correct the residual it feeds.
 // Blocks per SM: FP32 6 (40 registers), one-reduction FP32 5 (its extra sums spill under
 // 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4.
-template <typename T, int L, int REC, int JZ>
-__global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC == 2 ? 5 : 6) : 5)))
+// V4 (FP32 recurrences on stencil masks of at most 8 offsets): four consecutive rows per
+// thread with 16-byte loads; the host checks n % 4 == 0, a square matrix and 16-byte
+// aligned vectors (8-byte aligned masks).
+template <typename T, int L, int REC, int JZ, bool V4 = false>
+__global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4 ? (REC == 2 ? 5 : 6) : 5))))
     cg_spmv(CSRView<T> A,
                                                                      const T* __restrict__ z,
                                                   T* P0, T* P1, T* __restrict__ q, T* x,
@@ -350,9 +370,17 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC ==
     constexpr bool ONE = REC == 2;
     pdl_wait();
     pdl_release();
-    if (c->status != kRun) {
+    // every control field of the launch, loaded together ahead of the status test (one
+    // round trip to L2 instead of two dependent ones)
+    const int status = c->status;
+    const int mode = c->pmode, par = c->par;
+    const bool xpend = REC && c->xpend;
+    const T alphaPrev = (T)c->alpha;
+    const T zc = (T)c->zc;
+    const T beta = (T)c->beta;
+    if (status != kRun) {
         if constexpr (std::is_same<T, float>::value) {
-            if (c->status == kRefresh) {
+            if (status == kRefresh) {
                 if constexpr (ONE) // the cg_update slot folded x: the FP64 residual comes here
                     cg_refresh_residual<JZ>(refresh_view(A),
                                             const_cast<T*>(z), nullptr, nullptr, c, s);
@@ -362,13 +390,8 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC ==
         }
         return;
     }
-    const int mode = c->pmode, par = c->par;
-    const bool xpend = REC && c->xpend;
-    const T alphaPrev = (T)c->alpha;
-    const T zc = (T)c->zc;
     // JZ = 2: z = zc r is formed here from r (passed as z), never stored
     auto zat = [&](size_t j) { return JZ == 2 ? zc * z[j] : z[j]; };
-    const T beta = (T)c->beta;
     const T* __restrict__ pOld = par ? P1 : P0;
     T* __restrict__ pNew = par ? P0 : P1;
     T acc = T(0), rr = T(0), rq = T(0), qq = T(0);
@@ -403,7 +426,117 @@ __global__ void __launch_bounds__(kBlock, (L > 1 ? 4 : (sizeof(T) == 4 ? (REC ==
         return mode ? fma(beta, pOld[j], zat(j)) : zat(j);
     };
     auto ownr = [&](size_t row, T sum) { own(row, (REC && JZ == 2) ? zc * sum : sum); };
-    if (L == 1 && REC && (A.mask || A.gnz) && A.ulen <= 8) {
+    if constexpr (V4 && L == 1 && REC && sizeof(T) == 4) {
+        // Rows 4g .. 4g+3 on one thread, lanes of a warp on consecutive groups g. Offset
+        // d takes the rows' values
+        //   d % 4 == 0:  from the aligned group g + d/4 (one 16-byte load);
+        //   |d| < 4:     from this lane's own group and its neighbours' (warp shuffles; lanes
+        //                0 and 31 load the group beyond the warp);
+        //   otherwise:   from the aligned groups g + floor(d/4) and the one after it.
+        // A needed element lies in [0, n) and n % 4 == 0, so its whole group does too; the
+        // loads are issued for every group inside [0, n / 4) whatever the masks say, so
+        // that they do not wait for the mask load (the masks only pick the FMAs). Group
+        // indices are 32-bit and wrap (n / 4 < 2^30, |d| < 2^31), so one unsigned compare
+        // bounds them. Each row's sum, p, q and x follow the row-per-thread path operation
+        // for operation (the same bits); only the order in which a thread adds its rows
+        // into the partial sums differs.
+        const uint32_t n4 = A.nrow >> 2, stride = gridDim.x * blockDim.x;
+        const uint32_t lane = threadIdx.x & 31u;
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4* z4 = reinterpret_cast<const float4*>(z);
+        float4* p4 = reinterpret_cast<float4*>(P0);
+        float4* q4 = reinterpret_cast<float4*>(q);
+        float4* x4 = reinterpret_cast<float4*>(x);
+        int npos = 0, nneg = 0; // reach of the offsets 0 < |d| < 4 to either side
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k < (int)A.ulen) {
+                const int d = A.udelta[k];
+                if (d > npos && d < 4) npos = d;
+                if (-d > nneg && d > -4) nneg = -d;
+            }
+        // the loop bound is the same on every lane of a warp (all lanes shuffle)
+        for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane < n4; g += stride) {
+            const bool act = g < n4;
+            float4 zr4 = zero, po4 = zero, qo4 = zero, xo4 = zero;
+            uint32_t m[4] = {0u, 0u, 0u, 0u};
+            if (act) {
+                zr4 = z4[g];
+                po4 = p4[g];
+                qo4 = q4[g];
+                if (xpend) xo4 = x4[g];
+                if (A.gnz) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) m[j] = grid_mask(A, 4u * g + (uint32_t)j);
+                } else {
+                    const uint2 mm = __ldg(reinterpret_cast<const uint2*>(A.mask) + g);
+                    m[0] = mm.x & 0xffffu;
+                    m[1] = mm.x >> 16;
+                    m[2] = mm.y & 0xffffu;
+                    m[3] = mm.y >> 16;
+                }
+            }
+            float4 pv = zero, nx = zero; // groups g - 1 and g + 1
+            if (nneg) {
+                pv.w = __shfl_up_sync(0xffffffffu, zr4.w, 1);
+                if (nneg > 1) pv.z = __shfl_up_sync(0xffffffffu, zr4.z, 1);
+                if (nneg > 2) pv.y = __shfl_up_sync(0xffffffffu, zr4.y, 1);
+                if (lane == 0 && act && g > 0) pv = z4[g - 1];
+            }
+            if (npos) {
+                nx.x = __shfl_down_sync(0xffffffffu, zr4.x, 1);
+                if (npos > 1) nx.y = __shfl_down_sync(0xffffffffu, zr4.y, 1);
+                if (npos > 2) nx.z = __shfl_down_sync(0xffffffffu, zr4.z, 1);
+                if (lane == 31 && g + 1 < n4) nx = z4[g + 1];
+            }
+            float4 xs[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                xs[k] = zero;
+                if (k < (int)A.ulen) {
+                    const int d = A.udelta[k];
+                    const uint32_t ga = g + (uint32_t)(d >> 2); // floor(d / 4), wrapped
+                    if ((d & 3) == 0) {
+                        if (act && ga < n4) xs[k] = z4[ga];
+                    } else if (d > -4 && d < 4) {
+                        xs[k] = d > 0 ? f4shift(zr4, nx, d) : f4shift(pv, zr4, 4 + d);
+                    } else {
+                        float4 a = zero, b = zero;
+                        if (act && ga < n4) a = z4[ga];
+                        if (act && ga + 1u < n4) b = z4[ga + 1u];
+                        xs[k] = f4shift(a, b, d & 3);
+                    }
+                }
+            }
+            float pn[4], qn[4], xn[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float sum = 0.f;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if ((m[j] >> k) & 1u) sum = fmaf(A.uval[k], f4c(xs[k], j), sum);
+                if (JZ == 2) sum = zc * sum;
+                const float zraw = f4c(zr4, j);
+                const float zi = JZ == 2 ? zc * zraw : zraw;
+                const float po = f4c(po4, j);
+                xn[j] = fmaf(alphaPrev, po, f4c(xo4, j));
+                pn[j] = mode ? fmaf(beta, po, zi) : zi;
+                qn[j] = mode ? fmaf(beta, f4c(qo4, j), sum) : sum;
+                // inactive lanes hold zeros: their terms add +0 to the partial sums
+                acc = fmaf(qn[j], pn[j], acc);
+                if (ONE) {
+                    rr = fmaf(zraw, zraw, rr);
+                    rq = fmaf(zraw, qn[j], rq);
+                    qq = fmaf(qn[j], qn[j], qq);
+                }
+            }
+            if (act) {
+                p4[g] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+                q4[g] = make_float4(qn[0], qn[1], qn[2], qn[3]);
+                if (xpend) x4[g] = make_float4(xn[0], xn[1], xn[2], xn[3]);
+            }
+        }
+    } else if (L == 1 && REC && (A.mask || A.gnz) && A.ulen <= 8) {
         // stencil masks of at most 8 offsets (the 5- and 7-point stencils): 32-bit row
         // indices, each gather one signed offset from the row's own address, and no
         // offset-count tests (the mask has no bits at or above ulen)
@@ -646,14 +779,16 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_r(uint32_t n, T* __restri
 {
     pdl_wait();
     pdl_release();
+    // the control fields, loaded together ahead of the tests
     const int st = c->status;
+    const unsigned skipUpd = c->skipUpd, numIter = c->numIter;
+    const T alpha = (T)c->alpha;
     if (st != kRun) {
         if constexpr (std::is_same<T, float>::value)
             if (st == kRefresh) cg_refresh_fold(n, x, P0, c);
         return;
     }
-    if (c->skipUpd == c->numIter + 1) return;
-    const T alpha = (T)c->alpha;
+    if (skipUpd == numIter + 1) return;
     using V = typename V16<T>::t;
     constexpr int W = V16<T>::W;
     const size_t nv = n / W;
@@ -971,8 +1106,14 @@ void CGEngine<T>::launch_spmv_kernel()
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red);
     };
+    auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
+    // four rows per thread (FP32 recurrences on stencil masks, see cg_spmv)
+    const bool v4 = sizeof(T) == 4 && recurrence && A->lanes == 1 && (V.mask || V.gnz) &&
+                    V.ulen <= 8 && V.nrow % 4 == 0 && V.nrow == V.mcol && al(zz, 16) &&
+                    al(P0, 16) && al(q, 16) && al(x, 16) && (V.gnz || al(V.mask, 8));
 #define CG_SPMV_LANES(RR, JJ)                                                              \
-    switch (A->lanes) {                                                                    \
+    switch (v4 ? 0 : A->lanes) {                                                           \
+        case 0: go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4)>); break;              \
         case 1: go(cg_spmv<T, 1, RR, JJ>); break;                                          \
         case 2: go(cg_spmv<T, 2, RR, JJ>); break;                                          \
         case 4: go(cg_spmv<T, 4, RR, JJ>); break;                                          \
