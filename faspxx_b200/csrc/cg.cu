@@ -358,13 +358,14 @@ __device__ __forceinline__ float4 f4shift(const float4& a, const float4& b, int 
 // 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4.
 // V4 (FP32 recurrences on stencil masks of at most 8 offsets): four consecutive rows per
 // thread with 16-byte loads; the host checks n % 4 == 0, a square matrix and 16-byte
-// aligned vectors (8-byte aligned masks).
-template <typename T, int L, int REC, int JZ, bool V4 = false>
+// aligned vectors (8-byte aligned masks). SH = 5 or 7: the offsets are
+// known to be [-S1, -1, 0, 1, S1] or [-S2, -S1, -1, 0, 1, S1, S2] with S1, S2 multiples of
+// 4 (the 2D and 3D Laplacian stencils on lexicographic grids), so that every gather is one
+// aligned 16-byte word or a fixed shift of the row's own and a neighbouring word.
+template <typename T, int L, int REC, int JZ, bool V4 = false, int SH = 0>
 __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4 ? (REC == 2 ? 5 : 6) : 5))))
-    cg_spmv(CSRView<T> A,
-                                                                     const T* __restrict__ z,
-                                                  T* P0, T* P1, T* __restrict__ q, T* x,
-                                                  CGCtl* c, Scratch s)
+    cg_spmv(CSRView<T> A, const T* __restrict__ z, T* P0, T* P1, T* __restrict__ q, T* x,
+            CGCtl* c, Scratch s, MarchPlan mp)
 {
     static_assert(REC != 2 || JZ != 1, "one-reduction iterations need z = r or z = zc r");
     constexpr bool ONE = REC == 2;
@@ -426,6 +427,33 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
         return mode ? fma(beta, pOld[j], zat(j)) : zat(j);
     };
     auto ownr = [&](size_t row, T sum) { own(row, (REC && JZ == 2) ? zc * sum : sum); };
+    // rows 4g .. 4g+3 from the masks m, the values xs[k] at each offset and the row's own
+    // z, p, q, x: the row-per-thread arithmetic operation for operation (the same bits);
+    // only the order in which a thread adds its rows into the partial sums differs
+    auto group4 = [&](const uint32_t (&m)[4], const float4 (&xs)[8], const float4& zr4,
+                      const float4& po4, const float4& qo4, const float4& xo4, float* pn,
+                      float* qn, float* xn) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float sum = 0.f;
+#pragma unroll
+            for (int k = 0; k < (SH ? SH : 8); ++k)
+                if ((m[j] >> k) & 1u) sum = fmaf((float)A.uval[k], f4c(xs[k], j), sum);
+            if (JZ == 2) sum = (float)zc * sum;
+            const float zraw = f4c(zr4, j);
+            const float zi = JZ == 2 ? (float)zc * zraw : zraw;
+            const float po = f4c(po4, j);
+            xn[j] = fmaf((float)alphaPrev, po, f4c(xo4, j));
+            pn[j] = mode ? fmaf((float)beta, po, zi) : zi;
+            qn[j] = mode ? fmaf((float)beta, f4c(qo4, j), sum) : sum;
+            acc = fmaf(qn[j], pn[j], (float)acc);
+            if (ONE) {
+                rr = fmaf(zraw, zraw, (float)rr);
+                rq = fmaf(zraw, qn[j], (float)rq);
+                qq = fmaf(qn[j], qn[j], (float)qq);
+            }
+        }
+    };
     if constexpr (V4 && L == 1 && REC && sizeof(T) == 4) {
         // Rows 4g .. 4g+3 on one thread, lanes of a warp on consecutive groups g. Offset
         // d takes the rows' values
@@ -447,14 +475,70 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
         float4* p4 = reinterpret_cast<float4*>(P0);
         float4* q4 = reinterpret_cast<float4*>(q);
         float4* x4 = reinterpret_cast<float4*>(x);
-        int npos = 0, nneg = 0; // reach of the offsets 0 < |d| < 4 to either side
+        int npos = SH ? 1 : 0, nneg = SH ? 1 : 0; // reach of the offsets 0 < |d| < 4
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-            if (k < (int)A.ulen) {
+            if (!SH && k < (int)A.ulen) {
                 const int d = A.udelta[k];
                 if (d > npos && d < 4) npos = d;
                 if (-d > nneg && d > -4) nneg = -d;
             }
+        if (SH == 7 && mp.p4) {
+            // Plane columns (MarchPlan, cols = p4 groups a plane): item w = (column w % cols,
+            // chunk w / cols) walks groups g = column + k cols over the planes k of its chunk.
+            // cols % 32 == 0, so a warp's lanes share the chunk and hold consecutive columns
+            // (every lane takes part in the shuffles); the -S2 / +S2 groups rotate through
+            // registers, one new z load a step.
+            const uint32_t cols = mp.p4, nz = mp.nz, C = mp.chunk;
+            const uint32_t items = cols * ((nz + C - 1) / C);
+            const int o1 = A.udelta[1] >> 2, o5 = A.udelta[5] >> 2; // -S1 / 4, S1 / 4
+            for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w - lane < items;
+                 w += stride) {
+                if (w >= items) break; // whole warps (items % 32 == 0)
+                const uint32_t k0 = (w / cols) * C, k1 = min(k0 + C, nz);
+                uint32_t g = w % cols + k0 * cols;
+                float4 below = k0 > 0 ? z4[g - cols] : zero, cur = z4[g];
+                for (uint32_t k = k0; k < k1; ++k, g += cols) {
+                    const float4 above = k + 1 < nz ? z4[g + cols] : zero;
+                    const float4 po4 = p4[g], qo4 = q4[g];
+                    const float4 xo4 = xpend ? x4[g] : zero;
+                    uint32_t m[4];
+                    if (A.gnz) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) m[j] = grid_mask(A, 4u * g + (uint32_t)j);
+                    } else {
+                        const uint2 mm = __ldg(reinterpret_cast<const uint2*>(A.mask) + g);
+                        m[0] = mm.x & 0xffffu;
+                        m[1] = mm.x >> 16;
+                        m[2] = mm.y & 0xffffu;
+                        m[3] = mm.y >> 16;
+                    }
+                    const uint32_t ga = g + (uint32_t)o1, gb = g + (uint32_t)o5;
+                    const float4 s1lo = ga < n4 ? z4[ga] : zero, s1hi = gb < n4 ? z4[gb] : zero;
+                    float4 pv = zero, nx = zero;
+                    pv.w = __shfl_up_sync(0xffffffffu, cur.w, 1);
+                    nx.x = __shfl_down_sync(0xffffffffu, cur.x, 1);
+                    if (lane == 0 && g > 0) pv = z4[g - 1];
+                    if (lane == 31 && g + 1 < n4) nx = z4[g + 1];
+                    float4 xs[8];
+                    xs[0] = below;
+                    xs[1] = s1lo;
+                    xs[2] = make_float4(pv.w, cur.x, cur.y, cur.z);
+                    xs[3] = cur;
+                    xs[4] = make_float4(cur.y, cur.z, cur.w, nx.x);
+                    xs[5] = s1hi;
+                    xs[6] = above;
+                    xs[7] = zero;
+                    float pn[4], qn[4], xn[4];
+                    group4(m, xs, cur, po4, qo4, xo4, pn, qn, xn);
+                    p4[g] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+                    q4[g] = make_float4(qn[0], qn[1], qn[2], qn[3]);
+                    if (xpend) x4[g] = make_float4(xn[0], xn[1], xn[2], xn[3]);
+                    below = cur;
+                    cur = above;
+                }
+            }
+        } else
         // the loop bound is the same on every lane of a warp (all lanes shuffle)
         for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane < n4; g += stride) {
             const bool act = g < n4;
@@ -493,7 +577,19 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 xs[k] = zero;
-                if (k < (int)A.ulen) {
+                if (SH) { // fixed shape: offsets -1, 0, 1 sit at SH/2 - 1 .. SH/2
+                    if (k >= SH) continue;
+                    if (k == SH / 2) {
+                        xs[k] = zr4;
+                    } else if (k == SH / 2 - 1) {
+                        xs[k] = make_float4(pv.w, zr4.x, zr4.y, zr4.z);
+                    } else if (k == SH / 2 + 1) {
+                        xs[k] = make_float4(zr4.y, zr4.z, zr4.w, nx.x);
+                    } else {
+                        const uint32_t ga = g + (uint32_t)(A.udelta[k] >> 2);
+                        if (act && ga < n4) xs[k] = z4[ga];
+                    }
+                } else if (k < (int)A.ulen) {
                     const int d = A.udelta[k];
                     const uint32_t ga = g + (uint32_t)(d >> 2); // floor(d / 4), wrapped
                     if ((d & 3) == 0) {
@@ -509,27 +605,8 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
                 }
             }
             float pn[4], qn[4], xn[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                float sum = 0.f;
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if ((m[j] >> k) & 1u) sum = fmaf(A.uval[k], f4c(xs[k], j), sum);
-                if (JZ == 2) sum = zc * sum;
-                const float zraw = f4c(zr4, j);
-                const float zi = JZ == 2 ? zc * zraw : zraw;
-                const float po = f4c(po4, j);
-                xn[j] = fmaf(alphaPrev, po, f4c(xo4, j));
-                pn[j] = mode ? fmaf(beta, po, zi) : zi;
-                qn[j] = mode ? fmaf(beta, f4c(qo4, j), sum) : sum;
-                // inactive lanes hold zeros: their terms add +0 to the partial sums
-                acc = fmaf(qn[j], pn[j], acc);
-                if (ONE) {
-                    rr = fmaf(zraw, zraw, rr);
-                    rq = fmaf(zraw, qn[j], rq);
-                    qq = fmaf(qn[j], qn[j], qq);
-                }
-            }
+            // inactive lanes hold zeros: their terms add +0 to the partial sums
+            group4(m, xs, zr4, po4, qo4, xo4, pn, qn, xn);
             if (act) {
                 p4[g] = make_float4(pn[0], pn[1], pn[2], pn[3]);
                 q4[g] = make_float4(qn[0], qn[1], qn[2], qn[3]);
@@ -1078,13 +1155,13 @@ CSRView<float> view_of<float>(const Mat& A) { return A.v32(); }
 // Launch with programmatic stream serialization when pdl is set (captured into the graph as
 // a programmatic edge), so the kernel's launch overlaps its predecessor's reduction tail.
 template <typename... P, typename... A>
-static void launch_overlapped(void (*kern)(P...), int grid, cudaStream_t s, bool pdl,
-                              A&&... args)
+static void launch_overlapped_smem(void (*kern)(P...), int grid, size_t smem, cudaStream_t s,
+                                   bool pdl, A&&... args)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(kBlock);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1092,6 +1169,45 @@ static void launch_overlapped(void (*kern)(P...), int grid, cudaStream_t s, bool
     cfg.attrs = at;
     cfg.numAttrs = pdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+template <typename... P, typename... A>
+static void launch_overlapped(void (*kern)(P...), int grid, cudaStream_t s, bool pdl,
+                              A&&... args)
+{
+    launch_overlapped_smem(kern, grid, 0, s, pdl, std::forward<A>(args)...);
+}
+
+// cg_spmv's SH for a stencil-mask view: 5 or 7 when its sorted offsets are
+// [-S1, -1, 0, 1, S1] or [-S2, -S1, -1, 0, 1, S1, S2] with S1, S2 multiples of 4, else 0.
+template <typename V>
+static int stencil_shape(const V& A)
+{
+    if (A.ulen != 5 && A.ulen != 7) return 0;
+    const int mid = (int)A.ulen / 2;
+    if (A.udelta[mid] != 0 || A.udelta[mid - 1] != -1 || A.udelta[mid + 1] != 1) return 0;
+    for (int k = 0; k < (int)A.ulen; ++k)
+        if ((k < mid - 1 || k > mid + 1) && A.udelta[k] % 4 != 0) return 0;
+    return (int)A.ulen;
+}
+
+// The plane columns of a 3D seven-point stencil (SH = 7) with offsets +-S2, S2 a multiple
+// of 128 (a warp's 32 groups stay in one plane) dividing n: chunk planes per thread, so
+// that grid x kBlock threads cover every (column, chunk) item in one pass.
+template <typename V>
+static MarchPlan march_plan(const V& A, int sh, int grid)
+{
+    MarchPlan mp;
+    if (sh != 7 || A.udelta[0] != -A.udelta[6]) return mp;
+    const long long s2 = A.udelta[6];
+    if (s2 % 128 != 0 || (long long)A.nrow % s2 != 0 || (long long)A.nrow / s2 < 2) return mp;
+    const long long p4 = s2 / 4, nz = (long long)A.nrow / s2;
+    const long long threads = (long long)grid * kBlock;
+    long long chunk = (nz * p4 + threads - 1) / threads;
+    if (chunk < 1) chunk = 1;
+    mp.p4 = (uint32_t)p4;
+    mp.nz = (uint32_t)nz;
+    mp.chunk = (uint32_t)chunk;
+    return mp;
 }
 
 // The two fused kernels, each on one resident wave (grid from the occupancy limit).
@@ -1102,9 +1218,11 @@ void CGEngine<T>::launch_spmv_kernel()
     const int need = spmv_grid_cg(*c, A->nrow, A->lanes);
     const int jm = jmode();
     const T* zz = jm == 1 ? z : r;
+    const int sh = stencil_shape(V);
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
-        launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red);
+        launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red,
+                          march_plan(V, sh, g));
     };
     auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
     // four rows per thread (FP32 recurrences on stencil masks, see cg_spmv)
@@ -1113,7 +1231,14 @@ void CGEngine<T>::launch_spmv_kernel()
                     al(P0, 16) && al(q, 16) && al(x, 16) && (V.gnz || al(V.mask, 8));
 #define CG_SPMV_LANES(RR, JJ)                                                              \
     switch (v4 ? 0 : A->lanes) {                                                           \
-        case 0: go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4)>); break;              \
+        case 0:                                                                            \
+            if (sh == 5)                                                                   \
+                go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4), 5>);                  \
+            else if (sh == 7)                                                              \
+                go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4), 7>);                  \
+            else                                                                           \
+                go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4)>);                     \
+            break;                                                                         \
         case 1: go(cg_spmv<T, 1, RR, JJ>); break;                                          \
         case 2: go(cg_spmv<T, 2, RR, JJ>); break;                                          \
         case 4: go(cg_spmv<T, 4, RR, JJ>); break;                                          \

@@ -63,6 +63,15 @@ struct CGCtl {
     double   histScale;  // inner solves record scale * residual
 };
 
+// Plane columns of the FP32 CG SpMV on 3D seven-point stencil masks (cg_spmv with V4 and
+// SH = 7): the matrix is nz planes of 4 p4 rows (the offset +-S2 = 4 p4 is one plane), and
+// a thread walks `chunk` consecutive planes of one column of 4-row groups, so that the z
+// groups at -S2, 0 and +S2 of a plane are the previous, current and next plane's group
+// of the same column, held in registers. p4 == 0: not in use.
+struct MarchPlan {
+    uint32_t p4 = 0, nz = 0, chunk = 0;
+};
+
 // Device-driven PCG on one square matrix. T = double (the reference's arithmetic) or
 // float (inner solves). The preconditioner is fused: identity (z aliases r) or one Jacobi
 // sweep from zero, z = weight/diag .* r (Jacobi::Solve with minIter = maxIter = 1).

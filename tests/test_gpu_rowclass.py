@@ -129,12 +129,13 @@ def _banded(shape, offsets, vals):
     return P._from_stencil(shape, offsets, lambda k: vals[k])
 
 
-@pytest.mark.parametrize("name", ["band3", "band27", "grid18"])
+@pytest.mark.parametrize("name", ["band3", "band27", "grid18", "grid32"])
 def test_four_row_path_every_offset_kind(gpu, name):
     """Mixed-precision CG on stencil masks with n % 4 == 0 runs four rows per thread. Its
     three ways of reaching a neighbour -- an aligned 16-byte group (d % 4 == 0), warp
     shuffles of the neighbouring lanes' groups (|d| < 4) and two aligned groups (the rest)
-    -- must give the solve of the row-per-thread kernel on the CSR form."""
+    -- and the seven-point kernel that walks columns of planes (plane stride a multiple of
+    128, grid32) must give the solve of the row-per-thread kernel on the CSR form."""
     from faspxx_b200 import capi
     if name == "band3":      # offsets -3 .. 3: shuffles reaching three elements each way
         A = _banded((1000, 1, 1), [(d, 0, 0) for d in range(-3, 4)],
@@ -142,8 +143,10 @@ def test_four_row_path_every_offset_kind(gpu, name):
     elif name == "band27":   # offsets +-2 (shuffles) and +-7 (two groups)
         A = _banded((1000, 1, 1), [(-7, 0, 0), (-2, 0, 0), (0, 0, 0), (2, 0, 0), (7, 0, 0)],
                     [-0.4, -0.55, 2.0, -0.55, -0.4])
-    else:                    # 18 x 10 x 8 grid: +-1 shuffles, +-18 two groups, +-180 aligned
+    elif name == "grid18":   # 18 x 10 x 8 grid: +-1 shuffles, +-18 two groups, +-180 aligned
         A = _banded((18, 10, 8), P._OFF3D, [-1.0, -1.0, -1.0, 6.0, -1.0, -1.0, -1.0])
+    else:                    # 32 x 32 x 12 grid: planes of 1024 rows walked in columns
+        A = _banded((32, 32, 12), P._OFF3D, [-1.0, -1.0, -1.0, 6.0, -1.0, -1.0, -1.0])
     assert A.nrow % 4 == 0
     b = A.matvec(np.random.default_rng(7).uniform(-1, 1, A.nrow))
     out = []
