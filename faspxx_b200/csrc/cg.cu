@@ -356,9 +356,10 @@ __device__ __forceinline__ float4 f4shift(const float4& a, const float4& b, int 
 // the FP64 refreshes of reliable updates correct the residual it feeds.
 // Blocks per SM: FP32 6 (40 registers), one-reduction FP32 5 (its extra sums spill under
 // 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4.
-// V4 (FP32 recurrences on stencil masks of at most 8 offsets): four consecutive rows per
-// thread with 16-byte loads; the host checks n % 4 == 0, a square matrix and 16-byte
-// aligned vectors (8-byte aligned masks). SH = 5 or 7: the offsets are
+// V4 (stencil masks of at most 8 offsets): consecutive rows per thread with 16-byte loads,
+// four for the FP32 recurrences, two for FP64 (REC = 0, fixed shapes only); the host checks
+// n % 4 (FP64: n % 2) == 0, a square matrix and 16-byte aligned vectors (8- or 4-byte
+// aligned masks). SH = 5 or 7: the offsets are
 // known to be [-S1, -1, 0, 1, S1] or [-S2, -S1, -1, 0, 1, S1, S2] with S1, S2 multiples of
 // 4 (the 2D and 3D Laplacian stencils on lexicographic grids), so that every gather is one
 // aligned 16-byte word or a fixed shift of the row's own and a neighbouring word.
@@ -611,6 +612,129 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
                 p4[g] = make_float4(pn[0], pn[1], pn[2], pn[3]);
                 q4[g] = make_float4(qn[0], qn[1], qn[2], qn[3]);
                 if (xpend) x4[g] = make_float4(xn[0], xn[1], xn[2], xn[3]);
+            }
+        }
+    } else if constexpr (V4 && L == 1 && !REC && sizeof(T) == 8 && SH != 0) {
+        // FP64 in the reference's order (p = z + beta p_old formed for every gathered entry,
+        // CG.cxx:233 folded into the SpMV): rows 2g, 2g+1 on one thread, lanes on
+        // consecutive groups; the gathered p of group h comes from z and p_old at h with the
+        // row-per-thread formula, -1/+1 from the neighbouring lanes' groups (shuffles; lanes
+        // 0 and 31 form the group beyond the warp), +-S1 (and +-S2 outside a plane walk) from
+        // aligned groups. Each row's sum and its p, q follow the row-per-thread path
+        // operation for operation (the same bits); the partial sums group rows by two.
+        const uint32_t n2 = A.nrow >> 1, stride = gridDim.x * blockDim.x;
+        const uint32_t lane = threadIdx.x & 31u;
+        const double2 zero = make_double2(0.0, 0.0);
+        const double2* z2 = reinterpret_cast<const double2*>(z);
+        const double2* po2 = reinterpret_cast<const double2*>(pOld);
+        double2* pn2 = reinterpret_cast<double2*>(pNew);
+        double2* q2 = reinterpret_cast<double2*>(q);
+        constexpr int MID = SH / 2;
+        auto pat = [&](uint32_t h) { // the gathered p of rows 2h, 2h+1
+            const double2 zz = z2[h];
+            const double a = JZ == 2 ? (double)zc * zz.x : zz.x;
+            const double b = JZ == 2 ? (double)zc * zz.y : zz.y;
+            if (!mode) return make_double2(a, b);
+            const double2 o = po2[h];
+            return make_double2(fma((double)beta, o.x, a), fma((double)beta, o.y, b));
+        };
+        auto masks = [&](uint32_t g, uint32_t& m0, uint32_t& m1) {
+            if (A.gnz) {
+                m0 = grid_mask(A, 2u * g);
+                m1 = grid_mask(A, 2u * g + 1u);
+            } else {
+                const uint32_t mm = __ldg(reinterpret_cast<const uint32_t*>(A.mask) + g);
+                m0 = mm & 0xffffu;
+                m1 = mm >> 16;
+            }
+        };
+        // the two rows' sums from the values at each offset, then p, q and (q, p)
+        auto rows2 = [&](uint32_t g, uint32_t m0, uint32_t m1, const double2 (&xs)[SH],
+                         const double2& pc) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < SH; ++k) {
+                if ((m0 >> k) & 1u) s0 = fma((double)A.uval[k], xs[k].x, s0);
+                if ((m1 >> k) & 1u) s1 = fma((double)A.uval[k], xs[k].y, s1);
+            }
+            pn2[g] = pc;
+            q2[g] = make_double2(s0, s1);
+            acc = fma(s0, pc.x, (double)acc);
+            acc = fma(s1, pc.y, (double)acc);
+        };
+        // -1 / +1 neighbours of a warp's consecutive groups
+        auto sides = [&](uint32_t g, bool act, const double2& pc, double2& pv, double2& nx) {
+            pv = zero;
+            nx = zero;
+            pv.y = __shfl_up_sync(0xffffffffu, pc.y, 1);
+            nx.x = __shfl_down_sync(0xffffffffu, pc.x, 1);
+            if (lane == 0 && act && g > 0) pv = pat(g - 1);
+            if (lane == 31 && act && g + 1 < n2) nx = pat(g + 1);
+        };
+        bool walked = false;
+        if constexpr (SH == 7) {
+          if (mp.p4) {
+            walked = true;
+            // plane columns (MarchPlan with two-row groups: cols = S2 / 2 per plane)
+            const uint32_t cols = mp.p4, nz = mp.nz, C = mp.chunk;
+            const uint32_t items = cols * ((nz + C - 1) / C);
+            const int o1 = A.udelta[1] >> 1, o5 = A.udelta[5] >> 1;
+            for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w - lane < items;
+                 w += stride) {
+                if (w >= items) break; // whole warps (items % 32 == 0)
+                const uint32_t k0 = (w / cols) * C, k1 = min(k0 + C, nz);
+                uint32_t g = w % cols + k0 * cols;
+                double2 below = k0 > 0 ? pat(g - cols) : zero, cur = pat(g);
+                for (uint32_t k = k0; k < k1; ++k, g += cols) {
+                    const double2 above = k + 1 < nz ? pat(g + cols) : zero;
+                    uint32_t m0, m1;
+                    masks(g, m0, m1);
+                    const uint32_t ga = g + (uint32_t)o1, gb = g + (uint32_t)o5;
+                    double2 xs[SH];
+                    xs[0] = below;
+                    xs[1] = ga < n2 ? pat(ga) : zero;
+                    double2 pv, nx;
+                    sides(g, true, cur, pv, nx);
+                    xs[2] = make_double2(pv.y, cur.x);
+                    xs[3] = cur;
+                    xs[4] = make_double2(cur.y, nx.x);
+                    xs[5] = gb < n2 ? pat(gb) : zero;
+                    xs[6] = above;
+                    rows2(g, m0, m1, xs, cur);
+                    below = cur;
+                    cur = above;
+                }
+            }
+          }
+        }
+        if (!walked) {
+            // the loop bound is the same on every lane of a warp (all lanes shuffle)
+            for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane < n2;
+                 g += stride) {
+                const bool act = g < n2;
+                double2 pc = zero;
+                uint32_t m0 = 0u, m1 = 0u;
+                if (act) {
+                    pc = pat(g);
+                    masks(g, m0, m1);
+                }
+                double2 pv, nx;
+                sides(g, act, pc, pv, nx);
+                double2 xs[SH];
+#pragma unroll
+                for (int k = 0; k < SH; ++k) {
+                    if (k == MID) {
+                        xs[k] = pc;
+                    } else if (k == MID - 1) {
+                        xs[k] = make_double2(pv.y, pc.x);
+                    } else if (k == MID + 1) {
+                        xs[k] = make_double2(pc.y, nx.x);
+                    } else {
+                        const uint32_t ga = g + (uint32_t)(A.udelta[k] >> 1);
+                        xs[k] = act && ga < n2 ? pat(ga) : zero;
+                    }
+                }
+                if (act) rows2(g, m0, m1, xs, pc);
             }
         }
     } else if (L == 1 && REC && (A.mask || A.gnz) && A.ulen <= 8) {
@@ -1191,16 +1315,17 @@ static int stencil_shape(const V& A)
 }
 
 // The plane columns of a 3D seven-point stencil (SH = 7) with offsets +-S2, S2 a multiple
-// of 128 (a warp's 32 groups stay in one plane) dividing n: chunk planes per thread, so
-// that grid x kBlock threads cover every (column, chunk) item in one pass.
+// of 32 groups of rpg rows (a warp's groups stay in one plane) dividing n: chunk planes per
+// thread, so that grid x kBlock threads cover every (column, chunk) item in one pass.
 template <typename V>
-static MarchPlan march_plan(const V& A, int sh, int grid)
+static MarchPlan march_plan(const V& A, int sh, int grid, int rpg)
 {
     MarchPlan mp;
     if (sh != 7 || A.udelta[0] != -A.udelta[6]) return mp;
     const long long s2 = A.udelta[6];
-    if (s2 % 128 != 0 || (long long)A.nrow % s2 != 0 || (long long)A.nrow / s2 < 2) return mp;
-    const long long p4 = s2 / 4, nz = (long long)A.nrow / s2;
+    if (s2 % (32 * rpg) != 0 || (long long)A.nrow % s2 != 0 || (long long)A.nrow / s2 < 2)
+        return mp;
+    const long long p4 = s2 / rpg, nz = (long long)A.nrow / s2;
     const long long threads = (long long)grid * kBlock;
     long long chunk = (nz * p4 + threads - 1) / threads;
     if (chunk < 1) chunk = 1;
@@ -1222,20 +1347,25 @@ void CGEngine<T>::launch_spmv_kernel()
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red,
-                          march_plan(V, sh, g));
+                          march_plan(V, sh, g, sizeof(T) == 4 ? 4 : 2));
     };
     auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
-    // four rows per thread (FP32 recurrences on stencil masks, see cg_spmv)
-    const bool v4 = sizeof(T) == 4 && recurrence && A->lanes == 1 && (V.mask || V.gnz) &&
-                    V.ulen <= 8 && V.nrow % 4 == 0 && V.nrow == V.mcol && al(zz, 16) &&
-                    al(P0, 16) && al(q, 16) && al(x, 16) && (V.gnz || al(V.mask, 8));
+    // vector rows (stencil masks, see cg_spmv): four per thread for the FP32 recurrences,
+    // two for FP64 on the 5- and 7-point shapes
+    const bool base = A->lanes == 1 && (V.mask || V.gnz) && V.ulen <= 8 && V.nrow == V.mcol &&
+                      V.nrow < (1u << 30) && al(zz, 16) && al(P0, 16) && al(q, 16);
+    const bool v4 = sizeof(T) == 4
+                        ? base && recurrence && V.nrow % 4 == 0 && al(x, 16) &&
+                              (V.gnz || al(V.mask, 8))
+                        : base && !recurrence && sh != 0 && V.nrow % 2 == 0 && al(P1, 16) &&
+                              (V.gnz || al(V.mask, 4));
 #define CG_SPMV_LANES(RR, JJ)                                                              \
     switch (v4 ? 0 : A->lanes) {                                                           \
         case 0:                                                                            \
             if (sh == 5)                                                                   \
-                go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4), 5>);                  \
+                go(cg_spmv<T, 1, RR, JJ, (sizeof(T) == 4 ? RR > 0 : RR == 0), 5>);         \
             else if (sh == 7)                                                              \
-                go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4), 7>);                  \
+                go(cg_spmv<T, 1, RR, JJ, (sizeof(T) == 4 ? RR > 0 : RR == 0), 7>);         \
             else                                                                           \
                 go(cg_spmv<T, 1, RR, JJ, (RR > 0 && sizeof(T) == 4)>);                     \
             break;                                                                         \

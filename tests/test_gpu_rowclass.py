@@ -165,3 +165,35 @@ def test_four_row_path_every_offset_kind(gpu, name):
     assert np.linalg.norm(out[1][2] - out[0][2]) <= 1e-6 * np.linalg.norm(out[0][2])
     r = b - A.matvec(out[1][2])
     assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 12), (20, 20, 10), (40, 40)])
+def test_fp64_two_row_path(gpu, oracle_built, shape):
+    """FP64 CG on 5- and 7-point stencil masks with n % 2 == 0 runs two rows per thread
+    (walking columns of planes when the plane stride is a multiple of 64: 32 x 32 x 12).
+    Every row is formed as in the row-per-thread kernel; only the grouping of the FP64 dot
+    products differs, so the solve must agree with the CSR form and with the oracle's
+    iteration count."""
+    O = oracle_built
+    if len(shape) == 3:
+        A = _banded(shape, P._OFF3D, [-1.0, -1.0, -1.0, 6.0, -1.0, -1.0, -1.0])
+    else:
+        A = _banded((shape[0], shape[1], 1), P._OFF2D, [-1.0, -1.0, 4.0, -1.0, -1.0])
+    b = A.matvec(np.random.default_rng(11).uniform(-1, 1, A.nrow))
+    kw = dict(maxIter=3000, relTol=1e-10, absTol=0.0, pcd="jacobi", pcdWeight=1.0, pcdIter=1)
+    out = []
+    for form in (CSR, MASKS):
+        M = gpu.MAT(A)
+        M.SetRowClass(form)
+        s = gpu.configure("cg", **kw)
+        s.Setup(M)
+        x = np.zeros(A.nrow)
+        code = s.Solve(b, x)
+        out.append((code, s.GetIterations(), x, np.nan_to_num(s.History())))
+    ref = O.solve("port", A, "cg", b, np.zeros(A.nrow), **kw)
+    assert out[0][0] == out[1][0] == ref.code == 0
+    assert out[0][1] == out[1][1]
+    assert abs(out[1][1] - ref.iters) <= 1
+    assert np.linalg.norm(out[1][2] - out[0][2]) <= 1e-9 * np.linalg.norm(out[0][2])
+    assert np.linalg.norm(out[1][2] - ref.x) <= 1e-8 * np.linalg.norm(ref.x)
+    np.testing.assert_allclose(out[1][3], out[0][3], rtol=1e-6, atol=0.0)
