@@ -1301,18 +1301,6 @@ static void launch_overlapped(void (*kern)(P...), int grid, cudaStream_t s, bool
     launch_overlapped_smem(kern, grid, 0, s, pdl, std::forward<A>(args)...);
 }
 
-// cg_spmv's SH for a stencil-mask view: 5 or 7 when its sorted offsets are
-// [-S1, -1, 0, 1, S1] or [-S2, -S1, -1, 0, 1, S1, S2] with S1, S2 multiples of 4, else 0.
-template <typename V>
-static int stencil_shape(const V& A)
-{
-    if (A.ulen != 5 && A.ulen != 7) return 0;
-    const int mid = (int)A.ulen / 2;
-    if (A.udelta[mid] != 0 || A.udelta[mid - 1] != -1 || A.udelta[mid + 1] != 1) return 0;
-    for (int k = 0; k < (int)A.ulen; ++k)
-        if ((k < mid - 1 || k > mid + 1) && A.udelta[k] % 4 != 0) return 0;
-    return (int)A.ulen;
-}
 
 // The plane columns of a 3D seven-point stencil (SH = 7) with offsets +-S2, S2 a multiple
 // of 32 groups of rpg rows (a warp's groups stay in one plane) dividing n: chunk planes per

@@ -349,6 +349,19 @@ __device__ __forceinline__ void pdl_release()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The fixed stencil shape of a stencil-mask view (the vector-row SpMV kernels' SH): 5 or 7 when its sorted offsets are
+// [-S1, -1, 0, 1, S1] or [-S2, -S1, -1, 0, 1, S1, S2] with S1, S2 multiples of 4, else 0.
+template <typename V>
+inline int stencil_shape(const V& A)
+{
+    if (A.ulen != 5 && A.ulen != 7) return 0;
+    const int mid = (int)A.ulen / 2;
+    if (A.udelta[mid] != 0 || A.udelta[mid - 1] != -1 || A.udelta[mid + 1] != 1) return 0;
+    for (int k = 0; k < (int)A.ulen; ++k)
+        if ((k < mid - 1 || k > mid + 1) && A.udelta[k] % 4 != 0) return 0;
+    return (int)A.ulen;
+}
+
 __host__ __device__ inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 } // namespace fb
