@@ -116,8 +116,10 @@ __device__ void bi_checks(BiCtl* c, const double* red, int phase)
     }
 }
 
-// ptmp = D (A pj) with the loop-top sums.
-template <typename T, int L, int JAC>
+// ptmp = D (A pj) with the loop-top sums. SH = 5 or 7: stencil masks of that fixed shape,
+// 16-byte row groups per thread (stencil_group; each row's product is the same bits, the
+// partial sums group the rows by W).
+template <typename T, int L, int JAC, int SH = 0>
 __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict__ pj,
                                                const T* __restrict__ rj,
                                                const T* __restrict__ r0s,
@@ -135,7 +137,24 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
         a2 = fma(r, r, a2);
     };
     auto xv = [&](uint32_t j) { return pj[j]; };
-    if (L == 1) {
+    if constexpr (SH != 0) {
+        using V = typename Vec16<T>::V;
+        constexpr int W = Vec16<T>::W;
+        const uint32_t nw = A.nrow / W, stride = gridDim.x * blockDim.x;
+        const V* pv = reinterpret_cast<const V*>(pj);
+        for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - (threadIdx.x & 31u) < nw;
+             g += stride) {
+            const bool act = g < nw;
+            T sm[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) sm[j] = T(0);
+            V c;
+            stencil_group<T, SH>(A, g, nw, act, [&](uint32_t h) { return pv[h]; }, c, sm);
+            if (act)
+#pragma unroll
+                for (int j = 0; j < W; ++j) own((size_t)W * g + j, sm[j]);
+        }
+    } else if (L == 1) {
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x)
             own(row, row_apply<T, false>(A, row, xv));
@@ -163,8 +182,9 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
 }
 
 // sj = rj - alpha ptmp (on the fly for the gathers, stored for the owned rows),
-// stmp = D (A sj), omega = (stmp, sj) / (stmp, stmp)  (BiCGStab.cxx:103-113).
-template <typename T, int L, int JAC>
+// stmp = D (A sj), omega = (stmp, sj) / (stmp, stmp)  (BiCGStab.cxx:103-113). SH as bi_p,
+// with sj's groups formed from rj and ptmp by the same FMA.
+template <typename T, int L, int JAC, int SH = 0>
 __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict__ rj,
                                                const T* __restrict__ ptmp,
                                                const T* __restrict__ dinv, T* __restrict__ sj,
@@ -182,7 +202,33 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
         a0 = fma(st, sjv, a0);
         a1 = fma(st, st, a1);
     };
-    if (L == 1) {
+    if constexpr (SH != 0) {
+        using VT = Vec16<T>;
+        using V = typename VT::V;
+        constexpr int W = VT::W;
+        const uint32_t nw = A.nrow / W, stride = gridDim.x * blockDim.x;
+        const V* rv = reinterpret_cast<const V*>(rj);
+        const V* tv = reinterpret_cast<const V*>(ptmp);
+        auto sg = [&](uint32_t h) { // sj at group h
+            const V r = rv[h], t = tv[h];
+            T e[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) e[j] = fma(T(1), VT::at(r, j), nalpha * VT::at(t, j));
+            return VT::make(e);
+        };
+        for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - (threadIdx.x & 31u) < nw;
+             g += stride) {
+            const bool act = g < nw;
+            T sm[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) sm[j] = T(0);
+            V c;
+            stencil_group<T, SH>(A, g, nw, act, sg, c, sm);
+            if (act)
+#pragma unroll
+                for (int j = 0; j < W; ++j) own((size_t)W * g + j, sm[j]);
+        }
+    } else if (L == 1) {
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x)
             own(row, row_apply<T, false>(A, row, sv));
@@ -307,8 +353,19 @@ int BiEngine<T>::launch_iter()
         KS<T, LL, JJ><<<fit((const void*)KS<T, LL, JJ>, needS), kBlock, 0, c->stream>>>(   \
             V, rj, ptmp, dinv, sj, stmp, ctl, c->red);                                     \
     } while (0)
+    // 16-byte row groups on 5- and 7-point stencil masks (bi_p / bi_s with SH)
+    const int sh = L == 1 ? stencil_vec_shape(V, pj, rj, ptmp) : 0;
+#define BI_SPMV_SH(JJ, SS)                                                                 \
+    do {                                                                                   \
+        bi_p<T, 1, JJ, SS><<<fit((const void*)bi_p<T, 1, JJ, SS>, needV), kBlock, 0,       \
+                             c->stream>>>(V, pj, rj, r0s, dinv, ptmp, ctl, c->red);        \
+        bi_s<T, 1, JJ, SS><<<fit((const void*)bi_s<T, 1, JJ, SS>, needV), kBlock, 0,       \
+                             c->stream>>>(V, rj, ptmp, dinv, sj, stmp, ctl, c->red);       \
+    } while (0)
 #define BI_LANES(JJ)                                                                       \
-    switch (L) {                                                                           \
+    switch (sh ? -sh : L) {                                                                \
+        case -5: BI_SPMV_SH(JJ, 5); break;                                                 \
+        case -7: BI_SPMV_SH(JJ, 7); break;                                                 \
         case 1: BI_SPMV(bi_p, bi_s, 1, JJ); break;                                         \
         case 2: BI_SPMV(bi_p, bi_s, 2, JJ); break;                                         \
         case 4: BI_SPMV(bi_p, bi_s, 4, JJ); break;                                         \
@@ -326,6 +383,7 @@ int BiEngine<T>::launch_iter()
             n, x, rj, pj, sj, stmp, r0s, dinv, ctl, c->red);
     }
 #undef BI_LANES
+#undef BI_SPMV_SH
 #undef BI_SPMV
     bi_dir<T><<<fit((const void*)bi_dir<T>, needV), kBlock, 0, c->stream>>>(n, pj, rj, ptmp,
                                                                              ctl);

@@ -226,12 +226,6 @@ int v_copy(Ctx& c, uint32_t n, const T* src, T* dst)
 
 constexpr int KC = 8;
 
-template <typename T>
-struct Vec16 {
-    typedef typename std::conditional<sizeof(T) == 8, double2, float4>::type type;
-    static constexpr int W = 16 / (int)sizeof(T);
-};
-
 // Grid of the Gram-Schmidt kernels (one grid for all three, so the fused kernel maps
 // elements to threads exactly as the separate ones): 3 blocks per SM, all resident at once
 // (each kernel is compiled for 3 blocks of kBlock threads) -- one wave, each thread keeping

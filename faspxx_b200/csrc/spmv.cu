@@ -20,57 +20,8 @@ namespace fb {
 
 constexpr int kSlotResidualXinf = kSlots - 1;
 
-// 16-byte groups of rows: four FP32 or two FP64 values.
-template <typename T>
-struct Vec16;
-template <>
-struct Vec16<float> {
-    using V = float4;
-    static constexpr int W = 4;
-    __device__ static float at(const float4& v, int j)
-    {
-        return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
-    }
-    __device__ static float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-    // (prev last, v.x, v.y, v.z) and (v.y, v.z, v.w, next first): the -1 and +1 neighbours
-    __device__ static float4 down(float prevLast, const float4& v)
-    {
-        return make_float4(prevLast, v.x, v.y, v.z);
-    }
-    __device__ static float4 up(const float4& v, float nextFirst)
-    {
-        return make_float4(v.y, v.z, v.w, nextFirst);
-    }
-    __device__ static float first(const float4& v) { return v.x; }
-    __device__ static float last(const float4& v) { return v.w; }
-    __device__ static float4 make(const float* s) { return make_float4(s[0], s[1], s[2], s[3]); }
-};
-template <>
-struct Vec16<double> {
-    using V = double2;
-    static constexpr int W = 2;
-    __device__ static double at(const double2& v, int j) { return j == 0 ? v.x : v.y; }
-    __device__ static double2 zero() { return make_double2(0.0, 0.0); }
-    __device__ static double2 down(double prevLast, const double2& v)
-    {
-        return make_double2(prevLast, v.x);
-    }
-    __device__ static double2 up(const double2& v, double nextFirst)
-    {
-        return make_double2(v.y, nextFirst);
-    }
-    __device__ static double first(const double2& v) { return v.x; }
-    __device__ static double last(const double2& v) { return v.y; }
-    __device__ static double2 make(const double* s) { return make_double2(s[0], s[1]); }
-};
-
 // y = A x (RES: r = b - A x, with the x ~ 0 shortcut of MAT::Residual) on stencil masks of
-// the fixed 5- or 7-point shape (SH): W consecutive rows per thread, lanes of a warp on
-// consecutive groups; offsets -1/+1 from the neighbouring lanes' x groups (shuffles; lanes
-// 0 and 31 load the group beyond the warp), +-S from aligned 16-byte groups (loaded for
-// every group inside [0, n / W) whatever the masks say; a needed element lies in [0, n)
-// and n % W == 0, so its group does too). Each row sums its entries in offset order with
-// one FMA each, as row_apply does (the same bits).
+// the fixed 5- or 7-point shape (SH), W consecutive rows per thread (stencil_group).
 template <typename T, int SH, bool RES>
 __global__ void __launch_bounds__(kBlock) k_stencil_vec(CSRView<T> A, const T* __restrict__ x,
                                                         const T* __restrict__ b,
@@ -79,7 +30,7 @@ __global__ void __launch_bounds__(kBlock) k_stencil_vec(CSRView<T> A, const T* _
 {
     using VT = Vec16<T>;
     using V = typename VT::V;
-    constexpr int W = VT::W, MID = SH / 2;
+    constexpr int W = VT::W;
     const bool shortcut = RES && *xinf < kCloseZero;
     const uint32_t nw = A.nrow / W, stride = gridDim.x * blockDim.x;
     const uint32_t lane = threadIdx.x & 31u;
@@ -93,50 +44,8 @@ __global__ void __launch_bounds__(kBlock) k_stencil_vec(CSRView<T> A, const T* _
 #pragma unroll
         for (int j = 0; j < W; ++j) s[j] = T(0);
         if (!shortcut) {
-            V c = VT::zero();
-            uint32_t m[W];
-#pragma unroll
-            for (int j = 0; j < W; ++j) m[j] = 0u;
-            if (act) {
-                c = xv[g];
-                if (A.gnz) {
-#pragma unroll
-                    for (int j = 0; j < W; ++j) m[j] = grid_mask(A, W * g + (uint32_t)j);
-                } else if constexpr (W == 4) {
-                    const uint2 mm = __ldg(reinterpret_cast<const uint2*>(A.mask) + g);
-                    m[0] = mm.x & 0xffffu;
-                    m[1] = mm.x >> 16;
-                    m[2] = mm.y & 0xffffu;
-                    m[3] = mm.y >> 16;
-                } else {
-                    const uint32_t mm = __ldg(reinterpret_cast<const uint32_t*>(A.mask) + g);
-                    m[0] = mm & 0xffffu;
-                    m[1] = mm >> 16;
-                }
-            }
-            T pl = __shfl_up_sync(0xffffffffu, VT::last(c), 1);
-            T nf = __shfl_down_sync(0xffffffffu, VT::first(c), 1);
-            if (lane == 0 && act && g > 0) pl = VT::last(xv[g - 1]);
-            if (lane == 31 && act && g + 1 < nw) nf = VT::first(xv[g + 1]);
-            V xs[SH];
-#pragma unroll
-            for (int k = 0; k < SH; ++k) {
-                if (k == MID) {
-                    xs[k] = c;
-                } else if (k == MID - 1) {
-                    xs[k] = VT::down(pl, c);
-                } else if (k == MID + 1) {
-                    xs[k] = VT::up(c, nf);
-                } else {
-                    const uint32_t ga = g + (uint32_t)(A.udelta[k] / W); // wrapped
-                    xs[k] = act && ga < nw ? xv[ga] : VT::zero();
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < W; ++j)
-#pragma unroll
-                for (int k = 0; k < SH; ++k)
-                    if ((m[j] >> k) & 1u) s[j] = fma(A.uval[k], VT::at(xs[k], j), s[j]);
+            V c;
+            stencil_group<T, SH>(A, g, nw, act, [&](uint32_t h) { return xv[h]; }, c, s);
         }
         if (act) {
             if (RES) {
@@ -149,19 +58,6 @@ __global__ void __launch_bounds__(kBlock) k_stencil_vec(CSRView<T> A, const T* _
     }
 }
 
-// The vector-row stencil kernel applies: stencil masks (or a grid operator) of the 5- or
-// 7-point shape, a square matrix, n % W == 0, 16-byte aligned vectors and aligned masks.
-template <typename T>
-static int stencil_vec_shape(const CSRView<T>& A, const void* p0, const void* p1,
-                             const void* p2)
-{
-    constexpr int W = 16 / (int)sizeof(T);
-    auto al = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; };
-    if (!(A.mask || A.gnz) || A.nrow != A.mcol || A.nrow % W != 0 || A.nrow >= (1u << 30))
-        return 0;
-    if (!al(p0, 16) || !al(p1, 16) || !al(p2, 16) || (A.mask && !al(A.mask, 2 * W))) return 0;
-    return stencil_shape(A);
-}
 
 template <typename T, int L, bool PAT>
 __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restrict__ x,
