@@ -980,7 +980,23 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_r(uint32_t n, T* __restri
 {
     pdl_wait();
     pdl_release();
-    // the control fields, loaded together ahead of the tests
+    using V = typename V16<T>::t;
+    constexpr int W = V16<T>::W;
+    const size_t nv = n / W;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    // the thread's first two groups are loaded with the control fields (they do not
+    // depend on them), so the launch waits for one L2 round trip before its FMAs, not two
+    T ra[2][W], qa[2][W];
+    bool has[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        has[h] = tid + h * stride < nv;
+        if (has[h]) {
+            *(V*)ra[h] = ((const V*)r)[tid + h * stride];
+            *(V*)qa[h] = ((const V*)q)[tid + h * stride];
+        }
+    }
     const int st = c->status;
     const unsigned skipUpd = c->skipUpd, numIter = c->numIter;
     const T alpha = (T)c->alpha;
@@ -990,14 +1006,15 @@ __global__ void __launch_bounds__(kBlock, 4) cg_update_r(uint32_t n, T* __restri
         return;
     }
     if (skipUpd == numIter + 1) return;
-    using V = typename V16<T>::t;
-    constexpr int W = V16<T>::W;
-    const size_t nv = n / W;
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    size_t i = tid;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+        if (has[h]) {
+#pragma unroll
+            for (int u = 0; u < W; ++u) ra[h][u] = fma(-alpha, qa[h][u], ra[h][u]);
+            ((V*)r)[tid + h * stride] = *(V*)ra[h];
+        }
+    size_t i = tid + 2 * stride;
     for (; i + stride < nv; i += 2 * stride) {
-        T ra[2][W], qa[2][W];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             *(V*)ra[h] = ((const V*)r)[i + h * stride];
