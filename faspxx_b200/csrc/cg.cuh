@@ -63,11 +63,12 @@ struct CGCtl {
     double   histScale;  // inner solves record scale * residual
 };
 
-// Plane columns of the FP32 CG SpMV on 3D seven-point stencil masks (cg_spmv with V4 and
-// SH = 7): the matrix is nz planes of 4 p4 rows (the offset +-S2 = 4 p4 is one plane), and
-// a thread walks `chunk` consecutive planes of one column of 4-row groups, so that the z
-// groups at -S2, 0 and +S2 of a plane are the previous, current and next plane's group
-// of the same column, held in registers. p4 == 0: not in use.
+// Plane columns of the CG SpMV on 3D seven-point stencil masks (cg_spmv with V4 and SH = 7;
+// groups of rpg = 4 FP32 or 2 FP64 rows): the matrix is nz planes of p4 groups (the offset
+// +-S2 = rpg p4 rows is one plane), and a thread walks `chunk` consecutive planes of one
+// column of groups, so that the z (or p) groups at -S2, 0 and +S2 of a plane are the
+// previous, current and next plane's group of the same column, held in registers.
+// p4 == 0: not in use.
 struct MarchPlan {
     uint32_t p4 = 0, nz = 0, chunk = 0;
 };
