@@ -468,7 +468,9 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
         // indices are 32-bit and wrap (n / 4 < 2^30, |d| < 2^31), so one unsigned compare
         // bounds them. Each row's sum, p, q and x follow the row-per-thread path operation
         // for operation (the same bits); only the order in which a thread adds its rows
-        // into the partial sums differs.
+        // into the partial sums differs. With a fixed shape (SH) the offsets' kinds are known
+        // at compile time (no per-offset branches or selects), and SH = 7 with a MarchPlan
+        // walks columns of planes (below).
         const uint32_t n4 = A.nrow >> 2, stride = gridDim.x * blockDim.x;
         const uint32_t lane = threadIdx.x & 31u;
         const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
