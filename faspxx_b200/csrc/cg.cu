@@ -355,7 +355,8 @@ __device__ __forceinline__ float4 f4shift(const float4& a, const float4& b, int 
 // owned row (half the gathers). Its rounding differs from A p by a term that beta < 1 damps;
 // the FP64 refreshes of reliable updates correct the residual it feeds.
 // Blocks per SM: FP32 6 (40 registers), one-reduction FP32 5 (its extra sums spill under
-// 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4.
+// 40 registers and the spills cost more than the sixth block), FP64 5, lanes 4, vector rows
+// 3 (80 registers; 4 blocks at 64 registers spilled and measured slower).
 // V4 (stencil masks of at most 8 offsets): consecutive rows per thread with 16-byte loads,
 // four for the FP32 recurrences, two for FP64 (REC = 0, fixed shapes only); the host checks
 // n % 4 (FP64: n % 2) == 0, a square matrix and 16-byte aligned vectors (8- or 4-byte
