@@ -82,6 +82,11 @@ SIGNATURES = {
     "fasp_gpu_mat_rowclass_info": (_i, [_vp, _P(_i), _P(_u32), _P(_u32), _P(_u32)]),
     "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _i, _P(_d)]),
     "fasp_gpu_mat_sampled_outer": (_i, [_vp, _vp, _vp, _d, _vp]),
+    "fasp_gpu_mat_mult_transpose_add": (_i, [_vp, _vp, _vp, _vp]),
+    "fasp_gpu_mat_apply_async": (_i, [_vp, _vp, _vp, _vp]),
+    "fasp_gpu_mat_residual_async": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "fasp_gpu_mat_mult_transpose_add_async": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "fasp_gpu_mat_sampled_outer_async": (_i, [_vp, _vp, _vp, _d, _vp, _vp]),
     "fasp_gpu_vec_dot": (_i, [_u32, _vp, _vp, _P(_d)]),
     "fasp_gpu_vec_norm2": (_i, [_u32, _vp, _P(_d)]),
     "fasp_gpu_vec_norminf": (_i, [_u32, _vp, _P(_d)]),
@@ -91,20 +96,31 @@ SIGNATURES = {
     "fasp_gpu_vec_waxpby": (_i, [_u32, _d, _vp, _d, _vp, _vp]),
     "fasp_gpu_vec_scale": (_i, [_u32, _d, _vp]),
     "fasp_gpu_vec_dot_noalloc": (_i, [_u32, _vp, _vp, _P(_d)]),
+    "fasp_gpu_vec_dot_async": (_i, [_u32, _vp, _vp, _vp, _vp]),
+    "fasp_gpu_vec_norm2_async": (_i, [_u32, _vp, _vp, _vp]),
+    "fasp_gpu_vec_norminf_async": (_i, [_u32, _vp, _vp, _vp]),
+    "fasp_gpu_vec_axpy_async": (_i, [_u32, _d, _vp, _vp, _vp]),
+    "fasp_gpu_vec_xpay_async": (_i, [_u32, _d, _vp, _vp, _vp]),
+    "fasp_gpu_vec_axpby_async": (_i, [_u32, _d, _d, _vp, _vp, _vp]),
+    "fasp_gpu_vec_waxpby_async": (_i, [_u32, _d, _vp, _d, _vp, _vp, _vp]),
+    "fasp_gpu_vec_scale_async": (_i, [_u32, _d, _vp, _vp]),
     "fasp_gpu_solver_create": (_i, [_P(Config), _P(_vp)]),
     "fasp_gpu_solver_setup": (_i, [_vp, _vp]),
     "fasp_gpu_solver_set_mg_transfer": (_i, [_vp, _u32, _vp, _vp, _vp]),
     "fasp_gpu_solver_solve": (_i, [_vp, _vp, _vp, _P(Info)]),
     "fasp_gpu_solver_solve_host": (_i, [_vp, _vp, _vp, _P(Info)]),
+    "fasp_gpu_solver_solve_async": (_i, [_vp, _vp, _vp, _P(Info), _vp]),
     "fasp_gpu_solver_history": (_i, [_vp, _vp, _u32, _P(_u32)]),
     "fasp_gpu_solver_clean": (_i, [_vp]),
     "fasp_gpu_solver_destroy": (_i, [_vp]),
     "fasp_gpu_solver_last_time": (_i, [_vp, _P(_d)]),
     "fasp_gpu_solver_kernel_times": (_i, [_vp, _u32, _i, _P(_d)]),
     "fasp_gpu_solver_solve_adjoint": (_i, [_vp, _vp, _vp, _P(Info)]),
+    "fasp_gpu_solver_solve_adjoint_async": (_i, [_vp, _vp, _vp, _P(Info), _vp]),
     "fasp_gpu_batch_create": (_i, [_u32, _vp, _u32, _vp, _vp, _vp, _u32, _P(_vp)]),
     "fasp_gpu_batch_set_shape": (_i, [_vp, _i, _i]),
     "fasp_gpu_batch_solve": (_i, [_vp, _vp, _vp, _d, _u32, _i, _d, _vp, _vp]),
+    "fasp_gpu_batch_solve_async": (_i, [_vp, _vp, _vp, _d, _u32, _i, _d, _vp, _vp, _vp]),
     "fasp_gpu_batch_last_time": (_i, [_vp, _P(_d)]),
     "fasp_gpu_batch_destroy": (_i, [_vp]),
 }

@@ -105,8 +105,12 @@ __global__ void __launch_bounds__(512) batch_pcg(BatchArgs<T> a)
         uint32_t it = 0;
         int par = 0;
         double last[NR];
+        uint32_t itk[NR]; // each right-hand side's own count: the iteration that stopped it
 #pragma unroll
-        for (int k = 0; k < NR; ++k) last[k] = 1.0;
+        for (int k = 0; k < NR; ++k) {
+            last[k] = 1.0;
+            itk[k] = 0;
+        }
         while (nact > 0 && it < a.maxIter) {
             ++it;
             const T* pOld = par ? a.p1 : a.p0;
@@ -182,6 +186,7 @@ __global__ void __launch_bounds__(512) batch_pcg(BatchArgs<T> a)
                 last[k] = res;
                 if (res < tol[k] || !(sh[NR + k] == sh[NR + k])) {
                     active[k] = false;
+                    itk[k] = it;
                 } else {
                     beta[k] = sh[NR + k] / rz[k];
                     rz[k] = sh[NR + k];
@@ -190,11 +195,13 @@ __global__ void __launch_bounds__(512) batch_pcg(BatchArgs<T> a)
             }
             par ^= 1;
         }
-        if (threadIdx.x < NR) {
-            const int k = threadIdx.x;
-            a.iters[(size_t)sys * a.nrhs + k] += it;
-            a.resRel[(size_t)sys * a.nrhs + k] = tol[k] > 0 ? last[k] * a.relTol / tol[k] : 0.0;
-        }
+#pragma unroll
+        for (int k = 0; k < NR; ++k)
+            if (threadIdx.x == k) {
+                a.iters[(size_t)sys * a.nrhs + k] += active[k] ? it : itk[k];
+                a.resRel[(size_t)sys * a.nrhs + k] =
+                    tol[k] > 0 ? last[k] * a.relTol / tol[k] : 0.0;
+            }
     }
 }
 
@@ -218,9 +225,10 @@ __global__ void __launch_bounds__(512) batch_pcg_rel(BatchArgs<float> a, BatchRe
     // per right-hand side scalars, uniform across the block: thread 0 updates them after
     // each block reduction, the others read them after the barrier
     struct Rhs {
-        double rz, rzold, beta, rmax, res, true0, prev, sc, pq;
-        float  alpha;
-        int    active, fresh, stall, trig;
+        double   rz, rzold, beta, rmax, res, true0, prev, sc, pq;
+        float    alpha;
+        int      active, fresh, stall, trig;
+        unsigned its; // the iteration that stopped this right-hand side
     };
     __shared__ Rhs st[kMaxRhs];
     __shared__ unsigned item;
@@ -257,6 +265,7 @@ __global__ void __launch_bounds__(512) batch_pcg_rel(BatchArgs<float> a, BatchRe
                     st[k].fresh = 1; // the next p is z (first iteration, or after a restart)
                     st[k].stall = 0;
                     st[k].beta = 0.0;
+                    st[k].its = 0;
                 }
             __syncthreads();
         }
@@ -440,6 +449,7 @@ __global__ void __launch_bounds__(512) batch_pcg_rel(BatchArgs<float> a, BatchRe
                         }
                         if (tr < a.relTol * st[k].true0 || !(tr == tr) || st[k].stall >= 3) {
                             st[k].active = 0;
+                            st[k].its = it;
                             st[k].res = tr / st[k].sc;
                         } else {
                             const double rs = sqrt(rr[NR + k]);
@@ -474,7 +484,7 @@ __global__ void __launch_bounds__(512) batch_pcg_rel(BatchArgs<float> a, BatchRe
             }
         if (threadIdx.x < NR) {
             const int k = threadIdx.x;
-            a.iters[(size_t)sys * a.nrhs + k] += it;
+            a.iters[(size_t)sys * a.nrhs + k] += st[k].active ? it : st[k].its;
             a.resRel[(size_t)sys * a.nrhs + k] =
                 st[k].true0 > 0 ? st[k].res * st[k].sc / st[k].true0 : 0.0;
         }
@@ -604,9 +614,7 @@ int fasp_gpu_batch_create(uint32_t count, const uint32_t* sysRow, uint32_t nnz,
     const uint32_t N = hs[count];
     fasp_gpu_batch h = new (std::nothrow) fasp_gpu_batch_s();
     if (!h) return kErrAlloc;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int e = h->c.init(dev);
+    int e = h->c.init(library_device());
     // the matrix upload validates the structure (CheckCSR) before any kernel reads it
     if (!e) e = m_upload(h->M, N, N, nnz, rowPtr, colInd, values, false, h->c.stream);
     if (!e) {
@@ -777,11 +785,26 @@ int fasp_gpu_batch_solve(fasp_gpu_batch h, const double* b, double* x, double re
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     if (!e && cudaGetLastError() != cudaSuccess) e = kErrCuda;
-    if (!e && iters)
-        e = cudaMemcpy(iters, B.iters, (size_t)cnt * nr * 4, cudaMemcpyDeviceToHost) ? kErrCuda : kOk;
-    if (!e && resRel)
-        e = cudaMemcpy(resRel, B.resRel, (size_t)cnt * nr * 8, cudaMemcpyDeviceToHost) ? kErrCuda : kOk;
+    if (!e && iters &&
+        cudaMemcpyAsync(iters, B.iters, (size_t)cnt * nr * 4, cudaMemcpyDeviceToHost, B.c.stream))
+        e = kErrCuda;
+    if (!e && resRel &&
+        cudaMemcpyAsync(resRel, B.resRel, (size_t)cnt * nr * 8, cudaMemcpyDeviceToHost,
+                        B.c.stream))
+        e = kErrCuda;
+    if (!e && cudaStreamSynchronize(B.c.stream) != cudaSuccess) e = kErrCuda;
     return e;
+}
+
+int fasp_gpu_batch_solve_async(fasp_gpu_batch h, const double* b, double* x, double relTol,
+                               uint32_t maxIter, int precision, double innerRelTol,
+                               uint32_t* iters, double* resRel, fasp_gpu_stream stream)
+{
+    if (!h) return kErrInputPar;
+    return on_stream(h->c, reinterpret_cast<cudaStream_t>(stream), [&]() {
+        return fasp_gpu_batch_solve(h, b, x, relTol, maxIter, precision, innerRelTol, iters,
+                                    resRel);
+    });
 }
 
 int fasp_gpu_batch_last_time(fasp_gpu_batch h, double* ms)

@@ -33,6 +33,11 @@ int Ctx::init(int device)
 void Ctx::destroy()
 {
     if (stream) cudaStreamSynchronize(stream);
+    for (cudaEvent_t& ev : joinEv)
+        if (ev) {
+            cudaEventDestroy(ev);
+            ev = nullptr;
+        }
     cudaFree(red.partials);
     cudaFree(red.ticket);
     cudaFree(dslot);
@@ -42,6 +47,24 @@ void Ctx::destroy()
     dslot = nullptr;
     hslot = nullptr;
     stream = nullptr;
+}
+
+int Ctx::join_from(cudaStream_t user)
+{
+    if (user == stream) return kOk;
+    if (!joinEv[0]) FB_CUDA(cudaEventCreateWithFlags(&joinEv[0], cudaEventDisableTiming));
+    FB_CUDA(cudaEventRecord(joinEv[0], user));
+    FB_CUDA(cudaStreamWaitEvent(stream, joinEv[0], 0));
+    return kOk;
+}
+
+int Ctx::join_to(cudaStream_t user)
+{
+    if (user == stream) return kOk;
+    if (!joinEv[1]) FB_CUDA(cudaEventCreateWithFlags(&joinEv[1], cudaEventDisableTiming));
+    FB_CUDA(cudaEventRecord(joinEv[1], stream));
+    FB_CUDA(cudaStreamWaitEvent(user, joinEv[1], 0));
+    return kOk;
 }
 
 int Ctx::sync()
@@ -62,6 +85,10 @@ int Ctx::fetch(int slot, double* out)
 
 static int g_device = 0;
 
+namespace fb {
+int library_device() { return g_device; }
+} // namespace fb
+
 // Per-thread context for the stand-alone VEC entry points.
 static Ctx* vec_ctx(int* err)
 {
@@ -76,6 +103,18 @@ static Ctx* vec_ctx(int* err)
     *err = c->init(g_device);
     cdev = g_device;
     return c;
+}
+
+static cudaStream_t user_stream(fasp_gpu_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Stream-ordered VEC operations on the calling thread's context.
+template <typename F>
+static int vec_async(fasp_gpu_stream st, F&& work)
+{
+    int err = 0;
+    Ctx* c = vec_ctx(&err);
+    if (err) return err;
+    return on_stream(*c, user_stream(st), [&]() { return work(*c); });
 }
 
 // A handle whose matrix is built by `build` on the handle's own stream.
@@ -362,6 +401,48 @@ int fasp_gpu_mat_residual(fasp_gpu_mat A, const double* b, const double* x, doub
     return A->c.sync();
 }
 
+// A's exact transpose, built once and cached on the handle (adjoint solves and
+// MultTransposeAdd share it).
+static int cached_transpose(fasp_gpu_mat A)
+{
+    if (A->T) return kOk;
+    return fasp_gpu_mat_transpose(A, &A->T);
+}
+
+int fasp_gpu_mat_mult_transpose_add(fasp_gpu_mat A, const double* v1, const double* v2,
+                                    double* v)
+{
+    if (!A || !v1 || !v2 || !v) return kErrInputPar;
+    int e = cached_transpose(A);
+    if (!e) e = m_mult_transpose_add(A->c, A->T->M, v1, v2, v);
+    if (e) return e;
+    return A->c.sync();
+}
+
+int fasp_gpu_mat_apply_async(fasp_gpu_mat A, const double* v, double* w, fasp_gpu_stream st)
+{
+    if (!A || !v || !w) return kErrInputPar;
+    return on_stream(A->c, user_stream(st), [&]() { return m_spmv(A->c, A->M, v, w); });
+}
+
+int fasp_gpu_mat_residual_async(fasp_gpu_mat A, const double* b, const double* x, double* r,
+                                fasp_gpu_stream st)
+{
+    if (!A || !b || !x || !r) return kErrInputPar;
+    return on_stream(A->c, user_stream(st),
+                     [&]() { return m_residual(A->c, A->M, b, x, r, nullptr); });
+}
+
+int fasp_gpu_mat_mult_transpose_add_async(fasp_gpu_mat A, const double* v1, const double* v2,
+                                          double* v, fasp_gpu_stream st)
+{
+    if (!A || !v1 || !v2 || !v) return kErrInputPar;
+    int e = cached_transpose(A);
+    if (e) return e;
+    return on_stream(A->c, user_stream(st),
+                     [&]() { return m_mult_transpose_add(A->c, A->T->M, v1, v2, v); });
+}
+
 int fasp_gpu_mat_transpose(fasp_gpu_mat A, fasp_gpu_mat* out)
 {
     if (!A || !out) return kErrInputPar;
@@ -460,6 +541,14 @@ int fasp_gpu_mat_sampled_outer(fasp_gpu_mat A, const double* lam, const double* 
     return A->c.sync();
 }
 
+int fasp_gpu_mat_sampled_outer_async(fasp_gpu_mat A, const double* lam, const double* x,
+                                     double scale, double* dA, fasp_gpu_stream st)
+{
+    if (!A || !lam || !x || !dA) return kErrInputPar;
+    return on_stream(A->c, user_stream(st),
+                     [&]() { return m_sampled_outer(A->c, A->M, lam, x, scale, dA); });
+}
+
 // ---- VEC ------------------------------------------------------------------------------
 
 static int vec_reduce(int which, uint32_t n, const double* a, const double* b, double* result)
@@ -501,6 +590,46 @@ int fasp_gpu_vec_waxpby(uint32_t n, double a, const double* v1, double b, const 
     VEC_CALL(v_waxpby(*c, n, Scal::h(a), v1, Scal::h(b), v2, w))
 }
 int fasp_gpu_vec_scale(uint32_t n, double a, double* x) { VEC_CALL(v_scale(*c, n, Scal::h(a), x)) }
+
+int fasp_gpu_vec_dot_async(uint32_t n, const double* a, const double* b, double* dres,
+                           fasp_gpu_stream st)
+{
+    if (!dres) return kErrInputPar;
+    return vec_async(st, [&](Ctx& c) { return v_dot(c, n, a, b, dres); });
+}
+int fasp_gpu_vec_norm2_async(uint32_t n, const double* a, double* dres, fasp_gpu_stream st)
+{
+    if (!dres) return kErrInputPar;
+    return vec_async(st, [&](Ctx& c) { return v_norm2(c, n, a, dres); });
+}
+int fasp_gpu_vec_norminf_async(uint32_t n, const double* a, double* dres, fasp_gpu_stream st)
+{
+    if (!dres) return kErrInputPar;
+    return vec_async(st, [&](Ctx& c) { return v_norminf(c, n, a, dres); });
+}
+int fasp_gpu_vec_axpy_async(uint32_t n, double a, const double* x, double* y, fasp_gpu_stream st)
+{
+    return vec_async(st, [&](Ctx& c) { return v_axpy(c, n, Scal::h(a), x, y); });
+}
+int fasp_gpu_vec_xpay_async(uint32_t n, double a, const double* x, double* y, fasp_gpu_stream st)
+{
+    return vec_async(st, [&](Ctx& c) { return v_xpay(c, n, Scal::h(a), x, y); });
+}
+int fasp_gpu_vec_axpby_async(uint32_t n, double a, double b, const double* y, double* x,
+                             fasp_gpu_stream st)
+{
+    return vec_async(st, [&](Ctx& c) { return v_axpby(c, n, Scal::h(a), Scal::h(b), y, x); });
+}
+int fasp_gpu_vec_waxpby_async(uint32_t n, double a, const double* v1, double b, const double* v2,
+                              double* w, fasp_gpu_stream st)
+{
+    return vec_async(st,
+                     [&](Ctx& c) { return v_waxpby(c, n, Scal::h(a), v1, Scal::h(b), v2, w); });
+}
+int fasp_gpu_vec_scale_async(uint32_t n, double a, double* x, fasp_gpu_stream st)
+{
+    return vec_async(st, [&](Ctx& c) { return v_scale(c, n, Scal::h(a), x); });
+}
 
 // ---- SOL ------------------------------------------------------------------------------
 
@@ -557,6 +686,13 @@ int fasp_gpu_solver_solve(fasp_gpu_solver s, const double* b, double* x, fasp_gp
 {
     if (!s || !b || !x) return kErrInputPar;
     return s->s.solve(b, x, info);
+}
+
+int fasp_gpu_solver_solve_async(fasp_gpu_solver s, const double* b, double* x,
+                                fasp_gpu_info* info, fasp_gpu_stream st)
+{
+    if (!s || !b || !x) return kErrInputPar;
+    return on_stream(s->s.c, user_stream(st), [&]() { return s->s.solve(b, x, info); });
 }
 
 int fasp_gpu_solver_solve_host(fasp_gpu_solver s, const double* b, double* x, fasp_gpu_info* info)
@@ -624,23 +760,20 @@ int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, int flushL2, 
     return kErrSolverType;
 }
 
-int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* lam,
-                                  fasp_gpu_info* info)
+// The adjoint solver: a solver of s's configuration bound to the cached exact transpose.
+static int adjoint_solver(fasp_gpu_solver s)
 {
-    if (!s || !g || !lam || !s->s.Ah) return kErrInputPar;
     SolverImpl& S = s->s;
     fasp_gpu_mat Ah = S.Ah;
-    if (!Ah->T) {
-        // MAT::TransInPlace into a handle cached on (and destroyed with) the matrix
-        int e = fasp_gpu_mat_transpose(Ah, &Ah->T);
-        if (e) return e;
-    }
+    // MAT::TransInPlace into a handle cached on (and destroyed with) the matrix
+    int e = cached_transpose(Ah);
+    if (e) return e;
     if (!S.adj) {
         // a solver of the same configuration bound to A^T
         S.adj = new (std::nothrow) SolverImpl();
         if (!S.adj) return kErrAlloc;
         S.adj->cfg = S.cfg;
-        int e = S.adj->c.init(g_device);
+        e = S.adj->c.init(g_device);
         if (!e) e = S.adj->setup(Ah->T);
         if (e) {
             S.adj->destroy();
@@ -650,8 +783,30 @@ int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* la
             return e;
         }
     }
-    const int e = S.adj->solve(g, lam, info);
+    return kOk;
+}
+
+int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* lam,
+                                  fasp_gpu_info* info)
+{
+    if (!s || !g || !lam || !s->s.Ah) return kErrInputPar;
+    SolverImpl& S = s->s;
+    int e = adjoint_solver(s);
+    if (e) return e;
+    e = S.adj->solve(g, lam, info);
     S.lastMs = S.adj->lastMs; // last_time reports the most recent solve, adjoint included
+    return e;
+}
+
+int fasp_gpu_solver_solve_adjoint_async(fasp_gpu_solver s, const double* g, double* lam,
+                                        fasp_gpu_info* info, fasp_gpu_stream st)
+{
+    if (!s || !g || !lam || !s->s.Ah) return kErrInputPar;
+    SolverImpl& S = s->s;
+    int e = adjoint_solver(s);
+    if (e) return e;
+    e = on_stream(S.adj->c, user_stream(st), [&]() { return S.adj->solve(g, lam, info); });
+    S.lastMs = S.adj->lastMs;
     return e;
 }
 

@@ -68,22 +68,48 @@ struct Ctx {
     double*      dslot = nullptr;  // device scalars [kSlots]
     double*      hslot = nullptr;  // pinned host mirror [kSlots]
     unsigned long long launches = 0; // kernels launched on this context
+    cudaEvent_t  joinEv[2] = {nullptr, nullptr}; // stream-ordering events (created on use)
     int init(int device);
     void destroy();
+    // Stream ordering with a caller's stream (the _async entry points): join_from makes this
+    // context's stream wait for all work enqueued on `user` so far; join_to makes `user` wait
+    // for all work enqueued on this context's stream so far. No-ops when user == stream.
+    int  join_from(cudaStream_t user);
+    int  join_to(cudaStream_t user);
     // fixed-size grids (reductions depend on them): at most perSM blocks per SM
     int  grid(long long work, int perBlock, int perSM = 8) const;
     int  sync();
     int  fetch(int slot, double* out);               // read one device scalar (synchronous)
 };
 
+// The device chosen by fasp_gpu_init (capi.cu).
+int library_device();
+
+// Runs `work` (which enqueues on c.stream) ordered after everything the caller enqueued on
+// `user` before the call, and orders the caller's later work on `user` after it.
+template <typename F>
+int on_stream(Ctx& c, cudaStream_t user, F&& work)
+{
+    int e = c.join_from(user);
+    if (!e) e = work();
+    const int j = c.join_to(user);
+    return e ? e : j;
+}
+
 // Blocks of `fn` at `block` threads that are resident at once on the whole device (one
 // wave): SM count x the occupancy limit (registers, shared memory), capped at kMaxGrid.
 // Grid-stride kernels launched with min(work, this) never run a partial second wave.
 int resident_grid(const Ctx& c, const void* fn, int block);
 
+// Reads `bytes` of `buf` (a multiple of 16) through L2 on stream s and writes nothing (blas.cu):
+// after a read of more than the L2's 126 MB, L2 holds only clean lines of buf, so a kernel
+// timed next reads its inputs from HBM without paying to write back dirty lines first.
+int l2_flush_read(Ctx& c, const void* buf, size_t bytes);
+
 // Average device time (ms) of one call of `launch` over reps calls. flushL2 = 0: the calls
 // run back to back between two events. flushL2 = 1: each call is timed alone with events
-// after a 256 MB write that evicts L2 (126 MB), so its inputs come from HBM.
+// after a 256 MB read that evicts L2 (126 MB) and leaves it clean, so its inputs come from
+// HBM and no write-back of dirty lines lands in the timed launch.
 template <typename F>
 int time_launches(Ctx& c, unsigned reps, int flushL2, F&& launch, double* ms)
 {
@@ -93,13 +119,14 @@ int time_launches(Ctx& c, unsigned reps, int flushL2, F&& launch, double* ms)
         cudaGetLastError();
         return kErrAlloc;
     }
+    if (flushL2) cudaMemsetAsync(flush, 0, fbytes, c.stream);
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     double tot = 0.0;
     int e = kOk;
     for (unsigned i = 0; i < (flushL2 ? reps : 1u); ++i) {
-        if (flushL2) cudaMemsetAsync(flush, (int)(i & 0xff), fbytes, c.stream);
+        if (flushL2) l2_flush_read(c, flush, fbytes);
         cudaEventRecord(t0, c.stream);
         for (unsigned k = 0; k < (flushL2 ? 1u : reps); ++k)
             if ((e = launch())) break;
@@ -279,6 +306,8 @@ int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r
 int m_residual(Ctx& c, const Mat& A, const float* b, const float* x, float* r,
                const double* xinf);
 int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR -> CSC, exact
+// v = A^T v1 + v2 on T = m_transpose(A), in MAT::MultTransposeAdd's order (MAT.cxx:541-606)
+int m_mult_transpose_add(Ctx& c, const Mat& T, const double* v1, const double* v2, double* v);
 int lanes_for(double meanRowLen);                                         // SpMV mapping
 int m_autotune(Ctx& c, Mat& A);
 // dA[k] = scale * lam[row(k)] * x[col(k)] on the sparsity pattern (sampled outer product)

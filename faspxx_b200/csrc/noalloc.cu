@@ -2,23 +2,27 @@
 // that must not allocate device memory.
 //
 // fasp_gpu_vec_dot creates a per-thread context on first use (a stream, reduction scratch,
-// pinned host memory). Some callers cannot do that: code that runs while another thread
-// captures a CUDA graph in global mode (cudaMalloc is then illegal), code running under a
-// framework whose memory pool has reserved the device memory, and latency-critical loops
-// in which cudaMalloc/cudaFree would synchronize the device. This variant keeps its scratch
-// in a file-scope device array instead, created with the module and held by every GPU that
-// loads the library until the process exits:
+// pinned host memory). Some callers cannot do that: an application whose memory pool has
+// reserved the device memory up front and forbids further driver allocations, and
+// latency-critical loops in which cudaMalloc/cudaFree would synchronize the device. This
+// variant keeps its scratch in a file-scope device array instead, created with the module
+// and held by every GPU that loads the library until the process exits:
 //   - one partial sum per block (kNoAllocMaxBlocks doubles), a block ticket and the result,
 //     about 32 KB in all;
 //   - each block sums a fixed chunk of kNoAllocChunk elements, so n is limited to
 //     kNoAllocMaxBlocks * kNoAllocChunk = 8,388,608; larger n returns ERROR_VEC_SIZE (-14)
 //     without touching the GPU.
-// Every call shares that one array and leaves its contents behind: the ticket is cleared
-// at the start of each call, the partials and the result are overwritten. Calls whose work
+// It runs on the device chosen by fasp_gpu_init (the calling thread's current device is
+// switched to it for the call and restored afterwards), on that device's legacy default
+// stream, and blocks until the result has been copied to the host.
+// Every call shares the one array and leaves its contents behind: the ticket is cleared at
+// the start of each call, the partials and the result are overwritten. Calls whose work
 // overlaps on the GPU (several host threads, or device work still running from an earlier
 // call on another stream) race on the array; callers must serialise them.
 // The first call on each device looks up the array's device address (cudaGetSymbolAddress)
-// with that device current; make that first call before any stream capture begins.
+// with that device current and keeps it for later calls; make that first call before any
+// stream capture begins. The kept address does not survive cudaDeviceReset (the module is
+// reloaded and the array may move): do not use this entry point after a device reset.
 #include <mutex>
 
 #include "../../include/fasp_b200.h"
@@ -121,14 +125,32 @@ extern "C" int fasp_gpu_vec_dot_noalloc(uint32_t n, const double* a, const doubl
         *result = 0.0;
         return kOk;
     }
+    // run on the library's device; the caller's current device is restored on return
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrNoDevice;
+    }
+    const int dev = library_device();
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return kErrNoDevice;
+    }
     int err = kOk;
     NoAllocScratch* s = scratch_for_current_device(&err);
-    if (!s) return err;
-    const int grid = (int)((n + kNoAllocChunk - 1) / kNoAllocChunk);
-    // legacy default stream: ordered after the caller's earlier default-stream work
-    FB_CUDA(cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned), 0));
-    k_dot_noalloc<<<grid, kNoAllocBlock, 0, 0>>>(n, a, b, s);
-    FB_CUDA(cudaGetLastError());
-    FB_CUDA(cudaMemcpy(result, &s->result, sizeof(double), cudaMemcpyDeviceToHost));
-    return kOk;
+    if (s) {
+        const int grid = (int)((n + kNoAllocChunk - 1) / kNoAllocChunk);
+        // legacy default stream: ordered after the caller's earlier default-stream work
+        if (cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned), 0) != cudaSuccess) err = kErrCuda;
+        if (!err) {
+            k_dot_noalloc<<<grid, kNoAllocBlock, 0, 0>>>(n, a, b, s);
+            if (cudaGetLastError() != cudaSuccess) err = kErrCuda;
+        }
+        if (!err && cudaMemcpy(result, &s->result, sizeof(double), cudaMemcpyDeviceToHost) !=
+                        cudaSuccess)
+            err = kErrCuda;
+        if (err) cudaGetLastError();
+    }
+    if (prev != dev) cudaSetDevice(prev);
+    return err;
 }

@@ -787,6 +787,50 @@ int m_sampled_outer(Ctx& c, const Mat& A, const double* lam, const double* x, do
     return kOk;
 }
 
+// ---- MAT::MultTransposeAdd: v = A^T v1 + v2 (MAT.cxx:541-606) ---------------------------
+// T is A's exact transpose (m_transpose, the order of MAT::TransInPlace). As the reference,
+// each v[i] starts from v2[i] and adds the products of row i of T left to right, each
+// product rounded before the add (no fused multiply-add), so the results are the
+// reference's bit for bit wherever its loop bounds are right (structurally symmetric A).
+// Pattern-only matrices count every stored entry as 1, as MAT::Apply does; a grid operator
+// walks its stencil points in ascending offset, which is its CSR order.
+template <bool GRID, bool PAT>
+__global__ void k_mult_transpose_add(CSRView<double> T, const double* __restrict__ v1,
+                                     const double* __restrict__ v2, double* __restrict__ v)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < T.nrow;
+         i += (size_t)gridDim.x * blockDim.x) {
+        double acc = v2[i];
+        if (GRID) {
+            const uint32_t m = grid_mask(T, (uint32_t)i);
+            for (uint32_t k = 0; k < T.ulen; ++k)
+                if ((m >> k) & 1u)
+                    acc = __dadd_rn(acc, __dmul_rn(v1[(long long)i + T.udelta[k]], T.uval[k]));
+        } else {
+            const uint32_t b = T.rowPtr[i], e = T.rowPtr[i + 1];
+            for (uint32_t k = b; k < e; ++k)
+                acc = __dadd_rn(acc, PAT ? v1[T.colInd[k]]
+                                         : __dmul_rn(v1[T.colInd[k]], T.val[k]));
+        }
+        v[i] = acc;
+    }
+}
+
+int m_mult_transpose_add(Ctx& c, const Mat& T, const double* v1, const double* v2, double* v)
+{
+    if (T.nrow == 0) return kOk;
+    const int g = std::max(1, std::min(ceil_div(T.nrow, kBlock), c.nsm * 8));
+    CSRView<double> V = T.view<double>(T.val, nullptr);
+    if (T.grid)
+        k_mult_transpose_add<true, false><<<g, kBlock, 0, c.stream>>>(V, v1, v2, v);
+    else if (!T.val)
+        k_mult_transpose_add<false, true><<<g, kBlock, 0, c.stream>>>(V, v1, v2, v);
+    else
+        k_mult_transpose_add<false, false><<<g, kBlock, 0, c.stream>>>(V, v1, v2, v);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
 // ---- structured-grid (matrix-free) operators --------------------------------------------
 // The GPU counterpart of the reference's matrix-free LOP example (example/TestMatFree.cxx:
 // 26-176): y = A x on an nx x ny x nz grid with a constant-coefficient stencil, Dirichlet

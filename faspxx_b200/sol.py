@@ -179,6 +179,12 @@ class MAT:
     def Residual(self, b: DVec, x: DVec, r: DVec) -> None:
         check(lib.fasp_gpu_mat_residual(self.h, b.ptr, x.ptr, r.ptr), "Residual")
 
+    def MultTransposeAdd(self, v1: DVec, v2: DVec, v: DVec) -> None:
+        """MAT::MultTransposeAdd (src/MAT.cxx:541-606): v = A^T v1 + v2 on the cached exact
+        transpose, in the reference's operation order."""
+        check(lib.fasp_gpu_mat_mult_transpose_add(self.h, v1.ptr, v2.ptr, v.ptr),
+              "MultTransposeAdd")
+
     def SetRowClass(self, mode) -> None:
         """Matrix form of the SpMV kernels: 0/False = CSR, 1 = row classes, 2/True = row
         classes with stencil masks (the default when built)."""

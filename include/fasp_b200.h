@@ -11,6 +11,16 @@
  *
  * Threading: one handle per host thread. All device work of a handle runs on the handle's
  * own CUDA stream; calls that return results block until they are ready.
+ *
+ * Streams: every call that enqueues device work per operation or per solve has an _async
+ * form that takes the caller's CUDA stream (fasp_gpu_stream, the runtime's cudaStream_t).
+ * It orders its device work after all work the caller enqueued on that stream before the
+ * call, and orders all work the caller enqueues on the stream after the call after it, with
+ * two events and no device-wide synchronisation; the handle's own stream still runs the work
+ * (its reduction scratch and control blocks belong to it). Operator and VEC forms return
+ * once the work is enqueued (reductions then write their result to DEVICE memory); solver
+ * forms return once the solve has finished on the device (the solvers decide convergence
+ * from device scalars) and fill info as the blocking forms do.
  */
 #ifndef FASP_B200_H
 #define FASP_B200_H
@@ -109,6 +119,9 @@ typedef struct {
 
 typedef struct fasp_gpu_mat_s*    fasp_gpu_mat;
 typedef struct fasp_gpu_solver_s* fasp_gpu_solver;
+/* A CUDA stream: the same type as the CUDA runtime's cudaStream_t (struct CUstream_st*), so
+ * a cudaStream_t passes unchanged; NULL is the legacy default stream. */
+typedef struct CUstream_st*       fasp_gpu_stream;
 
 /* ---- library ------------------------------------------------------------------------ */
 int         fasp_gpu_init(int device);              /* select the device; checks sm_100 */
@@ -199,6 +212,18 @@ int fasp_gpu_mat_apply(fasp_gpu_mat A, const double* v, double* w);
 int fasp_gpu_mat_residual(fasp_gpu_mat A, const double* b, const double* x, double* r);
 /* MAT::TransInPlace (MAT.cxx:479-538) into a new handle; structure and order bit-exact. */
 int fasp_gpu_mat_transpose(fasp_gpu_mat A, fasp_gpu_mat* out);
+/* MAT::MultTransposeAdd, v = A^T v1 + v2 (MAT.cxx:541-606), device vectors: v1 has nrow
+ * entries, v2 and v mcol. The transpose is formed once (MAT::TransInPlace's order, as
+ * fasp_gpu_mat_transpose) and cached on A -- the reference rebuilds it on every call. Each
+ * v[i] starts from v2[i] and adds the products of column i of A in ascending row order,
+ * each product rounded before the add: the reference's results bit for bit. The reference
+ * bounds each column by A's own rowPtr[i + 1] (MAT.cxx:603), which is right only when A's row
+ * pointers equal its transpose's (structurally symmetric A, every workload here); this
+ * function uses the transpose's own bounds for every A, rectangular included. Pattern-only
+ * matrices count each stored entry as 1 (as MAT::Apply; the reference reads its empty
+ * values array), grid operators their stencil. */
+int fasp_gpu_mat_mult_transpose_add(fasp_gpu_mat A, const double* v1, const double* v2,
+                                    double* v);
 /* MAT::GetDiag (MAT.cxx:256-267) into a device vector. */
 int fasp_gpu_mat_diag(fasp_gpu_mat A, double* diag);
 /* Rows-per-warp autotuner: times every lanes-per-row choice on A; returns the pick. */
@@ -227,6 +252,16 @@ int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2
  * matrix gradient dL/dA of x = A^-1 b is the case scale = -1 (no reference counterpart). */
 int fasp_gpu_mat_sampled_outer(fasp_gpu_mat A, const double* lam, const double* x,
                                double scale, double* dA);
+/* Stream-ordered forms of MAT::Apply, MAT::Residual, MAT::MultTransposeAdd and the sampled
+ * outer product (see Streams above): they return once the work is enqueued. The first
+ * MultTransposeAdd on a matrix forms its transpose synchronously. */
+int fasp_gpu_mat_apply_async(fasp_gpu_mat A, const double* v, double* w, fasp_gpu_stream stream);
+int fasp_gpu_mat_residual_async(fasp_gpu_mat A, const double* b, const double* x, double* r,
+                                fasp_gpu_stream stream);
+int fasp_gpu_mat_mult_transpose_add_async(fasp_gpu_mat A, const double* v1, const double* v2,
+                                          double* v, fasp_gpu_stream stream);
+int fasp_gpu_mat_sampled_outer_async(fasp_gpu_mat A, const double* lam, const double* x,
+                                     double scale, double* dA, fasp_gpu_stream stream);
 
 /* ---- VEC kernels on device vectors (src/VEC.cxx) ------------------------------------ */
 int fasp_gpu_vec_dot(uint32_t n, const double* a, const double* b, double* result);    /* :468 */
@@ -238,16 +273,36 @@ int fasp_gpu_vec_axpby(uint32_t n, double a, double b, const double* y, double* 
 int fasp_gpu_vec_waxpby(uint32_t n, double a, const double* v1, double b, const double* v2,
                         double* w);                                                    /* :329 */
 int fasp_gpu_vec_scale(uint32_t n, double a, double* x);                               /* :154 */
+/* Stream-ordered forms of the VEC operations above (see Streams): reductions write their
+ * FP64 result to the DEVICE address dres; all return once the work is enqueued. They run on
+ * the calling thread's VEC context, so calls from one thread are ordered among themselves. */
+int fasp_gpu_vec_dot_async(uint32_t n, const double* a, const double* b, double* dres,
+                           fasp_gpu_stream stream);
+int fasp_gpu_vec_norm2_async(uint32_t n, const double* a, double* dres, fasp_gpu_stream stream);
+int fasp_gpu_vec_norminf_async(uint32_t n, const double* a, double* dres,
+                               fasp_gpu_stream stream);
+int fasp_gpu_vec_axpy_async(uint32_t n, double a, const double* x, double* y,
+                            fasp_gpu_stream stream);
+int fasp_gpu_vec_xpay_async(uint32_t n, double a, const double* x, double* y,
+                            fasp_gpu_stream stream);
+int fasp_gpu_vec_axpby_async(uint32_t n, double a, double b, const double* y, double* x,
+                             fasp_gpu_stream stream);
+int fasp_gpu_vec_waxpby_async(uint32_t n, double a, const double* v1, double b,
+                              const double* v2, double* w, fasp_gpu_stream stream);
+int fasp_gpu_vec_scale_async(uint32_t n, double a, double* x, fasp_gpu_stream stream);
 /* No counterpart in the reference. The dot product of fasp_gpu_vec_dot for callers that
- * cannot allocate device memory (for example code running while a CUDA graph is being
- * captured in global mode, code under a memory pool that has reserved the device, or a
- * latency-critical loop where cudaMalloc/cudaFree would synchronize the device). It calls
- * no allocator: its reduction scratch (about 32 KB) is a static device array that every GPU
- * loading this library holds until exit. n is limited to 8,388,608 elements; larger n
- * returns ERROR_VEC_SIZE. Runs on the legacy default stream and blocks until *result (host)
- * is written. All calls share the one scratch array: calls that overlap on the GPU race and
- * must be serialised by the caller. The first call on each device sets up the array's
- * address with that device current; make it before any stream capture begins. */
+ * cannot allocate device memory (for example an application whose memory pool has reserved
+ * the device memory up front and forbids further driver allocations, or a latency-critical
+ * loop where cudaMalloc/cudaFree would synchronize the device). It calls no allocator: its
+ * reduction scratch (about 32 KB) is a static device array that every GPU loading this
+ * library holds until exit. n is limited to 8,388,608 elements; larger n returns
+ * ERROR_VEC_SIZE. It runs on the device chosen by fasp_gpu_init (from any host thread; the
+ * thread's current device is restored on return), on that device's legacy default stream,
+ * and blocks until *result (host) is written. All calls share the one scratch array: calls
+ * that overlap on the GPU race and must be serialised by the caller. The first call on each
+ * device looks up the array's address with that device current and keeps it; make it
+ * before any stream capture begins, and do not call this entry point after
+ * cudaDeviceReset (the kept address is then stale). */
 int fasp_gpu_vec_dot_noalloc(uint32_t n, const double* a, const double* b, double* result);
 
 /* ---- SOL: solvers (src/SOL.hxx and subclasses) -------------------------------------- */
@@ -271,6 +326,12 @@ int fasp_gpu_solver_set_mg_transfer(fasp_gpu_solver s, uint32_t level, fasp_gpu_
                                     fasp_gpu_mat R, fasp_gpu_mat Ac);
 /* Solve(b, x) on DEVICE vectors: x is the initial guess in, the solution out. */
 int fasp_gpu_solver_solve(fasp_gpu_solver s, const double* b, double* x, fasp_gpu_info* info);
+/* Solve(b, x) ordered on the caller's stream (see Streams): the solve starts after the
+ * caller's earlier work on `stream` (for example the kernel that forms b) and the caller's
+ * later work on `stream` starts after it, with no device-wide synchronisation. Returns once
+ * the solve has finished, with info filled. */
+int fasp_gpu_solver_solve_async(fasp_gpu_solver s, const double* b, double* x,
+                                fasp_gpu_info* info, fasp_gpu_stream stream);
 /* Solve(b, x) on HOST vectors: copies in, solves, copies out (end-to-end path). */
 int fasp_gpu_solver_solve_host(fasp_gpu_solver s, const double* b, double* x,
                                fasp_gpu_info* info);
@@ -294,6 +355,9 @@ int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, int flushL2, 
  * matrix (built once, cached). */
 int fasp_gpu_solver_solve_adjoint(fasp_gpu_solver s, const double* g, double* lam,
                                   fasp_gpu_info* info);
+/* The same, ordered on the caller's stream (see Streams). */
+int fasp_gpu_solver_solve_adjoint_async(fasp_gpu_solver s, const double* g, double* lam,
+                                        fasp_gpu_info* info, fasp_gpu_stream stream);
 
 /* ---- batched CG (no reference counterpart) ------------------------------------------ */
 /* count independent SPD systems solved by Jacobi-PCG in one persistent launch. The systems
@@ -317,6 +381,10 @@ int fasp_gpu_batch_set_shape(fasp_gpu_batch bt, int block, int blocksPerSM);
 int fasp_gpu_batch_solve(fasp_gpu_batch bt, const double* b, double* x, double relTol,
                          uint32_t maxIter, int precision, double innerRelTol,
                          uint32_t* iters, double* resRel);
+/* The same, ordered on the caller's stream (see Streams); returns once the batch is solved. */
+int fasp_gpu_batch_solve_async(fasp_gpu_batch bt, const double* b, double* x, double relTol,
+                               uint32_t maxIter, int precision, double innerRelTol,
+                               uint32_t* iters, double* resRel, fasp_gpu_stream stream);
 int fasp_gpu_batch_last_time(fasp_gpu_batch bt, double* ms);
 int fasp_gpu_batch_destroy(fasp_gpu_batch bt);
 

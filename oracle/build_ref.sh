@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
 # Builds _ref/liboracle_ref.so: the FASP++ reference solvers compiled from their own
-# source tree (default /root/reference, read-only) plus ref_shim.cxx, for use as a test
+# source tree (the first argument, else $FASPXX_REFERENCE, else the default below; read
+# only) plus ref_shim.cxx, for use as a test
 # oracle and as the timed CPU baseline. Sources are copied to a temporary directory, the
 # build-time fixes below are applied there, and only the shared library lands in _ref/.
 #   1. GMRES.cxx:214,224,386,396 / FGMRES.cxx:209,219: unsigned back-substitution loops
@@ -11,7 +12,7 @@
 # Compiled with -O2 -ffp-contract=off so that results are bit-comparable with the C
 # restatement (fasp_oracle.c), which is built with the same flags.
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${FASPXX_REFERENCE:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then

@@ -234,6 +234,38 @@ void orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* r
     if (tDiagPtr) orc_diagptr(m, tRowPtr, tColInd, tDiagPtr);
 }
 
+/* MAT::MultTransposeAdd, MAT.cxx:541-606: the transpose formed as TransInPlace forms it
+ * (:556-590), then v = v2 (:592) and v[i] += v1[col] * value over row i of the transpose in
+ * order (:595-605), each product rounded before the add. */
+int orc_mult_transpose_add(uint32_t nrow, uint32_t mcol, const uint32_t* rowPtr,
+                           const uint32_t* colInd, const double* values, const double* v1,
+                           const double* v2, double* v)
+{
+    const uint32_t nnz = rowPtr[nrow];
+    uint32_t* trp = (uint32_t*)calloc((size_t)mcol + 2, sizeof(uint32_t));
+    uint32_t* tci = (uint32_t*)malloc(((size_t)nnz + 1) * sizeof(uint32_t));
+    double*   tva = values ? (double*)malloc(((size_t)nnz + 1) * sizeof(double)) : NULL;
+    if (!trp || !tci || (values && !tva)) {
+        free(trp);
+        free(tci);
+        free(tva);
+        return -20;
+    }
+    orc_transpose(nrow, mcol, nnz, rowPtr, colInd, values, trp, tci, tva, NULL);
+    for (uint32_t i = 0; i < mcol; ++i) {
+        double acc = v2[i];
+        for (uint32_t j = trp[i]; j < trp[i + 1]; ++j) {
+            const double prod = v1[tci[j]] * (tva ? tva[j] : 1.0);
+            acc += prod;
+        }
+        v[i] = acc;
+    }
+    free(trp);
+    free(tci);
+    free(tva);
+    return 0;
+}
+
 /* ------------------------------------------------------------------------------------
  * ReadMat's conversions (src/ReadData.cxx:361-446, src/MATUtil.cxx:110-476)
  * ---------------------------------------------------------------------------------- */

@@ -87,6 +87,17 @@ double orc_norminf(uint32_t n, const double* a);
 void   orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* rowPtr,
                      const uint32_t* colInd, const double* values, uint32_t* tRowPtr,
                      uint32_t* tColInd, double* tValues, uint32_t* tDiagPtr);
+/* MAT::MultTransposeAdd (MAT.cxx:541-606): v = A^T v1 + v2 for A (nrow x mcol); v1 has
+ * nrow entries, v2 and v mcol. v starts as v2 and each v[i] adds the products of column i in
+ * the transpose's order (ascending row). The reference bounds each row of the transpose by
+ * A's own rowPtr[i + 1] (MAT.cxx:603); the restatement uses the transpose's row end, which
+ * is the same whenever A's row pointers equal its transpose's (structurally symmetric A).
+ * values == NULL: every stored entry counts as 1, as in MAT::Apply. Returns 0. The
+ * reference shim returns ORC_REF_UNDEFINED for nrow != mcol (its loop then reads past
+ * A's row pointers). */
+int    orc_mult_transpose_add(uint32_t nrow, uint32_t mcol, const uint32_t* rowPtr,
+                              const uint32_t* colInd, const double* values, const double* v1,
+                              const double* v2, double* v);
 /* MAT::FormDiagPtr */
 void   orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
                    uint32_t* diagPtr);

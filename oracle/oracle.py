@@ -47,9 +47,10 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
 def build(ref: bool = True) -> None:
-    """Compile the restatement (and the reference, when its tree is present)."""
+    """Compile the restatement and, with ref=True, the reference (build_ref.sh finds the
+    reference tree from FASPXX_REFERENCE or its own default and skips when it is absent)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle_port.so"], check=True)
-    if ref and os.path.isdir("/root/reference/src"):
+    if ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
@@ -233,6 +234,20 @@ def transpose(kind, mat):
 
 # ORC_REF_UNDEFINED (fasp_oracle.h): the reference indexes out of bounds on this input.
 REF_UNDEFINED = -1000
+
+
+def mult_transpose_add(kind, mat, v1, v2):
+    """MAT::MultTransposeAdd: (code, v = A^T v1 + v2); the reference back end returns
+    REF_UNDEFINED (and no v) where its loop would read past A's row pointers."""
+    lib = load(kind)
+    lib.orc_mult_transpose_add.restype = C.c_int
+    lib.orc_mult_transpose_add.argtypes = [C.c_uint32, C.c_uint32, _u32p, _u32p, C.c_void_p,
+                                           _f64p, _f64p, _f64p]
+    v = np.zeros(mat.mcol)
+    code = lib.orc_mult_transpose_add(mat.nrow, mat.mcol, mat.rowPtr, mat.colInd,
+                                      _vptr(mat.values), np.ascontiguousarray(v1, np.float64),
+                                      np.ascontiguousarray(v2, np.float64), v)
+    return code, (v if code == 0 else None)
 
 
 def _converted(code, nnz_out, rp, ci, va):

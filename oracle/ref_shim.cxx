@@ -338,6 +338,23 @@ void orc_transpose(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t* r
     }
 }
 
+int orc_mult_transpose_add(uint32_t nrow, uint32_t mcol, const uint32_t* rowPtr,
+                           const uint32_t* colInd, const double* values, const double* v1,
+                           const double* v2, double* v)
+{
+    /* the reference's last loop reads A's rowPtr[i + 1] for every row i of A^T (MAT.cxx:603):
+     * past its end unless A is square; a pattern-only A reads its empty values array */
+    if (nrow != mcol || !values) return ORC_REF_UNDEFINED;
+    const uint32_t nnz = rowPtr[nrow];
+    std::vector<USI> rp(rowPtr, rowPtr + nrow + 1), ci(colInd, colInd + nnz);
+    std::vector<DBL> va(values, values + nnz);
+    MAT A(nrow, mcol, nnz, va, ci, rp);
+    VEC a(nrow, v1), b(mcol, v2), out(mcol, 0.0);
+    A.MultTransposeAdd(a, b, out);
+    for (uint32_t i = 0; i < mcol; ++i) v[i] = out[i];
+    return 0;
+}
+
 void orc_diagptr(uint32_t nrow, const uint32_t* rowPtr, const uint32_t* colInd,
                  uint32_t* diagPtr)
 {

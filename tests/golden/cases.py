@@ -229,3 +229,48 @@ def add_cases() -> dict:
         out[key[4:]] = (m["a"], A, m["b"], B, (z[key + "__C_rowPtr"], z[key + "__C_colInd"],
                                                   z[key + "__C_values"]))
     return out
+
+
+# ---- MAT::MultTransposeAdd (reference_mta.npz / .json, written by make_golden.py) ----------
+
+def mta_matrices():
+    """name -> square matrix for MAT::MultTransposeAdd. The first five are structurally
+    symmetric (A's row pointers equal its transpose's), where the reference's loop bound
+    (MAT.cxx:603, A's rowPtr instead of the transpose's) is right; ``rand_nonsym`` is not,
+    and there the reference's result is not A^T v1 + v2."""
+    from faspxx_b200 import problems as P
+    out = {name: matrix(name) for name in ("fdm_10X10", "fem_small", "poisson3d_12",
+                                           "convdiff_pe10", "vardiff_8")}
+    rng = np.random.default_rng(31)
+    n = 40
+    rows, cols = [], []
+    for i in range(n):
+        extra = rng.choice(n, size=int(rng.integers(0, 6)), replace=False)
+        for j in sorted(set(extra.tolist()) | {i}):
+            rows.append(i)
+            cols.append(j)
+    rows, cols = np.array(rows), np.array(cols)
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(rows, minlength=n), out=rp[1:])
+    out["rand_nonsym"] = P.CSRMatrix(n, n, rp.astype(np.uint32), cols.astype(np.uint32),
+                                     rng.standard_normal(len(cols)))
+    return out
+
+
+def mta_vectors(A, seed=3):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(A.nrow), rng.standard_normal(A.mcol)
+
+
+def mta_cases() -> dict:
+    """name -> (A, v1, v2, the reference's v, structurally symmetric?)."""
+    import json
+    meta = json.load(open(os.path.join(HERE, "reference_mta.json")))
+    z = np.load(os.path.join(HERE, "reference_mta.npz"))
+    mats = mta_matrices()
+    out = {}
+    for name, m in meta.items():
+        A = mats[name]
+        v1, v2 = mta_vectors(A)
+        out[name] = (A, v1, v2, z[name + "__v"], m["symmetric_structure"])
+    return out

@@ -1,7 +1,8 @@
 """Generate the golden fixtures under tests/golden/ from the FASP++ reference itself.
 
-Run in a container that has the reference tree (default /root/reference) after
-``make -C oracle``; the GPU box never runs this script, it only reads its outputs:
+Run in a container that has the reference tree (given as the first argument or in
+FASPXX_REFERENCE) after ``make -C oracle``; the GPU box never runs this script, it only
+reads its outputs:
 
 * ``fdm_10X10.npz``, ``fem_small.npz`` -- the reference's bundled matrices
   (data/fdm_10X10.csr, data/fem_small.csr) as 0-based uint32/float64 CSR arrays;
@@ -24,8 +25,12 @@ Run in a container that has the reference tree (default /root/reference) after
   computed by the reference (stencil squares, rectangular random factors, an interpolation
   product; stencil plus diagonal, unsorted random rows, repeated appended columns).
 
-    python tests/golden/make_golden.py [/path/to/reference]
+* ``reference_mta.npz`` + ``reference_mta.json`` -- MAT::MultTransposeAdd, v = A^T v1 + v2,
+  computed by the reference on five structurally symmetric matrices and one that is not.
+
+    python tests/golden/make_golden.py /path/to/reference
                                        [--ingest-only | --matfree-only | --mult-only]
+    python tests/golden/make_golden.py --mta-only
 """
 from __future__ import annotations
 
@@ -377,9 +382,32 @@ def make_mult() -> None:
     print("wrote", len(mult_cases()), "MAT::Mult and", len(add_cases()), "MAT::Add cases")
 
 
+def make_mta() -> None:
+    """MAT::MultTransposeAdd run by the reference on the cases' matrices."""
+    O.build(ref=True)
+    arr, meta = {}, {}
+    for name, A in G.mta_matrices().items():
+        v1, v2 = G.mta_vectors(A)
+        code, v = O.mult_transpose_add("ref", A, v1, v2)
+        assert code == 0, name
+        trp, _, _, _ = O.transpose("port", A)
+        arr[name + "__v"] = v
+        meta[name] = {"symmetric_structure": bool(np.array_equal(trp, A.rowPtr))}
+    np.savez_compressed(os.path.join(HERE, "reference_mta.npz"), **arr)
+    with open(os.path.join(HERE, "reference_mta.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", len(meta), "MAT::MultTransposeAdd cases")
+
+
 if __name__ == "__main__":
+    if "--mta-only" in sys.argv:
+        make_mta()
+        sys.exit(0)
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    root = args[0] if args else "/root/reference"
+    root = args[0] if args else os.environ.get("FASPXX_REFERENCE")
+    if not root or not os.path.isdir(os.path.join(root, "src")):
+        sys.exit("make_golden.py: give the reference source tree as the first argument or "
+                 "in FASPXX_REFERENCE")
     if "--mult-only" in sys.argv:
         make_mult()
         sys.exit(0)
@@ -389,3 +417,4 @@ if __name__ == "__main__":
         make_ingest(root)
     make_matfree()
     make_mult()
+    make_mta()

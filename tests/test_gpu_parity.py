@@ -8,12 +8,15 @@ C ABI. Tolerances, stated per check:
 * VEC reductions: 1e-13 relative;
 * transpose (CSR -> CSC): bit-exact structure, order and values;
 * solvers: the same return code, iteration count within +-1, the solution within
-  1e-6 of the oracle's (relative to max(|x|, |x0|)); residual history within 1e-10
-  relative of the oracle's over the first 10 iterations (those above 1e-3 of the initial
-  residual, before round-off differences are amplified) and within 1e-6 of the initial
-  residual over the whole run. Cases whose stopping test sits at the rounding floor
-  (FLOOR) or that the reference's own history shows to be erratic (ERRATIC) are held to
-  the return code and a looser iteration window, stated below.
+  1e-6 of the oracle's (relative to max(|x|, |x0|)); residual history entry k within
+  max(1e-10, 10 x the case's sensitivity envelope up to entry k + 3) relative, plus the
+  rounding floor of a residual norm (1e-15 of the initial residual). The envelope is the
+  oracle (pinned bit for bit to the reference) rerun with every entry of b and x0 moved
+  by one ulp: the GPU's reordered sums perturb each step by about that much, so where the
+  reference reproduces itself the bar is 1e-10 over the whole history. Cases whose
+  stopping test sits at the rounding floor (FLOOR) or that the reference's own history
+  shows to be erratic (ERRATIC) are held to the return code and a looser iteration window,
+  stated below.
 """
 import json
 import os
@@ -38,6 +41,26 @@ FLOOR = {"fdm_cg_tolsmall": (0, -34), "fdm_bicgstab_tolsmall": (0, -34, -18)}
 # BiCGStab on fem_small from x0 = 1, b = 0: the residual norm oscillates by orders of
 # magnitude near the threshold; two reruns of the reference with reordered sums differ too
 ERRATIC = {"fem_bicgstab": 3, "fem_bicgstab_jac": 3}
+
+
+def perturbed(v, seed=1):
+    """Every entry moved by one ulp, up or down (seeded)."""
+    up = np.random.default_rng(seed).random(len(v)) < 0.5
+    return np.where(up, np.nextafter(v, np.inf), np.nextafter(v, -np.inf))
+
+
+def history_bound(h_ref, h_env):
+    """Per-entry absolute bound: max(1e-10, 10 x running envelope 3 entries ahead) relative
+    plus 1e-15 of the initial residual (the rounding floor of a residual norm)."""
+    m = min(len(h_ref), len(h_env))
+    env = np.zeros(len(h_ref))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        env[:m] = np.nan_to_num(np.abs(h_env[:m] - h_ref[:m]) / h_ref[:m], nan=0.0)
+    if m < len(h_ref):
+        env[m:] = np.inf  # the perturbed run stopped earlier: no bar beyond it
+    run = np.maximum.accumulate(env)
+    ahead = np.minimum(np.arange(len(h_ref)) + 3, len(h_ref) - 1)
+    return np.maximum(1e-10, 10.0 * run[ahead]) * h_ref + 1e-15 * h_ref[0]
 
 
 @pytest.fixture(scope="module")
@@ -195,13 +218,17 @@ def _check_case(gpu, oracle, name, engine="graph"):
         m = min(len(h), len(ref.hist))
         fin = np.isfinite(ref.hist[:m])
         assert np.array_equal(fin, np.isfinite(h[:m])), key
-        hr, hg = ref.hist[:m][fin], h[:m][fin]
-        if name in ERRATIC or len(hr) == 0:
+        if not fin.any():
             continue
-        early = np.arange(len(hr)) < 10
-        early &= hr >= 1e-3 * hr[0]  # the first 10 entries above 1e-3 of the initial
-        assert np.all(np.abs(hg[early] - hr[early]) <= 1e-10 * hr[early]), key
-        assert np.all(np.abs(hg - hr) <= 1e-6 * hr[0]), key
+        if rep > 0:
+            continue  # repeated solves on one object: the first solve's envelope only
+        # a fresh oracle object, so that state kept between solves (FGMRES's Z) is untouched
+        env = oracle.Solver("port", A, case["alg"], **case["kw"]).solve(perturbed(b),
+                                                                         perturbed(x0))
+        bound = history_bound(ref.hist[:m], env.hist)
+        dev = np.abs(h[:m] - ref.hist[:m])
+        bad = np.nonzero(fin & (dev > bound))[0]
+        assert len(bad) == 0, (key, int(bad[0]), float(dev[bad[0]] / ref.hist[bad[0]]))
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

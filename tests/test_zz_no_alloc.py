@@ -1,10 +1,11 @@
 """fasp_gpu_vec_dot_noalloc: the dot product for callers that cannot allocate device memory
-(code running during a global-mode graph capture, under a memory pool that owns the device,
-or in latency-critical loops where cudaMalloc/cudaFree would synchronize). It keeps its
-reduction scratch in a static device array instead of allocating; this test checks it
-through the C ABI against fasp_gpu_vec_dot, the allocating entry point, on two calls in a
-row (the array keeps the previous call's contents), and checks that sizes beyond the
-array's limit are refused. The test allocates its own inputs; the entry point does not.
+(an application whose memory pool owns the device memory, or a latency-critical loop where
+cudaMalloc/cudaFree would synchronize). It keeps its reduction scratch in a static device
+array instead of allocating; this test checks it through the C ABI against
+fasp_gpu_vec_dot, the allocating entry point, on two calls in a row (the array keeps the
+previous call's contents), from a fresh host thread that never selected a device (the
+entry point runs on the library's device), and checks that sizes beyond the array's limit
+are refused. The test allocates its own inputs; the entry point does not.
 
 This file is named to be collected last, and passes alone in a fresh process as well.
 """
@@ -55,6 +56,40 @@ def test_noalloc_dot_matches_allocating_dot_twice():
     finally:
         for p in bufs:
             lib.fasp_gpu_free(p)
+
+
+def test_noalloc_dot_from_a_fresh_thread():
+    """A worker thread with no CUDA device selected gets the library's device."""
+    import threading
+    from faspxx_b200 import capi
+    capi.init(0)
+    lib = capi.lib
+    rng = np.random.default_rng(23)
+    n = 1_048_579
+    a, b = rng.standard_normal(n), rng.standard_normal(n)
+    da, db = _dev(capi, a), _dev(capi, b)
+    try:
+        ref = C.c_double()
+        capi.check(lib.fasp_gpu_vec_dot(n, da, db, C.byref(ref)), "dot")
+        out = {}
+
+        def worker():
+            r = C.c_double(np.nan)
+            out["codes"] = [lib.fasp_gpu_vec_dot_noalloc(n, da, db, C.byref(r))]
+            out["vals"] = [r.value]
+            out["codes"].append(lib.fasp_gpu_vec_dot_noalloc(n, da, db, C.byref(r)))
+            out["vals"].append(r.value)
+
+        t = threading.Thread(target=worker)
+        t.start()
+        t.join()
+        assert out["codes"] == [0, 0]
+        scale = float(np.abs(a * b).sum())
+        for g in out["vals"]:
+            assert abs(g - ref.value) <= TOL * scale, (g, ref.value)
+    finally:
+        lib.fasp_gpu_free(da)
+        lib.fasp_gpu_free(db)
 
 
 def test_noalloc_dot_rejects_sizes_beyond_its_scratch():
