@@ -91,6 +91,14 @@ int main()
         S.Add(2.0, A, -1.0, A);
         std::printf("mult %d %u %u\n", C.Status(), C.GetNNZ(), C.GetRowSize());
         std::printf("add %d %u %u\n", S.Status(), S.GetNNZ(), S.GetRowSize());
+        // MAT::MultTransposeAdd on the symmetric Laplacian: A^T 1 + 1 = A 1 + 1
+        VEC ones(A.GetRowSize(), 1.0), out;
+        DVEC d1(ones), d2(ones), dv(A.GetRowSize()), da(A.GetRowSize());
+        A.MultTransposeAdd(d1, d2, dv);
+        A.Apply(d1, da);
+        da.AXPY(1.0, d2);
+        da.AXPY(-1.0, dv);
+        std::printf("mta %.3e %.3e\n", dv.Norm2(), da.NormInf());
     }
     // 3. ReadMat of a MatrixMarket file (unsorted triplets, 1-based)
     {

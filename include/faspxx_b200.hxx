@@ -168,6 +168,11 @@ public:
     {
         fasp_gpu_mat_residual(h_, b.data(), x.data(), r.data());
     }
+    /* MAT::MultTransposeAdd (MAT.cxx:541-606): v = A^T v1 + v2, on a transpose formed once */
+    void MultTransposeAdd(const DVEC& v1, const DVEC& v2, DVEC& v) const
+    {
+        fasp_gpu_mat_mult_transpose_add(h_, v1.data(), v2.data(), v.data());
+    }
     /* B200 option: matrix form of the SpMV kernels, 0 CSR, 1 row classes, 2 row classes
      * with stencil masks (bit-identical results; set before a solver's Setup) */
     void SetRowClass(int mode) { fasp_gpu_mat_set_rowclass(h_, mode); }

@@ -63,7 +63,8 @@ def test_feature_driver_compiles():
 @pytest.mark.gpu
 def test_feature_driver_runs_on_gpu():
     """StencilLOP (the matrix-free example at dim 64: 121 CG iterations and the L2 error the
-    reference prints, 1.0041e-04), MAT::Mult/Add, ReadMat of a MatrixMarket file, and
+    reference prints, 1.0041e-04), MAT::Mult/Add/MultTransposeAdd, ReadMat of a MatrixMarket
+    file, and
     MG-preconditioned CG through the façade."""
     with tempfile.TemporaryDirectory() as d:
         exe = os.path.join(d, "f")
@@ -74,5 +75,7 @@ def test_feature_driver_runs_on_gpu():
     assert abs(float(r["matfree_cg"][2]) - 1.0041e-04) <= 2e-8
     assert r["mult"] == ["0", "352", "36"]  # the 13-point square of the 5-point stencil
     assert r["add"] == ["0", "156", "36"]   # 2A - A keeps A's pattern
+    # MultTransposeAdd on a symmetric matrix equals Apply + v2 (within rounding)
+    assert float(r["mta"][0]) > 0 and float(r["mta"][1]) <= 1e-13
     assert r["readmat"] == ["0", "3", "5"]  # every row has its diagonal: nothing inserted
     assert r["mg_pcg"][0] == "0" and int(r["mg_pcg"][1]) <= 12
