@@ -265,38 +265,64 @@ static bool vec_ok(const T* V, size_t ld, const T* w)
            ld % Vec16<T>::W == 0;
 }
 
-// dres[j] = (V_j, w), j in [j0, j0+k)
-template <typename T, int VEC>
+// The Gram-Schmidt kernels take the number of basis vectors of a launch, K, at compile time:
+// every 16-byte load of an element group (w and the K basis vectors) is issued before the
+// group's FMAs, and with K <= 3 each thread takes two groups per step, so a thread keeps
+// K + 1 or 2 (K + 1) loads in flight instead of waiting on each vector in turn (the
+// one-wave grid gives each thread only a few steps). The groups, and the elements in each
+// group, are accumulated in the same order as one group at a time, so the results do not
+// depend on the grouping. Two groups per step only for K <= 3: more would exceed the 85
+// registers a thread has at 3 blocks of kBlock threads per SM.
+template <int K>
+__host__ __device__ constexpr int gs_unroll() { return K <= 3 ? 2 : 1; }
+
+// dres[j] = (V_j, w), j < K
+template <typename T, int VEC, int K>
 __global__ void __launch_bounds__(kBlock, 3)
-k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
-                           const T* __restrict__ w, Scratch s, double* dres, const int* stop)
+k_multidot(uint32_t n, const T* __restrict__ V, size_t ld, const T* __restrict__ w, Scratch s,
+           double* dres, const int* stop)
 {
     if (stop && *stop) return;
     using VT = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::W;
-    T t[KC];
-    double acc[KC];
-    int ops[KC];
+    constexpr int U = gs_unroll<K>();
+    T t[K];
+    double acc[K];
+    int ops[K];
 #pragma unroll
-    for (int j = 0; j < KC; ++j) {
+    for (int j = 0; j < K; ++j) {
         t[j] = T(0);
         ops[j] = kSum;
     }
     size_t i0 = 0;
     if (VEC) {
-        const size_t nv = n / W;
-        GRID_STRIDE(iv, nv)
-        {
-            T wv[W];
+        const size_t nv = n / W, stride = (size_t)gridDim.x * blockDim.x;
+        size_t iv = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        for (; iv + (U - 1) * stride < nv; iv += U * stride) {
+            T wv[U][W], vv[U][K][W];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                *(VT*)wv[u] = ((const VT*)w)[iv + u * stride];
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+                    *(VT*)vv[u][j] = ((const VT*)(V + j * ld))[iv + u * stride];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int e = 0; e < W; ++e) t[j] = fma(vv[u][j][e], wv[u][e], t[j]);
+        }
+        for (; iv < nv; iv += stride) {
+            T wv[W], vv[K][W];
             *(VT*)wv = ((const VT*)w)[iv];
 #pragma unroll
-            for (int j = 0; j < KC; ++j)
-                if (j < k) {
-                    T vv[W];
-                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+            for (int j = 0; j < K; ++j) *(VT*)vv[j] = ((const VT*)(V + j * ld))[iv];
 #pragma unroll
-                    for (int u = 0; u < W; ++u) t[j] = fma(vv[u], wv[u], t[j]);
-                }
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < W; ++e) t[j] = fma(vv[j][e], wv[e], t[j]);
         }
         i0 = nv * W;
     }
@@ -304,48 +330,65 @@ k_multidot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
          i += (size_t)gridDim.x * blockDim.x) {
         const T wi = w[i];
 #pragma unroll
-        for (int j = 0; j < KC; ++j)
-            if (j < k) t[j] = fma(V[j * ld + i], wi, t[j]);
+        for (int j = 0; j < K; ++j) t[j] = fma(V[j * ld + i], wi, t[j]);
     }
 #pragma unroll
-    for (int j = 0; j < KC; ++j) acc[j] = (double)t[j];
-    grid_reduce<KC>(acc, ops, s, [=] __device__(const double* v) {
-        for (int j = 0; j < k; ++j) dres[j] = v[j];
+    for (int j = 0; j < K; ++j) acc[j] = (double)t[j];
+    grid_reduce<K>(acc, ops, s, [=] __device__(const double* v) {
+        for (int j = 0; j < K; ++j) dres[j] = v[j];
     });
 }
 
-// w -= sign * sum_j h[j] V_j; with dnorm != null also ||w_new|| -> *dnorm.
-template <typename T, int VEC>
+// w -= sign * sum_j h[j] V_j (j < K); with dnorm != null also ||w_new|| -> *dnorm.
+template <typename T, int VEC, int K>
 __global__ void __launch_bounds__(kBlock, 3)
-k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
-                            const double* __restrict__ h, double sign, T* __restrict__ w,
-                            Scratch s, double* dnorm, const int* stop)
+k_multiaxpy(uint32_t n, const T* __restrict__ V, size_t ld, const double* __restrict__ h,
+            double sign, T* __restrict__ w, Scratch s, double* dnorm, const int* stop)
 {
     if (stop && *stop) return;
     using VT = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::W;
-    T hj[KC];
+    constexpr int U = gs_unroll<K>();
+    T hj[K];
 #pragma unroll
-    for (int j = 0; j < KC; ++j) hj[j] = j < k ? (T)(sign * h[j]) : T(0);
+    for (int j = 0; j < K; ++j) hj[j] = (T)(sign * h[j]);
     T t = T(0);
     size_t i0 = 0;
     if (VEC) {
-        const size_t nv = n / W;
-        GRID_STRIDE(iv, nv)
-        {
-            T wv[W];
+        const size_t nv = n / W, stride = (size_t)gridDim.x * blockDim.x;
+        size_t iv = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        for (; iv + (U - 1) * stride < nv; iv += U * stride) {
+            T wv[U][W], vv[U][K][W];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                *(VT*)wv[u] = ((const VT*)w)[iv + u * stride];
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+                    *(VT*)vv[u][j] = ((const VT*)(V + j * ld))[iv + u * stride];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int e = 0; e < W; ++e) wv[u][e] = fma(-hj[j], vv[u][j][e], wv[u][e]);
+                ((VT*)w)[iv + u * stride] = *(VT*)wv[u];
+#pragma unroll
+                for (int e = 0; e < W; ++e) t = fma(wv[u][e], wv[u][e], t);
+            }
+        }
+        for (; iv < nv; iv += stride) {
+            T wv[W], vv[K][W];
             *(VT*)wv = ((const VT*)w)[iv];
 #pragma unroll
-            for (int j = 0; j < KC; ++j)
-                if (j < k) {
-                    T vv[W];
-                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+            for (int j = 0; j < K; ++j) *(VT*)vv[j] = ((const VT*)(V + j * ld))[iv];
 #pragma unroll
-                    for (int u = 0; u < W; ++u) wv[u] = fma(-hj[j], vv[u], wv[u]);
-                }
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < W; ++e) wv[e] = fma(-hj[j], vv[j][e], wv[e]);
             ((VT*)w)[iv] = *(VT*)wv;
 #pragma unroll
-            for (int u = 0; u < W; ++u) t = fma(wv[u], wv[u], t);
+            for (int e = 0; e < W; ++e) t = fma(wv[e], wv[e], t);
         }
         i0 = nv * W;
     }
@@ -353,8 +396,7 @@ k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
          i += (size_t)gridDim.x * blockDim.x) {
         T wi = w[i];
 #pragma unroll
-        for (int j = 0; j < KC; ++j)
-            if (j < k) wi = fma(-hj[j], V[j * ld + i], wi);
+        for (int j = 0; j < K; ++j) wi = fma(-hj[j], V[j * ld + i], wi);
         w[i] = wi;
         t = fma(wi, wi, t);
     }
@@ -364,54 +406,69 @@ k_multiaxpy(uint32_t n, int k, const T* __restrict__ V, size_t ld,
 }
 
 // CGS2's second projection and its re-orthogonalisation dots in one pass over the basis,
-// for k <= KF<T> vectors (16 FP32, 8 FP64: what fits in registers): w -= sum_j h[j] V_j,
-// then dres[j] = (V_j, w_new). Each element's
-// FMA sequence, each thread's elements (the same grid and mapping as k_multidot) and the
-// reduction order equal those of k_multiaxpy followed by k_multidot, so the results are
-// bit-identical to the two passes; V is read once instead of twice.
+// for K <= 8 vectors (what fits in registers with every load hoisted): w -= sum_j h[j] V_j,
+// then dres[j] = (V_j, w_new), each basis vector loaded once. Each element's FMA sequence,
+// each thread's elements (the same grid and mapping as k_multidot) and the reduction order
+// equal those of k_multiaxpy followed by k_multidot, so the results are bit-identical to
+// the two passes; V is read once instead of twice.
 template <typename T>
-__host__ __device__ constexpr int kf() { return sizeof(T) == 8 ? 8 : 16; }
+__host__ __device__ constexpr int kf() { return 8; }
 
-template <typename T, int VEC>
+template <typename T, int VEC, int K>
 __global__ void __launch_bounds__(kBlock, 3)
-k_multiaxpy_dot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
-                const double* __restrict__ h, T* __restrict__ w, Scratch s, double* dres,
-                const int* stop)
+k_multiaxpy_dot(uint32_t n, const T* __restrict__ V, size_t ld, const double* __restrict__ h,
+                T* __restrict__ w, Scratch s, double* dres, const int* stop)
 {
     if (stop && *stop) return;
-    constexpr int KF_ = kf<T>();
     using VT = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::W;
-    __shared__ T hs[KF_];
-    if (threadIdx.x < KF_) hs[threadIdx.x] = (int)threadIdx.x < k ? (T)(1.0 * h[threadIdx.x]) : T(0);
+    constexpr int U = gs_unroll<K>();
+    __shared__ T hs[K];
+    if (threadIdx.x < K) hs[threadIdx.x] = (T)(1.0 * h[threadIdx.x]);
     __syncthreads();
-    T t[KF_];
+    T t[K];
 #pragma unroll
-    for (int j = 0; j < KF_; ++j) t[j] = T(0);
+    for (int j = 0; j < K; ++j) t[j] = T(0);
     size_t i0 = 0;
     if (VEC) {
-        const size_t nv = n / W;
-        GRID_STRIDE(iv, nv)
-        {
-            T wv[W];
+        const size_t nv = n / W, stride = (size_t)gridDim.x * blockDim.x;
+        size_t iv = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        for (; iv + (U - 1) * stride < nv; iv += U * stride) {
+            T wv[U][W], vv[U][K][W];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                *(VT*)wv[u] = ((const VT*)w)[iv + u * stride];
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+                    *(VT*)vv[u][j] = ((const VT*)(V + j * ld))[iv + u * stride];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int e = 0; e < W; ++e) wv[u][e] = fma(-hs[j], vv[u][j][e], wv[u][e]);
+                ((VT*)w)[iv + u * stride] = *(VT*)wv[u];
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+#pragma unroll
+                    for (int e = 0; e < W; ++e) t[j] = fma(vv[u][j][e], wv[u][e], t[j]);
+            }
+        }
+        for (; iv < nv; iv += stride) {
+            T wv[W], vv[K][W];
             *(VT*)wv = ((const VT*)w)[iv];
 #pragma unroll
-            for (int j = 0; j < KF_; ++j)
-                if (j < k) {
-                    T vv[W];
-                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+            for (int j = 0; j < K; ++j) *(VT*)vv[j] = ((const VT*)(V + j * ld))[iv];
 #pragma unroll
-                    for (int u = 0; u < W; ++u) wv[u] = fma(-hs[j], vv[u], wv[u]);
-                }
+            for (int j = 0; j < K; ++j)
+#pragma unroll
+                for (int e = 0; e < W; ++e) wv[e] = fma(-hs[j], vv[j][e], wv[e]);
             ((VT*)w)[iv] = *(VT*)wv;
 #pragma unroll
-            for (int j = 0; j < KF_; ++j)
-                if (j < k) {
-                    T vv[W];
-                    *(VT*)vv = ((const VT*)(V + j * ld))[iv];
+            for (int j = 0; j < K; ++j)
 #pragma unroll
-                    for (int u = 0; u < W; ++u) t[j] = fma(vv[u], wv[u], t[j]);
-                }
+                for (int e = 0; e < W; ++e) t[j] = fma(vv[j][e], wv[e], t[j]);
         }
         i0 = nv * W;
     }
@@ -419,39 +476,235 @@ k_multiaxpy_dot(uint32_t n, int k, const T* __restrict__ V, size_t ld,
          i += (size_t)gridDim.x * blockDim.x) {
         T wi = w[i];
 #pragma unroll
-        for (int j = 0; j < KF_; ++j)
-            if (j < k) wi = fma(-hs[j], V[j * ld + i], wi);
+        for (int j = 0; j < K; ++j) wi = fma(-hs[j], V[j * ld + i], wi);
         w[i] = wi;
 #pragma unroll
-        for (int j = 0; j < KF_; ++j)
-            if (j < k) t[j] = fma(V[j * ld + i], wi, t[j]);
+        for (int j = 0; j < K; ++j) t[j] = fma(V[j * ld + i], wi, t[j]);
     }
-    double acc[KF_];
-    int ops[KF_];
+    double acc[K];
+    int ops[K];
 #pragma unroll
-    for (int j = 0; j < KF_; ++j) {
+    for (int j = 0; j < K; ++j) {
         acc[j] = (double)t[j];
         ops[j] = kSum;
     }
-    grid_reduce<KF_>(acc, ops, s, [=] __device__(const double* v) {
-        for (int j = 0; j < k; ++j) dres[j] = v[j];
+    grid_reduce<K>(acc, ops, s, [=] __device__(const double* v) {
+        for (int j = 0; j < K; ++j) dres[j] = v[j];
     });
+}
+
+// Compile-time K from a runtime count k in [1, KMAX]: calls f(std::integral_constant<int, K>).
+template <int KMAX, typename F>
+static void with_k(int k, F&& f)
+{
+    switch (k) {
+        case 1: f(std::integral_constant<int, 1>()); break;
+        case 2: f(std::integral_constant<int, 2>()); break;
+        case 3: f(std::integral_constant<int, 3>()); break;
+        case 4: f(std::integral_constant<int, 4>()); break;
+        case 5: f(std::integral_constant<int, 5>()); break;
+        case 6: f(std::integral_constant<int, 6>()); break;
+        case 7: f(std::integral_constant<int, 7>()); break;
+        case 8: f(std::integral_constant<int, 8>()); break;
+        default:
+            if constexpr (KMAX > 8) {
+                switch (k) {
+                    case 9: f(std::integral_constant<int, 9>()); break;
+                    case 10: f(std::integral_constant<int, 10>()); break;
+                    case 11: f(std::integral_constant<int, 11>()); break;
+                    case 12: f(std::integral_constant<int, 12>()); break;
+                    case 13: f(std::integral_constant<int, 13>()); break;
+                    case 14: f(std::integral_constant<int, 14>()); break;
+                    case 15: f(std::integral_constant<int, 15>()); break;
+                    default: f(std::integral_constant<int, 16>()); break;
+                }
+            }
+            break;
+    }
+}
+
+// ---- one launch per Gram-Schmidt pass ---------------------------------------------------
+// k_gs handles up to kGsMaxK basis vectors in one launch (a GMRES(30) Arnoldi step has up
+// to 31), so a CGS2 step is three launches whatever its size instead of three per 8
+// vectors: each launch has a fixed cost (ramp, one-wave tail, the reduction's last block)
+// of about 5 us on B200, against 10-20 us of streaming. MODE 0: dres[j] = (V_j, w);
+// MODE 1: w -= sum_j h[j] V_j, then dres[j] = (V_j, w_new); MODE 2: w -= sign sum_j h[j] V_j
+// and, with dnorm, ||w_new||. Each thread walks its 16-byte element groups (grid stride,
+// the same groups in every mode) and, per group, the basis vectors in batches of
+// gs_batch loads issued before their FMAs; its dot accumulators live in shared memory
+// (k x blockDim values), so k does not cost registers. MODE 1 reads each vector's group
+// again for the dots right after the projection used it: from L1 or L2, not from DRAM, so
+// the fused pass streams V once. A thread adds its groups in order, the block adds its
+// threads in a fixed tree and the last block adds the blocks in order: MODE 1's dots equal
+// MODE 2 (sign 1) followed by MODE 0 bit for bit, and reruns give the same bits.
+constexpr int kGsMaxK = 32;
+// loads in flight per batch: 8 basis groups, 4 in the fused mode (which also keeps w's
+// group live across its two passes; 8 there exceeds the 85-register budget)
+template <int MODE>
+__host__ __device__ constexpr int gs_batch() { return MODE == 1 ? 4 : 8; }
+
+template <typename T>
+static size_t gs_smem(int k) { return (size_t)k * kBlock * sizeof(T) + kGsMaxK * sizeof(T); }
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kBlock, 3)
+k_gs(uint32_t n, int k, const T* __restrict__ V, size_t ld, const double* __restrict__ h,
+     double sign, T* __restrict__ w, Scratch s, double* dres, double* dnorm, const int* stop)
+{
+    extern __shared__ __align__(16) unsigned char gs_raw[];
+    T* sacc = reinterpret_cast<T*>(gs_raw);           // [k][blockDim]
+    T* sh = sacc + (size_t)k * blockDim.x;            // [kGsMaxK] coefficients (sign folded)
+    __shared__ bool amLast;
+    if (stop && *stop) return;
+    using VT = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    constexpr int B = gs_batch<MODE>();
+    const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    if (MODE >= 1)
+        for (int j = tid; j < k; j += bd) sh[j] = (T)(sign * h[j]);
+    if (MODE <= 1)
+        for (int j = 0; j < k; ++j) sacc[j * bd + tid] = T(0);
+    __syncthreads();
+    T nrm = T(0);
+    auto project = [&](T* wv, auto load) {
+        for (int j0 = 0; j0 < k; j0 += B) {
+            T vv[B][W];
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (j0 + u < k) load(j0 + u, vv[u]);
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (j0 + u < k)
+#pragma unroll
+                    for (int e = 0; e < W; ++e) wv[e] = fma(-sh[j0 + u], vv[u][e], wv[e]);
+        }
+    };
+    auto dots = [&](const T* wv, auto load) {
+        for (int j0 = 0; j0 < k; j0 += B) {
+            T vv[B][W];
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (j0 + u < k) load(j0 + u, vv[u]);
+#pragma unroll
+            for (int u = 0; u < B; ++u)
+                if (j0 + u < k) {
+                    T a = sacc[(j0 + u) * bd + tid];
+#pragma unroll
+                    for (int e = 0; e < W; ++e) a = fma(vv[u][e], wv[e], a);
+                    sacc[(j0 + u) * bd + tid] = a;
+                }
+        }
+    };
+    const size_t nv = n / W;
+    GRID_STRIDE(iv, nv)
+    {
+        auto ld16 = [&](int j, T* out) { *(VT*)out = ((const VT*)(V + j * ld))[iv]; };
+        T wv[W];
+        *(VT*)wv = ((const VT*)w)[iv];
+        if (MODE >= 1) {
+            project(wv, ld16);
+            ((VT*)w)[iv] = *(VT*)wv;
+#pragma unroll
+            for (int e = 0; e < W; ++e) nrm = fma(wv[e], wv[e], nrm);
+        }
+        if (MODE <= 1) dots(wv, ld16);
+    }
+    for (size_t i = nv * W + (size_t)blockIdx.x * bd + tid; i < n; i += (size_t)gridDim.x * bd) {
+        auto ld1 = [&](int j, T* out) {
+            out[0] = V[j * ld + i];
+#pragma unroll
+            for (int e = 1; e < W; ++e) out[e] = T(0);
+        };
+        T wv[W];
+        wv[0] = w[i];
+#pragma unroll
+        for (int e = 1; e < W; ++e) wv[e] = T(0);
+        if (MODE >= 1) {
+            project(wv, ld1);
+            w[i] = wv[0];
+            nrm = fma(wv[0], wv[0], nrm);
+        }
+        if (MODE <= 1) dots(wv, ld1);
+    }
+    if (MODE == 2) {
+        double acc[1] = {(double)nrm};
+        const int ops[1] = {kSum};
+        if (dnorm) grid_reduce<1>(acc, ops, s, [=] __device__(const double* v) { *dnorm = sqrt(v[0]); });
+        return;
+    }
+    // block partials: warp g adds column j = g, g + warps, ... over the block's threads
+    // (lane l sums threads l, l + 32, ... in order, then a shuffle tree)
+    __syncthreads();
+    const int lane = tid & 31, wid = tid >> 5, nwarp = bd >> 5;
+    for (int j = wid; j < k; j += nwarp) {
+        double a = 0.0;
+        for (uint32_t t = lane; t < bd; t += 32) a += (double)sacc[j * bd + t];
+        a = warp_reduce(a, kSum);
+        if (lane == 0) s.partials[(size_t)j * gridDim.x + blockIdx.x] = a;
+    }
+    __syncthreads();
+    if (tid == 0) amLast = last_block_ticket(s.ticket);
+    __syncthreads();
+    if (!amLast) return;
+    // the last block: dres[j] = the blocks' partials added in block order (lane l takes
+    // blocks l, l + 32, ..., then a shuffle tree)
+    for (int j = wid; j < k; j += nwarp) {
+        double a = 0.0;
+        for (uint32_t b = lane; b < gridDim.x; b += 32)
+            a += __ldcg(&s.partials[(size_t)j * gridDim.x + b]);
+        a = warp_reduce(a, kSum);
+        if (lane == 0) dres[j] = a;
+    }
+}
+
+// Launches k_gs over the basis in chunks of kGsMaxK vectors. MODE 1 with more than one
+// chunk runs as MODE 2 over every chunk, then MODE 0 over every chunk (the projection must
+// be complete before any dot).
+template <typename T, int MODE>
+static int gs_launch(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
+                     double sign, T* w, double* dres, double* dnorm, const int* stop)
+{
+    // the shared-memory opt-in above 48 KB, once per device
+    static bool attr[64] = {};
+    if (c.dev < 0 || c.dev >= 64) return kErrNoDevice;
+    if (!attr[c.dev]) {
+        FB_CUDA(cudaFuncSetAttribute(k_gs<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)gs_smem<T>(kGsMaxK)));
+        attr[c.dev] = true;
+    }
+    const int g = mgrid(c, n);
+    for (int j0 = 0; j0 < k; j0 += kGsMaxK) {
+        const int kk = k - j0 < kGsMaxK ? k - j0 : kGsMaxK;
+        const bool last = j0 + kGsMaxK >= k;
+        ++c.launches;
+        k_gs<T, MODE><<<g, kBlock, gs_smem<T>(kk), c.stream>>>(
+            n, kk, V + j0 * ld, ld, h ? h + j0 : nullptr, sign, w, c.red,
+            dres ? dres + j0 : nullptr, last ? dnorm : nullptr, stop);
+        FB_CUDA(cudaGetLastError());
+    }
+    return kOk;
 }
 
 template <typename T>
 int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, double* dres,
                const int* stop)
 {
+    if (vec_ok(V, ld, w))
+        return gs_launch<T, 0>(c, n, k, V, ld, nullptr, 1.0, const_cast<T*>(w), dres, nullptr,
+                               stop);
     const bool vec = vec_ok(V, ld, w);
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         ++c.launches;
-        if (vec)
-            k_multidot<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(
-                n, kk, V + j0 * ld, ld, w, c.red, dres + j0, stop);
-        else
-            k_multidot<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(
-                n, kk, V + j0 * ld, ld, w, c.red, dres + j0, stop);
+        with_k<KC>(kk, [&](auto KK) {
+            constexpr int K = decltype(KK)::value;
+            if (vec)
+                k_multidot<T, 1, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                    n, V + j0 * ld, ld, w, c.red, dres + j0, stop);
+            else
+                k_multidot<T, 0, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                    n, V + j0 * ld, ld, w, c.red, dres + j0, stop);
+        });
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
@@ -461,17 +714,22 @@ template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
                 double sign, T* w, double* dnorm, const int* stop)
 {
+    if (vec_ok(V, ld, (const T*)w))
+        return gs_launch<T, 2>(c, n, k, V, ld, h, sign, w, nullptr, dnorm, stop);
     const bool vec = vec_ok(V, ld, (const T*)w);
     for (int j0 = 0; j0 < k; j0 += KC) {
         const int kk = k - j0 < KC ? k - j0 : KC;
         const bool last = j0 + KC >= k;
         ++c.launches;
-        if (vec)
-            k_multiaxpy<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(
-                n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
-        else
-            k_multiaxpy<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(
-                n, kk, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
+        with_k<KC>(kk, [&](auto KK) {
+            constexpr int K = decltype(KK)::value;
+            if (vec)
+                k_multiaxpy<T, 1, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                    n, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
+            else
+                k_multiaxpy<T, 0, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(
+                    n, V + j0 * ld, ld, h + j0, sign, w, c.red, last ? dnorm : nullptr, stop);
+        });
         FB_CUDA(cudaGetLastError());
     }
     return kOk;
@@ -481,17 +739,27 @@ template <typename T>
 int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h, T* w,
                     double* dres, const int* stop)
 {
+    if (vec_ok(V, ld, (const T*)w)) {
+        if (k <= kGsMaxK)
+            return gs_launch<T, 1>(c, n, k, V, ld, h, 1.0, w, dres, nullptr, stop);
+        int e = gs_launch<T, 2>(c, n, k, V, ld, h, 1.0, w, nullptr, nullptr, stop);
+        return e ? e : gs_launch<T, 0>(c, n, k, V, ld, nullptr, 1.0, w, dres, nullptr, stop);
+    }
     if (k > kf<T>()) {
         int e = v_multiaxpy(c, n, k, V, ld, h, 1.0, w, (double*)nullptr, stop);
         return e ? e : v_multidot(c, n, k, V, ld, (const T*)w, dres, stop);
     }
     ++c.launches;
-    if (vec_ok(V, ld, (const T*)w))
-        k_multiaxpy_dot<T, 1><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, k, V, ld, h, w, c.red,
-                                                                    dres, stop);
-    else
-        k_multiaxpy_dot<T, 0><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, k, V, ld, h, w, c.red,
-                                                                    dres, stop);
+    const bool vec = vec_ok(V, ld, (const T*)w);
+    with_k<kf<T>()>(k, [&](auto KK) {
+        constexpr int K = decltype(KK)::value;
+        if (vec)
+            k_multiaxpy_dot<T, 1, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, V, ld, h, w, c.red,
+                                                                           dres, stop);
+        else
+            k_multiaxpy_dot<T, 0, K><<<mgrid(c, n), kBlock, 0, c.stream>>>(n, V, ld, h, w, c.red,
+                                                                           dres, stop);
+    });
     FB_CUDA(cudaGetLastError());
     return kOk;
 }

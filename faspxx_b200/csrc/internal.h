@@ -106,10 +106,14 @@ int resident_grid(const Ctx& c, const void* fn, int block);
 // timed next reads its inputs from HBM without paying to write back dirty lines first.
 int l2_flush_read(Ctx& c, const void* buf, size_t bytes);
 
-// Average device time (ms) of one call of `launch` over reps calls. flushL2 = 0: the calls
-// run back to back between two events. flushL2 = 1: each call is timed alone with events
-// after a 256 MB read that evicts L2 (126 MB) and leaves it clean, so its inputs come from
-// HBM and no write-back of dirty lines lands in the timed launch.
+// Average device time (ms) of one call of `launch` over reps calls, CUDA events on c.stream.
+// flushL2 = 0: the calls run back to back between two events (inputs that fit L2 stay
+// there). flushL2 = 1: every call follows a 256 MB read that evicts L2 (126 MB) and leaves
+// it clean, so its inputs come from HBM and no write-back of dirty lines lands in it; the
+// reps (flush, call) pairs run back to back between two events, the reps flushes alone are
+// timed the same way, and the difference is the calls' time. Timing each call alone between
+// its own two events instead would add the launch latency of an idle stream (measured
+// about 14 us on B200, against a 42 us SpMV) to every call.
 template <typename F>
 int time_launches(Ctx& c, unsigned reps, int flushL2, F&& launch, double* ms)
 {
@@ -123,19 +127,31 @@ int time_launches(Ctx& c, unsigned reps, int flushL2, F&& launch, double* ms)
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
-    double tot = 0.0;
     int e = kOk;
-    for (unsigned i = 0; i < (flushL2 ? reps : 1u); ++i) {
-        if (flushL2) l2_flush_read(c, flush, fbytes);
+    auto window = [&](bool withCall, bool withFlush, double* out) {
         cudaEventRecord(t0, c.stream);
-        for (unsigned k = 0; k < (flushL2 ? 1u : reps); ++k)
-            if ((e = launch())) break;
+        for (unsigned k = 0; k < reps && !e; ++k) {
+            if (withFlush) l2_flush_read(c, flush, fbytes);
+            if (withCall) e = launch();
+        }
         cudaEventRecord(t1, c.stream);
         cudaEventSynchronize(t1);
         float t = 0.f;
         cudaEventElapsedTime(&t, t0, t1);
-        tot += t;
-        if (e) break;
+        *out = t;
+    };
+    double tot = 0.0;
+    if (!flushL2) {
+        window(true, false, &tot);
+    } else {
+        double pair = 0.0, alone = 0.0;
+        if (!e) { // untimed warm-up pair
+            l2_flush_read(c, flush, fbytes);
+            e = launch();
+        }
+        window(true, true, &pair);
+        window(false, true, &alone);
+        tot = pair > alone ? pair - alone : 0.0;
     }
     *ms = tot / reps;
     cudaEventDestroy(t0);
@@ -267,8 +283,8 @@ int v_multidot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const T* w, dou
 template <typename T>
 int v_multiaxpy(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h,
                 double sign, T* w, double* dnorm, const int* stop = nullptr);
-// w -= sum_j h[j] V_j then dres[j] = (V_j, w), in one pass for k <= 16 (FP32) or 8 (FP64)
-// (bit-identical to v_multiaxpy followed by v_multidot, which it falls back to above)
+// w -= sum_j h[j] V_j then dres[j] = (V_j, w), in one pass for k <= 8 (bit-identical to
+// v_multiaxpy followed by v_multidot, which it falls back to above)
 template <typename T>
 int v_multiaxpy_dot(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const double* h, T* w,
                     double* dres, const int* stop = nullptr);

@@ -23,6 +23,8 @@ enum {
     SL_T0 = 0, SL_T1, SL_T2, SL_T3, SL_T4, SL_T5, SL_T6, SL_T7,
     SL_XINF = 16,  // NormInf of a residual's x (MAT::Residual shortcut)
     SL_ONE = 17,   // constant 1: disables the shortcut (MAT::Apply + XPAY paths)
+    SL_XINF2 = 18, // the fused Jacobi sweeps' second NormInf slot (ping-pong with SL_XINF)
+    SL_JRES = 19,  // ||r|| of the sweep that tests convergence
 };
 
 double SolverImpl::fetch(const double* dptr)
@@ -61,6 +63,118 @@ __global__ void k_jacobi_update(uint32_t n, const T* __restrict__ dinv,
     double acc[1] = {(double)m};
     const int ops[1] = {kMax};
     grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *dxinf = t[0]; });
+}
+
+template <typename T>
+static CSRView<T> pcd_view(const Mat& A);
+template <>
+CSRView<double> pcd_view<double>(const Mat& A) { return A.v64(); }
+template <>
+CSRView<float> pcd_view<float>(const Mat& A) { return A.v32(); }
+
+// One Jacobi sweep in one pass (Jacobi::Solve, Iter.cxx:83-92, with MAT::Residual,
+// MAT.cxx:455-476): r = b - A x_in, or r = b when NormInf(x_in) < CLOSE_ZERO; x_out = x_in
+// + diagInv .* r; NormInf(x_out) for the next sweep's shortcut and, with NORM, ||r|| -- the
+// residual of x_in, which Jacobi::Solve tests before it updates x. Each row is summed as
+// MAT::Residual's thread-per-row kernel sums it and updated with the same expression as
+// k_jacobi_update, so the sweeps give the two-kernel path's x bit for bit. x_in and x_out
+// are different vectors (every row reads x_in's neighbours).
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(kBlock) k_jacobi_sweep(CSRView<T> A, const T* __restrict__ b,
+                                                         const T* __restrict__ xin,
+                                                         const T* __restrict__ dinv,
+                                                         T* __restrict__ xout,
+                                                         const double* __restrict__ xinfIn,
+                                                         Scratch s, double* xinfOut,
+                                                         double* rnorm)
+{
+    const bool shortcut = *xinfIn < kCloseZero;
+    T m = T(0), rr = T(0);
+    auto xv = [&](uint32_t j) { return xin[j]; };
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.nrow;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const T sum = shortcut ? T(0) : row_apply<T, false>(A, i, xv);
+        const T r = b[i] - sum;
+        const T xi = xin[i] + r * dinv[i];
+        xout[i] = xi;
+        m = fmax(m, fabs(xi));
+        if (NORM) rr = fma(r, r, rr);
+    }
+    if (NORM) {
+        double acc[2] = {(double)m, (double)rr};
+        const int ops[2] = {kMax, kSum};
+        grid_reduce<2>(acc, ops, s, [=] __device__(const double* t) {
+            *xinfOut = t[0];
+            *rnorm = sqrt(t[1]);
+        });
+    } else {
+        double acc[1] = {(double)m};
+        const int ops[1] = {kMax};
+        grid_reduce<1>(acc, ops, s, [=] __device__(const double* t) { *xinfOut = t[0]; });
+    }
+}
+
+// A whole Jacobi::Solve (Iter.cxx:56-112) on a small matrix in one single-block launch:
+// NormInf(x), then per sweep the residual (with MAT::Residual's shortcut) into work, its
+// norm and Jacobi::Solve's convergence test when numIter >= minIter, and x += diagInv .*
+// work, each phase separated by a block barrier. A coarse MG level thus costs one launch
+// instead of 2 per sweep. The sums of each row and the updates are those of the
+// multi-block kernels, so x is the same bit for bit; the residual norms that decide when
+// to stop are block reductions in a fixed order (the tests' outcome can differ from the
+// multi-block reductions' only at the rounding level).
+constexpr uint32_t kJacobiBlockRows = 16384;
+constexpr int kJacobiBlockThreads = 1024;
+
+// The block's sum or max of v, returned to EVERY thread (warp_reduce leaves its result in
+// lane 0 only; it is broadcast), so that the branches taken on it -- the residual
+// shortcut, the convergence test -- are the same in the whole block and every thread
+// reaches the same barriers.
+__device__ __forceinline__ double block_allreduce(double v, int op, double* sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_reduce(v, op);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    const double t = warp_reduce(lane < nw ? sh[lane] : red_ident(op), op);
+    return __shfl_sync(0xffffffffu, t, 0); // each warp forms the same value in the same order
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kJacobiBlockThreads) k_jacobi_block(
+    CSRView<T> A, const T* __restrict__ b, T* __restrict__ x, const T* __restrict__ dinv,
+    T* __restrict__ work, fasp_gpu_params prm)
+{
+    __shared__ double sh[32];
+    const uint32_t n = A.nrow;
+    auto xv = [&](uint32_t j) { return x[j]; };
+    double m = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, (double)fabs(x[i]));
+    double xinf = block_allreduce(m, kMax, sh);
+    double denAbs = 1.0;
+    for (uint32_t it = 0; it < prm.maxIter; ++it) {
+        const bool shortcut = xinf < kCloseZero;
+        T rr = T(0);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const T sum = shortcut ? T(0) : row_apply<T, false>(A, i, xv);
+            const T r = b[i] - sum;
+            work[i] = r;
+            rr = fma(r, r, rr);
+        }
+        if (it >= prm.minIter) {
+            const double resAbs = sqrt(block_allreduce((double)rr, kSum, sh));
+            if (it == prm.minIter) denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+            if (resAbs / denAbs < prm.relTol || resAbs < prm.absTol) break;
+        }
+        __syncthreads(); // every row's residual read the old x
+        m = 0.0;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const T xi = x[i] + work[i] * dinv[i];
+            x[i] = xi;
+            m = fmax(m, (double)fabs(xi));
+        }
+        xinf = block_allreduce(m, kMax, sh); // its barriers order the writes of x
+    }
 }
 
 int Pcd::setup(Ctx& c, const Mat* M, int t, double w, const fasp_gpu_params& p)
@@ -140,8 +254,64 @@ int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm
         if (k >= hist->size()) hist->resize((size_t)k + 1, kNaN);
         (*hist)[k] = v;
     };
-    double* xinf = c.dslot + SL_XINF;
     double resAbs = 1.0, resRel = 1.0, denAbs = 1.0;
+    const CSRView<T> V = pcd_view<T>(*A);
+    const bool fusable = A->lanes == 1 && (V.val || V.gnz) && (const void*)b != (const void*)x;
+    if (fusable && !hist && !norm2 && !normInf && n <= kJacobiBlockRows) {
+        // nothing reads the norms back: the whole solve in one single-block launch
+        ++c.launches;
+        k_jacobi_block<T><<<1, kJacobiBlockThreads, 0, c.stream>>>(V, b, x, dinv, work, prm);
+        FB_CUDA(cudaGetLastError());
+        numIter = prm.maxIter; // the convergence test ran on the device
+        return kOk;
+    }
+    if (fusable) {
+        // one launch per sweep; x and work take turns as the sweep's input and output
+        double* xinf[2] = {c.dslot + SL_XINF, c.dslot + SL_XINF2};
+        int e = v_norminf(c, n, x, xinf[0]);
+        if (e) return e;
+        T* cur = x;
+        T* nxt = work;
+        int p = 0;
+        auto sweep = [&](auto kern) {
+            const int g = std::min(c.grid(n, kBlock), resident_grid(c, (const void*)kern, kBlock));
+            kern<<<g, kBlock, 0, c.stream>>>(V, b, cur, dinv, nxt, xinf[p], c.red, xinf[p ^ 1],
+                                            c.dslot + SL_JRES);
+        };
+        numIter = 0;
+        while (numIter < prm.maxIter) {
+            const bool test = numIter >= prm.minIter;
+            ++c.launches;
+            if (test)
+                sweep(k_jacobi_sweep<T, true>);
+            else
+                sweep(k_jacobi_sweep<T, false>);
+            FB_CUDA(cudaGetLastError());
+            if (test) {
+                resAbs = fetch(c.dslot + SL_JRES);
+                if (numIter == prm.minIter) denAbs = (kCloseZero > resAbs) ? kCloseZero : resAbs;
+                resRel = resAbs / denAbs;
+                rec(numIter, resAbs);
+                if (resRel < prm.relTol || resAbs < prm.absTol) break; // x_in stays
+            }
+            std::swap(cur, nxt);
+            p ^= 1;
+            ++numIter;
+        }
+        if (cur != x && (e = v_copy(c, n, (const T*)cur, x))) return e;
+        if (!(numIter == prm.minIter && numIter == prm.maxIter)) {
+            if ((e = m_residual(c, *A, b, x, work, xinf[p]))) return e;
+            v_norm2(c, n, work, c.dslot + SL_T7);
+            v_norminf(c, n, work, c.dslot + SL_T6);
+            resAbs = fetch(c.dslot + SL_T7);
+            const double ni = fetch(c.dslot + SL_T6);
+            if (norm2) *norm2 = resAbs;
+            if (normInf) *normInf = ni;
+            rec(numIter, resAbs);
+        }
+        return kOk;
+    }
+    double* xinf = c.dslot + SL_XINF;
     int e = v_norminf(c, n, x, xinf);
     if (e) return e;
     numIter = 0;

@@ -27,7 +27,10 @@ b moved by one ulp (tests/golden/make_fullsize.py). The bars:
   is 1e-10 over the whole history; BiCGStab on the 96^3 matrices is chaotic in the
   reference itself (one ulp in b moves its history by a factor 57 at Pe 0.1 by iteration
   146), so there the bar is 1e-10 until the reference's own history stops reproducing
-  (entry 20 at Pe 0.1, 27 at Pe 10) and the envelope after it. GMRES/FGMRES run the
+  (entry 20 at Pe 0.1, 27 at Pe 10) and 10 x the envelope after it, until the envelope
+  reaches 1e-2: from there on the reference's trajectories under one-ulp changes have
+  decorrelated, any other rounding gives another equally valid trajectory, and the case is
+  held to its return code, iteration window and solution only. GMRES/FGMRES run the
   reference's modified Gram-Schmidt op sequence here (orth = MGS); the default CGS2 is
   held to the same code, iteration, solution and history bars;
 * adjoint: forward and adjoint iteration counts within +-1, gradient projections on 32
@@ -51,6 +54,7 @@ SOLVER_CASES = sorted(k for k, v in FULL.items() if "alg" in v)
 
 HIST_REL = 1e-10   # history bar where the reference reproduces itself
 FLOOR = 1e-15      # rounding floor of a residual norm, relative to ||r_0||
+DECORRELATED = 1e-2  # envelope level past which histories are not compared entry by entry
 
 
 @pytest.fixture(scope="module")
@@ -92,11 +96,14 @@ def hist_deviation(h_gpu, h_ref):
 
 
 def hist_bound(name, m):
-    """Per-entry relative bound on the first m history entries (module docstring)."""
+    """Per-entry relative bound on the first m history entries (module docstring); inf
+    where the reference's own one-ulp envelope has reached DECORRELATED."""
     env = ARR[name + "__env_dev"]
     run = np.maximum.accumulate(np.nan_to_num(env, nan=0.0))
     ahead = np.minimum(np.arange(m) + 3, len(run) - 1)
-    return np.maximum(HIST_REL, 10.0 * run[ahead])
+    bound = np.maximum(HIST_REL, 10.0 * run[ahead])
+    bound[run[ahead] >= DECORRELATED] = np.inf
+    return bound
 
 
 def check_history(name, h):

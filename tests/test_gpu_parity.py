@@ -13,7 +13,9 @@ C ABI. Tolerances, stated per check:
   rounding floor of a residual norm (1e-15 of the initial residual). The envelope is the
   oracle (pinned bit for bit to the reference) rerun with every entry of b and x0 moved
   by one ulp: the GPU's reordered sums perturb each step by about that much, so where the
-  reference reproduces itself the bar is 1e-10 over the whole history. Cases whose
+  reference reproduces itself the bar is 1e-10 over the whole history; entries past the
+  point where the envelope reaches 1e-2 (the reference's own trajectories have
+  decorrelated: chaotic BiCGStab) are not compared one by one. Cases whose
   stopping test sits at the rounding floor (FLOOR) or that the reference's own history
   shows to be erratic (ERRATIC) are held to the return code and a looser iteration window,
   stated below.
@@ -60,7 +62,10 @@ def history_bound(h_ref, h_env):
         env[m:] = np.inf  # the perturbed run stopped earlier: no bar beyond it
     run = np.maximum.accumulate(env)
     ahead = np.minimum(np.arange(len(h_ref)) + 3, len(h_ref) - 1)
-    return np.maximum(1e-10, 10.0 * run[ahead]) * h_ref + 1e-15 * h_ref[0]
+    bound = np.maximum(1e-10, 10.0 * run[ahead]) * h_ref + 1e-15 * h_ref[0]
+    # past 1e-2 the reference's own perturbed trajectory has decorrelated: not compared
+    bound[run[ahead] >= 1e-2] = np.inf
+    return bound
 
 
 @pytest.fixture(scope="module")
