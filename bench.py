@@ -298,6 +298,15 @@ def run_ours(args):
         return s
 
     mixed, fp64 = make(capi.MIXED_RELIABLE), make(capi.FP64)
+    if args.profile_solve:
+        # for a time-only ncu launch list: three identical mixed solves and nothing else
+        db, dx = sol.DVec.from_numpy(b), sol.DVec(n)
+        for _ in range(3):
+            dx.Scale(0.0)
+            code = mixed.Solve(db, dx)
+            print(f"profile-solve code {code} iterations {mixed.GetIterations()} "
+                  f"{mixed.LastTimeMs():.3f} ms launches {mixed.info.launches}")
+        return 0
     restarted = make(capi.MIXED)
     if args.profile:
         # 3 warm-up + 1 launch of cg_spmv and cg_update per engine: FP32 first, then FP64
@@ -1077,6 +1086,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
                          "one 60-iteration BiCGStab and GMRES(30) solve (krylov96)")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="poisson128: three mixed solves only (for an ncu launch list)")
     ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",
                                            "pcg2d256", "matfree", "mg127"],
                     default="poisson128")

@@ -115,6 +115,7 @@ SIGNATURES = {
     "fasp_gpu_solver_destroy": (_i, [_vp]),
     "fasp_gpu_solver_last_time": (_i, [_vp, _P(_d)]),
     "fasp_gpu_solver_kernel_times": (_i, [_vp, _u32, _i, _P(_d)]),
+    "fasp_gpu_solver_set_barrier_limit": (_i, [_vp, _u32]),
     "fasp_gpu_solver_solve_adjoint": (_i, [_vp, _vp, _vp, _P(Info)]),
     "fasp_gpu_solver_solve_adjoint_async": (_i, [_vp, _vp, _vp, _P(Info), _vp]),
     "fasp_gpu_batch_create": (_i, [_u32, _vp, _u32, _vp, _vp, _vp, _u32, _P(_vp)]),

@@ -751,6 +751,16 @@ int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms)
     return kOk;
 }
 
+int fasp_gpu_solver_set_barrier_limit(fasp_gpu_solver s, uint32_t polls)
+{
+    if (!s) return kErrInputPar;
+    SolverImpl& S = s->s;
+    S.barLimit = polls;
+    if (S.cg64) S.cg64->barLimit = polls;
+    if (S.cg32) S.cg32->barLimit = polls;
+    return kOk;
+}
+
 int fasp_gpu_solver_kernel_times(fasp_gpu_solver s, uint32_t reps, int flushL2, double* ms)
 {
     if (!s || !ms || reps == 0) return kErrInputPar;

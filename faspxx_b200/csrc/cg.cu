@@ -1134,7 +1134,9 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
 }
 
 // Software grid barrier for a co-resident (cooperatively launched) grid. The spin is
-// bounded: after ~2^24 polls it raises bar->error and every block leaves the kernel.
+// bounded: after bar->limit polls (0: 2^24) it raises bar->error and every block leaves the
+// kernel -- a block that was released before the error leaves at its next barrier, where it
+// sees the flag -- so no block waits for good.
 __device__ bool grid_sync(GridBar* bar, unsigned* gen)
 {
     __shared__ int ok;
@@ -1150,12 +1152,13 @@ __device__ bool grid_sync(GridBar* bar, unsigned* gen)
             atomicExch(&bar->gen, g + 1);
         } else {
             unsigned spins = 0;
+            const unsigned limit = bar->limit ? bar->limit : (1u << 24);
             while (ld_acquire_u32(&bar->gen) == g) {
                 if (ld_acquire_u32(&bar->error)) {
                     good = 0;
                     break;
                 }
-                if (++spins > (1u << 24)) {
+                if (++spins > limit) {
                     atomicExch(&bar->error, 1u);
                     good = 0;
                     break;
@@ -1576,11 +1579,14 @@ int CGEngine<T>::run_persistent(unsigned iterCap)
     Scratch s = c->red;
     void* args[] = {&V, &x, &r, &zz, &P0, &P1, &q, (void*)&dinv, &ctl, &s, &bar, &iterCap};
     const void* fn = jacobi ? (const void*)cg_persistent<T, 1> : (const void*)cg_persistent<T, 0>;
+    FB_CUDA(cudaMemcpyAsync(&bar->limit, &barLimit, sizeof(unsigned), cudaMemcpyHostToDevice,
+                            c->stream));
     FB_CUDA(cudaLaunchCooperativeKernel(fn, pgrid, kPBlock, args, 0, c->stream));
     GridBar hb;
     FB_CUDA(cudaMemcpyAsync(&hb, bar, sizeof(GridBar), cudaMemcpyDeviceToHost, c->stream));
     FB_CUDA(cudaStreamSynchronize(c->stream));
     if (hb.error) {
+        // every block has left (the flag releases the others); reset for the next launch
         cudaMemsetAsync(bar, 0, sizeof(GridBar), c->stream);
         cudaStreamSynchronize(c->stream);
         return kErrCuda;

@@ -14,9 +14,10 @@ enum CGReason { kNoReason = 0, kBreakdown = 1, kSave = 2, kStag = 3, kCheck3 = 4
 // The locals of CG::Solve (CG.cxx:55-64) plus the parameters it reads, kept in device
 // memory so that the finalize thread of each fused kernel can run the reference's control
 // flow between iterations without a host round trip.
-// Grid barrier state of the persistent kernel (device memory, zero at creation).
+// Grid barrier state of the persistent kernel (device memory, zero at creation). limit:
+// polls a block makes at one barrier before it gives up (0: 2^24, on the order of a second).
 struct GridBar {
-    unsigned count, gen, error, pad;
+    unsigned count, gen, error, limit;
 };
 
 struct CGCtl {
@@ -113,6 +114,7 @@ struct CGEngine {
     bool       persistent = false;
     int        pgrid = 0;
     GridBar*   bar = nullptr;
+    unsigned   barLimit = 0;      // GridBar::limit written before each persistent launch
     int        run_persistent(unsigned iterCap);
 
     int  init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool graph);

@@ -64,6 +64,7 @@ struct Space {
 
 struct SolverImpl {
     fasp_gpu_config cfg{};
+    unsigned        barLimit = 0;   // persistent CG: polls per grid barrier (0: 2^24)
     Ctx             c;
     Mat*            A = nullptr;    // bound by Setup (borrowed)
     fasp_gpu_mat    Ah = nullptr;

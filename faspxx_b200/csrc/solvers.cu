@@ -417,6 +417,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             if (fusable && cfg.precision == FASP_GPU_FP64) {
                 cg64 = new CGEngine<double>();
                 cg64->wantPersistent = cfg.persistent != 0;
+                cg64->barLimit = barLimit;
                 cg64->pdl = cfg.overlapLaunch != 0;
                 // Jacobi::Setup's diagInv = (1 / diag) * weight, one value for all rows
                 cg64->constDiag = cfg.pcd == 1 && A->diagConst;
@@ -428,6 +429,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 if ((e = Ah->M.ensure32(c.stream))) return e;
                 cg32 = new CGEngine<float>();
                 cg32->wantPersistent = cfg.persistent != 0;
+                cg32->barLimit = barLimit;
                 cg32->pdl = cfg.overlapLaunch != 0;
                 cg32->recurrence = cfg.fp32Recurrence != 0;
                 cg32->constDiag = cfg.pcd == 1 && A->diagConst;

@@ -343,6 +343,12 @@ int fasp_gpu_solver_destroy(fasp_gpu_solver s);
 /* Device time of the last Solve (or adjoint solve) in milliseconds (CUDA events around its
  * device work). */
 int fasp_gpu_solver_last_time(fasp_gpu_solver s, double* ms);
+/* Persistent CG engine (persistent = 1): the number of polls a thread block makes at one
+ * software grid barrier before it gives up (0, the default: 2^24 polls with a 32 ns sleep,
+ * on the order of a second). A barrier that gives up raises an error flag that makes every
+ * block leave the kernel; the solve then returns FASP_GPU_ERROR_CUDA and the context stays
+ * usable (no counterpart in the reference; a failure-detection bound and its test hook). */
+int fasp_gpu_solver_set_barrier_limit(fasp_gpu_solver s, uint32_t polls);
 /* Device-driven CG only: average duration (ms) of each of its two fused kernels over reps
  * launches, timed alone with CUDA events on the solver's stream (control logic bypassed;
  * the solver's internal vectors are overwritten). ms must hold 3 values: ms[0] SpMV

@@ -274,3 +274,42 @@ def mta_cases() -> dict:
         v1, v2 = mta_vectors(A)
         out[name] = (A, v1, v2, z[name + "__v"], m["symmetric_structure"])
     return out
+
+
+# ---- faults on the host side: bad inputs the solvers must report, not hang on -------------
+
+def fault_cases():
+    """name -> (alg, solver keywords, A, b, x0, compare x?) for the inputs CG.cxx:105-119,
+    BiCGStab.cxx:118-124 and Iter.cxx:29-53 meet with NaN/Inf, a zero diagonal, maxIter = 1,
+    a zero right-hand side and a zero matrix (every dot zero: the breakdown branches). The
+    reference's own outcome on each is recorded by running it (tests/test_faults_cpu.py);
+    x is compared only where the reference defines it (its CG breakdown reads an
+    uninitialised alpha)."""
+    from faspxx_b200 import problems as P
+    A = matrix("fdm_10X10")
+    n = A.nrow
+    rng = np.random.default_rng(1)
+    b = A.matvec(rng.random(n))
+    bnan, binf = b.copy(), b.copy()
+    bnan[5], binf[5] = np.nan, np.inf
+    x0nan = np.zeros(n)
+    x0nan[3] = np.nan
+    vals = A.values.copy()
+    vals[A.diag_ptr()[7]] = 0.0
+    Azd = P.CSRMatrix(n, n, A.rowPtr, A.colInd, vals)
+    Az0 = P.CSRMatrix(n, n, A.rowPtr, A.colInd, np.zeros(A.nnz))
+    base = dict(maxIter=100, minIter=0, relTol=1e-8, absTol=0.0)
+    out = {}
+    for alg in ("cg", "bicgstab", "gmres", "fgmres"):
+        for pname, pkw in (("id", {}), ("jac", dict(pcd="jacobi", pcdWeight=1.0, pcdIter=1))):
+            kw = dict(base, **pkw)
+            faults = [("nan_b", A, bnan, np.zeros(n)), ("inf_b", A, binf, np.zeros(n)),
+                      ("nan_x0", A, b, x0nan), ("b0_x0", A, np.zeros(n), np.zeros(n))]
+            if pkw:  # a zero diagonal is a fault only where Jacobi inverts it (Iter.cxx:45-47)
+                faults.append(("zero_diag", Azd, b, np.zeros(n)))
+            for tag, M, bb, x0 in faults:
+                out[f"{alg}_{pname}_{tag}"] = (alg, kw, M, bb, x0, True)
+            out[f"{alg}_{pname}_maxit1"] = (alg, dict(kw, maxIter=1), A, b, np.zeros(n), True)
+        out[f"{alg}_zero_matrix"] = (alg, dict(base), Az0, np.ones(n), np.zeros(n),
+                                     alg not in ("cg", "bicgstab"))
+    return out
