@@ -554,6 +554,26 @@ def run_ours(args):
             cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
 
+    # the other configurations of the path, compactly (one GPU only; about 30 s)
+    workloads = None
+    if rank == 0 and ws == 1 and not args.no_workloads:
+        t0 = time.perf_counter()
+        ref_its = fullsize_reference()
+        p2, p2cpu = pcg2d_results(3, cpu=not args.no_cpu_baseline)
+        if "p2d256_pcg" in ref_its:
+            p2["reference_iterations"] = ref_its["p2d256_pcg"]
+        workloads = {
+            "pcg2d256": {"config": "2D 5-point 256x256, Jacobi-PCG rtol 1e-8, x0 = 0",
+                         "gpu": p2, "cpu_baseline": p2cpu},
+            "krylov96": {"config": "96^3 upwind convection-diffusion, Pe 0.1 and 10, weighted "
+                                   "Jacobi 2/3, rtol 1e-8, GMRES restart fixed at 30",
+                         "results": krylov_results(96, 2, algs=("bicgstab", "gmres"),
+                                                   reference=ref_its)},
+            "batch4096": batch_results(args, None, 0, 1, local, loop_sample=4),
+            "adjoint64": adjoint_results(64, 2, fd_dirs=0),
+        }
+        workloads["wall_s"] = round(time.perf_counter() - t0, 1)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(mixed_ms, 3), "unit": "ms", "n_gpus": ws,
@@ -596,6 +616,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "workloads": workloads,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -603,71 +624,109 @@ def run_ours(args):
     return 0
 
 
-def run_batch(args):
-    """4,096 shifted 2D Poisson systems (m ~ U{16..128}, sigma ~ U[0,1]), 4 right-hand sides
-    each (b ~ N(0,1)), Jacobi-PCG to rtol 1e-8 in one persistent launch, against a loop of
-    per-system FP64 GPU solves (timed on a sample of systems and scaled by total rows)."""
+M_BINS = np.linspace(16, 129, 9)  # strata of the batch's grid sizes m for the loop sample
+
+
+def batch_results(args, dist=None, rank=0, ws=1, local=0, loop_sample=8):
+    """The batched workload: 4,096 shifted 2D Poisson systems (m ~ U{16..128}, sigma ~
+    U[0,1]), 4 right-hand sides each (b ~ N(0,1)), Jacobi-PCG to rtol 1e-8. Under torchrun
+    every rank builds and solves only its share of the systems (shard.partition: LPT by
+    nnz, the same on every rank, no data-path collective) in one persistent launch; the
+    batch's time is the slowest rank's. On one GPU also the loop of per-system FP64 GPU
+    solves it replaces, timed on a stratified sample (loop_sample systems from each of 8
+    bins of m, all 4 right-hand sides) and scaled per bin by the bin's system count."""
     from faspxx_b200 import batch as BT
-    from faspxx_b200 import capi, problems as P, sol
-    capi.init(0)
+    from faspxx_b200 import capi, problems as P, shard as S, sol
     count = args.batch_count
     ms, sig, rhs = P.batch_systems(count=count, nrhs=4, seed=42)
-    mats = BT.shifted_poisson_batch(ms, sig)
-    B = BT.Batch(mats, nrhs=4)
+    work = 5 * ms.astype(np.int64) ** 2
+    shards = S.partition(work, ws)
+    mine = shards[rank]
+    mats = [P.poisson2d(int(ms[i]), shift=float(sig[i])) for i in mine]
+    B = BT.Batch(mats, nrhs=4, device=local)
     b = np.zeros((4, B.N))
-    for k in range(count):
-        b[:, B.sys_row[k]:B.sys_row[k + 1]] = rhs[k]
+    for k, i in enumerate(mine):
+        b[:, B.sys_row[k]:B.sys_row[k + 1]] = rhs[i]
     db = BT._Dev(np.ascontiguousarray(b))
     shape64, _ = B.autotune(b, precision=capi.FP64)
     res = {}
-    for name, prec, tol in (("fp64", capi.FP64, 1e-4), ("mixed", capi.MIXED_RELIABLE, 1e-2),
-                            ("restarted", capi.MIXED, 1e-4)):
-        for _ in range(args.warmup):
+    steps = max(1, min(args.steps, 5))
+    for name, prec, tol in (("fp64", capi.FP64, 1e-4), ("mixed", capi.MIXED_RELIABLE, 1e-2)):
+        for _ in range(2):
             B.solve(db, relTol=1e-8, precision=prec, innerRelTol=tol)
         t = []
-        for _ in range(args.steps):
+        for _ in range(steps):
+            barrier(dist)
             x, it, rr, m = B.solve(db, relTol=1e-8, precision=prec, innerRelTol=tol)
             t.append(m)
-        res[name] = (statistics.mean(t), int(it.sum()), float(rr.max()))
-    # the loop of per-system solves (device-driven FP64 CG, setup excluded), on a sample
-    rng = np.random.default_rng(1)
-    sample = rng.choice(count, size=min(args.batch_sample, count), replace=False)
-    loop_ms, rows = 0.0, 0
-    for k in sample:
-        M = sol.MAT(mats[k])
-        s = sol.configure("cg", maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
-                          pcdWeight=1.0, pcdIter=1)
-        s.Setup(M)
-        n = mats[k].nrow
-        dbk, dxk = sol.DVec(n), sol.DVec(n)
-        for j in range(4):
-            dbk.set(rhs[k][j])
-            dxk.Scale(0.0)
-            lib = capi.lib
-            lib.fasp_gpu_synchronize()
-            t0 = time.perf_counter()
-            s.Solve(dbk, dxk)
-            loop_ms += (time.perf_counter() - t0) * 1e3
-        rows += n
-    loop_full = loop_ms * (B.N / rows)
-    line = {"metric": "Batched Jacobi-PCG, 4096 uneven systems x 4 RHS to rtol 1e-8",
-            "value": round(res["mixed"][0], 3), "unit": "ms", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-            "dtype": "f32 Krylov iterations / f64 reliable updates", "data": "synthetic",
-            "config": {"workload": f"{count} systems, 2D 5-point m~U{{16..128}} + sigma I, "
-                                   f"sigma~U[0,1], 4 RHS b~N(0,1), rows {B.N}, nnz {B.A.nnz}",
-                       "shape": list(shape64)},
-            "fp64_batched_ms": round(res["fp64"][0], 3),
-            "restarted_refinement_ms": round(res["restarted"][0], 3),
-            "iterations_total": {"fp64": res["fp64"][1], "mixed": res["mixed"][1],
-                                 "restarted_inner": res["restarted"][1]},
-            "max_rel_residual": {"fp64": res["fp64"][2], "mixed": res["mixed"][2],
-                                 "restarted": res["restarted"][2]},
-            "loop_per_system_fp64_ms": round(loop_full, 1),
-            "loop_sample": f"{len(sample)} systems x 4 RHS timed, scaled by rows",
-            "speedup_vs_loop": {"fp64": round(loop_full / res["fp64"][0], 1),
-                                "mixed": round(loop_full / res["mixed"][0], 1)}}
-    print(json.dumps(line))
+        res[name] = (dist_max(dist, statistics.mean(t)), int(it.sum()), float(rr.max()))
+    local_res = {"systems": mine.tolist(), "iters": it.tolist(), "rows": int(B.N)}
+    gathered = S.gather_results(dist, rank, ws, local_res)
+    out = {"systems": count, "rows_total": int(sum(int(m) ** 2 for m in ms)),
+           "shape": list(shape64), "ranks": ws,
+           "fp64_ms": round(res["fp64"][0], 3), "mixed_ms": round(res["mixed"][0], 3),
+           "iterations_mixed_this_rank": res["mixed"][1],
+           "max_rel_residual": {"fp64": res["fp64"][2], "mixed": res["mixed"][2]}}
+    if rank == 0 and gathered:
+        out["systems_gathered"] = sum(len(g["systems"]) for g in gathered)
+        out["imbalance"] = round(S.imbalance(work, shards), 4)
+    if ws == 1:
+        # the loop of per-system FP64 GPU solves (device-driven CG, setup excluded), stratified
+        rng = np.random.default_rng(1)
+        loop_total, sampled = 0.0, 0
+        for lo, hi in zip(M_BINS[:-1], M_BINS[1:]):
+            cand = np.nonzero((ms >= lo) & (ms < hi))[0]
+            if len(cand) == 0:
+                continue
+            pick = rng.choice(cand, size=min(loop_sample, len(cand)), replace=False)
+            tsum = 0.0
+            for k in pick:
+                Mk = sol.MAT(P.poisson2d(int(ms[k]), shift=float(sig[k])))
+                s = sol.configure("cg", maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
+                                  pcdWeight=1.0, pcdIter=1)
+                s.Setup(Mk)
+                n = int(ms[k]) ** 2
+                dbk, dxk = sol.DVec(n), sol.DVec(n)
+                for j in range(4):
+                    dbk.set(rhs[k][j])
+                    dxk.Scale(0.0)
+                    capi.lib.fasp_gpu_synchronize()
+                    t0 = time.perf_counter()
+                    s.Solve(dbk, dxk)
+                    tsum += (time.perf_counter() - t0) * 1e3
+            loop_total += tsum / len(pick) * len(cand)
+            sampled += len(pick)
+        out["loop_per_system_fp64_ms"] = round(loop_total, 1)
+        out["loop_sample"] = (f"{sampled} systems (up to {loop_sample} from each of 8 bins of m "
+                              f"over [16, 128]) x 4 RHS timed (host wall clock per solve), "
+                              f"each bin's mean scaled by its system count")
+        out["speedup_vs_loop"] = {"fp64": round(loop_total / res["fp64"][0], 1),
+                                  "mixed": round(loop_total / res["mixed"][0], 1)}
+    return out
+
+
+def run_batch(args):
+    """--workload batch: the batched workload on its own JSON line; under torchrun the
+    systems shard across ranks (strong scaling: the whole batch's time)."""
+    ws, rank, local = dist_env()
+    dist = dist_init(ws)
+    from faspxx_b200 import capi
+    capi.init(local)
+    r = batch_results(args, dist, rank, ws, local)
+    if rank == 0:
+        line = {"metric": "Batched Jacobi-PCG, 4096 uneven systems x 4 RHS to rtol 1e-8",
+                "value": r["mixed_ms"], "unit": "ms", "n_gpus": ws, "steps": args.steps,
+                "warmup": 2, "ms_per_step": r["mixed_ms"], "higher_is_better": False,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32 Krylov iterations / f64 reliable updates", "data": "synthetic",
+                "config": {"workload": "4096 systems, 2D 5-point m~U{16..128} + sigma I, "
+                                       "sigma~U[0,1], 4 RHS b~N(0,1), Jacobi-PCG rtol 1e-8",
+                           "parallelism": f"systems sharded over {ws} ranks (LPT by nnz)"
+                                          if ws > 1 else "single GPU"},
+                "results": r}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 
@@ -684,12 +743,66 @@ def _time_solve(s, db, dx, reps, warm=2, flush=None):
     return statistics.mean(ts), code
 
 
+def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=None):
+    """Nonsymmetric 3D convection-diffusion -Laplace(u) + beta.grad(u) on N^3 (first-order
+    upwind, direction (1, 0.5, 0.25), cell Peclet 0.1 and 10), b = A x* with x* ~ U[-1,1)
+    (seed 42), x0 = 0, rtol 1e-8, weighted Jacobi (omega = 2/3, one sweep), GMRES/FGMRES with
+    a fixed restart of 30: FP64 and FP32 inner iterations inside FP64 refinement (FP64
+    residual, update and Hessenberg/Givens least squares). reference: the reference's
+    iteration counts by case name, where recorded."""
+    from faspxx_b200 import capi, problems as P, sol
+    flush = sol.DVec(32 << 20)
+    rows = []
+    for pe, tag in ((0.1, "pe01"), (10.0, "pe10")):
+        A = P.convdiff3d(N, pe)
+        xs = P.seeded_uniform(A.nrow, 42, -1.0, 1.0)
+        b = A.matvec(xs)
+        M = sol.MAT(A)
+        M.Autotune()
+        db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
+        for alg in algs:
+            res = {}
+            for prec in ("fp64", "mixed"):
+                kw = dict(maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
+                          pcdWeight=2.0 / 3.0, pcdIter=1)
+                if alg != "bicgstab":
+                    kw.update(restart=30, maxRestart=30, minRestart=30)
+                s = sol.configure(alg, **kw)
+                if prec == "mixed":
+                    s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
+                s.Setup(M)
+                ms, code = _time_solve(s, db, dx, steps, flush=flush)
+                x = dx.numpy()
+                rel = float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b))
+                # code 0 at maxIter is the reference's convention (FGMRES.cxx:226 tests
+                # numIter > maxIter): say plainly whether the tolerance was met
+                res[prec] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
+                             "outer": s.info.outerIter if prec == "mixed" else None,
+                             "rel_residual": rel,
+                             "converged": bool(rel <= 1.01e-8),
+                             "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
+            row = {"peclet": pe, "solver": alg, **{k: v for k, v in res.items()},
+                   "mixed_over_fp64": round(res["mixed"]["ms"] / res["fp64"]["ms"], 3)}
+            key = f"cd{N}_{tag}_{alg}"
+            if reference and key in reference:
+                row["reference_iterations"] = reference[key]
+            rows.append(row)
+    return rows
+
+
+def fullsize_reference():
+    """Iteration counts of the reference on the full-size systems, recorded from the reference
+    compiled from its own sources (tests/golden/fullsize.json); {} when absent."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "fullsize.json")) as f:
+            d = json.load(f)
+    except OSError:
+        return {}
+    return {k: v["iters"] for k, v in d.items() if "iters" in v}
+
+
 def run_krylov(args):
-    """Nonsymmetric 3D convection-diffusion -Laplace(u) + beta.grad(u) on 96^3 (n = 884,736,
-    7-point, first-order upwind, direction (1, 0.5, 0.25), cell Peclet 0.1 and 10), b = A x*
-    with x* ~ U[-1,1) (seed 42), x0 = 0, rtol 1e-8, weighted Jacobi (omega = 2/3, one sweep):
-    BiCGStab, GMRES(30) and FGMRES(30) in FP64 and with FP32 inner iterations inside FP64
-    refinement (FP64 residual, update and Hessenberg/Givens least squares)."""
+    """--workload krylov96: BiCGStab / GMRES(30) / FGMRES(30) at 96^3, FP64 and mixed."""
     from faspxx_b200 import capi, problems as P, sol
     capi.init(0)
     N = args.size if args.size != N_GRID else 96
@@ -713,39 +826,8 @@ def run_krylov(args):
             print(f"profile {alg} code {code} iterations {s.GetIterations()} "
                   f"{s.LastTimeMs():.3f} ms")
         return 0
-    flush = sol.DVec(32 << 20)
-    rows, total_mixed = [], 0.0
-    for pe in (0.1, 10.0):
-        A = P.convdiff3d(N, pe)
-        xs = P.seeded_uniform(A.nrow, 42, -1.0, 1.0)
-        b = A.matvec(xs)
-        M = sol.MAT(A)
-        M.Autotune()
-        db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
-        for alg in ("bicgstab", "gmres", "fgmres"):
-            res = {}
-            for prec in ("fp64", "mixed"):
-                kw = dict(maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
-                          pcdWeight=2.0 / 3.0, pcdIter=1)
-                if alg != "bicgstab":
-                    kw.update(restart=30, maxRestart=30, minRestart=30)
-                s = sol.configure(alg, **kw)
-                if prec == "mixed":
-                    s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
-                s.Setup(M)
-                ms, code = _time_solve(s, db, dx, args.steps, flush=flush)
-                x = dx.numpy()
-                rel = float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b))
-                # code 0 at maxIter is the reference's convention (FGMRES.cxx:226 tests
-                # numIter > maxIter): say plainly whether the tolerance was met
-                res[prec] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
-                             "outer": s.info.outerIter if prec == "mixed" else None,
-                             "rel_residual": rel,
-                             "converged": bool(rel <= 1.01e-8),
-                             "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
-            total_mixed += res["mixed"]["ms"]
-            rows.append({"peclet": pe, "solver": alg, **{k: v for k, v in res.items()},
-                         "mixed_over_fp64": round(res["mixed"]["ms"] / res["fp64"]["ms"], 3)})
+    rows = krylov_results(N, args.steps, reference=fullsize_reference())
+    total_mixed = sum(r["mixed"]["ms"] for r in rows)
     line = {"metric": "Time to rtol 1e-8, 96^3 convection-diffusion, BiCGStab / GMRES(30) / "
                       "FGMRES(30): FP32-inner refinement vs FP64",
             "value": round(total_mixed, 3), "unit": "ms (sum of the six mixed solves)",
@@ -759,16 +841,14 @@ def run_krylov(args):
     return 0
 
 
-def run_adjoint(args):
+def adjoint_results(N, steps, fd_dirs):
     """Differentiable solve of -div(kappa grad u) = b on 64^3 (kappa = exp(N(0,1)) per cell,
     harmonic face averages; b ~ N(0,1)); loss 0.5 ||x - x_t||^2 (x_t ~ N(0,1)). Forward CG to
     rtol 1e-10 (Jacobi), backward the adjoint CG on the exact transpose + the sampled outer
     product. FP64 and FP32-iteration (reliable-update) variants; gradients checked by central
     differences (eps 1e-6) along 32 seeded random directions and against the FP64 gradient."""
     from faspxx_b200 import capi, problems as P, sol
-    capi.init(0)
     lib = capi.lib
-    N = args.size if args.size != N_GRID else 64
     rng = np.random.default_rng(42)
     kappa = np.exp(rng.standard_normal(N ** 3))
     A = P.vardiff3d(N, kappa)
@@ -792,7 +872,7 @@ def run_adjoint(args):
         s = make(M, prec)
         fwd, bwd, outer_ms = [], [], []
         info = capi.Info()
-        for i in range(2 + args.steps):
+        for i in range(2 + steps):
             dx.Scale(0.0)
             s.Solve(db, dx)
             f = s.LastTimeMs()
@@ -836,7 +916,7 @@ def run_adjoint(args):
 
     errs = []
     drng = np.random.default_rng(7)
-    for _ in range(args.fd_dirs):
+    for _ in range(fd_dirs):
         dbdir = drng.standard_normal(n)
         dAdir = drng.standard_normal(nnz) * np.abs(A.values)
         lp = loss(A.values + eps * dAdir, b + eps * dbdir)
@@ -845,31 +925,56 @@ def run_adjoint(args):
         an = float(np.dot(g64b, dbdir) + np.dot(g64A, dAdir))
         errs.append(abs(fd - an) / max(abs(an), 1e-300))
     del s64, x0
+    out_d = {"n": n, "nnz": nnz,
+             "fp64": {k: v for k, v in out["fp64"].items() if not k.startswith(("grad", "x"))},
+             "fp32_iter": {k: v for k, v in out["fp32_iter"].items()
+                           if not k.startswith(("grad", "x"))},
+             "fp32_iter_grad_rel_err_vs_fp64": {"b": rel(out["fp32_iter"]["grad_b"], g64b),
+                                                 "A": rel(out["fp32_iter"]["grad_A"], g64A)},
+             "central_difference": {"directions": fd_dirs, "eps": eps,
+                                    "max_rel_err": max(errs) if errs else None,
+                                    "median_rel_err": statistics.median(errs) if errs else None}}
+    # against the reference's own gradient (recorded from the reference compiled from its
+    # sources: forward CG, adjoint CG on its MAT::TransInPlace, -lambda_i x_j), projected on
+    # the same 32 seeded directions
+    try:
+        z = np.load(os.path.join(ROOT, "tests", "golden", "fullsize.npz"))
+        proj_ref = z["vd64_adjoint__proj"]
+        drng = np.random.default_rng(7)
+        proj = np.array([float(np.dot(g64b, drng.standard_normal(n)) +
+                               np.dot(g64A, drng.standard_normal(nnz))) for _ in range(32)])
+        if N == 64:
+            out_d["fp64_grad_vs_reference_projections_max_rel_err"] = float(
+                np.max(np.abs(proj - proj_ref) / np.abs(proj_ref)))
+    except (OSError, KeyError):
+        pass
+    return out_d
+
+
+def run_adjoint(args):
+    """--workload adjoint64: the differentiable 64^3 solve on its own JSON line."""
+    from faspxx_b200 import capi
+    capi.init(0)
+    N = args.size if args.size != N_GRID else 64
+    r = adjoint_results(N, args.steps, args.fd_dirs)
     line = {"metric": "Differentiable 64^3 variable-coefficient solve: forward + adjoint time, "
                       "gradient agreement",
-            "value": round(out["fp64"]["forward_ms"] + out["fp64"]["adjoint_ms"], 3),
+            "value": round(r["fp64"]["forward_ms"] + r["fp64"]["adjoint_ms"], 3),
             "unit": "ms (FP64 forward + adjoint)", "n_gpus": 1, "steps": args.steps,
             "warmup": 2, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{N}^3 -div(kappa grad u), kappa=exp(N(0,1)), n={n}, "
-                                   f"nnz={nnz}, CG rtol 1e-10, Jacobi"},
-            "fp64": {k: v for k, v in out["fp64"].items() if not k.startswith(("grad", "x"))},
-            "fp32_iter": {k: v for k, v in out["fp32_iter"].items()
-                          if not k.startswith(("grad", "x"))},
-            "fp32_iter_grad_rel_err_vs_fp64": {"b": rel(out["fp32_iter"]["grad_b"], g64b),
-                                                "A": rel(out["fp32_iter"]["grad_A"], g64A)},
-            "central_difference": {"directions": args.fd_dirs, "eps": eps,
-                                   "max_rel_err": max(errs) if errs else None,
-                                   "median_rel_err": statistics.median(errs) if errs else None}}
+            "config": {"workload": f"{N}^3 -div(kappa grad u), kappa=exp(N(0,1)), "
+                                   f"n={r['n']}, nnz={r['nnz']}, CG rtol 1e-10, Jacobi"},
+            "results": r}
     print(json.dumps(line))
     return 0
 
 
-def run_pcg2d(args):
+def pcg2d_results(steps, cpu=True):
     """2D 5-point Poisson on a 256 x 256 grid (n = 65,536, nnz = 326,656), x* ~ U[0,1) (seed
     42), b = A x*, x0 = 0, Jacobi-PCG to rtol 1e-8, max 2000 iterations: the reference's PCG
-    example at its own size, device-driven FP64 and FP32-iteration (reliable-update) CG."""
+    example at its own size, device-driven FP64 and FP32-iteration (reliable-update) CG; with
+    cpu, one complete solve by the reference (compiled from its sources) on the host."""
     from faspxx_b200 import capi, problems as P, sol
-    capi.init(0)
     A = P.poisson2d(256)
     xs = P.seeded_uniform(A.nrow, 42)
     b = A.matvec(xs)
@@ -884,19 +989,27 @@ def run_pcg2d(args):
         if prec != capi.FP64:
             s.SetPrecision(prec, innerRelTol=1e-2)
         s.Setup(M)
-        ms, code = _time_solve(s, db, dx, args.steps, flush=flush)
+        ms, code = _time_solve(s, db, dx, steps, flush=flush)
         x = dx.numpy()
         res[name] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
                      "rel_residual": float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)),
                      "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
-    cpu = None
-    if not args.no_cpu_baseline:
+    cpu_res = None
+    if cpu:
         from oracle import oracle as O
         kind = "ref" if os.path.exists(O.REF_SO) else "port"
-        per_iter, _ = reference_sample(A, b, 200, kind)
-        cpu = {"value": round(per_iter * res["fp64"]["iters"], 2), "unit": "ms", "cores": 1,
-               "kind": "reference" if kind == "ref" else "port",
-               "sample": "200 Jacobi-PCG iterations, scaled by the FP64 iteration count"}
+        full_ms, iters, code = reference_full(A, b, kind)
+        cpu_res = {"value": round(full_ms, 2), "unit": "ms", "cores": 1,
+                   "kind": "reference" if kind == "ref" else "port", "iterations": iters,
+                   "sample": "one complete Jacobi-PCG solve of the same system on the host"}
+    return res, cpu_res
+
+
+def run_pcg2d(args):
+    """--workload pcg2d256: the reference's PCG example at 256 x 256."""
+    from faspxx_b200 import capi
+    capi.init(0)
+    res, cpu = pcg2d_results(args.steps, cpu=not args.no_cpu_baseline)
     line = {"metric": "Time to rtol 1e-8, 2D Poisson 256x256 Jacobi-PCG",
             "value": res["fp64"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
             "warmup": 2, "higher_is_better": False, "dtype": "f64", "data": "synthetic",
@@ -1082,6 +1195,8 @@ def main():
                     help="reliable-update factor of the headline mixed solve")
     ap.add_argument("--ref-sample", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="leave out the other configurations' compact block")
     ap.add_argument("--lanes", type=int, default=0, help="force SpMV lanes per row")
     ap.add_argument("--profile", action="store_true",
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
