@@ -279,6 +279,8 @@ def run_ours(args):
     n, nnz = A.nrow, A.nnz
     M = sol.MAT(A)
     lanes = M.Autotune() if not args.lanes else (M.SetLanes(args.lanes) or args.lanes)
+    if args.form == "csr":
+        M.SetRowClass(0)
 
     def make(precision):
         s = sol.CG()
@@ -302,7 +304,7 @@ def run_ours(args):
         # for a time-only ncu launch list: three identical mixed solves and nothing else
         db, dx = sol.DVec.from_numpy(b), sol.DVec(n)
         for _ in range(3):
-            dx.Scale(0.0)
+            dx.Zero()
             code = mixed.Solve(db, dx)
             print(f"profile-solve code {code} iterations {mixed.GetIterations()} "
                   f"{mixed.LastTimeMs():.3f} ms launches {mixed.info.launches}")
@@ -323,7 +325,7 @@ def run_ours(args):
     l2flush = sol.DVec(32 << 20)
 
     def solve(s):
-        dx.Scale(0.0)  # x0 = 0 on the device
+        dx.Zero()  # x0 = 0 on the device
         l2flush.Norm2()
         code = s.Solve(db, dx)
         if code != 0:
@@ -338,7 +340,7 @@ def run_ours(args):
     # accuracy of each variant: FP64 residual and error against an FP64 CG solve to 1e-13
     tight = make(capi.FP64)
     tight.SetRelTol(1e-13)
-    dx.Scale(0.0)
+    dx.Zero()
     tight.Solve(db, dx)
     xref = dx.numpy()
     del tight
@@ -386,13 +388,17 @@ def run_ours(args):
     rc_mode_used = M.RowClassInfo()[0]
     M.SetRowClass(0)
     csr_res = {}
-    for tag, prec in (("mixed", capi.MIXED_RELIABLE), ("fp64", capi.FP64)):
-        sc = make(prec)
-        for _ in range(2):
-            solve(sc)
-        ts = [solve(sc) for _ in range(args.steps)]
-        csr_res[tag] = (dist_max(dist, statistics.mean(t[0] for t in ts)), ts[-1][1])
-        del sc
+    for col16 in (True, False):
+        M.SetCol16(col16)
+        for tag, prec in (("mixed", capi.MIXED_RELIABLE), ("fp64", capi.FP64)):
+            sc = make(prec)
+            for _ in range(2):
+                solve(sc)
+            ts = [solve(sc) for _ in range(args.steps)]
+            csr_res[(tag, col16)] = (dist_max(dist, statistics.mean(t[0] for t in ts)),
+                                     ts[-1][1])
+            del sc
+    M.SetCol16(True)
     M.SetRowClass(rc_mode_used)
 
     # end to end: host b, x0 in pinned memory -> device -> solve -> x back to host
@@ -590,12 +596,16 @@ def run_ours(args):
                        "reliable_update_delta": args.delta,
                        "precision_mode": "MIXED_RELIABLE"},
             "fp64_ms": round(fp64_ms, 3), "mixed_over_fp64": round(mixed_ms / fp64_ms, 3),
-            "csr_form": {"mixed_ms": round(csr_res["mixed"][0], 3),
-                         "fp64_ms": round(csr_res["fp64"][0], 3),
-                         "iterations": csr_res["fp64"][1],
-                         "note": "the same solves with the matrix in plain CSR form (no "
-                                 "row-class or stencil-mask compression), as a general "
-                                 "FASP++ matrix runs"},
+            "csr_form": {"mixed_ms": round(csr_res[("mixed", True)][0], 3),
+                         "fp64_ms": round(csr_res[("fp64", True)][0], 3),
+                         "iterations": csr_res[("fp64", True)][1],
+                         "col32_mixed_ms": round(csr_res[("mixed", False)][0], 3),
+                         "col32_fp64_ms": round(csr_res[("fp64", False)][0], 3),
+                         "note": "the same solves with the matrix in CSR form (no row-class "
+                                 "or stencil-mask compression), as a general FASP++ matrix "
+                                 "runs: with 16-bit column offsets (every entry of this "
+                                 "matrix is within 16,384 columns of its row) and, col32_*, "
+                                 "with the 32-bit column indices"},
             "restarted_refinement": {"ms": round(restarted_ms, 3),
                                      "over_fp64": round(restarted_ms / fp64_ms, 3),
                                      "inner_rel_tol": args.inner_tol,
@@ -689,7 +699,7 @@ def batch_results(args, dist=None, rank=0, ws=1, local=0, loop_sample=8):
                 dbk, dxk = sol.DVec(n), sol.DVec(n)
                 for j in range(4):
                     dbk.set(rhs[k][j])
-                    dxk.Scale(0.0)
+                    dxk.Zero()
                     capi.lib.fasp_gpu_synchronize()
                     t0 = time.perf_counter()
                     s.Solve(dbk, dxk)
@@ -734,7 +744,7 @@ def _time_solve(s, db, dx, reps, warm=2, flush=None):
     """Mean device time (ms) of reps solves from x0 = 0 (after warm untimed ones)."""
     ts = []
     for i in range(warm + reps):
-        dx.Scale(0.0)
+        dx.Zero()
         if flush is not None:
             flush.Norm2()  # read-only: evicts L2 without leaving dirty lines
         code = s.Solve(db, dx)
@@ -821,7 +831,7 @@ def run_krylov(args):
                 kw.update(restart=30, maxRestart=30, minRestart=30)
             s = sol.configure(alg, **kw)
             s.Setup(M)
-            dx.Scale(0.0)
+            dx.Zero()
             code = s.Solve(db, dx)
             print(f"profile {alg} code {code} iterations {s.GetIterations()} "
                   f"{s.LastTimeMs():.3f} ms")
@@ -873,12 +883,12 @@ def adjoint_results(N, steps, fd_dirs):
         fwd, bwd, outer_ms = [], [], []
         info = capi.Info()
         for i in range(2 + steps):
-            dx.Scale(0.0)
+            dx.Zero()
             s.Solve(db, dx)
             f = s.LastTimeMs()
             x = dx.numpy()
             dg.set(x - xt)
-            dlam.Scale(0.0)  # lambda0 = 0
+            dlam.Zero()  # lambda0 = 0
             lib.fasp_gpu_synchronize()
             capi.check(lib.fasp_gpu_solver_solve_adjoint(s.h, dg.ptr, dlam.ptr, C.byref(info)),
                        "adjoint")
@@ -1201,6 +1211,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
                          "one 60-iteration BiCGStab and GMRES(30) solve (krylov96)")
+    ap.add_argument("--form", choices=["auto", "csr"], default="auto",
+                    help="poisson128: matrix form of the solves (csr: plain CSR, as a general "
+                         "matrix; auto: the compressed form the matrix admits)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="poisson128: three mixed solves only (for an ncu launch list)")
     ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",

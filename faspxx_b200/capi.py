@@ -59,6 +59,7 @@ SIGNATURES = {
     "fasp_gpu_free": (_i, [_vp]),
     "fasp_gpu_memcpy_h2d": (_i, [_vp, _vp, _sz]),
     "fasp_gpu_memcpy_d2h": (_i, [_vp, _vp, _sz]),
+    "fasp_gpu_memset": (_i, [_vp, _i, _sz]),
     "fasp_gpu_synchronize": (_i, []),
     "fasp_gpu_host_alloc": (_i, [_P(_vp), _sz]),
     "fasp_gpu_host_free": (_i, [_vp]),
@@ -81,6 +82,8 @@ SIGNATURES = {
     "fasp_gpu_mat_set_rowclass": (_i, [_vp, _i]),
     "fasp_gpu_mat_rowclass_info": (_i, [_vp, _P(_i), _P(_u32), _P(_u32), _P(_u32)]),
     "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _i, _P(_d)]),
+    "fasp_gpu_mat_set_col16": (_i, [_vp, _i]),
+    "fasp_gpu_mat_col16_info": (_i, [_vp, _P(_i), _P(_i)]),
     "fasp_gpu_mat_sampled_outer": (_i, [_vp, _vp, _vp, _d, _vp]),
     "fasp_gpu_mat_mult_transpose_add": (_i, [_vp, _vp, _vp, _vp]),
     "fasp_gpu_mat_apply_async": (_i, [_vp, _vp, _vp, _vp]),

@@ -538,6 +538,10 @@ static void with_k(int k, F&& f)
 // threads in a fixed tree and the last block adds the blocks in order: MODE 1's dots equal
 // MODE 2 (sign 1) followed by MODE 0 bit for bit, and reruns give the same bits.
 constexpr int kGsMaxK = 32;
+// basis vectors per batch when two element groups share it (2 in the fused mode, which
+// keeps both groups of w live across its two passes)
+template <int MODE>
+__host__ __device__ constexpr int gs_pair() { return MODE == 1 ? 2 : 4; }
 // loads in flight per batch: 8 basis groups, 4 in the fused mode (which also keeps w's
 // group live across its two passes; 8 there exceeds the 85-register budget)
 template <int MODE>
@@ -595,19 +599,65 @@ k_gs(uint32_t n, int k, const T* __restrict__ V, size_t ld, const double* __rest
                 }
         }
     };
-    const size_t nv = n / W;
-    GRID_STRIDE(iv, nv)
-    {
-        auto ld16 = [&](int j, T* out) { *(VT*)out = ((const VT*)(V + j * ld))[iv]; };
-        T wv[W];
-        *(VT*)wv = ((const VT*)w)[iv];
-        if (MODE >= 1) {
-            project(wv, ld16);
-            ((VT*)w)[iv] = *(VT*)wv;
+    // 16-byte groups, two at a time: a thread's groups iv and iv + stride share each batch
+    // of gs_pair basis vectors, so twice as many loads are in flight per wait and a thread
+    // waits half as often; each dot still adds group iv's elements before group iv +
+    // stride's
+    constexpr int kGsPair = gs_pair<MODE>();
+    const size_t nv = n / W, stride = (size_t)gridDim.x * bd;
+    for (size_t iv = (size_t)blockIdx.x * bd + tid; iv < nv; iv += 2 * stride) {
+        const int ng = iv + stride < nv ? 2 : 1;
+        const size_t ivs[2] = {iv, iv + stride};
+        T wv[2][W];
 #pragma unroll
-            for (int e = 0; e < W; ++e) nrm = fma(wv[e], wv[e], nrm);
+        for (int u = 0; u < 2; ++u)
+            if (u < ng) *(VT*)wv[u] = ((const VT*)w)[ivs[u]];
+        auto batch = [&](int j0, T (&vv)[2][kGsPair][W]) {
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+#pragma unroll
+                for (int q = 0; q < kGsPair; ++q)
+                    if (u < ng && j0 + q < k)
+                        *(VT*)vv[u][q] = ((const VT*)(V + (j0 + q) * ld))[ivs[u]];
+        };
+        if (MODE >= 1) {
+            for (int j0 = 0; j0 < k; j0 += kGsPair) {
+                T vv[2][kGsPair][W];
+                batch(j0, vv);
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+#pragma unroll
+                    for (int q = 0; q < kGsPair; ++q)
+                        if (u < ng && j0 + q < k)
+#pragma unroll
+                            for (int e = 0; e < W; ++e)
+                                wv[u][e] = fma(-sh[j0 + q], vv[u][q][e], wv[u][e]);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (u < ng) {
+                    ((VT*)w)[ivs[u]] = *(VT*)wv[u];
+#pragma unroll
+                    for (int e = 0; e < W; ++e) nrm = fma(wv[u][e], wv[u][e], nrm);
+                }
         }
-        if (MODE <= 1) dots(wv, ld16);
+        if (MODE <= 1) {
+            for (int j0 = 0; j0 < k; j0 += kGsPair) {
+                T vv[2][kGsPair][W];
+                batch(j0, vv);
+#pragma unroll
+                for (int q = 0; q < kGsPair; ++q)
+                    if (j0 + q < k) {
+                        T a = sacc[(j0 + q) * bd + tid];
+#pragma unroll
+                        for (int u = 0; u < 2; ++u)
+                            if (u < ng)
+#pragma unroll
+                                for (int e = 0; e < W; ++e) a = fma(vv[u][q][e], wv[u][e], a);
+                        sacc[(j0 + q) * bd + tid] = a;
+                    }
+            }
+        }
     }
     for (size_t i = nv * W + (size_t)blockIdx.x * bd + tid; i < n; i += (size_t)gridDim.x * bd) {
         auto ld1 = [&](int j, T* out) {

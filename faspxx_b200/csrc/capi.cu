@@ -239,6 +239,12 @@ int fasp_gpu_memcpy_d2h(void* dst, const void* src, size_t bytes)
     return kOk;
 }
 
+int fasp_gpu_memset(void* dst, int value, size_t bytes)
+{
+    FB_CUDA(cudaMemset(dst, value, bytes));
+    return kOk;
+}
+
 int fasp_gpu_synchronize(void)
 {
     FB_CUDA(cudaDeviceSynchronize());
@@ -489,6 +495,21 @@ int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode)
     if (A->M.grid) return kOk; // a grid operator has no stored form to choose
     A->M.rcOn = mode >= 1 && A->M.rcCls != nullptr;
     A->M.skOn = mode == 2;
+    return kOk;
+}
+
+int fasp_gpu_mat_set_col16(fasp_gpu_mat A, int on)
+{
+    if (!A) return kErrInputPar;
+    A->M.cd16On = on != 0;
+    return kOk;
+}
+
+int fasp_gpu_mat_col16_info(fasp_gpu_mat A, int* built, int* inUse)
+{
+    if (!A) return kErrInputPar;
+    if (built) *built = A->M.cd16 != nullptr;
+    if (inUse) *inUse = A->M.cd16 != nullptr && A->M.cd16On && !A->M.rcOn;
     return kOk;
 }
 

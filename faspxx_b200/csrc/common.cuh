@@ -181,6 +181,10 @@ struct CSRView {
     uint32_t        nrow, mcol, nnz;
     const uint32_t* rowPtr;
     const uint32_t* colInd;
+    // 16-bit column offsets (optional, thread-per-row kernels): colInd[k] - row as int16_t,
+    // present when every entry of the matrix is within 32,767 columns of its row; the
+    // thread-per-row kernels then stream 2 bytes per entry instead of 4.
+    const int16_t*  cd16;
     const T*        val;   // nullptr: pattern only (every stored entry is 1)
     // Row classes (optional, thread-per-row kernels): rows with identical column offsets
     // (col - row) and values share one table entry; cls[row] picks it. Entries of class k
@@ -255,6 +259,7 @@ __device__ __forceinline__ uint32_t grid_mask(const V& A, uint32_t row)
 // The matrix is streamed once per SpMV: evict-first loads keep it from displacing the
 // vectors, which are reused every iteration and fit in the 126 MB L2 at the benchmark sizes.
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) { return __ldcs(p); }
+__device__ __forceinline__ int16_t ld_stream(const int16_t* p) { return __ldcs(p); }
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
 __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 
@@ -263,7 +268,8 @@ __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 // column/value loads issued before any gather, so a 7-entry stencil row has all its
 // matrix loads in flight at once.
 template <typename T, bool PAT, typename XV>
-__device__ __forceinline__ T row_dot(const CSRView<T>& A, uint32_t b, uint32_t e, XV xv)
+__device__ __forceinline__ T row_dot(const CSRView<T>& A, size_t row, uint32_t b, uint32_t e,
+                                     XV xv)
 {
     T s = T(0);
 #pragma unroll 2
@@ -273,7 +279,10 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, uint32_t b, uint32_t e
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const bool in = k + u < e;
-            c[u] = in ? ld_stream(A.colInd + k + u) : 0u;
+            if (A.cd16)
+                c[u] = in ? (uint32_t)((long long)row + ld_stream(A.cd16 + k + u)) : 0u;
+            else
+                c[u] = in ? ld_stream(A.colInd + k + u) : 0u;
             v[u] = PAT ? T(in ? 1 : 0) : (in ? ld_stream(A.val + k + u) : T(0));
         }
 #pragma unroll
@@ -335,7 +344,7 @@ __device__ __forceinline__ T row_apply(const CSRView<T>& A, size_t row, XV xv)
         return s;
     }
     const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
-    return row_dot<T, PAT>(A, b, e, xv);
+    return row_dot<T, PAT>(A, row, b, e, xv);
 }
 
 // Programmatic dependent launch: a kernel launched with the programmatic-serialization

@@ -172,6 +172,8 @@ struct Mat {
     double*   diag = nullptr;    // GetDiag (1 for pattern-only)
     int       lanes = 8;         // lanes per row of the SpMV (autotuned or from row lengths)
     bool      diagConst = false; // every row stores a diagonal entry, all with one value
+    int16_t*  cd16 = nullptr;    // colInd - row when every entry is within 32,767 columns
+    bool      cd16On = true;     // the thread-per-row kernels use cd16 when it is built
     double    diagValue = 0.0;
     uint32_t  maxRowLen = 0;
     double    meanRowLen = 0;
@@ -204,6 +206,7 @@ struct Mat {
         V.nnz = nnz;
         V.rowPtr = rowPtr;
         V.colInd = colInd;
+        V.cd16 = (cd16On && !(rcOn && rcCls && v && cv)) ? cd16 : nullptr;
         V.val = v;
         if (grid) {
             V.ulen = skLen;
@@ -322,6 +325,9 @@ int m_residual(Ctx& c, const Mat& A, const double* b, const double* x, double* r
 int m_residual(Ctx& c, const Mat& A, const float* b, const float* x, float* r,
                const double* xinf);
 int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR -> CSC, exact
+// Builds M.cd16 (16-bit column offsets) when every |col - row| <= 32767; otherwise leaves it
+// null. Synchronises the stream.
+int m_build_col16(Mat& M, cudaStream_t s);
 // v = A^T v1 + v2 on T = m_transpose(A), in MAT::MultTransposeAdd's order (MAT.cxx:541-606)
 int m_mult_transpose_add(Ctx& c, const Mat& T, const double* v1, const double* v2, double* v);
 int lanes_for(double meanRowLen);                                         // SpMV mapping

@@ -26,7 +26,8 @@ PRINT_NONE, PRINT_MIN, PRINT_SOME, PRINT_MORE, PRINT_MAX = 0, 2, 4, 6, 8
 
 
 class DVec:
-    """A VEC resident in device memory (float64)."""
+    """A VEC resident in device memory (float64); DVec(n) holds n zeros, as VEC(size) does
+    (src/VEC.hxx:43)."""
 
     def __init__(self, n: int, host: np.ndarray | None = None):
         capi.init()
@@ -36,6 +37,12 @@ class DVec:
         self.ptr = p
         if host is not None:
             self.set(host)
+        else:
+            self.Zero()
+
+    def Zero(self) -> None:
+        """Every entry 0.0 (a memset: unlike Scale(0.0), it also clears NaN and Inf)."""
+        check(lib.fasp_gpu_memset(self.ptr, 0, max(8, self.n * 8)), "fasp_gpu_memset")
 
     @classmethod
     def from_numpy(cls, a) -> "DVec":
@@ -190,6 +197,16 @@ class MAT:
         classes with stencil masks (the default when built)."""
         mode = 2 if mode is True else (0 if mode is False else int(mode))
         check(lib.fasp_gpu_mat_set_rowclass(self.h, mode), "SetRowClass")
+
+    def SetCol16(self, on: bool) -> None:
+        """Use (True, the default when built) or ignore the 16-bit column offsets."""
+        check(lib.fasp_gpu_mat_set_col16(self.h, 1 if on else 0), "SetCol16")
+
+    def Col16Info(self):
+        """(built, in use) of the 16-bit column offsets."""
+        b, u = C.c_int(), C.c_int()
+        check(lib.fasp_gpu_mat_col16_info(self.h, C.byref(b), C.byref(u)), "Col16Info")
+        return bool(b.value), bool(u.value)
 
     def RowClassInfo(self):
         """(mode in use, classes, table entries, stencil length); 0 classes: no row-class

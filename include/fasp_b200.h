@@ -134,6 +134,7 @@ int fasp_gpu_malloc(void** dptr, size_t bytes);
 int fasp_gpu_free(void* dptr);
 int fasp_gpu_memcpy_h2d(void* dst, const void* src, size_t bytes);
 int fasp_gpu_memcpy_d2h(void* dst, const void* src, size_t bytes);
+int fasp_gpu_memset(void* dptr, int value, size_t bytes); /* every byte set to value */
 int fasp_gpu_synchronize(void);
 int fasp_gpu_host_alloc(void** hptr, size_t bytes); /* page-locked host memory */
 int fasp_gpu_host_free(void* hptr);
@@ -244,6 +245,15 @@ int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes);
 int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode);
 int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uint32_t* entries,
                                uint32_t* stencil);
+/* 16-bit column offsets of the CSR form: built at upload (and for transposes) when every
+ * stored entry lies within 32,767 columns of its row -- banded FDM/FEM matrices, the 128^3
+ * Laplacian's bandwidth is 16,384 -- as colInd[k] - row; the thread-per-row kernels (lanes =
+ * 1) then stream 2 bytes per entry for the columns instead of 4 and form each column by one
+ * add. The entries and their order are unchanged, so results are bit-identical. on = 0
+ * makes the kernels read the 32-bit colInd again (set it before a solver's Setup); info
+ * reports whether the offsets exist and whether they are in use. */
+int fasp_gpu_mat_set_col16(fasp_gpu_mat A, int on);
+int fasp_gpu_mat_col16_info(fasp_gpu_mat A, int* built, int* inUse);
 /* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
  * value copy (fp32 = 1), timed with CUDA events on the matrix's stream (inputs: x = 0). */
 int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2,

@@ -10,8 +10,9 @@ reference's (the reference itself prints 6 significant digits, which are cross-c
 Stored per case (the solutions are too large to commit whole): code, iterations, norms,
 the full-precision residual history, the reference's printed history, the solution at
 8,192 seeded positions, its 2-norm and sum, and the case's sensitivity envelope: the same
-algorithm (the restatement) rerun with every entry of b moved by one ulp up or down
-(seeded), its iteration count, solution difference and per-iteration history deviation.
+algorithm (the restatement) rerun four times with every entry of b moved by one ulp up or
+down (four seeds), the iteration counts, the largest solution difference and, per
+iteration, the largest history deviation.
 A GPU that sums in another order perturbs every step by about that much, so the envelope
 shows how closely any reordered implementation can follow the reference on the case.
 Cases:
@@ -46,6 +47,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 NSAMPLE = 8192
+ENV_SEEDS = (1, 2, 3, 4)
 SYN = dict(minIter=0, absTol=0.0)
 JAC1 = dict(pcd="jacobi", pcdWeight=1.0, pcdIter=1)
 JAC23 = dict(pcd="jacobi", pcdWeight=2.0 / 3.0, pcdIter=1)
@@ -136,17 +138,27 @@ def run_solver_case(name: str):
     if rel.size and rel.max() > 1e-5:
         raise AssertionError(f"{name}: printed history differs ({rel.max():.2e})")
     idx = sample_index(A.nrow)
-    # sensitivity envelope: every entry of b moved by one ulp, up or down (seeded)
-    up = np.random.default_rng(1).random(A.nrow) < 0.5
-    bp = np.where(up, np.nextafter(b, np.inf), np.nextafter(b, -np.inf))
-    pert = O.Solver("port", A, alg, **kw).solve(bp, x0)
-    mp = min(len(pert.hist), len(port.hist))
-    env = np.abs(pert.hist[:mp] - port.hist[:mp]) / np.maximum(port.hist[:mp], 1e-300)
+    # sensitivity envelope: every entry of b moved by one ulp, up or down, four seeded
+    # times; per entry the largest deviation of the four histories, the iteration counts and
+    # the largest solution difference
+    env = np.zeros(len(port.hist))
+    its, xdev, codes = [], 0.0, []
+    for seed in ENV_SEEDS:
+        up = np.random.default_rng(seed).random(A.nrow) < 0.5
+        bp = np.where(up, np.nextafter(b, np.inf), np.nextafter(b, -np.inf))
+        pert = O.Solver("port", A, alg, **kw).solve(bp, x0)
+        mp = min(len(pert.hist), len(port.hist))
+        dev = np.abs(pert.hist[:mp] - port.hist[:mp]) / np.maximum(port.hist[:mp], 1e-300)
+        env[:mp] = np.fmax(env[:mp], dev)
+        if mp < len(env):
+            env[mp:] = np.inf  # a perturbed run stopped earlier: nothing to compare
+        its.append(pert.iters)
+        codes.append(pert.code)
+        xdev = max(xdev, float(np.max(np.abs(pert.x[idx] - ref.x[idx])) / np.max(np.abs(ref.x))))
     over = np.nonzero(env > 1e-10)[0]
-    envelope = dict(iters=pert.iters, code=pert.code, hist_max=float(np.nanmax(env)),
-                    first_over_1e10=int(over[0]) if len(over) else None,
-                    x_dev=float(np.max(np.abs(pert.x[idx] - ref.x[idx])) /
-                                np.max(np.abs(ref.x))))
+    envelope = dict(iters=its, codes=codes, hist_max=float(np.nanmax(env[np.isfinite(env)])),
+                    first_over_1e10=int(over[0]) if len(over) else None, x_dev=xdev,
+                    seeds=list(ENV_SEEDS))
     meta = dict(alg=alg, spec=list(spec), rhs=rk, kw=kw, n=A.nrow, nnz=A.nnz, code=ref.code,
                 iters=ref.iters, norm2=ref.norm2, normInf=ref.normInf,
                 x_norm2=float(np.linalg.norm(ref.x)), x_sum=float(ref.x.sum()),

@@ -12,12 +12,12 @@ Bars (stated per check):
 The GPU sums every dot product and norm in another order than the reference's sequential
 loops (VEC.cxx:424-485), which perturbs each step by about one ulp. How much such a
 perturbation can move a solve is measured on the reference's algorithm itself: the
-fixtures hold each case's sensitivity envelope, the restatement rerun with every entry of
-b moved by one ulp (tests/golden/make_fullsize.py). The bars:
+fixtures hold each case's sensitivity envelope, the restatement rerun four times with every
+entry of b moved by one ulp (four seeds; tests/golden/make_fullsize.py). The bars:
 
-* return code equal to the reference's; iteration count within max(1, the envelope's
-  iteration difference) -- +-1 everywhere except BiCGStab at Pe 10, whose own envelope moves
-  by 2;
+* return code equal to the reference's; iteration count within max(1, the largest
+  iteration difference of the envelope's four perturbed runs) -- +-1 everywhere except
+  BiCGStab, whose own perturbed runs move by up to 2;
 * solution at 8,192 seeded positions within max(1e-6, 10 x the envelope's difference) of
   max|x|, its 2-norm within the same relative bound;
 * residual history, entry k: within max(1e-10, 10 x the envelope's largest deviation up to
@@ -119,7 +119,7 @@ def check_history(name, h):
 
 def iter_window(name):
     meta = FULL[name]
-    return max(1, abs(meta["envelope"]["iters"] - meta["iters"]))
+    return max([1] + [abs(i - meta["iters"]) for i in meta["envelope"]["iters"]])
 
 
 def check_solution(name, x):
