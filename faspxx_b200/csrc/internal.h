@@ -173,7 +173,8 @@ struct Mat {
     int       lanes = 8;         // lanes per row of the SpMV (autotuned or from row lengths)
     bool      diagConst = false; // every row stores a diagonal entry, all with one value
     int16_t*  cd16 = nullptr;    // colInd - row when every entry is within 32,767 columns
-    bool      cd16On = true;     // the thread-per-row kernels use cd16 when it is built
+    bool      cd16On = false;    // the thread-per-row kernels use cd16 (opt-in: measured
+                                 // slower than the 32-bit colInd on B200)
     double    diagValue = 0.0;
     uint32_t  maxRowLen = 0;
     double    meanRowLen = 0;

@@ -199,7 +199,7 @@ class MAT:
         check(lib.fasp_gpu_mat_set_rowclass(self.h, mode), "SetRowClass")
 
     def SetCol16(self, on: bool) -> None:
-        """Use (True, the default when built) or ignore the 16-bit column offsets."""
+        """Use (True) or ignore (False, the default) the 16-bit column offsets."""
         check(lib.fasp_gpu_mat_set_col16(self.h, 1 if on else 0), "SetCol16")
 
     def Col16Info(self):

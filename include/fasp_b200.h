@@ -245,13 +245,14 @@ int fasp_gpu_mat_set_lanes(fasp_gpu_mat A, int lanes);
 int fasp_gpu_mat_set_rowclass(fasp_gpu_mat A, int mode);
 int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uint32_t* entries,
                                uint32_t* stencil);
-/* 16-bit column offsets of the CSR form: built at upload (and for transposes) when every
- * stored entry lies within 32,767 columns of its row -- banded FDM/FEM matrices, the 128^3
- * Laplacian's bandwidth is 16,384 -- as colInd[k] - row; the thread-per-row kernels (lanes =
- * 1) then stream 2 bytes per entry for the columns instead of 4 and form each column by one
- * add. The entries and their order are unchanged, so results are bit-identical. on = 0
- * makes the kernels read the 32-bit colInd again (set it before a solver's Setup); info
- * reports whether the offsets exist and whether they are in use. */
+/* 16-bit column offsets of the CSR form (opt-in): built at upload (and for transposes) when
+ * every stored entry lies within 32,767 columns of its row -- banded FDM/FEM matrices, the
+ * 128^3 Laplacian's bandwidth is 16,384 -- as colInd[k] - row; with on = 1 the
+ * thread-per-row kernels (lanes = 1) stream 2 bytes per entry for the columns instead of 4
+ * and form each column by one add. The entries and their order are unchanged, so results
+ * are bit-identical. Off by default: on B200 the 2-byte loads measured slower than the
+ * 4-byte colInd (128^3 CSR CG, FP32 iterations 17.4 against 14.9 ms). Set it before a
+ * solver's Setup; info reports whether the offsets exist and whether they are in use. */
 int fasp_gpu_mat_set_col16(fasp_gpu_mat A, int on);
 int fasp_gpu_mat_col16_info(fasp_gpu_mat A, int* built, int* inUse);
 /* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
