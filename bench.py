@@ -596,6 +596,8 @@ def run_ours(args):
                        "reliable_update_delta": args.delta,
                        "precision_mode": "MIXED_RELIABLE"},
             "fp64_ms": round(fp64_ms, 3), "mixed_over_fp64": round(mixed_ms / fp64_ms, 3),
+            "step_ms": {"mixed": [round(t, 3) for t in times],
+                        "fp64": [round(t, 3) for t in times64]},
             "csr_form": {"mixed_ms": round(csr_res[("mixed", False)][0], 3),
                          "fp64_ms": round(csr_res[("fp64", False)][0], 3),
                          "iterations": csr_res[("fp64", False)][1],

@@ -84,6 +84,8 @@ SIGNATURES = {
     "fasp_gpu_mat_time_apply": (_i, [_vp, _u32, _i, _i, _P(_d)]),
     "fasp_gpu_mat_set_col16": (_i, [_vp, _i]),
     "fasp_gpu_mat_col16_info": (_i, [_vp, _P(_i), _P(_i)]),
+    "fasp_gpu_mat_tile_info": (_i, [_vp, _P(_u32), _P(_i), _P(_i), _P(_i)]),
+    "fasp_gpu_tile_timeouts": (_i, [_P(_u32)]),
     "fasp_gpu_mat_sampled_outer": (_i, [_vp, _vp, _vp, _d, _vp]),
     "fasp_gpu_mat_mult_transpose_add": (_i, [_vp, _vp, _vp, _vp]),
     "fasp_gpu_mat_apply_async": (_i, [_vp, _vp, _vp, _vp]),

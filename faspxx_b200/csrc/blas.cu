@@ -7,6 +7,7 @@
 // results agree to rounding, not bit for bit.
 #include <cstdint>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <type_traits>
 
@@ -18,16 +19,17 @@ namespace fb {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < (size_t)(n); \
          i += (size_t)gridDim.x * blockDim.x)
 
-int resident_grid(const Ctx& c, const void* fn, int block)
+int resident_grid(const Ctx& c, const void* fn, int block, size_t smem)
 {
     static std::mutex mu;
-    static std::map<std::pair<const void*, int>, int> cache;
+    static std::map<std::tuple<const void*, int, size_t>, int> cache;
     std::lock_guard<std::mutex> lock(mu);
-    const auto key = std::make_pair(fn, block);
+    const auto key = std::make_tuple(fn, block, smem);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0) != cudaSuccess || nb < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, smem) != cudaSuccess ||
+        nb < 1) {
         cudaGetLastError();
         nb = 1;
     }
@@ -35,6 +37,23 @@ int resident_grid(const Ctx& c, const void* fn, int block)
     if (g > kMaxGrid) g = kMaxGrid;
     cache[key] = (int)g;
     return (int)g;
+}
+
+bool tiles_fit(const void* fn, size_t smem)
+{
+    static std::mutex mu;
+    static std::map<const void*, size_t> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(fn);
+    if (it == cache.end()) {
+        cudaFuncAttributes at{};
+        if (cudaFuncGetAttributes(&at, fn) != cudaSuccess) {
+            cudaGetLastError();
+            at.sharedSizeBytes = 48 * 1024; // unknown: no tiles
+        }
+        it = cache.emplace(fn, at.sharedSizeBytes).first;
+    }
+    return it->second + smem <= 48 * 1024;
 }
 
 int Ctx::grid(long long work, int perBlock, int perSM) const

@@ -513,6 +513,27 @@ int fasp_gpu_mat_col16_info(fasp_gpu_mat A, int* built, int* inUse)
     return kOk;
 }
 
+int fasp_gpu_mat_tile_info(fasp_gpu_mat A, uint32_t* span, int* fits64, int* fits32,
+                           int* inUse)
+{
+    if (!A) return kErrInputPar;
+    const Mat& M = A->M;
+    const bool f64 = M.tileSpan > 0 && M.tileSpan <= TileShape<double>::cap;
+    const bool f32 = M.tileSpan > 0 && M.tileSpan <= TileShape<float>::cap;
+    if (span) *span = M.tileSpan;
+    if (fits64) *fits64 = f64;
+    if (fits32) *fits32 = f32;
+    if (inUse) *inUse = !M.grid && !M.rcOn && !(M.cd16 && M.cd16On) && M.lanes == 1;
+    return kOk;
+}
+
+int fasp_gpu_tile_timeouts(uint32_t* count)
+{
+    if (!count) return kErrInputPar;
+    *count = tile_timeouts_spmv() + tile_timeouts_solvers();
+    return kOk;
+}
+
 int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uint32_t* entries,
                                uint32_t* stencil)
 {

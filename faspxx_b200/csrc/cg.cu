@@ -759,10 +759,7 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
             ownr(row, sum);
         }
     } else if (L == 1) { // thread per row
-        const size_t stride = (size_t)gridDim.x * blockDim.x;
-        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += stride)
-            ownr(row, row_apply<T, false>(A, row, gv));
+        for_rows<T, false>(A, gv, ownr);
     }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
@@ -1355,6 +1352,10 @@ void CGEngine<T>::launch_spmv_kernel()
     const int jm = jmode();
     const T* zz = jm == 1 ? z : r;
     const int sh = stencil_shape(V);
+    // The fused iteration kernels walk CSR rows one at a time, without block tiles: with its
+    // p, q, x updates per row a tile's block barrier stalls every warp on the slowest one,
+    // and on B200 the 128^3 CSR solves measured slower with tiles (mixed 16.3 against 14.9
+    // ms, FP64 28.9 against 25.0 ms) although the product alone is faster.
     auto go = [&](auto kern) {
         const int g = std::min(need, resident_grid(*c, (const void*)kern, kBlock));
         launch_overlapped(kern, g, c->stream, pdl, V, zz, P0, P1, q, x, ctl, c->red,

@@ -213,6 +213,11 @@ struct CSRView {
     uint32_t        gmx, gmxy;      // FastDiv multipliers for nx and nx ny
     uint8_t         gsx[2], gsxy[2]; // and their shifts
     uint16_t        glo[12], ghi[12];
+    // Block tiles of plain CSR (csr_tile_rows): tileSpan is the most entries any 256-row
+    // tile covers once widened to multiples of 4 (from the upload; 0 unknown), and tiles is
+    // set by a launch that gives its blocks the tile stages (with_tiles).
+    uint32_t        tileSpan;
+    uint32_t        tiles;
 };
 
 // Division of a 32-bit unsigned n by a divisor fixed at launch (Granlund and Montgomery,
@@ -292,6 +297,178 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, size_t row, uint32_t b
     return s;
 }
 
+// ---- block tiles of plain CSR, streamed by bulk async copies ------------------------------
+// Thread per row streams each row's column indices and values on its own: the lanes of a
+// warp read 4-byte words some 28 bytes apart (a 7-entry row), and a thread has one row's
+// loads in flight at a time, too few bytes to cover the latency of HBM. A block tile takes
+// 256 consecutive rows, one per thread, whose entries are one contiguous range: one thread
+// copies the tile's row pointers, column indices and values into shared memory with bulk
+// asynchronous copies (cp.async.bulk, completion counted in bytes on an mbarrier), two
+// tiles ahead, so the copy engine keeps the stream in flight while the threads gather x for
+// the current tile. Each thread sums its row from the stage in CSR order with one FMA per
+// entry (the bits of row_dot). The copies start at an entry index that is a multiple of 4
+// (16-byte aligned) and run to the next multiple of 4 past the tile's last entry: up to 3
+// entries beyond nnz, inside the spare bytes every matrix array is allocated with.
+constexpr uint32_t kTileRows = 256; // rows per tile = threads per block
+constexpr int kTileStages = 2;
+constexpr uint32_t kTileRp = kTileRows + 4;
+
+template <typename T>
+struct TileShape {
+    // bytes per stage: 2 stages and the kernels' own static shared memory (at most 3 KB)
+    // stay under the 48 KB a launch gets without opting in; FP32 takes less so that more
+    // blocks fit on an SM. Both hold a 256-row tile of a 7-point stencil (1,798 entries).
+    static constexpr uint32_t bytes = sizeof(T) == 8 ? 22800u : 16000u;
+    static constexpr uint32_t cap = ((bytes - kTileRp * 4u) / (4u + sizeof(T))) & ~3u;
+};
+
+template <typename T>
+struct alignas(16) TileStage {
+    uint32_t rp[kTileRp];
+    uint32_t c[TileShape<T>::cap];
+    T v[TileShape<T>::cap];
+};
+
+template <typename T>
+struct alignas(16) TileSmem {
+    TileStage<T> st[kTileStages];
+    unsigned long long full[kTileStages]; // mbarriers: one phase per copied tile
+    uint32_t a[kTileStages];              // the stage's first entry index
+    uint32_t ok[kTileStages];             // entries staged (else only the row pointers)
+};
+
+// Waits that ran out (a bulk copy that never completed): counted here, per translation
+// unit, and read by tile_timeouts() on the host.
+static __device__ unsigned fb_tile_timeouts;
+
+extern __shared__ __align__(16) unsigned char fb_tile_smem[];
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// An L2 policy that marks the lines it touches first to evict: the matrix is streamed once
+// per product, and at normal priority it would push the solver's vectors (reused every
+// iteration, resident in the 126 MB L2 at the benchmark sizes) out of L2, as the
+// evict-first loads (ld_stream) of the row-at-a-time kernels do not.
+__device__ __forceinline__ unsigned long long l2_evict_first()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              unsigned long long* bar, unsigned long long pol)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 ".L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
+                 : "memory");
+}
+
+// At most 2^20 polls (each try_wait itself suspends for a bounded time), then false.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < (1u << 20); ++it) {
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+                     "selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done)
+                     : "r"(smem_addr(bar)), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Rows of a plain CSR view in block tiles; own(row, sum) on the row's thread. Block b takes
+// tiles b, b + G, b + 2G, ... (G = gridDim.x), so thread t of the grid owns rows t, t + S,
+// t + 2S, ... (S = the grid's threads) in that order, as the row-at-a-time loops do. Every
+// thread of the block calls it (it synchronises the block). A tile whose entries do not fit
+// a stage (only possible when the caller ignored the span check of with_tiles) is summed
+// from global memory.
+template <typename T, bool PAT, typename XV, typename OWN>
+__device__ __forceinline__ void csr_tile_rows(const CSRView<T>& A, TileSmem<T>& sm, XV xv,
+                                              OWN own)
+{
+    constexpr uint32_t CAP = TileShape<T>::cap;
+    const size_t n = A.nrow;
+    const size_t ntiles = (n + kTileRows - 1) / kTileRows;
+    const uint32_t tid = threadIdx.x;
+    const size_t mine =
+        blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const unsigned long long pol = tid == 0 ? l2_evict_first() : 0ull;
+    auto issue = [&](size_t k) { // thread 0: tile k of this block into stage k % stages
+        const int s = (int)(k % kTileStages);
+        const size_t r0 = (blockIdx.x + k * gridDim.x) * kTileRows;
+        const size_t rows = n - r0 < kTileRows ? n - r0 : kTileRows;
+        const uint32_t beg = A.rowPtr[r0], end = A.rowPtr[r0 + rows];
+        const uint32_t a = beg & ~3u, ar = (uint32_t)(((size_t)end + 3) & ~size_t(3));
+        const bool ok = ar - a <= CAP;
+        const uint32_t rpn = (uint32_t)((rows + 1 + 3) & ~size_t(3));
+        const uint32_t eb = PAT ? 4u : 4u + (uint32_t)sizeof(T);
+        sm.a[s] = a;
+        sm.ok[s] = ok ? 1u : 0u;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_addr(&sm.full[s])),
+                     "r"(rpn * 4u + (ok ? (ar - a) * eb : 0u))
+                     : "memory");
+        bulk_copy_g2s(sm.st[s].rp, A.rowPtr + r0, rpn * 4u, &sm.full[s], pol);
+        if (ok && ar > a) {
+            bulk_copy_g2s(sm.st[s].c, A.colInd + a, (ar - a) * 4u, &sm.full[s], pol);
+            if (!PAT)
+                bulk_copy_g2s(sm.st[s].v, A.val + a, (ar - a) * (uint32_t)sizeof(T),
+                              &sm.full[s], pol);
+        }
+    };
+    if (tid == 0) {
+        for (int s = 0; s < kTileStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&sm.full[s]))
+                         : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (size_t k = 0; k < (size_t)kTileStages && k < mine; ++k) issue(k);
+    }
+    __syncthreads();
+    for (size_t k = 0; k < mine; ++k) {
+        const int s = (int)(k % kTileStages);
+        if (!mbar_wait_bounded(&sm.full[s], (uint32_t)((k / kTileStages) & 1)))
+            atomicAdd(&fb_tile_timeouts, 1u);
+        const size_t row = (blockIdx.x + k * gridDim.x) * kTileRows + tid;
+        if (row < n) {
+            const TileStage<T>& st = sm.st[s];
+            const uint32_t b = st.rp[tid], e = st.rp[tid + 1];
+            T sum = T(0);
+            if (sm.ok[s]) {
+                const uint32_t a = sm.a[s];
+#pragma unroll 2
+                for (uint32_t k4 = b; k4 < e; k4 += 4) {
+                    uint32_t cc[4];
+                    T v[4], xs[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const bool in = k4 + u < e;
+                        cc[u] = in ? st.c[k4 + u - a] : 0u;
+                        v[u] = PAT ? T(in ? 1 : 0) : (in ? st.v[k4 + u - a] : T(0));
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) xs[u] = k4 + u < e ? xv(cc[u]) : T(0);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (k4 + u < e) sum = fma(v[u], xs[u], sum);
+                }
+            } else {
+                sum = row_dot<T, PAT>(A, row, b, e, xv);
+            }
+            own(row, sum);
+        }
+        __syncthreads(); // stage s is free again
+        if (tid == 0 && k + kTileStages < mine) issue(k + kTileStages);
+    }
+}
+
 // Row `row` of A times the gathered vector, through the row-class table when A has one
 // (2 bytes streamed per row instead of the row's column indices and values), else through
 // the CSR arrays. Both accumulate the entries in CSR order with one FMA each, so the two
@@ -345,6 +522,51 @@ __device__ __forceinline__ T row_apply(const CSRView<T>& A, size_t row, XV xv)
     }
     const uint32_t b = ld_stream(A.rowPtr + row), e = ld_stream(A.rowPtr + row + 1);
     return row_dot<T, PAT>(A, row, b, e, xv);
+}
+
+// Every row of A once, own(row, sum) on the thread that owns it: thread t of the grid owns
+// rows t, t + S, t + 2S, ... (S = the grid's threads) in that order. Views launched with
+// block tiles (A.tiles, see with_tiles) stream them; call it with every thread of the block.
+template <typename T, bool PAT, typename XV, typename OWN>
+__device__ __forceinline__ void for_rows(const CSRView<T>& A, XV xv, OWN own)
+{
+    if (A.tiles) {
+        csr_tile_rows<T, PAT>(A, *reinterpret_cast<TileSmem<T>*>(fb_tile_smem), xv, own);
+        return;
+    }
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+         row += stride)
+        own(row, row_apply<T, PAT>(A, row, xv));
+}
+
+// Block tiles for a plain CSR view (no row classes, stencil masks, grid form or 16-bit
+// offsets) whose every 256-row tile fits a stage (tileSpan, from the upload), with 16-byte
+// aligned arrays, launched with blocks of kTileRows threads: marks the view and returns the
+// dynamic shared memory its kernel must be launched with (0, view unmarked, otherwise).
+// Launchers then call tiles_fit with the kernel, which unmarks the view again when the
+// kernel's static shared memory and the stages together exceed 48 KB.
+template <typename T>
+inline size_t with_tiles(CSRView<T>& V, int block)
+{
+    auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+    const bool ok = V.nrow > 0 && !V.cls && !V.mask && !V.gnz && !V.cd16 &&
+                    V.tileSpan > 0 && V.tileSpan <= TileShape<T>::cap &&
+                    block == (int)kTileRows && al(V.rowPtr) && al(V.colInd) &&
+                    (!V.val || al(V.val));
+    V.tiles = ok ? 1u : 0u;
+    return ok ? sizeof(TileSmem<T>) : 0;
+}
+
+// This translation unit's count of tile waits that ran out.
+static inline unsigned tile_timeouts()
+{
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, fb_tile_timeouts, sizeof(v)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return v;
 }
 
 // Programmatic dependent launch: a kernel launched with the programmatic-serialization

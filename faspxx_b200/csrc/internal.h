@@ -99,7 +99,10 @@ int on_stream(Ctx& c, cudaStream_t user, F&& work)
 // Blocks of `fn` at `block` threads that are resident at once on the whole device (one
 // wave): SM count x the occupancy limit (registers, shared memory), capped at kMaxGrid.
 // Grid-stride kernels launched with min(work, this) never run a partial second wave.
-int resident_grid(const Ctx& c, const void* fn, int block);
+int resident_grid(const Ctx& c, const void* fn, int block, size_t smem = 0);
+// Whether fn's static shared memory plus smem bytes of block tiles stay within the 48 KB a
+// launch gets without opting in (else the launcher runs the kernel without tiles).
+bool tiles_fit(const void* fn, size_t smem);
 
 // Reads `bytes` of `buf` (a multiple of 16) through L2 on stream s and writes nothing (blas.cu):
 // after a read of more than the L2's 126 MB, L2 holds only clean lines of buf, so a kernel
@@ -175,6 +178,7 @@ struct Mat {
     int16_t*  cd16 = nullptr;    // colInd - row when every entry is within 32,767 columns
     bool      cd16On = false;    // the thread-per-row kernels use cd16 (opt-in: measured
                                  // slower than the 32-bit colInd on B200)
+    uint32_t  tileSpan = 0;      // most entries of a 256-row tile (m_tile_span), 0 unknown
     double    diagValue = 0.0;
     uint32_t  maxRowLen = 0;
     double    meanRowLen = 0;
@@ -209,6 +213,7 @@ struct Mat {
         V.colInd = colInd;
         V.cd16 = (cd16On && !(rcOn && rcCls && v && cv)) ? cd16 : nullptr;
         V.val = v;
+        V.tileSpan = tileSpan;
         if (grid) {
             V.ulen = skLen;
             for (uint32_t u = 0; u < skLen; ++u) {
@@ -329,6 +334,12 @@ int m_transpose(Ctx& c, const Mat& A, Mat& T);                            // CSR
 // Builds M.cd16 (16-bit column offsets) when every |col - row| <= 32767; otherwise leaves it
 // null. Synchronises the stream.
 int m_build_col16(Mat& M, cudaStream_t s);
+// Mat::tileSpan from the row pointers (the block tiles' fit test, csr_tile_rows).
+int m_tile_span(Mat& M, cudaStream_t s);
+// Tile waits that ran out in the kernels of spmv.cu and solvers.cu (bulk copies that never
+// landed).
+unsigned tile_timeouts_spmv();
+unsigned tile_timeouts_solvers();
 // v = A^T v1 + v2 on T = m_transpose(A), in MAT::MultTransposeAdd's order (MAT.cxx:541-606)
 int m_mult_transpose_add(Ctx& c, const Mat& T, const double* v1, const double* v2, double* v);
 int lanes_for(double meanRowLen);                                         // SpMV mapping

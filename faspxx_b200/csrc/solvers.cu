@@ -1479,10 +1479,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_apply(CSRView<T> A, const T* __re
     if (*stop) return;
     auto xv = [&](uint32_t j) { return MODE == 1 ? v[j] * dinv[j] : v[j]; };
     auto out = [&](size_t row, T sum) { y[row] = MODE == 2 ? sum * dinv[row] : sum; };
-    if (L == 1) {
-        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += (size_t)gridDim.x * blockDim.x)
-            out(row, row_apply<T, false>(A, row, xv));
+    if (L == 1) { // thread per row, or block tiles of plain CSR (A.tiles)
+        for_rows<T, false>(A, xv, out);
         return;
     }
     const int lane = threadIdx.x & (L - 1);
@@ -1575,12 +1573,11 @@ __global__ void __launch_bounds__(kBlock) k_fg_apply(CSRView<T> A, const T* __re
 {
     if (*stop) return;
     auto xv = [&](uint32_t j) { return t[j]; };
-    if (L == 1) {
-        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += (size_t)gridDim.x * blockDim.x) {
-            y[row] = row_apply<T, false>(A, row, xv);
+    if (L == 1) { // thread per row, or block tiles of plain CSR (A.tiles)
+        for_rows<T, false>(A, xv, [&](size_t row, T sum) {
+            y[row] = sum;
             z[row] = t[row];
-        }
+        });
         return;
     }
     const int lane = threadIdx.x & (L - 1);
@@ -1620,9 +1617,13 @@ static void gm_apply_launch(Ctx& c, const Mat& A, CSRView<T> V, const T* v, cons
                             T* y, const int* stop)
 {
     const int need = c.grid((long long)A.nrow * A.lanes, kBlock);
+    const size_t tiles = A.lanes == 1 ? with_tiles(V, kBlock) : 0;
     auto go = [&](auto kern) {
-        kern<<<std::min(need, resident_grid(c, (const void*)kern, kBlock)), kBlock, 0,
-               c.stream>>>(V, v, dinv, y, stop);
+        CSRView<T> W = V;
+        size_t smem = tiles;
+        if (smem && !tiles_fit((const void*)kern, smem)) W.tiles = 0, smem = 0;
+        kern<<<std::min(need, resident_grid(c, (const void*)kern, kBlock, smem)), kBlock, smem,
+               c.stream>>>(W, v, dinv, y, stop);
     };
     switch (A.lanes) {
         case 1: go(k_gm_apply<T, 1, MODE>); break;
@@ -1697,8 +1698,11 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
             }
             lanes_launch<T>(c, *S.A, [&](auto LL) {
                 auto kern = k_fg_apply<T, decltype(LL)::value>;
-                kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock)), kBlock, 0,
-                       c.stream>>>(AV, t, zj, vnew, stop);
+                CSRView<T> W = AV;
+                size_t smem = S.A->lanes == 1 ? with_tiles(W, kBlock) : 0;
+                if (smem && !tiles_fit((const void*)kern, smem)) W.tiles = 0, smem = 0;
+                kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock, smem)),
+                       kBlock, smem, c.stream>>>(W, t, zj, vnew, stop);
             });
         } else if (mode == 0)
             gm_apply_launch<T, 0>(c, *S.A, AV, vin, dinv, vnew, stop);
@@ -2335,5 +2339,7 @@ int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
     info->launches = (uint32_t)(c.launches - l0);
     return e;
 }
+
+unsigned tile_timeouts_solvers() { return tile_timeouts(); }
 
 } // namespace fb

@@ -63,11 +63,8 @@ template <typename T, int L, bool PAT>
 __global__ void __launch_bounds__(kBlock) k_spmv(CSRView<T> A, const T* __restrict__ x,
                                                  T* __restrict__ y)
 {
-    if (L == 1) { // thread per row: short rows (stencils)
-        auto xv = [&](uint32_t j) { return x[j]; };
-        const size_t stride = (size_t)gridDim.x * blockDim.x;
-        for (size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x; r < A.nrow; r += stride)
-            y[r] = row_apply<T, PAT>(A, r, xv);
+    if (L == 1) { // thread per row, or warp tiles of plain CSR: short rows (stencils)
+        for_rows<T, PAT>(A, [&](uint32_t j) { return x[j]; }, [&](size_t r, T s) { y[r] = s; });
         return;
     }
     const int lane = threadIdx.x & (L - 1);
@@ -99,11 +96,13 @@ __global__ void __launch_bounds__(kBlock) k_residual(CSRView<T> A, const T* __re
 {
     const bool shortcut = *xinf < kCloseZero;
     if (L == 1) {
-        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += (size_t)gridDim.x * blockDim.x) {
-            T s = T(0);
-            if (!shortcut) s = row_apply<T, false>(A, row, [&](uint32_t j) { return x[j]; });
-            r[row] = b[row] - s;
+        if (shortcut) {
+            for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+                 row += (size_t)gridDim.x * blockDim.x)
+                r[row] = b[row] - T(0);
+        } else {
+            for_rows<T, false>(A, [&](uint32_t j) { return x[j]; },
+                               [&](size_t row, T s) { r[row] = b[row] - s; });
         }
         return;
     }
@@ -164,9 +163,13 @@ static int launch_spmv(Ctx& c, CSRView<T> A, int L, const T* x, T* y)
             return kOk;
         }
     }
+    const size_t tiles = L == 1 ? with_tiles(A, kBlock) : 0;
     auto go = [&](auto kern) {
-        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c.stream>>>(A, x, y);
+        CSRView<T> V = A;
+        size_t smem = tiles;
+        if (smem && !tiles_fit((const void*)kern, smem)) V.tiles = 0, smem = 0;
+        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock, smem));
+        kern<<<g, kBlock, smem, c.stream>>>(V, x, y);
     };
 #define SPMV_CASE(LL)                                                                     \
     case LL:                                                                              \
@@ -229,9 +232,13 @@ static int residual_t(Ctx& c, const Mat& A, CSRView<T> V, const T* b, const T* x
             return kOk;
         }
     }
+    const size_t tiles = A.lanes == 1 ? with_tiles(V, kBlock) : 0;
     auto go = [&](auto kern) {
-        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock));
-        kern<<<g, kBlock, 0, c.stream>>>(V, b, x, r, xinf);
+        CSRView<T> W = V;
+        size_t smem = tiles;
+        if (smem && !tiles_fit((const void*)kern, smem)) W.tiles = 0, smem = 0;
+        const int g = std::min(need, resident_grid(c, (const void*)kern, kBlock, smem));
+        kern<<<g, kBlock, smem, c.stream>>>(W, b, x, r, xinf);
     };
     ++c.launches;
     switch (A.lanes) {
@@ -289,8 +296,9 @@ __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restri
 
 static int dmalloc(void** p, size_t bytes)
 {
-    // 16 spare bytes keep vectorised/bulk tail accesses inside the allocation
-    cudaError_t e = cudaMalloc(p, bytes + 16);
+    // 32 spare bytes keep vectorised/bulk tail accesses inside the allocation (the warp
+    // tiles' 16-byte loads read up to 3 entries past the last one)
+    cudaError_t e = cudaMalloc(p, bytes + 32);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
@@ -366,6 +374,47 @@ int m_build_col16(Mat& M, cudaStream_t s)
     M.cd16 = out;
     return kOk;
 }
+
+// The most entries any 256-row tile covers once widened to multiples of 4: the block tiles
+// of csr_tile_rows take a matrix only when every tile fits a stage.
+__global__ void k_tile_span(uint32_t nrow, const uint32_t* __restrict__ rowPtr,
+                            unsigned* __restrict__ span)
+{
+    const size_t ntiles = ((size_t)nrow + kTileRows - 1) / kTileRows;
+    unsigned m = 0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < ntiles;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t r0 = t * kTileRows;
+        const size_t r1 = r0 + kTileRows < nrow ? r0 + kTileRows : nrow;
+        const unsigned long long a = rowPtr[r0] & ~3u;
+        const unsigned long long ar = ((unsigned long long)rowPtr[r1] + 3) & ~3ull;
+        const unsigned long long w = ar - a;
+        m = max(m, (unsigned)(w < 0xffffffffull ? w : 0xffffffffull));
+    }
+    atomicMax(span, m);
+}
+
+int m_tile_span(Mat& M, cudaStream_t s)
+{
+    M.tileSpan = 0;
+    if (M.grid || M.nrow == 0 || !M.rowPtr) return kOk;
+    unsigned* d = nullptr;
+    int e;
+    if ((e = dmalloc((void**)&d, 4))) return e;
+    FB_CUDA(cudaMemsetAsync(d, 0, 4, s));
+    const int tiles = ceil_div(M.nrow, (int)kTileRows);
+    k_tile_span<<<std::max(1, std::min(ceil_div(tiles, kBlock), 148 * 8)), kBlock, 0, s>>>(
+        M.nrow, M.rowPtr, d);
+    FB_CUDA(cudaGetLastError());
+    unsigned h = 0;
+    FB_CUDA(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+    cudaFree(d);
+    M.tileSpan = h;
+    return kOk;
+}
+
+unsigned tile_timeouts_spmv() { return tile_timeouts(); }
 
 // ---- row classes ------------------------------------------------------------------------
 // A row's class is its length, its column offsets col - row and its values (bit patterns),
@@ -588,7 +637,7 @@ int m_upload(Mat& M, uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t*
             return e;
         }
     }
-    if ((e = m_build_col16(T, s))) {
+    if ((e = m_build_col16(T, s)) || (e = m_tile_span(T, s))) {
         m_free(T);
         return e;
     }
@@ -775,7 +824,7 @@ int m_transpose(Ctx& c, const Mat& A, Mat& T)
     FB_CUDA(cudaMemcpy(hrp.data(), R.rowPtr, hrp.size() * 4, cudaMemcpyDeviceToHost));
     for (uint32_t j = 0; j < m; ++j) R.maxRowLen = std::max(R.maxRowLen, hrp[j + 1] - hrp[j]);
     R.lanes = A.lanes;
-    if ((e = m_build_col16(R, s))) {
+    if ((e = m_build_col16(R, s)) || (e = m_tile_span(R, s))) {
         m_free(R);
         return e;
     }

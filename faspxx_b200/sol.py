@@ -208,6 +208,15 @@ class MAT:
         check(lib.fasp_gpu_mat_col16_info(self.h, C.byref(b), C.byref(u)), "Col16Info")
         return bool(b.value), bool(u.value)
 
+    def TileInfo(self):
+        """(span, fits FP64, fits FP32, CSR form with one thread per row in use) of the
+        block tiles: the most entries a 256-row tile covers and whether every tile fits a
+        stage; the tiles run where the form is in use and the tile fits."""
+        sp, f64, f32, u = C.c_uint32(), C.c_int(), C.c_int(), C.c_int()
+        check(lib.fasp_gpu_mat_tile_info(self.h, C.byref(sp), C.byref(f64), C.byref(f32),
+                                         C.byref(u)), "TileInfo")
+        return sp.value, bool(f64.value), bool(f32.value), bool(u.value)
+
     def RowClassInfo(self):
         """(mode in use, classes, table entries, stencil length); 0 classes: no row-class
         form, stencil 0: no masks."""
@@ -264,6 +273,14 @@ class MAT:
         if getattr(self, "h", None):
             lib.fasp_gpu_mat_destroy(self.h)
             self.h = None
+
+
+def tile_timeouts() -> int:
+    """Block-tile waits that ran out since the library was loaded (0 on a healthy device)."""
+    capi.init()
+    c = C.c_uint32()
+    check(lib.fasp_gpu_tile_timeouts(C.byref(c)), "tile_timeouts")
+    return c.value
 
 
 def _count(a) -> int:

@@ -255,6 +255,20 @@ int fasp_gpu_mat_rowclass_info(fasp_gpu_mat A, int* mode, uint32_t* classes, uin
  * solver's Setup; info reports whether the offsets exist and whether they are in use. */
 int fasp_gpu_mat_set_col16(fasp_gpu_mat A, int on);
 int fasp_gpu_mat_col16_info(fasp_gpu_mat A, int* built, int* inUse);
+/* Block tiles of the CSR form (thread-per-row kernels, lanes = 1): 256 consecutive rows per
+ * block, their row pointers, column indices and values copied into shared memory by bulk
+ * asynchronous copies two tiles ahead of the threads that sum the rows (each row in CSR
+ * order with one FMA per entry: results bit-identical to the row-at-a-time kernels). span =
+ * the most entries a tile covers, widened to multiples of 4; fits64 / fits32 = every tile
+ * fits a stage with the FP64 values / the FP32 value copy (1812 / 1868 entries: a 7-point
+ * 3D or 5-point 2D stencil fits, a 9-point 2D one does not); inUse = the plain CSR form is
+ * the one in use (no row classes, stencil masks or 16-bit offsets) with lanes = 1, so the
+ * tiles run wherever the tile fits. */
+int fasp_gpu_mat_tile_info(fasp_gpu_mat A, uint32_t* span, int* fits64, int* fits32,
+                           int* inUse);
+/* Tile waits that ran out since the library was loaded: a bulk copy that never completed,
+ * after which the kernel went on with what the stage held. 0 on a healthy device. */
+int fasp_gpu_tile_timeouts(uint32_t* count);
 /* Average duration (ms) of one MAT::Apply over reps launches on FP64 (fp32 = 0) or the FP32
  * value copy (fp32 = 1), timed with CUDA events on the matrix's stream (inputs: x = 0). */
 int fasp_gpu_mat_time_apply(fasp_gpu_mat A, uint32_t reps, int fp32, int flushL2,

@@ -101,7 +101,7 @@ def hist_bound(name, m):
     env = ARR[name + "__env_dev"]
     run = np.maximum.accumulate(np.nan_to_num(env, nan=0.0))
     ahead = np.minimum(np.arange(m) + 3, len(run) - 1)
-    bound = np.maximum(HIST_REL, 10.0 * run[ahead])
+    bound = np.maximum(HIST_REL, 10.0 * np.minimum(run[ahead], 1.0))  # no overflow on inf
     bound[run[ahead] >= DECORRELATED] = np.inf
     return bound
 

@@ -62,7 +62,7 @@ def history_bound(h_ref, h_env):
         env[m:] = np.inf  # the perturbed run stopped earlier: no bar beyond it
     run = np.maximum.accumulate(env)
     ahead = np.minimum(np.arange(len(h_ref)) + 3, len(h_ref) - 1)
-    bound = np.maximum(1e-10, 10.0 * run[ahead]) * h_ref + 1e-15 * h_ref[0]
+    bound = np.maximum(1e-10, 10.0 * np.minimum(run[ahead], 1.0)) * h_ref + 1e-15 * h_ref[0]
     # past 1e-2 the reference's own perturbed trajectory has decorrelated: not compared
     bound[run[ahead] >= 1e-2] = np.inf
     return bound

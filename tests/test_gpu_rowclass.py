@@ -92,8 +92,11 @@ def test_classes_without_a_common_stencil(gpu):
     assert np.array_equal(y1.numpy(), y0.numpy())
 
 
+# 81^3 = 531,441 rows: more than the resident grid's threads, so the FP32 CG kernel on the
+# CSR form takes rows two per thread (and one row on the threads past the last pair)
 @pytest.mark.parametrize("alg,prec,dim", [("cg", "FP64", 18), ("cg", "MIXED_RELIABLE", 17),
                                           ("cg", "MIXED_RELIABLE", 18),
+                                          ("cg", "MIXED_RELIABLE", 81),
                                           ("bicgstab", "FP64", 14), ("gmres", "FP64", 14),
                                           ("fgmres", "MIXED", 14)])
 def test_solves_identical_in_every_form(gpu, alg, prec, dim):
@@ -197,3 +200,47 @@ def test_fp64_two_row_path(gpu, oracle_built, shape):
     assert np.linalg.norm(out[1][2] - out[0][2]) <= 1e-9 * np.linalg.norm(out[0][2])
     assert np.linalg.norm(out[1][2] - ref.x) <= 1e-8 * np.linalg.norm(ref.x)
     np.testing.assert_allclose(out[1][3], out[0][3], rtol=1e-6, atol=0.0)
+
+
+def test_mixed_cg_irregular_csr_rows(gpu):
+    """FP32 CG iterations on a general CSR matrix of 400,001 rows with 1 to about 30 entries
+    a row, and rows 0 and n-1 (where the clipped columns pile up) with a few thousand (more
+    rows than the resident grid's threads: two rows per thread, rows of unequal length side
+    by side, one row on the threads past the last pair). The mixed solve must
+    meet the FP64 tolerance and agree with the FP64 solve, whose kernel walks one row at a
+    time."""
+    import scipy.sparse as sp
+    from faspxx_b200 import capi
+    n = 400_001
+    rng = np.random.default_rng(5)
+    deg = rng.integers(0, 8, n)
+    rows = np.repeat(np.arange(n), deg)
+    cols = np.clip(rows + rng.integers(-5000, 5001, rows.size), 0, n - 1)
+    keep = rows != cols
+    S = sp.coo_matrix((-rng.uniform(0.1, 1.0, keep.sum()), (rows[keep], cols[keep])),
+                      shape=(n, n)).tocsr()
+    S = (S + S.T).tocsr()
+    S.sum_duplicates()
+    d = -np.asarray(S.sum(axis=1)).ravel() + rng.uniform(0.05, 0.5, n)
+    S = (S + sp.diags(d)).tocsr()
+    S.sort_indices()
+    cnt = np.diff(S.indptr)
+    assert cnt.min() == 1 and cnt[1:-1].max() >= 20 and min(cnt[0], cnt[-1]) > 1000
+    A = P.CSRMatrix(n, n, S.indptr.astype(np.uint32), S.indices.astype(np.uint32),
+                    S.data.astype(np.float64))
+    b = A.matvec(rng.uniform(-1, 1, n))
+    out = {}
+    for prec in ("FP64", "MIXED_RELIABLE"):
+        M = gpu.MAT(A)
+        assert M.RowClassInfo()[0] == CSR
+        s = gpu.configure("cg", maxIter=2000, relTol=1e-9, absTol=0.0, pcd="jacobi",
+                          pcdWeight=1.0, pcdIter=1)
+        s.SetPrecision(getattr(capi, prec))
+        s.Setup(M)
+        x = np.zeros(n)
+        assert s.Solve(b, x) == 0
+        assert np.linalg.norm(b - A.matvec(x)) <= 1e-9 * np.linalg.norm(b)
+        out[prec] = (s.GetIterations(), x)
+    assert abs(out["MIXED_RELIABLE"][0] - out["FP64"][0]) <= max(3, out["FP64"][0] // 20)
+    assert np.linalg.norm(out["MIXED_RELIABLE"][1] - out["FP64"][1]) <= \
+        1e-7 * np.linalg.norm(out["FP64"][1])
