@@ -281,6 +281,13 @@ def run_ours(args):
     lanes = M.Autotune() if not args.lanes else (M.SetLanes(args.lanes) or args.lanes)
     if args.form == "csr":
         M.SetRowClass(0)
+    if args.profile_apply:
+        # for ncu: MAT::Apply on FP64 in the chosen form, 3 warm-up and 4 timed launches
+        sp = C.c_double()
+        capi.check(lib.fasp_gpu_mat_time_apply(M.h, 4, 0, 0, C.byref(sp)), "time_apply")
+        print(f"profile-apply form {M.RowClassInfo()[0]} tiles {M.TileInfo()} "
+              f"{sp.value * 1e3:.1f} us per launch")
+        return 0
 
     def make(precision):
         s = sol.CG()
@@ -1217,6 +1224,8 @@ def main():
                          "matrix; auto: the compressed form the matrix admits)")
     ap.add_argument("--profile-solve", action="store_true",
                     help="poisson128: three mixed solves only (for an ncu launch list)")
+    ap.add_argument("--profile-apply", action="store_true",
+                    help="poisson128: a few FP64 MAT::Apply launches only (for ncu)")
     ap.add_argument("--workload", choices=["poisson128", "batch", "krylov96", "adjoint64",
                                            "pcg2d256", "matfree", "mg127"],
                     default="poisson128")
