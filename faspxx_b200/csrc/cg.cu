@@ -759,7 +759,10 @@ __global__ void __launch_bounds__(kBlock, (V4 ? 3 : (L > 1 ? 4 : (sizeof(T) == 4
             ownr(row, sum);
         }
     } else if (L == 1) { // thread per row
-        for_rows<T, false>(A, gv, ownr);
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
+        for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
+             row += stride)
+            ownr(row, row_apply<T, false>(A, row, gv));
     }
     const int lane = threadIdx.x & (L - 1);
     const size_t warpRows = 32 / L;
