@@ -765,9 +765,10 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
     """Nonsymmetric 3D convection-diffusion -Laplace(u) + beta.grad(u) on N^3 (first-order
     upwind, direction (1, 0.5, 0.25), cell Peclet 0.1 and 10), b = A x* with x* ~ U[-1,1)
     (seed 42), x0 = 0, rtol 1e-8, weighted Jacobi (omega = 2/3, one sweep), GMRES/FGMRES with
-    a fixed restart of 30: FP64 and FP32 inner iterations inside FP64 refinement (FP64
-    residual, update and Hessenberg/Givens least squares). reference: the reference's
-    iteration counts by case name, where recorded."""
+    a fixed restart of 30: FP64, FP32 inner iterations inside FP64 refinement (FP64
+    residual, update and Hessenberg/Givens least squares) and, for BiCGStab, FP32 iterations
+    with FP64 reliable updates. reference: the reference's iteration counts by case name,
+    where recorded."""
     from faspxx_b200 import capi, problems as P, sol
     flush = sol.DVec(32 << 20)
     rows = []
@@ -780,7 +781,8 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
         db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
         for alg in algs:
             res = {}
-            for prec in ("fp64", "mixed"):
+            precs = ("fp64", "mixed") + (("reliable",) if alg == "bicgstab" else ())
+            for prec in precs:
                 kw = dict(maxIter=5000, relTol=1e-8, absTol=0.0, pcd="jacobi",
                           pcdWeight=2.0 / 3.0, pcdIter=1)
                 if alg != "bicgstab":
@@ -788,6 +790,8 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
                 s = sol.configure(alg, **kw)
                 if prec == "mixed":
                     s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
+                elif prec == "reliable":
+                    s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-2)
                 s.Setup(M)
                 ms, code = _time_solve(s, db, dx, steps, flush=flush)
                 x = dx.numpy()
@@ -795,12 +799,14 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
                 # code 0 at maxIter is the reference's convention (FGMRES.cxx:226 tests
                 # numIter > maxIter): say plainly whether the tolerance was met
                 res[prec] = {"ms": round(ms, 3), "code": code, "iters": s.GetIterations(),
-                             "outer": s.info.outerIter if prec == "mixed" else None,
+                             "outer": s.info.outerIter if prec != "fp64" else None,
                              "rel_residual": rel,
                              "converged": bool(rel <= 1.01e-8),
                              "err_vs_xstar": float(np.linalg.norm(x - xs) / np.linalg.norm(xs))}
             row = {"peclet": pe, "solver": alg, **{k: v for k, v in res.items()},
                    "mixed_over_fp64": round(res["mixed"]["ms"] / res["fp64"]["ms"], 3)}
+            if "reliable" in res:
+                row["reliable_over_fp64"] = round(res["reliable"]["ms"] / res["fp64"]["ms"], 3)
             key = f"cd{N}_{tag}_{alg}"
             if reference and key in reference:
                 row["reference_iterations"] = reference[key]
@@ -825,19 +831,22 @@ def run_krylov(args):
     capi.init(0)
     N = args.size if args.size != N_GRID else 96
     if args.profile:
-        # for ncu: one 60-iteration FP64 solve of BiCGStab and of GMRES(30) at Pe 0.1
+        # for ncu: one 60-iteration FP64 solve of BiCGStab and of GMRES(30) at Pe 0.1, then
+        # one of BiCGStab with FP32 iterations and reliable updates
         A = P.convdiff3d(N, 0.1)
         b = A.matvec(P.seeded_uniform(A.nrow, 42, -1.0, 1.0))
         M = sol.MAT(A)
         if args.lanes:
             M.SetLanes(args.lanes)
         db, dx = sol.DVec.from_numpy(b), sol.DVec(A.nrow)
-        for alg in ("bicgstab", "gmres"):
+        for alg in ("bicgstab", "gmres", "bicgstab-reliable"):
             kw = dict(maxIter=60, relTol=1e-8, absTol=0.0, pcd="jacobi", pcdWeight=2.0 / 3.0,
                       pcdIter=1)
-            if alg != "bicgstab":
+            if alg == "gmres":
                 kw.update(restart=30, maxRestart=30, minRestart=30)
-            s = sol.configure(alg, **kw)
+            s = sol.configure(alg.split("-")[0], **kw)
+            if alg == "bicgstab-reliable":
+                s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-2)
             s.Setup(M)
             dx.Zero()
             code = s.Solve(db, dx)

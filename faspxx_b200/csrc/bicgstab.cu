@@ -83,6 +83,13 @@ __device__ void bi_checks(BiCtl* c, const double* red, int phase)
                 bi_esc(c, kBiSave, 1, red);
                 return;
             }
+            if (c->reliable) { // the host folds x and recomputes r in FP64, then phase 3
+                if (c->resAbs > c->rmax) c->rmax = c->resAbs;
+                if (c->resAbs < c->delta * c->rmax) {
+                    bi_esc(c, kBiRefresh, 3, red);
+                    return;
+                }
+            }
         }
         if (phase <= 1 && c->ratio > kKsmChkRatio && c->numIter > c->minIter) {
             if (red[2] < c->solStagTol) {
@@ -126,6 +133,8 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
                                                const T* __restrict__ dinv, T* __restrict__ ptmp,
                                                BiCtl* c, Scratch s)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) return;
     T a0 = 0, a1 = 0, a2 = 0;
     auto own = [&](size_t row, T ap) {
@@ -190,6 +199,8 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
                                                const T* __restrict__ dinv, T* __restrict__ sj,
                                                T* __restrict__ stmp, BiCtl* c, Scratch s)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) return;
     const T nalpha = (T)(-c->alpha);
     auto sv = [&](uint32_t j) { return fma(T(1), rj[j], nalpha * ptmp[j]); };
@@ -288,6 +299,8 @@ __global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T*
                                                const T* __restrict__ r0s,
                                                const T* __restrict__ dinv, BiCtl* c, Scratch s)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) return;
     const T alpha = (T)c->alpha, omega = (T)c->omega, nomega = (T)(-c->omega);
     BiXSums<T> a;
@@ -335,6 +348,8 @@ __global__ void __launch_bounds__(kBlock) bi_dir(uint32_t n, T* __restrict__ pj,
                                                  const T* __restrict__ rj,
                                                  const T* __restrict__ ptmp, const BiCtl* c)
 {
+    pdl_wait();
+    pdl_release();
     if (c->status != kRun) return;
     const T beta = (T)c->beta, nomega = (T)(-c->omega);
     GRID_STRIDE(i, n)
@@ -376,6 +391,23 @@ CSRView<double> bi_view<double>(const Mat& A) { return A.v64(); }
 template <>
 CSRView<float> bi_view<float>(const Mat& A) { return A.v32(); }
 
+// A launch that may overlap the previous kernel's tail (programmatic dependent launch): the
+// kernels wait for it to complete (pdl_wait) before their first memory access.
+template <typename... P, typename... A>
+static void bi_launch(void (*kern)(P...), int grid, cudaStream_t s, bool pdl, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 template <typename T>
 int BiEngine<T>::launch_iter()
 {
@@ -387,19 +419,21 @@ int BiEngine<T>::launch_iter()
     auto fit = [&](const void* k, int need) { return std::min(need, resident_grid(*c, k, kBlock)); };
 #define BI_SPMV(KP, KS, LL, JJ)                                                            \
     do {                                                                                   \
-        KP<T, LL, JJ><<<fit((const void*)KP<T, LL, JJ>, needS), kBlock, 0, c->stream>>>(   \
-            V, pj, rj, r0s, dinv, ptmp, ctl, c->red);                                      \
-        KS<T, LL, JJ><<<fit((const void*)KS<T, LL, JJ>, needS), kBlock, 0, c->stream>>>(   \
-            V, rj, ptmp, dinv, sj, stmp, ctl, c->red);                                     \
+        bi_launch(KP<T, LL, JJ>, fit((const void*)KP<T, LL, JJ>, needS), c->stream, pdl, V,  \
+                  (const T*)pj, (const T*)rj, (const T*)r0s, dinv, ptmp, ctl, c->red);      \
+        bi_launch(KS<T, LL, JJ>, fit((const void*)KS<T, LL, JJ>, needS), c->stream, pdl, V,  \
+                  (const T*)rj, (const T*)ptmp, dinv, sj, stmp, ctl, c->red);               \
     } while (0)
     // 16-byte row groups on 5- and 7-point stencil masks (bi_p / bi_s with SH)
     const int sh = L == 1 ? stencil_vec_shape(V, pj, rj, ptmp) : 0;
 #define BI_SPMV_SH(JJ, SS)                                                                 \
     do {                                                                                   \
-        bi_p<T, 1, JJ, SS><<<fit((const void*)bi_p<T, 1, JJ, SS>, needV), kBlock, 0,       \
-                             c->stream>>>(V, pj, rj, r0s, dinv, ptmp, ctl, c->red);        \
-        bi_s<T, 1, JJ, SS><<<fit((const void*)bi_s<T, 1, JJ, SS>, needV), kBlock, 0,       \
-                             c->stream>>>(V, rj, ptmp, dinv, sj, stmp, ctl, c->red);       \
+        bi_launch(bi_p<T, 1, JJ, SS>, fit((const void*)bi_p<T, 1, JJ, SS>, needV),         \
+                  c->stream, pdl, V, (const T*)pj, (const T*)rj, (const T*)r0s, dinv, ptmp, \
+                  ctl, c->red);                                                            \
+        bi_launch(bi_s<T, 1, JJ, SS>, fit((const void*)bi_s<T, 1, JJ, SS>, needV),         \
+                  c->stream, pdl, V, (const T*)rj, (const T*)ptmp, dinv, sj, stmp, ctl,     \
+                  c->red);                                                                 \
     } while (0)
 #define BI_LANES(JJ)                                                                       \
     switch (sh ? -sh : L) {                                                                \
@@ -416,8 +450,8 @@ int BiEngine<T>::launch_iter()
     const bool vx = (((uintptr_t)x | (uintptr_t)rj | (uintptr_t)pj | (uintptr_t)sj |
                       (uintptr_t)stmp | (uintptr_t)r0s | (uintptr_t)(jacobi ? dinv : pj)) & 15) == 0;
     auto launch_x = [&](auto kern) {
-        kern<<<fit((const void*)kern, needV), kBlock, 0, c->stream>>>(n, x, rj, pj, sj, stmp, r0s,
-                                                                      dinv, ctl, c->red);
+        bi_launch(kern, fit((const void*)kern, needV), c->stream, pdl, n, x, rj, (const T*)pj,
+                  (const T*)sj, (const T*)stmp, (const T*)r0s, dinv, ctl, c->red);
     };
     if (jacobi) {
         BI_LANES(1)
@@ -435,8 +469,8 @@ int BiEngine<T>::launch_iter()
 #undef BI_LANES
 #undef BI_SPMV_SH
 #undef BI_SPMV
-    bi_dir<T><<<fit((const void*)bi_dir<T>, needV), kBlock, 0, c->stream>>>(n, pj, rj, ptmp,
-                                                                             ctl);
+    bi_launch(bi_dir<T>, fit((const void*)bi_dir<T>, needV), c->stream, pdl, n, pj,
+              (const T*)rj, (const T*)ptmp, (const BiCtl*)ctl);
     if (!capturing) c->launches += 4;
     FB_CUDA(cudaGetLastError());
     return kOk;

@@ -7,7 +7,7 @@
 
 namespace fb {
 
-enum BiReason { kBiNone = 0, kBiSave = 1, kBiStag = 2, kBiCheck = 3 };
+enum BiReason { kBiNone = 0, kBiSave = 1, kBiStag = 2, kBiCheck = 3, kBiRefresh = 4 };
 
 // The locals of BiCGStab::Solve (BiCGStab.cxx:70-82) and the parameters it reads, in device
 // memory so that the finalize thread of each fused kernel runs the reference's control flow.
@@ -23,6 +23,10 @@ struct BiCtl {
     unsigned histCap;
     unsigned histOffset;
     double   histScale;
+    // reliable updates (FP32 iterations of MIXED_RELIABLE): escalate kBiRefresh once the
+    // recursive residual has fallen below delta x its largest value since the last refresh
+    int      reliable;
+    double   delta, rmax;
 };
 
 // One iteration is four kernels (Jacobi from zero is a diagonal scaling, D = weight/diag):
@@ -47,6 +51,7 @@ struct BiEngine {
     cudaGraphExec_t gexec = nullptr;
     int        itersPerGraph = 8;
     bool       useGraph = true;
+    bool       pdl = true; // programmatic dependent launch between the iteration's kernels
     bool       capturing = false;
     uint32_t   n = 0;
 

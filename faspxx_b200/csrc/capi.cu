@@ -688,7 +688,8 @@ int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out)
         cfg->alg != FASP_GPU_BICGSTAB && cfg->alg != FASP_GPU_GMRES &&
         cfg->alg != FASP_GPU_FGMRES)
         return kErrSolverType;
-    if (cfg->precision == FASP_GPU_MIXED_RELIABLE && cfg->alg != FASP_GPU_CG)
+    if (cfg->precision == FASP_GPU_MIXED_RELIABLE && cfg->alg != FASP_GPU_CG &&
+        cfg->alg != FASP_GPU_BICGSTAB)
         return kErrSolverType;
     if (cfg->precision < FASP_GPU_FP64 || cfg->precision > FASP_GPU_MIXED_RELIABLE)
         return kErrInputPar;

@@ -140,6 +140,7 @@ struct SolverImpl {
     int cg_device(const double* b, double* x, fasp_gpu_info* info);
     int cg_mixed(const double* b, double* x, fasp_gpu_info* info);
     int cg_reliable(const double* b, double* x, fasp_gpu_info* info);
+    int bicgstab_reliable(const double* b, double* x, fasp_gpu_info* info);
     template <typename T>
     int bicgstab(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu_params& P, Space<T> S);
     template <typename T>

@@ -443,6 +443,10 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 // FP64: the outer residual; FP32: the inner solve's 12 vectors + b, e
                 if ((e = alloc_vecs(w, 1, n)) || (e = alloc_vecs(w32, 14, n))) return e;
                 if ((e = Ah->M.ensure32(c.stream))) return e;
+            } else if (cfg.precision == FASP_GPU_MIXED_RELIABLE) {
+                // FP64 x and residual; the FP32 engine holds the iteration's vectors
+                if ((e = alloc_vecs(w, 2, n))) return e;
+                if ((e = Ah->M.ensure32(c.stream))) return e;
             } else if ((e = alloc_vecs(w, 12, n))) {
                 return e;
             }
@@ -451,13 +455,18 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             if (fusable) {
                 dhistCap = cfg.prm.maxIter + 2;
                 if (cudaMalloc(&dhist, (size_t)dhistCap * 8) != cudaSuccess) return kErrAlloc;
-                if (cfg.precision == FASP_GPU_MIXED) {
+                if (cfg.precision == FASP_GPU_MIXED ||
+                    cfg.precision == FASP_GPU_MIXED_RELIABLE) {
                     bi32 = new BiEngine<float>();
+                    bi32->pdl = cfg.overlapLaunch != 0;
                     if ((e = bi32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
                 } else {
                     bi64 = new BiEngine<double>();
+                    bi64->pdl = cfg.overlapLaunch != 0;
                     if ((e = bi64->init(&c, A, cfg.pcd, pcd.dinv, cfg.useGraph != 0))) return e;
                 }
+            } else if (cfg.precision == FASP_GPU_MIXED_RELIABLE) {
+                return kErrPcdType; // reliable updates run in the fused FP32 engine
             }
             break;
         }
@@ -1058,6 +1067,119 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
     info->numIter = iters;
     info->outerIter = refreshes;
     info->escalations = hostRefreshes;
+    info->code = code;
+    info->norm2 = rn;
+    v_norminf(c, n, r64, c.dslot + SL_T2);
+    info->normInf = fetch(c.dslot + SL_T2);
+    v_copy(c, n, x64, x);
+    const uint32_t len = std::min<uint32_t>(iters + 1, dhistCap);
+    hist.assign(len, kNaN);
+    FB_CUDA(cudaMemcpyAsync(hist.data(), dhist, (size_t)len * 8, cudaMemcpyDeviceToHost, c.stream));
+    FB_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto& pt : patches) rec(pt.first, pt.second);
+    return kOk;
+}
+
+// BiCGStab with reliable updates (no reference counterpart; the scheme of cg_reliable): the
+// FP32 engine iterates on the residual scaled by s = ||b - A x0|| and accumulates its
+// correction e. Whenever its recursive residual has fallen by delta (innerRelTol) since the
+// last refresh, or meets the stop test, or the run ends, the host folds x += s e in FP64,
+// recomputes r = b - A x in FP64 and stops if ||r|| / ||r0|| < relTol (or ||r|| < absTol);
+// otherwise the same Krylov process continues from the refreshed residual: p and r0* are
+// kept, (r, r0*) and beta come from the refreshed r (bi_resume at phase 3). The save and
+// stagnation tests of the reference look at the whole solution, which the FP32 correction
+// is not, so they are off; a refresh that gains less than sqrt(delta) three times in a row
+// ends the solve with ERROR_SOLVER_TOLSMALL.
+int SolverImpl::bicgstab_reliable(const double* b, double* x, fasp_gpu_info* info)
+{
+    const fasp_gpu_params& P = cfg.prm;
+    if (!bi32) return kErrPcdType;
+    BiEngine<float>& E = *bi32;
+    BiCtl& h = *E.hctl;
+    double *x64 = w[0], *r64 = w[1];
+    int e;
+    v_copy(c, n, x, x64);
+    const double delta = cfg.innerRelTol > 0 && cfg.innerRelTol < 1 ? cfg.innerRelTol : 1e-2;
+    ++c.launches;
+    k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
+    std::vector<std::pair<uint32_t, double>> patches;
+    auto true_res = [&](double* rn) {
+        int err = apply_residual(c, *A, b, x64, r64);
+        if (err) return err;
+        if ((err = v_norm2(c, n, r64, c.dslot + SL_T1))) return err;
+        *rn = fetch(c.dslot + SL_T1);
+        return (int)kOk;
+    };
+    double rn = 0.0;
+    if ((e = true_res(&rn))) return e;
+    const double den = (kCloseZero > rn) ? kCloseZero : rn;
+    patches.push_back({0u, rn});
+    int code = kOk;
+    uint32_t iters = 0, refreshes = 0, stall = 0;
+    double prev = den;
+    bool converged = rn / den < P.relTol || rn < P.absTol;
+    if (!converged && std::isfinite(rn) && P.maxIter > 0) {
+        const double s = rn;
+        // e = 0, r = (b - A x) / s, r0* = p = r (BiCGStab.cxx:70-78 on the scaled system)
+        if ((e = convert_scaled(c, n, r64, 1.0 / s, E.rj)) || (e = set32(c, n, E.x))) return e;
+        v_copy(c, n, (const float*)E.rj, E.r0s);
+        v_copy(c, n, (const float*)E.rj, E.pj);
+        std::memset(&h, 0, sizeof(BiCtl));
+        h.status = kRun;
+        h.code = kOk;
+        h.minIter = 0;
+        h.maxIter = P.maxIter;
+        h.savIter = 0xffffffffu;
+        h.restart = P.restart;
+        h.relTol = P.relTol * den / s;
+        h.absTol = P.absTol / s;
+        h.solStagTol = 0.0;           // no solution-stagnation stop on the correction
+        h.stagStep = kMaxStagNum + 1; // nor a stagnation restart
+        h.resAbs = h.resRel = h.denAbs = h.resAbsOld = 1.0;
+        h.hist = dhist;
+        h.histCap = dhistCap;
+        h.histOffset = 0;
+        h.histScale = s;
+        h.reliable = 1;
+        h.delta = delta;
+        h.rmax = 1.0; // ||r / s|| at the start
+        if ((e = E.push_ctl())) return e;
+        unsigned launches = 0;
+        for (uint32_t guard = 0;; ++guard) {
+            if (h.status == kRun) {
+                if ((e = E.run(&launches)) || (e = E.pull_ctl())) return e;
+                c.launches += launches;
+                launches = 0;
+                continue;
+            }
+            // a refresh, the FP32 stop test, or the end of the run (maxIter, breakdown)
+            if ((e = update_from32(c, n, s, E.x, x64)) || (e = set32(c, n, E.x))) return e;
+            if ((e = true_res(&rn))) return e;
+            ++refreshes;
+            patches.push_back({h.numIter, rn});
+            converged = rn / den < P.relTol || rn < P.absTol;
+            stall = rn > std::sqrt(delta) * prev ? stall + 1 : 0;
+            prev = rn;
+            if (!converged && stall >= 3) code = kErrTolSmall;
+            if (h.status == kDone || converged || !std::isfinite(rn) || guard > P.maxIter ||
+                code != kOk) {
+                if (!converged && h.status == kDone && h.code != kOk) code = h.code;
+                break;
+            }
+            if ((e = convert_scaled(c, n, r64, 1.0 / s, E.rj))) return e;
+            h.resAbs = rn / s;
+            h.resRel = h.resAbs / h.denAbs;
+            h.rmax = h.resAbs;
+            h.phase = 3;
+            h.status = kRun;
+            if ((e = E.push_ctl()) || (e = E.launch_resume()) || (e = E.pull_ctl())) return e;
+        }
+        iters = h.numIter;
+    }
+    if (!converged && code == kOk) code = kErrMaxIt;
+    info->numIter = iters;
+    info->outerIter = refreshes;
+    info->escalations = refreshes;
     info->code = code;
     info->norm2 = rn;
     v_norminf(c, n, r64, c.dslot + SL_T2);
@@ -2307,8 +2429,12 @@ int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
                 e = cg_generic(b, x, info);
             break;
         case FASP_GPU_BICGSTAB:
-            e = cfg.precision == FASP_GPU_MIXED ? refine(b, x, info)
-                                                : bicgstab<double>(b, x, info, cfg.prm, sp64());
+            if (cfg.precision == FASP_GPU_MIXED)
+                e = refine(b, x, info);
+            else if (cfg.precision == FASP_GPU_MIXED_RELIABLE)
+                e = bicgstab_reliable(b, x, info);
+            else
+                e = bicgstab<double>(b, x, info, cfg.prm, sp64());
             break;
         case FASP_GPU_GMRES:
             if (cfg.precision == FASP_GPU_MIXED)

@@ -53,8 +53,10 @@ enum fasp_gpu_alg {
 enum fasp_gpu_precision {
     FASP_GPU_FP64 = 0,  /* every vector and reduction in FP64, the reference's arithmetic */
     FASP_GPU_MIXED = 1, /* FP32 inner Krylov iterations inside FP64 iterative refinement */
-    FASP_GPU_MIXED_RELIABLE = 2 /* CG only: one FP32 Krylov run with FP64 reliable updates of
-                                   x and r; the search direction survives each update */
+    FASP_GPU_MIXED_RELIABLE = 2 /* CG and BiCGStab (with Identity or one Jacobi sweep): one
+                                   FP32 Krylov run with FP64 reliable updates of x and r; the
+                                   search direction survives each update. Other solvers:
+                                   ERROR_SOLVER_TYPE at creation. */
 };
 
 /* Gram-Schmidt variant of the GMRES/FGMRES Arnoldi step. */
@@ -98,9 +100,9 @@ typedef struct {
                                     cooperative launch (when the device allows it);
                                     default 0: CUDA graphs of the two fused kernels
                                     measure faster on B200 at every size */
-    int             overlapLaunch; /* 1 (default): the CG iteration kernels use programmatic
-                                    dependent launch, each one's launch overlapping its
-                                    predecessor's reduction tail */
+    int             overlapLaunch; /* 1 (default): the CG and BiCGStab iteration kernels
+                                    use programmatic dependent launch, each one's launch
+                                    overlapping its predecessor's reduction tail */
     int             fp32Recurrence; /* MIXED, MIXED_RELIABLE CG: 1 (default) = the FP32
                                     iterations form q = A p as A z + beta q_old (the SpMV
                                     gathers one vector); 0 = as the reference, A (z + beta p) */

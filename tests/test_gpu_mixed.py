@@ -185,10 +185,12 @@ def test_mixed_precision_rejected_for_stationary_solvers(gpu):
         with pytest.raises(capi.FaspError) as e:
             s.Setup(gpu.MAT(A))
         assert e.value.code == -30
-    s = gpu.configure("bicgstab", maxIter=10)
-    s.SetPrecision(capi.MIXED_RELIABLE)
-    with pytest.raises(capi.FaspError):
-        s.Setup(gpu.MAT(A))
+    for alg in ("gmres", "fgmres"):  # reliable updates: CG and BiCGStab only
+        s = gpu.configure(alg, maxIter=10)
+        s.SetPrecision(capi.MIXED_RELIABLE)
+        with pytest.raises(capi.FaspError) as e:
+            s.Setup(gpu.MAT(A))
+        assert e.value.code == -30
 
 
 def test_reliable_stops_below_attainable_accuracy(gpu):
