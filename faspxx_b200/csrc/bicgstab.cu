@@ -125,7 +125,9 @@ __device__ void bi_checks(BiCtl* c, const double* red, int phase)
 
 // ptmp = D (A pj) with the loop-top sums. SH = 5 or 7: stencil masks of that fixed shape,
 // 16-byte row groups per thread (stencil_group; each row's product is the same bits, the
-// partial sums group the rows by W).
+// partial sums group the rows by W). JAC = 2 (reliable updates on a matrix whose diagonal
+// varies): ptmp = A (D pj), the right-preconditioned product, so that the recursive
+// residual stays b - A x (the reference's order keeps it so only when D commutes with A).
 template <typename T, int L, int JAC, int SH = 0>
 __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict__ pj,
                                                const T* __restrict__ rj,
@@ -136,16 +138,17 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
     pdl_wait();
     pdl_release();
     if (c->status != kRun) return;
+    static_assert(SH == 0 || JAC != 2, "right preconditioning runs the row kernels");
     T a0 = 0, a1 = 0, a2 = 0;
     auto own = [&](size_t row, T ap) {
-        const T pt = JAC ? ap * dinv[row] : ap;
+        const T pt = JAC == 1 ? ap * dinv[row] : ap;
         ptmp[row] = pt;
         const T r = rj[row], r0 = r0s[row];
         a0 = fma(pt, r0, a0);
         a1 = fma(r, r0, a1);
         a2 = fma(r, r, a2);
     };
-    auto xv = [&](uint32_t j) { return pj[j]; };
+    auto xv = [&](uint32_t j) { return JAC == 2 ? pj[j] * dinv[j] : pj[j]; };
     if constexpr (SH != 0) {
         using V = typename Vec16<T>::V;
         constexpr int W = Vec16<T>::W;
@@ -178,7 +181,7 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
             T sum = T(0);
             if (row < A.nrow)
                 for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
-                    sum = fma(A.val[k], pj[A.colInd[k]], sum);
+                    sum = fma(A.val[k], xv(A.colInd[k]), sum);
             sum = group_sum<L>(sum);
             if (lane == 0 && row < A.nrow) own(row, sum);
         }
@@ -202,13 +205,15 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
     pdl_wait();
     pdl_release();
     if (c->status != kRun) return;
+    static_assert(SH == 0 || JAC != 2, "right preconditioning runs the row kernels");
     const T nalpha = (T)(-c->alpha);
     auto sv = [&](uint32_t j) { return fma(T(1), rj[j], nalpha * ptmp[j]); };
+    auto gv = [&](uint32_t j) { return JAC == 2 ? sv(j) * dinv[j] : sv(j); };
     T a0 = 0, a1 = 0;
     auto own = [&](size_t row, T as) {
         const T sjv = sv((uint32_t)row);
         sj[row] = sjv;
-        const T st = JAC ? as * dinv[row] : as;
+        const T st = JAC == 1 ? as * dinv[row] : as;
         stmp[row] = st;
         a0 = fma(st, sjv, a0);
         a1 = fma(st, st, a1);
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
     } else if (L == 1) {
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
              row += (size_t)gridDim.x * blockDim.x)
-            own(row, row_apply<T, false>(A, row, sv));
+            own(row, row_apply<T, false>(A, row, gv));
     } else {
         const int lane = threadIdx.x & (L - 1);
         const size_t warpRows = 32 / L;
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict
             T sum = T(0);
             if (row < A.nrow)
                 for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
-                    sum = fma(A.val[k], sv(A.colInd[k]), sum);
+                    sum = fma(A.val[k], gv(A.colInd[k]), sum);
             sum = group_sum<L>(sum);
             if (lane == 0 && row < A.nrow) own(row, sum);
         }
@@ -453,7 +458,20 @@ int BiEngine<T>::launch_iter()
         bi_launch(kern, fit((const void*)kern, needV), c->stream, pdl, n, x, rj, (const T*)pj,
                   (const T*)sj, (const T*)stmp, (const T*)r0s, dinv, ctl, c->red);
     };
-    if (jacobi) {
+    if (jacobi && rightPcd) { // A (D v): the row kernels (no stencil groups)
+        switch (L) {
+            case 1: BI_SPMV(bi_p, bi_s, 1, 2); break;
+            case 2: BI_SPMV(bi_p, bi_s, 2, 2); break;
+            case 4: BI_SPMV(bi_p, bi_s, 4, 2); break;
+            case 8: BI_SPMV(bi_p, bi_s, 8, 2); break;
+            case 16: BI_SPMV(bi_p, bi_s, 16, 2); break;
+            default: BI_SPMV(bi_p, bi_s, 32, 2); break;
+        }
+        if (vx)
+            launch_x(bi_x<T, 1, 1>);
+        else
+            launch_x(bi_x<T, 1, 0>);
+    } else if (jacobi) {
         BI_LANES(1)
         if (vx)
             launch_x(bi_x<T, 1, 1>);

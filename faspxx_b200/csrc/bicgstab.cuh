@@ -52,6 +52,10 @@ struct BiEngine {
     int        itersPerGraph = 8;
     bool       useGraph = true;
     bool       pdl = true; // programmatic dependent launch between the iteration's kernels
+    // Jacobi applied on the right, ptmp = A (D pj) and stmp = A (D sj), so that the
+    // recursive residual is b - A x whatever the diagonal (reliable updates replace it by
+    // the true residual); false: the reference's D (A pj), the same when D is a constant
+    bool       rightPcd = false;
     bool       capturing = false;
     uint32_t   n = 0;
 

@@ -459,6 +459,8 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                     cfg.precision == FASP_GPU_MIXED_RELIABLE) {
                     bi32 = new BiEngine<float>();
                     bi32->pdl = cfg.overlapLaunch != 0;
+                    bi32->rightPcd = cfg.precision == FASP_GPU_MIXED_RELIABLE && cfg.pcd == 1 &&
+                                     !A->diagConst;
                     if ((e = bi32->init(&c, A, cfg.pcd, pcd.dinv32, cfg.useGraph != 0))) return e;
                 } else {
                     bi64 = new BiEngine<double>();
