@@ -494,11 +494,16 @@ int BiEngine<T>::launch_iter()
     return kOk;
 }
 
+// The checks resume at c->phase and end with beta; the direction update of the same
+// iteration (BiCGStab.cxx:184-185, after every branch of the checks, a restart's pj = 0
+// included) follows when they leave the status at kRun: the escalation stopped the graph
+// before its bi_dir, and the next graph starts at bi_p.
 template <typename T>
 int BiEngine<T>::launch_resume()
 {
-    ++c->launches;
+    c->launches += 2;
     bi_resume<T><<<c->grid(n, kBlock), kBlock, 0, c->stream>>>(n, rj, r0s, ctl, c->red);
+    bi_dir<T><<<c->grid(n, kBlock), kBlock, 0, c->stream>>>(n, pj, rj, ptmp, ctl);
     FB_CUDA(cudaGetLastError());
     return kOk;
 }

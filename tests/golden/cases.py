@@ -145,6 +145,16 @@ def solver_cases():
                           x0="zero", store_b=True, kw=kw))
     C.append(dict(name="vd_cg", mat="vardiff_8", alg="cg", rhs="normal", x0="zero", store_b=True,
                   kw=dict(maxIter=2000, minIter=0, relTol=1e-10, absTol=0.0)))
+    # The save branch taken in most iterations (savIter small: BiCGStab.cxx:133, CG.cxx's
+    # safe copy): the iteration goes on after it with its direction update, and the saved x
+    # is returned when numIter > savIter.
+    C.append(dict(name="cd_pe01_bicgstab_sav3", mat="convdiff_pe01", alg="bicgstab",
+                  rhs="xstar11", x0="zero", store_b=True, kw=dict(syn, **jac23, savIter=3)))
+    C.append(dict(name="fdm_bicgstab_sav2", mat="fdm_10X10", alg="bicgstab",
+                  kw=dict(ip, savIter=2)))
+    C.append(dict(name="p2d_pcg_sav3", mat="poisson2d_32", alg="cg", rhs="xstar01", x0="zero",
+                  store_b=True, kw=dict(syn, pcd="jacobi", pcdWeight=1.0, pcdIter=1,
+                                        savIter=3)))
     return C
 
 

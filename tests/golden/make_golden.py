@@ -29,7 +29,8 @@ reads its outputs:
   computed by the reference on five structurally symmetric matrices and one that is not.
 
     python tests/golden/make_golden.py /path/to/reference
-                                       [--ingest-only | --matfree-only | --mult-only]
+                                       [--runs-only | --ingest-only | --matfree-only |
+                                        --mult-only]
     python tests/golden/make_golden.py --mta-only
 """
 from __future__ import annotations
@@ -410,6 +411,9 @@ if __name__ == "__main__":
                  "in FASPXX_REFERENCE")
     if "--mult-only" in sys.argv:
         make_mult()
+        sys.exit(0)
+    if "--runs-only" in sys.argv:  # the solver runs and transposes only
+        main(root)
         sys.exit(0)
     if "--ingest-only" not in sys.argv and "--matfree-only" not in sys.argv:
         main(root)

@@ -37,8 +37,9 @@ CASES = {c["name"]: c for c in G.solver_cases()}
 
 # stopping test at the rounding floor: relTol 1e-17 (see tests/golden/cases.py). The run
 # ends in rounding noise: converged, ERROR_SOLVER_TOLSMALL after the false-convergence
-# restarts, or (BiCGStab) the breakdown test |(ptmp, r0*)| <= 1e-40 once the residual of this
-# 100-unknown system has reached zero (ERROR_DIVIDE_ZERO); the true residual is checked.
+# restarts, or (BiCGStab) the breakdown test |(ptmp, r0*)| <= 1e-40 between restarts
+# (ERROR_DIVIDE_ZERO): the reference itself ends so for 14 of 40 one-ulp perturbations of
+# b (after 65 to 317 iterations), TOLSMALL after 318-366 for the others.
 FLOOR = {"fdm_cg_tolsmall": (0, -34), "fdm_bicgstab_tolsmall": (0, -34, -18)}
 # BiCGStab on fem_small from x0 = 1, b = 0: the residual norm oscillates by orders of
 # magnitude near the threshold; two reruns of the reference with reordered sums differ too
@@ -209,16 +210,20 @@ def _check_case(gpu, oracle, name, engine="graph"):
             assert code == meta["code"], (key, code, meta["code"])
         it = s.GetIterations()
         if name in FLOOR:
-            # the count of false-convergence restarts at the floor is chaotic: require the
-            # true residual to have reached the rounding floor instead
-            r = b - A.matvec(x)
-            assert np.linalg.norm(r) <= 1e-13 * np.linalg.norm(b), key
-            continue
-        window = ERRATIC.get(name, 1)
-        assert abs(it - meta["iters"]) <= window, (key, it, meta["iters"])
-        scale = max(np.max(np.abs(ref.x)), np.max(np.abs(x0)), 1e-300)
-        xtol = 1e-3 if name in ERRATIC else 1e-6
-        assert np.max(np.abs(x - ref.x)) <= xtol * scale, key
+            # the count of false-convergence restarts at the floor is chaotic: a converged or
+            # TOLSMALL run must have reached the rounding floor; a breakdown may strike right
+            # after a restart (the reference's own perturbed runs end so with true residuals
+            # from 1e-14 to 0.15); the history is compared below up to where the
+            # reference's own perturbed run decorrelates
+            if code != -18:
+                r = b - A.matvec(x)
+                assert np.linalg.norm(r) <= 1e-13 * np.linalg.norm(b), key
+        else:
+            window = ERRATIC.get(name, 1)
+            assert abs(it - meta["iters"]) <= window, (key, it, meta["iters"])
+            scale = max(np.max(np.abs(ref.x)), np.max(np.abs(x0)), 1e-300)
+            xtol = 1e-3 if name in ERRATIC else 1e-6
+            assert np.max(np.abs(x - ref.x)) <= xtol * scale, key
         h = s.History()
         m = min(len(h), len(ref.hist))
         fin = np.isfinite(ref.hist[:m])
