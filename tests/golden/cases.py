@@ -155,6 +155,12 @@ def solver_cases():
     C.append(dict(name="p2d_pcg_sav3", mat="poisson2d_32", alg="cg", rhs="xstar01", x0="zero",
                   store_b=True, kw=dict(syn, pcd="jacobi", pcdWeight=1.0, pcdIter=1,
                                         savIter=3)))
+    # GMRES and FGMRES take it once per restart cycle (GMRES.cxx, FGMRES.cxx): restart 10
+    for alg in ("gmres", "fgmres"):
+        C.append(dict(name=f"cd_pe01_{alg}_sav3", mat="convdiff_pe01", alg=alg, rhs="xstar11",
+                      x0="zero", store_b=True,
+                      kw=dict(syn, **jac23, savIter=3, restart=10, maxRestart=10,
+                              minRestart=10)))
     return C
 
 
