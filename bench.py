@@ -796,7 +796,7 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
                 if prec == "mixed":
                     s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
                 elif prec == "reliable":
-                    s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-2)
+                    s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-3)
                 s.Setup(M)
                 ms, code = _time_solve(s, db, dx, steps, flush=flush)
                 x = dx.numpy()

@@ -1084,7 +1084,8 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
 
 // BiCGStab with reliable updates (no reference counterpart; the scheme of cg_reliable): the
 // FP32 engine iterates on the residual scaled by s = ||b - A x0|| and accumulates its
-// correction e. Whenever its recursive residual has fallen by delta (innerRelTol) since the
+// correction e. Whenever its recursive residual has fallen by delta (innerRelTol, default
+// 1e-3: the fewest refreshes without extra iterations on B200 at 96^3) since the
 // last refresh, or meets the stop test, or the run ends, the host folds x += s e in FP64,
 // recomputes r = b - A x in FP64 and stops if ||r|| / ||r0|| < relTol (or ||r|| < absTol);
 // otherwise the same Krylov process continues from the refreshed residual: p and r0* are
@@ -1101,7 +1102,7 @@ int SolverImpl::bicgstab_reliable(const double* b, double* x, fasp_gpu_info* inf
     double *x64 = w[0], *r64 = w[1];
     int e;
     v_copy(c, n, x, x64);
-    const double delta = cfg.innerRelTol > 0 && cfg.innerRelTol < 1 ? cfg.innerRelTol : 1e-2;
+    const double delta = cfg.innerRelTol > 0 && cfg.innerRelTol < 1 ? cfg.innerRelTol : 1e-3;
     ++c.launches;
     k_fill<<<c.grid(dhistCap, kBlock), kBlock, 0, c.stream>>>(dhistCap, kNaN, dhist);
     std::vector<std::pair<uint32_t, double>> patches;

@@ -92,7 +92,8 @@ typedef struct {
     int             orth;        /* fasp_gpu_orth */
     double          innerRelTol; /* MIXED: relative tolerance of each FP32 inner solve;
                                     MIXED_RELIABLE: an FP64 update each time the FP32
-                                    residual has fallen by this factor (0 or >= 1: 1e-2) */
+                                    residual has fallen by this factor (0 or >= 1: 1e-2
+                                    for CG, 1e-3 for BiCGStab) */
     uint32_t        innerMaxIter;/* MIXED: iteration cap of each inner solve */
     uint32_t        maxOuter;    /* MIXED: refinement steps cap */
     int             useGraph;    /* 1: device-driven iterations captured in CUDA graphs */
