@@ -123,53 +123,85 @@ __device__ void bi_checks(BiCtl* c, const double* red, int phase)
     }
 }
 
-// ptmp = D (A pj) with the loop-top sums. SH = 5 or 7: stencil masks of that fixed shape,
-// 16-byte row groups per thread (stencil_group; each row's product is the same bits, the
-// partial sums group the rows by W). JAC = 2 (reliable updates on a matrix whose diagonal
-// varies): ptmp = A (D pj), the right-preconditioned product, so that the recursive
-// residual stays b - A x (the reference's order keeps it so only when D commutes with A).
+// pj = rj + beta (pj_old - omega ptmp_old) (BiCGStab.cxx:184-185, the previous iteration's
+// direction update, formed for every gathered entry in the reference's operand order:
+// tmp = fma(1, pj, -omega ptmp), pj = fma(1, rj, beta tmp)) and ptmp = D (A pj) with the
+// loop-top sums; pj and ptmp of the owned rows go to the
+// other buffer of each pair, and the finalize flips c->par to it. SH = 5 or 7: stencil
+// masks of that fixed shape, 16-byte row groups per thread (stencil_group; each row's
+// product is the same bits, the partial sums group the rows by W). JAC = 2 (reliable
+// updates on a matrix whose diagonal varies): ptmp = A (D pj), the right-preconditioned
+// product, so that the recursive residual stays b - A x (the reference's order keeps it so
+// only when D commutes with A).
 template <typename T, int L, int JAC, int SH = 0>
-__global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict__ pj,
-                                               const T* __restrict__ rj,
+__global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, T* __restrict__ p0,
+                                               T* __restrict__ p1, T* __restrict__ t0,
+                                               T* __restrict__ t1, const T* __restrict__ rj,
                                                const T* __restrict__ r0s,
-                                               const T* __restrict__ dinv, T* __restrict__ ptmp,
-                                               BiCtl* c, Scratch s)
+                                               const T* __restrict__ dinv, BiCtl* c, Scratch s)
 {
     pdl_wait();
     pdl_release();
     if (c->status != kRun) return;
     static_assert(SH == 0 || JAC != 2, "right preconditioning runs the row kernels");
+    const int par = c->par;
+    const T* __restrict__ pOld = par ? p1 : p0;
+    const T* __restrict__ tOld = par ? t1 : t0;
+    T* __restrict__ pNew = par ? p0 : p1;
+    T* __restrict__ tNew = par ? t0 : t1;
+    const T beta = (T)c->beta, nomega = (T)(-c->omega);
+    auto pat = [&](size_t j) { // the updated pj at j
+        const T tmp = fma(T(1), pOld[j], nomega * tOld[j]);
+        return fma(T(1), rj[j], beta * tmp);
+    };
     T a0 = 0, a1 = 0, a2 = 0;
     auto own = [&](size_t row, T ap) {
         const T pt = JAC == 1 ? ap * dinv[row] : ap;
-        ptmp[row] = pt;
+        tNew[row] = pt;
         const T r = rj[row], r0 = r0s[row];
         a0 = fma(pt, r0, a0);
         a1 = fma(r, r0, a1);
         a2 = fma(r, r, a2);
     };
-    auto xv = [&](uint32_t j) { return JAC == 2 ? pj[j] * dinv[j] : pj[j]; };
+    auto xv = [&](uint32_t j) { return JAC == 2 ? pat(j) * dinv[j] : pat(j); };
     if constexpr (SH != 0) {
-        using V = typename Vec16<T>::V;
-        constexpr int W = Vec16<T>::W;
+        using VT = Vec16<T>;
+        using V = typename VT::V;
+        constexpr int W = VT::W;
         const uint32_t nw = A.nrow / W, stride = gridDim.x * blockDim.x;
-        const V* pv = reinterpret_cast<const V*>(pj);
+        const V* rv = reinterpret_cast<const V*>(rj);
+        const V* pv = reinterpret_cast<const V*>(pOld);
+        const V* tv = reinterpret_cast<const V*>(tOld);
+        auto pg = [&](uint32_t h) { // pj at group h
+            const V r = rv[h], p = pv[h], t = tv[h];
+            T e[W];
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                const T tmp = fma(T(1), VT::at(p, j), nomega * VT::at(t, j));
+                e[j] = fma(T(1), VT::at(r, j), beta * tmp);
+            }
+            return VT::make(e);
+        };
         for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - (threadIdx.x & 31u) < nw;
              g += stride) {
             const bool act = g < nw;
             T sm[W];
 #pragma unroll
             for (int j = 0; j < W; ++j) sm[j] = T(0);
-            V c;
-            stencil_group<T, SH>(A, g, nw, act, [&](uint32_t h) { return pv[h]; }, c, sm);
-            if (act)
+            V cg;
+            stencil_group<T, SH>(A, g, nw, act, pg, cg, sm);
+            if (act) {
+                reinterpret_cast<V*>(pNew)[g] = cg; // the group's own pj
 #pragma unroll
                 for (int j = 0; j < W; ++j) own((size_t)W * g + j, sm[j]);
+            }
         }
     } else if (L == 1) {
         for (size_t row = (size_t)blockIdx.x * blockDim.x + threadIdx.x; row < A.nrow;
-             row += (size_t)gridDim.x * blockDim.x)
+             row += (size_t)gridDim.x * blockDim.x) {
+            pNew[row] = pat(row);
             own(row, row_apply<T, false>(A, row, xv));
+        }
     } else {
         const int lane = threadIdx.x & (L - 1);
         const size_t warpRows = 32 / L;
@@ -183,13 +215,18 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
                 for (uint32_t k = A.rowPtr[row] + lane; k < A.rowPtr[row + 1]; k += L)
                     sum = fma(A.val[k], xv(A.colInd[k]), sum);
             sum = group_sum<L>(sum);
-            if (lane == 0 && row < A.nrow) own(row, sum);
+            if (lane == 0 && row < A.nrow) {
+                pNew[row] = pat(row);
+                own(row, sum);
+            }
         }
     }
     double a[3] = {(double)a0, (double)a1, (double)a2};
     const int ops[3] = {kSum, kSum, kSum};
     grid_reduce_ctl<3>(a, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
-        if (!cs->bench) bi_after_p(cs, t);
+        if (cs->bench) return;
+        cs->par ^= 1;
+        bi_after_p(cs, t);
     });
 }
 
@@ -198,13 +235,15 @@ __global__ void __launch_bounds__(kBlock) bi_p(CSRView<T> A, const T* __restrict
 // with sj's groups formed from rj and ptmp by the same FMA.
 template <typename T, int L, int JAC, int SH = 0>
 __global__ void __launch_bounds__(kBlock) bi_s(CSRView<T> A, const T* __restrict__ rj,
-                                               const T* __restrict__ ptmp,
+                                               const T* __restrict__ t0,
+                                               const T* __restrict__ t1,
                                                const T* __restrict__ dinv, T* __restrict__ sj,
                                                T* __restrict__ stmp, BiCtl* c, Scratch s)
 {
     pdl_wait();
     pdl_release();
     if (c->status != kRun) return;
+    const T* __restrict__ ptmp = c->par ? t1 : t0;
     static_assert(SH == 0 || JAC != 2, "right preconditioning runs the row kernels");
     const T nalpha = (T)(-c->alpha);
     auto sv = [&](uint32_t j) { return fma(T(1), rj[j], nalpha * ptmp[j]); };
@@ -298,7 +337,8 @@ __device__ __forceinline__ void bi_x_elem(T alpha, T omega, T nomega, T p, T sv,
 
 template <typename T, int JAC, int VEC>
 __global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T* __restrict__ rj,
-                                               const T* __restrict__ pj,
+                                               const T* __restrict__ p0,
+                                               const T* __restrict__ p1,
                                                const T* __restrict__ sj,
                                                const T* __restrict__ stmp,
                                                const T* __restrict__ r0s,
@@ -307,6 +347,7 @@ __global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T*
     pdl_wait();
     pdl_release();
     if (c->status != kRun) return;
+    const T* __restrict__ pj = c->par ? p1 : p0;
     const T alpha = (T)c->alpha, omega = (T)c->omega, nomega = (T)(-c->omega);
     BiXSums<T> a;
     uint32_t i0 = 0;
@@ -345,23 +386,6 @@ __global__ void __launch_bounds__(kBlock) bi_x(uint32_t n, T* __restrict__ x, T*
     grid_reduce_ctl<5>(red, ops, s, c, [=] __device__(BiCtl* cs, const double* t) {
         if (!cs->bench) bi_checks(cs, t, 0);
     });
-}
-
-// pj = rj + beta (pj - omega ptmp)  (BiCGStab.cxx:184-185)
-template <typename T>
-__global__ void __launch_bounds__(kBlock) bi_dir(uint32_t n, T* __restrict__ pj,
-                                                 const T* __restrict__ rj,
-                                                 const T* __restrict__ ptmp, const BiCtl* c)
-{
-    pdl_wait();
-    pdl_release();
-    if (c->status != kRun) return;
-    const T beta = (T)c->beta, nomega = (T)(-c->omega);
-    GRID_STRIDE(i, n)
-    {
-        const T tmp = fma(T(1), pj[i], nomega * ptmp[i]);
-        pj[i] = fma(T(1), rj[i], beta * tmp);
-    }
 }
 
 // After the host finished an escalated branch (rj may have been recomputed and pj zeroed):
@@ -422,23 +446,27 @@ int BiEngine<T>::launch_iter()
     const int needS = c->grid(rows, kBlock);
     const int needV = c->grid(n, kBlock);
     auto fit = [&](const void* k, int need) { return std::min(need, resident_grid(*c, k, kBlock)); };
+    T *p0 = pj2[0], *p1 = pj2[1], *t0 = ptmp2[0], *t1 = ptmp2[1];
 #define BI_SPMV(KP, KS, LL, JJ)                                                            \
     do {                                                                                   \
         bi_launch(KP<T, LL, JJ>, fit((const void*)KP<T, LL, JJ>, needS), c->stream, pdl, V,  \
-                  (const T*)pj, (const T*)rj, (const T*)r0s, dinv, ptmp, ctl, c->red);      \
+                  p0, p1, t0, t1, (const T*)rj, (const T*)r0s, dinv, ctl, c->red);          \
         bi_launch(KS<T, LL, JJ>, fit((const void*)KS<T, LL, JJ>, needS), c->stream, pdl, V,  \
-                  (const T*)rj, (const T*)ptmp, dinv, sj, stmp, ctl, c->red);               \
+                  (const T*)rj, (const T*)t0, (const T*)t1, dinv, sj, stmp, ctl, c->red);   \
     } while (0)
     // 16-byte row groups on 5- and 7-point stencil masks (bi_p / bi_s with SH)
-    const int sh = L == 1 ? stencil_vec_shape(V, pj, rj, ptmp) : 0;
+    auto al16 = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    const int sh = L == 1 && al16(p1) && al16(t1) && al16(r0s) && al16(sj) && al16(stmp)
+                       ? stencil_vec_shape(V, p0, rj, t0)
+                       : 0;
 #define BI_SPMV_SH(JJ, SS)                                                                 \
     do {                                                                                   \
         bi_launch(bi_p<T, 1, JJ, SS>, fit((const void*)bi_p<T, 1, JJ, SS>, needV),         \
-                  c->stream, pdl, V, (const T*)pj, (const T*)rj, (const T*)r0s, dinv, ptmp, \
-                  ctl, c->red);                                                            \
-        bi_launch(bi_s<T, 1, JJ, SS>, fit((const void*)bi_s<T, 1, JJ, SS>, needV),         \
-                  c->stream, pdl, V, (const T*)rj, (const T*)ptmp, dinv, sj, stmp, ctl,     \
+                  c->stream, pdl, V, p0, p1, t0, t1, (const T*)rj, (const T*)r0s, dinv, ctl, \
                   c->red);                                                                 \
+        bi_launch(bi_s<T, 1, JJ, SS>, fit((const void*)bi_s<T, 1, JJ, SS>, needV),         \
+                  c->stream, pdl, V, (const T*)rj, (const T*)t0, (const T*)t1, dinv, sj,    \
+                  stmp, ctl, c->red);                                                      \
     } while (0)
 #define BI_LANES(JJ)                                                                       \
     switch (sh ? -sh : L) {                                                                \
@@ -452,11 +480,12 @@ int BiEngine<T>::launch_iter()
         default: BI_SPMV(bi_p, bi_s, 32, JJ); break;                                       \
     }
     // 16-byte groups when every vector bi_x touches starts on a 16-byte boundary
-    const bool vx = (((uintptr_t)x | (uintptr_t)rj | (uintptr_t)pj | (uintptr_t)sj |
-                      (uintptr_t)stmp | (uintptr_t)r0s | (uintptr_t)(jacobi ? dinv : pj)) & 15) == 0;
+    const bool vx = (((uintptr_t)x | (uintptr_t)rj | (uintptr_t)p0 | (uintptr_t)p1 |
+                      (uintptr_t)sj | (uintptr_t)stmp | (uintptr_t)r0s |
+                      (uintptr_t)(jacobi ? dinv : p0)) & 15) == 0;
     auto launch_x = [&](auto kern) {
-        bi_launch(kern, fit((const void*)kern, needV), c->stream, pdl, n, x, rj, (const T*)pj,
-                  (const T*)sj, (const T*)stmp, (const T*)r0s, dinv, ctl, c->red);
+        bi_launch(kern, fit((const void*)kern, needV), c->stream, pdl, n, x, rj, (const T*)p0,
+                  (const T*)p1, (const T*)sj, (const T*)stmp, (const T*)r0s, dinv, ctl, c->red);
     };
     if (jacobi && rightPcd) { // A (D v): the row kernels (no stencil groups)
         switch (L) {
@@ -487,23 +516,19 @@ int BiEngine<T>::launch_iter()
 #undef BI_LANES
 #undef BI_SPMV_SH
 #undef BI_SPMV
-    bi_launch(bi_dir<T>, fit((const void*)bi_dir<T>, needV), c->stream, pdl, n, pj,
-              (const T*)rj, (const T*)ptmp, (const BiCtl*)ctl);
-    if (!capturing) c->launches += 4;
+    if (!capturing) c->launches += 3;
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
 // The checks resume at c->phase and end with beta; the direction update of the same
 // iteration (BiCGStab.cxx:184-185, after every branch of the checks, a restart's pj = 0
-// included) follows when they leave the status at kRun: the escalation stopped the graph
-// before its bi_dir, and the next graph starts at bi_p.
+// included) is the next bi_p's, which forms it from whatever the host left in pj(par).
 template <typename T>
 int BiEngine<T>::launch_resume()
 {
-    c->launches += 2;
+    ++c->launches;
     bi_resume<T><<<c->grid(n, kBlock), kBlock, 0, c->stream>>>(n, rj, r0s, ctl, c->red);
-    bi_dir<T><<<c->grid(n, kBlock), kBlock, 0, c->stream>>>(n, pj, rj, ptmp, ctl);
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -533,7 +558,7 @@ int BiEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool grap
     dinv = dinvv;
     useGraph = graph;
     const size_t bytes = ((size_t)n + 4) * sizeof(T);
-    T** vecs[] = {&x, &rj, &r0s, &pj, &ptmp, &sj, &stmp};
+    T** vecs[] = {&x, &rj, &r0s, &pj2[0], &pj2[1], &ptmp2[0], &ptmp2[1], &sj, &stmp};
     for (T** v : vecs)
         if (cudaMalloc(v, bytes) != cudaSuccess) {
             cudaGetLastError();
@@ -567,7 +592,7 @@ void BiEngine<T>::destroy()
 {
     if (gexec) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
-    T** vecs[] = {&x, &rj, &r0s, &pj, &ptmp, &sj, &stmp};
+    T** vecs[] = {&x, &rj, &r0s, &pj2[0], &pj2[1], &ptmp2[0], &ptmp2[1], &sj, &stmp};
     for (T** v : vecs) {
         cudaFree(*v);
         *v = nullptr;
@@ -593,7 +618,7 @@ int BiEngine<T>::run(unsigned* launches)
             FB_CUDA(cudaMemcpyAsync(hstatus, &ctl->status, sizeof(int), cudaMemcpyDeviceToHost,
                                     c->stream));
             FB_CUDA(cudaStreamSynchronize(c->stream));
-            if (launches) *launches += 4 * itersPerGraph;
+            if (launches) *launches += 3 * itersPerGraph;
             if (*hstatus != kRun) return kOk;
         }
     }
@@ -611,7 +636,7 @@ int BiEngine<T>::run(unsigned* launches)
             err = kErrCuda;
             break;
         }
-        if (launches) *launches += 4 * itersPerGraph;
+        if (launches) *launches += 3 * itersPerGraph;
         if (cudaEventSynchronize(ev[cur]) != cudaSuccess) {
             err = kErrCuda;
             break;
@@ -619,7 +644,7 @@ int BiEngine<T>::run(unsigned* launches)
         if (*hstatus != kRun) break;
         cur ^= 1;
     }
-    if (launches) *launches += 4 * itersPerGraph;
+    if (launches) *launches += 3 * itersPerGraph;
     cudaStreamSynchronize(c->stream);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);

@@ -27,24 +27,30 @@ struct BiCtl {
     // recursive residual has fallen below delta x its largest value since the last refresh
     int      reliable;
     double   delta, rmax;
+    // which of the two direction buffers (pj, ptmp) holds the current iteration's values:
+    // bi_p reads the other pair and flips it in its finalize
+    int      par;
 };
 
-// One iteration is four kernels (Jacobi from zero is a diagonal scaling, D = weight/diag):
-//   bi_p      ptmp = D A pj, with (ptmp, r0*), (rj, r0*) and (rj, rj)      (CG.cxx-style
-//             loop top, BiCGStab.cxx:79-102)
+// One iteration is three kernels (Jacobi from zero is a diagonal scaling, D = weight/diag):
+//   bi_p      pj = rj + beta (pj_old - omega ptmp_old), the previous iteration's direction
+//             update (:184-185), formed for every gathered entry and stored for the owned
+//             rows into the other buffer of a pair; ptmp = D A pj, with (ptmp, r0*),
+//             (rj, r0*) and (rj, rj) (the loop top, BiCGStab.cxx:79-102). beta = 0 at the
+//             start makes pj = rj (:78).
 //   bi_s      sj = rj - alpha ptmp formed on the fly, stmp = D A sj, with (stmp, sj) and
 //             (stmp, stmp)                                                  (:103-113)
 //   bi_x      x += alpha D pj + omega D sj, rj = sj - omega stmp, with (r,r), (r,r0*), max|x|,
-//             (p,p), (x,x) and the checks of :117-175                        (:114-175)
-//   bi_dir    pj = rj + beta (pj - omega ptmp)                              (:177-186)
+//             (p,p), (x,x) and the checks of :117-175 ending with beta       (:114-183)
 template <typename T>
 struct BiEngine {
     Ctx*       c = nullptr;
     const Mat* A = nullptr;
     int        jacobi = 0;
     const T*   dinv = nullptr;
-    T *x = nullptr, *rj = nullptr, *r0s = nullptr, *pj = nullptr, *ptmp = nullptr,
-      *sj = nullptr, *stmp = nullptr;
+    T *x = nullptr, *rj = nullptr, *r0s = nullptr, *sj = nullptr, *stmp = nullptr;
+    T *pj2[2] = {nullptr, nullptr}, *ptmp2[2] = {nullptr, nullptr}; // chosen by ctl->par
+    T* pj(int par) const { return pj2[par & 1]; } // the direction of iteration par
     BiCtl*     ctl = nullptr;     // device
     BiCtl*     hctl = nullptr;    // pinned host copy
     int*       hstatus = nullptr; // pinned, written at the end of every graph launch

@@ -1123,10 +1123,11 @@ int SolverImpl::bicgstab_reliable(const double* b, double* x, fasp_gpu_info* inf
     bool converged = rn / den < P.relTol || rn < P.absTol;
     if (!converged && std::isfinite(rn) && P.maxIter > 0) {
         const double s = rn;
-        // e = 0, r = (b - A x) / s, r0* = p = r (BiCGStab.cxx:70-78 on the scaled system)
+        // e = 0, r = (b - A x) / s, r0* = p = r (BiCGStab.cxx:70-78 on the scaled system;
+        // the first bi_p forms p = r from zeroed direction buffers and beta = omega = 0)
         if ((e = convert_scaled(c, n, r64, 1.0 / s, E.rj)) || (e = set32(c, n, E.x))) return e;
         v_copy(c, n, (const float*)E.rj, E.r0s);
-        v_copy(c, n, (const float*)E.rj, E.pj);
+        if ((e = set32(c, n, E.pj(0))) || (e = set32(c, n, E.ptmp2[0]))) return e;
         std::memset(&h, 0, sizeof(BiCtl));
         h.status = kRun;
         h.code = kOk;
@@ -1348,12 +1349,14 @@ int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info*
     T* sv = (*S.w)[11];
     std::vector<std::pair<uint32_t, double>> patches; // raw values, recorded through rec()
     int e;
-    // BiCGStab.cxx:70-78: rj = b - A x, r0star = rj, pj = rj
+    // BiCGStab.cxx:70-78: rj = b - A x, r0star = rj, pj = rj (the first bi_p forms pj =
+    // rj + beta (pj(0) - omega ptmp(0)) with beta = omega = 0 from zeroed buffers)
     v_copy(c, n, (const T*)x, E.x);
-    if ((e = m_spmv(c, *A, (const T*)E.x, E.ptmp))) return e;
-    v_waxpby(c, n, Scal::h(1.0), b, Scal::h(-1.0), (const T*)E.ptmp, E.rj);
+    if ((e = m_spmv(c, *A, (const T*)E.x, E.sj))) return e;
+    v_waxpby(c, n, Scal::h(1.0), b, Scal::h(-1.0), (const T*)E.sj, E.rj);
     v_copy(c, n, (const T*)E.rj, E.r0s);
-    v_copy(c, n, (const T*)E.rj, E.pj);
+    v_set(c, n, 0.0, E.pj(0));
+    v_set(c, n, 0.0, E.ptmp2[0]);
     std::memset(&h, 0, sizeof(BiCtl));
     h.status = P.maxIter > 0 ? kRun : kDone;
     h.code = kOk;
@@ -1399,7 +1402,7 @@ int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info*
                 h.code = kErrStag;
                 stop = true;
             } else {
-                v_set(c, n, 0.0, E.pj);
+                v_set(c, n, 0.0, E.pj(h.par));
                 ++h.stagStep;
             }
         } else if (h.reason == kBiCheck) { // :164-175
@@ -1410,7 +1413,7 @@ int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info*
                 h.code = kErrTolSmall;
                 stop = true;
             } else {
-                v_set(c, n, 0.0, E.pj);
+                v_set(c, n, 0.0, E.pj(h.par));
                 ++h.moreStep;
             }
         }
