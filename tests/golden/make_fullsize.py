@@ -22,6 +22,7 @@ Cases:
 * ``cd96_pe{01,10}_{bicgstab,gmres}`` -- 96^3 upwind convection-diffusion, weighted Jacobi
   2/3, rtol 1e-8, GMRES(30) with a fixed restart;
 * ``cd96_pe{01,10}_fgmres300`` -- FGMRES(30), its first 300 iterations;
+* ``cd96_pe{01,10}_gmresvar`` -- GMRES with the reference's default variable restart;
 * ``vd64_adjoint`` -- 64^3 variable-coefficient diffusion, forward CG to rtol 1e-10, the
   adjoint CG on MAT::TransInPlace(A) (the reference's transpose), dL/db = lambda and
   dL/dA_k = -lambda_row(k) x_col(k); stored as projections on 32 seeded directions plus
@@ -67,6 +68,9 @@ def solver_cases() -> dict:
                                   dict(SYN, maxIter=5000, relTol=1e-8, **JAC23, **GM30))
         C[f"cd96_{tag}_fgmres300"] = (("convdiff3d", 96, pe), "fgmres", "xstar11",
                                       dict(SYN, maxIter=300, relTol=1e-8, **JAC23, **GM30))
+        # the reference's default variable restart (between 10 and 30, GMRES.cxx:255-265)
+        C[f"cd96_{tag}_gmresvar"] = (("convdiff3d", 96, pe), "gmres", "xstar11",
+                                     dict(SYN, maxIter=5000, relTol=1e-8, **JAC23))
     return C
 
 
