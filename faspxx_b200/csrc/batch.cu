@@ -715,6 +715,7 @@ int fasp_gpu_batch_solve(fasp_gpu_batch h, const double* b, double* x, double re
                          uint32_t* iters, double* resRel)
 {
     if (!h || !b || !x || relTol <= 0) return kErrInputPar;
+    TraceRange trace("fasp batch solve");
     fasp_gpu_batch_s& B = *h;
     const uint32_t N = B.M.nrow, cnt = B.count, nr = B.nrhs;
     const size_t vN = (size_t)nr * N;

@@ -273,6 +273,7 @@ static int mat_create(uint32_t nrow, uint32_t mcol, uint32_t nnz, const uint32_t
                       const uint32_t* colInd, const double* values, bool host,
                       fasp_gpu_mat* out)
 {
+    TraceRange trace("fasp matrix upload");
     if (!out || !rowPtr || !colInd) return kErrInputPar;
     *out = nullptr;
     fasp_gpu_mat h = new (std::nothrow) fasp_gpu_mat_s();
@@ -709,6 +710,7 @@ int fasp_gpu_solver_create(const fasp_gpu_config* cfg, fasp_gpu_solver* out)
 int fasp_gpu_solver_setup(fasp_gpu_solver s, fasp_gpu_mat A)
 {
     if (!s || !A) return kErrInputPar;
+    TraceRange trace("fasp solver setup");
     s->s.destroy();
     return s->s.setup(A);
 }

@@ -2,13 +2,26 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
+#include <string>
 #include <vector>
 
 #include "common.cuh"
 
 namespace fb {
+
+// An NVTX range over a scope: the solver's phases (matrix upload, setup, solve, the
+// reliable-update refreshes, batched solves) appear as named ranges under a tracing tool
+// (Nsight Systems, ncu --nvtx); with no tool attached the calls return at once.
+struct TraceRange {
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    explicit TraceRange(const std::string& name) { nvtxRangePushA(name.c_str()); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
 
 // Return codes: the FaspRetCode values of FASP++ (src/RetCode.hxx:24-55), plus two for the
 // device layer.

@@ -1041,6 +1041,7 @@ int SolverImpl::cg_reliable(const double* b, double* x, fasp_gpu_info* info)
             }
             // a host refresh: the stop test or delta reached (persistent engine), or the end
             // of the FP32 run (maxIter, breakdown)
+            TraceRange refresh("fasp reliable refresh");
             if ((e = E.apply_pending_x()) || (e = update_from32(c, n, s, E.x, x64)) ||
                 (e = set32(c, n, E.x)))
                 return e;
@@ -1157,6 +1158,7 @@ int SolverImpl::bicgstab_reliable(const double* b, double* x, fasp_gpu_info* inf
                 continue;
             }
             // a refresh, the FP32 stop test, or the end of the run (maxIter, breakdown)
+            TraceRange refresh("fasp reliable refresh");
             if ((e = update_from32(c, n, s, E.x, x64)) || (e = set32(c, n, E.x))) return e;
             if ((e = true_res(&rn))) return e;
             ++refreshes;
@@ -2411,6 +2413,14 @@ int SolverImpl::refine(const double* b, double* x, fasp_gpu_info* info)
 int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
 {
     if (!A) return kErrInputPar;
+    static const char* const kAlg[] = {"?", "CG", "BiCGStab", "?", "GMRES", "FGMRES"};
+    static const char* const kPrec[] = {"FP64", "MIXED", "MIXED_RELIABLE"};
+    const char* an = cfg.alg >= 0 && cfg.alg <= 5 ? kAlg[cfg.alg]
+                     : cfg.alg == FASP_GPU_JACOBI ? "Jacobi"
+                     : cfg.alg == FASP_GPU_MG     ? "MG"
+                                                  : "?";
+    const char* pn = cfg.precision >= 0 && cfg.precision <= 2 ? kPrec[cfg.precision] : "?";
+    TraceRange trace(std::string("fasp solve ") + an + " " + pn);
     fasp_gpu_info tmp;
     if (!info) info = &tmp;
     std::memset(info, 0, sizeof(*info));
