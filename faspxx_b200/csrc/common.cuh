@@ -297,6 +297,43 @@ __device__ __forceinline__ T row_dot(const CSRView<T>& A, size_t row, uint32_t b
     return s;
 }
 
+// Two CSR rows r0, r1 on one thread, interleaved: both rows' pointers, then both rows'
+// chunks of four column/value loads, then their gathers, then the FMAs, each row left to
+// right as row_dot sums it (the same bits). A thread that walks its rows one at a time waits
+// for three dependent round trips per row (row pointer, entries, gathers); two at a time it
+// waits half as often.
+template <typename T, typename XV>
+__device__ __forceinline__ void row_dot2(const CSRView<T>& A, size_t r0, size_t r1, XV xv,
+                                         T& s0, T& s1)
+{
+    const uint32_t b0 = ld_stream(A.rowPtr + r0), e0 = ld_stream(A.rowPtr + r0 + 1);
+    const uint32_t b1 = ld_stream(A.rowPtr + r1), e1 = ld_stream(A.rowPtr + r1 + 1);
+    s0 = T(0);
+    s1 = T(0);
+    for (uint32_t k = 0; b0 + k < e0 || b1 + k < e1; k += 4) {
+        uint32_t c0[4], c1[4];
+        T v0[4], v1[4], x0[4], x1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool in0 = b0 + k + u < e0, in1 = b1 + k + u < e1;
+            c0[u] = in0 ? ld_stream(A.colInd + b0 + k + u) : 0u;
+            c1[u] = in1 ? ld_stream(A.colInd + b1 + k + u) : 0u;
+            v0[u] = in0 ? ld_stream(A.val + b0 + k + u) : T(0);
+            v1[u] = in1 ? ld_stream(A.val + b1 + k + u) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            x0[u] = b0 + k + u < e0 ? xv(c0[u]) : T(0);
+            x1[u] = b1 + k + u < e1 ? xv(c1[u]) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (b0 + k + u < e0) s0 = fma(v0[u], x0[u], s0);
+            if (b1 + k + u < e1) s1 = fma(v1[u], x1[u], s1);
+        }
+    }
+}
+
 // ---- block tiles of plain CSR, streamed by bulk async copies ------------------------------
 // Thread per row streams each row's column indices and values on its own: the lanes of a
 // warp read 4-byte words some 28 bytes apart (a 7-entry row), and a thread has one row's
