@@ -372,10 +372,13 @@ struct alignas(16) TileSmem {
     unsigned long long full[kTileStages]; // mbarriers: one phase per copied tile
     uint32_t a[kTileStages];              // the stage's first entry index
     uint32_t ok[kTileStages];             // entries staged (else only the row pointers)
+    uint32_t bad;                         // a tile wait ran out: the block leaves
 };
 
 // Waits that ran out (a bulk copy that never completed): counted here, per translation
-// unit, and read by tile_timeouts() on the host.
+// unit, and read by tile_timeouts() on the host. The block then stops: it waits (bounded
+// again) for the copies it still has in flight and returns, leaving the rest of its rows
+// unwritten.
 static __device__ unsigned fb_tile_timeouts;
 
 extern __shared__ __align__(16) unsigned char fb_tile_smem[];
@@ -462,6 +465,7 @@ __device__ __forceinline__ void csr_tile_rows(const CSRView<T>& A, TileSmem<T>& 
         }
     };
     if (tid == 0) {
+        sm.bad = 0;
         for (int s = 0; s < kTileStages; ++s)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&sm.full[s]))
                          : "memory");
@@ -471,10 +475,13 @@ __device__ __forceinline__ void csr_tile_rows(const CSRView<T>& A, TileSmem<T>& 
     __syncthreads();
     for (size_t k = 0; k < mine; ++k) {
         const int s = (int)(k % kTileStages);
-        if (!mbar_wait_bounded(&sm.full[s], (uint32_t)((k / kTileStages) & 1)))
+        const bool landed = mbar_wait_bounded(&sm.full[s], (uint32_t)((k / kTileStages) & 1));
+        if (!landed) {
             atomicAdd(&fb_tile_timeouts, 1u);
+            sm.bad = 1;
+        }
         const size_t row = (blockIdx.x + k * gridDim.x) * kTileRows + tid;
-        if (row < n) {
+        if (landed && row < n) {
             const TileStage<T>& st = sm.st[s];
             const uint32_t b = st.rp[tid], e = st.rp[tid + 1];
             T sum = T(0);
@@ -502,6 +509,13 @@ __device__ __forceinline__ void csr_tile_rows(const CSRView<T>& A, TileSmem<T>& 
             own(row, sum);
         }
         __syncthreads(); // stage s is free again
+        if (sm.bad) { // every thread sees it after the barrier: leave together
+            if (tid == 0) // the copies this block still has in flight (tiles k .. k + 1)
+                for (size_t j = k; j < k + kTileStages && j < mine; ++j)
+                    mbar_wait_bounded(&sm.full[j % kTileStages],
+                                      (uint32_t)((j / kTileStages) & 1));
+            return;
+        }
         if (tid == 0 && k + kTileStages < mine) issue(k + kTileStages);
     }
 }
