@@ -767,7 +767,7 @@ def _time_solve(s, db, dx, reps, warm=2, flush=None):
     return statistics.mean(ts), code
 
 
-def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=None):
+def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=None, orth=None):
     """Nonsymmetric 3D convection-diffusion -Laplace(u) + beta.grad(u) on N^3 (first-order
     upwind, direction (1, 0.5, 0.25), cell Peclet 0.1 and 10), b = A x* with x* ~ U[-1,1)
     (seed 42), x0 = 0, rtol 1e-8, weighted Jacobi (omega = 2/3, one sweep), GMRES/FGMRES with
@@ -775,7 +775,8 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
     between 10 and 30: FP64, FP32 inner iterations inside FP64 refinement (FP64 residual,
     update and Hessenberg/Givens least squares) and, for BiCGStab, FP32 iterations with FP64
     reliable updates. reference: the reference's iteration counts by case name,
-    where recorded."""
+    where recorded. orth: the GMRES/FGMRES Gram-Schmidt variant (None: the library's
+    default)."""
     from faspxx_b200 import capi, problems as P, sol
     flush = sol.DVec(32 << 20)
     rows = []
@@ -796,6 +797,8 @@ def krylov_results(N, steps, algs=("bicgstab", "gmres", "fgmres"), reference=Non
                     kw.update(restart=30, maxRestart=30, minRestart=30)
                 # gmresvar: the reference's default variable restart (10 to 30)
                 s = sol.configure("gmres" if alg == "gmresvar" else alg, **kw)
+                if orth is not None and alg in ("gmres", "gmresvar", "fgmres"):
+                    s.SetOrth(orth)
                 if prec == "mixed":
                     s.SetPrecision(capi.MIXED, innerRelTol=1e-4, maxOuter=50)
                 elif prec == "reliable":
@@ -853,6 +856,8 @@ def run_krylov(args):
             if alg == "gmres":
                 kw.update(restart=30, maxRestart=30, minRestart=30)
             s = sol.configure(alg.split("-")[0], **kw)
+            if alg == "gmres" and args.orth != "default":
+                s.SetOrth(getattr(capi, "ORTH_" + args.orth.upper()))
             if alg == "bicgstab-reliable":
                 s.SetPrecision(capi.MIXED_RELIABLE, innerRelTol=1e-2)
             s.Setup(M)
@@ -861,8 +866,9 @@ def run_krylov(args):
             print(f"profile {alg} code {code} iterations {s.GetIterations()} "
                   f"{s.LastTimeMs():.3f} ms")
         return 0
+    orth = None if args.orth == "default" else getattr(capi, "ORTH_" + args.orth.upper())
     rows = krylov_results(N, args.steps, algs=("bicgstab", "gmres", "gmresvar", "fgmres"),
-                          reference=fullsize_reference())
+                          reference=fullsize_reference(), orth=orth)
     total_mixed = sum(r["mixed"]["ms"] for r in rows)
     line = {"metric": "Time to rtol 1e-8, 96^3 convection-diffusion, BiCGStab / GMRES(30) / "
                       "FGMRES(30): FP32-inner refinement vs FP64",
@@ -1234,6 +1240,8 @@ def main():
     ap.add_argument("--no-workloads", action="store_true",
                     help="leave out the other configurations' compact block")
     ap.add_argument("--lanes", type=int, default=0, help="force SpMV lanes per row")
+    ap.add_argument("--orth", choices=["default", "cgs2", "dcgs2", "mgs"], default="default",
+                    help="krylov96: the GMRES/FGMRES Gram-Schmidt variant")
     ap.add_argument("--profile", action="store_true",
                     help="short runs for ncu: each fused CG kernel 4 times (poisson128), or "
                          "one 60-iteration BiCGStab and GMRES(30) solve (krylov96)")

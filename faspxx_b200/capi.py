@@ -19,7 +19,7 @@ lib = C.CDLL(LIB_PATH)
 # fasp_gpu_alg / precision / orth
 IDENTITY, CG, BICGSTAB, GMRES, FGMRES, JACOBI, MG = 0, 1, 2, 4, 5, 11, 21
 FP64, MIXED, MIXED_RELIABLE = 0, 1, 2
-ORTH_CGS2, ORTH_MGS = 0, 1
+ORTH_CGS2, ORTH_MGS, ORTH_DCGS2 = 0, 1, 2
 ERROR_CUDA, ERROR_NO_DEVICE = -101, -102
 
 

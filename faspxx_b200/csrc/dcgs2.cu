@@ -1,0 +1,469 @@
+// dcgs2.cu -- the Arnoldi step of GMRES (GMRES.cxx:160-210, the orthogonalisation of
+// :169-175) as classical Gram-Schmidt with delayed re-orthogonalisation (DCGS2: Bielich,
+// Langou, Thomas, Swirydowicz, Yamazaki, Boman, "Low-synch Gram-Schmidt with delayed
+// reorthogonalization for Krylov solvers", Parallel Computing 112, 2022).
+//
+// Step j starts from the orthonormal q_0 .. q_{j-1} (Q) and u, the candidate for q_j
+// projected once against Q, in basis slot j. It runs the product w = A M u and two passes
+// over the basis:
+//   dots    a = Q^T u, b = Q^T w, c = u^T w, d = u^T u in one grid reduction; the last block
+//           then re-orthogonalises u in exact arithmetic (t = sqrt(d - a^T a), q_j = (u -
+//           Q a) / t), completes Hessenberg column j - 1 (+= a, subdiagonal t), applies the
+//           reference's Givens step to it, and forms the tentative column j of A M q_j =
+//           (w - Q_{j+1} H a) / t: h = (b - H a) / t, h_j = ((c - a^T b) / t - t a_{j-1}) / t
+//   update  q_j = (u - Q a) / t into slot j and u_{j+1} = (w - Q b - q_j g) / t into slot
+//           j + 1, g = (c - a^T b) / t, the candidate projected once against q_0 .. q_j
+// Each pass streams the basis once, where CGS2 streams it three times (multi-dot, fused
+// projection + multi-dot, projection + norm) and then scales the new vector: 2j + 6
+// vectors of traffic per step instead of 3j + 10, and two launches instead of five.
+// Iteration i of the reference (Hessenberg column i - 1) completes in the dots pass of
+// step i; a restart cycle of s iterations ends with a dots pass without a product.
+//
+// Both passes stream 16 KB chunks of each vector through a ring of shared-memory stages
+// with bulk asynchronous copies (cp.async.bulk, completion counted in bytes on an
+// mbarrier), issued by one thread six stages ahead of the consuming threads; block b takes
+// the contiguous element range b of the grid, chunk by chunk, and per chunk the vectors in
+// a fixed order (u, w, then Q). Sums are fixed-order: a thread adds its 8 (FP64) or 16
+// (FP32) elements of an item, the warp a shuffle tree, each warp its items in chunk order,
+// the block its warps in order and the last block the blocks in order -- reruns give the
+// same bits.
+#include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
+
+#include "common.cuh"
+#include "gmres.cuh"
+
+namespace fb {
+
+constexpr uint32_t kDcStageBytes = 16384;
+constexpr int      kDcStages = 6;
+constexpr int      kDcThreads = 256;
+constexpr int      kDcWarps = kDcThreads / 32;
+constexpr int      kDcMaxNV = 2 * kDcMaxK + 2; // values of one dots pass
+
+template <typename T>
+struct DcShape {
+    static constexpr int      W = Vec16<T>::W;                    // elements per 16 bytes
+    static constexpr uint32_t C = kDcStageBytes / sizeof(T);      // elements per chunk
+    static constexpr int      G = (int)(C / W) / kDcThreads;      // 16-byte groups a thread
+};
+
+struct alignas(16) DcRing {
+    unsigned char      st[kDcStages][kDcStageBytes];
+    unsigned long long full[kDcStages];
+    int                bad;
+};
+
+// The basis, the product and the step.
+template <typename T>
+struct DcArgs {
+    T*       V;    // basis slots 0 .. j + 1, leading dimension ld
+    size_t   ld;
+    const T* w;    // A M u (null in the closing dots pass of a cycle)
+    uint32_t n;
+    int      j;
+};
+
+// The contiguous element range of this block: a multiple of the 16-byte group.
+template <typename T>
+__device__ __forceinline__ void dc_range(uint32_t n, size_t& e0, size_t& e1)
+{
+    constexpr int W = DcShape<T>::W;
+    const size_t per = (((size_t)n + gridDim.x - 1) / gridDim.x + W - 1) / W * W;
+    e0 = std::min((size_t)n, (size_t)blockIdx.x * per);
+    e1 = std::min((size_t)n, e0 + per);
+}
+
+// A bulk copy at the default L2 priority: the basis is read again in the next pass and the
+// next step, and stays in L2 while it fits.
+__device__ __forceinline__ void bulk_copy_g2s_plain(void* dst, const void* src, uint32_t bytes,
+                                                    unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+                 " [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Streams items k = 0 .. total-1 (chunk k / nItem, vector k % nItem of src(v)) through the
+// ring; consume(k, stage, len) runs on every thread once the item's bytes have landed, the
+// block synchronises after each item and thread 0 then refills that stage. The copies start
+// on 16-byte boundaries (the range starts are) and round their length up to 16 bytes: at
+// most 8 bytes past the last element, inside every vector's allocation. False when a wait
+// ran out: the block has then drained its copies in flight (bounded) and stopped.
+template <typename T, typename Src, typename Consume>
+__device__ __forceinline__ bool dc_stream(DcRing& ring, size_t e0, size_t e1, int nItem, Src src,
+                                          Consume consume)
+{
+    constexpr uint32_t C = DcShape<T>::C;
+    const uint32_t tid = threadIdx.x;
+    const size_t nc = (e1 - e0 + C - 1) / C;
+    const size_t total = nc * (size_t)nItem;
+    auto issue = [&](size_t k) {
+        const int s = (int)(k % kDcStages);
+        const size_t base = e0 + (k / nItem) * C;
+        const size_t len = std::min((size_t)C, e1 - base);
+        const uint32_t bytes = (uint32_t)((len * sizeof(T) + 15) & ~size_t(15));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_addr(&ring.full[s])),
+                     "r"(bytes)
+                     : "memory");
+        bulk_copy_g2s_plain(ring.st[s], src((int)(k % nItem)) + base, bytes, &ring.full[s]);
+    };
+    if (tid == 0) {
+        ring.bad = 0;
+        for (int s = 0; s < kDcStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring.full[s]))
+                         : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (size_t k = 0; k < (size_t)kDcStages && k < total; ++k) issue(k);
+    }
+    __syncthreads();
+    for (size_t k = 0; k < total; ++k) {
+        const int s = (int)(k % kDcStages);
+        // the consumers hold warp-collective sums: a warp consumes only if all its lanes saw
+        // the bytes land
+        const bool mine = mbar_wait_bounded(&ring.full[s], (uint32_t)((k / kDcStages) & 1));
+        const bool landed = __all_sync(0xffffffffu, mine);
+        if (!landed) {
+            if (!mine) atomicAdd(&fb_tile_timeouts, 1u);
+            ring.bad = 1;
+        }
+        const size_t base = e0 + (k / nItem) * C;
+        if (landed) consume(k, (const T*)ring.st[s], (uint32_t)std::min((size_t)C, e1 - base));
+        __syncthreads(); // stage s is free again
+        if (ring.bad) {
+            if (tid == 0)
+                for (size_t i = k; i < k + kDcStages && i < total; ++i)
+                    mbar_wait_bounded(&ring.full[i % kDcStages], (uint32_t)((i / kDcStages) & 1));
+            return false;
+        }
+        if (tid == 0 && k + kDcStages < total) issue(k + kDcStages);
+    }
+    return true;
+}
+
+// A thread's elements of a chunk: groups tid, tid + 256, ... (a warp reads 512 contiguous
+// bytes per group); entries at or past len read as zero.
+template <typename T>
+__device__ __forceinline__ void dc_load(const T* st, uint32_t len,
+                                        T (&r)[DcShape<T>::G][DcShape<T>::W])
+{
+    using S = DcShape<T>;
+    using VT = typename Vec16<T>::type;
+#pragma unroll
+    for (int g = 0; g < S::G; ++g) {
+        const uint32_t i0 = (uint32_t)(g * kDcThreads + threadIdx.x) * S::W;
+        if (i0 + S::W <= len) {
+            *(VT*)r[g] = *(const VT*)(st + i0);
+        } else {
+#pragma unroll
+            for (int e = 0; e < S::W; ++e) r[g][e] = i0 + e < len ? st[i0 + e] : T(0);
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T dc_dot(const T (&x)[DcShape<T>::G][DcShape<T>::W],
+                                    const T (&y)[DcShape<T>::G][DcShape<T>::W])
+{
+    T s = T(0);
+#pragma unroll
+    for (int g = 0; g < DcShape<T>::G; ++g)
+#pragma unroll
+        for (int e = 0; e < DcShape<T>::W; ++e) s = fma(x[g][e], y[g][e], s);
+    return s;
+}
+
+// ---- the dots pass and the step's scalar work ----------------------------------------
+
+// Value slots: a_l at l, then (with w) b_l at j + l, c at 2j, and d last.
+template <typename T, bool HASW>
+__global__ void __launch_bounds__(kDcThreads, 2)
+k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
+{
+    extern __shared__ __align__(16) unsigned char dc_raw[];
+    DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
+    __shared__ double wacc[kDcWarps][kDcMaxNV];
+    __shared__ double tot[kDcMaxNV];
+    __shared__ double col[kDcMaxK + 2], hcol[kDcMaxK];
+    __shared__ bool amLast;
+    if (g->stop) return;
+    using S = DcShape<T>;
+    const int j = P.j;
+    const int nv = HASW ? 2 * j + 2 : j + 1;
+    const int nItem = 1 + (HASW ? 1 : 0) + j;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int v = tid; v < kDcWarps * nv; v += kDcThreads) wacc[v / nv][v % nv] = 0.0;
+    size_t e0, e1;
+    dc_range<T>(P.n, e0, e1);
+    __syncthreads();
+    T u[S::G][S::W], w[S::G][S::W];
+    auto src = [&](int v) -> const T* {
+        if (v == 0) return P.V + (size_t)j * P.ld;
+        if (HASW && v == 1) return P.w;
+        return P.V + (size_t)(v - 1 - (HASW ? 1 : 0)) * P.ld;
+    };
+    auto add = [&](int slot, double x) { // the warp's sum of an item, lane 0 keeps it
+        x = warp_reduce(x, kSum);
+        if (lane == 0) wacc[wid][slot] += x;
+    };
+    const bool ok = dc_stream<T>(ring, e0, e1, nItem, src, [&](size_t k, const T* st, uint32_t len) {
+        const int v = (int)(k % nItem);
+        if (v == 0) {
+            dc_load<T>(st, len, u);
+            add(nv - 1, (double)dc_dot<T>(u, u));
+        } else if (HASW && v == 1) {
+            dc_load<T>(st, len, w);
+            add(2 * j, (double)dc_dot<T>(u, w));
+        } else {
+            const int l = v - 1 - (HASW ? 1 : 0);
+            T q[S::G][S::W];
+            dc_load<T>(st, len, q);
+            add(l, (double)dc_dot<T>(q, u));
+            if (HASW) add(j + l, (double)dc_dot<T>(q, w));
+        }
+    });
+    // a block that stopped early still takes its ticket, with NaN partials: the step then
+    // sees t = NaN and breaks the cycle off (the reference's breakdown exit)
+    __syncthreads();
+    for (int v = tid; v < nv; v += kDcThreads) {
+        double a = 0.0;
+        for (int q = 0; q < kDcWarps; ++q) a += wacc[q][v];
+        s.partials[(size_t)v * gridDim.x + blockIdx.x] = ok ? a : (double)NAN;
+    }
+    __syncthreads();
+    if (tid == 0) amLast = last_block_ticket(s.ticket);
+    __syncthreads();
+    if (!amLast) return;
+    // totals: warp q adds value v = q, q + 8, ... over the blocks (lane l takes blocks l,
+    // l + 32, ... in order, then a shuffle tree)
+    for (int v = wid; v < nv; v += kDcWarps) {
+        double a = 0.0;
+        for (uint32_t b = lane; b < gridDim.x; b += 32)
+            a += __ldcg(&s.partials[(size_t)v * gridDim.x + b]);
+        a = warp_reduce(a, kSum);
+        if (lane == 0) tot[v] = a;
+    }
+    __syncthreads();
+    const size_t m = L.m;
+#define HR(i, l) L.hraw[(size_t)(i) * m + (l)]
+    const double* A = tot;     // a_l
+    const double* B = tot + j; // b_l (with w)
+    double t = 1.0, tinv = 1.0;
+    if (j >= 1) {
+        // re-orthogonalisation of u: column j - 1 gains a, its subdiagonal is ||u - Q a||
+        double ssq = 0.0;
+        for (int l = 0; l < j; ++l) ssq = fma(A[l], A[l], ssq);
+        const double t2 = tot[nv - 1] - ssq;
+        t = t2 > 0.0 ? sqrt(t2) : (t2 <= 0.0 ? 0.0 : t2); // a NaN stays NaN
+        tinv = 1.0 / t;
+        for (int i = tid; i <= j; i += kDcThreads) {
+            const double v = i < j ? HR(i, j - 1) + A[i] : t;
+            col[i] = v;
+            HR(i, j - 1) = v;
+        }
+        __syncthreads();
+    }
+    // the tentative column j: h_i = (b_i - sum_l H(i, l) a_l) / t, rows i < j, in l order
+    double hj = 0.0, gco = 0.0;
+    if (HASW) {
+        if (j == 0) {
+            gco = hj = tot[2 * j];
+        } else {
+            for (int i = tid; i < j; i += kDcThreads) {
+                double acc = B[i];
+                for (int l = i > 0 ? i - 1 : 0; l < j; ++l)
+                    acc = fma(-(l == j - 1 ? col[i] : HR(i, l)), A[l], acc);
+                hcol[i] = acc * tinv;
+            }
+            double ab = 0.0;
+            for (int l = 0; l < j; ++l) ab = fma(A[l], B[l], ab);
+            gco = (tot[2 * j] - ab) * tinv;
+            hj = (gco - t * A[j - 1]) * tinv;
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && j >= 1) { // iteration j: the Givens step on the completed column j - 1
+        auto C = [&](int i) -> double& { return col[i]; };
+        auto Sn = [&](int i) { return L.hsin[i]; };
+        auto Cs = [&](int i) { return L.hcos[i]; };
+        gm_givens_serial(L, j, j - 1, t, C, Sn, Cs, g);
+    }
+    __syncthreads();
+    if (j >= 1)
+        for (int i = tid; i <= j; i += kDcThreads) L.hh[(size_t)i * m + (j - 1)] = col[i];
+    if constexpr (HASW) {
+        if (g->stop) return;
+        for (int i = tid; i <= j; i += kDcThreads) HR(i, j) = i < j ? hcol[i] : hj;
+        for (int l = tid; l < j; l += kDcThreads) {
+            L.ca[l] = A[l];
+            L.cb[l] = B[l];
+        }
+        if (tid == 0) {
+            L.cs[0] = gco;
+            L.cs[1] = tinv;
+        }
+    }
+#undef HR
+}
+
+// ---- the update pass -----------------------------------------------------------------
+
+template <typename T>
+__global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayout L,
+                                                             const GmCtl* g)
+{
+    extern __shared__ __align__(16) unsigned char dc_raw[];
+    DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
+    __shared__ T ca[kDcMaxK], cb[kDcMaxK];
+    if (g->stop) return;
+    using S = DcShape<T>;
+    using VT = typename Vec16<T>::type;
+    const int j = P.j;
+    const int nItem = 2 + j;
+    const uint32_t tid = threadIdx.x;
+    for (int l = tid; l < j; l += kDcThreads) {
+        ca[l] = (T)L.ca[l];
+        cb[l] = (T)L.cb[l];
+    }
+    const T gco = (T)L.cs[0], tinv = (T)L.cs[1];
+    size_t e0, e1;
+    dc_range<T>(P.n, e0, e1);
+    __syncthreads();
+    T u[S::G][S::W], w[S::G][S::W], sa[S::G][S::W], sb[S::G][S::W];
+    T* qj = P.V + (size_t)j * P.ld;
+    T* un = P.V + (size_t)(j + 1) * P.ld;
+    auto src = [&](int v) -> const T* {
+        if (v == 0) return P.V + (size_t)j * P.ld;
+        if (v == 1) return P.w;
+        return P.V + (size_t)(v - 2) * P.ld;
+    };
+    dc_stream<T>(ring, e0, e1, nItem, src, [&](size_t k, const T* st, uint32_t len) {
+        const int v = (int)(k % nItem);
+        if (v == 0) {
+            dc_load<T>(st, len, u);
+#pragma unroll
+            for (int q = 0; q < S::G; ++q)
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) sa[q][e] = sb[q][e] = T(0);
+        } else if (v == 1) {
+            dc_load<T>(st, len, w);
+        } else {
+            const int l = v - 2;
+            T q[S::G][S::W];
+            dc_load<T>(st, len, q);
+            const T al = ca[l], bl = cb[l];
+#pragma unroll
+            for (int r = 0; r < S::G; ++r)
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) {
+                    sa[r][e] = fma(al, q[r][e], sa[r][e]);
+                    sb[r][e] = fma(bl, q[r][e], sb[r][e]);
+                }
+        }
+        if (v == nItem - 1) { // the chunk's last item: q_j and u_{j+1}
+            const size_t base = e0 + (k / nItem) * S::C;
+#pragma unroll
+            for (int r = 0; r < S::G; ++r) {
+                const uint32_t i0 = (uint32_t)(r * kDcThreads + tid) * S::W;
+                T qo[S::W], uo[S::W];
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) {
+                    qo[e] = j > 0 ? (u[r][e] - sa[r][e]) * tinv : u[r][e];
+                    const T x = fma(-qo[e], gco, w[r][e] - sb[r][e]);
+                    uo[e] = j > 0 ? x * tinv : x;
+                }
+                if (i0 + S::W <= len) {
+                    if (j > 0) *(VT*)(qj + base + i0) = Vec16<T>::make(qo);
+                    *(VT*)(un + base + i0) = Vec16<T>::make(uo);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < S::W; ++e)
+                        if (i0 + e < len) {
+                            if (j > 0) qj[base + i0 + e] = qo[e];
+                            un[base + i0 + e] = uo[e];
+                        }
+                }
+            }
+        }
+    });
+}
+
+// ---- launchers -------------------------------------------------------------------------
+
+// The shared-memory opt-in above 48 KB, once per kernel and device.
+static void dc_optin(const void* kern)
+{
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.insert({kern, dev}).second)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(DcRing));
+}
+
+// Resident blocks (two per SM), at least 1024 elements a block, and no more blocks than the
+// reduction scratch holds partials of nv values for.
+static int dc_grid(const Ctx& c, const void* fn, uint32_t n, int nv)
+{
+    int g = resident_grid(c, fn, kDcThreads, sizeof(DcRing));
+    g = std::min(g, (int)std::max<uint32_t>(1u, (n + 1023) / 1024));
+    g = std::min(g, (kMaxRedValues * kMaxGrid) / std::max(nv, 1));
+    return std::max(g, 1);
+}
+
+template <typename T>
+int dc_dots(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L,
+            GmCtl* g)
+{
+    if (j > kDcMaxK) return kErrInputPar;
+    DcArgs<T> P{V, ld, w, n, j};
+    ++c.launches;
+    if (w) {
+        auto kern = k_dc_dots<T, true>;
+        dc_optin((const void*)kern);
+        kern<<<dc_grid(c, (const void*)kern, n, 2 * j + 2), kDcThreads, sizeof(DcRing),
+               c.stream>>>(P, c.red, L, g);
+    } else {
+        auto kern = k_dc_dots<T, false>;
+        dc_optin((const void*)kern);
+        kern<<<dc_grid(c, (const void*)kern, n, j + 1), kDcThreads, sizeof(DcRing),
+               c.stream>>>(P, c.red, L, g);
+    }
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
+int dc_update(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L,
+              const GmCtl* g)
+{
+    if (j > kDcMaxK) return kErrInputPar;
+    DcArgs<T> P{V, ld, w, n, j};
+    ++c.launches;
+    auto kern = k_dc_update<T>;
+    dc_optin((const void*)kern);
+    kern<<<dc_grid(c, (const void*)kern, n, 1), kDcThreads, sizeof(DcRing), c.stream>>>(P, L,
+                                                                                         g);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template int dc_dots<double>(Ctx&, uint32_t, int, double*, size_t, const double*,
+                             const GmLayout&, GmCtl*);
+template int dc_dots<float>(Ctx&, uint32_t, int, float*, size_t, const float*, const GmLayout&,
+                            GmCtl*);
+template int dc_update<double>(Ctx&, uint32_t, int, double*, size_t, const double*,
+                               const GmLayout&, const GmCtl*);
+template int dc_update<float>(Ctx&, uint32_t, int, float*, size_t, const float*,
+                              const GmLayout&, const GmCtl*);
+
+unsigned tile_timeouts_dcgs2() { return tile_timeouts(); }
+
+} // namespace fb

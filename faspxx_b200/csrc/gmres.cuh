@@ -1,0 +1,105 @@
+// gmres.cuh -- the device-side Hessenberg least-squares state of GMRES/FGMRES (GMRES.cxx:
+// 114-280, FGMRES.cxx:108-271) shared by the Gram-Schmidt variants: the rotated Hessenberg
+// hh, the Givens sines and cosines, the right-hand side var, and the Givens step that
+// completes one Hessenberg column.
+#pragma once
+
+#include "internal.h"
+#include "solver.h"
+
+namespace fb {
+
+struct GmLayout {
+    double *hh, *hcos, *hsin, *var, *h1, *h2, *out;
+    // delayed reorthogonalisation: the Hessenberg before rotation (column j - 1 final once
+    // step j has re-orthogonalised its vector, column j tentative), and the coefficients the
+    // update pass of step j reads: ca[0..j) and cb[0..j), then cs = {g, 1/t}
+    double *hraw, *ca, *cb, *cs;
+    size_t  m;
+};
+
+// Doubles of the layout for restart length m.
+inline size_t gm_layout_size(size_t m)
+{
+    return (m + 1) * m + (m + 1) + m + (m + 1) + 2 * (m + 1) + 4 + (m + 1) * m + 2 * (m + 1) + 4;
+}
+
+inline GmLayout gm_layout(double* gm, size_t m)
+{
+    GmLayout L;
+    L.m = m;
+    L.hh = gm;
+    L.hcos = L.hh + (m + 1) * m;
+    L.hsin = L.hcos + (m + 1);
+    L.var = L.hsin + m;
+    L.h1 = L.var + (m + 1);
+    L.h2 = L.h1 + (m + 1);
+    L.out = L.h2 + (m + 1);
+    L.hraw = L.out + 4;
+    L.ca = L.hraw + (m + 1) * m;
+    L.cb = L.ca + (m + 1);
+    L.cs = L.cb + (m + 1);
+    return L;
+}
+
+// Basis vectors a DCGS2 step handles: restart lengths up to this use it.
+constexpr int kDcMaxK = 48;
+
+// Hessenberg columns up to this length are staged in shared memory by the Givens kernel.
+constexpr int kGmShared = 512;
+
+// GMRES.cxx:168-209 after the Arnoldi step, on one thread: C(count) = t, then the previous
+// rotations applied to column c1 in order, the new rotation, the updated right-hand side and
+// the residual estimate |var[count]| (out[0]); out[1] = 0 when t is not > SMALL_DBL (the
+// reference leaves the restart cycle before rotating). With a control block g: numIter is
+// incremented (the top of the step, GMRES.cxx:162), the estimate recorded in the history,
+// and the in-cycle stop test of GMRES.cxx:205-209 applied. C(j) is the column entry j (a
+// reference), S(j) / K(j) the sine / cosine of rotation j.
+template <typename CF, typename SF, typename KF>
+__device__ __forceinline__ void gm_givens_serial(const GmLayout& L, int count, int c1, double t,
+                                                 CF C, SF S, KF K, GmCtl* g)
+{
+    C(count) = t;
+    if (g) {
+        g->numIter += 1;
+        g->count = count;
+    }
+    if (!(fabs(t) > kSmallDbl)) {
+        L.out[1] = 0.0;
+        if (g) g->stop = 1;
+        return;
+    }
+    L.out[1] = 1.0;
+    for (int j = 1; j < count; ++j) {
+        t = C(j - 1);
+        C(j - 1) = S(j - 1) * C(j) + K(j - 1) * t;
+        C(j) = -S(j - 1) * t + K(j - 1) * C(j);
+    }
+    t = C(count) * C(count);
+    t += C(c1) * C(c1);
+    t = sqrt(t);
+    const double gamma = t > kSmallDbl ? t : kSmallDbl;
+    L.hcos[c1] = C(c1) / gamma;
+    L.hsin[c1] = C(count) / gamma;
+    C(c1) = L.hsin[c1] * C(count) + L.hcos[c1] * C(c1);
+    L.var[count] = -L.hsin[c1] * L.var[c1];
+    L.var[c1] = L.hcos[c1] * L.var[c1];
+    L.out[0] = fabs(L.var[count]);
+    if (g) {
+        const double resAbs = L.out[0];
+        g->resAbs = resAbs;
+        const unsigned k = g->numIter + g->histOffset;
+        if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;
+        if ((resAbs < g->absTol || resAbs / g->denAbs < g->relTol) && g->numIter > g->minIter)
+            g->stop = 2;
+    }
+}
+
+template <typename T>
+int dc_dots(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L, GmCtl* g);
+template <typename T>
+int dc_update(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L,
+              const GmCtl* g);
+unsigned tile_timeouts_dcgs2();
+
+} // namespace fb

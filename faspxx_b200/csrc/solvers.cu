@@ -12,6 +12,7 @@
 
 #include <new>
 
+#include "gmres.cuh"
 #include "solver.h"
 
 namespace fb {
@@ -507,8 +508,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                     cudaMemset(Z, 0, vb);
                 }
             }
-            const size_t m = maxRestart;
-            const size_t gmSize = (m + 1) * m + (m + 1) + m + (m + 1) + 2 * (m + 1) + 4;
+            const size_t gmSize = gm_layout_size(maxRestart);
             if (cudaMalloc(&gm, gmSize * 8) != cudaSuccess) return kErrAlloc;
             cudaMemset(gm, 0, gmSize * 8);
             if (cudaMalloc(&gmc, sizeof(GmCtl)) != cudaSuccess ||
@@ -1452,30 +1452,8 @@ int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info*
 
 // ---- GMRES / FGMRES: the Hessenberg least-squares stays in FP64 on the device -----------
 
-struct GmLayout {
-    double *hh, *hcos, *hsin, *var, *h1, *h2, *out;
-    size_t  m;
-};
-
-static GmLayout gm_layout(double* gm, size_t m)
-{
-    GmLayout L;
-    L.m = m;
-    L.hh = gm;
-    L.hcos = L.hh + (m + 1) * m;
-    L.hsin = L.hcos + (m + 1);
-    L.var = L.hsin + m;
-    L.h1 = L.var + (m + 1);
-    L.h2 = L.h1 + (m + 1);
-    L.out = L.h2 + (m + 1);
-    return L;
-}
-
-// GMRES.cxx:168-203 after the dots: hh[j][c1] (CGS2: h1+h2), t = ||w||, then the previous
-// rotations, the new rotation and the updated residual estimate |var[count]|. out[1] = 0
-// when t is not > SMALL_DBL (the reference leaves the restart cycle before rotating).
-constexpr int kGmShared = 512; // Hessenberg columns up to this length are staged in shared memory
-
+// GMRES.cxx:168-203 after the dots: hh[j][c1] (CGS2: h1+h2), t = ||w||, then the Givens
+// step of gm_givens_serial on a shared-memory copy of the column.
 __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int c1, int cgs,
                                                       const double* tnorm, GmCtl* g)
 {
@@ -1500,42 +1478,7 @@ __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int
         auto C = [&](int j) -> double& { return sh ? col[j] : HH(j, c1); };
         auto S = [&](int j) { return sh ? sn[j] : L.hsin[j]; };
         auto K = [&](int j) { return sh ? cs[j] : L.hcos[j]; };
-        double t = *tnorm;
-        C(count) = t;
-        if (g) { // ++numIter at the top of the step (GMRES.cxx:162)
-            g->numIter += 1;
-            g->count = count;
-        }
-        if (!(fabs(t) > kSmallDbl)) {
-            L.out[1] = 0.0;
-            if (g) g->stop = 1;
-        } else {
-            L.out[1] = 1.0;
-            for (int j = 1; j < count; ++j) {
-                t = C(j - 1);
-                C(j - 1) = S(j - 1) * C(j) + K(j - 1) * t;
-                C(j) = -S(j - 1) * t + K(j - 1) * C(j);
-            }
-            t = C(count) * C(count);
-            t += C(c1) * C(c1);
-            t = sqrt(t);
-            const double gamma = t > kSmallDbl ? t : kSmallDbl;
-            L.hcos[c1] = C(c1) / gamma;
-            L.hsin[c1] = C(count) / gamma;
-            C(c1) = L.hsin[c1] * C(count) + L.hcos[c1] * C(c1);
-            L.var[count] = -L.hsin[c1] * L.var[c1];
-            L.var[c1] = L.hcos[c1] * L.var[c1];
-            L.out[0] = fabs(L.var[count]);
-            if (g) { // GMRES.cxx:205-209: the estimate, its record and the in-cycle stop test
-                const double resAbs = L.out[0];
-                g->resAbs = resAbs;
-                const unsigned k = g->numIter + g->histOffset;
-                if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;
-                if ((resAbs < g->absTol || resAbs / g->denAbs < g->relTol) &&
-                    g->numIter > g->minIter)
-                    g->stop = 2;
-            }
-        }
+        gm_givens_serial(L, count, c1, *tnorm, C, S, K, g);
     }
     if (sh) {
         __syncthreads();
@@ -1778,7 +1721,7 @@ CSRView<float> gm_view<float>(const Mat& A) { return A.v32(); }
 template <typename T>
 static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t steps, bool left,
                            uint32_t& count, uint32_t& numIter, double& resAbs, double denAbs,
-                           const fasp_gpu_params& P, int& stopped, T* Z = nullptr,
+                           const fasp_gpu_params& P, int& stopped, T* wbuf, T* Z = nullptr,
                            T* tmp = nullptr)
 {
     Ctx& c = S.c;
@@ -1808,7 +1751,30 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
     const int mode = S.pcd.type == 0 ? 0 : (left ? 2 : 1);
     double* tn = c.dslot + SL_T5;
     const int needS = c.grid((long long)n * S.A->lanes, kBlock);
-    for (uint32_t k = 1; k <= steps; ++k) {
+    // DCGS2 (dcgs2.cu): step j applies A M to the candidate u_j in slot j, then one dots
+    // pass completes iteration j (Hessenberg column j - 1) and one update pass writes q_j and
+    // the next candidate; a dots pass without a product closes the cycle
+    const bool dc = S.cfg.orth == FASP_GPU_ORTH_DCGS2 && !Z && wbuf && S.maxRestart <= kDcMaxK;
+    for (uint32_t k = 1; dc && k <= steps; ++k) {
+        const uint32_t j = k - 1;
+        const T* u = V + j * ld;
+        if (mode == 0)
+            gm_apply_launch<T, 0>(c, *S.A, AV, u, dinv, wbuf, stop);
+        else if (mode == 1)
+            gm_apply_launch<T, 1>(c, *S.A, AV, u, dinv, wbuf, stop);
+        else
+            gm_apply_launch<T, 2>(c, *S.A, AV, u, dinv, wbuf, stop);
+        ++c.launches;
+        int e;
+        if ((e = dc_dots<T>(c, n, (int)j, V, ld, wbuf, L, S.gmc)) ||
+            (e = dc_update<T>(c, n, (int)j, V, ld, wbuf, L, S.gmc)))
+            return e;
+    }
+    if (dc) {
+        int e;
+        if ((e = dc_dots<T>(c, n, (int)steps, V, ld, (const T*)nullptr, L, S.gmc))) return e;
+    }
+    for (uint32_t k = 1; !dc && k <= steps; ++k) {
         const T* vin = V + (k - 1) * ld;
         T* vnew = V + k * ld;
         if (Z) { // FGMRES: Z_{k-1} = P(V_{k-1}) from its warm start, then A Z_{k-1}
@@ -1929,7 +1895,7 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
             const uint32_t steps = std::min<uint32_t>(restart, P.maxIter - numIter);
             int stopped = 0;
             if ((e = gm_cycle_device<T>(*this, L, V, steps, false, count, numIter, resAbs, denAbs,
-                                        P, stopped, flexible ? Z : nullptr, tmp)))
+                                        P, stopped, wk, flexible ? Z : nullptr, tmp)))
                 return e;
             count_1 = count - 1;
             if (!(stopped == 1 && count == 1)) { // a breakdown step updates nothing
@@ -2049,7 +2015,7 @@ int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu
             const uint32_t steps = std::min<uint32_t>(restart, P.maxIter - numIter);
             int stopped = 0;
             if ((e = gm_cycle_device<T>(*this, L, V, steps, true, count, numIter, resAbs, denAbs,
-                                        P, stopped)))
+                                        P, stopped, wk)))
                 return e;
             count_1 = count - 1;
             if (!(stopped == 1 && count == 1)) {
@@ -2482,6 +2448,6 @@ int SolverImpl::solve(const double* b, double* x, fasp_gpu_info* info)
     return e;
 }
 
-unsigned tile_timeouts_solvers() { return tile_timeouts(); }
+unsigned tile_timeouts_solvers() { return tile_timeouts() + tile_timeouts_dcgs2(); }
 
 } // namespace fb

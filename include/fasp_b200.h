@@ -62,7 +62,11 @@ enum fasp_gpu_precision {
 /* Gram-Schmidt variant of the GMRES/FGMRES Arnoldi step. */
 enum fasp_gpu_orth {
     FASP_GPU_ORTH_CGS2 = 0, /* classical GS + one reorthogonalisation, fused multi-dot/AXPY */
-    FASP_GPU_ORTH_MGS = 1   /* modified GS, the reference's op sequence (GMRES.cxx:169-172) */
+    FASP_GPU_ORTH_MGS = 1,  /* modified GS, the reference's op sequence (GMRES.cxx:169-172) */
+    FASP_GPU_ORTH_DCGS2 = 2 /* CGS2 with the re-orthogonalisation delayed into the next step:
+                               two passes over the basis per step; GMRES restart cycles run on
+                               the device (Identity or one Jacobi sweep) with a restart length
+                               up to 48, else as CGS2 */
 };
 
 /* SOLParams (src/Param.hxx:57-80) without the name and verbosity fields. */

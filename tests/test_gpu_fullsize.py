@@ -142,14 +142,18 @@ def test_fullsize_solver_parity(gpu, name):
     check_history(name, h)
 
 
+@pytest.mark.parametrize("orth", ["cgs2", "dcgs2"])
 @pytest.mark.parametrize("name", [n for n in SOLVER_CASES if FULL[n]["alg"] in ("gmres",
                                                                                  "fgmres")])
-def test_fullsize_gmres_cgs2(gpu, name):
-    """The default classical Gram-Schmidt with reorthogonalisation meets the same code,
-    iteration, solution and history bars as the reference's modified Gram-Schmidt."""
+def test_fullsize_gmres_cgs2(gpu, name, orth):
+    """Classical Gram-Schmidt with reorthogonalisation, in three passes per step (CGS2) or
+    with the reorthogonalisation delayed into the next step (DCGS2; FGMRES keeps CGS2),
+    meets the same code, iteration, solution and history bars as the reference's modified
+    Gram-Schmidt."""
     capi, sol = gpu
     meta = FULL[name]
-    code, it, x, h = run_case(capi, sol, name)
+    code, it, x, h = run_case(capi, sol, name,
+                              orth=capi.ORTH_DCGS2 if orth == "dcgs2" else capi.ORTH_CGS2)
     assert code == meta["code"]
     assert abs(it - meta["iters"]) <= iter_window(name), (name, it, meta["iters"])
     check_solution(name, x)

@@ -187,11 +187,13 @@ def test_invalid_csr_is_rejected_before_upload(gpu):
     assert e.value.code == -17
 
 
-def _check_case(gpu, oracle, name, engine="graph"):
+def _check_case(gpu, oracle, name, engine="graph", orth=None):
     case = CASES[name]
     A, b, x0 = G.case_inputs(case)
     M = gpu.MAT(A)
     s = gpu.configure(case["alg"], **case["kw"])
+    if orth is not None:
+        s.SetOrth(orth)
     s.SetPersistent(engine == "persistent")
     s.SetUseGraph(engine in ("graph", "graph_serial"))
     s.SetOverlapLaunch(engine != "graph_serial")
@@ -254,6 +256,17 @@ def test_cg_engines_match(gpu, oracle, name, engine):
     overlapped launches (the default, exercised by test_solver_parity), as graphs with
     ordinary launches, as one persistent cooperative kernel, and as plain launches."""
     _check_case(gpu, oracle, name, engine=engine)
+
+
+@pytest.mark.parametrize("name", sorted(n for n in CASES if CASES[n]["alg"] in ("gmres",
+                                                                                  "fgmres")))
+def test_gmres_dcgs2_parity(gpu, oracle, name):
+    """GMRES with the reorthogonalisation delayed into the next Arnoldi step (DCGS2) meets
+    the bars of the default CGS2 against the reference's modified Gram-Schmidt: code,
+    iteration count, solution and the residual history within the reference's own one-ulp
+    envelope (configurations outside the device cycles, and FGMRES, run CGS2)."""
+    from faspxx_b200 import capi
+    _check_case(gpu, oracle, name, orth=capi.ORTH_DCGS2)
 
 
 def test_known_answer_jacobi(gpu):
