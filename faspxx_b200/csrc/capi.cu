@@ -199,7 +199,7 @@ void fasp_gpu_default_config(fasp_gpu_config* cfg, int alg)
     cfg->mgSmoothPrm = d;
     cfg->mgCoarsePrm = d;
     cfg->precision = FASP_GPU_FP64;
-    cfg->orth = FASP_GPU_ORTH_CGS2;
+    cfg->orth = FASP_GPU_ORTH_DCGS2;
     cfg->innerRelTol = 1e-4;
     cfg->innerMaxIter = 0;
     cfg->maxOuter = 50;

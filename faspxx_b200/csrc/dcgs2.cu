@@ -42,6 +42,7 @@ constexpr int      kDcStages = 6;
 constexpr int      kDcThreads = 256;
 constexpr int      kDcWarps = kDcThreads / 32;
 constexpr int      kDcMaxNV = 2 * kDcMaxK + 2; // values of one dots pass
+constexpr int      kDcMaxGrid = 384;            // blocks of a pass (a multiple of 32)
 
 template <typename T>
 struct DcShape {
@@ -87,61 +88,88 @@ __device__ __forceinline__ void bulk_copy_g2s_plain(void* dst, const void* src, 
                  : "memory");
 }
 
-// Streams items k = 0 .. total-1 (chunk k / nItem, vector k % nItem of src(v)) through the
-// ring; consume(k, stage, len) runs on every thread once the item's bytes have landed, the
-// block synchronises after each item and thread 0 then refills that stage. The copies start
-// on 16-byte boundaries (the range starts are) and round their length up to 16 bytes: at
-// most 8 bytes past the last element, inside every vector's allocation. False when a wait
-// ran out: the block has then drained its copies in flight (bounded) and stopped.
-template <typename T, typename Src, typename Consume>
+// Streams the items of the block's range through the ring: chunk after chunk, vectors
+// v = 0 .. nItem-1 of src(v) per chunk. consume(v, base, stage, len) runs on every thread
+// once the item's bytes have landed (base: the chunk's first element), the block
+// synchronises after each item and thread 0 then refills that stage. ready() runs on every
+// thread once the first copies are in flight, before the first item (a kernel that may start
+// before its predecessor has finished waits for it there). Items are walked with
+// counters (no division: a 64-bit division by nItem per item had made the passes
+// instruction-bound). The copies start on 16-byte boundaries (the range starts are) and
+// round their length up to 16 bytes: at most 8 bytes past the last element, inside every
+// vector's allocation. False when a wait ran out: the block has then drained its copies in
+// flight (bounded) and stopped.
+template <typename T, typename Src, typename Consume, typename Ready>
 __device__ __forceinline__ bool dc_stream(DcRing& ring, size_t e0, size_t e1, int nItem, Src src,
-                                          Consume consume)
+                                          Consume consume, Ready ready)
 {
     constexpr uint32_t C = DcShape<T>::C;
     const uint32_t tid = threadIdx.x;
-    const size_t nc = (e1 - e0 + C - 1) / C;
-    const size_t total = nc * (size_t)nItem;
-    auto issue = [&](size_t k) {
-        const int s = (int)(k % kDcStages);
-        const size_t base = e0 + (k / nItem) * C;
-        const size_t len = std::min((size_t)C, e1 - base);
-        const uint32_t bytes = (uint32_t)((len * sizeof(T) + 15) & ~size_t(15));
+    const uint32_t total = (uint32_t)((e1 - e0 + C - 1) / C) * (uint32_t)nItem;
+    // the issuing thread's position: the next item to copy
+    int iv = 0, is = 0;
+    size_t ib = e0;
+    auto issue = [&]() {
+        const uint32_t len = (uint32_t)std::min((size_t)C, e1 - ib);
+        const uint32_t bytes = (len * (uint32_t)sizeof(T) + 15u) & ~15u;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                         smem_addr(&ring.full[s])),
+                         smem_addr(&ring.full[is])),
                      "r"(bytes)
                      : "memory");
-        bulk_copy_g2s_plain(ring.st[s], src((int)(k % nItem)) + base, bytes, &ring.full[s]);
+        bulk_copy_g2s_plain(ring.st[is], src(iv) + ib, bytes, &ring.full[is]);
+        if (++is == kDcStages) is = 0;
+        if (++iv == nItem) {
+            iv = 0;
+            ib += C;
+        }
     };
     if (tid == 0) {
         ring.bad = 0;
-        for (int s = 0; s < kDcStages; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring.full[s]))
+        for (int q = 0; q < kDcStages; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring.full[q]))
                          : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (size_t k = 0; k < (size_t)kDcStages && k < total; ++k) issue(k);
+        for (uint32_t k = 0; k < (uint32_t)kDcStages && k < total; ++k) issue();
+    }
+    // every thread: false leaves before the first item (the block drains its first copies)
+    if (!ready()) {
+        if (tid == 0)
+            for (uint32_t q = 0; q < (uint32_t)kDcStages && q < total; ++q)
+                mbar_wait_bounded(&ring.full[q], 0u);
+        return false;
     }
     __syncthreads();
-    for (size_t k = 0; k < total; ++k) {
-        const int s = (int)(k % kDcStages);
+    int v = 0, st = 0;
+    uint32_t ph = 0;
+    size_t base = e0;
+    for (uint32_t k = 0; k < total; ++k) {
         // the consumers hold warp-collective sums: a warp consumes only if all its lanes saw
         // the bytes land
-        const bool mine = mbar_wait_bounded(&ring.full[s], (uint32_t)((k / kDcStages) & 1));
+        const bool mine = mbar_wait_bounded(&ring.full[st], ph);
         const bool landed = __all_sync(0xffffffffu, mine);
         if (!landed) {
             if (!mine) atomicAdd(&fb_tile_timeouts, 1u);
             ring.bad = 1;
         }
-        const size_t base = e0 + (k / nItem) * C;
-        if (landed) consume(k, (const T*)ring.st[s], (uint32_t)std::min((size_t)C, e1 - base));
-        __syncthreads(); // stage s is free again
+        if (landed)
+            consume(v, base, (const T*)ring.st[st], (uint32_t)std::min((size_t)C, e1 - base));
+        __syncthreads(); // stage st is free again
         if (ring.bad) {
-            if (tid == 0)
-                for (size_t i = k; i < k + kDcStages && i < total; ++i)
-                    mbar_wait_bounded(&ring.full[i % kDcStages], (uint32_t)((i / kDcStages) & 1));
+            if (tid == 0) // the copies still in flight: items k .. k + stages - 1
+                for (uint32_t i = 0, q = st, p = ph; i < (uint32_t)kDcStages && k + i < total;
+                     ++i) {
+                    mbar_wait_bounded(&ring.full[q], p);
+                    if (++q == (uint32_t)kDcStages) q = 0, p ^= 1u;
+                }
             return false;
         }
-        if (tid == 0 && k + kDcStages < total) issue(k + kDcStages);
+        if (tid == 0 && k + kDcStages < total) issue();
+        if (++st == kDcStages) st = 0, ph ^= 1u;
+        if (++v == nItem) {
+            v = 0;
+            base += C;
+        }
     }
     return true;
 }
@@ -178,6 +206,36 @@ __device__ __forceinline__ T dc_dot(const T (&x)[DcShape<T>::G][DcShape<T>::W],
     return s;
 }
 
+// Warp sums of 16 values at once (a butterfly reduce-scatter): each level halves the values
+// a lane holds and exchanges the other half with its partner, 8 + 4 + 2 + 1 + 1 shuffles of
+// a double instead of 16 x 5. Returns value (lane >> 1) & 15 summed over the warp (lanes 2r
+// and 2r + 1 both hold value r). Every sum is a fixed tree over the lanes, the same on every
+// run (a + b and b + a are the same bits).
+__device__ __forceinline__ double warp_sum16(const double (&x)[16])
+{
+    const uint32_t lane = threadIdx.x & 31;
+    double y[8], z[4], t[2];
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const double send = b4 ? x[i] : x[i + 8];
+        y[i] = (b4 ? x[i + 8] : x[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const double send = b3 ? y[i] : y[i + 4];
+        z[i] = (b3 ? y[i + 4] : y[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const double send = b2 ? z[i] : z[i + 2];
+        t[i] = (b2 ? z[i + 2] : z[i]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    const double send = b1 ? t[0] : t[1];
+    const double u = (b1 ? t[1] : t[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
+    return u + __shfl_xor_sync(0xffffffffu, u, 1);
+}
+
 // ---- the dots pass and the step's scalar work ----------------------------------------
 
 // Value slots: a_l at l, then (with w) b_l at j + l, c at 2j, and d last.
@@ -191,6 +249,8 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     __shared__ double tot[kDcMaxNV];
     __shared__ double col[kDcMaxK + 2], hcol[kDcMaxK];
     __shared__ bool amLast;
+    // the update pass that follows may be scheduled as soon as blocks of this one leave
+    pdl_release();
     if (g->stop) return;
     using S = DcShape<T>;
     const int j = P.j;
@@ -202,6 +262,11 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     dc_range<T>(P.n, e0, e1);
     __syncthreads();
     T u[S::G][S::W], w[S::G][S::W];
+    // a thread's products with Q_l for the window of 8 basis vectors l0 .. l0 + 7 (slot
+    // l & 7), summed over the warp when the window is full or the chunk's basis ends
+    double wa[8], wb[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) wa[q] = wb[q] = 0.0;
     auto src = [&](int v) -> const T* {
         if (v == 0) return P.V + (size_t)j * P.ld;
         if (HASW && v == 1) return P.w;
@@ -211,8 +276,8 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
         x = warp_reduce(x, kSum);
         if (lane == 0) wacc[wid][slot] += x;
     };
-    const bool ok = dc_stream<T>(ring, e0, e1, nItem, src, [&](size_t k, const T* st, uint32_t len) {
-        const int v = (int)(k % nItem);
+    const bool ok = dc_stream<T>(ring, e0, e1, nItem, src,
+                                 [&](int v, size_t, const T* st, uint32_t len) {
         if (v == 0) {
             dc_load<T>(st, len, u);
             add(nv - 1, (double)dc_dot<T>(u, u));
@@ -223,10 +288,30 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
             const int l = v - 1 - (HASW ? 1 : 0);
             T q[S::G][S::W];
             dc_load<T>(st, len, q);
-            add(l, (double)dc_dot<T>(q, u));
-            if (HASW) add(j + l, (double)dc_dot<T>(q, w));
+            const double pa = (double)dc_dot<T>(q, u);
+            const double pb = HASW ? (double)dc_dot<T>(q, w) : 0.0;
+            const int r = l & 7;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (i == r) {
+                    wa[i] = pa;
+                    wb[i] = pb;
+                }
+            if (r == 7 || l == j - 1) { // the window's warp sums: slot l0 + i (a), j + l0 + i (b)
+                double x[16];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    x[i] = wa[i];
+                    x[i + 8] = wb[i];
+                    wa[i] = wb[i] = 0.0;
+                }
+                const double sum = warp_sum16(x);
+                const int r2 = (int)(lane >> 1) & 15, i = r2 & 7, l0 = l - r;
+                if (!(lane & 1) && l0 + i < j && (HASW || r2 < 8))
+                    wacc[wid][(r2 < 8 ? 0 : j) + l0 + i] += sum;
+            }
         }
-    });
+    }, [] { return true; });
     // a block that stopped early still takes its ticket, with NaN partials: the step then
     // sees t = NaN and breaks the cycle off (the reference's breakdown exit)
     __syncthreads();
@@ -240,16 +325,44 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     __syncthreads();
     if (!amLast) return;
     // totals: warp q adds value v = q, q + 8, ... over the blocks (lane l takes blocks l,
-    // l + 32, ... in order, then a shuffle tree)
-    for (int v = wid; v < nv; v += kDcWarps) {
-        double a = 0.0;
-        for (uint32_t b = lane; b < gridDim.x; b += 32)
-            a += __ldcg(&s.partials[(size_t)v * gridDim.x + b]);
-        a = warp_reduce(a, kSum);
-        if (lane == 0) tot[v] = a;
+    // l + 32, ... in order, then a shuffle tree); a lane's loads for a value are issued
+    // together, two values at a time
+    const uint32_t G = gridDim.x;
+    for (int v0 = wid; v0 < nv; v0 += 2 * kDcWarps) {
+        double x[2][kDcMaxGrid / 32];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int q = 0; q < kDcMaxGrid / 32; ++q) {
+                const int v = v0 + h * kDcWarps;
+                const uint32_t b = lane + 32u * q;
+                x[h][q] = v < nv && b < G ? __ldcg(&s.partials[(size_t)v * G + b]) : 0.0;
+            }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double a = 0.0;
+#pragma unroll
+            for (int q = 0; q < kDcMaxGrid / 32; ++q) a += x[h][q];
+            a = warp_reduce(a, kSum);
+            if (lane == 0 && v0 + h * kDcWarps < nv) tot[v0 + h * kDcWarps] = a;
+        }
+    }
+    // the finalize reads the Hessenberg columns 0 .. j-2 and the rotations from shared memory
+    // (the ring's stages are free now): loaded by all threads at once rather than one
+    // dependent global load at a time
+    double* Hs = reinterpret_cast<double*>(ring.st); // [j][j], row i from column i - 1
+    double* snS = Hs + (size_t)kDcMaxK * kDcMaxK;
+    double* csS = snS + kDcMaxK;
+    const size_t m = L.m;
+    for (int e = tid; e < j * j; e += kDcThreads) {
+        const int i = e / j, l = e - i * j;
+        if (l + 1 >= i && l < j - 1) Hs[e] = L.hraw[(size_t)i * m + l];
+    }
+    for (int i = tid; i < j; i += kDcThreads) {
+        snS[i] = L.hsin[i];
+        csS[i] = L.hcos[i];
     }
     __syncthreads();
-    const size_t m = L.m;
 #define HR(i, l) L.hraw[(size_t)(i) * m + (l)]
     const double* A = tot;     // a_l
     const double* B = tot + j; // b_l (with w)
@@ -277,7 +390,7 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
             for (int i = tid; i < j; i += kDcThreads) {
                 double acc = B[i];
                 for (int l = i > 0 ? i - 1 : 0; l < j; ++l)
-                    acc = fma(-(l == j - 1 ? col[i] : HR(i, l)), A[l], acc);
+                    acc = fma(-(l == j - 1 ? col[i] : Hs[i * j + l]), A[l], acc);
                 hcol[i] = acc * tinv;
             }
             double ab = 0.0;
@@ -289,8 +402,8 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     __syncthreads();
     if (tid == 0 && j >= 1) { // iteration j: the Givens step on the completed column j - 1
         auto C = [&](int i) -> double& { return col[i]; };
-        auto Sn = [&](int i) { return L.hsin[i]; };
-        auto Cs = [&](int i) { return L.hcos[i]; };
+        auto Sn = [&](int i) { return snS[i]; };
+        auto Cs = [&](int i) { return csS[i]; };
         gm_givens_serial(L, j, j - 1, t, C, Sn, Cs, g);
     }
     __syncthreads();
@@ -320,20 +433,28 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
     extern __shared__ __align__(16) unsigned char dc_raw[];
     DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
     __shared__ T ca[kDcMaxK], cb[kDcMaxK];
-    if (g->stop) return;
     using S = DcShape<T>;
     using VT = typename Vec16<T>::type;
     const int j = P.j;
     const int nItem = 2 + j;
     const uint32_t tid = threadIdx.x;
-    for (int l = tid; l < j; l += kDcThreads) {
-        ca[l] = (T)L.ca[l];
-        cb[l] = (T)L.cb[l];
-    }
-    const T gco = (T)L.cs[0], tinv = (T)L.cs[1];
+    T gco = T(0), tinv = T(1);
     size_t e0, e1;
     dc_range<T>(P.n, e0, e1);
-    __syncthreads();
+    // launched programmatically after the dots pass: the copies of u, w and the basis start
+    // at once (the dots pass writes none of them: only the Hessenberg state and the
+    // coefficients), and the coefficients are read once it has finished
+    auto ready = [&]() {
+        pdl_wait();
+        if (g->stop) return false;
+        for (int l = tid; l < j; l += kDcThreads) {
+            ca[l] = (T)L.ca[l];
+            cb[l] = (T)L.cb[l];
+        }
+        gco = (T)L.cs[0];
+        tinv = (T)L.cs[1];
+        return true;
+    };
     T u[S::G][S::W], w[S::G][S::W], sa[S::G][S::W], sb[S::G][S::W];
     T* qj = P.V + (size_t)j * P.ld;
     T* un = P.V + (size_t)(j + 1) * P.ld;
@@ -342,8 +463,7 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
         if (v == 1) return P.w;
         return P.V + (size_t)(v - 2) * P.ld;
     };
-    dc_stream<T>(ring, e0, e1, nItem, src, [&](size_t k, const T* st, uint32_t len) {
-        const int v = (int)(k % nItem);
+    dc_stream<T>(ring, e0, e1, nItem, src, [&](int v, size_t base, const T* st, uint32_t len) {
         if (v == 0) {
             dc_load<T>(st, len, u);
 #pragma unroll
@@ -366,7 +486,6 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
                 }
         }
         if (v == nItem - 1) { // the chunk's last item: q_j and u_{j+1}
-            const size_t base = e0 + (k / nItem) * S::C;
 #pragma unroll
             for (int r = 0; r < S::G; ++r) {
                 const uint32_t i0 = (uint32_t)(r * kDcThreads + tid) * S::W;
@@ -390,7 +509,7 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
                 }
             }
         }
-    });
+    }, ready);
 }
 
 // ---- launchers -------------------------------------------------------------------------
@@ -415,6 +534,7 @@ static int dc_grid(const Ctx& c, const void* fn, uint32_t n, int nv)
     int g = resident_grid(c, fn, kDcThreads, sizeof(DcRing));
     g = std::min(g, (int)std::max<uint32_t>(1u, (n + 1023) / 1024));
     g = std::min(g, (kMaxRedValues * kMaxGrid) / std::max(nv, 1));
+    g = std::min(g, kDcMaxGrid);
     return std::max(g, 1);
 }
 
@@ -449,8 +569,17 @@ int dc_update(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLa
     ++c.launches;
     auto kern = k_dc_update<T>;
     dc_optin((const void*)kern);
-    kern<<<dc_grid(c, (const void*)kern, n, 1), kDcThreads, sizeof(DcRing), c.stream>>>(P, L,
-                                                                                         g);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)dc_grid(c, (const void*)kern, n, 1));
+    cfg.blockDim = dim3(kDcThreads);
+    cfg.dynamicSmemBytes = sizeof(DcRing);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    FB_CUDA(cudaLaunchKernelEx(&cfg, kern, P, L, g));
     FB_CUDA(cudaGetLastError());
     return kOk;
 }

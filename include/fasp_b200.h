@@ -63,10 +63,11 @@ enum fasp_gpu_precision {
 enum fasp_gpu_orth {
     FASP_GPU_ORTH_CGS2 = 0, /* classical GS + one reorthogonalisation, fused multi-dot/AXPY */
     FASP_GPU_ORTH_MGS = 1,  /* modified GS, the reference's op sequence (GMRES.cxx:169-172) */
-    FASP_GPU_ORTH_DCGS2 = 2 /* CGS2 with the re-orthogonalisation delayed into the next step:
-                               two passes over the basis per step; GMRES restart cycles run on
-                               the device (Identity or one Jacobi sweep) with a restart length
-                               up to 48, else as CGS2 */
+    FASP_GPU_ORTH_DCGS2 = 2 /* the default of fasp_gpu_default_config: CGS2 with the
+                               re-orthogonalisation delayed into the next step, two passes over
+                               the basis per step; used by GMRES restart cycles on the device
+                               (Identity or one Jacobi sweep, restart length up to 48), the
+                               other configurations and FGMRES run CGS2 */
 };
 
 /* SOLParams (src/Param.hxx:57-80) without the name and verbosity fields. */
@@ -93,7 +94,7 @@ typedef struct {
     /* B200 options (no reference counterpart) */
     int             leftPrecond; /* GMRES::SetLeftPrecond (GMRES.cxx:28) */
     int             precision;   /* fasp_gpu_precision */
-    int             orth;        /* fasp_gpu_orth */
+    int             orth;        /* fasp_gpu_orth (default DCGS2) */
     double          innerRelTol; /* MIXED: relative tolerance of each FP32 inner solve;
                                     MIXED_RELIABLE: an FP64 update each time the FP32
                                     residual has fallen by this factor (0 or >= 1: 1e-2

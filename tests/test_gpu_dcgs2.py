@@ -140,4 +140,6 @@ def test_dcgs2_mixed_precision(gpu, pe):
     assert c1 == 0 and c2 == 0
     assert np.linalg.norm(b - A.matvec(x1)) <= 1e-8 * np.linalg.norm(b)
     assert abs(i1 - i2) <= max(3, 0.05 * i2), (i1, i2)
-    assert np.max(np.abs(x1 - xs)) <= 1e-6 * np.max(np.abs(xs))
+    # relTol 1e-8 bounds the residual, not the error: the error against x* is CGS2's
+    e1, e2 = np.max(np.abs(x1 - xs)), np.max(np.abs(x2 - xs))
+    assert e1 <= 2.0 * e2 + 1e-9 * np.max(np.abs(xs)), (e1, e2)
