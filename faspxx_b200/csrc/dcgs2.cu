@@ -247,7 +247,8 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
     __shared__ double wacc[kDcWarps][kDcMaxNV];
     __shared__ double tot[kDcMaxNV];
-    __shared__ double col[kDcMaxK + 2], hcol[kDcMaxK];
+    __shared__ double col[kDcMaxK + 2], hcol[kDcMaxK], var[2];
+    __shared__ GmCtl gs;
     __shared__ bool amLast;
     // the update pass that follows may be scheduled as soon as blocks of this one leave
     pdl_release();
@@ -362,6 +363,11 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
         snS[i] = L.hsin[i];
         csS[i] = L.hcos[i];
     }
+    if (tid == 32) gs = *g;
+    if (tid == 64 && j >= 1) {
+        var[0] = L.var[j - 1];
+        var[1] = L.var[j];
+    }
     __syncthreads();
 #define HR(i, l) L.hraw[(size_t)(i) * m + (l)]
     const double* A = tot;     // a_l
@@ -404,13 +410,17 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
         auto C = [&](int i) -> double& { return col[i]; };
         auto Sn = [&](int i) { return snS[i]; };
         auto Cs = [&](int i) { return csS[i]; };
-        gm_givens_serial(L, j, j - 1, t, C, Sn, Cs, g);
+        auto Var = [&](int i) -> double& { return var[i == j - 1 ? 0 : 1]; };
+        gm_givens_serial(L, j, j - 1, t, C, Sn, Cs, Var, &gs);
+        L.var[j - 1] = var[0];
+        L.var[j] = var[1];
+        *g = gs;
     }
     __syncthreads();
     if (j >= 1)
         for (int i = tid; i <= j; i += kDcThreads) L.hh[(size_t)i * m + (j - 1)] = col[i];
     if constexpr (HASW) {
-        if (g->stop) return;
+        if (gs.stop) return;
         for (int i = tid; i <= j; i += kDcThreads) HR(i, j) = i < j ? hcol[i] : hj;
         for (int l = tid; l < j; l += kDcThreads) {
             L.ca[l] = A[l];

@@ -53,11 +53,13 @@ constexpr int kGmShared = 512;
 // the residual estimate |var[count]| (out[0]); out[1] = 0 when t is not > SMALL_DBL (the
 // reference leaves the restart cycle before rotating). With a control block g: numIter is
 // incremented (the top of the step, GMRES.cxx:162), the estimate recorded in the history,
-// and the in-cycle stop test of GMRES.cxx:205-209 applied. C(j) is the column entry j (a
-// reference), S(j) / K(j) the sine / cosine of rotation j.
-template <typename CF, typename SF, typename KF>
+// and the in-cycle stop test of GMRES.cxx:205-209 applied. C(j) is the column entry j, S(j)
+// / K(j) the sine / cosine of rotation j and Var(j) entry j of the right-hand side, each a
+// reference into shared memory in the callers, as is g: one thread's chain of dependent
+// global loads and stores (about 10 L2 round trips) had cost several microseconds a step.
+template <typename CF, typename SF, typename KF, typename VF>
 __device__ __forceinline__ void gm_givens_serial(const GmLayout& L, int count, int c1, double t,
-                                                 CF C, SF S, KF K, GmCtl* g)
+                                                 CF C, SF S, KF K, VF Var, GmCtl* g)
 {
     C(count) = t;
     if (g) {
@@ -79,14 +81,15 @@ __device__ __forceinline__ void gm_givens_serial(const GmLayout& L, int count, i
     t += C(c1) * C(c1);
     t = sqrt(t);
     const double gamma = t > kSmallDbl ? t : kSmallDbl;
-    L.hcos[c1] = C(c1) / gamma;
-    L.hsin[c1] = C(count) / gamma;
-    C(c1) = L.hsin[c1] * C(count) + L.hcos[c1] * C(c1);
-    L.var[count] = -L.hsin[c1] * L.var[c1];
-    L.var[c1] = L.hcos[c1] * L.var[c1];
-    L.out[0] = fabs(L.var[count]);
+    const double cs = C(c1) / gamma, sn = C(count) / gamma;
+    L.hcos[c1] = cs;
+    L.hsin[c1] = sn;
+    C(c1) = sn * C(count) + cs * C(c1);
+    Var(count) = -sn * Var(c1);
+    Var(c1) = cs * Var(c1);
+    const double resAbs = fabs(Var(count));
+    L.out[0] = resAbs;
     if (g) {
-        const double resAbs = L.out[0];
         g->resAbs = resAbs;
         const unsigned k = g->numIter + g->histOffset;
         if (g->hist && k < g->histCap) g->hist[k] = resAbs * g->histScale;

@@ -1460,9 +1460,11 @@ __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int
     if (g && g->stop) return;
     const size_t m = L.m;
 #define HH(i, j) L.hh[(size_t)(i) * m + (j)]
-    // the column c1 and the previous rotations, loaded by all threads; one thread then runs
-    // the reference's serial sequence on shared memory, with the same operations and order
-    __shared__ double col[kGmShared + 1], sn[kGmShared], cs[kGmShared];
+    // the column c1, the previous rotations, var[c1] and the control block, loaded by all
+    // threads at once; one thread then runs the reference's serial sequence on shared
+    // memory, with the same operations and order
+    __shared__ double col[kGmShared + 1], sn[kGmShared], cs[kGmShared], var[2];
+    __shared__ GmCtl gs;
     const bool sh = count <= kGmShared;
     if (sh) {
         for (int j = threadIdx.x; j < count; j += blockDim.x) {
@@ -1470,15 +1472,22 @@ __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int
             sn[j] = L.hsin[j];
             cs[j] = L.hcos[j];
         }
-        __syncthreads();
     }
+    if (threadIdx.x == 32) var[0] = L.var[c1];
+    if (threadIdx.x == 64 && g) gs = *g;
+    __syncthreads();
     if (threadIdx.x == 0) {
         if (!sh && cgs)
             for (int j = 0; j < count; ++j) HH(j, c1) = L.h1[j] + L.h2[j];
         auto C = [&](int j) -> double& { return sh ? col[j] : HH(j, c1); };
         auto S = [&](int j) { return sh ? sn[j] : L.hsin[j]; };
         auto K = [&](int j) { return sh ? cs[j] : L.hcos[j]; };
-        gm_givens_serial(L, count, c1, *tnorm, C, S, K, g);
+        auto Var = [&](int j) -> double& { return var[j == c1 ? 0 : 1]; };
+        var[1] = L.var[count];
+        gm_givens_serial(L, count, c1, *tnorm, C, S, K, Var, g ? &gs : nullptr);
+        L.var[c1] = var[0];
+        L.var[count] = var[1];
+        if (g) *g = gs;
     }
     if (sh) {
         __syncthreads();
@@ -1488,10 +1497,38 @@ __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int
 }
 
 // GMRES.cxx:213-219 (signed loop): back substitution into var[0..count)
-__global__ void k_gmres_backsolve(GmLayout L, int count, int c1)
+// Restart lengths up to 64 stage the triangle and var in shared memory (loaded by all
+// threads at once) before thread 0 runs the same serial sequence: one thread's dependent
+// global loads had cost about 40 us per cycle.
+constexpr int kGmBack = 64;
+
+__global__ void __launch_bounds__(128) k_gmres_backsolve(GmLayout L, int count, int c1)
 {
     const size_t m = L.m;
 #define HH(i, j) L.hh[(size_t)(i) * m + (j)]
+    __shared__ double hs[kGmBack * kGmBack], vs[kGmBack];
+    if (count < 1) return; // every cycle makes at least one step
+    if (count <= kGmBack) {
+        for (int e = threadIdx.x; e < count * count; e += blockDim.x) {
+            const int i = e / count, j = e - i * count;
+            if (j >= i) hs[e] = HH(i, j);
+        }
+        for (int i = threadIdx.x; i < count; i += blockDim.x) vs[i] = L.var[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            vs[c1] = vs[c1] / hs[c1 * count + c1];
+            for (int k = count - 2; k >= 0; --k) {
+                double t = 0.0;
+                for (int j = k + 1; j < count; ++j) t -= hs[k * count + j] * vs[j];
+                t += vs[k];
+                vs[k] = t / hs[k * count + k];
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < count; i += blockDim.x) L.var[i] = vs[i];
+        return;
+    }
+    if (threadIdx.x != 0) return;
     L.var[c1] = L.var[c1] / HH(c1, c1);
     for (int k = count - 2; k >= 0; --k) {
         double t = 0.0;
@@ -1929,7 +1966,7 @@ int SolverImpl::gmres_right(const T* b, T* x, fasp_gpu_info* info, const fasp_gp
 
         ++c.launches;
 
-        k_gmres_backsolve<<<1, 1, 0, c.stream>>>(L, (int)count, (int)count_1);
+        k_gmres_backsolve<<<1, 128, 0, c.stream>>>(L, (int)count, (int)count_1);
         v_set(c, n, 0.0, wk);
         v_multiaxpy(c, n, (int)count, flexible ? Z : V, ld, L.var, -1.0, wk, nullptr);
         if (flexible) {
@@ -2043,7 +2080,7 @@ int SolverImpl::gmres_left(const T* b, T* x, fasp_gpu_info* info, const fasp_gpu
 
         ++c.launches;
 
-        k_gmres_backsolve<<<1, 1, 0, c.stream>>>(L, (int)count, (int)count_1);
+        k_gmres_backsolve<<<1, 128, 0, c.stream>>>(L, (int)count, (int)count_1);
         v_set(c, n, 0.0, wk);
         v_multiaxpy(c, n, (int)count, V, ld, L.var, -1.0, wk, nullptr);
         v_axpy(c, n, Scal::h(1.0), wk, x);
