@@ -19,11 +19,11 @@
 // Iteration i of the reference (Hessenberg column i - 1) completes in the dots pass of
 // step i; a restart cycle of s iterations ends with a dots pass without a product.
 //
-// Both passes stream 16 KB chunks of each vector through a ring of shared-memory stages
+// Both passes stream 12 KB chunks of each vector through a ring of shared-memory stages
 // with bulk asynchronous copies (cp.async.bulk, completion counted in bytes on an
 // mbarrier), issued by one thread six stages ahead of the consuming threads; block b takes
 // the contiguous element range b of the grid, chunk by chunk, and per chunk the vectors in
-// a fixed order (u, w, then Q). Sums are fixed-order: a thread adds its 8 (FP64) or 16
+// a fixed order (u, w, then Q). Sums are fixed-order: a thread adds its 6 (FP64) or 12
 // (FP32) elements of an item, the warp a shuffle tree, each warp its items in chunk order,
 // the block its warps in order and the last block the blocks in order -- reruns give the
 // same bits.
@@ -37,7 +37,10 @@
 
 namespace fb {
 
-constexpr uint32_t kDcStageBytes = 16384;
+// 12 KB stages, six per block, two blocks per SM: of rings of 4-12 stages of 4-20 KB, with
+// two or three blocks per SM, this one ran the 96^3 GMRES(30) profile fastest (5.05 ms for
+// 60 steps; 6 x 16 KB 5.47, 8 x 12 KB 5.08, 12 x 8 KB 5.6, three blocks per SM 6.3-8.0)
+constexpr uint32_t kDcStageBytes = 12288;
 constexpr int      kDcStages = 6;
 constexpr int      kDcThreads = 256;
 constexpr int      kDcWarps = kDcThreads / 32;

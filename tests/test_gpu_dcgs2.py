@@ -6,7 +6,7 @@ CGS2's results on the same inputs, and to the true residual:
 
 * same return code; iteration count within one of CGS2's; solutions agree to 1e-6 of
   max|x| at relTol 1e-8; the true residual meets the tolerance (x checked in numpy);
-* the streamed passes cut vectors into 16 KB chunks over contiguous block ranges: sizes
+* the streamed passes cut vectors into 12 KB chunks over contiguous block ranges: sizes
   from 1 to a few chunks per block, odd (FP64) and non-multiple-of-4 (FP32) lengths;
 * reruns give identical bits; a restart length above 48 runs as CGS2 (bit-identical to it);
 * maxIter inside a restart cycle, variable restart, left preconditioning, no
