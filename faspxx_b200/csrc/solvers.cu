@@ -1609,6 +1609,52 @@ __global__ void __launch_bounds__(kBlock) k_gm_apply(CSRView<T> A, const T* __re
     }
 }
 
+// The same product on stencil masks of the fixed 5- or 7-point shape SH: W consecutive rows
+// per thread in 16-byte groups (stencil_group, as MAT::Apply's vector-row kernel), the
+// preconditioner folded into the gather (mode 1: v .* diagInv per element) or the result
+// (mode 2). Each row sum is the one k_gm_apply forms, bit for bit.
+template <typename T, int SH, int MODE>
+__global__ void __launch_bounds__(kBlock) k_gm_apply_vec(CSRView<T> A, const T* __restrict__ v,
+                                                         const T* __restrict__ dinv,
+                                                         T* __restrict__ y, const int* stop)
+{
+    if (*stop) return;
+    using VT = Vec16<T>;
+    using V = typename VT::V;
+    constexpr int W = VT::W;
+    const uint32_t nw = A.nrow / W, stride = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    const V* vv = reinterpret_cast<const V*>(v);
+    const V* dv = reinterpret_cast<const V*>(dinv);
+    V* yv = reinterpret_cast<V*>(y);
+    auto gather = [&](uint32_t h) {
+        const V a = vv[h];
+        if (MODE != 1) return a;
+        const V d = dv[h];
+        T t[W];
+#pragma unroll
+        for (int e = 0; e < W; ++e) t[e] = VT::at(a, e) * VT::at(d, e);
+        return VT::make(t);
+    };
+    // the loop bound is the same on every lane of a warp (all lanes shuffle)
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane < nw; g += stride) {
+        const bool act = g < nw;
+        T s[W];
+#pragma unroll
+        for (int e = 0; e < W; ++e) s[e] = T(0);
+        V c;
+        stencil_group<T, SH>(A, g, nw, act, gather, c, s);
+        if (act) {
+            if (MODE == 2) {
+                const V d = dv[g];
+#pragma unroll
+                for (int e = 0; e < W; ++e) s[e] = s[e] * VT::at(d, e);
+            }
+            yv[g] = VT::make(s);
+        }
+    }
+}
+
 // w *= 1 / t (Scale by a device scalar, as v_scale(Scal::dinv(t)))
 template <typename T>
 __global__ void k_gm_scale(uint32_t n, const double* __restrict__ tn, T* __restrict__ w,
@@ -1726,6 +1772,21 @@ template <typename T, int MODE>
 static void gm_apply_launch(Ctx& c, const Mat& A, CSRView<T> V, const T* v, const T* dinv,
                             T* y, const int* stop)
 {
+    if (A.lanes == 1) { // fixed 5- or 7-point stencil masks: 16-byte row groups
+        const int sh = stencil_vec_shape(V, v, y, MODE == 0 ? (const void*)v : (const void*)dinv);
+        if (sh) {
+            auto gv = [&](auto kern) {
+                const int g = std::min(c.grid((long long)V.nrow / Vec16<T>::W, kBlock),
+                                       resident_grid(c, (const void*)kern, kBlock));
+                kern<<<g, kBlock, 0, c.stream>>>(V, v, dinv, y, stop);
+            };
+            if (sh == 5)
+                gv(k_gm_apply_vec<T, 5, MODE>);
+            else
+                gv(k_gm_apply_vec<T, 7, MODE>);
+            return;
+        }
+    }
     const int need = c.grid((long long)A.nrow * A.lanes, kBlock);
     const size_t tiles = A.lanes == 1 ? with_tiles(V, kBlock) : 0;
     auto go = [&](auto kern) {

@@ -98,6 +98,7 @@ def test_classes_without_a_common_stencil(gpu):
                                           ("cg", "MIXED_RELIABLE", 18),
                                           ("cg", "MIXED_RELIABLE", 81),
                                           ("bicgstab", "FP64", 14), ("gmres", "FP64", 14),
+                                          ("gmres", "MIXED", 14), ("gmres_left", "FP64", 14),
                                           ("fgmres", "MIXED", 14)])
 def test_solves_identical_in_every_form(gpu, alg, prec, dim):
     from faspxx_b200 import capi
