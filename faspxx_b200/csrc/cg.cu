@@ -1188,6 +1188,19 @@ __device__ bool grid_sync(GridBar* bar, unsigned* gen)
     return ok != 0;
 }
 
+// The one-cluster variant of the persistent kernel (small systems): its blocks are one
+// thread-block cluster, co-scheduled by construction, and meet at the hardware cluster
+// barrier (release/acquire at cluster scope orders the partials and vectors in global memory
+// that the other blocks read next) instead of the atomic grid barrier. Every block takes the
+// same branches on bit-identical scalars, as at a __syncthreads.
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+constexpr int kCBlock = 1024; // threads per block of the one-cluster kernel
+
 // Sum of the partials of slot k over all blocks, fixed order; every block gets the same.
 template <int NV>
 __device__ __forceinline__ void all_reduce_partials(const Scratch s, const int (&slot)[NV],
@@ -1208,8 +1221,8 @@ __device__ __forceinline__ void write_partials(Scratch s, const int (&slot)[NV],
         for (int k = 0; k < NV; ++k) s.partials[slot[k] * kMaxGrid + blockIdx.x] = acc[k];
 }
 
-template <typename T, int JAC>
-__global__ void __launch_bounds__(kPBlock, 4)
+template <typename T, int JAC, bool CL = false>
+__global__ void __launch_bounds__(CL ? kCBlock : kPBlock, CL ? 1 : 4)
 cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __restrict__ dinv,
               CGCtl* gctl, Scratch s, GridBar* bar, unsigned iterCap)
 {
@@ -1218,9 +1231,17 @@ cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __res
     __shared__ double bc[5];
     if (threadIdx.x == 0) {
         c = *gctl;
-        gen = ld_acquire_u32(&bar->gen);
+        if (!CL) gen = ld_acquire_u32(&bar->gen);
     }
     __syncthreads();
+    auto sync = [&]() -> bool {
+        if constexpr (CL) {
+            cluster_sync_all();
+            return true;
+        } else {
+            return grid_sync(bar, &gen);
+        }
+    };
     const uint32_t n = A.nrow;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
@@ -1247,7 +1268,7 @@ cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __res
             double a[1] = {(double)acc};
             const int sl[1] = {kSlotPhase1}, ops[1] = {kSum};
             write_partials<1>(s, sl, ops, a);
-            if (!grid_sync(bar, &gen)) return;
+            if (!sync()) return;
             double t[1];
             all_reduce_partials<1>(s, sl, ops, t);
             if (threadIdx.x == 0) {
@@ -1282,7 +1303,7 @@ cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __res
             double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
             const int sl[5] = {0, 1, 2, 3, 4}, ops[5] = {kSum, kSum, kSum, kMax, kSum};
             write_partials<5>(s, sl, ops, a);
-            if (!grid_sync(bar, &gen)) return;
+            if (!sync()) return;
             double t[5];
             all_reduce_partials<5>(s, sl, ops, t);
             if (threadIdx.x == 0) {
@@ -1563,6 +1584,41 @@ int CGEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool grap
         FB_CUDA(cudaGraphInstantiate(&gexec, g, 0));
         cudaGraphDestroy(g);
     }
+    if (wantPersistent && wantCluster) {
+        // one cluster of 16 blocks (8 if the device refuses the non-portable size)
+        const void* fn = jacobi ? (const void*)cg_persistent<T, 1, true>
+                                : (const void*)cg_persistent<T, 0, true>;
+        cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaGetLastError();
+        for (int cs : {16, 8}) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)cs);
+            cfg.blockDim = dim3(kCBlock);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)cs;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int nc = 0;
+            if (cudaOccupancyMaxActiveClusters(&nc, fn, &cfg) == cudaSuccess && nc >= 1) {
+                cgrid = cs;
+                break;
+            }
+            cudaGetLastError();
+        }
+        if (cgrid > 0) {
+            // the control flow needs no barrier state, but the kernel takes the pointer
+            if (cudaMalloc(&bar, sizeof(GridBar)) != cudaSuccess) {
+                cudaGetLastError();
+                return kErrAlloc;
+            }
+            FB_CUDA(cudaMemsetAsync(bar, 0, sizeof(GridBar), c->stream));
+            cluster = persistent = true;
+            return kOk;
+        }
+    }
     if (wantPersistent) {
         // one cooperative launch needs every block resident: size the grid from occupancy
         int coop = 0, nb = 0;
@@ -1595,6 +1651,27 @@ int CGEngine<T>::run_persistent(unsigned iterCap)
     CSRView<T> V = view_of<T>(*A);
     T* zz = jacobi ? z : r;
     Scratch s = c->red;
+    if (cluster) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)cgrid);
+        cfg.blockDim = dim3(kCBlock);
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cgrid;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (jacobi)
+            FB_CUDA(cudaLaunchKernelEx(&cfg, cg_persistent<T, 1, true>, V, x, r, zz, P0, P1, q,
+                                       dinv, ctl, s, bar, iterCap));
+        else
+            FB_CUDA(cudaLaunchKernelEx(&cfg, cg_persistent<T, 0, true>, V, x, r, zz, P0, P1, q,
+                                       dinv, ctl, s, bar, iterCap));
+        FB_CUDA(cudaStreamSynchronize(c->stream));
+        return kOk;
+    }
     void* args[] = {&V, &x, &r, &zz, &P0, &P1, &q, (void*)&dinv, &ctl, &s, &bar, &iterCap};
     const void* fn = jacobi ? (const void*)cg_persistent<T, 1> : (const void*)cg_persistent<T, 0>;
     FB_CUDA(cudaMemcpyAsync(&bar->limit, &barLimit, sizeof(unsigned), cudaMemcpyHostToDevice,
@@ -1626,7 +1703,8 @@ void CGEngine<T>::destroy()
     cudaFree(ctl);
     cudaFree(bar);
     bar = nullptr;
-    persistent = false;
+    persistent = cluster = false;
+    cgrid = 0;
     if (hctl) cudaFreeHost(hctl);
     if (hstatus) cudaFreeHost(hstatus);
     x = r = z = q = P0 = P1 = nullptr;

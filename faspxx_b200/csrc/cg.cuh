@@ -112,6 +112,11 @@ struct CGEngine {
     // persistent engine: one cooperative launch runs the iterations
     bool       wantPersistent = true; // set before init
     bool       persistent = false;
+    // ... as one thread-block cluster (wantCluster, set before init with wantPersistent):
+    // cgrid blocks of 1024 threads meeting at the hardware cluster barrier
+    bool       wantCluster = false;
+    bool       cluster = false;
+    int        cgrid = 0;
     int        pgrid = 0;
     GridBar*   bar = nullptr;
     unsigned   barLimit = 0;      // GridBar::limit written before each persistent launch

@@ -418,6 +418,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
             if (fusable && cfg.precision == FASP_GPU_FP64) {
                 cg64 = new CGEngine<double>();
                 cg64->wantPersistent = cfg.persistent != 0;
+                cg64->wantCluster = cfg.persistent == 2;
                 cg64->barLimit = barLimit;
                 cg64->pdl = cfg.overlapLaunch != 0;
                 // Jacobi::Setup's diagInv = (1 / diag) * weight, one value for all rows
@@ -430,6 +431,7 @@ int SolverImpl::setup(fasp_gpu_mat Mh)
                 if ((e = Ah->M.ensure32(c.stream))) return e;
                 cg32 = new CGEngine<float>();
                 cg32->wantPersistent = cfg.persistent != 0;
+                cg32->wantCluster = cfg.persistent == 2;
                 cg32->barLimit = barLimit;
                 cg32->pdl = cfg.overlapLaunch != 0;
                 cg32->recurrence = cfg.fp32Recurrence != 0;

@@ -353,8 +353,9 @@ class SOL:
     def SetOrth(self, orth):
         self.cfg.orth = orth
 
-    def SetPersistent(self, flag: bool):
-        self.cfg.persistent = 1 if flag else 0
+    def SetPersistent(self, flag):
+        """False: CUDA graphs; True (1): one cooperative launch; 2: one thread-block cluster."""
+        self.cfg.persistent = int(flag)
 
     def SetOverlapLaunch(self, flag: bool):
         self.cfg.overlapLaunch = 1 if flag else 0

@@ -104,8 +104,10 @@ typedef struct {
     int             useGraph;    /* 1: device-driven iterations captured in CUDA graphs */
     int             persistent;  /* 1: device-driven CG runs all iterations in one
                                     cooperative launch (when the device allows it);
-                                    default 0: CUDA graphs of the two fused kernels
-                                    measure faster on B200 at every size */
+                                    2: ... as one thread-block cluster of 16 blocks (8
+                                    where 16 is refused) meeting at the hardware
+                                    cluster barrier, for small systems;
+                                    default 0: CUDA graphs of the two fused kernels */
     int             overlapLaunch; /* 1 (default): the CG and BiCGStab iteration kernels
                                     use programmatic dependent launch, each one's launch
                                     overlapping its predecessor's reduction tail */

@@ -194,7 +194,7 @@ def _check_case(gpu, oracle, name, engine="graph", orth=None):
     s = gpu.configure(case["alg"], **case["kw"])
     if orth is not None:
         s.SetOrth(orth)
-    s.SetPersistent(engine == "persistent")
+    s.SetPersistent(2 if engine == "cluster" else engine == "persistent")
     s.SetUseGraph(engine in ("graph", "graph_serial"))
     s.SetOverlapLaunch(engine != "graph_serial")
     s.Setup(M)
@@ -248,14 +248,38 @@ def test_solver_parity(gpu, oracle, name):
     _check_case(gpu, oracle, name)
 
 
-@pytest.mark.parametrize("engine", ["persistent", "plain", "graph_serial"])
+@pytest.mark.parametrize("engine", ["persistent", "cluster", "plain", "graph_serial"])
 @pytest.mark.parametrize("name", ["fdm_pcg", "fem_pcg", "p2d_pcg", "p3d_cg", "vd_cg",
                                   "fdm_cg_min5", "fdm_cg_tolsmall"])
 def test_cg_engines_match(gpu, oracle, name, engine):
     """The device-driven CG meets the same bars run as CUDA graphs of its two kernels with
     overlapped launches (the default, exercised by test_solver_parity), as graphs with
-    ordinary launches, as one persistent cooperative kernel, and as plain launches."""
+    ordinary launches, as one persistent cooperative kernel, as one persistent thread-block
+    cluster, and as plain launches."""
     _check_case(gpu, oracle, name, engine=engine)
+
+
+@pytest.mark.parametrize("prec", ["FP64", "MIXED_RELIABLE"])
+def test_cluster_engine_small_system(gpu, prec):
+    """The one-cluster persistent CG (16 blocks meeting at the hardware cluster barrier) on a
+    2D Poisson system, FP64 and FP32 iterations with reliable updates: the default engine's
+    code and iteration count, the tolerance on the true residual."""
+    from faspxx_b200 import capi, problems as P
+    A = P.poisson2d(128)
+    b = A.matvec(P.seeded_uniform(A.nrow, 42))
+    out = []
+    for mode in (0, 2):
+        s = gpu.configure("cg", maxIter=2000, relTol=1e-8, absTol=0.0, pcd="jacobi",
+                          pcdWeight=1.0, pcdIter=1)
+        if prec != "FP64":
+            s.SetPrecision(getattr(capi, prec), innerRelTol=1e-2)
+        s.SetPersistent(mode)
+        s.Setup(gpu.MAT(A))
+        x = np.zeros(A.nrow)
+        out.append((s.Solve(b, x), s.GetIterations(), x))
+    (c0, i0, _), (c2, i2, x2) = out
+    assert c0 == c2 == 0 and abs(i0 - i2) <= 1, (i0, i2)
+    assert np.linalg.norm(b - A.matvec(x2)) <= 1e-8 * np.linalg.norm(b)
 
 
 @pytest.mark.parametrize("name", sorted(n for n in CASES if CASES[n]["alg"] in ("gmres",
