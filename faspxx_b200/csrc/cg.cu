@@ -14,6 +14,8 @@
 #include <type_traits>
 #include <utility>
 
+#include <cooperative_groups.h>
+
 #include "cg.cuh"
 
 namespace fb {
@@ -1317,6 +1319,174 @@ cg_persistent(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __res
     if (blockIdx.x == 0 && threadIdx.x == 0) *gctl = c;
 }
 
+// ---- small systems: one cluster, the vectors in distributed shared memory ---------------
+// cg_persistent's iteration for a system whose vectors fit in the shared memory of one
+// cluster: block b holds rows [b S, (b + 1) S) of x, r, z, both direction buffers and q in
+// its own shared memory (S a power of two) and gathers the columns that other blocks own
+// through distributed shared memory; the block partials are exchanged the same way and every
+// block adds them in rank order, so all blocks take the same branches on the same scalars.
+// Nothing of an iteration goes through L2 but the matrix and diagInv. The slices are loaded
+// from the engine's vectors at entry and stored back at exit, where the host-side branches
+// (escalations, reliable refreshes) read them; a block leaves only after the last cluster
+// barrier, so no block reads the shared memory of one that has gone.
+constexpr int kDsVecs = 6; // x, r, z, P0, P1, q
+// rows a thread holds at most: a block's slice is at most 4,096 FP64 or 8,192 FP32 rows
+// (six vectors in 227 KB), 1,024 threads a block
+template <typename T>
+constexpr int kDsRows = sizeof(T) == 8 ? 4 : 8;
+
+template <typename T, int JAC>
+__global__ void __launch_bounds__(kCBlock, 1)
+cg_dsmem(CSRView<T> A, T* x, T* r, T* z, T* P0, T* P1, T* q, const T* __restrict__ dinv,
+         CGCtl* gctl, unsigned iterCap, int shift)
+{
+    namespace cgx = cooperative_groups;
+    cgx::cluster_group cl = cgx::this_cluster();
+    extern __shared__ __align__(16) unsigned char ds_raw[];
+    const uint32_t S = 1u << shift;
+    T* sx = reinterpret_cast<T*>(ds_raw);
+    T* sr = sx + S;
+    T* sz = sr + S;
+    T* sp0 = sz + S;
+    T* sp1 = sp0 + S;
+    T* sq = sp1 + S;
+    __shared__ CGCtl c;
+    __shared__ double part[2][5]; // this block's totals: the product phase, the update phase
+    __shared__ double gath[16][5]; // every block's totals, fetched one block per thread
+    __shared__ double bc[5];
+    const uint32_t n = A.nrow, rank = cl.block_rank(), nb = cl.num_blocks();
+    const uint32_t r0 = rank << shift;
+    const uint32_t rows = r0 < n ? min(S, n - r0) : 0u;
+    const uint32_t tid = threadIdx.x, bd = blockDim.x;
+    for (uint32_t i = tid; i < rows; i += bd) {
+        sx[i] = x[r0 + i];
+        sr[i] = r[r0 + i];
+        if (JAC) sz[i] = z[r0 + i];
+        sp0[i] = P0[r0 + i];
+        sp1[i] = P1[r0 + i];
+        sq[i] = q[r0 + i];
+    }
+    if (tid == 0) c = *gctl;
+    cl.sync();
+    T* szz = JAC ? sz : sr;
+    auto at = [&](T* base, uint32_t j) -> T {
+        const uint32_t o = j >> shift, l = j & (S - 1u);
+        return o == rank ? base[l] : cl.map_shared_rank(base, o)[l];
+    };
+    // a thread's rows i = tid + u blockDim (u < R), unrolled so that their loads overlap;
+    // its diagInv entries stay in registers for the whole launch
+    constexpr int R = kDsRows<T>;
+    T dv[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        const uint32_t i = tid + u * bd;
+        dv[u] = JAC && i < rows ? __ldg(dinv + r0 + i) : T(0);
+    }
+    unsigned done = 0;
+    while (c.status == kRun && done < iterCap) {
+        // phase 1: ax = A p with p = z + beta p_old formed on the fly, and (ax, p)
+        {
+            const int mode = c.pmode, par = c.par;
+            const T beta = (T)c.beta;
+            T* pOld = par ? sp1 : sp0;
+            T* pNew = par ? sp0 : sp1;
+            T sum[R], pv[R];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const uint32_t i = tid + u * bd;
+                sum[u] = pv[u] = T(0);
+                if (i < rows) {
+                    sum[u] = row_apply<T, false>(A, r0 + i, [&](uint32_t j) {
+                        return mode ? fma(beta, at(pOld, j), at(szz, j)) : at(szz, j);
+                    });
+                    pv[u] = mode ? fma(beta, pOld[i], szz[i]) : szz[i];
+                }
+            }
+            T acc = T(0);
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const uint32_t i = tid + u * bd;
+                if (i < rows) {
+                    pNew[i] = pv[u];
+                    sq[i] = sum[u];
+                    acc = fma(sum[u], pv[u], acc);
+                }
+            }
+            double a[1] = {(double)acc};
+            const int ops[1] = {kSum};
+            block_reduce<1>(a, ops);
+            if (tid == 0) part[0][0] = a[0];
+            cl.sync();
+            if (tid < nb) gath[tid][0] = *cl.map_shared_rank(&part[0][0], tid);
+            __syncthreads();
+            if (tid == 0) {
+                double t = 0.0;
+                for (uint32_t b = 0; b < nb; ++b) t += gath[b][0];
+                c.par = par ^ 1;
+                if (!c.bench) cg_after_spmv(&c, t);
+            }
+            __syncthreads();
+            if (c.status != kRun) break;
+        }
+        // phase 2: x += alpha p, r -= alpha ax, z = diagInv .* r, and the five reductions
+        {
+            const T alpha = (T)c.alpha;
+            const T* p = c.par ? sp1 : sp0;
+            T rr = 0, zr = 0, xx = 0, xm = 0, pp = 0;
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const uint32_t i = tid + u * bd;
+                if (i >= rows) continue;
+                const T pi = p[i];
+                const T xi = fma(alpha, pi, sx[i]);
+                const T ri = fma(-alpha, sq[i], sr[i]);
+                sx[i] = xi;
+                sr[i] = ri;
+                T zi = ri;
+                if (JAC) {
+                    zi = dv[u] * ri;
+                    sz[i] = zi;
+                }
+                rr = fma(ri, ri, rr);
+                zr = fma(zi, ri, zr);
+                xx = fma(xi, xi, xx);
+                xm = fmax(xm, fabs(xi));
+                pp = fma(pi, pi, pp);
+            }
+            double a[5] = {(double)rr, (double)zr, (double)xx, (double)xm, (double)pp};
+            const int ops[5] = {kSum, kSum, kSum, kMax, kSum};
+            block_reduce<5>(a, ops);
+            if (tid == 0)
+                for (int k = 0; k < 5; ++k) part[1][k] = a[k];
+            cl.sync();
+            if (tid < nb) {
+                const double* pb = cl.map_shared_rank(&part[1][0], tid);
+                for (int k = 0; k < 5; ++k) gath[tid][k] = pb[k];
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+                for (uint32_t b = 0; b < nb; ++b)
+                    for (int k = 0; k < 5; ++k) t[k] = red_apply(t[k], gath[b][k], ops[k]);
+                for (int k = 0; k < 5; ++k) bc[k] = t[k];
+                if (!c.bench) cg_checks(&c, bc, 0);
+            }
+            __syncthreads();
+        }
+        ++done;
+    }
+    cl.sync(); // every remote read of this block's slices is done
+    for (uint32_t i = tid; i < rows; i += bd) {
+        x[r0 + i] = sx[i];
+        r[r0 + i] = sr[i];
+        if (JAC) z[r0 + i] = sz[i];
+        P0[r0 + i] = sp0[i];
+        P1[r0 + i] = sp1[i];
+        q[r0 + i] = sq[i];
+    }
+    if (rank == 0 && tid == 0) *gctl = c;
+}
+
 // ---- engine ------------------------------------------------------------------------------
 
 static int spmv_grid_cg(const Ctx& c, uint32_t nrow, int L)
@@ -1585,6 +1755,51 @@ int CGEngine<T>::init(Ctx* ctx, const Mat* M, int jac, const T* dinvv, bool grap
         cudaGraphDestroy(g);
     }
     if (wantPersistent && wantCluster) {
+        // the vectors in distributed shared memory: 16 (else 8) blocks of 2^k rows each
+        const void* fd = jacobi ? (const void*)cg_dsmem<T, 1> : (const void*)cg_dsmem<T, 0>;
+        cudaFuncSetAttribute(fd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaGetLastError();
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev);
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, fd) != cudaSuccess) {
+            cudaGetLastError();
+            optin = 0;
+        }
+        for (int cs : {16, 8}) {
+            int k = 0;
+            while (((size_t)cs << k) < (size_t)n) ++k;
+            const size_t bytes = (size_t)kDsVecs * ((size_t)1 << k) * sizeof(T);
+            if (bytes + fa.sharedSizeBytes > (size_t)optin) continue;
+            if (((size_t)1 << k) > (size_t)kDsRows<T> * kCBlock) continue;
+            if (cudaFuncSetAttribute(fd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes) != cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)cs);
+            cfg.blockDim = dim3(kCBlock);
+            cfg.dynamicSmemBytes = bytes;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)cs;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int nc = 0;
+            if (cudaOccupancyMaxActiveClusters(&nc, fd, &cfg) == cudaSuccess && nc >= 1) {
+                cgrid = cs;
+                dshift = k;
+                dsBytes = bytes;
+                dsmem = cluster = persistent = true;
+                return kOk;
+            }
+            cudaGetLastError();
+        }
+    }
+    if (wantPersistent && wantCluster) {
         // one cluster of 16 blocks (8 if the device refuses the non-portable size)
         const void* fn = jacobi ? (const void*)cg_persistent<T, 1, true>
                                 : (const void*)cg_persistent<T, 0, true>;
@@ -1651,6 +1866,28 @@ int CGEngine<T>::run_persistent(unsigned iterCap)
     CSRView<T> V = view_of<T>(*A);
     T* zz = jacobi ? z : r;
     Scratch s = c->red;
+    if (dsmem) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)cgrid);
+        cfg.blockDim = dim3(kCBlock);
+        cfg.dynamicSmemBytes = dsBytes;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)cgrid;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (jacobi)
+            FB_CUDA(cudaLaunchKernelEx(&cfg, cg_dsmem<T, 1>, V, x, r, zz, P0, P1, q, dinv, ctl,
+                                       iterCap, dshift));
+        else
+            FB_CUDA(cudaLaunchKernelEx(&cfg, cg_dsmem<T, 0>, V, x, r, zz, P0, P1, q, dinv, ctl,
+                                       iterCap, dshift));
+        FB_CUDA(cudaStreamSynchronize(c->stream));
+        return kOk;
+    }
     if (cluster) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)cgrid);
@@ -1703,7 +1940,7 @@ void CGEngine<T>::destroy()
     cudaFree(ctl);
     cudaFree(bar);
     bar = nullptr;
-    persistent = cluster = false;
+    persistent = cluster = dsmem = false;
     cgrid = 0;
     if (hctl) cudaFreeHost(hctl);
     if (hstatus) cudaFreeHost(hstatus);

@@ -117,6 +117,11 @@ struct CGEngine {
     bool       wantCluster = false;
     bool       cluster = false;
     int        cgrid = 0;
+    // ... with the vectors in the cluster's distributed shared memory, 2^dshift rows a block,
+    // when they fit (dsBytes of dynamic shared memory a block)
+    bool       dsmem = false;
+    int        dshift = 0;
+    size_t     dsBytes = 0;
     int        pgrid = 0;
     GridBar*   bar = nullptr;
     unsigned   barLimit = 0;      // GridBar::limit written before each persistent launch

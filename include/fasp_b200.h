@@ -106,7 +106,10 @@ typedef struct {
                                     cooperative launch (when the device allows it);
                                     2: ... as one thread-block cluster of 16 blocks (8
                                     where 16 is refused) meeting at the hardware
-                                    cluster barrier, for small systems;
+                                    cluster barrier, the vectors in the cluster's
+                                    distributed shared memory when they fit (n up to
+                                    65,536 FP64 / 131,072 FP32): faster than the
+                                    graphs only for the smallest systems;
                                     default 0: CUDA graphs of the two fused kernels */
     int             overlapLaunch; /* 1 (default): the CG and BiCGStab iteration kernels
                                     use programmatic dependent launch, each one's launch
