@@ -104,7 +104,8 @@ __device__ __forceinline__ void bulk_copy_g2s_plain(void* dst, const void* src, 
 // flight (bounded) and stopped.
 template <typename T, typename Src, typename Consume, typename Ready>
 __device__ __forceinline__ bool dc_stream(DcRing& ring, size_t e0, size_t e1, int nItem, Src src,
-                                          Consume consume, Ready ready)
+                                          Consume consume, Ready ready,
+                                          uint32_t pre = (uint32_t)kDcStages)
 {
     constexpr uint32_t C = DcShape<T>::C;
     const uint32_t tid = threadIdx.x;
@@ -133,15 +134,18 @@ __device__ __forceinline__ bool dc_stream(DcRing& ring, size_t e0, size_t e1, in
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ring.full[q]))
                          : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (uint32_t k = 0; k < (uint32_t)kDcStages && k < total; ++k) issue();
+        for (uint32_t k = 0; k < pre && k < (uint32_t)kDcStages && k < total; ++k) issue();
     }
     // every thread: false leaves before the first item (the block drains its first copies)
     if (!ready()) {
         if (tid == 0)
-            for (uint32_t q = 0; q < (uint32_t)kDcStages && q < total; ++q)
+            for (uint32_t q = 0; q < pre && q < (uint32_t)kDcStages && q < total; ++q)
                 mbar_wait_bounded(&ring.full[q], 0u);
         return false;
     }
+    // the rest of the first stages: items that may only be read once ready() has passed
+    if (tid == 0)
+        for (uint32_t k = pre; k < (uint32_t)kDcStages && k < total; ++k) issue();
     __syncthreads();
     int v = 0, st = 0;
     uint32_t ph = 0;
@@ -241,11 +245,25 @@ __device__ __forceinline__ double warp_sum16(const double (&x)[16])
 
 // ---- the dots pass and the step's scalar work ----------------------------------------
 
+// The product w = A M u of the step, formed by the dots pass itself on stencil masks of the
+// fixed 5- or 7-point shape SH: each thread forms its 16-byte groups of w from the
+// gathered u (stencil_group: the row sums of k_gm_apply_vec, bit for bit; MODE 1 folds
+// diagInv into the gather, MODE 2 scales the result), stores them for the update pass and
+// keeps them for the dots. It saves the product's launch and the re-read of w.
+template <typename T>
+struct DcApply {
+    CSRView<T> A;
+    const T*   dinv;
+    T*         wout;
+};
+
 // Value slots: a_l at l, then (with w) b_l at j + l, c at 2j, and d last.
-template <typename T, bool HASW>
+template <typename T, bool HASW, int SH = 0, int MODE = 0>
 __global__ void __launch_bounds__(kDcThreads, 2)
-k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
+k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g, DcApply<T> Ap)
 {
+    constexpr bool FUSE = HASW && SH != 0;
+    constexpr int WI = HASW && !FUSE ? 1 : 0; // w streamed as item 1
     extern __shared__ __align__(16) unsigned char dc_raw[];
     DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
     __shared__ double wacc[kDcWarps][kDcMaxNV];
@@ -259,7 +277,7 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     using S = DcShape<T>;
     const int j = P.j;
     const int nv = HASW ? 2 * j + 2 : j + 1;
-    const int nItem = 1 + (HASW ? 1 : 0) + j;
+    const int nItem = 1 + WI + j;
     const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int v = tid; v < kDcWarps * nv; v += kDcThreads) wacc[v / nv][v % nv] = 0.0;
     size_t e0, e1;
@@ -273,23 +291,68 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
     for (int q = 0; q < 8; ++q) wa[q] = wb[q] = 0.0;
     auto src = [&](int v) -> const T* {
         if (v == 0) return P.V + (size_t)j * P.ld;
-        if (HASW && v == 1) return P.w;
-        return P.V + (size_t)(v - 1 - (HASW ? 1 : 0)) * P.ld;
+        if (WI && v == 1) return P.w;
+        return P.V + (size_t)(v - 1 - WI) * P.ld;
     };
     auto add = [&](int slot, double x) { // the warp's sum of an item, lane 0 keeps it
         x = warp_reduce(x, kSum);
         if (lane == 0) wacc[wid][slot] += x;
     };
+    // the fused product: the thread's groups of w = A M u (every lane of a warp takes part)
+    auto product = [&](size_t base, uint32_t len) {
+        if constexpr (FUSE) {
+            using VT = Vec16<T>;
+            using V = typename VT::V;
+            const V* uv = reinterpret_cast<const V*>(P.V + (size_t)j * P.ld);
+            const V* dv = reinterpret_cast<const V*>(Ap.dinv);
+            const uint32_t nw = P.n / S::W;
+            auto gather = [&](uint32_t h) {
+                const V a = uv[h];
+                if (MODE != 1) return a;
+                const V d = dv[h];
+                T t[S::W];
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) t[e] = VT::at(a, e) * VT::at(d, e);
+                return VT::make(t);
+            };
+#pragma unroll
+            for (int r = 0; r < S::G; ++r) {
+                const uint32_t i0 = (uint32_t)(r * kDcThreads + tid) * S::W;
+                const uint32_t gi = (uint32_t)(base / S::W) + (uint32_t)(r * kDcThreads + tid);
+                // every group of the vector takes part, so that a lane's neighbours in the
+                // shuffles are the real groups g - 1 and g + 1 also past the end of this
+                // block's range; only the block's own groups are stored and summed
+                const bool act = gi < nw, own = i0 + S::W <= len;
+                T sum[S::W];
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) sum[e] = T(0);
+                V cgrp;
+                stencil_group<T, SH>(Ap.A, gi, nw, act, gather, cgrp, sum);
+                if (own && MODE == 2) {
+                    const V d = dv[gi];
+#pragma unroll
+                    for (int e = 0; e < S::W; ++e) sum[e] = sum[e] * VT::at(d, e);
+                }
+                if (own) reinterpret_cast<V*>(Ap.wout)[gi] = VT::make(sum);
+#pragma unroll
+                for (int e = 0; e < S::W; ++e) w[r][e] = own ? sum[e] : T(0);
+            }
+        }
+    };
     const bool ok = dc_stream<T>(ring, e0, e1, nItem, src,
-                                 [&](int v, size_t, const T* st, uint32_t len) {
+                                 [&](int v, size_t base, const T* st, uint32_t len) {
         if (v == 0) {
             dc_load<T>(st, len, u);
             add(nv - 1, (double)dc_dot<T>(u, u));
-        } else if (HASW && v == 1) {
+            if (FUSE) {
+                product(base, len);
+                add(2 * j, (double)dc_dot<T>(u, w));
+            }
+        } else if (WI && v == 1) {
             dc_load<T>(st, len, w);
             add(2 * j, (double)dc_dot<T>(u, w));
         } else {
-            const int l = v - 1 - (HASW ? 1 : 0);
+            const int l = v - 1 - WI;
             T q[S::G][S::W];
             dc_load<T>(st, len, q);
             const double pa = (double)dc_dot<T>(q, u);
@@ -439,7 +502,9 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g)
 
 // ---- the update pass -----------------------------------------------------------------
 
-template <typename T>
+// WLAST: w, written by a dots pass that formed the product, is each chunk's last item, and
+// only the items before the first w are copied ahead of the grid dependency.
+template <typename T, bool WLAST = false>
 __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayout L,
                                                              const GmCtl* g)
 {
@@ -471,10 +536,11 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
     T u[S::G][S::W], w[S::G][S::W], sa[S::G][S::W], sb[S::G][S::W];
     T* qj = P.V + (size_t)j * P.ld;
     T* un = P.V + (size_t)(j + 1) * P.ld;
+    const int wv = WLAST ? nItem - 1 : 1; // w's place in a chunk
     auto src = [&](int v) -> const T* {
         if (v == 0) return P.V + (size_t)j * P.ld;
-        if (v == 1) return P.w;
-        return P.V + (size_t)(v - 2) * P.ld;
+        if (v == wv) return P.w;
+        return P.V + (size_t)(v - (WLAST ? 1 : 2)) * P.ld;
     };
     dc_stream<T>(ring, e0, e1, nItem, src, [&](int v, size_t base, const T* st, uint32_t len) {
         if (v == 0) {
@@ -483,10 +549,10 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
             for (int q = 0; q < S::G; ++q)
 #pragma unroll
                 for (int e = 0; e < S::W; ++e) sa[q][e] = sb[q][e] = T(0);
-        } else if (v == 1) {
+        } else if (v == wv) {
             dc_load<T>(st, len, w);
         } else {
-            const int l = v - 2;
+            const int l = v - (WLAST ? 1 : 2);
             T q[S::G][S::W];
             dc_load<T>(st, len, q);
             const T al = ca[l], bl = cb[l];
@@ -522,7 +588,7 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
                 }
             }
         }
-    }, ready);
+    }, ready, WLAST ? (uint32_t)wv : (uint32_t)kDcStages);
 }
 
 // ---- launchers -------------------------------------------------------------------------
@@ -557,30 +623,57 @@ int dc_dots(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayo
 {
     if (j > kDcMaxK) return kErrInputPar;
     DcArgs<T> P{V, ld, w, n, j};
+    DcApply<T> none{};
     ++c.launches;
     if (w) {
         auto kern = k_dc_dots<T, true>;
         dc_optin((const void*)kern);
         kern<<<dc_grid(c, (const void*)kern, n, 2 * j + 2), kDcThreads, sizeof(DcRing),
-               c.stream>>>(P, c.red, L, g);
+               c.stream>>>(P, c.red, L, g, none);
     } else {
         auto kern = k_dc_dots<T, false>;
         dc_optin((const void*)kern);
         kern<<<dc_grid(c, (const void*)kern, n, j + 1), kDcThreads, sizeof(DcRing),
-               c.stream>>>(P, c.red, L, g);
+               c.stream>>>(P, c.red, L, g, none);
     }
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
 
 template <typename T>
+int dc_dots_apply(Ctx& c, const CSRView<T>& A, int mode, const T* dinv, uint32_t n, int j,
+                  T* V, size_t ld, T* w, const GmLayout& L, GmCtl* g)
+{
+    if (j > kDcMaxK) return kErrInputPar;
+    const int sh = stencil_vec_shape(A, V + (size_t)j * ld, w,
+                                     mode == 0 ? (const void*)w : (const void*)dinv);
+    if (!sh) return kErrInputPar;
+    DcArgs<T> P{V, ld, w, n, j};
+    DcApply<T> Ap{A, dinv, w};
+    ++c.launches;
+    auto go = [&](auto kern) {
+        dc_optin((const void*)kern);
+        kern<<<dc_grid(c, (const void*)kern, n, 2 * j + 2), kDcThreads, sizeof(DcRing),
+               c.stream>>>(P, c.red, L, g, Ap);
+    };
+    if (sh == 5)
+        mode == 0 ? go(k_dc_dots<T, true, 5, 0>) : mode == 1 ? go(k_dc_dots<T, true, 5, 1>)
+                                                 : go(k_dc_dots<T, true, 5, 2>);
+    else
+        mode == 0 ? go(k_dc_dots<T, true, 7, 0>) : mode == 1 ? go(k_dc_dots<T, true, 7, 1>)
+                                                 : go(k_dc_dots<T, true, 7, 2>);
+    FB_CUDA(cudaGetLastError());
+    return kOk;
+}
+
+template <typename T>
 int dc_update(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L,
-              const GmCtl* g)
+              const GmCtl* g, bool wlast)
 {
     if (j > kDcMaxK) return kErrInputPar;
     DcArgs<T> P{V, ld, w, n, j};
     ++c.launches;
-    auto kern = k_dc_update<T>;
+    auto kern = wlast ? k_dc_update<T, true> : k_dc_update<T, false>;
     dc_optin((const void*)kern);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)dc_grid(c, (const void*)kern, n, 1));
@@ -602,9 +695,13 @@ template int dc_dots<double>(Ctx&, uint32_t, int, double*, size_t, const double*
 template int dc_dots<float>(Ctx&, uint32_t, int, float*, size_t, const float*, const GmLayout&,
                             GmCtl*);
 template int dc_update<double>(Ctx&, uint32_t, int, double*, size_t, const double*,
-                               const GmLayout&, const GmCtl*);
+                               const GmLayout&, const GmCtl*, bool);
 template int dc_update<float>(Ctx&, uint32_t, int, float*, size_t, const float*,
-                              const GmLayout&, const GmCtl*);
+                              const GmLayout&, const GmCtl*, bool);
+template int dc_dots_apply<double>(Ctx&, const CSRView<double>&, int, const double*, uint32_t,
+                                   int, double*, size_t, double*, const GmLayout&, GmCtl*);
+template int dc_dots_apply<float>(Ctx&, const CSRView<float>&, int, const float*, uint32_t,
+                                  int, float*, size_t, float*, const GmLayout&, GmCtl*);
 
 unsigned tile_timeouts_dcgs2() { return tile_timeouts(); }
 

@@ -102,7 +102,13 @@ template <typename T>
 int dc_dots(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L, GmCtl* g);
 template <typename T>
 int dc_update(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayout& L,
-              const GmCtl* g);
+              const GmCtl* g, bool wlast);
+// The dots pass of step j forming the product w = A M u itself (mode 0: A u, 1: A (D u),
+// 2: D (A u)) on stencil masks of the fixed 5- or 7-point shape; kErrInputPar when the
+// matrix or the vectors do not have that form (the caller then launches the product).
+template <typename T>
+int dc_dots_apply(Ctx& c, const CSRView<T>& A, int mode, const T* dinv, uint32_t n, int j,
+                  T* V, size_t ld, T* w, const GmLayout& L, GmCtl* g);
 unsigned tile_timeouts_dcgs2();
 
 } // namespace fb
