@@ -143,3 +143,42 @@ def test_dcgs2_mixed_precision(gpu, pe):
     # relTol 1e-8 bounds the residual, not the error: the error against x* is CGS2's
     e1, e2 = np.max(np.abs(x1 - xs)), np.max(np.abs(x2 - xs))
     assert e1 <= 2.0 * e2 + 1e-9 * np.max(np.abs(xs)), (e1, e2)
+
+
+def _upwind_2d(nx, pe):
+    """A nonsymmetric 5-point operator on an nx x nx grid: the 2D Laplacian plus first-order
+    upwind convection along x (the 5-point shape of the stencil-mask product)."""
+    A = P.poisson2d(nx)
+    rows = np.repeat(np.arange(A.nrow), np.diff(A.rowPtr.astype(np.int64)))
+    vals = A.values.copy()
+    d = A.colInd.astype(np.int64) - rows
+    vals[d == 0] += pe
+    vals[d == -1] -= pe
+    return P.CSRMatrix(A.nrow, A.mcol, A.rowPtr, A.colInd, vals)
+
+
+@pytest.mark.parametrize("alg", ["gmres", "gmres_left"])
+@pytest.mark.parametrize("shape", ["7-point", "5-point"])
+def test_dcgs2_fused_product_same_bits(gpu, alg, shape):
+    """The FP32 cycles form the product inside the dots pass on stencil masks of the fixed
+    5- or 7-point shape; on plain CSR the product is a separate kernel. Both give each row's
+    sum with the same operations: the mixed solves agree bit for bit, at a size with several
+    blocks and block ranges that end inside a warp's groups."""
+    capi, sol = gpu
+    A = P.convdiff3d(40, 10.0) if shape == "7-point" else _upwind_2d(300, 0.5)
+    b = A.matvec(np.random.default_rng(9).uniform(-1, 1, A.nrow))
+    out = []
+    for form in (0, 2):  # plain CSR, stencil masks
+        M = sol.MAT(A)
+        M.SetRowClass(form)
+        s = sol.configure(alg, maxIter=3000, relTol=1e-8, absTol=0.0, restart=30, pcd="jacobi",
+                          pcdWeight=2.0 / 3.0, pcdIter=1)
+        s.SetPrecision(capi.MIXED)
+        s.Setup(M)
+        x = np.zeros(A.nrow)
+        code = s.Solve(b, x)
+        out.append((code, s.GetIterations(), x))
+    assert out[0][0] == out[1][0] == 0
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.linalg.norm(b - A.matvec(out[1][2])) <= 1e-8 * np.linalg.norm(b)
