@@ -182,3 +182,14 @@ def test_dcgs2_fused_product_same_bits(gpu, alg, shape):
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][2], out[1][2])
     assert np.linalg.norm(b - A.matvec(out[1][2])) <= 1e-8 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("prec", ["FP64", "MIXED"])
+def test_dcgs2_restart_48(gpu, prec):
+    """The longest restart the delayed passes take (48 basis vectors: 98 values in one dots
+    reduction), against CGS2 on the same system."""
+    A = P.convdiff3d(32, 10.0)
+    b = A.matvec(np.random.default_rng(11).uniform(-1, 1, A.nrow))
+    kw = dict(restart=48, maxRestart=48, minRestart=48, prec=prec)
+    _agree(A, b, _run(gpu, A, b, "dcgs2", **kw), _run(gpu, A, b, "cgs2", **kw),
+           tol=1e-8, xtol=1e-6 if prec == "FP64" else 1e-5)
