@@ -271,7 +271,10 @@ k_dc_dots(DcArgs<T> P, Scratch s, GmLayout L, GmCtl* g, DcApply<T> Ap)
     __shared__ double col[kDcMaxK + 2], hcol[kDcMaxK], var[2];
     __shared__ GmCtl gs;
     __shared__ bool amLast;
-    // the update pass that follows may be scheduled as soon as blocks of this one leave
+    // launched programmatically after the product or the previous update pass: every input
+    // may still be in flight until the grid dependency resolves; the update pass that
+    // follows may be scheduled as soon as blocks of this one start
+    pdl_wait();
     pdl_release();
     if (g->stop) return;
     using S = DcShape<T>;
@@ -511,6 +514,7 @@ __global__ void __launch_bounds__(kDcThreads, 2) k_dc_update(DcArgs<T> P, GmLayo
     extern __shared__ __align__(16) unsigned char dc_raw[];
     DcRing& ring = *reinterpret_cast<DcRing*>(dc_raw);
     __shared__ T ca[kDcMaxK], cb[kDcMaxK];
+    pdl_release(); // the next step's first kernel waits for this one's completion itself
     using S = DcShape<T>;
     using VT = typename Vec16<T>::type;
     const int j = P.j;
@@ -606,6 +610,25 @@ static void dc_optin(const void* kern)
                              (int)sizeof(DcRing));
 }
 
+// Launches kern with programmatic stream serialization (the kernel waits for its predecessor
+// with pdl_wait before reading anything).
+template <typename... P, typename... A>
+static int dc_launch(void (*kern)(P...), int grid, size_t smem, cudaStream_t st, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kDcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    FB_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...));
+    return kOk;
+}
+
 // Resident blocks (two per SM), at least 1024 elements a block, and no more blocks than the
 // reduction scratch holds partials of nv values for.
 static int dc_grid(const Ctx& c, const void* fn, uint32_t n, int nv)
@@ -625,17 +648,19 @@ int dc_dots(Ctx& c, uint32_t n, int j, T* V, size_t ld, const T* w, const GmLayo
     DcArgs<T> P{V, ld, w, n, j};
     DcApply<T> none{};
     ++c.launches;
+    int e;
     if (w) {
         auto kern = k_dc_dots<T, true>;
         dc_optin((const void*)kern);
-        kern<<<dc_grid(c, (const void*)kern, n, 2 * j + 2), kDcThreads, sizeof(DcRing),
-               c.stream>>>(P, c.red, L, g, none);
+        e = dc_launch(kern, dc_grid(c, (const void*)kern, n, 2 * j + 2), sizeof(DcRing),
+                      c.stream, P, c.red, L, g, none);
     } else {
         auto kern = k_dc_dots<T, false>;
         dc_optin((const void*)kern);
-        kern<<<dc_grid(c, (const void*)kern, n, j + 1), kDcThreads, sizeof(DcRing),
-               c.stream>>>(P, c.red, L, g, none);
+        e = dc_launch(kern, dc_grid(c, (const void*)kern, n, j + 1), sizeof(DcRing), c.stream,
+                      P, c.red, L, g, none);
     }
+    if (e) return e;
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -653,15 +678,17 @@ int dc_dots_apply(Ctx& c, const CSRView<T>& A, int mode, const T* dinv, uint32_t
     ++c.launches;
     auto go = [&](auto kern) {
         dc_optin((const void*)kern);
-        kern<<<dc_grid(c, (const void*)kern, n, 2 * j + 2), kDcThreads, sizeof(DcRing),
-               c.stream>>>(P, c.red, L, g, Ap);
+        return dc_launch(kern, dc_grid(c, (const void*)kern, n, 2 * j + 2), sizeof(DcRing),
+                         c.stream, P, c.red, L, g, Ap);
     };
+    int e;
     if (sh == 5)
-        mode == 0 ? go(k_dc_dots<T, true, 5, 0>) : mode == 1 ? go(k_dc_dots<T, true, 5, 1>)
-                                                 : go(k_dc_dots<T, true, 5, 2>);
+        e = mode == 0 ? go(k_dc_dots<T, true, 5, 0>)
+                      : mode == 1 ? go(k_dc_dots<T, true, 5, 1>) : go(k_dc_dots<T, true, 5, 2>);
     else
-        mode == 0 ? go(k_dc_dots<T, true, 7, 0>) : mode == 1 ? go(k_dc_dots<T, true, 7, 1>)
-                                                 : go(k_dc_dots<T, true, 7, 2>);
+        e = mode == 0 ? go(k_dc_dots<T, true, 7, 0>)
+                      : mode == 1 ? go(k_dc_dots<T, true, 7, 1>) : go(k_dc_dots<T, true, 7, 2>);
+    if (e) return e;
     FB_CUDA(cudaGetLastError());
     return kOk;
 }

@@ -1620,6 +1620,8 @@ __global__ void __launch_bounds__(kBlock) k_gm_apply_vec(CSRView<T> A, const T* 
                                                          const T* __restrict__ dinv,
                                                          T* __restrict__ y, const int* stop)
 {
+    pdl_wait(); // launched programmatically in the DCGS2 cycles: v may still be in flight
+    pdl_release();
     if (*stop) return;
     using VT = Vec16<T>;
     using V = typename VT::V;
@@ -1780,7 +1782,16 @@ static void gm_apply_launch(Ctx& c, const Mat& A, CSRView<T> V, const T* v, cons
             auto gv = [&](auto kern) {
                 const int g = std::min(c.grid((long long)V.nrow / Vec16<T>::W, kBlock),
                                        resident_grid(c, (const void*)kern, kBlock));
-                kern<<<g, kBlock, 0, c.stream>>>(V, v, dinv, y, stop);
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)g);
+                cfg.blockDim = dim3(kBlock);
+                cfg.stream = c.stream;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                cudaLaunchKernelEx(&cfg, kern, V, v, dinv, y, stop);
             };
             if (sh == 5)
                 gv(k_gm_apply_vec<T, 5, MODE>);
