@@ -578,6 +578,8 @@ k_gs(uint32_t n, int k, const T* __restrict__ V, size_t ld, const double* __rest
     T* sacc = reinterpret_cast<T*>(gs_raw);           // [k][blockDim]
     T* sh = sacc + (size_t)k * blockDim.x;            // [kGsMaxK] coefficients (sign folded)
     __shared__ bool amLast;
+    pdl_wait(); // launched programmatically (gs_launch)
+    pdl_release();
     if (stop && *stop) return;
     using VT = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::W;
@@ -746,9 +748,9 @@ static int gs_launch(Ctx& c, uint32_t n, int k, const T* V, size_t ld, const dou
         const int kk = k - j0 < kGsMaxK ? k - j0 : kGsMaxK;
         const bool last = j0 + kGsMaxK >= k;
         ++c.launches;
-        k_gs<T, MODE><<<g, kBlock, gs_smem<T>(kk), c.stream>>>(
-            n, kk, V + j0 * ld, ld, h ? h + j0 : nullptr, sign, w, c.red,
-            dres ? dres + j0 : nullptr, last ? dnorm : nullptr, stop);
+        FB_CUDA(launch_pdl(k_gs<T, MODE>, dim3((unsigned)g), dim3(kBlock), gs_smem<T>(kk),
+                           c.stream, n, kk, V + j0 * ld, ld, h ? h + j0 : nullptr, sign, w,
+                           c.red, dres ? dres + j0 : nullptr, last ? dnorm : nullptr, stop));
         FB_CUDA(cudaGetLastError());
     }
     return kOk;

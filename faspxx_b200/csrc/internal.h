@@ -6,11 +6,32 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
 
 namespace fb {
+
+// Launches kern with programmatic stream serialization: the kernel calls pdl_wait() before
+// its first read of anything a predecessor wrote, so its launch overlaps the predecessor's
+// tail without changing what it reads.
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kern)(P...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, A&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 // An NVTX range over a scope: the solver's phases (matrix upload, setup, solve, the
 // reliable-update refreshes, batched solves) appear as named ranges under a tracing tool

@@ -1459,6 +1459,8 @@ int SolverImpl::bicgstab_engine(BiEngine<T>& E, const T* b, T* x, fasp_gpu_info*
 __global__ void __launch_bounds__(128) k_gmres_givens(GmLayout L, int count, int c1, int cgs,
                                                       const double* tnorm, GmCtl* g)
 {
+    pdl_wait(); // launched programmatically
+    pdl_release();
     if (g && g->stop) return;
     const size_t m = L.m;
 #define HH(i, j) L.hh[(size_t)(i) * m + (j)]
@@ -1563,8 +1565,9 @@ static int orthogonalize(SolverImpl& S, const GmLayout& L, int count, int c1, co
         v_multiaxpy(c, n, count, V, ld, L.h2, 1.0, wv, tn);
     }
     ++c.launches;
-    k_gmres_givens<<<1, 128, 0, c.stream>>>(L, count, c1, S.cfg.orth != FASP_GPU_ORTH_MGS, tn,
-                                            nullptr);
+    FB_CUDA(launch_pdl(k_gmres_givens, dim3(1), dim3(128), 0, c.stream, L, count, c1,
+                       (int)(S.cfg.orth != FASP_GPU_ORTH_MGS), (const double*)tn,
+                       (GmCtl*)nullptr));
     FB_CUDA(cudaGetLastError());
     v_scale(c, n, Scal::dinv(tn), wv);
     return kOk;
@@ -1664,6 +1667,8 @@ template <typename T>
 __global__ void k_gm_scale(uint32_t n, const double* __restrict__ tn, T* __restrict__ w,
                            const int* stop)
 {
+    pdl_wait(); // launched programmatically
+    pdl_release();
     if (*stop) return;
     const T inv = (T)(1.0 / *tn);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -1679,6 +1684,8 @@ template <typename T>
 __global__ void k_fg_norminf(uint32_t n, const T* __restrict__ z, Scratch s, double* dres,
                              const int* stop)
 {
+    pdl_wait(); // launched programmatically
+    pdl_release();
     if (*stop) return;
     T m = T(0);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -1696,6 +1703,8 @@ __global__ void __launch_bounds__(kBlock) k_fg_sweep(CSRView<T> A, const T* __re
                                                      const double* __restrict__ zinf,
                                                      T* __restrict__ t, const int* stop)
 {
+    pdl_wait(); // launched programmatically
+    pdl_release();
     if (*stop) return;
     const bool shortcut = *zinf < kCloseZero; // MAT::Residual (MAT.cxx:459-462)
     auto xv = [&](uint32_t j) { return zj[j]; };
@@ -1731,6 +1740,8 @@ __global__ void __launch_bounds__(kBlock) k_fg_apply(CSRView<T> A, const T* __re
                                                      T* __restrict__ z, T* __restrict__ y,
                                                      const int* stop)
 {
+    pdl_wait(); // launched programmatically
+    pdl_release();
     if (*stop) return;
     auto xv = [&](uint32_t j) { return t[j]; };
     if (L == 1) { // thread per row, or block tiles of plain CSR (A.tiles)
@@ -1902,13 +1913,16 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
             T* zj = Z + (k - 1) * ld;
             const T* t = vin;
             if (S.pcd.type != 0) {
-                k_fg_norminf<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(
-                    n, (const T*)zj, c.red, c.dslot + SL_T6, stop);
+                FB_CUDA(launch_pdl(k_fg_norminf<T>, dim3((unsigned)c.grid(n, kBlock)),
+                                   dim3(kBlock), 0, c.stream, n, (const T*)zj, c.red,
+                                   c.dslot + SL_T6, stop));
                 lanes_launch<T>(c, *S.A, [&](auto LL) {
                     auto kern = k_fg_sweep<T, decltype(LL)::value>;
-                    kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock)), kBlock,
-                           0, c.stream>>>(AV, vin, (const T*)zj, dinv, c.dslot + SL_T6, tmp,
-                                          stop);
+                    launch_pdl(kern,
+                               dim3((unsigned)std::min(
+                                   needS, resident_grid(c, (const void*)kern, kBlock))),
+                               dim3(kBlock), 0, c.stream, AV, vin, (const T*)zj, dinv,
+                               (const double*)(c.dslot + SL_T6), tmp, stop);
                 });
                 t = tmp;
                 c.launches += 2;
@@ -1918,8 +1932,10 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
                 CSRView<T> W = AV;
                 size_t smem = S.A->lanes == 1 ? with_tiles(W, kBlock) : 0;
                 if (smem && !tiles_fit((const void*)kern, smem)) W.tiles = 0, smem = 0;
-                kern<<<std::min(needS, resident_grid(c, (const void*)kern, kBlock, smem)),
-                       kBlock, smem, c.stream>>>(W, t, zj, vnew, stop);
+                launch_pdl(kern,
+                           dim3((unsigned)std::min(
+                               needS, resident_grid(c, (const void*)kern, kBlock, smem))),
+                           dim3(kBlock), smem, c.stream, W, t, zj, vnew, stop);
             });
         } else if (mode == 0)
             gm_apply_launch<T, 0>(c, *S.A, AV, vin, dinv, vnew, stop);
@@ -1930,8 +1946,10 @@ static int gm_cycle_device(SolverImpl& S, const GmLayout& L, T* V, uint32_t step
         v_multidot(c, n, (int)k, (const T*)V, ld, (const T*)vnew, L.h1, stop);
         v_multiaxpy_dot(c, n, (int)k, (const T*)V, ld, L.h1, vnew, L.h2, stop);
         v_multiaxpy(c, n, (int)k, (const T*)V, ld, L.h2, 1.0, vnew, tn, stop);
-        k_gmres_givens<<<1, 128, 0, c.stream>>>(L, (int)k, (int)k - 1, 1, tn, S.gmc);
-        k_gm_scale<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, tn, vnew, stop);
+        FB_CUDA(launch_pdl(k_gmres_givens, dim3(1), dim3(128), 0, c.stream, L, (int)k,
+                           (int)k - 1, 1, (const double*)tn, S.gmc));
+        FB_CUDA(launch_pdl(k_gm_scale<T>, dim3((unsigned)c.grid(n, kBlock)), dim3(kBlock), 0,
+                           c.stream, n, (const double*)tn, vnew, stop));
         c.launches += 3;
     }
     FB_CUDA(cudaGetLastError());
