@@ -74,6 +74,8 @@ template <typename T>
 __global__ void k_dot(uint32_t n, const T* __restrict__ a, const T* __restrict__ b, Scratch s,
                       double* dres)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     T t = T(0);
     GRID_STRIDE(i, n) t = fma(a[i], b[i], t);
     double acc[1] = {(double)t};
@@ -84,6 +86,8 @@ __global__ void k_dot(uint32_t n, const T* __restrict__ a, const T* __restrict__
 template <typename T>
 __global__ void k_norm2(uint32_t n, const T* __restrict__ a, Scratch s, double* dres)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     T t = T(0);
     GRID_STRIDE(i, n) t = fma(a[i], a[i], t);
     double acc[1] = {(double)t};
@@ -94,6 +98,8 @@ __global__ void k_norm2(uint32_t n, const T* __restrict__ a, Scratch s, double* 
 template <typename T>
 __global__ void k_norminf(uint32_t n, const T* __restrict__ a, Scratch s, double* dres)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     T t = T(0);
     GRID_STRIDE(i, n) t = fmax(t, fabs(a[i]));
     double acc[1] = {(double)t};
@@ -105,7 +111,8 @@ template <typename T>
 int v_dot(Ctx& c, uint32_t n, const T* a, const T* b, double* dres)
 {
     ++c.launches;
-    k_dot<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, b, c.red, dres);
+    FB_CUDA(launch_pdl(k_dot<T>, dim3((unsigned)c.grid(n, kBlock)), dim3(kBlock), 0, c.stream, n,
+                       a, b, c.red, dres));
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -114,7 +121,8 @@ template <typename T>
 int v_norm2(Ctx& c, uint32_t n, const T* a, double* dres)
 {
     ++c.launches;
-    k_norm2<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
+    FB_CUDA(launch_pdl(k_norm2<T>, dim3((unsigned)c.grid(n, kBlock)), dim3(kBlock), 0, c.stream,
+                       n, a, c.red, dres));
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -123,7 +131,8 @@ template <typename T>
 int v_norminf(Ctx& c, uint32_t n, const T* a, double* dres)
 {
     ++c.launches;
-    k_norminf<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, a, c.red, dres);
+    FB_CUDA(launch_pdl(k_norminf<T>, dim3((unsigned)c.grid(n, kBlock)), dim3(kBlock), 0,
+                       c.stream, n, a, c.red, dres));
     FB_CUDA(cudaGetLastError());
     return kOk;
 }
@@ -133,6 +142,8 @@ int v_norminf(Ctx& c, uint32_t n, const T* a, double* dres)
 template <typename T>
 __global__ void k_axpy(uint32_t n, Scal a, const T* __restrict__ x, T* __restrict__ y)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const T av = (T)eval(a);
     GRID_STRIDE(i, n) y[i] = fma(av, x[i], y[i]);
 }
@@ -140,6 +151,8 @@ __global__ void k_axpy(uint32_t n, Scal a, const T* __restrict__ x, T* __restric
 template <typename T>
 __global__ void k_xpay(uint32_t n, Scal a, const T* __restrict__ x, T* __restrict__ y)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const T av = (T)eval(a);
     GRID_STRIDE(i, n) y[i] = fma(av, y[i], x[i]);
 }
@@ -147,6 +160,8 @@ __global__ void k_xpay(uint32_t n, Scal a, const T* __restrict__ x, T* __restric
 template <typename T>
 __global__ void k_axpby(uint32_t n, Scal a, Scal b, const T* __restrict__ y, T* __restrict__ x)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const T av = (T)eval(a), bv = (T)eval(b);
     GRID_STRIDE(i, n) x[i] = fma(av, x[i], bv * y[i]);
 }
@@ -155,6 +170,8 @@ template <typename T>
 __global__ void k_waxpby(uint32_t n, Scal a, const T* __restrict__ v1, Scal b,
                          const T* __restrict__ v2, T* __restrict__ w)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const T av = (T)eval(a), bv = (T)eval(b);
     GRID_STRIDE(i, n) w[i] = fma(av, v1[i], bv * v2[i]);
 }
@@ -162,6 +179,8 @@ __global__ void k_waxpby(uint32_t n, Scal a, const T* __restrict__ v1, Scal b,
 template <typename T>
 __global__ void k_scale(uint32_t n, Scal a, T* __restrict__ x)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const T av = (T)eval(a);
     GRID_STRIDE(i, n) x[i] *= av;
 }
@@ -169,18 +188,24 @@ __global__ void k_scale(uint32_t n, Scal a, T* __restrict__ x)
 template <typename T>
 __global__ void k_set(uint32_t n, T v, T* __restrict__ x)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     GRID_STRIDE(i, n) x[i] = v;
 }
 
 template <typename T>
 __global__ void k_pmult(uint32_t n, const T* __restrict__ d, T* __restrict__ x)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     GRID_STRIDE(i, n) x[i] *= d[i];
 }
 
 template <typename T>
 __global__ void k_add(uint32_t n, const T* __restrict__ d, T* __restrict__ x)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     GRID_STRIDE(i, n) x[i] += d[i];
 }
 
@@ -188,13 +213,16 @@ __global__ void k_add(uint32_t n, const T* __restrict__ d, T* __restrict__ x)
 __global__ void k_recip_scale(uint32_t n, double w, const double* __restrict__ d,
                               double* __restrict__ out)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     GRID_STRIDE(i, n) out[i] = (1.0 / d[i]) * w;
 }
 
 #define LAUNCH_EW(kernel, n, ...)                                                          \
     do {                                                                                   \
         if ((n) == 0) return kOk;                                                          \
-        kernel<<<c.grid((n), kBlock), kBlock, 0, c.stream>>>((n), __VA_ARGS__);            \
+        FB_CUDA(launch_pdl(kernel, dim3((unsigned)c.grid((n), kBlock)), dim3(kBlock), 0,   \
+                           c.stream, (n), __VA_ARGS__));                                   \
         ++c.launches;                                                                      \
         FB_CUDA(cudaGetLastError());                                                       \
         return kOk;                                                                        \

@@ -52,6 +52,8 @@ __global__ void k_jacobi_update(uint32_t n, const T* __restrict__ dinv,
                                 const T* __restrict__ work, T* __restrict__ x,
                                 Scratch s, double* dxinf)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     // work .*= diagInv; x += work (Iter.cxx:91-92); also NormInf(x_new) for the next
     // residual's shortcut test
     T m = T(0);
@@ -89,6 +91,8 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_sweep(CSRView<T> A, const T* 
                                                          Scratch s, double* xinfOut,
                                                          double* rnorm)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     const bool shortcut = *xinfIn < kCloseZero;
     T m = T(0), rr = T(0);
     auto xv = [&](uint32_t j) { return xin[j]; };
@@ -146,6 +150,8 @@ __global__ void __launch_bounds__(kJacobiBlockThreads) k_jacobi_block(
     CSRView<T> A, const T* __restrict__ b, T* __restrict__ x, const T* __restrict__ dinv,
     T* __restrict__ work, fasp_gpu_params prm)
 {
+    pdl_wait(); // may be launched programmatically (launch_pdl)
+    pdl_release();
     __shared__ double sh[32];
     const uint32_t n = A.nrow;
     auto xv = [&](uint32_t j) { return x[j]; };
@@ -261,7 +267,8 @@ int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm
     if (fusable && !hist && !norm2 && !normInf && n <= kJacobiBlockRows) {
         // nothing reads the norms back: the whole solve in one single-block launch
         ++c.launches;
-        k_jacobi_block<T><<<1, kJacobiBlockThreads, 0, c.stream>>>(V, b, x, dinv, work, prm);
+        FB_CUDA(launch_pdl(k_jacobi_block<T>, dim3(1), dim3(kJacobiBlockThreads), 0, c.stream, V, b,
+                           x, dinv, work, prm));
         FB_CUDA(cudaGetLastError());
         numIter = prm.maxIter; // the convergence test ran on the device
         return kOk;
@@ -276,8 +283,8 @@ int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm
         int p = 0;
         auto sweep = [&](auto kern) {
             const int g = std::min(c.grid(n, kBlock), resident_grid(c, (const void*)kern, kBlock));
-            kern<<<g, kBlock, 0, c.stream>>>(V, b, cur, dinv, nxt, xinf[p], c.red, xinf[p ^ 1],
-                                            c.dslot + SL_JRES);
+            launch_pdl(kern, dim3((unsigned)g), dim3(kBlock), 0, c.stream, V, b, (const T*)cur,
+                       dinv, nxt, (const double*)xinf[p], c.red, xinf[p ^ 1], c.dslot + SL_JRES);
         };
         numIter = 0;
         while (numIter < prm.maxIter) {
@@ -327,8 +334,8 @@ int Pcd::solve(Ctx& c, const T* b, T* x, std::vector<double>* hist, double* norm
             if (resRel < prm.relTol || resAbs < prm.absTol) break;
         }
         ++c.launches;
-        k_jacobi_update<T><<<c.grid(n, kBlock), kBlock, 0, c.stream>>>(n, dinv, work, x, c.red,
-                                                                        xinf);
+        FB_CUDA(launch_pdl(k_jacobi_update<T>, dim3((unsigned)c.grid(n, kBlock)), dim3(kBlock), 0,
+                           c.stream, n, dinv, (const T*)work, x, c.red, xinf));
         FB_CUDA(cudaGetLastError());
         ++numIter;
     }
