@@ -585,7 +585,9 @@ def run_ours(args):
                          "gpu": p2, "cpu_baseline": p2cpu},
             "krylov96": {"config": "96^3 upwind convection-diffusion, Pe 0.1 and 10, weighted "
                                    "Jacobi 2/3, rtol 1e-8, GMRES restart fixed at 30 "
-                                   "(gmres) or the reference's default 10-30 (gmresvar)",
+                                   "(gmres) or the reference's default 10-30 (gmresvar), "
+                                   "Arnoldi by classical Gram-Schmidt with the "
+                                   "reorthogonalisation delayed into the next step",
                          "results": krylov_results(96, 2, algs=("bicgstab", "gmres", "gmresvar"),
                                                    reference=ref_its)},
             "batch4096": batch_results(args, None, 0, 1, local, loop_sample=4),
@@ -877,6 +879,8 @@ def run_krylov(args):
             "dtype": "f32 inner / f64 refinement", "data": "synthetic",
             "config": {"workload": f"{N}^3 upwind convection-diffusion, Pe 0.1 and 10, "
                                    "weighted Jacobi 2/3, x0=0, b=A x*, x*~U[-1,1)",
+                       "arnoldi": "GMRES: " + (args.orth if args.orth != "default" else "dcgs2")
+                                  + "; FGMRES: cgs2" if args.orth != "mgs" else "mgs",
                        "l2": "L2 flushed between timed solves"},
             "results": rows}
     print(json.dumps(line))
