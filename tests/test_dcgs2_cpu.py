@@ -3,8 +3,9 @@ into the next step), restated in numpy exactly as the GPU passes form them (dcgs
 against the reference's modified Gram-Schmidt Arnoldi (GMRES.cxx:160-210) on the same
 operator: the Givens residual estimates of a 30-step cycle agree to 1e-8 relative (above a
 floor of rounding in ||r0||), the basis is orthonormal to rounding, and a lucky breakdown
-(t = 0) ends with the estimate at rounding level instead of NaN. Step j: a = Q^T u, b = Q^T w, c = u^T w, d = u^T u;
-t = sqrt(d - a^T a); column j - 1 += a with subdiagonal t; h = (b - H a) / t,
+(t = 0) ends with the estimate at rounding level instead of NaN. Step j: a = Q^T u,
+b = Q^T w, c = u^T w, d = u^T u; t = sqrt(d - a^T a); column j - 1 += a with subdiagonal t;
+h = (b - H a) / t,
 h_j = ((c - a^T b) / t - t a_{j-1}) / t; q_j = (u - Q a) / t; u_{j+1} = (w - Q b - q_j g) / t
 with g = (c - a^T b) / t.
 """
